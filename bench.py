@@ -1,0 +1,367 @@
+"""Benchmark of the rcsr device hot path on B200.
+
+Default workload (`--workload score`): batched evaluation + squared-error
+scoring of P = 4096 random expression programs over N = 1,048,576 rows x 5
+features (the batched-scoring configuration), metric expr*row evals/s.
+`--workload fit`: batched LM fit of P = 2048 candidates (1-20 constants,
+5-60 nodes, 20 iterations) over N = 262,144 rows x 8 features, metric fitted
+candidates/s.
+
+One step is one pass of the hot path over the whole batch. `value` is
+device-timed with CUDA events on the library's stream (inputs resident in
+HBM, L2 flushed between steps); `e2e` is the same metric through the public
+C-ABI call with host buffers (program upload, decode, launches, result
+download inside the timed region). The CPU baseline times the f64 oracle (a
+restatement of the reference's CPU path) on a bounded sample on the host's
+cores.
+
+Multi-GPU: candidates shard across ranks with no data-path collective
+(weak scaling); every rank scores its own P-candidate batch.
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import importlib
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+PKG = "the-rule-and-compass_b200"
+
+
+def load_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {"hbm_gbs": 6650.0, "sm_max_mhz": 1965.0, "fallback": True}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def flush_l2(buf):
+    """Write a buffer larger than the 126 MB L2 between timed steps."""
+    if buf is not None:
+        buf.zero_()
+
+
+def postfix_ops(prog, off):
+    """Per program: bytecode ops excluding HALT (const/var count one op)."""
+    out = []
+    for i in range(len(off) - 1):
+        w = prog[off[i]:off[i + 1]]
+        k, ops = 0, 0
+        while k < len(w):
+            if w[k] in (0, 1):
+                k += 2
+            elif w[k] == 255:
+                break
+            else:
+                k += 1
+            ops += 1
+        out.append(ops)
+    return np.asarray(out)
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle on a bounded sample, parallel over candidates.
+# ---------------------------------------------------------------------------
+
+def cpu_score_baseline(trees, x, y, n_rows, n_cand, threads):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.lib()
+    x64 = np.ascontiguousarray(x[:, :n_rows].astype(np.float64)).reshape(-1)
+    y64 = y[:n_rows].astype(np.float64)
+    sample = trees[:n_cand]
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+        list(ex.map(lambda t: O.score(t, x64, n_rows, x.shape[0], y64, O.SQUARED), sample))
+    dt = time.perf_counter() - t0
+    return n_cand * n_rows / dt, dt
+
+
+def cpu_fit_baseline(trees, x, y, n_rows, n_cand, iters, threads):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.lib()
+    x64 = np.ascontiguousarray(x[:, :n_rows]).reshape(-1)
+    y64 = y[:n_rows]
+    sample = trees[:n_cand]
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+        list(ex.map(lambda t: O.fit(t, x64, n_rows, x.shape[0], y64, iters), sample))
+    dt = time.perf_counter() - t0
+    # per-candidate cost grows linearly in rows: scale to the full row count
+    return n_cand / dt, dt
+
+
+# ---------------------------------------------------------------------------
+
+def run_reference(args, rank, world):
+    """The reference arm: the reference's CPU path (its f64 restatement; the
+    Rust reference cannot be built here) on all host threads, on a bounded
+    sample of this arm's workload per step."""
+    if rank != 0:
+        return
+    W = importlib.import_module(PKG + ".workloads")
+    threads = os.cpu_count() or 1
+    if args.workload == "score":
+        P, N = 4096, 1 << 20
+        trees, x, y = W.scoring_workload(256, 1 << 16, seed=0)
+        n_rows, n_cand = 1 << 16, 64
+        metric, unit = "expr_row_evals_per_s", "expr*row/s"
+        fn = lambda: cpu_score_baseline(trees, x, y, n_rows, n_cand, threads)  # noqa: E731
+        sample = f"{n_cand} programs x {n_rows} rows of the P={P}, N={N} workload per step"
+        cfg = {"workload": "batched scoring, P=4096 programs, N=1048576 rows x 5 features",
+               "metric_kind": "squared"}
+    else:
+        trees, x, y = W.fit_workload(64, 1 << 14, seed=0)
+        n_rows, n_cand = 1 << 14, 16
+        metric, unit = "fitted_candidates_per_s", "candidates/s"
+
+        def fn():
+            v, dt = cpu_fit_baseline(trees, x, y, n_rows, n_cand, 20, threads)
+            return v * n_rows / 262144.0, dt
+        sample = (f"{n_cand} candidates x {n_rows} rows x 20 LM iterations, scaled linearly "
+                  f"to N=262144")
+        cfg = {"workload": "batched LM fit, P=2048, N=262144 rows x 8 features, 20 iters"}
+    for _ in range(args.warmup):
+        fn()
+    vals, total = [], 0.0
+    for _ in range(args.steps):
+        v, dt = fn()
+        vals.append(v)
+        total += dt
+    value = float(np.mean(vals))
+    line = {"impl": "reference", "metric": metric, "value": value, "unit": unit,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": cfg,
+            "cpu_baseline": {"value": value, "unit": unit, "cores": threads, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def bench_score(args, rank, world, dev, pkg, W, flushbuf):
+    P, N, V = args.P or 4096, args.N or (1 << 20), 5
+    trees, x, y = W.scoring_workload(P, N, seed=rank)
+    ev = pkg.GpuEvaluator(x.reshape(-1), N, V, y)
+    pop = pkg.Population(trees)
+    prog, off = pop.programs()
+    assert len(pop) == P
+    ops = postfix_ops(prog, off)
+    alg_ops = float(N) * float((ops + 2).sum())      # lane-ops per launch
+    pcount = np.zeros(P, np.int32)
+    # warm-up
+    for _ in range(args.warmup):
+        ev.score_batch(prog, off, 0, pcount)
+    dev_ms, wall = [], []
+    import torch
+    torch.cuda.synchronize()
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clk:
+        for _ in range(args.steps):
+            flush_l2(flushbuf)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            vals, status, ms = ev.score_batch(prog, off, 0, pcount)
+            wall.append(time.perf_counter() - t0)
+            dev_ms.append(ms)
+    stats = ev.last_stats()
+    clocks = clk.summary()
+    ev.close()
+    h2d = int(prog.nbytes + off.nbytes + pcount.nbytes)
+    d2h = int(P * (8 + 4))
+    return dict(P=P, N=N, dev_ms=dev_ms, wall=wall, alg_ops=alg_ops, clocks=clocks,
+                h2d=h2d, d2h=d2h, trees=trees, x=x, y=y, stats=stats,
+                launches_per_step=2, unit_count=float(P) * N)
+
+
+def bench_fit(args, rank, world, dev, pkg, W, flushbuf):
+    P, N = args.P or 2048, args.N or 262144
+    trees, x, y = W.fit_workload(P, N, seed=rank)
+    ev = pkg.GpuEvaluator(x.astype(np.float32).reshape(-1), N, x.shape[0], y.astype(np.float32))
+    ev.set_fit_data(x.reshape(-1), y)
+    plans = [pkg.gpu_fit_plan(t) for t in trees]
+    prog, off, pcount, c0, gauge, kmax = pkg.pack_plans(plans)
+    for _ in range(args.warmup):
+        ev.fit_batch_fused(prog, off, pcount, c0, gauge, kmax, 20)
+    dev_ms, wall = [], []
+    import torch
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clk:
+        for _ in range(args.steps):
+            flush_l2(flushbuf)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            _, _, st, ms = ev.fit_batch_fused(prog, off, pcount, c0, gauge, kmax, 20)
+            wall.append(time.perf_counter() - t0)
+            dev_ms.append(ms)
+    clocks = clk.summary()
+    ev.close()
+    h2d = int(prog.nbytes + off.nbytes + pcount.nbytes + c0.nbytes + gauge.nbytes)
+    d2h = int(P * (kmax * 8 + 8 + 4))
+    return dict(P=P, N=N, dev_ms=dev_ms, wall=wall, clocks=clocks, h2d=h2d, d2h=d2h,
+                trees=trees, x=x, y=y, launches_per_step=4, unit_count=float(P))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="score", choices=["score", "fit"])
+    ap.add_argument("--P", type=int, default=0)
+    ap.add_argument("--N", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    pkg = importlib.import_module(PKG)
+    W = importlib.import_module(PKG + ".workloads")
+    flushbuf = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    if args.workload == "score":
+        r = bench_score(args, rank, world, local, pkg, W, flushbuf)
+    else:
+        r = bench_fit(args, rank, world, local, pkg, W, flushbuf)
+    torch.cuda.synchronize()
+
+    dev_s = sum(r["dev_ms"]) / 1e3
+    wall_s = sum(r["wall"])
+    if world > 1:
+        t = torch.tensor([dev_s, wall_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_s, wall_s = float(t[0]), float(t[1])
+        dist.barrier()
+    units = r["unit_count"] * args.steps * world
+    value = units / dev_s
+    e2e = units / wall_s
+    peaks = load_peaks()
+    if rank == 0:
+        if args.workload == "score":
+            metric, unit = "expr_row_evals_per_s", "expr*row/s"
+            per_launch_ms = float(np.mean(r["dev_ms"]))
+            achieved = r["alg_ops"] / (per_launch_ms / 1e3) / 1e9
+            peak = 148 * 128 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e9
+            roof = {"bound": "fp32_issue", "achieved": achieved, "peak": peak,
+                    "unit": "Glane-op/s", "frac": achieved / peak, "traffic": None,
+                    "note": "interpreter ops (bytecode ops + residual + loss) per row per "
+                            "candidate / event time of the scoring launches; peak = 148 SMs x "
+                            "128 FP32 lanes x sm_max_mhz from MEASURED_PEAKS.json"}
+            cfg = {"workload": f"batched scoring, P={r['P']} programs, N={r['N']} rows x 5 "
+                               f"features, squared error", "l2": "flushed between steps"}
+        else:
+            metric, unit = "fitted_candidates_per_s", "candidates/s"
+            roof = None
+            cfg = {"workload": f"batched LM fit, P={r['P']}, N={r['N']} rows x 8 features, "
+                               f"20 iters, fused adjoint", "l2": "flushed between steps"}
+        line = {"metric": metric, "value": value, "unit": unit, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 * dev_s / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32 rows, f64 sums",
+                "data": "synthetic", "config": cfg, "roofline": roof,
+                "clocks": r["clocks"],
+                "e2e": {"value": e2e, "unit": unit, "h2d_bytes_per_step": r["h2d"],
+                        "d2h_bytes_per_step": r["d2h"]},
+                "gpu_launches": r["launches_per_step"] * args.steps}
+        if not args.no_cpu_baseline and world == 1:
+            threads = os.cpu_count() or 1
+            if args.workload == "score":
+                v, dt = cpu_score_baseline(r["trees"], r["x"], r["y"], 1 << 16, 64, threads)
+                line["cpu_baseline"] = {"value": v, "unit": unit, "cores": threads,
+                                        "kind": "port",
+                                        "sample": "64 programs x 65536 rows, f64 oracle"}
+            else:
+                v, dt = cpu_fit_baseline(r["trees"], r["x"], r["y"], 1 << 14, 16, 20, threads)
+                line["cpu_baseline"] = {"value": v * (1 << 14) / r["N"], "unit": unit,
+                                        "cores": threads, "kind": "port",
+                                        "sample": "16 candidates x 16384 rows x 20 iters, "
+                                                  "scaled linearly in rows"}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

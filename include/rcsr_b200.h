@@ -1,0 +1,216 @@
+/*
+ * rcsr_b200.h -- the C ABI of the B200-native device library for rcsr's
+ * per-generation hot path (batched bytecode evaluation, loss scoring,
+ * batched LM/IRLS constant fitting, exact rank sums, input gradients).
+ *
+ * The first block is a drop-in for the reference's device library: every
+ * symbol, argument order, struct layout and return convention matches the
+ * definitions in my-version/src/cuda/eval.cu and the binding block in
+ * my-version/src/gpu.rs:668-824 (cited per entry point below). Linking the
+ * reference's Rust crate against librcsr_b200.so instead of its own build.rs
+ * object changes no Rust code.
+ *
+ * Conventions (the reference's):
+ *   - float-returning calls return kernel milliseconds >= 0 on success and a
+ *     negative value when every output must be discarded;
+ *   - int-returning calls return 0 on success and -1 on failure;
+ *   - host buffers are caller-owned and only borrowed for the call; device
+ *     memory is owned by the context and grows at the high-water mark;
+ *   - every call completes before it returns, except rc_eval_submit /
+ *     rc_eval_collect;
+ *   - a context is used by one host thread at a time.
+ *
+ * Program formats:
+ *   - "postfix words" (scoring): [OP_CONST, f32 bits] | [OP_VAR, column] |
+ *     operator word ... OP_HALT, packed with off[nprog + 1] word offsets
+ *     (my-version/src/gpu.rs:349-438);
+ *   - "fit records" (fitting, ranks, gradients): post-order 4-word records
+ *     [op, kid0, kid1, slot] with constants in c0[cand * kmax + slot]
+ *     (my-version/src/fit.rs:985-1056).
+ */
+#ifndef RCSR_B200_H
+#define RCSR_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Host-side ledger of one batch, in milliseconds (eval.cu:95-107). */
+typedef struct RcStats {
+    double kernel_ms;
+    double launch_ms;
+    double sync_ms;
+    double alloc_ms;
+    double h2d_ms;
+    double d2h_ms;
+    double wall_ms;
+    unsigned long long h2d_bytes;
+    unsigned long long d2h_bytes;
+    int batch;
+    int failed;
+} RcStats;
+
+/* Arena / copy-mode snapshot (eval.cu:116-135). */
+typedef struct RcArenaReport {
+    int async_copy;
+    char reason[96];
+    unsigned long long pinned_bytes;
+    unsigned long long alloc_calls;
+    unsigned long long steady_alloc_calls;
+    unsigned long long overlapped_uploads;
+    unsigned long long batches;
+    unsigned long long fs_alloc_calls;
+    unsigned long long fs_growths;
+    unsigned long long fs_steady_alloc_calls;
+    unsigned long long fs_batches;
+    unsigned long long fs_dev_bytes;
+    unsigned long long fs_pinned_bytes;
+} RcArenaReport;
+
+/* Exact maximum-error scan output per segment (eval.cu:4529-4535). */
+typedef struct RcMaxOut {
+    double vmax;
+    double lo;
+    double hi;
+    int row;
+    int status;
+} RcMaxOut;
+
+/* ---- context -------------------------------------------------------- */
+
+/* eval.cu:3137 rc_create: copies f32 column-major cols[v*n + row] and y[n];
+   NULL on failure. Reads RCSR_GPU_SYNC. */
+void *rc_create(const float *cols, int n, int v, const float *y);
+/* eval.cu:3221 rc_destroy. */
+void rc_destroy(void *ctx);
+/* eval.cu:3882 rc_set_fit_data: f64 twins of the rows (+ optional base row
+   weights) used by the f64 polish, the rank keys and the order statistics. */
+int rc_set_fit_data(void *ctx, const double *cols, const double *y, const double *w);
+/* eval.cu:3935 rc_set_score_weights: NULL clears (every row weighs 1). */
+int rc_set_score_weights(void *ctx, const double *w);
+/* eval.cu:3955 rc_set_fit_sign: label sign t = 2l-1 per row; NULL clears. */
+int rc_set_fit_sign(void *ctx, const double *sign);
+
+/* ---- scoring -------------------------------------------------------- */
+
+/* eval.cu:3268 rc_set_programs: stage a packed postfix batch. */
+int rc_set_programs(void *ctx, const unsigned int *prog, const unsigned int *off, int nprog);
+/* eval.cu:3429 rc_eval: f32 sum of the row loss (0 squared, 1 log-squashed,
+   4 absolute) per staged program; a non-finite or |pred| > 1e30 row adds 1e30. */
+float rc_eval(void *ctx, float *out, int loss);
+/* eval.cu:3344 / :3395 split submit/collect of rc_eval. */
+int rc_eval_submit(void *ctx, int loss);
+float rc_eval_collect(void *ctx, float *out);
+/* eval.cu:3803 rc_score_batch: native objectives (RC_SCORE_* codes 0..14);
+   out[P] f64, status[P] (0 ok, 2 non-finite, 4 all-zero weight). pcount is
+   read only by the AIC family. */
+float rc_score_batch(void *ctx, const unsigned int *prog, const unsigned int *off, int nprog,
+                     int kind, const int *pcount, double *out, int *status);
+/* eval.cu:3514 / :3550 / :3565: fixed-stride, double-buffered program pool. */
+int rc_pool_reserve(void *ctx, int nprog, int width);
+int rc_pool_upload(void *ctx, int which, const unsigned int *prog, int nprog);
+float rc_pool_eval(void *ctx, int which, int nprog, int width, float *out, int loss);
+/* eval.cu:3823 rc_pool_score. */
+float rc_pool_score(void *ctx, int which, int nprog, int width, int kind, const int *pcount,
+                    double *out, int *status);
+/* eval.cu:3864 rc_pool_hash: FNV-1a of each slot up to and including HALT. */
+int rc_pool_hash(void *ctx, int which, int nprog, int width, unsigned long long *out);
+/* eval.cu:3438 rc_predict: raw P x N predictions, row-major, no 1e30 rule. */
+int rc_predict(void *ctx, const unsigned int *prog, const unsigned int *off, int nprog,
+               float *out);
+
+/* ---- fitting -------------------------------------------------------- */
+
+/* eval.cu:4001 rc_fit_batch: batched LM/IRLS over fit records. metric:
+   0 squared, 1 log-squashed, 2 correlation, 3 correlation_signed,
+   4 absolute, 5 logistic. outc[P*kmax], outsse[P] (the configured objective),
+   outstatus[P] (0 ok, 1 no finite step, 2 no finite iterate, 4 rank
+   deficient, 5 recovered, 6 no improvement, 7 start unusable, 8 recovered
+   with skipped rows). kmax > 20 is refused. */
+float rc_fit_batch(void *ctx, const unsigned int *prog, const unsigned int *off,
+                   const int *pcount, int nprog, int kmax, const double *c0, const int *gauge,
+                   int iters, int metric, double *outc, double *outsse, int *outstatus);
+/* eval.cu:4084 rc_fit_kernel_info: block width, dynamic shared bytes and the
+   constant cap of the launch shape a batch with kmax constants uses. */
+int rc_fit_kernel_info(int kmax, int *threads, int *smem_bytes, int *max_constants);
+
+/* ---- exact statistics ----------------------------------------------- */
+
+/* eval.cu:4270 rc_rank_score_batch: exact 128-bit rank sums per segment
+   (seg = set * ntrials + trial): out[4*seg] = (ab_hi, ab_lo, aa_hi, aa_lo);
+   out_bb = (hi, lo) of the target's sum B^2. */
+float rc_rank_score_batch(void *ctx, const unsigned int *prog, const unsigned int *off,
+                          const int *pcount, int nsets, int ntrials, int kmax, const double *c0,
+                          unsigned long long *out, int *out_status, unsigned long long *out_bb);
+/* eval.cu:4852 rc_rank_debug_b: the cached target ranks B per row. */
+int rc_rank_debug_b(void *ctx, long long *out);
+/* eval.cu:4743 rc_order_stat_score_batch: exact median (what=0) or
+   interquartile mean (what=1) of |r| per segment. */
+float rc_order_stat_score_batch(void *ctx, const unsigned int *prog, const unsigned int *off,
+                                const int *pcount, int nsets, int ntrials, int kmax,
+                                const double *c0, int what, double *out_value, int *out_status);
+/* eval.cu:4651 rc_max_scan_batch: exact max |r| per segment. */
+float rc_max_scan_batch(void *ctx, const unsigned int *prog, const unsigned int *off,
+                        const int *pcount, int nsets, int ntrials, int kmax, const double *c0,
+                        const int *coords, const double *levels, RcMaxOut *out);
+
+/* ---- telemetry / probe ---------------------------------------------- */
+
+/* eval.cu:3836 / :3855. */
+void rc_stats_begin(void *ctx);
+int rc_last_stats(void *ctx, RcStats *out);
+/* eval.cu:3469 / :3494. */
+int rc_arena_report(void *ctx, RcArenaReport *out);
+int rc_arena_force_sync(void *ctx, int sync);
+/* eval.cu:4886 / :4872 / :4863. */
+int rc_device_count(void);
+const char *rc_device_name(void);
+int rc_unified(void);
+
+/* ---- additive entry points (no counterpart in the reference ABI) ----- */
+
+/* Batched LM with the fused forward+adjoint sweep: one persistent launch per
+   node-count bucket runs every LM iteration of every candidate on the device,
+   fed by a cost-ordered work queue; the whole batch (upload, launches,
+   download) is replayed from a cached CUDA graph when the batch shape repeats.
+   Arguments, outputs and status codes are rc_fit_batch's; metric adds
+   6 = implicit (minimises sum w (f/|grad_x f|)^2 with a central-difference
+   constant Jacobian over the fused input-adjoint sweep). flags: bit 0 skips
+   the f64 polish. */
+float rc_fit_batch_fused(void *ctx, const unsigned int *prog, const unsigned int *off,
+                         const int *pcount, int nprog, int kmax, const double *c0,
+                         const int *gauge, int iters, int metric, int flags, double *outc,
+                         double *outsse, int *outstatus);
+/* The plain comparison arm: the same LM, one candidate per launch, each
+   launch a single block, candidates run back to back. Same arguments and
+   outputs as rc_fit_batch. */
+float rc_fit_batch_plain(void *ctx, const unsigned int *prog, const unsigned int *off,
+                         const int *pcount, int nprog, int kmax, const double *c0,
+                         const int *gauge, int iters, int metric, double *outc,
+                         double *outsse, int *outstatus);
+/* Per-row gradients of fit-record programs from the fused adjoint sweep, over
+   rows [row0, row0 + nrows): want = 1 writes d f / d c_j (f32,
+   out[(cand * nrows + r) * kmax + j]); want = 2 writes d f / d x_k
+   (out[(cand * nrows + r) * v + k]). value[cand * nrows + r] receives f. */
+int rc_grad_batch(void *ctx, const unsigned int *prog, const unsigned int *off,
+                  const int *pcount, int nprog, int kmax, const double *c, int want, int row0,
+                  int nrows, float *value, float *out);
+/* The implicit metric mean_w |f| / ||grad_x f|| per candidate from the fused
+   input-adjoint sweep; status 2 (+inf) when any positive-weight row has a
+   non-finite value, a non-finite gradient or a zero gradient norm. */
+float rc_implicit_score_batch(void *ctx, const unsigned int *prog, const unsigned int *off,
+                              const int *pcount, int nprog, int kmax, const double *c,
+                              double *out, int *status);
+/* Autotune the scoring launch shape (candidates per work item, rows per work
+   item) for this context's (N, feature count) and the length buckets of the
+   staged program batch; the choice is cached per (N, V, bucket) and, when
+   path is non-NULL, persisted to / loaded from that file. Returns the number
+   of cached entries, or -1. */
+int rc_autotune(void *ctx, const unsigned int *prog, const unsigned int *off, int nprog,
+                const char *path);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RCSR_B200_H */

@@ -1,0 +1,211 @@
+"""ctypes wrapper of the CPU f64 oracle (`oracle/oracle.cpp`).
+
+TEST INFRASTRUCTURE ONLY: the checker for the device path and the timed CPU
+baseline. Only `tests/`, `__graft_entry__.smoke()` and `bench.py`'s CPU-baseline
+leg load it. Trees are passed as pre-order `(op, val)` arrays (any object with
+a `prefix()` method works, e.g. the package's `expr.Node`).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+
+# Metric codes of the oracle (regression block equals the device score codes).
+SQUARED, ABSOLUTE, LOG_SQUASHED, SIGNED, MAXIMUM = 0, 1, 2, 3, 4
+CORRELATION, CORRELATION_SIGNED, AIC, AICC, BIC = 5, 6, 7, 8, 9
+MEDIAN, INTERQUARTILE = 15, 16
+RANK_CORRELATION, RANK_CORRELATION_SIGNED = 20, 21
+
+_lib = None
+
+
+def build() -> str:
+    subprocess.run(["make", "-C", HERE, "-s"], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH) or (
+                os.path.getmtime(LIB_PATH) < os.path.getmtime(os.path.join(HERE, "oracle.cpp"))):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        P = ctypes.POINTER
+        i32p, f64p, f32p, u64p, i64p = (P(ctypes.c_int32), P(ctypes.c_double), P(ctypes.c_float),
+                                        P(ctypes.c_uint64), P(ctypes.c_int64))
+        ci, cd = ctypes.c_int, ctypes.c_double
+        sig = {
+            "or_tree_ok": (ci, [i32p, f64p, ci]),
+            "or_predict": (ci, [i32p, f64p, ci, f64p, ci, ci, f64p]),
+            "or_cpu_sse": (cd, [i32p, f64p, ci, f32p, ci, ci, f32p]),
+            "or_score": (cd, [i32p, f64p, ci, f64p, ci, ci, f64p, f64p, ci]),
+            "or_score_pred": (cd, [f64p, f64p, f64p, ci, ci, ci]),
+            "or_fit": (cd, [i32p, f64p, ci, f64p, ci, ci, f64p, f64p, ci, ci]),
+            "or_flat_sse": (cd, [i32p, f64p, ci, f64p, ci, ci, f64p, f64p]),
+            "or_row_grad": (ci, [i32p, f64p, ci, f64p, ci, f64p, f64p, f64p]),
+            "or_implicit_score": (cd, [i32p, f64p, ci, f64p, ci, ci, f64p]),
+            "or_implicit_fit": (cd, [i32p, f64p, ci, f64p, ci, ci, f64p, ci]),
+            "or_rank_sums": (ci, [f64p, f64p, ci, u64p]),
+            "or_centred_ranks_doubled": (ci, [f64p, ci, i64p]),
+            "or_erf": (cd, [cd]),
+            "or_erfc": (cd, [cd]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _ptr(a, ct):
+    if a is None:
+        return None
+    return a.ctypes.data_as(ctypes.POINTER(ct))
+
+
+def _tree(t):
+    ops, vals = t.prefix()
+    return np.ascontiguousarray(ops, np.int32), np.ascontiguousarray(vals, np.float64)
+
+
+def _cols(cols):
+    c = np.ascontiguousarray(cols, np.float64)
+    return c
+
+
+def predict(t, cols, n, v):
+    ops, vals = _tree(t)
+    c = _cols(cols)
+    out = np.empty(n, np.float64)
+    rc = lib().or_predict(_ptr(ops, ctypes.c_int32), _ptr(vals, ctypes.c_double), len(ops),
+                          _ptr(c, ctypes.c_double), n, v, _ptr(out, ctypes.c_double))
+    assert rc == 0
+    return out
+
+
+def cpu_sse(t, cols32, n, v, y32):
+    ops, vals = _tree(t)
+    c = np.ascontiguousarray(cols32, np.float32)
+    y = np.ascontiguousarray(y32, np.float32)
+    return lib().or_cpu_sse(_ptr(ops, ctypes.c_int32), _ptr(vals, ctypes.c_double), len(ops),
+                            _ptr(c, ctypes.c_float), n, v, _ptr(y, ctypes.c_float))
+
+
+def score(t, cols, n, v, y, metric, w=None):
+    ops, vals = _tree(t)
+    c = _cols(cols)
+    y = np.ascontiguousarray(y, np.float64)
+    w = None if w is None else np.ascontiguousarray(w, np.float64)
+    return lib().or_score(_ptr(ops, ctypes.c_int32), _ptr(vals, ctypes.c_double), len(ops),
+                          _ptr(c, ctypes.c_double), n, v, _ptr(y, ctypes.c_double),
+                          _ptr(w, ctypes.c_double), metric)
+
+
+def score_pred(pred, y, metric, k=0, w=None):
+    p = np.ascontiguousarray(pred, np.float64)
+    y = np.ascontiguousarray(y, np.float64)
+    w = None if w is None else np.ascontiguousarray(w, np.float64)
+    return lib().or_score_pred(_ptr(p, ctypes.c_double), _ptr(y, ctypes.c_double),
+                               _ptr(w, ctypes.c_double), len(p), metric, k)
+
+
+def fit(t, cols, n, v, y, iters, metric=SQUARED, w=None):
+    """fit::fit_weighted_metric; returns (objective, fitted tree)."""
+    ops, vals = _tree(t)
+    c = _cols(cols)
+    y = np.ascontiguousarray(y, np.float64)
+    w = None if w is None else np.ascontiguousarray(w, np.float64)
+    r = lib().or_fit(_ptr(ops, ctypes.c_int32), _ptr(vals, ctypes.c_double), len(ops),
+                     _ptr(c, ctypes.c_double), n, v, _ptr(y, ctypes.c_double),
+                     _ptr(w, ctypes.c_double), iters, metric)
+    out = t.clone()
+    out.set_prefix_values(vals)
+    return r, out
+
+
+def flat_sse(t, cols, n, v, y, w=None):
+    ops, vals = _tree(t)
+    c = _cols(cols)
+    y = np.ascontiguousarray(y, np.float64)
+    w = None if w is None else np.ascontiguousarray(w, np.float64)
+    return lib().or_flat_sse(_ptr(ops, ctypes.c_int32), _ptr(vals, ctypes.c_double), len(ops),
+                             _ptr(c, ctypes.c_double), n, v, _ptr(y, ctypes.c_double),
+                             _ptr(w, ctypes.c_double))
+
+
+def row_grad(t, row):
+    """(value, d/dconstants, d/dinputs) of one row via backward_impl."""
+    ops, vals = _tree(t)
+    r = np.ascontiguousarray(row, np.float64)
+    nconst = len(t.constants())
+    val = ctypes.c_double(0.0)
+    cg = np.zeros(max(nconst, 1), np.float64)
+    ig = np.zeros(len(r), np.float64)
+    k = lib().or_row_grad(_ptr(ops, ctypes.c_int32), _ptr(vals, ctypes.c_double), len(ops),
+                          _ptr(r, ctypes.c_double), len(r), ctypes.byref(val),
+                          _ptr(cg, ctypes.c_double), _ptr(ig, ctypes.c_double))
+    assert k == nconst
+    return val.value, cg[:nconst], ig
+
+
+def implicit_score(t, cols, n, v, w=None):
+    ops, vals = _tree(t)
+    c = _cols(cols)
+    w = None if w is None else np.ascontiguousarray(w, np.float64)
+    return lib().or_implicit_score(_ptr(ops, ctypes.c_int32), _ptr(vals, ctypes.c_double),
+                                   len(ops), _ptr(c, ctypes.c_double), n, v,
+                                   _ptr(w, ctypes.c_double))
+
+
+def implicit_fit(t, cols, n, v, iters, w=None):
+    ops, vals = _tree(t)
+    c = _cols(cols)
+    w = None if w is None else np.ascontiguousarray(w, np.float64)
+    r = lib().or_implicit_fit(_ptr(ops, ctypes.c_int32), _ptr(vals, ctypes.c_double), len(ops),
+                              _ptr(c, ctypes.c_double), n, v, _ptr(w, ctypes.c_double), iters)
+    out = t.clone()
+    out.set_prefix_values(vals)
+    return r, out
+
+
+def _i128(hi, lo):
+    v = (int(hi) << 64) | int(lo)
+    if v >= 1 << 127:
+        v -= 1 << 128
+    return v
+
+
+def rank_sums(pred, y):
+    """(ab, aa, bb) as Python ints, or None when a value is not finite."""
+    p = np.ascontiguousarray(pred, np.float64)
+    yy = np.ascontiguousarray(y, np.float64)
+    out = np.zeros(6, np.uint64)
+    rc = lib().or_rank_sums(_ptr(p, ctypes.c_double), _ptr(yy, ctypes.c_double), len(p),
+                            _ptr(out, ctypes.c_uint64))
+    if rc != 0:
+        return None
+    return _i128(out[0], out[1]), _i128(out[2], out[3]), _i128(out[4], out[5])
+
+
+def centred_ranks_doubled(v):
+    a = np.ascontiguousarray(v, np.float64)
+    out = np.zeros(len(a), np.int64)
+    rc = lib().or_centred_ranks_doubled(_ptr(a, ctypes.c_double), len(a),
+                                        _ptr(out, ctypes.c_int64))
+    return None if rc != 0 else out
+
+
+def erf(x):
+    return lib().or_erf(float(x))
+
+
+def erfc(x):
+    return lib().or_erfc(float(x))

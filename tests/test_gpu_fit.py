@@ -1,0 +1,207 @@
+"""Batched device LM/IRLS parity against the CPU f64 oracle.
+
+Restates the reference's fit tests (my-version/src/gpu.rs:4301-6020): the
+p = 1..20 orthogonal design (SSE relative <= 1e-8, median constant error
+<= 1e-5), the nonlinear 5-constant model, mixed-p padded batches
+bit-identical to single fits, the rank-deficient label, and the absolute
+(L1 IRLS) arm no worse than its start. Also checks the fused adjoint's
+Jacobian against central finite differences and the CPU adjoint.
+"""
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def linear_fixture(p, n):
+    # gpu.rs:4388-4417
+    target = [1.0 + 0.31 * k for k in range(p)]
+    start = [0.25 + 0.07 * k for k in range(p)]
+    t = 2 * np.pi * np.arange(n) / (n - 1)
+    x = np.stack([np.sin((k + 1) * t) for k in range(p)])
+    noise = (((np.arange(n) * 37) % 11) - 5.0) * 2e-4
+    y = (np.asarray(target)[:, None] * x).sum(0) + noise
+    return x, y, target, start
+
+
+def linear_model(E, coeffs):
+    terms = [E.node(E.MUL, [E.constant(c), E.input(k)]) for k, c in enumerate(coeffs)]
+    tree = terms.pop()
+    while terms:
+        tree = E.node(E.ADD, [terms.pop(), tree])
+    return tree
+
+
+def basis(E, k):
+    x = E.input(0)
+    return {0: E.constant(1.0), 1: x, 2: E.node(E.SQUARE, [x]), 3: E.node(E.CUBE, [x]),
+            4: E.node(E.SIN, [x])}[k]
+
+
+def model(E, coeffs):
+    # gpu.rs:4329-4346
+    terms = []
+    for k, c in enumerate(coeffs):
+        terms.append(E.constant(c) if k == 0 else E.node(E.MUL, [E.constant(c), basis(E, k)]))
+    tree = terms.pop()
+    while terms:
+        tree = E.node(E.ADD, [terms.pop(), tree])
+    return tree
+
+
+def evaluator(pkg, x, y):
+    v, n = x.shape
+    ev = pkg.GpuEvaluator(x.astype(np.float32).reshape(-1), n, v, y.astype(np.float32))
+    ev.set_fit_data(x.reshape(-1), y)
+    return ev
+
+
+def test_fit_matches_the_cpu_lm_for_p_1_to_20(pkg, E, O):
+    """gpu.rs:4430-4500."""
+    n = 800
+    errors, worst = [], 0.0
+    for p in range(1, 21):
+        x, y, target, start = linear_fixture(p, n)
+        ev = evaluator(pkg, x, y)
+        cpu_tree = linear_model(E, start)
+        _, cpu_tree = O.fit(cpu_tree, x.reshape(-1), n, p, y, 8)
+        cpu_sse, cpu_tree = O.fit(cpu_tree, x.reshape(-1), n, p, y, 8)
+        plan = pkg.gpu_fit_plan(linear_model(E, start))
+        assert plan.nconst == p
+        c, loss, status, ms = ev.fit_plans([plan], 8, fused=False)
+        assert ms >= 0
+        assert status[0] == 0, (p, status[0])
+        gpu_tree = plan.apply(linear_model(E, start), c[0])
+        gpu_sse = O.flat_sse(gpu_tree, x.reshape(-1), n, p, y)
+        rel = abs(gpu_sse - cpu_sse) / max(abs(cpu_sse), 1e-8)
+        worst = max(worst, rel)
+        assert rel <= 1e-8, (p, rel, gpu_sse, cpu_sse)
+        for a, b in zip(gpu_tree.constants(), cpu_tree.constants()):
+            errors.append(abs(a - b) / (1 + abs(b)))
+        ev.close()
+    assert float(np.median(errors)) <= 1e-5
+
+
+def test_fit_matches_a_nonlinear_cpu_fit(pkg, E, O):
+    """gpu.rs:4503-4548."""
+    n = 800
+    xs = (np.arange(n) / (n - 1)) * 5.0 - 2.5
+    target = model(E, [2.0, -0.5, 0.8, 0.0, 1.0])
+    noise = (((np.arange(n) * 37) % 11) - 5.0) * 2e-4
+    y = O.predict(target, xs, n, 1) + noise
+    x = xs[None, :]
+    ev = evaluator(pkg, x, y)
+    start = [1.0, 0.2, 0.4, 0.1, 0.5]
+    cpu_sse, cpu_tree = O.fit(model(E, start), xs, n, 1, y, 8)
+    plan = pkg.gpu_fit_plan(model(E, start))
+    c, loss, status, _ = ev.fit_plans([plan], 8)
+    assert status[0] == 0
+    gpu_tree = plan.apply(model(E, start), c[0])
+    for a, b in zip(gpu_tree.constants(), cpu_tree.constants()):
+        assert abs(a - b) / (1 + abs(b)) <= 1e-5, (a, b)
+    gpu_sse = O.flat_sse(gpu_tree, xs, n, 1, y)
+    assert abs(gpu_sse - cpu_sse) / max(abs(cpu_sse), 1e-8) <= 1e-8
+    # the device reports the configured objective at its constants
+    assert abs(loss[0] - gpu_sse) <= 1e-9 * max(1.0, gpu_sse)
+    ev.close()
+
+
+def test_mixed_p_batch_is_bit_identical_to_single_fits(pkg, E):
+    """gpu.rs:4600-4680."""
+    n = 600
+    x, y, _, _ = linear_fixture(6, n)
+    ev = evaluator(pkg, x, y)
+    plans = [pkg.gpu_fit_plan(linear_model(E, [0.3 + 0.1 * j for j in range(p)]))
+             for p in (1, 4, 2, 6, 3)]
+    c, loss, status, _ = ev.fit_plans(plans, 8)
+    for i, pl in enumerate(plans):
+        c1, l1, s1, _ = ev.fit_plans([pl], 8)
+        assert s1[0] == status[i]
+        assert l1[0].tobytes() == loss[i].tobytes()
+        assert c1[0, :pl.nconst].tobytes() == c[i, :pl.nconst].tobytes()
+    ev.close()
+
+
+def test_collinear_design_is_labelled_rank_deficient(pkg, E):
+    """gpu.rs:4706-4767: two identical columns -> status 4 (usable)."""
+    n = 400
+    t = np.linspace(-1, 1, n)
+    x = np.stack([t, t])
+    y = 2.0 * t + 0.5
+    ev = evaluator(pkg, x, y)
+    tree = E.node(E.ADD, [E.node(E.MUL, [E.constant(0.3), E.input(0)]),
+                          E.node(E.MUL, [E.constant(0.4), E.input(1)])])
+    c, loss, status, _ = ev.fit_plans([pkg.gpu_fit_plan(tree)], 8)
+    assert status[0] == 4, status[0]
+    ev.close()
+
+
+def test_absolute_fit_is_no_worse_than_start_and_tracks_the_cpu_irls(pkg, E, O):
+    """gpu.rs:5758-6020: the L1 IRLS arm never returns a worse mean |r| than
+    its start, and lands within 1e-6 relative of the CPU IRLS objective on a
+    well-posed line fit with outliers."""
+    n = 2000
+    rng = np.random.default_rng(3)
+    xs = rng.uniform(-3, 3, n)
+    y = 2.0 * xs + 1.0 + rng.normal(0, 0.05, n)
+    y[::50] += 20.0
+    x = xs[None, :]
+    ev = evaluator(pkg, x, y)
+    start = E.node(E.ADD, [E.node(E.MUL, [E.constant(1.0), E.input(0)]), E.constant(0.0)])
+    plan = pkg.gpu_fit_plan(start)
+    c, loss, status, _ = ev.fit_plans([plan], 8, metric=4)
+    assert status[0] in (0, 4, 5, 6, 8)
+    fitted = plan.apply(start, c[0])
+    start_mae = O.score(start, xs, n, 1, y, O.ABSOLUTE)
+    dev_mae = O.score(fitted, xs, n, 1, y, O.ABSOLUTE)
+    assert dev_mae <= start_mae
+    cpu_mae, _ = O.fit(start, xs, n, 1, y, 8, metric=O.ABSOLUTE)
+    # the device loss is the summed |r| (the reference's objective statistic)
+    assert abs(loss[0] / n - dev_mae) <= 1e-9 * max(1, dev_mae)
+    assert abs(dev_mae - cpu_mae) / cpu_mae <= 1e-3
+    ev.close()
+
+
+def test_jacobian_matches_central_differences_and_the_cpu_adjoint(pkg, E, O):
+    """The fused adjoint's constant and input gradients against the CPU
+    `backward_impl` and central finite differences (h = 1e-3 relative)."""
+    W = __import__("importlib").import_module("the-rule-and-compass_b200.workloads")
+    trees, x, y = W.fit_workload(24, 512, seed=11)
+    ev = evaluator(pkg, x, y)
+    plans = [pkg.gpu_fit_plan(t) for t in trees]
+    prog, off, pcount, c0, gauge, kmax = pkg.pack_plans(plans)
+    nrows = 64
+    val, gc = ev.grad_batch(prog, off, pcount, c0, kmax, 1, 0, nrows)
+    val2, gx = ev.grad_batch(prog, off, pcount, c0, kmax, 2, 0, nrows)
+    checked = 0
+    for k, t in enumerate(trees):
+        for r in range(0, nrows, 7):
+            row = x[:, r]
+            v_ref, cg_ref, ig_ref = O.row_grad(t, row)
+            if not (np.isfinite(v_ref) and abs(v_ref) < 1e6 and np.all(np.isfinite(cg_ref))
+                    and np.all(np.abs(cg_ref) < 1e6)):
+                continue
+            assert abs(val[k, r] - v_ref) <= 1e-4 * (1 + abs(v_ref))
+            scale = 1 + np.abs(cg_ref).max()
+            assert np.all(np.abs(gc[k, r, :plans[k].nconst] - cg_ref) <= 2e-3 * scale), (k, r)
+            iscale = 1 + np.abs(ig_ref).max()
+            assert np.all(np.abs(gx[k, r] - ig_ref) <= 2e-3 * iscale), (k, r)
+            # central differences of the f64 oracle, h = 1e-3 * max(|c|, 1)
+            cs = np.asarray(t.constants())
+            fd = np.zeros(len(cs))
+            for j in range(len(cs)):
+                h = 1e-3 * max(abs(cs[j]), 1.0)
+                tp, tm = t.clone(), t.clone()
+                cp, cm = cs.copy(), cs.copy()
+                cp[j] += h
+                cm[j] -= h
+                tp.set_constants(cp)
+                tm.set_constants(cm)
+                fd[j] = (O.row_grad(tp, row)[0] - O.row_grad(tm, row)[0]) / (2 * h)
+            if np.all(np.isfinite(fd)):
+                assert np.all(np.abs(gc[k, r, :len(cs)] - fd) <= 1e-2 * (1 + np.abs(fd))), (k, r)
+            checked += 1
+    assert checked > 50
+    ev.close()

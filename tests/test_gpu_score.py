@@ -1,0 +1,215 @@
+"""Device scoring parity against the CPU f64 oracle.
+
+Restates the reference's scorer tests (my-version/src/gpu.rs:3147-3458):
+native objectives vs the CPU reducer on the device's own f32 predictions,
+non-finite -> +inf / status 2, composition-free bits, the device stack guard,
+and the f32-vs-f64 SSE agreement (relative error < 1e-4), plus a seeded
+random batch with the benchmark's tree distribution.
+"""
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def fixture(E):
+    # gpu.rs:2925-2956
+    n, nv = 128, 2
+    cols = np.zeros((nv, n), np.float32)
+    y = np.zeros(n, np.float32)
+    for i in range(n):
+        x0 = np.float32(i / n * 2.0 - 1.0)
+        x1 = np.float32(((i * 7) % 31) / 31.0 - 0.5)
+        cols[0, i] = x0
+        cols[1, i] = x1
+        y[i] = np.float32(np.sin(x0) + np.float32(0.25) * x1 * x1)
+    trees = [
+        E.node(E.ADD, [E.node(E.MUL, [E.input(0), E.constant(2.0)]), E.constant(1.0)]),
+        E.node(E.SIN, [E.input(0)]),
+        E.node(E.ADD, [E.node(E.SQUARE, [E.input(0)]), E.node(E.MUL, [E.input(1),
+                                                                      E.constant(0.5)])]),
+        E.node(E.DIV, [E.constant(1.0), E.node(E.ADD, [E.input(0), E.constant(3.0)])]),
+    ]
+    return cols, n, nv, y, trees
+
+
+@pytest.fixture(scope="module")
+def ev_fix(pkg, E):
+    cols, n, nv, y, trees = fixture(E)
+    ev = pkg.GpuEvaluator(cols.reshape(-1), n, nv, y)
+    yield ev, cols, n, nv, y, trees
+    ev.close()
+
+
+def test_batch_sse_matches_cpu_reference(pkg, E, O, ev_fix):
+    """gpu.rs:3349-3369: f32 device SSE vs the f64 CPU SSE, rel < 1e-4."""
+    ev, cols, n, nv, y, trees = ev_fix
+    pop = pkg.Population(trees)
+    prog, off = pop.programs()
+    sse, ms = ev.eval_batch(prog, off, 0)
+    assert ms >= 0
+    for i, t in enumerate(trees):
+        cpu = O.cpu_sse(t, cols.reshape(-1), n, nv, y)
+        rel = abs(float(sse[i]) - cpu) / (1.0 + abs(cpu))
+        assert rel < 1e-4, (i, sse[i], cpu)
+
+
+OBJECTIVES = [0, 1, 2, 3, 4, 5, 6, 7, 8, 9]
+
+
+def test_native_objectives_match_the_cpu_reducer(pkg, E, O, ev_fix):
+    """gpu.rs:3147-3212: every native objective equals the CPU reducer on the
+    device's own predictions widened to f64 (only reduction order differs)."""
+    ev, cols, n, nv, y, trees = ev_fix
+    pop = pkg.Population(trees)
+    prog, off = pop.programs()
+    preds = ev.predictions(prog, off).astype(np.float64)
+    y64 = y.astype(np.float64)
+    pcount = np.full(len(trees), 2, np.int32)
+    for kind in OBJECTIVES:
+        vals, status, ms = ev.score_batch(prog, off, kind, pcount)
+        assert ms >= 0
+        for k in range(len(trees)):
+            want = O.score_pred(preds[k], y64, kind, 2)
+            got = vals[k]
+            assert status[k] == 0, (kind, k)
+            if kind == 4:
+                assert got == want, (kind, k, got, want)
+            elif math.isinf(want):
+                assert got == want
+            elif kind in (5, 6):
+                assert abs(got - want) <= 1e-9, (kind, k, got, want)
+            else:
+                tol = 1e-12 * (1.0 + abs(want))
+                assert abs(got - want) <= tol, (kind, k, got, want)
+
+
+def test_nonfinite_is_inf_with_status(pkg, E):
+    """gpu.rs:3215-3252."""
+    n, nv = 16, 1
+    cols = np.arange(n, dtype=np.float32) / n
+    y = np.zeros(n, np.float32)
+    ev = pkg.GpuEvaluator(cols, n, nv, y)
+    trees = [E.constant(float("nan")), E.node(E.DIV, [E.constant(1.0), E.constant(0.0)])]
+    prog, off = pkg.Population(trees).programs()
+    for kind in OBJECTIVES:
+        vals, status, _ = ev.score_batch(prog, off, kind, np.zeros(2, np.int32))
+        assert list(status) == [2, 2], kind
+        assert all(math.isinf(v) and v > 0 for v in vals), kind
+    ev.close()
+
+
+def test_scores_are_composition_free_and_repeatable(pkg, E, ev_fix):
+    """gpu.rs:3256-3345: alone, in a batch of 7, in a batch of 447 and twice:
+    identical bits."""
+    ev, cols, n, nv, y, trees = ev_fix
+    seven = [trees[i % len(trees)] for i in range(7)]
+    prog, off = pkg.Population(seven).programs()
+    many = [trees[i % len(trees)] for i in range(447)]
+    mprog, moff = pkg.Population(many).programs()
+    for kind in OBJECTIVES:
+        pc7 = np.ones(7, np.int32)
+        a, _, _ = ev.score_batch(prog, off, kind, pc7)
+        b, _, _ = ev.score_batch(prog, off, kind, pc7)
+        for k in range(7):
+            one, _, _ = ev.score_batch(prog[off[k]:off[k + 1]],
+                                       np.array([0, off[k + 1] - off[k]], np.uint32), kind,
+                                       np.ones(1, np.int32))
+            assert a[k].tobytes() == one[0].tobytes(), (kind, k)
+            assert a[k].tobytes() == b[k].tobytes(), (kind, k)
+        m, _, _ = ev.score_batch(mprog, moff, kind, np.ones(447, np.int32))
+        assert m[0].tobytes() == a[0].tobytes()
+
+
+def test_device_stack_guard_scores_an_over_deep_program(pkg, E, ev_fix):
+    """gpu.rs:3377-3400: 65 pushes with no consumer is a hard failure on every
+    row (n * 1e30) instead of a stack overrun."""
+    ev, cols, n, nv, y, trees = ev_fix
+    words = []
+    for _ in range(65):
+        words += [0, np.float32(1.0).view(np.uint32)]
+    words.append(255)
+    prog = np.asarray(words, np.uint32)
+    off = np.array([0, len(words)], np.uint32)
+    sse, ms = ev.eval_batch(prog, off, 0)
+    want = n * 1e30
+    assert abs(sse[0] - want) / want < 1e-5
+    vals, status, _ = ev.score_batch(prog, off, 0)
+    assert status[0] == 2 and math.isinf(vals[0])
+
+
+def test_every_opcode_matches_the_f64_oracle(pkg, E, O):
+    """gpu.rs:3859-4090 (per-opcode agreement): raw device predictions of each
+    operator vs expr::eval in f64 on f32 inputs, within a few f32 ulps and with
+    identical NaN classification."""
+    n = 4096
+    rng = np.random.default_rng(5)
+    a = rng.uniform(-4, 4, n).astype(np.float32)
+    b = rng.uniform(-4, 4, n).astype(np.float32)
+    c = rng.uniform(-1, 1, n).astype(np.float32)
+    a[:8] = [0.0, -0.0, 1.0, -1.0, 0.5, 2.0, 3.0, -3.0]
+    b[:8] = [0.0, 1.0, 0.0, 2.0, -0.5, 0.5, 3.0, 1e-13]
+    cols = np.stack([a, b, c])
+    ev = pkg.GpuEvaluator(cols.reshape(-1), n, 3, np.zeros(n, np.float32))
+    unary = [E.SIN, E.COS, E.TAN, E.EXP, E.LOG, E.SQRT, E.ABS, E.TANH, E.SIG, E.SQUARE,
+             E.CUBE, E.NEG, E.GAUSS, E.STEP, E.SINH, E.COSH, E.FLOOR, E.CEIL, E.ROUND, E.ERF,
+             E.ERFC, E.SIGN, E.NOT]
+    binary = [E.ADD, E.SUB, E.MUL, E.DIV, E.POW, E.MOD, E.ATAN2, E.MIN, E.MAX, E.EQUAL,
+              E.LESS, E.LESS_OR_EQUAL, E.GREATER, E.GREATER_OR_EQUAL, E.AND, E.OR, E.XOR]
+    trees = [E.node(u, [E.input(0)]) for u in unary]
+    trees += [E.node(bb, [E.input(0), E.input(1)]) for bb in binary]
+    trees.append(E.node(E.IF, [E.input(2), E.input(0), E.input(1)]))
+    prog, off = pkg.Population(trees).programs()
+    dev = ev.predictions(prog, off).astype(np.float64)
+    x64 = cols.astype(np.float64).reshape(-1)
+    for k, t in enumerate(trees):
+        ref = O.predict(t, x64, n, 3)
+        d = dev[k]
+        nan_ref, nan_dev = np.isnan(ref), np.isnan(d)
+        # f32 overflow (sinh/cosh/exp beyond ~88) is inf on the device, finite in f64
+        big = np.abs(ref) > 3.0e38
+        mism = (nan_ref != nan_dev) & ~big
+        assert mism.sum() == 0, (E.NAMES[t.op], np.nonzero(mism)[0][:5])
+        ok = ~nan_ref & ~big & np.isfinite(ref)
+        err = np.abs(d[ok] - ref[ok]) / np.maximum(np.abs(ref[ok]), 1e-30)
+        # mod loses the f64 quotient's fraction only beyond 2^25; tiny absolute
+        # errors near zero crossings are ulps of the operands, not of the result
+        tol_abs = np.abs(d[ok] - ref[ok]) <= 4e-6 * np.maximum(1.0, np.abs(x64[:n][ok]))
+        assert np.all((err <= 4e-6) | tol_abs), (E.NAMES[t.op], float(err.max()))
+    ev.close()
+
+
+def test_random_batch_matches_the_oracle(pkg, E, O):
+    """A seeded batch with the benchmark's tree distribution at moderate size:
+    per-candidate squared and absolute losses within 1e-4 relative of the f64
+    oracle; non-finite classification identical except where f32 and f64
+    genuinely differ (reported, bounded)."""
+    W = pkg.workloads if hasattr(pkg, "workloads") else __import__(
+        "importlib").import_module("the-rule-and-compass_b200.workloads")
+    P, n = 256, 8192
+    trees, x, y = W.scoring_workload(P, n, seed=3)
+    ev = pkg.GpuEvaluator(x.reshape(-1), n, 5, y)
+    pop = pkg.Population(trees)
+    prog, off = pop.programs()
+    x64 = x.astype(np.float64).reshape(-1)
+    y64 = y.astype(np.float64)
+    for kind, metric in ((0, O.SQUARED), (1, O.ABSOLUTE)):
+        vals, status, _ = ev.score_batch(prog, off, kind)
+        mismatch = 0
+        for k, t in enumerate(trees):
+            # the device sees f32 constants: score the tree the device runs
+            t32 = t.clone()
+            t32.set_constants([float(np.float32(c)) for c in t.constants()])
+            want = O.score(t32, x64, n, 5, y64, metric)
+            pred = O.predict(t32, x64, n, 5)
+            cpu_bad = (not math.isfinite(want)) or bool(np.any(np.abs(pred) > 1e30))
+            if cpu_bad != (status[k] == 2):
+                mismatch += 1
+                continue
+            if cpu_bad:
+                continue
+            assert abs(vals[k] - want) <= 1e-4 * abs(want) + 1e-12, (k, vals[k], want, t)
+        assert mismatch <= P // 50, mismatch
+    ev.close()

@@ -1,0 +1,120 @@
+"""Host-side compiler and C-ABI surface (CPU only, no device calls).
+
+Restates the reference's host tests: emitted words (my-version/src/gpu.rs:
+349-438), the stack guard and lowering (gpu.rs:3402-3438), the fit-plan cap
+and rejection labels (gpu.rs:4554-4598, fit.rs:958-1056). The ABI test loads
+librcsr_b200.so and checks that it exports every function include/rcsr_b200.h
+declares.
+"""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def f32bits(v):
+    return int(np.float32(v).view(np.uint32))
+
+
+def test_emitted_words(pkg, E):
+    t = E.node(E.ADD, [E.node(E.MUL, [E.input(0), E.constant(2.0)]), E.constant(1.0)])
+    words, lowered = pkg.compile_program(t)
+    assert list(words) == [1, 0, 0, f32bits(2.0), 4, 0, f32bits(1.0), 2, 255]
+    assert not lowered
+
+
+def test_constants_are_rounded_to_f32(pkg, E):
+    words, _ = pkg.compile_program(E.constant(0.1))
+    assert list(words) == [0, f32bits(0.1), 255]
+
+
+def test_lowering_rewrites_inverse_hyperbolics(pkg, E, O):
+    for op in (E.ASINH, E.ACOSH, E.ATANH):
+        t = E.node(op, [E.input(0)])
+        words, lowered = pkg.compile_program(t)
+        assert lowered
+        assert 64 not in words and 65 not in words and 66 not in words
+
+
+def test_stack_guard(pkg, E):
+    deep = E.input(0)
+    for _ in range(56):
+        deep = E.node(E.ADD, [E.input(1), deep])
+    assert pkg.host.peak_stack(deep) > 56
+    with pytest.raises(pkg.host.CompileError):
+        pkg.compile_program(deep)
+    pop = pkg.Population([deep, E.input(0)])
+    assert len(pop) == 1 and pop.unsupported == 1
+
+
+def test_population_offsets(pkg, E):
+    trees = [E.input(0), E.node(E.SIN, [E.input(1)]), E.constant(3.0)]
+    pop = pkg.Population(trees)
+    prog, off = pop.programs()
+    assert list(off) == [0, 3, 7, 10]
+    assert len(prog) == 10
+
+
+def test_fit_plan_records(pkg, E):
+    # c0 * x0 + c1: post-order [const, var, mul, const, add]
+    t = E.node(E.ADD, [E.node(E.MUL, [E.constant(1.5), E.input(0)]), E.constant(-0.5)])
+    plan = pkg.gpu_fit_plan(t)
+    assert plan.nconst == 2
+    assert list(plan.c0) == [1.5, -0.5]
+    rec = plan.words.reshape(-1, 4)
+    assert [list(r) for r in rec] == [[0, 0, 0, 0], [1, 0, 0, 0], [4, 0, 1, 0xFFFFFFFF],
+                                      [0, 0, 0, 1], [2, 2, 3, 0xFFFFFFFF]]
+    # the correlation gauge: Add(Mul(Const, T), Const) -> (scale, offset)
+    assert list(plan.gauge) == [0, 1]
+
+
+def test_fit_plan_cap_and_rejections(pkg, E):
+    for p in range(1, 21):
+        terms = [E.node(E.MUL, [E.constant(0.1), E.input(k)]) for k in range(p)]
+        t = terms.pop()
+        while terms:
+            t = E.node(E.ADD, [terms.pop(), t])
+        assert pkg.gpu_fit_plan(t).nconst == p
+    t = E.node(E.ADD, [t, E.constant(1.0)])
+    with pytest.raises(pkg.host.GpuFitReject) as e:
+        pkg.gpu_fit_plan(t)
+    assert e.value.label == "too_many_constants"
+    with pytest.raises(pkg.host.GpuFitReject) as e:
+        pkg.gpu_fit_plan(E.node(E.SIN, [E.input(0)]))
+    assert e.value.label == "no_constants"
+    with pytest.raises(pkg.host.GpuFitReject) as e:
+        pkg.gpu_fit_plan(E.node(E.FLOOR, [E.node(E.MUL, [E.constant(2.0), E.input(0)])]))
+    assert e.value.label == "unsupported_op"
+
+
+def _declared_functions():
+    src = open(os.path.join(ROOT, "include", "rcsr_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = re.findall(r"\b(rc_[a-z0-9_]+)\s*\(", src)
+    return sorted(set(names))
+
+
+def test_library_exports_every_declared_symbol(pkg):
+    path = os.path.join(ROOT, "the-rule-and-compass_b200", "librcsr_b200.so")
+    assert os.path.exists(path), "build the CUDA library first"
+    lib = ctypes.CDLL(path)
+    names = _declared_functions()
+    assert len(names) >= 30
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    # the Python binding covers the same surface
+    from importlib import import_module
+    dev = import_module("the-rule-and-compass_b200.device")
+    assert sorted(dev.SIGNATURES) == names
+
+
+def test_fit_kernel_info_contract(pkg):
+    L = pkg.cuda_lib()
+    t, s, m = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    assert L.rc_fit_kernel_info(20, ctypes.byref(t), ctypes.byref(s), ctypes.byref(m)) == 0
+    assert m.value == 20 and t.value > 0 and s.value > 0
+    assert L.rc_fit_kernel_info(21, ctypes.byref(t), ctypes.byref(s), ctypes.byref(m)) == -1

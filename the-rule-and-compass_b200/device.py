@@ -1,0 +1,307 @@
+"""ctypes binding of the C ABI (`librcsr_b200.so`) and the host evaluator.
+
+`GpuEvaluator` mirrors the reference's `GpuEvaluator` (my-version/src/gpu.rs:
+1182-2896): it owns one device context over a resident dataset and offers the
+batched scorer, raw predictions, the batched fit, the implicit score and the
+per-row gradients. There is no CPU fallback: if the CUDA library is missing
+or a device call fails, the call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+CUDA_LIB = os.path.join(_HERE, "librcsr_b200.so")
+_lib = None
+
+P = ctypes.POINTER
+u32p, i32p, f32p, f64p, u64p, i64p = (P(ctypes.c_uint32), P(ctypes.c_int32), P(ctypes.c_float),
+                                      P(ctypes.c_double), P(ctypes.c_uint64), P(ctypes.c_int64))
+ci, cf, cvp = ctypes.c_int, ctypes.c_float, ctypes.c_void_p
+
+
+class RcStats(ctypes.Structure):
+    _fields_ = [("kernel_ms", ctypes.c_double), ("launch_ms", ctypes.c_double),
+                ("sync_ms", ctypes.c_double), ("alloc_ms", ctypes.c_double),
+                ("h2d_ms", ctypes.c_double), ("d2h_ms", ctypes.c_double),
+                ("wall_ms", ctypes.c_double), ("h2d_bytes", ctypes.c_ulonglong),
+                ("d2h_bytes", ctypes.c_ulonglong), ("batch", ctypes.c_int),
+                ("failed", ctypes.c_int)]
+
+
+class RcArenaReport(ctypes.Structure):
+    _fields_ = [("async_copy", ctypes.c_int), ("reason", ctypes.c_char * 96),
+                ("pinned_bytes", ctypes.c_ulonglong), ("alloc_calls", ctypes.c_ulonglong),
+                ("steady_alloc_calls", ctypes.c_ulonglong),
+                ("overlapped_uploads", ctypes.c_ulonglong), ("batches", ctypes.c_ulonglong),
+                ("fs_alloc_calls", ctypes.c_ulonglong), ("fs_growths", ctypes.c_ulonglong),
+                ("fs_steady_alloc_calls", ctypes.c_ulonglong),
+                ("fs_batches", ctypes.c_ulonglong), ("fs_dev_bytes", ctypes.c_ulonglong),
+                ("fs_pinned_bytes", ctypes.c_ulonglong)]
+
+
+class RcMaxOut(ctypes.Structure):
+    _fields_ = [("vmax", ctypes.c_double), ("lo", ctypes.c_double), ("hi", ctypes.c_double),
+                ("row", ctypes.c_int), ("status", ctypes.c_int)]
+
+
+# name -> (restype, argtypes): every symbol include/rcsr_b200.h declares.
+SIGNATURES = {
+    "rc_create": (cvp, [f32p, ci, ci, f32p]),
+    "rc_destroy": (None, [cvp]),
+    "rc_set_fit_data": (ci, [cvp, f64p, f64p, f64p]),
+    "rc_set_score_weights": (ci, [cvp, f64p]),
+    "rc_set_fit_sign": (ci, [cvp, f64p]),
+    "rc_set_programs": (ci, [cvp, u32p, u32p, ci]),
+    "rc_eval": (cf, [cvp, f32p, ci]),
+    "rc_eval_submit": (ci, [cvp, ci]),
+    "rc_eval_collect": (cf, [cvp, f32p]),
+    "rc_score_batch": (cf, [cvp, u32p, u32p, ci, ci, i32p, f64p, i32p]),
+    "rc_pool_reserve": (ci, [cvp, ci, ci]),
+    "rc_pool_upload": (ci, [cvp, ci, u32p, ci]),
+    "rc_pool_eval": (cf, [cvp, ci, ci, ci, f32p, ci]),
+    "rc_pool_score": (cf, [cvp, ci, ci, ci, ci, i32p, f64p, i32p]),
+    "rc_pool_hash": (ci, [cvp, ci, ci, ci, u64p]),
+    "rc_predict": (ci, [cvp, u32p, u32p, ci, f32p]),
+    "rc_fit_batch": (cf, [cvp, u32p, u32p, i32p, ci, ci, f64p, i32p, ci, ci, f64p, f64p, i32p]),
+    "rc_fit_kernel_info": (ci, [ci, i32p, i32p, i32p]),
+    "rc_rank_score_batch": (cf, [cvp, u32p, u32p, i32p, ci, ci, ci, f64p, u64p, i32p, u64p]),
+    "rc_rank_debug_b": (ci, [cvp, i64p]),
+    "rc_order_stat_score_batch": (cf, [cvp, u32p, u32p, i32p, ci, ci, ci, f64p, ci, f64p,
+                                       i32p]),
+    "rc_max_scan_batch": (cf, [cvp, u32p, u32p, i32p, ci, ci, ci, f64p, i32p, f64p,
+                               P(RcMaxOut)]),
+    "rc_stats_begin": (None, [cvp]),
+    "rc_last_stats": (ci, [cvp, P(RcStats)]),
+    "rc_arena_report": (ci, [cvp, P(RcArenaReport)]),
+    "rc_arena_force_sync": (ci, [cvp, ci]),
+    "rc_device_count": (ci, []),
+    "rc_device_name": (ctypes.c_char_p, []),
+    "rc_unified": (ci, []),
+    "rc_fit_batch_fused": (cf, [cvp, u32p, u32p, i32p, ci, ci, f64p, i32p, ci, ci, ci, f64p,
+                                f64p, i32p]),
+    "rc_fit_batch_plain": (cf, [cvp, u32p, u32p, i32p, ci, ci, f64p, i32p, ci, ci, f64p, f64p,
+                                i32p]),
+    "rc_grad_batch": (ci, [cvp, u32p, u32p, i32p, ci, ci, f64p, ci, ci, ci, f32p, f32p]),
+    "rc_implicit_score_batch": (cf, [cvp, u32p, u32p, i32p, ci, ci, f64p, f64p, i32p]),
+    "rc_autotune": (ci, [cvp, u32p, u32p, ci, ctypes.c_char_p]),
+}
+
+
+def lib():
+    """Load the CUDA library. Raises when it is not built: the device path has
+    no fallback."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(CUDA_LIB):
+            raise ImportError(f"{CUDA_LIB} is not built: run the package's build.py")
+        L = ctypes.CDLL(CUDA_LIB)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _p(a, ct):
+    if a is None:
+        return None
+    return a.ctypes.data_as(ctypes.POINTER(ct))
+
+
+def _c(a, dt):
+    return None if a is None else np.ascontiguousarray(a, dtype=dt)
+
+
+# Score objective codes (RC_SCORE_*, my-version/src/cuda/eval.cu:609-640).
+SCORE_SQUARED, SCORE_ABSOLUTE, SCORE_LOG_SQUASHED, SCORE_SIGNED, SCORE_MAXIMUM = 0, 1, 2, 3, 4
+SCORE_CORRELATION, SCORE_CORRELATION_SIGNED, SCORE_AIC, SCORE_AICC, SCORE_BIC = 5, 6, 7, 8, 9
+SCORE_LOG_LOSS, SCORE_BRIER, SCORE_HINGE_SIGMOID = 10, 11, 12
+SCORE_HINGE_ORDINARY, SCORE_HINGE_SQUARED = 13, 14
+# Fit metric codes (RC_LOSS_*, eval.cu:589-604) plus the additive implicit arm.
+LOSS_SQUARED, LOSS_LOG_SQUASHED, LOSS_CORRELATION, LOSS_CORRELATION_SIGNED = 0, 1, 2, 3
+LOSS_ABSOLUTE, LOSS_LOGISTIC, LOSS_IMPLICIT = 4, 5, 6
+# Fit statuses usable by the caller (my-version/src/fit/gpu.rs:103-105).
+FIT_STATUS_USABLE = {0, 4, 5, 6, 7, 8}
+
+
+class DeviceError(RuntimeError):
+    pass
+
+
+class GpuEvaluator:
+    """One device context over a resident dataset (f32 column-major)."""
+
+    def __init__(self, cols, n, v, y):
+        L = lib()
+        self.n, self.v = int(n), int(v)
+        self._cols = _c(cols, np.float32)
+        self._y = _c(y, np.float32)
+        self.ctx = L.rc_create(_p(self._cols, ctypes.c_float), self.n, self.v,
+                               _p(self._y, ctypes.c_float))
+        if not self.ctx:
+            raise DeviceError("rc_create failed (no usable CUDA device?)")
+
+    def close(self):
+        if self.ctx:
+            lib().rc_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- data ----------------------------------------------------------
+    def set_fit_data(self, cols64, y64, w=None):
+        c, y = _c(cols64, np.float64), _c(y64, np.float64)
+        w = _c(w, np.float64) if w is not None and len(w) else None
+        rc = lib().rc_set_fit_data(self.ctx, _p(c, ctypes.c_double), _p(y, ctypes.c_double),
+                                   _p(w, ctypes.c_double))
+        if rc != 0:
+            raise DeviceError("rc_set_fit_data failed")
+
+    def set_score_weights(self, w):
+        w = _c(w, np.float64)
+        if lib().rc_set_score_weights(self.ctx, _p(w, ctypes.c_double)) != 0:
+            raise DeviceError("rc_set_score_weights failed")
+
+    def set_fit_sign(self, sign):
+        s = _c(sign, np.float64)
+        if lib().rc_set_fit_sign(self.ctx, _p(s, ctypes.c_double)) != 0:
+            raise DeviceError("rc_set_fit_sign failed")
+
+    # -- scoring -------------------------------------------------------
+    def score_batch(self, prog, off, kind, pcount=None):
+        prog, off = _c(prog, np.uint32), _c(off, np.uint32)
+        P_ = len(off) - 1
+        pc = _c(pcount if pcount is not None else np.zeros(P_), np.int32)
+        out = np.zeros(P_, np.float64)
+        status = np.zeros(P_, np.int32)
+        ms = lib().rc_score_batch(self.ctx, _p(prog, ctypes.c_uint32), _p(off, ctypes.c_uint32),
+                                  P_, kind, _p(pc, ctypes.c_int32), _p(out, ctypes.c_double),
+                                  _p(status, ctypes.c_int32))
+        if ms < 0:
+            raise DeviceError(f"rc_score_batch failed ({ms})")
+        return out, status, ms
+
+    def eval_batch(self, prog, off, loss=0):
+        prog, off = _c(prog, np.uint32), _c(off, np.uint32)
+        P_ = len(off) - 1
+        L = lib()
+        if L.rc_set_programs(self.ctx, _p(prog, ctypes.c_uint32), _p(off, ctypes.c_uint32),
+                             P_) != 0:
+            raise DeviceError("rc_set_programs failed")
+        out = np.zeros(P_, np.float32)
+        ms = L.rc_eval(self.ctx, _p(out, ctypes.c_float), loss)
+        if ms < 0:
+            raise DeviceError("rc_eval failed")
+        return out, ms
+
+    def predictions(self, prog, off):
+        prog, off = _c(prog, np.uint32), _c(off, np.uint32)
+        P_ = len(off) - 1
+        out = np.zeros((P_, self.n), np.float32)
+        if lib().rc_predict(self.ctx, _p(prog, ctypes.c_uint32), _p(off, ctypes.c_uint32), P_,
+                            _p(out, ctypes.c_float)) != 0:
+            raise DeviceError("rc_predict failed")
+        return out
+
+    # -- fitting -------------------------------------------------------
+    def _fit(self, fn, prog, off, pcount, c0, gauge, kmax, iters, metric, flags=None):
+        prog, off = _c(prog, np.uint32), _c(off, np.uint32)
+        pcount, gauge = _c(pcount, np.int32), _c(gauge, np.int32)
+        c0 = _c(c0, np.float64)
+        P_ = len(off) - 1
+        outc = np.zeros((P_, kmax), np.float64)
+        outsse = np.zeros(P_, np.float64)
+        status = np.zeros(P_, np.int32)
+        args = [self.ctx, _p(prog, ctypes.c_uint32), _p(off, ctypes.c_uint32),
+                _p(pcount, ctypes.c_int32), P_, kmax, _p(c0, ctypes.c_double),
+                _p(gauge, ctypes.c_int32), iters, metric]
+        if flags is not None:
+            args.append(flags)
+        args += [_p(outc, ctypes.c_double), _p(outsse, ctypes.c_double),
+                 _p(status, ctypes.c_int32)]
+        ms = fn(*args)
+        if ms < 0:
+            raise DeviceError(f"fit launch failed ({ms})")
+        return outc, outsse, status, ms
+
+    def fit_batch(self, prog, off, pcount, c0, gauge, kmax, iters, metric=LOSS_SQUARED):
+        return self._fit(lib().rc_fit_batch, prog, off, pcount, c0, gauge, kmax, iters, metric)
+
+    def fit_batch_fused(self, prog, off, pcount, c0, gauge, kmax, iters, metric=LOSS_SQUARED,
+                        flags=0):
+        return self._fit(lib().rc_fit_batch_fused, prog, off, pcount, c0, gauge, kmax, iters,
+                         metric, flags)
+
+    def fit_batch_plain(self, prog, off, pcount, c0, gauge, kmax, iters, metric=LOSS_SQUARED):
+        return self._fit(lib().rc_fit_batch_plain, prog, off, pcount, c0, gauge, kmax, iters,
+                         metric)
+
+    def fit_plans(self, plans, iters, metric=LOSS_SQUARED, fused=True, flags=0):
+        """Fit a list of `host.GpuFitPlan`; returns (c[P][kmax], loss[P],
+        status[P], ms)."""
+        from .host import pack_plans
+        prog, off, pcount, c0, gauge, kmax = pack_plans(plans)
+        if fused:
+            return self.fit_batch_fused(prog, off, pcount, c0, gauge, kmax, iters, metric, flags)
+        return self.fit_batch(prog, off, pcount, c0, gauge, kmax, iters, metric)
+
+    # -- gradients / implicit -------------------------------------------
+    def grad_batch(self, prog, off, pcount, c, kmax, want, row0, nrows):
+        prog, off, pcount = _c(prog, np.uint32), _c(off, np.uint32), _c(pcount, np.int32)
+        c = _c(c, np.float64)
+        P_ = len(off) - 1
+        width = kmax if want == 1 else self.v
+        value = np.zeros((P_, nrows), np.float32)
+        out = np.zeros((P_, nrows, width), np.float32)
+        rc = lib().rc_grad_batch(self.ctx, _p(prog, ctypes.c_uint32), _p(off, ctypes.c_uint32),
+                                 _p(pcount, ctypes.c_int32), P_, kmax, _p(c, ctypes.c_double),
+                                 want, row0, nrows, _p(value, ctypes.c_float),
+                                 _p(out, ctypes.c_float))
+        if rc != 0:
+            raise DeviceError("rc_grad_batch failed")
+        return value, out
+
+    def implicit_score(self, prog, off, pcount, c, kmax):
+        prog, off, pcount = _c(prog, np.uint32), _c(off, np.uint32), _c(pcount, np.int32)
+        c = _c(c, np.float64)
+        P_ = len(off) - 1
+        out = np.zeros(P_, np.float64)
+        status = np.zeros(P_, np.int32)
+        ms = lib().rc_implicit_score_batch(self.ctx, _p(prog, ctypes.c_uint32),
+                                           _p(off, ctypes.c_uint32), _p(pcount, ctypes.c_int32),
+                                           P_, kmax, _p(c, ctypes.c_double),
+                                           _p(out, ctypes.c_double), _p(status, ctypes.c_int32))
+        if ms < 0:
+            raise DeviceError("rc_implicit_score_batch failed")
+        return out, status, ms
+
+    # -- telemetry -----------------------------------------------------
+    def stats_begin(self):
+        lib().rc_stats_begin(self.ctx)
+
+    def last_stats(self):
+        s = RcStats()
+        lib().rc_last_stats(self.ctx, ctypes.byref(s))
+        return s
+
+    def arena_report(self):
+        r = RcArenaReport()
+        lib().rc_arena_report(self.ctx, ctypes.byref(r))
+        return r
+
+
+def device_count() -> int:
+    return lib().rc_device_count()
+
+
+def device_name() -> str:
+    return lib().rc_device_name().decode()

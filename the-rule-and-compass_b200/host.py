@@ -1,0 +1,172 @@
+"""Tree -> device program, through the C++ host compiler (`librcsr_host.so`).
+
+Mirrors the reference's host API for this path:
+`compile_program` (my-version/src/gpu.rs:198-219), `Population`
+(my-version/src/gpu.rs:972-1068, the packed `prog` + `off[P+1]` batch) and
+`gpu_fit_plan_reason` / `GpuFitPlan` (my-version/src/fit.rs:929-1056).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import expr as E
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+HOST_LIB = os.path.join(_HERE, "librcsr_host.so")
+_lib = None
+
+HOST_MAX_STACK = 56
+GPU_FIT_MAX_CONSTANTS = 20
+GPU_FIT_MAX_NODES = 96
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(HOST_LIB):
+            raise ImportError(f"{HOST_LIB} is not built: run the package's build.py")
+        L = ctypes.CDLL(HOST_LIB)
+        P = ctypes.POINTER
+        L.rch_compile_program.restype = ctypes.c_int
+        L.rch_compile_program.argtypes = [P(ctypes.c_int32), P(ctypes.c_double), ctypes.c_int,
+                                          P(ctypes.c_uint32), ctypes.c_int, P(ctypes.c_int)]
+        L.rch_peak_stack.restype = ctypes.c_int
+        L.rch_peak_stack.argtypes = [P(ctypes.c_int32), P(ctypes.c_double), ctypes.c_int]
+        L.rch_fit_plan.restype = ctypes.c_int
+        L.rch_fit_plan.argtypes = [P(ctypes.c_int32), P(ctypes.c_double), ctypes.c_int,
+                                   P(ctypes.c_uint32), ctypes.c_int, P(ctypes.c_double),
+                                   ctypes.c_int, P(ctypes.c_int32), P(ctypes.c_int),
+                                   ctypes.c_int]
+        _lib = L
+    return _lib
+
+
+def _p(a, ct):
+    return a.ctypes.data_as(ctypes.POINTER(ct))
+
+
+class CompileError(Exception):
+    """Why a tree cannot run on the scoring kernel (gpu.rs:131-158)."""
+
+
+def compile_program(tree: E.Node):
+    """Postfix words (HALT-terminated) and whether `lower` rewrote the tree."""
+    ops, vals = tree.prefix()
+    cap = 4 * len(ops) * 16 + 64
+    words = np.zeros(cap, np.uint32)
+    lowered = ctypes.c_int(0)
+    n = lib().rch_compile_program(_p(ops, ctypes.c_int32), _p(vals, ctypes.c_double), len(ops),
+                                  _p(words, ctypes.c_uint32), cap, ctypes.byref(lowered))
+    if n == -1:
+        raise CompileError("unsupported operator")
+    if n == -2:
+        raise CompileError(f"postfix program needs more than {HOST_MAX_STACK} stack slots")
+    if n < 0:
+        raise CompileError(f"malformed tree ({n})")
+    return words[:n].copy(), bool(lowered.value)
+
+
+def peak_stack(tree: E.Node) -> int:
+    ops, vals = tree.prefix()
+    return lib().rch_peak_stack(_p(ops, ctypes.c_int32), _p(vals, ctypes.c_double), len(ops))
+
+
+class Population:
+    """Packed postfix batch `(prog, off)`; unsupported trees are counted and
+    skipped (gpu.rs:972-1068)."""
+
+    def __init__(self, trees=()):
+        self._words = []
+        self.offsets = [0]
+        self.unsupported = 0
+        self.lowered = 0
+        self.index = []
+        for i, t in enumerate(trees):
+            if self.add(t):
+                self.index.append(i)
+
+    def add(self, tree) -> bool:
+        try:
+            w, low = compile_program(tree)
+        except CompileError:
+            self.unsupported += 1
+            return False
+        self._words.append(w)
+        self.offsets.append(self.offsets[-1] + len(w))
+        self.lowered += int(low)
+        return True
+
+    def __len__(self):
+        return len(self.offsets) - 1
+
+    def programs(self):
+        prog = np.concatenate(self._words).astype(np.uint32) if self._words else \
+            np.zeros(0, np.uint32)
+        return prog, np.asarray(self.offsets, np.uint32)
+
+
+REJECT = {-1: "too_many_constants", -2: "too_many_nodes", -3: "no_constants",
+          -5: "unsupported_op", -4: "malformed", -6: "capacity"}
+
+
+class GpuFitPlan:
+    """One candidate flattened for the fit kernel (fit.rs:929-950)."""
+
+    def __init__(self, words, c0, gauge, nconst):
+        self.words = words
+        self.c0 = c0
+        self.gauge = gauge
+        self.nconst = nconst
+
+    @property
+    def nodes(self):
+        return len(self.words) // 4
+
+    def apply(self, tree: E.Node, c) -> E.Node:
+        """Write fitted constants back into a copy of `tree` (slot order is the
+        tree's pre-order constant order)."""
+        t = tree.clone()
+        t.set_constants(list(c)[: self.nconst])
+        return t
+
+
+class GpuFitReject(Exception):
+    def __init__(self, code):
+        super().__init__(REJECT.get(code, str(code)))
+        self.label = REJECT.get(code, str(code))
+
+
+def gpu_fit_plan(tree: E.Node, allow_no_constants=False) -> GpuFitPlan:
+    ops, vals = tree.prefix()
+    cap = 4 * max(len(ops), 1)
+    words = np.zeros(cap, np.uint32)
+    c0 = np.zeros(max(len(ops), 1), np.float64)
+    gauge = np.full(2, -1, np.int32)
+    nconst = ctypes.c_int(0)
+    m = lib().rch_fit_plan(_p(ops, ctypes.c_int32), _p(vals, ctypes.c_double), len(ops),
+                           _p(words, ctypes.c_uint32), cap, _p(c0, ctypes.c_double), len(c0),
+                           _p(gauge, ctypes.c_int32), ctypes.byref(nconst),
+                           1 if allow_no_constants else 0)
+    if m < 0:
+        raise GpuFitReject(m)
+    k = nconst.value
+    return GpuFitPlan(words[: 4 * m].copy(), c0[:k].copy(), gauge.copy(), k)
+
+
+def pack_plans(plans, kmax=None):
+    """Concatenate fit plans into the rc_fit_batch inputs:
+    (prog, off, pcount, c0[P*kmax], gauge[2P], kmax)."""
+    if kmax is None:
+        kmax = max([p.nconst for p in plans] + [1])
+    prog = np.concatenate([p.words for p in plans]).astype(np.uint32)
+    off = np.zeros(len(plans) + 1, np.uint32)
+    off[1:] = np.cumsum([len(p.words) for p in plans])
+    pcount = np.asarray([p.nconst for p in plans], np.int32)
+    c0 = np.zeros((len(plans), kmax), np.float64)
+    for i, p in enumerate(plans):
+        c0[i, : p.nconst] = p.c0
+    gauge = np.concatenate([p.gauge for p in plans]).astype(np.int32)
+    return prog, off, pcount, c0, gauge, kmax
