@@ -209,6 +209,31 @@ float rc_implicit_score_batch(void *ctx, const unsigned int *prog, const unsigne
 int rc_autotune(void *ctx, const unsigned int *prog, const unsigned int *off, int nprog,
                 const char *path);
 
+/* Scoring for callers that cannot allocate device memory. No counterpart in
+   the reference: it exists for host applications whose device memory is
+   owned by another allocator, and for pipelined callers on their own streams
+   for whom cudaMalloc/cudaFree (which synchronise the device) are not
+   acceptable. It calls no allocator at all; its scratch is a static
+   16 MiB device array that every GPU loading this library holds until exit.
+
+   Every buffer is a caller-owned device pointer: cols is column-major with
+   leading dimension ld (ld % 4 == 0, ld >= n rounded up to 1024 rows, those
+   padding rows readable), y has ld readable entries, cols and y are 16-byte
+   aligned, prog/off are the packed postfix batch (off[nprog + 1]), out/status
+   receive nprog results. kind is 0..4 (squared, absolute, log-squashed,
+   signed, maximum) with rc_score_batch's values and statuses; a program
+   needing more than 16 stack entries gets status 3 and NaN. The work is
+   enqueued on `stream` (a cudaStream_t, NULL = legacy default stream) and
+   the call returns without waiting. Returns 0; -2 when the batch needs more
+   scratch than the static maximum; -3 for an invalid argument or layout;
+   -1 for a CUDA error. The first call on a device looks up the scratch
+   address and sets kernel attributes, so make it before any stream capture.
+   All calls share the one scratch array: calls that overlap on the GPU race
+   and must be serialised by the caller. */
+int rc_score_batch_noalloc(const float *cols, const float *y, int n, int v, int ld,
+                           const unsigned int *prog, const unsigned int *off, int nprog, int kind,
+                           double *out, int *status, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

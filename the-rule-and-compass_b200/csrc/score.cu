@@ -27,6 +27,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <vector>
 
@@ -1155,5 +1156,278 @@ extern "C" int rc_pool_hash(void *ctx, int which, int nprog, int width, unsigned
                     cudaMemcpyDeviceToHost, c->s);
     if (rc_finish(c) != 0) return -1;
     memcpy(out, c->host + o, sizeof(unsigned long long) * nprog);
+    return 0;
+}
+
+/* ======================================================================
+ * Scoring without any allocation.
+ *
+ * Some callers cannot call cudaMalloc at all: a host application whose
+ * device memory belongs to another allocator (a caching pool that must not
+ * be bypassed or fragmented), or a pipelined search loop on its own streams
+ * where cudaMalloc/cudaFree would synchronise the whole device and stall
+ * the work in flight. rc_score_batch_noalloc serves them: the caller owns
+ * every input and output buffer on the device, and the kernel's scratch
+ * (decoded programs, per-tile partial sums, flags, the work counter) lives
+ * in one file-scope __device__ array of RC_NOALLOC_SCRATCH_BYTES, which
+ * every GPU that loads this library holds until the process exits.
+ *
+ * All calls share that array and it keeps the previous call's contents:
+ * the counter and flags are cleared at the start of every call, and two
+ * calls that overlap on the GPU (different streams, or host threads racing
+ * on one device) race on the scratch and produce garbage. Serialise them.
+ * ====================================================================== */
+
+#define RC_NOALLOC_SCRATCH_BYTES (16u << 20)
+#define RC_NOALLOC_MAX_DEVICES 64
+#define RC_NOALLOC_TOO_DEEP 3
+
+static __device__ __align__(256) unsigned char rc_noalloc_scratch[RC_NOALLOC_SCRATCH_BYTES];
+
+/* Device-side decoder: one thread per program, the same translation as the
+   host decoder (rc_decode_postfix) into a fixed stride of RC_MAX_INS
+   instructions. A program needing more than RC_SHALLOW_SLOTS spill slots is
+   replaced by K_NAN and flagged `deep`. */
+__global__ void rc_noalloc_decode(const unsigned int *__restrict__ prog,
+                                  const unsigned int *__restrict__ off, int nprog, int v,
+                                  RcIns *__restrict__ ins, int *__restrict__ ins_off,
+                                  int *__restrict__ order, int *__restrict__ cand_tiles,
+                                  int *__restrict__ deep, int ntiles)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p > nprog) return;
+    ins_off[p] = p * RC_MAX_INS;
+    if (p == nprog) return;
+    order[p] = p;
+    cand_tiles[p] = ntiles;
+    deep[p] = 0;
+    RcIns *out = ins + (size_t)p * RC_MAX_INS;
+    const unsigned int b = off[p], e = off[p + 1];
+    int depth = 0, maxslot = -1, n = 0;
+    bool ok = e >= b, halted = false;
+    unsigned int i = b;
+    while (ok && i < e) {
+        const unsigned int w = prog[i++];
+        RcIns in;
+        in.kind = 0;
+        in.op = 0;
+        in.arg = 0;
+        in.spill = 0xff;
+        in.imm = 0;
+        if (w == OP_CONST || w == OP_VAR) {
+            if (i >= e || depth >= RC_MAX_STACK) { ok = false; break; }
+            const unsigned int a = prog[i++];
+            if (w == OP_VAR && (long long)a >= (long long)v) { ok = false; break; }
+            in.kind = w == OP_CONST ? K_PUSH_CONST : K_PUSH_VAR;
+            in.spill = depth >= 1 ? (uint8_t)(depth - 1) : 0xff;
+            in.imm = a;
+            if (depth >= 1 && depth - 1 > maxslot) maxslot = depth - 1;
+            ++depth;
+        } else if (w == OP_HALT) {
+            if (depth < 1) { ok = false; break; }
+            in.kind = K_HALT;
+            in.arg = depth == 1 ? 1 : 0;
+            halted = true;
+        } else if (w == OP_ADD || w == OP_SUB || w == OP_MUL || w == OP_DIV || w == OP_POW ||
+                   w == OP_MOD || w == OP_ATAN2 || w == OP_MIN || w == OP_MAX ||
+                   w == OP_EQUAL || w == OP_LESS || w == OP_LESS_OR_EQUAL ||
+                   w == OP_GREATER || w == OP_GREATER_OR_EQUAL || w == OP_AND || w == OP_OR ||
+                   w == OP_XOR) {
+            if (depth < 2) { ok = false; break; }
+            in.kind = K_BIN_S;
+            in.op = (uint8_t)w;
+            in.arg = (uint8_t)(depth - 2);
+            --depth;
+            const bool fus = w == OP_ADD || w == OP_SUB || w == OP_MUL || w == OP_DIV ||
+                             w == OP_POW;
+            if (n > 0 && fus) {
+                RcIns &prev = out[n - 1];
+                if ((prev.kind == K_PUSH_VAR || prev.kind == K_PUSH_CONST) &&
+                    prev.spill != 0xff && prev.spill == in.arg) {
+                    prev.kind = prev.kind == K_PUSH_VAR ? K_BIN_V : K_BIN_C;
+                    prev.op = (uint8_t)w;
+                    prev.spill = 0xff;
+                    continue;
+                }
+            }
+        } else if (w == OP_IF) {
+            if (depth < 3) { ok = false; break; }
+            in.kind = K_IF;
+            in.arg = (uint8_t)(depth - 3);
+            depth -= 2;
+        } else {
+            if (depth < 1) { ok = false; break; }
+            in.kind = K_UNARY;
+            in.op = w > 253 ? 254 : (uint8_t)w;
+        }
+        if (n >= RC_MAX_INS) { ok = false; break; }
+        out[n++] = in;
+        if (halted) break;
+    }
+    if (!ok || !halted || maxslot + 1 > RC_SHALLOW_SLOTS) {
+        deep[p] = ok && halted ? 1 : 0;
+        RcIns bad;
+        bad.kind = K_NAN;
+        bad.op = 0;
+        bad.arg = 0;
+        bad.spill = 0xff;
+        bad.imm = 0;
+        out[0] = bad;
+    }
+}
+
+__global__ void rc_noalloc_mark_deep(int nprog, const int *__restrict__ deep,
+                                     double *__restrict__ out, int *__restrict__ status)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < nprog && deep[p]) {
+        out[p] = CUDART_NAN;
+        status[p] = RC_NOALLOC_TOO_DEEP;
+    }
+}
+
+namespace {
+struct NoallocDevice {
+    int ready;
+    unsigned char *scratch; /* device address of rc_noalloc_scratch */
+    int sm_count;
+    int grid_per_sm;
+};
+NoallocDevice g_noalloc[RC_NOALLOC_MAX_DEVICES];
+std::mutex g_noalloc_mu;
+}  // namespace
+
+extern "C" int rc_score_batch_noalloc(const float *cols, const float *y, int n, int v, int ld,
+                                      const unsigned int *prog, const unsigned int *off,
+                                      int nprog, int kind, double *out, int *status,
+                                      void *stream)
+{
+    const int T = 256;
+    const int SUB = T * 4;
+    if (!cols || !y || !prog || !off || !out || !status || n <= 0 || v <= 0 || nprog <= 0) {
+        fprintf(stderr, "rc_score_batch_noalloc: null pointer or empty size\n");
+        return -3;
+    }
+    if (kind < SM_SQUARED || kind > SM_MAXIMUM) {
+        fprintf(stderr, "rc_score_batch_noalloc: kind %d unsupported (0..4 only)\n", kind);
+        return -3;
+    }
+    if (v + 1 > stage_limit_cols() + 1) {
+        fprintf(stderr, "rc_score_batch_noalloc: %d columns exceed the staged limit %d\n", v,
+                stage_limit_cols());
+        return -3;
+    }
+    const long long need_rows = ((long long)n + SUB - 1) / SUB * SUB;
+    if ((long long)ld < need_rows || (ld % 4) != 0 || ((uintptr_t)cols % 16) != 0 ||
+        ((uintptr_t)y % 16) != 0) {
+        fprintf(stderr,
+                "rc_score_batch_noalloc: ld must be a multiple of 4 and >= %lld (n rounded up "
+                "to %d rows, readable), cols and y 16-byte aligned\n",
+                need_rows, SUB);
+        return -3;
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= RC_NOALLOC_MAX_DEVICES) {
+        cudaGetLastError();
+        return -1;
+    }
+    const int ntiles = (int)((n + TILE_ROWS - 1) / TILE_ROWS);
+    size_t cur = 0;
+    const size_t o_ins = rc_take(&cur, sizeof(RcIns) * (size_t)nprog * RC_MAX_INS);
+    const size_t o_insoff = rc_take(&cur, sizeof(int) * ((size_t)nprog + 1));
+    const size_t o_order = rc_take(&cur, sizeof(int) * (size_t)nprog);
+    const size_t o_ctiles = rc_take(&cur, sizeof(int) * (size_t)nprog);
+    const size_t o_deep = rc_take(&cur, sizeof(int) * (size_t)nprog);
+    const size_t o_part = rc_take(&cur, sizeof(double) * (size_t)nprog * ntiles);
+    const size_t o_bad = rc_take(&cur, sizeof(int) * (size_t)nprog);
+    const size_t o_cnt = rc_take(&cur, sizeof(int) * 8);
+    const size_t need = rc_take(&cur, 0);
+    if (need > RC_NOALLOC_SCRATCH_BYTES) {
+        fprintf(stderr,
+                "rc_score_batch_noalloc: %d programs over %d rows need %zu scratch bytes, the "
+                "static maximum is %u\n",
+                nprog, n, need, RC_NOALLOC_SCRATCH_BYTES);
+        return -2;
+    }
+    const int G = 8;
+    const size_t smem = (size_t)(v + 1) * T * 16 + (size_t)RC_SHALLOW_SLOTS * T * 16 +
+                        (size_t)G * T * 16 + (size_t)G * RC_MAX_INS * sizeof(RcIns);
+    NoallocDevice *d = &g_noalloc[dev];
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!d->ready) {
+            void *ptr = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&ptr, rc_noalloc_scratch);
+            if (e != cudaSuccess || !ptr) {
+                fprintf(stderr, "rc_score_batch_noalloc: cudaGetSymbolAddress failed: %s\n",
+                        cudaGetErrorString(e));
+                cudaGetLastError();
+                return -1;
+            }
+            const int maxsmem = (int)((size_t)(stage_limit_cols() + 1) * T * 16 +
+                                      (size_t)RC_SHALLOW_SLOTS * T * 16 + (size_t)G * T * 16 +
+                                      (size_t)G * RC_MAX_INS * sizeof(RcIns));
+            if (cudaFuncSetAttribute((const void *)rc_score_kernel<256, true>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     maxsmem) != cudaSuccess) {
+                cudaGetLastError();
+                return -1;
+            }
+            int sms = 1, per = 1;
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                    &per, rc_score_kernel<256, true>, T, (size_t)maxsmem) != cudaSuccess) {
+                cudaGetLastError();
+                per = 1;
+            }
+            d->scratch = (unsigned char *)ptr;
+            d->sm_count = sms > 0 ? sms : 1;
+            d->grid_per_sm = per > 0 ? per : 1;
+            d->ready = 1;
+        }
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned char *sc = d->scratch;
+    cudaMemsetAsync(sc + o_bad, 0, o_cnt - o_bad + sizeof(int) * 8, s);
+    rc_noalloc_decode<<<(nprog + 1 + 127) / 128, 128, 0, s>>>(
+        prog, off, nprog, v, reinterpret_cast<RcIns *>(sc + o_ins),
+        reinterpret_cast<int *>(sc + o_insoff), reinterpret_cast<int *>(sc + o_order),
+        reinterpret_cast<int *>(sc + o_ctiles), reinterpret_cast<int *>(sc + o_deep), ntiles);
+    ScoreArgs a;
+    memset(&a, 0, sizeof(a));
+    a.cols = cols;
+    a.y = y;
+    a.n = n;
+    a.npad = ld;
+    a.v = v;
+    a.ins = reinterpret_cast<const RcIns *>(sc + o_ins);
+    a.ins_off = reinterpret_cast<const int *>(sc + o_insoff);
+    a.order = reinterpret_cast<const int *>(sc + o_order);
+    a.ncand = nprog;
+    a.group = G < nprog ? G : nprog;
+    a.subtiles = TILE_ROWS / SUB;
+    a.ntiles = ntiles;
+    a.nitems = ((nprog + a.group - 1) / a.group) * ntiles;
+    a.maxins = RC_MAX_INS;
+    a.nslots = RC_SHALLOW_SLOTS;
+    a.counter = reinterpret_cast<int *>(sc + o_cnt);
+    a.partial = reinterpret_cast<double *>(sc + o_part);
+    a.partial2 = nullptr;
+    a.ptiles = ntiles;
+    a.bad = reinterpret_cast<int *>(sc + o_bad);
+    a.mode = kind;
+    int grid = d->sm_count * d->grid_per_sm;
+    if (grid > a.nitems) grid = a.nitems;
+    rc_score_kernel<256, true><<<grid, T, smem, s>>>(a);
+    rc_score_finalize<<<(nprog + 127) / 128, 128, 0, s>>>(
+        nprog, reinterpret_cast<const int *>(sc + o_ctiles), a.partial, nullptr, ntiles, a.bad, n,
+        kind, 0.0, out, status, nullptr, nullptr);
+    rc_noalloc_mark_deep<<<(nprog + 127) / 128, 128, 0, s>>>(
+        nprog, reinterpret_cast<const int *>(sc + o_deep), out, status);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        fprintf(stderr, "rc_score_batch_noalloc: launch failed: %s\n", cudaGetErrorString(e));
+        return -1;
+    }
     return 0;
 }

@@ -88,6 +88,7 @@ SIGNATURES = {
     "rc_grad_batch": (ci, [cvp, u32p, u32p, i32p, ci, ci, f64p, ci, ci, ci, f32p, f32p]),
     "rc_implicit_score_batch": (cf, [cvp, u32p, u32p, i32p, ci, ci, f64p, f64p, i32p]),
     "rc_autotune": (ci, [cvp, u32p, u32p, ci, ctypes.c_char_p]),
+    "rc_score_batch_noalloc": (ci, [cvp, cvp, ci, ci, ci, cvp, cvp, ci, ci, cvp, cvp, cvp]),
 }
 
 
