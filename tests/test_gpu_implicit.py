@@ -1,0 +1,105 @@
+"""The implicit |f|/||grad f|| metric on the device (the fused input adjoint)
+against the CPU oracle (my-version/src/implicit.rs:68-409; tests
+implicit.rs:436-495 and my-version/tests/implicit.rs:144-265)."""
+import importlib
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def circle_tree(E, c):
+    return E.node(E.SUB, [E.node(E.ADD, [E.node(E.SQUARE, [E.input(0)]),
+                                         E.node(E.SQUARE, [E.input(1)])]), E.constant(c)])
+
+
+def evaluator(pkg, cols):
+    v, n = cols.shape
+    ev = pkg.GpuEvaluator(cols.astype(np.float32).reshape(-1), n, v, np.zeros(n, np.float32))
+    ev.set_fit_data(cols.reshape(-1), np.zeros(n))
+    return ev
+
+
+def unit_circle(n):
+    th = 2 * np.pi * np.arange(n) / n
+    return np.stack([np.cos(th), np.sin(th)])
+
+
+def score(pkg, ev, trees):
+    plans = [pkg.gpu_fit_plan(t, allow_no_constants=True) for t in trees]
+    prog, off, pcount, c0, gauge, kmax = pkg.pack_plans(plans)
+    return ev.implicit_score(prog, off, pcount, c0, kmax)
+
+
+def test_level_set_distance_and_scale_freedom(pkg, E):
+    cols = unit_circle(512)
+    ev = evaluator(pkg, cols)
+    f = circle_tree(E, 1.0)
+    scaled = E.node(E.MUL, [E.constant(7.0), f])
+    vals, status, _ = score(pkg, ev, [f, scaled])
+    assert list(status) == [0, 0]
+    assert vals[0] < 1e-6
+    assert abs(vals[1] - vals[0]) <= 1e-6
+    ev.close()
+
+
+def test_zero_gradient_is_infeasible(pkg, E):
+    cols = unit_circle(64)
+    ev = evaluator(pkg, cols)
+    vals, status, _ = score(pkg, ev, [E.constant(0.0), E.constant(3.0)])
+    assert list(status) == [2, 2]
+    assert all(math.isinf(v) for v in vals)
+    ev.close()
+
+
+def test_implicit_score_matches_the_oracle(pkg, E, O):
+    W = importlib.import_module("the-rule-and-compass_b200.workloads")
+    trees, cols = W.implicit_workload(96, 4096, seed=4)
+    ev = evaluator(pkg, cols)
+    vals, status, _ = score(pkg, ev, trees)
+    x32 = cols.astype(np.float32).astype(np.float64).reshape(-1)
+    mismatch, checked = 0, 0
+    for k, t in enumerate(trees):
+        want = O.implicit_score(t, x32, cols.shape[1], cols.shape[0])
+        if math.isinf(want) != (status[k] == 2):
+            mismatch += 1
+            continue
+        if math.isinf(want):
+            continue
+        assert abs(vals[k] - want) <= 1e-4 * abs(want) + 1e-9, (k, vals[k], want, t)
+        checked += 1
+    assert checked >= 20
+    assert mismatch <= 2, mismatch
+
+
+def test_implicit_fit_recovers_the_radius(pkg, E, O):
+    cols = unit_circle(16)
+    ev = evaluator(pkg, cols)
+    t = circle_tree(E, 4.0)
+    plan = pkg.gpu_fit_plan(t)
+    c, loss, status, _ = ev.fit_plans([plan], 20, metric=6)
+    assert status[0] == 0
+    fitted = plan.apply(t, c[0])
+    radius = -O.predict(fitted, np.zeros(2), 1, 2)[0]
+    assert abs(radius - 1.0) < 1e-6
+    cpu_sse, _ = O.implicit_fit(t, cols.reshape(-1), 16, 2, 20)
+    assert loss[0] <= cpu_sse * (1 + 1e-6) + 1e-20
+    ev.close()
+
+
+def test_implicit_fit_on_noisy_circle_tracks_the_cpu_fit(pkg, E, O):
+    W = importlib.import_module("the-rule-and-compass_b200.workloads")
+    cols = W.implicit_data(2000, seed=9)
+    ev = evaluator(pkg, cols)
+    t = E.node(E.SUB, [E.node(E.ADD, [E.node(E.MUL, [E.constant(1.3), E.node(E.SQUARE, [E.input(0)])]),
+                                      E.node(E.SQUARE, [E.input(1)])]), E.constant(2.0)])
+    plan = pkg.gpu_fit_plan(t)
+    c, loss, status, _ = ev.fit_plans([plan], 20, metric=6)
+    assert status[0] in (0, 6)
+    cpu_sse, cpu_tree = O.implicit_fit(t, cols.reshape(-1), 2000, 4, 20)
+    assert abs(loss[0] - cpu_sse) <= 1e-6 * cpu_sse, (loss[0], cpu_sse)
+    for a, b in zip(plan.apply(t, c[0]).constants(), cpu_tree.constants()):
+        assert abs(a - b) <= 1e-5 * (1 + abs(b))
+    ev.close()

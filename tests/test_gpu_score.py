@@ -67,23 +67,28 @@ def test_native_objectives_match_the_cpu_reducer(pkg, E, O, ev_fix):
     prog, off = pop.programs()
     preds = ev.predictions(prog, off).astype(np.float64)
     y64 = y.astype(np.float64)
+    x64 = cols.astype(np.float64).reshape(-1)
     pcount = np.full(len(trees), 2, np.int32)
     for kind in OBJECTIVES:
         vals, status, ms = ev.score_batch(prog, off, kind, pcount)
         assert ms >= 0
         for k in range(len(trees)):
-            want = O.score_pred(preds[k], y64, kind, 2)
+            # a candidate is reduced from its f32 predictions, or -- when its
+            # error bound flags it -- rescored in f64 like the CPU oracle
+            want32 = O.score_pred(preds[k], y64, kind, 2)
+            t32 = trees[k].clone()
+            t32.set_constants([float(np.float32(c)) for c in t32.constants()])
+            want64 = O.score_pred(O.predict(t32, x64, n, nv), y64, kind, 2)
             got = vals[k]
             assert status[k] == 0, (kind, k)
             if kind == 4:
-                assert got == want, (kind, k, got, want)
-            elif math.isinf(want):
-                assert got == want
-            elif kind in (5, 6):
-                assert abs(got - want) <= 1e-9, (kind, k, got, want)
+                assert got in (want32, want64), (kind, k, got, want32, want64)
+            elif math.isinf(want32):
+                assert got == want32
             else:
-                tol = 1e-12 * (1.0 + abs(want))
-                assert abs(got - want) <= tol, (kind, k, got, want)
+                tol = (1e-9 if kind in (5, 6) else 1e-12) * (1.0 + abs(want32))
+                assert min(abs(got - want32), abs(got - want64)) <= tol, \
+                    (kind, k, got, want32, want64)
 
 
 def test_nonfinite_is_inf_with_status(pkg, E):
@@ -211,5 +216,31 @@ def test_random_batch_matches_the_oracle(pkg, E, O):
             if cpu_bad:
                 continue
             assert abs(vals[k] - want) <= 1e-4 * abs(want) + 1e-12, (k, vals[k], want, t)
-        assert mismatch <= P // 50, mismatch
+        assert mismatch == 0, mismatch
+    ev.close()
+
+
+def test_ill_conditioned_candidates_are_rescored_in_f64(pkg, E, O):
+    """A near-cancelling denominator amplifies f32 rounding far beyond 1e-4
+    (c / (sin(x1)/x4 - x0) on this seed's rows); the error bound flags it and
+    the f64 lane brings it back within the parity bar, as for every other
+    candidate of the batch."""
+    W = __import__("importlib").import_module("the-rule-and-compass_b200.workloads")
+    trees, x, y = W.scoring_workload(64, 4096, seed=1)
+    ev = pkg.GpuEvaluator(x.reshape(-1), 4096, 5, y)
+    prog, off = pkg.Population(trees).programs()
+    x64 = x.astype(np.float64).reshape(-1)
+    y64 = y.astype(np.float64)
+    for kind, metric in ((0, O.SQUARED), (1, O.ABSOLUTE), (2, O.LOG_SQUASHED), (3, O.SIGNED),
+                         (4, O.MAXIMUM)):
+        vals, status, _ = ev.score_batch(prog, off, kind)
+        for k, t in enumerate(trees):
+            t32 = t.clone()
+            t32.set_constants([float(np.float32(c)) for c in t.constants()])
+            want = O.score(t32, x64, 4096, 5, y64, metric)
+            pred = O.predict(t32, x64, 4096, 5)
+            cpu_bad = (not math.isfinite(want)) or bool(np.any(np.abs(pred) > 1e30))
+            assert cpu_bad == (status[k] == 2), (kind, k, t)
+            if not cpu_bad:
+                assert abs(vals[k] - want) <= 1e-4 * abs(want) + 1e-12, (kind, k, vals[k], want)
     ev.close()

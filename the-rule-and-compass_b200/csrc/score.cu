@@ -34,20 +34,7 @@
 #include "rc_internal.h"
 #include "rc_ops.cuh"
 
-/* Internal scoring modes. 0..9 are the RC_SCORE_* regression codes
-   (eval.cu:609-619); the rest are internal. */
-enum {
-    SM_SQUARED = 0, SM_ABSOLUTE = 1, SM_LOG_SQUASHED = 2, SM_SIGNED = 3, SM_MAXIMUM = 4,
-    SM_CORRELATION = 5, SM_CORRELATION_SIGNED = 6, SM_AIC = 7, SM_AICC = 8, SM_BIC = 9,
-    SM_LOG_LOSS = 10, SM_BRIER = 11, SM_HINGE_SIGMOID = 12, SM_HINGE_ORDINARY = 13,
-    SM_HINGE_SQUARED = 14,
-    SM_EVAL_SQUARED = 20, SM_EVAL_LOG_SQUASHED = 21, SM_EVAL_ABSOLUTE = 24,
-    SM_PREDICT = 30,
-    SM_CORR_PASS1 = 31, SM_CORR_PASS2 = 32
-};
-
-#define RC_SCORE_NONFINITE 2
-#define RC_SCORE_ALL_ZERO_WEIGHT 4
+#include "score_kernels.cuh"
 
 /* ---- host decoder --------------------------------------------------- */
 
@@ -153,577 +140,6 @@ int rc_decode_postfix(const uint32_t *words, size_t nwords, int v, RcIns *out, i
     return (int)ins.size();
 }
 
-/* ---- device interpreter --------------------------------------------- */
-
-#define U4(OPC)                                  \
-    {                                            \
-        t0 = rc_unary_f(OPC, t0);                \
-        t1 = rc_unary_f(OPC, t1);                \
-        t2 = rc_unary_f(OPC, t2);                \
-        t3 = rc_unary_f(OPC, t3);                \
-    }
-#define B4(OPC)                                  \
-    {                                            \
-        t0 = rc_binary_f(OPC, a0, b0);           \
-        t1 = rc_binary_f(OPC, a1, b1);           \
-        t2 = rc_binary_f(OPC, a2, b2);           \
-        t3 = rc_binary_f(OPC, a3, b3);           \
-    }
-
-/* Evaluate one decoded program on this thread's four rows. `xs` holds the
-   staged feature columns ([k][T] float4), `stk` the spill slots ([slot][T]
-   float4). Returns the four predictions in p. */
-template <int T>
-__device__ __forceinline__ void rc_run(const RcIns *__restrict__ prog, const float4 *xs,
-                                       float4 *stk, int tid, float4 &p)
-{
-    float t0 = 0.f, t1 = 0.f, t2 = 0.f, t3 = 0.f;
-    for (int pc = 0; pc < RC_MAX_INS; ++pc) {
-        const RcIns in = prog[pc];
-        const unsigned kind = in.kind;
-        if (kind <= K_PUSH_CONST) {
-            if (in.spill != 0xff) stk[in.spill * T + tid] = make_float4(t0, t1, t2, t3);
-            if (kind == K_PUSH_VAR) {
-                const float4 x = xs[in.imm * T + tid];
-                t0 = x.x; t1 = x.y; t2 = x.z; t3 = x.w;
-            } else {
-                const float c = __uint_as_float(in.imm);
-                t0 = c; t1 = c; t2 = c; t3 = c;
-            }
-            continue;
-        }
-        if (kind == K_UNARY) {
-            switch (in.op) {
-                case OP_SIN: U4(OP_SIN); break;
-                case OP_COS: U4(OP_COS); break;
-                case OP_TAN: U4(OP_TAN); break;
-                case OP_EXP: U4(OP_EXP); break;
-                case OP_LOG: U4(OP_LOG); break;
-                case OP_SQRT: U4(OP_SQRT); break;
-                case OP_ABS: U4(OP_ABS); break;
-                case OP_TANH: U4(OP_TANH); break;
-                case OP_SIG: U4(OP_SIG); break;
-                case OP_SQUARE: U4(OP_SQUARE); break;
-                case OP_CUBE: U4(OP_CUBE); break;
-                case OP_NEG: U4(OP_NEG); break;
-                case OP_GAUSS: U4(OP_GAUSS); break;
-                case OP_STEP: U4(OP_STEP); break;
-                case OP_SINH: U4(OP_SINH); break;
-                case OP_COSH: U4(OP_COSH); break;
-                case OP_FLOOR: U4(OP_FLOOR); break;
-                case OP_CEIL: U4(OP_CEIL); break;
-                case OP_ROUND: U4(OP_ROUND); break;
-                case OP_ERF: U4(OP_ERF); break;
-                case OP_ERFC: U4(OP_ERFC); break;
-                case OP_SIGN: U4(OP_SIGN); break;
-                case OP_NOT: U4(OP_NOT); break;
-                default: t0 = t1 = t2 = t3 = rc_nanf(); break;
-            }
-            continue;
-        }
-        if (kind <= K_BIN_C) {
-            float a0, a1, a2, a3, b0, b1, b2, b3;
-            if (kind == K_BIN_S) {
-                const float4 a = stk[in.arg * T + tid];
-                a0 = a.x; a1 = a.y; a2 = a.z; a3 = a.w;
-                b0 = t0; b1 = t1; b2 = t2; b3 = t3;
-            } else if (kind == K_BIN_V) {
-                const float4 b = xs[in.imm * T + tid];
-                a0 = t0; a1 = t1; a2 = t2; a3 = t3;
-                b0 = b.x; b1 = b.y; b2 = b.z; b3 = b.w;
-            } else {
-                const float c = __uint_as_float(in.imm);
-                a0 = t0; a1 = t1; a2 = t2; a3 = t3;
-                b0 = c; b1 = c; b2 = c; b3 = c;
-            }
-            switch (in.op) {
-                case OP_ADD: B4(OP_ADD); break;
-                case OP_SUB: B4(OP_SUB); break;
-                case OP_MUL: B4(OP_MUL); break;
-                case OP_DIV: B4(OP_DIV); break;
-                case OP_POW: B4(OP_POW); break;
-                case OP_MOD: B4(OP_MOD); break;
-                case OP_ATAN2: B4(OP_ATAN2); break;
-                case OP_MIN: B4(OP_MIN); break;
-                case OP_MAX: B4(OP_MAX); break;
-                case OP_EQUAL: B4(OP_EQUAL); break;
-                case OP_LESS: B4(OP_LESS); break;
-                case OP_LESS_OR_EQUAL: B4(OP_LESS_OR_EQUAL); break;
-                case OP_GREATER: B4(OP_GREATER); break;
-                case OP_GREATER_OR_EQUAL: B4(OP_GREATER_OR_EQUAL); break;
-                case OP_AND: B4(OP_AND); break;
-                case OP_OR: B4(OP_OR); break;
-                case OP_XOR: B4(OP_XOR); break;
-                default: t0 = t1 = t2 = t3 = rc_nanf(); break;
-            }
-            continue;
-        }
-        if (kind == K_IF) {
-            /* Both arms are already evaluated; the select discards the other
-               one, NaN included (eval.cu:515-521). */
-            const float4 cnd = stk[in.arg * T + tid];
-            const float4 a = stk[(in.arg + 1) * T + tid];
-            t0 = cnd.x > 0.0f ? a.x : t0;
-            t1 = cnd.y > 0.0f ? a.y : t1;
-            t2 = cnd.z > 0.0f ? a.z : t2;
-            t3 = cnd.w > 0.0f ? a.w : t3;
-            continue;
-        }
-        if (kind == K_HALT) {
-            if (in.arg == 1) {
-                p = make_float4(t0, t1, t2, t3);
-            } else {
-                p = stk[tid]; /* the reference returns s[0] (eval.cu:429) */
-            }
-            return;
-        }
-        break; /* K_NAN */
-    }
-    p = make_float4(rc_nanf(), rc_nanf(), rc_nanf(), rc_nanf());
-}
-
-/* The f32 row loss of the legacy evaluator (eval.cu:712-727). */
-__device__ __forceinline__ float rc_row_loss(float r, int loss)
-{
-    if (loss == 1) {
-        const float rr = r * r;
-        return isfinite(rr) ? log1pf(rr) : 2.0f * logf(fabsf(r));
-    }
-    if (loss == 4) return fabsf(r);
-    if (loss != 0) return rc_nanf();
-    return r * r;
-}
-
-__device__ __forceinline__ float rc_sigmoid_f(float x)
-{
-    if (x >= 0.0f) return 1.0f / (1.0f + expf(-x));
-    const float e = expf(x);
-    return e / (1.0f + e);
-}
-
-/* Labelled row loss (eval.cu:696-728 `rc_class_row_loss`). */
-__device__ __forceinline__ float rc_class_row_loss(float p, float tsign, int loss)
-{
-    const float u = tsign * p;
-    if (loss == SM_LOG_LOSS) {
-        const float a = fabsf(u);
-        return (u < 0.0f ? -u : 0.0f) + log1pf(expf(-a));
-    }
-    if (loss == SM_BRIER) {
-        const float l = 0.5f * (tsign + 1.0f);
-        const float d = rc_sigmoid_f(p) - l;
-        return d * d;
-    }
-    if (loss == SM_HINGE_ORDINARY) {
-        const float h = 1.0f - u;
-        return h > 0.0f ? h : 0.0f;
-    }
-    if (loss == SM_HINGE_SQUARED) {
-        const float h = 1.0f - u;
-        return h > 0.0f ? h * h : 0.0f;
-    }
-    if (loss == SM_HINGE_SIGMOID) {
-        const float s = 2.0f * rc_sigmoid_f(p) - 1.0f;
-        const float h = 1.0f - tsign * s;
-        return h > 0.0f ? h : 0.0f;
-    }
-    return rc_nanf();
-}
-
-struct ScoreArgs {
-    const float *cols;
-    const float *y;
-    const float *tsign;
-    const double *w;
-    int n, npad, v;
-    const RcIns *ins;
-    const int *ins_off;
-    const int *order;     /* candidate ids of this bucket, longest first */
-    int ncand;            /* candidates in this bucket */
-    int group;            /* candidates per work item */
-    int subtiles;         /* sub-tiles (T*4 rows each) per tile */
-    int ntiles;
-    int nitems;
-    int maxins;
-    int nslots;
-    int *counter;
-    double *partial;      /* [P][ptiles] */
-    double *partial2;     /* second moment (correlation pass 2, classification weight) */
-    int ptiles;
-    int *bad;             /* [P] */
-    float *pred;          /* SM_PREDICT: [P][n] */
-    const double *pbar;   /* SM_CORR_PASS2: per-candidate mean prediction */
-    double ybar;
-    int mode;
-};
-
-/* Per-row accumulation of one candidate. Returns 1 when the row is a hard
-   failure for the scoring modes. */
-template <int T>
-__device__ __forceinline__ void rc_accumulate(const ScoreArgs &a, int mode, float pr, float yv,
-                                              int row, int cand, double &acc, double &acc2,
-                                              int &bad)
-{
-    const bool finite = isfinite(pr) && fabsf(pr) <= 1e30f;
-    if (mode >= SM_EVAL_SQUARED && mode <= SM_EVAL_ABSOLUTE) {
-        if (!finite) acc += 1e30;
-        else acc += (double)rc_row_loss(pr - yv, mode - SM_EVAL_SQUARED);
-        return;
-    }
-    if (mode == SM_PREDICT) {
-        a.pred[(size_t)cand * (size_t)a.n + (size_t)row] = pr;
-        return;
-    }
-    if (mode >= SM_LOG_LOSS && mode <= SM_HINGE_SQUARED) {
-        const double wi = a.w ? a.w[row] : 1.0;
-        if (!isfinite(wi) || wi < 0.0) {
-            bad = 1;
-            return;
-        }
-        if (wi == 0.0) return;
-        const float t = a.tsign ? a.tsign[row] : rc_nanf();
-        if (!isfinite(t) || !finite) {
-            bad = 1;
-            return;
-        }
-        acc += wi * (double)rc_class_row_loss(pr, t, mode);
-        acc2 += wi;
-        return;
-    }
-    if (!finite) {
-        bad = 1;
-        return;
-    }
-    if (mode == SM_CORR_PASS1) {
-        acc += (double)pr;
-        return;
-    }
-    if (mode == SM_CORR_PASS2) {
-        const double dp = (double)pr - a.pbar[cand];
-        const double dy = (double)yv - a.ybar;
-        acc += dp * dp;
-        acc2 += dp * dy;
-        return;
-    }
-    const double r = (double)pr - (double)yv;
-    switch (mode) {
-        case SM_ABSOLUTE: acc += fabs(r); break;
-        case SM_LOG_SQUASHED: {
-            const double rr = r * r;
-            acc += isfinite(rr) ? log1p(rr) : 2.0 * log(fabs(r));
-        } break;
-        case SM_SIGNED: acc += r; break;
-        case SM_MAXIMUM: acc = fmax(acc, fabs(r)); break;
-        default: acc += r * r; break;
-    }
-}
-
-template <int T, bool STAGED>
-__global__ void __launch_bounds__(T) rc_score_kernel(ScoreArgs a)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int tid = threadIdx.x;
-    const int nx = a.v + 1;                   /* feature columns + y */
-    float4 *xs = reinterpret_cast<float4 *>(smem_raw);
-    float4 *stk = xs + (STAGED ? nx * T : 0);
-    double *sacc = reinterpret_cast<double *>(stk + a.nslots * T);
-    double *sacc2 = sacc + a.group * T;
-    RcIns *sprog = reinterpret_cast<RcIns *>(sacc2 + a.group * T);
-    __shared__ int s_item;
-    __shared__ int s_bad;
-    const int SUB = T * 4;
-    const int mode = a.mode;
-
-    for (;;) {
-        if (tid == 0) s_item = atomicAdd(a.counter, 1);
-        __syncthreads();
-        const int item = s_item;
-        if (item >= a.nitems) break;
-        const int g = item / a.ntiles;
-        const int tile = item - g * a.ntiles;
-        const int cbase = g * a.group;
-        const int gcount = min(a.group, a.ncand - cbase);
-
-        for (int c = 0; c < gcount; ++c) {
-            const int cand = a.order[cbase + c];
-            const int b = a.ins_off[cand], e = a.ins_off[cand + 1];
-            for (int q = tid; q < e - b; q += T) sprog[c * a.maxins + q] = a.ins[b + q];
-            sacc[c * T + tid] = 0.0;
-            sacc2[c * T + tid] = 0.0;
-        }
-        if (tid == 0) s_bad = 0;
-        unsigned badmask = 0;
-        __syncthreads();
-
-        for (int s = 0; s < a.subtiles; ++s) {
-            const int row0 = (tile * a.subtiles + s) * SUB;
-            if (row0 >= a.n) break;
-            const int myrow = row0 + 4 * tid;
-            const float4 *yp = reinterpret_cast<const float4 *>(a.y + myrow);
-            float4 yv4 = __ldg(yp);
-            if (STAGED) {
-                for (int k = 0; k < a.v; ++k) {
-                    xs[k * T + tid] = __ldg(reinterpret_cast<const float4 *>(
-                        a.cols + (size_t)k * (size_t)a.npad + (size_t)myrow));
-                }
-            }
-            __syncthreads();
-            for (int c = 0; c < gcount; ++c) {
-                const int cand = a.order[cbase + c];
-                float4 p;
-                if (STAGED) {
-                    rc_run<T>(sprog + c * a.maxins, xs, stk, tid, p);
-                }
-                double acc = sacc[c * T + tid];
-                double acc2 = sacc2[c * T + tid];
-                int bad = 0;
-                const float pr[4] = {p.x, p.y, p.z, p.w};
-                const float yy[4] = {yv4.x, yv4.y, yv4.z, yv4.w};
-#pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    const int row = myrow + i;
-                    if (row < a.n) rc_accumulate<T>(a, mode, pr[i], yy[i], row, cand, acc, acc2, bad);
-                }
-                sacc[c * T + tid] = acc;
-                sacc2[c * T + tid] = acc2;
-                if (bad) badmask |= 1u << c;
-            }
-            __syncthreads();
-        }
-
-        /* Fixed-order block tree per candidate, then one partial per tile. */
-        if (badmask) atomicOr(&s_bad, (int)badmask);
-        for (int st = T / 2; st > 0; st >>= 1) {
-            if (tid < st) {
-                for (int c = 0; c < gcount; ++c) {
-                    if (mode == SM_MAXIMUM) {
-                        sacc[c * T + tid] = fmax(sacc[c * T + tid], sacc[c * T + tid + st]);
-                    } else {
-                        sacc[c * T + tid] += sacc[c * T + tid + st];
-                        sacc2[c * T + tid] += sacc2[c * T + tid + st];
-                    }
-                }
-            }
-            __syncthreads();
-        }
-        if (tid < gcount) {
-            const int cand = a.order[cbase + tid];
-            a.partial[(size_t)cand * a.ptiles + tile] = sacc[tid * T];
-            if (a.partial2) a.partial2[(size_t)cand * a.ptiles + tile] = sacc2[tid * T];
-            if (s_bad & (1 << tid)) atomicOr(&a.bad[cand], 1);
-        }
-        __syncthreads();
-    }
-}
-
-/* Global-memory variant for wide tables (more columns than the staging
-   budget): identical arithmetic, features read straight from L2. */
-template <int T>
-__device__ __forceinline__ void rc_run_global(const RcIns *__restrict__ prog, const float *cols,
-                                              int npad, int myrow, float4 *stk, int tid, float4 &p)
-{
-    float t0 = 0.f, t1 = 0.f, t2 = 0.f, t3 = 0.f;
-    for (int pc = 0; pc < RC_MAX_INS; ++pc) {
-        const RcIns in = prog[pc];
-        const unsigned kind = in.kind;
-        if (kind <= K_PUSH_CONST) {
-            if (in.spill != 0xff) stk[in.spill * T + tid] = make_float4(t0, t1, t2, t3);
-            if (kind == K_PUSH_VAR) {
-                const float4 x = __ldg(reinterpret_cast<const float4 *>(
-                    cols + (size_t)in.imm * (size_t)npad + (size_t)myrow));
-                t0 = x.x; t1 = x.y; t2 = x.z; t3 = x.w;
-            } else {
-                const float c = __uint_as_float(in.imm);
-                t0 = c; t1 = c; t2 = c; t3 = c;
-            }
-            continue;
-        }
-        if (kind == K_UNARY) {
-            t0 = rc_unary_f(in.op, t0);
-            t1 = rc_unary_f(in.op, t1);
-            t2 = rc_unary_f(in.op, t2);
-            t3 = rc_unary_f(in.op, t3);
-            continue;
-        }
-        if (kind <= K_BIN_C) {
-            float4 av, bv;
-            if (kind == K_BIN_S) {
-                av = stk[in.arg * T + tid];
-                bv = make_float4(t0, t1, t2, t3);
-            } else if (kind == K_BIN_V) {
-                av = make_float4(t0, t1, t2, t3);
-                bv = __ldg(reinterpret_cast<const float4 *>(
-                    cols + (size_t)in.imm * (size_t)npad + (size_t)myrow));
-            } else {
-                const float c = __uint_as_float(in.imm);
-                av = make_float4(t0, t1, t2, t3);
-                bv = make_float4(c, c, c, c);
-            }
-            t0 = rc_binary_f(in.op, av.x, bv.x);
-            t1 = rc_binary_f(in.op, av.y, bv.y);
-            t2 = rc_binary_f(in.op, av.z, bv.z);
-            t3 = rc_binary_f(in.op, av.w, bv.w);
-            continue;
-        }
-        if (kind == K_IF) {
-            const float4 cnd = stk[in.arg * T + tid];
-            const float4 a = stk[(in.arg + 1) * T + tid];
-            t0 = cnd.x > 0.0f ? a.x : t0;
-            t1 = cnd.y > 0.0f ? a.y : t1;
-            t2 = cnd.z > 0.0f ? a.z : t2;
-            t3 = cnd.w > 0.0f ? a.w : t3;
-            continue;
-        }
-        if (kind == K_HALT) {
-            p = in.arg == 1 ? make_float4(t0, t1, t2, t3) : stk[tid];
-            return;
-        }
-        break;
-    }
-    p = make_float4(rc_nanf(), rc_nanf(), rc_nanf(), rc_nanf());
-}
-
-template <int T>
-__global__ void __launch_bounds__(T) rc_score_kernel_wide(ScoreArgs a)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int tid = threadIdx.x;
-    float4 *stk = reinterpret_cast<float4 *>(smem_raw);
-    double *sacc = reinterpret_cast<double *>(stk + a.nslots * T);
-    double *sacc2 = sacc + a.group * T;
-    RcIns *sprog = reinterpret_cast<RcIns *>(sacc2 + a.group * T);
-    __shared__ int s_item;
-    __shared__ int s_bad;
-    const int SUB = T * 4;
-    const int mode = a.mode;
-    for (;;) {
-        if (tid == 0) s_item = atomicAdd(a.counter, 1);
-        __syncthreads();
-        const int item = s_item;
-        if (item >= a.nitems) break;
-        const int g = item / a.ntiles;
-        const int tile = item - g * a.ntiles;
-        const int cbase = g * a.group;
-        const int gcount = min(a.group, a.ncand - cbase);
-        for (int c = 0; c < gcount; ++c) {
-            const int cand = a.order[cbase + c];
-            const int b = a.ins_off[cand], e = a.ins_off[cand + 1];
-            for (int q = tid; q < e - b; q += T) sprog[c * a.maxins + q] = a.ins[b + q];
-            sacc[c * T + tid] = 0.0;
-            sacc2[c * T + tid] = 0.0;
-        }
-        if (tid == 0) s_bad = 0;
-        unsigned badmask = 0;
-        __syncthreads();
-        for (int s = 0; s < a.subtiles; ++s) {
-            const int row0 = (tile * a.subtiles + s) * SUB;
-            if (row0 >= a.n) break;
-            const int myrow = row0 + 4 * tid;
-            const float4 yv4 = __ldg(reinterpret_cast<const float4 *>(a.y + myrow));
-            for (int c = 0; c < gcount; ++c) {
-                const int cand = a.order[cbase + c];
-                float4 p;
-                rc_run_global<T>(sprog + c * a.maxins, a.cols, a.npad, myrow, stk, tid, p);
-                double acc = sacc[c * T + tid];
-                double acc2 = sacc2[c * T + tid];
-                int bad = 0;
-                const float pr[4] = {p.x, p.y, p.z, p.w};
-                const float yy[4] = {yv4.x, yv4.y, yv4.z, yv4.w};
-#pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    const int row = myrow + i;
-                    if (row < a.n) rc_accumulate<T>(a, mode, pr[i], yy[i], row, cand, acc, acc2, bad);
-                }
-                sacc[c * T + tid] = acc;
-                sacc2[c * T + tid] = acc2;
-                if (bad) badmask |= 1u << c;
-            }
-        }
-        __syncthreads();
-        if (badmask) atomicOr(&s_bad, (int)badmask);
-        for (int st = T / 2; st > 0; st >>= 1) {
-            if (tid < st) {
-                for (int c = 0; c < gcount; ++c) {
-                    if (mode == SM_MAXIMUM) {
-                        sacc[c * T + tid] = fmax(sacc[c * T + tid], sacc[c * T + tid + st]);
-                    } else {
-                        sacc[c * T + tid] += sacc[c * T + tid + st];
-                        sacc2[c * T + tid] += sacc2[c * T + tid + st];
-                    }
-                }
-            }
-            __syncthreads();
-        }
-        if (tid < gcount) {
-            const int cand = a.order[cbase + tid];
-            a.partial[(size_t)cand * a.ptiles + tile] = sacc[tid * T];
-            if (a.partial2) a.partial2[(size_t)cand * a.ptiles + tile] = sacc2[tid * T];
-            if (s_bad & (1 << tid)) atomicOr(&a.bad[cand], 1);
-        }
-        __syncthreads();
-    }
-}
-
-/* Tiles of each candidate in ascending order: the final, fixed-order sum. */
-__global__ void rc_score_finalize(int nprog, const int *__restrict__ cand_tiles,
-                                  const double *__restrict__ partial,
-                                  const double *__restrict__ partial2, int ptiles,
-                                  const int *__restrict__ bad, int n, int mode, double syy,
-                                  double *__restrict__ out, int *__restrict__ status,
-                                  float *__restrict__ out_f32, double *__restrict__ pbar)
-{
-    const int cand = blockIdx.x * blockDim.x + threadIdx.x;
-    if (cand >= nprog) return;
-    const int nt = cand_tiles[cand];
-    double s = 0.0, s2 = 0.0;
-    for (int t = 0; t < nt; ++t) {
-        const double v = partial[(size_t)cand * ptiles + t];
-        if (mode == SM_MAXIMUM) s = fmax(s, v);
-        else s += v;
-        if (partial2) s2 += partial2[(size_t)cand * ptiles + t];
-    }
-    if (mode >= SM_EVAL_SQUARED && mode <= SM_EVAL_ABSOLUTE) {
-        out_f32[cand] = (float)s;
-        return;
-    }
-    if (mode == SM_PREDICT) return;
-    if (bad[cand]) {
-        if (out) out[cand] = INFINITY;
-        if (status) status[cand] = RC_SCORE_NONFINITE;
-        return;
-    }
-    const double dn = (double)n;
-    double v = 0.0;
-    int st = 0;
-    switch (mode) {
-        case SM_CORR_PASS1:
-            pbar[cand] = s / dn;
-            return;
-        case SM_CORRELATION:
-        case SM_CORRELATION_SIGNED: {
-            /* s = sum dp^2, s2 = sum dp dy (pass 2); the CPU rule: zero
-               variance on either side is rho = 0 (eval.cu:1003-1012). */
-            const double rho = (s <= 0.0 || syy <= 0.0) ? 0.0 : s2 / (sqrt(s) * sqrt(syy));
-            v = mode == SM_CORRELATION_SIGNED ? 1.0 - rho : 1.0 - fabs(rho);
-        } break;
-        case SM_AIC: case SM_AICC: case SM_BIC: v = s; break; /* RSS; host penalty */
-        case SM_SIGNED: v = fabs(s) / dn; break;
-        case SM_MAXIMUM: v = s; break;
-        case SM_LOG_LOSS: case SM_BRIER: case SM_HINGE_SIGMOID: case SM_HINGE_ORDINARY:
-        case SM_HINGE_SQUARED:
-            if (!(s2 > 0.0)) {
-                v = INFINITY;
-                st = RC_SCORE_ALL_ZERO_WEIGHT;
-            } else {
-                v = s / s2;
-            }
-            break;
-        default: v = s / dn; break;
-    }
-    out[cand] = v;
-    status[cand] = st;
-}
-
 /* ---- host launcher -------------------------------------------------- */
 
 namespace {
@@ -744,9 +160,42 @@ int occupancy_blocks(const void *fn, int threads, size_t smem)
     return blocks < 1 ? 1 : blocks;
 }
 
-/* Rows per tile: fixed per (bucket) so a candidate's reduction order depends
-   only on n and its own depth. */
-const int TILE_ROWS = 32768;
+/* Rows per tile: fixed so a candidate's reduction order depends only on n
+   and its own depth bucket. */
+const int TILE_ROWS = RC_TILE_ROWS;
+const int LANE_T = 128;
+
+const void *score_kernel_fn(int T, bool track)
+{
+    if (T == 256) return track ? (const void *)rc_score_kernel<256, true>
+                               : (const void *)rc_score_kernel<256, false>;
+    return track ? (const void *)rc_score_kernel<64, true> : (const void *)rc_score_kernel<64, false>;
+}
+
+void launch_score_kernel(int T, bool track, int grid, size_t smem, cudaStream_t s,
+                         const ScoreArgs &a)
+{
+    if (T == 256) {
+        if (track) rc_score_kernel<256, true><<<grid, 256, smem, s>>>(a);
+        else rc_score_kernel<256, false><<<grid, 256, smem, s>>>(a);
+    } else {
+        if (track) rc_score_kernel<64, true><<<grid, 64, smem, s>>>(a);
+        else rc_score_kernel<64, false><<<grid, 64, smem, s>>>(a);
+    }
+}
+
+int set_smem(const void *fn, size_t smem)
+{
+    if (smem <= 48 * 1024) return 0;
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess) {
+        cudaGetLastError();
+        return -1;
+    }
+    return 0;
+}
+
+size_t lane_smem(int nslots) { return (size_t)nslots * LANE_T * 16 + RC_MAX_INS * sizeof(RcIns) + LANE_T * 8; }
 
 }  // namespace
 
@@ -766,14 +215,14 @@ float rc_score_run(RcCtx *c, const uint32_t *words, const uint32_t *off, int wid
     ins.reserve((size_t)nprog * 16);
     std::vector<int> ins_off(nprog + 1, 0);
     std::vector<int> nslots(nprog, 0);
-    std::vector<RcIns> tmp(RC_MAX_INS + 64);
+    std::vector<RcIns> local;
     for (int p = 0; p < nprog; ++p) {
         size_t b = width > 0 ? (size_t)p * (size_t)width : off[p];
         size_t e = width > 0 ? b + (size_t)width : off[p + 1];
         if (e < b) e = b;
-        std::vector<RcIns> local(std::max<size_t>(e - b, 1) + 1);
+        local.resize(std::max<size_t>(e - b, 1) + 1);
         int ns = 0;
-        int cnt = rc_decode_postfix(words + b, e - b, c->v, local.data(), &ns);
+        const int cnt = rc_decode_postfix(words + b, e - b, c->v, local.data(), &ns);
         ins_off[p] = (int)ins.size();
         ins.insert(ins.end(), local.begin(), local.begin() + cnt);
         nslots[p] = ns;
@@ -782,11 +231,13 @@ float rc_score_run(RcCtx *c, const uint32_t *words, const uint32_t *off, int wid
 
     /* 2. bucket by depth; longest program first */
     Bucket bk[2];
+    int max_slots = 1;
     for (int p = 0; p < nprog; ++p) {
         const int b = nslots[p] <= RC_SHALLOW_SLOTS ? 0 : 1;
         bk[b].cands.push_back(p);
         bk[b].nslots = std::max(bk[b].nslots, nslots[p]);
         bk[b].maxins = std::max(bk[b].maxins, ins_off[p + 1] - ins_off[p]);
+        max_slots = std::max(max_slots, nslots[p]);
     }
     for (int b = 0; b < 2; ++b) {
         std::stable_sort(bk[b].cands.begin(), bk[b].cands.end(), [&](int x, int y) {
@@ -794,29 +245,18 @@ float rc_score_run(RcCtx *c, const uint32_t *words, const uint32_t *off, int wid
         });
     }
     const int Tb[2] = {256, 64};
-    const bool staged = (c->v + 1) <= stage_limit_cols() + 1;
-    int tiles_b[2], subt_b[2];
-    for (int b = 0; b < 2; ++b) {
-        const int sub = Tb[b] * 4;
-        subt_b[b] = TILE_ROWS / sub;
-        tiles_b[b] = (c->n + TILE_ROWS - 1) / TILE_ROWS;
-        if (tiles_b[b] < 1) tiles_b[b] = 1;
-    }
-    const int ptiles = std::max(tiles_b[0], tiles_b[1]);
-    std::vector<int> cand_tiles(nprog);
+    const int staged = (c->v + 1) <= stage_limit_cols() + 1 ? 1 : 0;
+    const int ntiles = std::max(1, (c->n + TILE_ROWS - 1) / TILE_ROWS);
+    std::vector<int> cand_tiles(nprog, ntiles);
     std::vector<int> order;
     order.reserve(nprog);
-    for (int b = 0; b < 2; ++b)
-        for (int p : bk[b].cands) {
-            cand_tiles[p] = tiles_b[b];
-            order.push_back(p);
-        }
+    for (int b = 0; b < 2; ++b) order.insert(order.end(), bk[b].cands.begin(), bk[b].cands.end());
 
     const bool corr = (mode == SM_CORRELATION || mode == SM_CORRELATION_SIGNED);
-    const bool two = corr || (mode >= SM_LOG_LOSS && mode <= SM_HINGE_SQUARED);
+    const bool track = mode < SM_EVAL_SQUARED;
 
-    /* 3. layout: inputs [ins | ins_off | order | cand_tiles] outputs
-       [out | status | out_f32] work [partial | partial2 | bad | counters | pbar] */
+    /* 3. layout: inputs [ins | ins_off | order | cand_tiles], outputs
+       [out | status | out_f32], work [part | bad | counters | pbar | lane]. */
     size_t cur = 0;
     const size_t o_ins = rc_take(&cur, sizeof(RcIns) * ins.size());
     const size_t o_insoff = rc_take(&cur, sizeof(int) * (nprog + 1));
@@ -827,11 +267,16 @@ float rc_score_run(RcCtx *c, const uint32_t *words, const uint32_t *off, int wid
     const size_t o_status = rc_take(&cur, sizeof(int) * nprog);
     const size_t o_f32 = rc_take(&cur, sizeof(float) * nprog);
     const size_t io_end = rc_take(&cur, 0);
-    const size_t o_part = rc_take(&cur, sizeof(double) * (size_t)nprog * ptiles);
-    const size_t o_part2 = rc_take(&cur, two ? sizeof(double) * (size_t)nprog * ptiles : 0);
+    const size_t o_part = rc_take(&cur, 4 * sizeof(double) * (size_t)nprog * ntiles);
     const size_t o_bad = rc_take(&cur, sizeof(int) * nprog);
-    const size_t o_cnt = rc_take(&cur, sizeof(int) * 8);
-    const size_t o_pbar = rc_take(&cur, corr ? sizeof(double) * nprog : 0);
+    const size_t o_bad64 = rc_take(&cur, sizeof(int) * nprog);
+    const size_t o_cnt = rc_take(&cur, sizeof(int) * 16);
+    const size_t o_zero_end = rc_take(&cur, 0);
+    const size_t o_pbar = rc_take(&cur, sizeof(double) * nprog);
+    const size_t o_pbarerr = rc_take(&cur, sizeof(double) * nprog);
+    const size_t o_pbar64 = rc_take(&cur, sizeof(double) * nprog);
+    const size_t o_flagged = rc_take(&cur, sizeof(int) * nprog);
+    const size_t o_part64 = rc_take(&cur, track ? 2 * sizeof(double) * (size_t)nprog * ntiles : 0);
     const size_t o_pred = rc_take(&cur, pred_out ? sizeof(float) * (size_t)nprog * c->n : 0);
     const size_t dev_end = rc_take(&cur, 0);
     double t = rc_now_ms();
@@ -847,10 +292,14 @@ float rc_score_run(RcCtx *c, const uint32_t *words, const uint32_t *off, int wid
     memcpy(host + o_order, order.data(), sizeof(int) * nprog);
     memcpy(host + o_ctiles, cand_tiles.data(), sizeof(int) * nprog);
     cudaMemcpyAsync(dev, host, in_end, cudaMemcpyHostToDevice, c->s);
-    cudaMemsetAsync(dev + o_bad, 0, o_cnt - o_bad + sizeof(int) * 8, c->s);
+    cudaMemsetAsync(dev + o_bad, 0, o_zero_end - o_bad, c->s);
     st->h2d_ms += rc_now_ms() - t;
     st->h2d_bytes += in_end;
 
+    int *d_cnt = reinterpret_cast<int *>(dev + o_cnt);
+    int *d_nflag = d_cnt + 8;
+    double *d_out = reinterpret_cast<double *>(dev + o_out);
+    int *d_status = reinterpret_cast<int *>(dev + o_status);
     ScoreArgs a;
     memset(&a, 0, sizeof(a));
     a.cols = c->d_cols;
@@ -860,17 +309,19 @@ float rc_score_run(RcCtx *c, const uint32_t *words, const uint32_t *off, int wid
     a.n = c->n;
     a.npad = c->npad;
     a.v = c->v;
+    a.staged = staged;
     a.ins = reinterpret_cast<const RcIns *>(dev + o_ins);
     a.ins_off = reinterpret_cast<const int *>(dev + o_insoff);
-    a.ptiles = ptiles;
-    a.partial = reinterpret_cast<double *>(dev + o_part);
-    a.partial2 = two ? reinterpret_cast<double *>(dev + o_part2) : nullptr;
+    a.nprog = nprog;
+    a.ptiles = ntiles;
+    a.ntiles = ntiles;
+    a.part = reinterpret_cast<double *>(dev + o_part);
     a.bad = reinterpret_cast<int *>(dev + o_bad);
     a.pred = pred_out ? reinterpret_cast<float *>(dev + o_pred) : nullptr;
-    a.pbar = corr ? reinterpret_cast<const double *>(dev + o_pbar) : nullptr;
+    a.pbar = reinterpret_cast<const double *>(dev + o_pbar);
+    a.pbar_err = reinterpret_cast<const double *>(dev + o_pbarerr);
     a.ybar = c->ybar;
     const int *d_ctiles = reinterpret_cast<const int *>(dev + o_ctiles);
-    int *d_cnt = reinterpret_cast<int *>(dev + o_cnt);
 
     t = rc_now_ms();
     cudaEventRecord(c->t0, c->s);
@@ -886,51 +337,78 @@ float rc_score_run(RcCtx *c, const uint32_t *words, const uint32_t *off, int wid
             int group = 8;
             auto it = c->tune.find(b);
             if (it != c->tune.end()) group = it->second.first;
-            if (group > nb) group = nb;
-            if (group < 1) group = 1;
+            group = std::max(1, std::min(group, std::min(nb, 32)));
             a.order = reinterpret_cast<const int *>(dev + o_order) + obase;
             a.ncand = nb;
             a.group = group;
-            a.subtiles = subt_b[b];
-            a.ntiles = tiles_b[b];
+            a.subtiles = TILE_ROWS / (T * 4);
             const int ngroups = (nb + group - 1) / group;
-            a.nitems = ngroups * a.ntiles;
+            a.nitems = ngroups * ntiles;
             a.maxins = bk[b].maxins;
             a.nslots = std::max(bk[b].nslots, 1);
             a.counter = d_cnt + b + 2 * pass;
             a.mode = kmode;
-            size_t smem = (staged ? (size_t)(c->v + 1) * T * 16 : 0) + (size_t)a.nslots * T * 16 +
-                          (size_t)group * T * 16 + (size_t)group * a.maxins * sizeof(RcIns);
-            const void *fn;
-            if (staged) fn = T == 256 ? (const void *)rc_score_kernel<256, true>
-                                      : (const void *)rc_score_kernel<64, true>;
-            else fn = T == 256 ? (const void *)rc_score_kernel_wide<256>
-                               : (const void *)rc_score_kernel_wide<64>;
-            if (smem > 48 * 1024) {
-                if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem) != cudaSuccess) {
-                    cudaGetLastError();
-                    st->failed = 1;
-                    return -1.0f;
-                }
+            const size_t smem = T == 256
+                ? ScoreSmem<256>::total(c->v, staged, a.nslots, group, a.maxins)
+                : ScoreSmem<64>::total(c->v, staged, a.nslots, group, a.maxins);
+            const void *fn = score_kernel_fn(T, track);
+            if (set_smem(fn, smem) != 0) {
+                st->failed = 1;
+                cudaStreamSynchronize(c->s);
+                return -1.0f;
             }
-            const int per_sm = occupancy_blocks(fn, T, smem);
-            int grid = c->sm_count * per_sm;
+            int grid = c->sm_count * occupancy_blocks(fn, T, smem);
             if (grid > a.nitems) grid = a.nitems;
-            if (staged) {
-                if (T == 256) rc_score_kernel<256, true><<<grid, 256, smem, c->s>>>(a);
-                else rc_score_kernel<64, true><<<grid, 64, smem, c->s>>>(a);
-            } else {
-                if (T == 256) rc_score_kernel_wide<256><<<grid, 256, smem, c->s>>>(a);
-                else rc_score_kernel_wide<64><<<grid, 64, smem, c->s>>>(a);
-            }
+            launch_score_kernel(T, track, grid, smem, c->s, a);
             obase += nb;
         }
         rc_score_finalize<<<(nprog + 127) / 128, 128, 0, c->s>>>(
-            nprog, d_ctiles, a.partial, a.partial2, ptiles, a.bad, c->n,
-            corr && pass == 1 ? mode : kmode, c->syy,
-            reinterpret_cast<double *>(dev + o_out), reinterpret_cast<int *>(dev + o_status),
-            reinterpret_cast<float *>(dev + o_f32), reinterpret_cast<double *>(dev + o_pbar));
+            nprog, d_ctiles, a.part, ntiles, a.bad, c->n, kmode, c->syy, d_out, d_status,
+            reinterpret_cast<float *>(dev + o_f32), reinterpret_cast<double *>(dev + o_pbar),
+            reinterpret_cast<double *>(dev + o_pbarerr), d_nflag,
+            track ? reinterpret_cast<int *>(dev + o_flagged) : nullptr);
+    }
+
+    /* 4. the f64 re-check lane over the flagged candidates */
+    if (track) {
+        Score64Args l;
+        memset(&l, 0, sizeof(l));
+        l.cols = c->d_cols;
+        l.y = c->d_y;
+        l.tsign = c->d_tsign;
+        l.w = c->d_w64;
+        l.n = c->n;
+        l.npad = c->npad;
+        l.ins = a.ins;
+        l.ins_off = a.ins_off;
+        l.flagged = reinterpret_cast<const int *>(dev + o_flagged);
+        l.nflag = d_nflag;
+        l.ntiles = ntiles;
+        l.nslots = max_slots;
+        l.part = reinterpret_cast<double *>(dev + o_part64);
+        l.nprog = nprog;
+        l.ptiles = ntiles;
+        l.bad = reinterpret_cast<int *>(dev + o_bad64);
+        l.pbar = reinterpret_cast<const double *>(dev + o_pbar64);
+        l.ybar = c->ybar;
+        const size_t smem = lane_smem(max_slots);
+        if (set_smem((const void *)rc_score64_kernel<LANE_T>, smem) != 0) {
+            st->failed = 1;
+            cudaStreamSynchronize(c->s);
+            return -1.0f;
+        }
+        const int grid = c->sm_count *
+                         occupancy_blocks((const void *)rc_score64_kernel<LANE_T>, LANE_T, smem);
+        for (int pass = 0; pass < passes; ++pass) {
+            const int kmode = corr ? (pass == 0 ? SM_CORR_PASS1 : SM_CORR_PASS2) : mode;
+            if (pass == 1) cudaMemsetAsync(dev + o_bad64, 0, sizeof(int) * nprog, c->s);
+            l.counter = d_cnt + 4 + pass;
+            l.mode = kmode;
+            rc_score64_kernel<LANE_T><<<grid, LANE_T, smem, c->s>>>(l);
+            rc_score64_finalize<<<(nprog + 127) / 128, 128, 0, c->s>>>(
+                l.flagged, d_nflag, ntiles, l.part, nprog, ntiles, l.bad, c->n, kmode, c->syy,
+                d_out, d_status, reinterpret_cast<double *>(dev + o_pbar64));
+        }
     }
     cudaEventRecord(c->t1, c->s);
     st->launch_ms += rc_now_ms() - t;
@@ -1292,6 +770,7 @@ struct NoallocDevice {
     unsigned char *scratch; /* device address of rc_noalloc_scratch */
     int sm_count;
     int grid_per_sm;
+    int lane_per_sm;
 };
 NoallocDevice g_noalloc[RC_NOALLOC_MAX_DEVICES];
 std::mutex g_noalloc_mu;
@@ -1338,9 +817,13 @@ extern "C" int rc_score_batch_noalloc(const float *cols, const float *y, int n, 
     const size_t o_order = rc_take(&cur, sizeof(int) * (size_t)nprog);
     const size_t o_ctiles = rc_take(&cur, sizeof(int) * (size_t)nprog);
     const size_t o_deep = rc_take(&cur, sizeof(int) * (size_t)nprog);
-    const size_t o_part = rc_take(&cur, sizeof(double) * (size_t)nprog * ntiles);
+    const size_t o_part = rc_take(&cur, 4 * sizeof(double) * (size_t)nprog * ntiles);
+    const size_t o_part64 = rc_take(&cur, 2 * sizeof(double) * (size_t)nprog * ntiles);
+    const size_t o_flagged = rc_take(&cur, sizeof(int) * (size_t)nprog);
     const size_t o_bad = rc_take(&cur, sizeof(int) * (size_t)nprog);
-    const size_t o_cnt = rc_take(&cur, sizeof(int) * 8);
+    const size_t o_bad64 = rc_take(&cur, sizeof(int) * (size_t)nprog);
+    const size_t o_cnt = rc_take(&cur, sizeof(int) * 16);
+    const size_t o_zero_end = rc_take(&cur, 0);
     const size_t need = rc_take(&cur, 0);
     if (need > RC_NOALLOC_SCRATCH_BYTES) {
         fprintf(stderr,
@@ -1350,8 +833,9 @@ extern "C" int rc_score_batch_noalloc(const float *cols, const float *y, int n, 
         return -2;
     }
     const int G = 8;
-    const size_t smem = (size_t)(v + 1) * T * 16 + (size_t)RC_SHALLOW_SLOTS * T * 16 +
-                        (size_t)G * T * 16 + (size_t)G * RC_MAX_INS * sizeof(RcIns);
+    const int group = G < nprog ? G : nprog;
+    const size_t smem = ScoreSmem<256>::total(v, 1, RC_SHALLOW_SLOTS, group, RC_MAX_INS);
+    const size_t lsmem = lane_smem(RC_SHALLOW_SLOTS);
     NoallocDevice *d = &g_noalloc[dev];
     {
         std::lock_guard<std::mutex> lock(g_noalloc_mu);
@@ -1364,35 +848,30 @@ extern "C" int rc_score_batch_noalloc(const float *cols, const float *y, int n, 
                 cudaGetLastError();
                 return -1;
             }
-            const int maxsmem = (int)((size_t)(stage_limit_cols() + 1) * T * 16 +
-                                      (size_t)RC_SHALLOW_SLOTS * T * 16 + (size_t)G * T * 16 +
-                                      (size_t)G * RC_MAX_INS * sizeof(RcIns));
-            if (cudaFuncSetAttribute((const void *)rc_score_kernel<256, true>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     maxsmem) != cudaSuccess) {
-                cudaGetLastError();
+            const size_t maxsmem =
+                ScoreSmem<256>::total(stage_limit_cols(), 1, RC_SHALLOW_SLOTS, G, RC_MAX_INS);
+            if (set_smem((const void *)rc_score_kernel<256, true>, maxsmem) != 0 ||
+                set_smem((const void *)rc_score64_kernel<LANE_T>, lsmem) != 0)
                 return -1;
-            }
-            int sms = 1, per = 1;
+            int sms = 1;
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                    &per, rc_score_kernel<256, true>, T, (size_t)maxsmem) != cudaSuccess) {
-                cudaGetLastError();
-                per = 1;
-            }
             d->scratch = (unsigned char *)ptr;
             d->sm_count = sms > 0 ? sms : 1;
-            d->grid_per_sm = per > 0 ? per : 1;
+            d->grid_per_sm =
+                occupancy_blocks((const void *)rc_score_kernel<256, true>, T, maxsmem);
+            d->lane_per_sm =
+                occupancy_blocks((const void *)rc_score64_kernel<LANE_T>, LANE_T, lsmem);
             d->ready = 1;
         }
     }
     cudaStream_t s = (cudaStream_t)stream;
     unsigned char *sc = d->scratch;
-    cudaMemsetAsync(sc + o_bad, 0, o_cnt - o_bad + sizeof(int) * 8, s);
+    cudaMemsetAsync(sc + o_bad, 0, o_zero_end - o_bad, s);
     rc_noalloc_decode<<<(nprog + 1 + 127) / 128, 128, 0, s>>>(
         prog, off, nprog, v, reinterpret_cast<RcIns *>(sc + o_ins),
         reinterpret_cast<int *>(sc + o_insoff), reinterpret_cast<int *>(sc + o_order),
         reinterpret_cast<int *>(sc + o_ctiles), reinterpret_cast<int *>(sc + o_deep), ntiles);
+    int *cnt = reinterpret_cast<int *>(sc + o_cnt);
     ScoreArgs a;
     memset(&a, 0, sizeof(a));
     a.cols = cols;
@@ -1400,19 +879,20 @@ extern "C" int rc_score_batch_noalloc(const float *cols, const float *y, int n, 
     a.n = n;
     a.npad = ld;
     a.v = v;
+    a.staged = 1;
     a.ins = reinterpret_cast<const RcIns *>(sc + o_ins);
     a.ins_off = reinterpret_cast<const int *>(sc + o_insoff);
     a.order = reinterpret_cast<const int *>(sc + o_order);
     a.ncand = nprog;
-    a.group = G < nprog ? G : nprog;
+    a.group = group;
     a.subtiles = TILE_ROWS / SUB;
     a.ntiles = ntiles;
     a.nitems = ((nprog + a.group - 1) / a.group) * ntiles;
     a.maxins = RC_MAX_INS;
     a.nslots = RC_SHALLOW_SLOTS;
-    a.counter = reinterpret_cast<int *>(sc + o_cnt);
-    a.partial = reinterpret_cast<double *>(sc + o_part);
-    a.partial2 = nullptr;
+    a.counter = cnt;
+    a.part = reinterpret_cast<double *>(sc + o_part);
+    a.nprog = nprog;
     a.ptiles = ntiles;
     a.bad = reinterpret_cast<int *>(sc + o_bad);
     a.mode = kind;
@@ -1420,8 +900,30 @@ extern "C" int rc_score_batch_noalloc(const float *cols, const float *y, int n, 
     if (grid > a.nitems) grid = a.nitems;
     rc_score_kernel<256, true><<<grid, T, smem, s>>>(a);
     rc_score_finalize<<<(nprog + 127) / 128, 128, 0, s>>>(
-        nprog, reinterpret_cast<const int *>(sc + o_ctiles), a.partial, nullptr, ntiles, a.bad, n,
-        kind, 0.0, out, status, nullptr, nullptr);
+        nprog, reinterpret_cast<const int *>(sc + o_ctiles), a.part, ntiles, a.bad, n, kind, 0.0,
+        out, status, nullptr, nullptr, nullptr, cnt + 8, reinterpret_cast<int *>(sc + o_flagged));
+    Score64Args l;
+    memset(&l, 0, sizeof(l));
+    l.cols = cols;
+    l.y = y;
+    l.n = n;
+    l.npad = ld;
+    l.ins = a.ins;
+    l.ins_off = a.ins_off;
+    l.flagged = reinterpret_cast<const int *>(sc + o_flagged);
+    l.nflag = cnt + 8;
+    l.ntiles = ntiles;
+    l.nslots = RC_SHALLOW_SLOTS;
+    l.counter = cnt + 4;
+    l.part = reinterpret_cast<double *>(sc + o_part64);
+    l.nprog = nprog;
+    l.ptiles = ntiles;
+    l.bad = reinterpret_cast<int *>(sc + o_bad64);
+    l.mode = kind;
+    rc_score64_kernel<LANE_T><<<d->sm_count * d->lane_per_sm, LANE_T, lsmem, s>>>(l);
+    rc_score64_finalize<<<(nprog + 127) / 128, 128, 0, s>>>(l.flagged, l.nflag, ntiles, l.part,
+                                                            nprog, ntiles, l.bad, n, kind, 0.0,
+                                                            out, status, nullptr);
     rc_noalloc_mark_deep<<<(nprog + 127) / 128, 128, 0, s>>>(
         nprog, reinterpret_cast<const int *>(sc + o_deep), out, status);
     const cudaError_t e = cudaGetLastError();
