@@ -1,30 +1,36 @@
 /*
  * Batched Levenberg-Marquardt / IRLS constant fitting with a fused
- * forward + reverse-mode adjoint sweep.
+ * forward + reverse-mode adjoint sweep, driven as a fixed sequence of device
+ * steps captured once in a CUDA graph.
  *
  * Semantics follow the reference's batched fit (my-version/src/cuda/eval.cu:
- * 1106-2606: the LM/IRLS control flow of `fit_kernel`, the per-row weights of
- * `ft_assemble` / `ft_assemble_d`, the objective sweeps `ft_loss` /
- * `ft_loss_d`, the Jacobi-equilibrated damped Cholesky with the ln-det gate
- * `ft_solve`, and the status labels 0-8) and the CPU fitter it stands in for
- * (my-version/src/fit.rs:2534-2624 `fit_lm`, :3092-3170 `irls_fit`). The
- * implicit arm follows my-version/src/implicit.rs:277-409.
+ * 2264-2606 `fit_kernel`: the LM/IRLS control flow, lambda law, Armijo
+ * halvings, f64 re-baseline and polish, status labels 0-8) and the CPU fitter
+ * it stands in for (my-version/src/fit.rs:2534-2624 `fit_lm`, :3092-3170
+ * `irls_fit`); the implicit arm follows my-version/src/implicit.rs:277-409.
  *
- * B200 design:
- *  - one block owns one candidate for its whole LM; blocks are persistent and
- *    pull candidates from a queue ordered by decreasing cost, one launch per
- *    node-count bucket so each bucket gets the shared memory it needs;
- *  - the per-row tape lives in shared memory, [node][thread]. The forward
- *    sweep writes values; the reverse sweep overwrites a child's value with
- *    its adjoint once its (single) parent has been processed, so one array
- *    serves both sweeps (a fit record program is a tree);
- *  - each chunk of rows deposits its scaled Jacobian rows and residuals in a
- *    shared f64 row buffer; J^T J and J^T r are accumulated by a 4x4
- *    register-blocked f64 SYRK (one block of the augmented Gram per thread,
- *    rows split across thread groups), then reduced across groups in a fixed
- *    order: deterministic, no atomics;
- *  - rows are f32 in the LM phase and f64 in the polish (as in the
- *    reference); the damped solve and accept/reject are f64.
+ * B200 design. The reference runs one block per candidate for the whole LM,
+ * so a candidate's 262,144 rows are swept by 128 threads while most of the
+ * GPU waits for the slowest candidate. Here every sweep is spread over
+ * (candidate x 4,096-row tile) work items for all active candidates at once:
+ *
+ *   step s:  sweep kernels, one per kind (f32 assembly, f64 assembly, f32
+ *            objective, f64 objective; implicit Jacobian / cost), each a
+ *            persistent grid over the (candidate, tile) items whose candidate
+ *            requested that kind -> per-tile partials (packed J^T J / J^T r
+ *            blocks, objective, flags);
+ *            control kernel: per candidate that had a sweep, reduce its tile
+ *            partials in ascending tile order, run the reference's LM state
+ *            machine (damped Jacobi-equilibrated Cholesky in f64, trial
+ *            clamp, accept / reject, lambda, IRLS rounds, polish) until it
+ *            needs the next sweep, and queue it for step s+1.
+ *
+ * The number of steps any candidate can need is bounded (two sweeps per LM
+ * iteration, four with L1 halvings, plus the polish), so the whole fit is a
+ * fixed graph of kernels replayed per batch; candidates that finish early
+ * simply stop queueing work. Every statistic is a fixed-order sum (per row
+ * chunk, SYRK row groups, tiles), so a candidate's result does not depend on
+ * the batch it is fitted in.
  */
 #include <algorithm>
 #include <cmath>
@@ -33,19 +39,39 @@
 #include <string>
 #include <vector>
 
-#include "rc_internal.h"
-#include "rc_ops.cuh"
+#include "fit_common.cuh"
 
-#define FT_MAX_CONST 20
-#define FT_MAX_NODES_ABI 96   /* the reference's plan cap (fit.rs:854) */
-#define FT_MAX_NODES 255      /* what this kernel accepts */
-#define FT_THREADS 128
-#define FT_L1_EPS 1e-6
-#define FT_LN_DET_FLOOR (-27.631021115928547)
+#define FT_TILE_ROWS 4096
+#define FT_NBLK_MAX 21                     /* 4x4 blocks of a 24-wide augmented Gram */
+#define FT_PART_LOSS (FT_NBLK_MAX * 16)
+#define FT_PART_BAD (FT_PART_LOSS + 1)
+#define FT_PART_SKIP (FT_PART_LOSS + 2)
+#define FT_PART_STRIDE (FT_PART_LOSS + 4)
+#define FT_NTRI (FT_MAX_CONST * (FT_MAX_CONST + 1) / 2)
 
 enum {
-    FM_SQUARED = 0, FM_LOG_SQUASHED = 1, FM_CORRELATION = 2, FM_CORRELATION_SIGNED = 3,
-    FM_ABSOLUTE = 4, FM_LOGISTIC = 5, FM_IMPLICIT = 6
+    FOP_NONE = 0, FOP_ASM32 = 1, FOP_ASM64 = 2, FOP_LOSS32 = 3, FOP_LOSS64 = 4,
+    FOP_IJAC = 5, FOP_ICOST = 6, FOP_COUNT = 7
+};
+
+enum {
+    PC_INIT = 0, PC_AFTER_FIRST_ASM, PC_ROUND, PC_ITER, PC_AFTER_ASM, PC_SOLVE,
+    PC_AFTER_TRIAL, PC_REBASE, PC_AFTER_REBASE, PC_POLISH, PC_AFTER_PASM, PC_AFTER_PTRIAL,
+    PC_END, PC_I_INIT, PC_I_AFTER_BASE, PC_I_ITER, PC_I_AFTER_JAC, PC_I_AFTER_TRIAL, PC_I_END,
+    PC_DONE
+};
+
+/* Per-candidate LM state, resident in device memory between steps. */
+struct FitState {
+    double c[FT_MAX_CONST];
+    double trial[FT_MAX_CONST];
+    double start_c[FT_MAX_CONST];
+    double jtj[FT_NTRI];
+    double jtr[FT_MAX_CONST];
+    double lambda, best, start_best;
+    int pc, op, sel;
+    int status, round, it, half, pit;
+    int assembled, improved, rank, skip, start;
 };
 
 struct FitArgs {
@@ -57,514 +83,104 @@ struct FitArgs {
     const double *tsign64;
     const double *w;
     int n, npad, v;
-    const uint4 *rec;      /* fit records, 16 bytes per node */
-    const int *node_off;   /* [P+1] node offsets */
+    const uint4 *rec;
+    const int *node_off;
     const int *pcount;
     int kmax;
     const double *c0;
-    const int *valid;      /* host-validated: 1 = a well-formed tree */
-    int iters;
-    int metric;
-    int flags;
-    const int *order;      /* candidates of this bucket, costliest first */
-    int ncand;
-    int *counter;
-    int mmax;              /* largest node count in the bucket */
-    int W;                 /* padded augmented width, multiple of 4, >= p + 1 */
+    const int *valid;
+    int iters, metric, flags;
+    int ntiles;
+    int mmax;
+    int Wmax;
+    int nprog;
+    FitState *state;
+    double *part;      /* [P][ntiles][FT_PART_STRIDE] */
+    int *lists;        /* [2][FOP_COUNT][P] */
+    int *counts;       /* [2][FOP_COUNT] candidates queued per kind */
+    int *work;         /* [2][FOP_COUNT] persistent-grid work counters */
     double *outc;
     double *outsse;
     int *outstatus;
 };
 
-/* ---- shared-memory layout ------------------------------------------- */
+/* ---- sweep kernels ------------------------------------------------------ */
 
-struct FitLayout {
-    size_t o_rec, o_tape, o_rows, o_gram, o_jtj, o_jtr, o_L, o_c, o_cf, o_trial, o_delta, o_red,
-        o_base, total;
-};
-
-__host__ __device__ inline size_t ft_align(size_t x) { return (x + 15) & ~(size_t)15; }
-
-__host__ __device__ inline FitLayout ft_layout(int mmax, int W, int T)
+__host__ __device__ inline bool ft_op_assembles(int opk)
 {
-    FitLayout L;
-    size_t cur = 0;
-    auto take = [&](size_t bytes) {
-        size_t o = cur;
-        cur = ft_align(cur + bytes);
-        return o;
-    };
-    L.o_rec = take(sizeof(uint4) * (size_t)mmax);
-    /* f32 tape [m][T] in the LM phase; f64 tape [m][T/2] in the polish. */
-    L.o_tape = take(sizeof(float) * (size_t)mmax * T);
-    /* Jacobian rows [T][W] f64; reused for the SYRK partials [T][16] f64. */
-    size_t rows = sizeof(double) * (size_t)T * W;
-    size_t part = sizeof(double) * (size_t)T * 16;
-    L.o_rows = take(rows > part ? rows : part);
-    L.o_gram = take(sizeof(double) * (size_t)W * W);
-    L.o_jtj = take(sizeof(double) * (FT_MAX_CONST * (FT_MAX_CONST + 1) / 2));
-    L.o_jtr = take(sizeof(double) * FT_MAX_CONST);
-    L.o_L = take(sizeof(double) * FT_MAX_CONST * (FT_MAX_CONST + 1));
-    L.o_c = take(sizeof(double) * FT_MAX_CONST);
-    L.o_cf = take(sizeof(float) * FT_MAX_CONST);
-    L.o_trial = take(sizeof(double) * FT_MAX_CONST);
-    L.o_delta = take(sizeof(double) * FT_MAX_CONST);
-    L.o_red = take(sizeof(double) * T);
-    L.o_base = take(sizeof(double) * FT_MAX_CONST);
-    L.total = cur;
-    return L;
+    return opk == FOP_ASM32 || opk == FOP_ASM64 || opk == FOP_IJAC;
 }
 
-struct FitCtx {
-    uint4 *rec;
-    float *tape;
-    double *tape64;
-    double *rows;
-    double *gram;
-    double *jtj;
-    double *jtr;
-    double *L;
-    double *c;
-    float *cf;
-    double *trial;
-    double *delta;
-    double *red;
-    double *base;
-};
-
-__device__ inline FitCtx ft_bind(unsigned char *smem, const FitLayout &L)
+__host__ __device__ inline size_t ft_rows_bytes(int Wmax, int T)
 {
-    FitCtx f;
-    f.rec = reinterpret_cast<uint4 *>(smem + L.o_rec);
-    f.tape = reinterpret_cast<float *>(smem + L.o_tape);
-    f.tape64 = reinterpret_cast<double *>(smem + L.o_tape);
-    f.rows = reinterpret_cast<double *>(smem + L.o_rows);
-    f.gram = reinterpret_cast<double *>(smem + L.o_gram);
-    f.jtj = reinterpret_cast<double *>(smem + L.o_jtj);
-    f.jtr = reinterpret_cast<double *>(smem + L.o_jtr);
-    f.L = reinterpret_cast<double *>(smem + L.o_L);
-    f.c = reinterpret_cast<double *>(smem + L.o_c);
-    f.cf = reinterpret_cast<float *>(smem + L.o_cf);
-    f.trial = reinterpret_cast<double *>(smem + L.o_trial);
-    f.delta = reinterpret_cast<double *>(smem + L.o_delta);
-    f.red = reinterpret_cast<double *>(smem + L.o_red);
-    f.base = reinterpret_cast<double *>(smem + L.o_base);
-    return f;
+    const size_t rows = sizeof(double) * (size_t)T * Wmax;
+    const size_t part = sizeof(double) * (size_t)T * 16;
+    return rows > part ? rows : part;
 }
 
-/* ---- per-row sweeps ---------------------------------------------------- */
+/* Dynamic shared memory of a sweep kernel: records, constants (f64 and f32),
+   the tape (f32 [node][T], or f64 [node][T/2]), the Jacobian row buffer for
+   the assembling kinds, and a reduction buffer. */
+__host__ __device__ inline size_t ft_sweep_smem(int opk, int mmax, int Wmax, int T)
+{
+    size_t s = 16 * (size_t)mmax + 16 * FT_MAX_CONST + 4 * (size_t)mmax * T;
+    if (ft_op_assembles(opk)) s += ft_rows_bytes(Wmax, T);
+    return s + 8 * (size_t)T;
+}
 
-/* f32 forward sweep of one row; `tp` is this thread's tape column (stride T). */
+/* Fixed-order reduction of the per-thread SYRK blocks over the row groups,
+   written packed ([block][16]) to the tile's partial. */
 template <int T>
-__device__ __forceinline__ float ft_fwd_f(const uint4 *rec, int m, const float *cols, int npad,
-                                          int row, const float *cf, float *tp)
-{
-    float val = 0.0f;
-    for (int i = 0; i < m; ++i) {
-        const uint4 r = rec[i];
-        if (r.x == OP_CONST) val = cf[r.w];
-        else if (r.x == OP_VAR) val = __ldg(cols + (size_t)r.w * npad + row);
-        else {
-            const float a = tp[r.y * T];
-            const float b = ft_op_binary(r.x) ? tp[r.z * T] : 0.0f;
-            val = ft_value_f(r.x, a, b);
-        }
-        tp[i * T] = val;
-    }
-    return val;
-}
-
-/* f64 forward sweep; `tp` has stride TS. */
-template <int TS>
-__device__ __forceinline__ double ft_fwd_d(const uint4 *rec, int m, const double *cols, int npad,
-                                           int row, const double *c, double *tp)
-{
-    double val = 0.0;
-    for (int i = 0; i < m; ++i) {
-        const uint4 r = rec[i];
-        if (r.x == OP_CONST) val = c[r.w];
-        else if (r.x == OP_VAR) val = __ldg(cols + (size_t)r.w * npad + row);
-        else {
-            const double a = tp[r.y * TS];
-            const double b = ft_op_binary(r.x) ? tp[r.z * TS] : 0.0;
-            val = ft_value_d(r.x, a, b);
-        }
-        tp[i * TS] = val;
-    }
-    return val;
-}
-
-/* f64 forward with the row's inputs given explicitly (implicit metric). */
-template <int TS>
-__device__ __forceinline__ double ft_fwd_d_x(const uint4 *rec, int m, const double *x,
-                                             const double *c, double *tp)
-{
-    double val = 0.0;
-    for (int i = 0; i < m; ++i) {
-        const uint4 r = rec[i];
-        if (r.x == OP_CONST) val = c[r.w];
-        else if (r.x == OP_VAR) val = x[r.w];
-        else {
-            const double a = tp[r.y * TS];
-            const double b = ft_op_binary(r.x) ? tp[r.z * TS] : 0.0;
-            val = ft_value_d(r.x, a, b);
-        }
-        tp[i * TS] = val;
-    }
-    return val;
-}
-
-/* Reverse sweep in place (f32). Adjoints of constants are written to
-   g[slot * gs] (f64), of inputs accumulated into ig[col * is] when ig != 0.
-   Every node of a fit-record tree has one parent, so a child's tape entry
-   switches from value to adjoint exactly when its parent is processed.
-   Mirrors eval.cu:1236-1317 (an adjoint of zero passes nothing). */
-template <int T>
-__device__ __forceinline__ void ft_bwd_f(const uint4 *rec, int m, float *tp, double *g, int gs,
-                                         float *ig, int is)
-{
-    tp[(m - 1) * T] = 1.0f;
-    for (int i = m - 1; i >= 0; --i) {
-        const uint4 r = rec[i];
-        const float a = tp[i * T];
-        if (r.x == OP_CONST) {
-            if (g) g[r.w * gs] += (double)a;
-            continue;
-        }
-        if (r.x == OP_VAR) {
-            if (ig) ig[r.w * is] += a;
-            continue;
-        }
-        const bool bin = ft_op_binary(r.x);
-        const float x = tp[r.y * T];
-        const float yv = bin ? tp[r.z * T] : 0.0f;
-        float c0 = 0.0f, c1 = 0.0f;
-        if (a != 0.0f && !(r.x == OP_POW && !(x > 0.0f))) {
-            float d0, d1;
-            ft_partials_f(r.x, x, yv, d0, d1);
-            c0 = a * d0;
-            c1 = a * d1;
-        }
-        tp[r.y * T] = c0;
-        if (bin) tp[r.z * T] = c1;
-    }
-}
-
-template <int TS>
-__device__ __forceinline__ void ft_bwd_d(const uint4 *rec, int m, double *tp, double *g, int gs,
-                                         double *ig, int is)
-{
-    tp[(m - 1) * TS] = 1.0;
-    for (int i = m - 1; i >= 0; --i) {
-        const uint4 r = rec[i];
-        const double a = tp[i * TS];
-        if (r.x == OP_CONST) {
-            if (g) g[r.w * gs] += a;
-            continue;
-        }
-        if (r.x == OP_VAR) {
-            if (ig) ig[r.w * is] += a;
-            continue;
-        }
-        const bool bin = ft_op_binary(r.x);
-        const double x = tp[r.y * TS];
-        const double yv = bin ? tp[r.z * TS] : 0.0;
-        double c0 = 0.0, c1 = 0.0;
-        if (a != 0.0 && !(r.x == OP_POW && !(x > 0.0))) {
-            double d0, d1;
-            ft_partials_d(r.x, x, yv, d0, d1);
-            c0 = a * d0;
-            c1 = a * d1;
-        }
-        tp[r.y * TS] = c0;
-        if (bin) tp[r.z * TS] = c1;
-    }
-}
-
-/* ---- objective pieces (eval.cu:638-693, 1492-1855) ------------------- */
-
-__device__ __forceinline__ float ft_row_loss_f(float r, int metric)
-{
-    if (metric == FM_LOG_SQUASHED) {
-        const float rr = r * r;
-        return isfinite(rr) ? log1pf(rr) : 2.0f * logf(fabsf(r));
-    }
-    if (metric == FM_ABSOLUTE) return fabsf(r);
-    return r * r;
-}
-
-__device__ __forceinline__ double ft_row_weight(double base, double r, int metric)
-{
-    if (metric == FM_LOG_SQUASHED) return base * 2.0 / (1.0 + r * r);
-    if (metric == FM_ABSOLUTE) return base / fmax(fabs(r), FT_L1_EPS);
-    return base;
-}
-
-__device__ __forceinline__ double ft_logistic_q(double u)
-{
-    double q;
-    if (u >= 0.0) q = 1.0 / (1.0 + exp(-u));
-    else {
-        const double e = exp(u);
-        q = e / (1.0 + e);
-    }
-    return fmin(1.0 - 1e-9, fmax(1e-9, q));
-}
-
-__device__ __forceinline__ double ft_softplus_neg(double u)
-{
-    const double a = fabs(u);
-    return (u < 0.0 ? -u : 0.0) + log1p(exp(-a));
-}
-
-/* ---- block reductions -------------------------------------------------- */
-
-template <int T>
-__device__ __forceinline__ double ft_block_sum(double v, double *red)
+__device__ __forceinline__ void ft_tile_gram_out(const Syrk &sy, const double acc[16],
+                                                 double *buf, double *pt)
 {
     const int tid = threadIdx.x;
-    red[tid] = v;
-    __syncthreads();
-    for (int st = T / 2; st > 0; st >>= 1) {
-        if (tid < st) red[tid] += red[tid + st];
-        __syncthreads();
-    }
-    const double total = red[0];
-    __syncthreads();
-    return total;
-}
-
-/* SYRK block assignment: the (W/4)x(W/4) block lower triangle of the
-   augmented Gram [J | r]^T [J | r] is split into nblk 4x4 blocks; thread t
-   owns block t % nblk and rows r == t / nblk (mod RG). */
-struct Syrk {
-    int nblk, RG, blk, rg, bi, bj;
-};
-
-template <int T>
-__device__ __forceinline__ Syrk ft_syrk_setup(int W)
-{
-    Syrk s;
-    const int nb = W / 4;
-    s.nblk = nb * (nb + 1) / 2;
-    s.RG = T / s.nblk;
-    if (s.RG < 1) s.RG = 1;
-    s.blk = threadIdx.x % s.nblk;
-    s.rg = threadIdx.x / s.nblk;
-    int b = s.blk, i = 0;
-    while (b > i) {
-        b -= i + 1;
-        ++i;
-    }
-    s.bi = i;
-    s.bj = b;
-    return s;
-}
-
-/* Accumulate rows [0, R) of the row buffer into this thread's block. */
-__device__ __forceinline__ void ft_syrk_chunk(const Syrk &s, const double *rows, int W, int R,
-                                              double acc[16])
-{
-    if (s.rg >= s.RG) return;
-    for (int r = s.rg; r < R; r += s.RG) {
-        const double *row = rows + (size_t)r * W;
-        const double2 a01 = *reinterpret_cast<const double2 *>(row + 4 * s.bi);
-        const double2 a23 = *reinterpret_cast<const double2 *>(row + 4 * s.bi + 2);
-        const double2 b01 = *reinterpret_cast<const double2 *>(row + 4 * s.bj);
-        const double2 b23 = *reinterpret_cast<const double2 *>(row + 4 * s.bj + 2);
-        const double av[4] = {a01.x, a01.y, a23.x, a23.y};
-        const double bv[4] = {b01.x, b01.y, b23.x, b23.y};
+    if (sy.rg < sy.RG) {
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) acc[i * 4 + j] = fma(av[i], bv[j], acc[i * 4 + j]);
+        for (int e = 0; e < 16; ++e) buf[(sy.rg * sy.nblk + sy.blk) * 16 + e] = acc[e];
     }
+    __syncthreads();
+    for (int q = tid; q < sy.nblk * 16; q += T) {
+        const int blk = q >> 4, e = q & 15;
+        double s = 0.0;
+        for (int g = 0; g < sy.RG; ++g) s += buf[(g * sy.nblk + blk) * 16 + e];
+        pt[q] = s;
+    }
+    __syncthreads();
 }
 
-/* Reduce the per-group partial blocks in ascending group order and unpack the
-   packed lower triangle J^T J (p(p+1)/2) and J^T r (p). */
+/* f32 assembly of one tile at the f32 constants `cf` (eval.cu:1692-1804). */
 template <int T>
-__device__ __forceinline__ void ft_syrk_finish(const Syrk &s, double acc[16], double *part,
-                                               double *gram, int W, int p, double *jtj,
-                                               double *jtr)
+__device__ void ft_tile_asm32(const FitArgs &a, const uint4 *rec, int m, int p, const float *cf,
+                              float *tape, double *rows, double *red, int r0, int r1, double *pt)
 {
     const int tid = threadIdx.x;
-    if (s.rg < s.RG) {
-#pragma unroll
-        for (int e = 0; e < 16; ++e) part[(s.rg * s.nblk + s.blk) * 16 + e] = acc[e];
-    }
-    __syncthreads();
-    for (int q = tid; q < s.nblk * 16; q += T) {
-        const int blk = q / 16, e = q % 16;
-        double sum = 0.0;
-        for (int g = 0; g < s.RG; ++g) sum += part[(g * s.nblk + blk) * 16 + e];
-        int b = blk, bi = 0;
-        while (b > bi) {
-            b -= bi + 1;
-            ++bi;
-        }
-        const int i = 4 * bi + e / 4, j = 4 * b + e % 4;
-        gram[i * W + j] = sum;
-    }
-    __syncthreads();
-    for (int q = tid; q < p * (p + 1) / 2 + p; q += T) {
-        if (q < p * (p + 1) / 2) {
-            int i = 0, k = q;
-            while (k > i) {
-                k -= i + 1;
-                ++i;
-            }
-            jtj[q] = gram[i * W + k];
-        } else {
-            const int j = q - p * (p + 1) / 2;
-            jtr[j] = gram[p * W + j];
-        }
-    }
-    __syncthreads();
-}
-
-/* ---- the damped solve (eval.cu:1873-1949 `ft_solve`) ----------------- */
-
-__device__ int ft_solve(const double *jtj, const double *jtr, double lambda, int p, double *delta,
-                        double *L)
-{
-    double dscale[FT_MAX_CONST];
-    for (int i = 0; i < p; ++i) {
-        const double aii = jtj[i * (i + 1) / 2 + i];
-        if (!(aii > 0.0) || !isfinite(aii)) return 1;
-        dscale[i] = sqrt(aii);
-    }
-    int rank_deficient = 0;
-    double sum_ln_L = 0.0;
-    int ok = 1;
-    for (int i = 0; i < p && ok; ++i) {
-        for (int j = 0; j <= i; ++j) {
-            double s = jtj[i * (i + 1) / 2 + j] / (dscale[i] * dscale[j]);
-            if (!isfinite(s)) return 1;
-            for (int k = 0; k < j; ++k) s -= L[i * p + k] * L[j * p + k];
-            if (i == j) {
-                if (!(s > 0.0) || !isfinite(s)) {
-                    ok = 0;
-                    break;
-                }
-                L[i * p + i] = sqrt(s);
-                sum_ln_L += 0.5 * log(s);
-            } else {
-                L[i * p + j] = s / L[j * p + j];
-            }
-        }
-    }
-    if (!ok) rank_deficient = 1;
-    else {
-        const double ln_det = 2.0 * sum_ln_L;
-        if (!isfinite(ln_det) || ln_det < FT_LN_DET_FLOOR) rank_deficient = 1;
-    }
-    for (int i = 0; i < p; ++i) {
-        for (int j = 0; j <= i; ++j) {
-            double s = jtj[i * (i + 1) / 2 + j] / (dscale[i] * dscale[j]);
-            if (i == j) s = s * (1.0 + lambda) + 1e-12;
-            for (int k = 0; k < j; ++k) s -= L[i * p + k] * L[j * p + k];
-            if (i == j) {
-                if (!(s > 1e-18) || !isfinite(s)) return 1;
-                L[i * p + i] = sqrt(s);
-            } else {
-                L[i * p + j] = s / L[j * p + j];
-            }
-        }
-    }
-    double rhs[FT_MAX_CONST];
-    for (int i = 0; i < p; ++i) rhs[i] = -jtr[i] / dscale[i];
-    for (int i = 0; i < p; ++i) {
-        double s = rhs[i];
-        for (int k = 0; k < i; ++k) s -= L[i * p + k] * rhs[k];
-        rhs[i] = s / L[i * p + i];
-    }
-    for (int i = p - 1; i >= 0; --i) {
-        double s = rhs[i];
-        for (int k = i + 1; k < p; ++k) s -= L[k * p + i] * delta[k];
-        delta[i] = s / L[i * p + i];
-    }
-    for (int i = 0; i < p; ++i) delta[i] /= dscale[i];
-    return rank_deficient ? 4 : 0;
-}
-
-/* Gaussian elimination with partial pivoting on (A + lambda diag A + 1e-12 I)
-   (implicit.rs:215-253). `M` is p x (p+1) scratch. Returns 0 or 1 (singular). */
-__device__ int ft_gauss_solve(const double *jtj, const double *jtr, double lambda, int p,
-                              double *delta, double *M)
-{
-    const int w = p + 1;
-    for (int i = 0; i < p; ++i) {
-        for (int j = 0; j < p; ++j) {
-            const int a = i > j ? i : j, b = i > j ? j : i;
-            M[i * w + j] = jtj[a * (a + 1) / 2 + b];
-        }
-        M[i * w + i] = M[i * w + i] * (1.0 + lambda) + 1e-12;
-        M[i * w + p] = -jtr[i];
-    }
-    for (int col = 0; col < p; ++col) {
-        int piv = col;
-        for (int r = col + 1; r < p; ++r)
-            if (fabs(M[r * w + col]) > fabs(M[piv * w + col])) piv = r;
-        if (fabs(M[piv * w + col]) < 1e-300) return 1;
-        if (piv != col)
-            for (int c = 0; c <= p; ++c) {
-                const double t = M[col * w + c];
-                M[col * w + c] = M[piv * w + c];
-                M[piv * w + c] = t;
-            }
-        for (int r = col + 1; r < p; ++r) {
-            const double f = M[r * w + col] / M[col * w + col];
-            if (f != 0.0)
-                for (int c = col; c <= p; ++c) M[r * w + c] -= f * M[col * w + c];
-        }
-    }
-    for (int i = p - 1; i >= 0; --i) {
-        double s = M[i * w + p];
-        for (int j = i + 1; j < p; ++j) s -= M[i * w + j] * delta[j];
-        delta[i] = s / M[i * w + i];
-    }
-    return 0;
-}
-
-/* ---- sweeps over all rows -------------------------------------------- */
-
-struct SweepOut {
-    double loss;
-    int bad;
-    int skipped;
-};
-
-/* f32 assembly at f.c (eval.cu:1692-1804): J^T J, J^T r and the objective. */
-template <int T>
-__device__ SweepOut ft_assemble_f(const FitArgs &a, const FitCtx &f, int m, int p, int W,
-                                  const Syrk &sy)
-{
-    const int tid = threadIdx.x;
+    const int W = 4 * ((p + 1 + 3) / 4);
+    const Syrk sy = ft_syrk_setup<T>(W);
     double acc[16];
 #pragma unroll
     for (int e = 0; e < 16; ++e) acc[e] = 0.0;
     double loss = 0.0;
     int bad = 0;
-    float *tp = f.tape + tid;
-    double *myrow = f.rows + (size_t)tid * W;
-    for (int base = 0; base < a.n; base += T) {
+    float *tp = tape + tid;
+    double *myrow = rows + (size_t)tid * W;
+    for (int base = r0; base < r1; base += T) {
         const int row = base + tid;
         for (int j = 0; j < W; ++j) myrow[j] = 0.0;
-        const double wr = (row < a.n && a.w) ? a.w[row] : 1.0;
-        if (row < a.n && wr > 0.0) {
-            const float pred = ft_fwd_f<T>(f.rec, m, a.cols, a.npad, row, f.cf, tp);
+        const double wr = (row < r1 && a.w) ? a.w[row] : 1.0;
+        if (row < r1 && wr > 0.0) {
+            const float pred = ft_fwd_f<T>(rec, m, a.cols, a.npad, row, cf, tp);
             const float r = pred - a.y[row];
             bool ok = isfinite(pred) && fabsf(pred) <= 1e30f && isfinite(r);
-            ft_bwd_f<T>(f.rec, m, tp, myrow, 1, nullptr, 0);
+            ft_bwd_f<T>(rec, m, tp, myrow, 1, nullptr, 0);
             double sw, resp = (double)r, rowloss;
             if (a.metric == FM_LOGISTIC) {
                 const double tt = a.tsign ? (double)a.tsign[row] : 0.0;
                 const double u = tt * (double)pred;
                 if (!a.tsign || !isfinite(tt)) ok = false;
-                const double q = ft_logistic_q(u);
-                sw = wr * q * (1.0 - q);
-                resp = -tt / q;
+                const double qq = ft_logistic_q(u);
+                sw = wr * qq * (1.0 - qq);
+                resp = -tt / qq;
                 rowloss = wr * ft_softplus_neg(u);
             } else {
                 sw = ft_row_weight(wr, (double)r, a.metric);
@@ -579,41 +195,47 @@ __device__ SweepOut ft_assemble_f(const FitArgs &a, const FitCtx &f, int m, int 
             else bad = 1;
         }
         __syncthreads();
-        ft_syrk_chunk(sy, f.rows, W, T, acc);
+        ft_syrk_chunk(sy, rows, W, T, acc);
         __syncthreads();
     }
-    SweepOut o;
-    o.bad = __syncthreads_or(bad);
-    o.loss = ft_block_sum<T>(loss, f.red);
-    o.skipped = 0;
-    ft_syrk_finish<T>(sy, acc, f.rows, f.gram, W, p, f.jtj, f.jtr);
-    return o;
+    bad = __syncthreads_or(bad);
+    loss = ft_block_sum<T>(loss, red);
+    ft_tile_gram_out<T>(sy, acc, rows, pt);
+    if (tid == 0) {
+        pt[FT_PART_LOSS] = loss;
+        pt[FT_PART_BAD] = bad ? 1.0 : 0.0;
+        pt[FT_PART_SKIP] = 0.0;
+    }
 }
 
-/* f64 assembly for the polish (eval.cu:1492-1630), T/2 rows per chunk. */
+/* f64 assembly of one tile at the f64 constants `cd` (eval.cu:1492-1630):
+   T/2 rows per chunk, each with an f64 tape column. */
 template <int T>
-__device__ SweepOut ft_assemble_d(const FitArgs &a, const FitCtx &f, int m, int p, int W,
-                                  const Syrk &sy)
+__device__ void ft_tile_asm64(const FitArgs &a, const uint4 *rec, int m, int p, const double *cd,
+                              double *tape64, double *rows, double *red, int r0, int r1,
+                              double *pt)
 {
     constexpr int TS = T / 2;
     const int tid = threadIdx.x;
+    const int W = 4 * ((p + 1 + 3) / 4);
+    const Syrk sy = ft_syrk_setup<T>(W);
     double acc[16];
 #pragma unroll
     for (int e = 0; e < 16; ++e) acc[e] = 0.0;
     double loss = 0.0;
     int bad = 0, skipped = 0;
-    double *tp = f.tape64 + tid;
-    double *myrow = f.rows + (size_t)tid * W;
-    for (int base = 0; base < a.n; base += TS) {
+    double *tp = tape64 + tid;
+    double *myrow = rows + (size_t)tid * W;
+    for (int base = r0; base < r1; base += TS) {
         const int row = base + tid;
         if (tid < TS) {
             for (int j = 0; j < W; ++j) myrow[j] = 0.0;
-            const double wr = (row < a.n && a.w) ? a.w[row] : 1.0;
-            if (row < a.n && wr > 0.0) {
-                const double pred = ft_fwd_d<TS>(f.rec, m, a.cols64, a.npad, row, f.c, tp);
+            const double wr = (row < r1 && a.w) ? a.w[row] : 1.0;
+            if (row < r1 && wr > 0.0) {
+                const double pred = ft_fwd_d<TS>(rec, m, a.cols64, a.npad, row, cd, tp);
                 const double r = pred - a.y64[row];
                 bool ok = isfinite(pred) && isfinite(r);
-                ft_bwd_d<TS>(f.rec, m, tp, myrow, 1, nullptr, 0);
+                ft_bwd_d<TS>(rec, m, tp, myrow, 1, nullptr, 0);
                 bool grad_ok = true;
                 for (int j = 0; j < p; ++j)
                     if (!isfinite(myrow[j])) grad_ok = false;
@@ -622,9 +244,9 @@ __device__ SweepOut ft_assemble_d(const FitArgs &a, const FitCtx &f, int m, int 
                     const double tt = a.tsign64 ? a.tsign64[row] : 0.0;
                     const double u = tt * pred;
                     if (!a.tsign64 || !isfinite(tt)) ok = false;
-                    const double q = ft_logistic_q(u);
-                    sw = wr * q * (1.0 - q);
-                    resp = -tt / q;
+                    const double qq = ft_logistic_q(u);
+                    sw = wr * qq * (1.0 - qq);
+                    resp = -tt / qq;
                     rho = ft_softplus_neg(u);
                 } else {
                     sw = ft_row_weight(wr, r, a.metric);
@@ -640,32 +262,34 @@ __device__ SweepOut ft_assemble_d(const FitArgs &a, const FitCtx &f, int m, int 
                 else bad = 1;
                 if (ok && !grad_ok) skipped = 1;
             }
-        } else if (tid < T) {
-            /* rows [TS, T) of the buffer stay unused in the polish */
         }
         __syncthreads();
-        ft_syrk_chunk(sy, f.rows, W, TS, acc);
+        ft_syrk_chunk(sy, rows, W, TS, acc);
         __syncthreads();
     }
-    SweepOut o;
-    o.bad = __syncthreads_or(bad);
-    o.skipped = __syncthreads_or(skipped);
-    o.loss = ft_block_sum<T>(loss, f.red);
-    ft_syrk_finish<T>(sy, acc, f.rows, f.gram, W, p, f.jtj, f.jtr);
-    return o;
+    bad = __syncthreads_or(bad);
+    skipped = __syncthreads_or(skipped);
+    loss = ft_block_sum<T>(loss, red);
+    ft_tile_gram_out<T>(sy, acc, rows, pt);
+    if (tid == 0) {
+        pt[FT_PART_LOSS] = loss;
+        pt[FT_PART_BAD] = bad ? 1.0 : 0.0;
+        pt[FT_PART_SKIP] = skipped ? 1.0 : 0.0;
+    }
 }
 
-/* f32 objective at constants `cf` (eval.cu:1808-1855). */
+/* f32 objective of one tile (eval.cu:1808-1855). */
 template <int T>
-__device__ double ft_loss_f(const FitArgs &a, const FitCtx &f, int m, const float *cf)
+__device__ void ft_tile_loss32(const FitArgs &a, const uint4 *rec, int m, const float *cf,
+                               float *tape, double *red, int r0, int r1, double *pt)
 {
     const int tid = threadIdx.x;
     double local = 0.0;
-    float *tp = f.tape + tid;
-    for (int row = tid; row < a.n; row += T) {
+    float *tp = tape + tid;
+    for (int row = r0 + tid; row < r1; row += T) {
         const double wr = a.w ? a.w[row] : 1.0;
         if (wr <= 0.0) continue;
-        const float pred = ft_fwd_f<T>(f.rec, m, a.cols, a.npad, row, cf, tp);
+        const float pred = ft_fwd_f<T>(rec, m, a.cols, a.npad, row, cf, tp);
         const float r = pred - a.y[row];
         if (!isfinite(pred) || fabsf(pred) > 1e30f || !isfinite(r)) local += 1e30;
         else if (a.metric == FM_LOGISTIC) {
@@ -674,22 +298,27 @@ __device__ double ft_loss_f(const FitArgs &a, const FitCtx &f, int m, const floa
         } else if (a.metric == FM_SQUARED) local += wr * (double)r * (double)r;
         else local += wr * (double)ft_row_loss_f(r, a.metric);
     }
-    return ft_block_sum<T>(local, f.red);
+    const double total = ft_block_sum<T>(local, red);
+    if (tid == 0) {
+        pt[FT_PART_LOSS] = total;
+        pt[FT_PART_BAD] = 0.0;
+    }
 }
 
-/* f64 objective at constants `c` (eval.cu:1634-1682), T/2 rows at a time. */
+/* f64 objective of one tile (eval.cu:1634-1682), T/2 rows at a time. */
 template <int T>
-__device__ double ft_loss_d(const FitArgs &a, const FitCtx &f, int m, const double *c)
+__device__ void ft_tile_loss64(const FitArgs &a, const uint4 *rec, int m, const double *cd,
+                               double *tape64, double *red, int r0, int r1, double *pt)
 {
     constexpr int TS = T / 2;
     const int tid = threadIdx.x;
     double local = 0.0;
     if (tid < TS) {
-        double *tp = f.tape64 + tid;
-        for (int row = tid; row < a.n; row += TS) {
+        double *tp = tape64 + tid;
+        for (int row = r0 + tid; row < r1; row += TS) {
             const double wr = a.w ? a.w[row] : 1.0;
             if (wr <= 0.0) continue;
-            const double pred = ft_fwd_d<TS>(f.rec, m, a.cols64, a.npad, row, c, tp);
+            const double pred = ft_fwd_d<TS>(rec, m, a.cols64, a.npad, row, cd, tp);
             const double r = pred - a.y64[row];
             if (!isfinite(pred) || !isfinite(r)) local += 1e30;
             else if (a.metric == FM_LOGISTIC) {
@@ -700,105 +329,60 @@ __device__ double ft_loss_d(const FitArgs &a, const FitCtx &f, int m, const doub
             else local += wr * log1p(r * r);
         }
     }
-    return ft_block_sum<T>(local, f.red);
+    const double total = ft_block_sum<T>(local, red);
+    if (tid == 0) {
+        pt[FT_PART_LOSS] = total;
+        pt[FT_PART_BAD] = 0.0;
+    }
 }
 
-/* ---- the implicit metric (implicit.rs:68-409) ---------------------------
- * Per row: d = f / ||grad_x f|| (f64 forward + input adjoint); a row with a
- * non-finite value or gradient, or a zero gradient norm, makes the whole
- * evaluation undefined. The LM's Jacobian is central differences of d with
- * h = 1e-6 (1 + |c_j|), exactly as the reference CPU arm. */
-
-#define FT_IMPLICIT_MAXV 16
-
-template <int TS>
-__device__ __forceinline__ bool ft_implicit_d(const uint4 *rec, int m, const double *x, int v,
-                                              const double *c, double *tp, double &d)
-{
-    const double fv = ft_fwd_d_x<TS>(rec, m, x, c, tp);
-    if (!isfinite(fv)) return false;
-    double ig[FT_IMPLICIT_MAXV];
-    for (int k = 0; k < FT_IMPLICIT_MAXV; ++k) ig[k] = 0.0;
-    /* input adjoint accumulated in registers: columns are < FT_IMPLICIT_MAXV */
-    tp[(m - 1) * TS] = 1.0;
-    for (int i = m - 1; i >= 0; --i) {
-        const uint4 r = rec[i];
-        const double a = tp[i * TS];
-        if (r.x == OP_CONST) continue;
-        if (r.x == OP_VAR) {
-#pragma unroll
-            for (int k = 0; k < FT_IMPLICIT_MAXV; ++k)
-                if ((int)r.w == k) ig[k] += a;
-            continue;
-        }
-        const bool bin = ft_op_binary(r.x);
-        const double xx = tp[r.y * TS];
-        const double yy = bin ? tp[r.z * TS] : 0.0;
-        double c0 = 0.0, c1 = 0.0;
-        if (a != 0.0 && !(r.x == OP_POW && !(xx > 0.0))) {
-            double d0, d1;
-            ft_partials_d(r.x, xx, yy, d0, d1);
-            c0 = a * d0;
-            c1 = a * d1;
-        }
-        tp[r.y * TS] = c0;
-        if (bin) tp[r.z * TS] = c1;
-    }
-    double nsq = 0.0;
-    for (int k = 0; k < FT_IMPLICIT_MAXV; ++k) {
-        if (k >= v) break;
-        if (!isfinite(ig[k])) return false;
-        nsq += ig[k] * ig[k];
-    }
-    const double norm = sqrt(nsq);
-    if (!(isfinite(norm) && norm > 0.0)) return false;
-    d = fv / norm;
-    return isfinite(d);
-}
-
-/* One implicit sweep at f.c: when `jac`, also the central-difference Jacobian
-   rows and the J^T J / J^T r assembly; returns the cost sum w d^2, or +inf
-   when any positive-weight row is undefined (at c or at a perturbation). */
-template <int T>
-__device__ double ft_implicit_sweep(const FitArgs &a, const FitCtx &f, int m, int p, int W,
-                                    const Syrk &sy, const double *c, bool jac, int *undefined)
+/* Implicit metric of one tile (implicit.rs:156-174, :302-333): the cost
+   sum w d^2 at `cd`, and with `jac` the central-difference Jacobian rows of
+   sqrt(w) d and their J^T J / J^T r. An undefined row marks the tile bad. */
+template <int T, bool JAC>
+__device__ void ft_tile_implicit(const FitArgs &a, const uint4 *rec, int m, int p,
+                                 const double *cd, double *tape64, double *rows, double *red,
+                                 int r0, int r1, double *pt)
 {
     constexpr int TS = T / 2;
     const int tid = threadIdx.x;
+    const int W = 4 * ((p + 1 + 3) / 4);
+    const Syrk sy = ft_syrk_setup<T>(W);
     double acc[16];
 #pragma unroll
     for (int e = 0; e < 16; ++e) acc[e] = 0.0;
     double cost = 0.0;
     int bad = 0;
-    double *tp = f.tape64 + tid;
-    double *myrow = f.rows + (size_t)tid * W;
+    double *tp = tape64 + tid;
+    double *myrow = rows + (size_t)tid * W;
     double x[FT_IMPLICIT_MAXV];
     double cp[FT_MAX_CONST];
-    for (int base = 0; base < a.n; base += TS) {
+    for (int base = r0; base < r1; base += TS) {
         const int row = base + tid;
         if (tid < TS) {
-            if (jac)
+            if (JAC)
                 for (int j = 0; j < W; ++j) myrow[j] = 0.0;
-            const double wr = (row < a.n && a.w) ? a.w[row] : 1.0;
-            if (row < a.n && wr > 0.0 && isfinite(wr)) {
+            const double wr = (row < r1 && a.w) ? a.w[row] : 1.0;
+            if (row < r1 && !(isfinite(wr) && wr >= 0.0)) bad = 1;
+            else if (row < r1 && wr > 0.0) {
                 for (int k = 0; k < FT_IMPLICIT_MAXV; ++k)
                     x[k] = k < a.v ? a.cols64[(size_t)k * a.npad + row] : 0.0;
                 double d;
-                if (!ft_implicit_d<TS>(f.rec, m, x, a.v, c, tp, d)) bad = 1;
+                if (!ft_implicit_d<TS>(rec, m, x, a.v, cd, tp, d)) bad = 1;
                 else {
                     const double sw = sqrt(wr);
                     const double r = sw * d;
                     cost += r * r;
-                    if (jac) {
-                        for (int j = 0; j < p; ++j) cp[j] = c[j];
+                    if (JAC) {
+                        for (int j = 0; j < p; ++j) cp[j] = cd[j];
                         for (int j = 0; j < p && !bad; ++j) {
-                            const double h = 1e-6 * (1.0 + fabs(c[j]));
+                            const double h = 1e-6 * (1.0 + fabs(cd[j]));
                             double dp, dm;
-                            cp[j] = c[j] + h;
-                            const bool okp = ft_implicit_d<TS>(f.rec, m, x, a.v, cp, tp, dp);
-                            cp[j] = c[j] - h;
-                            const bool okm = ft_implicit_d<TS>(f.rec, m, x, a.v, cp, tp, dm);
-                            cp[j] = c[j];
+                            cp[j] = cd[j] + h;
+                            const bool okp = ft_implicit_d<TS>(rec, m, x, a.v, cp, tp, dp);
+                            cp[j] = cd[j] - h;
+                            const bool okm = ft_implicit_d<TS>(rec, m, x, a.v, cp, tp, dm);
+                            cp[j] = cd[j];
                             if (!okp || !okm) {
                                 bad = 1;
                                 break;
@@ -809,285 +393,515 @@ __device__ double ft_implicit_sweep(const FitArgs &a, const FitCtx &f, int m, in
                         myrow[p] = r;
                     }
                 }
-            } else if (row < a.n && !(wr >= 0.0 && isfinite(wr))) {
-                bad = 1;
             }
         }
-        if (jac) {
+        if (JAC) {
             __syncthreads();
-            ft_syrk_chunk(sy, f.rows, W, TS, acc);
+            ft_syrk_chunk(sy, rows, W, TS, acc);
             __syncthreads();
         }
     }
-    *undefined = __syncthreads_or(bad);
-    const double total = ft_block_sum<T>(cost, f.red);
-    if (jac) ft_syrk_finish<T>(sy, acc, f.rows, f.gram, W, p, f.jtj, f.jtr);
-    return *undefined ? INFINITY : total;
-}
-
-/* ---- the LM driver, one candidate per block ----------------------------- */
-
-__device__ __forceinline__ void ft_set_c(const FitCtx &f, int p, const double *src)
-{
-    const int tid = threadIdx.x;
-    if (tid < p) {
-        f.c[tid] = src[tid];
-        f.cf[tid] = (float)src[tid];
-    }
-    __syncthreads();
-}
-
-template <int T>
-__device__ void ft_lm_standard(const FitArgs &a, const FitCtx &f, int m, int p, int W,
-                               const Syrk &sy, double &best_out, int &status_out)
-{
-    const int tid = threadIdx.x;
-    __shared__ double s_best, s_lambda, s_tsse;
-    __shared__ int s_flag, s_rank, s_improved, s_start, s_skip;
-    const int irls = (a.metric == FM_ABSOLUTE);
-    const int iters = a.iters;
-    const int rounds = irls ? (iters < 1 ? 1 : (iters < 4 ? iters : 4)) : 1;
-    const int inner = irls ? (iters / rounds < 1 ? 1 : iters / rounds) : iters;
-    int status = 0;
-    double best = 0.0;
+    bad = __syncthreads_or(bad);
+    cost = ft_block_sum<T>(cost, red);
+    if (JAC) ft_tile_gram_out<T>(sy, acc, rows, pt);
     if (tid == 0) {
-        s_rank = 0;
-        s_improved = 0;
-        s_start = 0;
-        s_skip = 0;
-        s_lambda = 1e-3;
+        pt[FT_PART_LOSS] = cost;
+        pt[FT_PART_BAD] = bad ? 1.0 : 0.0;
+        pt[FT_PART_SKIP] = 0.0;
     }
-    __syncthreads();
-    if (iters > 0) {
-        SweepOut o = ft_assemble_f<T>(a, f, m, p, W, sy);
-        int assembled = 1;
-        best = o.loss;
-        if (tid == 0) s_start = o.bad ? 0 : 1;
-        if (o.bad) status = 2;
-        for (int round = 0; round < rounds && status == 0 && best != 0.0; ++round) {
-            if (irls && round > 0) assembled = 0;
-            for (int it = 0; it < inner && status == 0; ++it) {
-                if (!assembled) {
-                    o = ft_assemble_f<T>(a, f, m, p, W, sy);
-                    assembled = 1;
-                    if (o.bad) {
-                        status = 2;
-                        break;
-                    }
-                }
-                if (tid == 0) {
-                    const int sv = ft_solve(f.jtj, f.jtr, s_lambda, p, f.delta, f.L);
-                    s_flag = sv != 1;
-                    if (sv == 4) s_rank = 1;
-                    if (s_flag)
-                        for (int j = 0; j < p; ++j) {
-                            const double t = f.c[j] + f.delta[j];
-                            f.trial[j] = fmin(1e6, fmax(-1e6, t));
-                        }
-                }
-                __syncthreads();
-                if (!s_flag) {
-                    status = 1;
-                    break;
-                }
-                /* f32 copy of the trial constants lives in `base` (as floats) */
-                float *tcf = reinterpret_cast<float *>(f.base);
-                if (tid < p) tcf[tid] = (float)f.trial[tid];
-                __syncthreads();
-                double tsse = ft_loss_f<T>(a, f, m, tcf);
-                /* True-metric Armijo for L1: two halvings (eval.cu:2486-2497). */
-                for (int half = 0; half < (irls ? 2 : 0) && !(tsse < best); ++half) {
-                    if (tid < p) {
-                        f.trial[tid] = f.c[tid] + 0.5 * (f.trial[tid] - f.c[tid]);
-                        tcf[tid] = (float)f.trial[tid];
-                    }
-                    __syncthreads();
-                    tsse = ft_loss_f<T>(a, f, m, tcf);
-                }
-                if (tsse < best) {
-                    ft_set_c(f, p, f.trial);
-                    best = tsse;
-                    if (tid == 0) {
-                        s_lambda = fmax(s_lambda / 8.0, 1e-12);
-                        s_improved = 1;
-                    }
-                    __syncthreads();
-                    assembled = 0;
-                    if (best == 0.0) break;
-                } else {
-                    if (tid == 0) s_lambda *= 6.0;
-                    __syncthreads();
-                    if (s_lambda > 1e9) break;
-                }
-            }
-        }
-        /* Re-baseline in f64, then the undamped Gauss-Newton polish in f64
-           (eval.cu:2537-2580). */
-        if (status == 0 && !(a.flags & 1)) {
-            const double exact = ft_loss_d<T>(a, f, m, f.c);
-            if (isfinite(exact)) best = exact;
-            for (int it = 0; it < 4 && status == 0 && best != 0.0; ++it) {
-                SweepOut od = ft_assemble_d<T>(a, f, m, p, W, sy);
-                if (tid == 0 && od.skipped) s_skip = 1;
-                if (od.bad) {
-                    status = 2;
-                    break;
-                }
-                if (tid == 0) {
-                    const int sv = ft_solve(f.jtj, f.jtr, 0.0, p, f.delta, f.L);
-                    s_flag = sv != 1;
-                    if (sv == 4) s_rank = 1;
-                    if (s_flag)
-                        for (int j = 0; j < p; ++j) {
-                            const double t = f.c[j] + f.delta[j];
-                            f.trial[j] = fmin(1e6, fmax(-1e6, t));
-                        }
-                }
-                __syncthreads();
-                if (!s_flag) break;
-                double tsse = ft_loss_d<T>(a, f, m, f.trial);
-                if (irls && !(tsse < best)) {
-                    if (tid < p) f.trial[tid] = f.c[tid] + 0.5 * (f.trial[tid] - f.c[tid]);
-                    __syncthreads();
-                    tsse = ft_loss_d<T>(a, f, m, f.trial);
-                }
-                if (tsse < best) {
-                    ft_set_c(f, p, f.trial);
-                    best = tsse;
-                    if (tid == 0) s_improved = 1;
-                    __syncthreads();
-                } else {
-                    break;
-                }
-            }
-        }
-    }
-    __syncthreads();
-    /* Status labels (eval.cu:2583-2600). */
-    if (status == 1 || status == 2) {
-        if (!s_start) status = 7;
-        else if (s_improved) status = 5;
-        else status = 6;
-    } else if (status == 0) {
-        if (s_skip) status = 8;
-        else if (s_rank) status = 4;
-        else if (!s_improved && iters > 0) status = 6;
-    }
-    best_out = best;
-    status_out = status;
-    (void)s_tsse;
-    (void)s_best;
 }
 
-/* implicit.rs:277-409: LM on the signed geometric residual. */
-template <int T>
-__device__ void ft_lm_implicit(const FitArgs &a, const FitCtx &f, int m, int p, int W,
-                               const Syrk &sy, double &best_out, int &status_out)
+/* One sweep kind over every queued (candidate, tile) item of step parity q. */
+template <int OPK, int T>
+__global__ void __launch_bounds__(T) ft_sweep(FitArgs a, int q)
 {
-    const int tid = threadIdx.x;
-    __shared__ double s_lambda;
-    __shared__ int s_flag, s_improved;
-    int undefined = 0;
-    if (tid == 0) {
-        s_lambda = 1e-3;
-        s_improved = 0;
-    }
-    __syncthreads();
-    /* the starting constants stay in f.base for the final comparison */
-    if (tid < p) f.base[tid] = f.c[tid];
-    __syncthreads();
-    double best = ft_implicit_sweep<T>(a, f, m, p, W, sy, f.c, false, &undefined);
-    if (undefined) {
-        best_out = INFINITY;
-        status_out = 7;
-        return;
-    }
-    const double start = best;
-    if (p > 0 && a.iters > 0) {
-        const int outer = a.iters < 1 ? 1 : a.iters;
-        for (int it = 0; it < outer; ++it) {
-            ft_implicit_sweep<T>(a, f, m, p, W, sy, f.c, true, &undefined);
-            if (undefined) break;
-            if (tid == 0) {
-                const int sv = ft_gauss_solve(f.jtj, f.jtr, s_lambda, p, f.delta, f.L);
-                s_flag = sv == 0;
-                if (s_flag)
-                    for (int j = 0; j < p; ++j)
-                        f.trial[j] = fmin(1e6, fmax(-1e6, f.c[j] + f.delta[j]));
-            }
-            __syncthreads();
-            if (!s_flag) {
-                if (tid == 0) s_lambda *= 6.0;
-                __syncthreads();
-                if (s_lambda > 1e9) break;
-                continue;
-            }
-            int und2 = 0;
-            const double s = ft_implicit_sweep<T>(a, f, m, p, W, sy, f.trial, false, &und2);
-            if (!und2 && s < best) {
-                best = s;
-                ft_set_c(f, p, f.trial);
-                if (tid == 0) {
-                    s_lambda = fmax(s_lambda / 8.0, 1e-12);
-                    s_improved = 1;
-                }
-                __syncthreads();
-                if (best == 0.0) break;
-            } else {
-                if (tid == 0) s_lambda *= 6.0;
-                __syncthreads();
-                if (s_lambda > 1e9) break;
-            }
-        }
-    }
-    /* The reference writes constants back only when they beat the start. */
-    if (!(best < start)) ft_set_c(f, p, f.base);
-    best_out = best;
-    status_out = s_improved ? 0 : 6;
-}
-
-template <int T>
-__global__ void __launch_bounds__(T) ft_kernel(FitArgs a)
-{
-    extern __shared__ __align__(16) unsigned char ft_smem[];
-    const FitLayout Lo = ft_layout(a.mmax, a.W, T);
-    const FitCtx f = ft_bind(ft_smem, Lo);
-    const int tid = threadIdx.x;
+    extern __shared__ __align__(16) unsigned char sm[];
+    uint4 *rec = reinterpret_cast<uint4 *>(sm);
+    double *cd = reinterpret_cast<double *>(sm + 16 * (size_t)a.mmax);
+    float *cf = reinterpret_cast<float *>(cd + FT_MAX_CONST);
+    float *tape = cf + 2 * FT_MAX_CONST;
+    double *tape64 = reinterpret_cast<double *>(tape);
+    double *rows = reinterpret_cast<double *>(tape + (size_t)a.mmax * T);
+    double *red = rows + (ft_op_assembles(OPK) ? ft_rows_bytes(a.Wmax, T) / 8 : 0);
     __shared__ int s_item;
+    const int tid = threadIdx.x;
+    const int *list = a.lists + ((size_t)q * FOP_COUNT + OPK) * a.nprog;
+    const int total = a.counts[q * FOP_COUNT + OPK] * a.ntiles;
+    int *work = a.work + q * FOP_COUNT + OPK;
     for (;;) {
-        if (tid == 0) s_item = atomicAdd(a.counter, 1);
+        if (tid == 0) s_item = atomicAdd(work, 1);
         __syncthreads();
         const int item = s_item;
         __syncthreads();
-        if (item >= a.ncand) break;
-        const int cand = a.order[item];
+        if (item >= total) break;
+        const int cand = list[item / a.ntiles];
+        const int tile = item % a.ntiles;
+        const FitState *st = a.state + cand;
         const int nb = a.node_off[cand];
         const int m = a.node_off[cand + 1] - nb;
         const int p = a.pcount[cand];
-        for (int i = tid; i < m; i += T) f.rec[i] = a.rec[nb + i];
+        const int sel = st->sel;
+        for (int i = tid; i < m; i += T) rec[i] = a.rec[nb + i];
         if (tid < p) {
-            const double c0 = a.c0[(size_t)cand * a.kmax + tid];
-            f.c[tid] = c0;
-            f.cf[tid] = (float)c0;
+            const double cv = sel ? st->trial[tid] : st->c[tid];
+            cd[tid] = cv;
+            cf[tid] = (float)cv;
         }
         __syncthreads();
-        double best = 0.0;
-        int status = 1;
-        if (a.valid[cand]) {
-            int W = 4 * ((p + 1 + 3) / 4);
-            const Syrk sy = ft_syrk_setup<T>(W);
-            if (a.metric == FM_IMPLICIT) ft_lm_implicit<T>(a, f, m, p, W, sy, best, status);
-            else ft_lm_standard<T>(a, f, m, p, W, sy, best, status);
-        } else {
-            best = INFINITY;
+        const int r0 = tile * FT_TILE_ROWS;
+        const int r1 = min(a.n, r0 + FT_TILE_ROWS);
+        double *pt = a.part + ((size_t)cand * a.ntiles + tile) * FT_PART_STRIDE;
+        if (OPK == FOP_ASM32) ft_tile_asm32<T>(a, rec, m, p, cf, tape, rows, red, r0, r1, pt);
+        else if (OPK == FOP_ASM64) ft_tile_asm64<T>(a, rec, m, p, cd, tape64, rows, red, r0, r1, pt);
+        else if (OPK == FOP_LOSS32) ft_tile_loss32<T>(a, rec, m, cf, tape, red, r0, r1, pt);
+        else if (OPK == FOP_LOSS64) ft_tile_loss64<T>(a, rec, m, cd, tape64, red, r0, r1, pt);
+        else if (OPK == FOP_IJAC) ft_tile_implicit<T, true>(a, rec, m, p, cd, tape64, rows, red, r0, r1, pt);
+        else ft_tile_implicit<T, false>(a, rec, m, p, cd, tape64, rows, red, r0, r1, pt);
+        __syncthreads();
+    }
+}
+
+/* ---- the per-candidate controller --------------------------------------- */
+
+/* Status labels of a finished fit (eval.cu:2583-2600), then the outputs. */
+__device__ void ft_finish(const FitArgs &a, FitState &st, int cand, int p)
+{
+    int status = st.status;
+    if (st.pc == PC_END) {
+        if (status == 1 || status == 2) {
+            if (!st.start) status = 7;
+            else if (st.improved) status = 5;
+            else status = 6;
+        } else if (status == 0) {
+            if (st.skip) status = 8;
+            else if (st.rank) status = 4;
+            else if (!st.improved && a.iters > 0) status = 6;
+        }
+    }
+    for (int j = 0; j < p; ++j) a.outc[(size_t)cand * a.kmax + j] = st.c[j];
+    a.outsse[cand] = st.best;
+    a.outstatus[cand] = status;
+    st.pc = PC_DONE;
+    st.op = FOP_NONE;
+}
+
+/* Advance one candidate's LM until it needs a sweep (st.op set) or is done.
+   `rl`, `rb`, `rs` are the reduced objective / bad / skipped flags of the
+   sweep that just ran; jtj/jtr of an assembly are already in `st`. The
+   control flow is eval.cu:2437-2580 (and implicit.rs:277-409 for metric 6),
+   unrolled into explicit states. Thread 0 only. */
+__device__ void ft_advance(const FitArgs &a, FitState &st, int cand, int p, double rl, int rb,
+                           int rs, double *L, double *delta)
+{
+    const int irls = a.metric == FM_ABSOLUTE;
+    const int iters = a.iters;
+    const int rounds = irls ? (iters < 1 ? 1 : (iters < 4 ? iters : 4)) : 1;
+    const int inner = irls ? (iters / rounds < 1 ? 1 : iters / rounds) : iters;
+    for (int guard = 0; guard < 256; ++guard) {
+        switch (st.pc) {
+            case PC_INIT:
+                st.lambda = 1e-3;
+                st.status = 0;
+                st.best = 0.0;
+                st.rank = st.skip = st.improved = st.start = 0;
+                st.assembled = 0;
+                if (!a.valid[cand]) {
+                    st.status = 1;
+                    st.best = INFINITY;
+                    st.pc = PC_DONE;
+                    ft_finish(a, st, cand, p);
+                    return;
+                }
+                if (a.metric == FM_IMPLICIT) {
+                    st.pc = PC_I_INIT;
+                    break;
+                }
+                if (iters <= 0) {
+                    st.pc = PC_END;
+                    break;
+                }
+                st.op = FOP_ASM32;
+                st.sel = 0;
+                st.pc = PC_AFTER_FIRST_ASM;
+                return;
+            case PC_AFTER_FIRST_ASM:
+                st.best = rl;
+                st.start = rb ? 0 : 1;
+                st.assembled = 1;
+                if (rb) {
+                    st.status = 2;
+                    st.pc = PC_REBASE;
+                    break;
+                }
+                st.round = 0;
+                st.pc = PC_ROUND;
+                break;
+            case PC_ROUND:
+                if (!(st.round < rounds && st.status == 0 && st.best != 0.0)) {
+                    st.pc = PC_REBASE;
+                    break;
+                }
+                if (irls && st.round > 0) st.assembled = 0;
+                st.it = 0;
+                st.pc = PC_ITER;
+                break;
+            case PC_ITER:
+                if (!(st.it < inner && st.status == 0)) {
+                    st.round++;
+                    st.pc = PC_ROUND;
+                    break;
+                }
+                if (!st.assembled) {
+                    st.op = FOP_ASM32;
+                    st.sel = 0;
+                    st.pc = PC_AFTER_ASM;
+                    return;
+                }
+                st.pc = PC_SOLVE;
+                break;
+            case PC_AFTER_ASM:
+                st.assembled = 1;
+                if (rb) {
+                    st.status = 2;
+                    st.round++;
+                    st.pc = PC_ROUND;
+                    break;
+                }
+                st.pc = PC_SOLVE;
+                break;
+            case PC_SOLVE: {
+                const int sv = ft_solve(st.jtj, st.jtr, st.lambda, p, delta, L);
+                if (sv == 1) {
+                    st.status = 1;
+                    st.round++;
+                    st.pc = PC_ROUND;
+                    break;
+                }
+                if (sv == 4) st.rank = 1;
+                for (int j = 0; j < p; ++j) st.trial[j] = fmin(1e6, fmax(-1e6, st.c[j] + delta[j]));
+                st.half = 0;
+                st.op = FOP_LOSS32;
+                st.sel = 1;
+                st.pc = PC_AFTER_TRIAL;
+                return;
+            }
+            case PC_AFTER_TRIAL: {
+                const double tsse = rl;
+                /* true-metric Armijo for L1: two halvings (eval.cu:2486-2497) */
+                if (irls && st.half < 2 && !(tsse < st.best)) {
+                    for (int j = 0; j < p; ++j) st.trial[j] = st.c[j] + 0.5 * (st.trial[j] - st.c[j]);
+                    st.half++;
+                    st.op = FOP_LOSS32;
+                    st.sel = 1;
+                    return;
+                }
+                if (tsse < st.best) {
+                    for (int j = 0; j < p; ++j) st.c[j] = st.trial[j];
+                    st.best = tsse;
+                    st.lambda = fmax(st.lambda / 8.0, 1e-12);
+                    st.improved = 1;
+                    st.assembled = 0;
+                    if (st.best == 0.0) {
+                        st.round++;
+                        st.pc = PC_ROUND;
+                        break;
+                    }
+                } else {
+                    st.lambda *= 6.0;
+                    if (st.lambda > 1e9) {
+                        st.round++;
+                        st.pc = PC_ROUND;
+                        break;
+                    }
+                }
+                st.it++;
+                st.pc = PC_ITER;
+                break;
+            }
+            case PC_REBASE:
+                if (st.status == 0 && !(a.flags & 1)) {
+                    st.op = FOP_LOSS64;
+                    st.sel = 0;
+                    st.pc = PC_AFTER_REBASE;
+                    return;
+                }
+                st.pc = PC_END;
+                break;
+            case PC_AFTER_REBASE:
+                if (isfinite(rl)) st.best = rl;
+                st.pit = 0;
+                st.pc = PC_POLISH;
+                break;
+            case PC_POLISH:
+                if (!(st.pit < 4 && st.status == 0 && st.best != 0.0)) {
+                    st.pc = PC_END;
+                    break;
+                }
+                st.op = FOP_ASM64;
+                st.sel = 0;
+                st.pc = PC_AFTER_PASM;
+                return;
+            case PC_AFTER_PASM: {
+                if (rs) st.skip = 1;
+                if (rb) {
+                    st.status = 2;
+                    st.pc = PC_END;
+                    break;
+                }
+                const int sv = ft_solve(st.jtj, st.jtr, 0.0, p, delta, L);
+                if (sv == 1) {
+                    st.pc = PC_END;
+                    break;
+                }
+                if (sv == 4) st.rank = 1;
+                for (int j = 0; j < p; ++j) st.trial[j] = fmin(1e6, fmax(-1e6, st.c[j] + delta[j]));
+                st.half = 0;
+                st.op = FOP_LOSS64;
+                st.sel = 1;
+                st.pc = PC_AFTER_PTRIAL;
+                return;
+            }
+            case PC_AFTER_PTRIAL: {
+                const double tsse = rl;
+                if (irls && st.half == 0 && !(tsse < st.best)) {
+                    for (int j = 0; j < p; ++j) st.trial[j] = st.c[j] + 0.5 * (st.trial[j] - st.c[j]);
+                    st.half = 1;
+                    st.op = FOP_LOSS64;
+                    st.sel = 1;
+                    return;
+                }
+                if (tsse < st.best) {
+                    for (int j = 0; j < p; ++j) st.c[j] = st.trial[j];
+                    st.best = tsse;
+                    st.improved = 1;
+                    st.pit++;
+                    st.pc = PC_POLISH;
+                    break;
+                }
+                st.pc = PC_END;
+                break;
+            }
+            case PC_END:
+                ft_finish(a, st, cand, p);
+                return;
+            /* ---- implicit metric ---- */
+            case PC_I_INIT:
+                for (int j = 0; j < p; ++j) st.start_c[j] = st.c[j];
+                st.op = FOP_ICOST;
+                st.sel = 0;
+                st.pc = PC_I_AFTER_BASE;
+                return;
+            case PC_I_AFTER_BASE:
+                if (rb) {
+                    st.best = INFINITY;
+                    st.status = 7;
+                    st.pc = PC_I_END;
+                    break;
+                }
+                st.best = rl;
+                st.start_best = rl;
+                st.it = 0;
+                st.pc = (p == 0 || iters <= 0) ? PC_I_END : PC_I_ITER;
+                break;
+            case PC_I_ITER:
+                if (st.it >= (iters < 1 ? 1 : iters)) {
+                    st.pc = PC_I_END;
+                    break;
+                }
+                st.op = FOP_IJAC;
+                st.sel = 0;
+                st.pc = PC_I_AFTER_JAC;
+                return;
+            case PC_I_AFTER_JAC: {
+                if (rb) {
+                    st.pc = PC_I_END;
+                    break;
+                }
+                const int sv = ft_gauss_solve(st.jtj, st.jtr, st.lambda, p, delta, L);
+                if (sv != 0) {
+                    st.lambda *= 6.0;
+                    st.it++;
+                    st.pc = st.lambda > 1e9 ? PC_I_END : PC_I_ITER;
+                    break;
+                }
+                for (int j = 0; j < p; ++j) st.trial[j] = fmin(1e6, fmax(-1e6, st.c[j] + delta[j]));
+                st.op = FOP_ICOST;
+                st.sel = 1;
+                st.pc = PC_I_AFTER_TRIAL;
+                return;
+            }
+            case PC_I_AFTER_TRIAL:
+                st.it++;
+                if (!rb && rl < st.best) {
+                    st.best = rl;
+                    for (int j = 0; j < p; ++j) st.c[j] = st.trial[j];
+                    st.lambda = fmax(st.lambda / 8.0, 1e-12);
+                    st.improved = 1;
+                    st.pc = st.best == 0.0 ? PC_I_END : PC_I_ITER;
+                } else {
+                    st.lambda *= 6.0;
+                    st.pc = st.lambda > 1e9 ? PC_I_END : PC_I_ITER;
+                }
+                break;
+            case PC_I_END:
+                /* the reference writes constants back only when they beat the
+                   start (implicit.rs:402-405) */
+                if (!(st.best < st.start_best))
+                    for (int j = 0; j < p; ++j) st.c[j] = st.start_c[j];
+                if (st.status != 7) st.status = st.improved ? 0 : 6;
+                ft_finish(a, st, cand, p);
+                return;
+            default:
+                st.op = FOP_NONE;
+                return;
+        }
+    }
+    /* Unreachable for well-formed state; close the candidate rather than spin. */
+    st.pc = PC_END;
+    ft_finish(a, st, cand, p);
+}
+
+#define FT_CTRL_T 128
+
+/* Reduce the tile partials of each candidate that had a sweep at parity q,
+   advance its LM and queue its next sweep at parity q^1. With `init`, start
+   every candidate instead. */
+__global__ void __launch_bounds__(FT_CTRL_T) ft_control(FitArgs a, int q, int init)
+{
+    __shared__ FitState sst;
+    __shared__ double L[FT_MAX_CONST * (FT_MAX_CONST + 1)];
+    __shared__ double delta[FT_MAX_CONST];
+    __shared__ double gram[24 * 24];
+    __shared__ int s_task, s_cand, s_op;
+    __shared__ double s_loss;
+    __shared__ int s_bad, s_skip;
+    const int tid = threadIdx.x;
+    const int nq = q ^ 1;
+    int total = 0;
+    if (init) total = a.nprog;
+    else
+        for (int k = 1; k < FOP_COUNT; ++k) total += a.counts[q * FOP_COUNT + k];
+    int *work = a.work + q * FOP_COUNT + FOP_NONE;
+    for (;;) {
+        if (tid == 0) {
+            const int t = atomicAdd(work, 1);
+            s_task = t;
+            if (t < total) {
+                int cand = t, op = FOP_NONE;
+                if (!init) {
+                    int k = 1, base = 0;
+                    while (t >= base + a.counts[q * FOP_COUNT + k]) {
+                        base += a.counts[q * FOP_COUNT + k];
+                        ++k;
+                    }
+                    op = k;
+                    cand = a.lists[((size_t)q * FOP_COUNT + k) * a.nprog + (t - base)];
+                }
+                s_cand = cand;
+                s_op = op;
+            }
+        }
+        __syncthreads();
+        if (s_task >= total) break;
+        const int cand = s_cand, op = s_op;
+        const int p = a.pcount[cand];
+        {
+            const double *src = reinterpret_cast<const double *>(a.state + cand);
+            double *dst = reinterpret_cast<double *>(&sst);
+            for (int i = tid; i < (int)(sizeof(FitState) / 8); i += FT_CTRL_T) dst[i] = src[i];
+        }
+        if (init && tid < p) {
+            /* fresh state: the caller's starting constants */
+            sst.c[tid] = a.c0[(size_t)cand * a.kmax + tid];
+        }
+        __syncthreads();
+        if (init && tid == 0) sst.pc = PC_INIT;
+        const double *pt = a.part + (size_t)cand * a.ntiles * FT_PART_STRIDE;
+        if (!init && ft_op_assembles(op)) {
+            const int W = 4 * ((p + 1 + 3) / 4);
+            const int nb = W / 4;
+            const int nblk = nb * (nb + 1) / 2;
+            for (int e = tid; e < nblk * 16; e += FT_CTRL_T) {
+                double s = 0.0;
+                for (int t = 0; t < a.ntiles; ++t) s += pt[(size_t)t * FT_PART_STRIDE + e];
+                int b = e >> 4, bi = 0;
+                while (b > bi) {
+                    b -= bi + 1;
+                    ++bi;
+                }
+                gram[(4 * bi + ((e & 15) >> 2)) * W + 4 * b + (e & 3)] = s;
+            }
+            __syncthreads();
+            for (int e = tid; e < p * (p + 1) / 2 + p; e += FT_CTRL_T) {
+                if (e < p * (p + 1) / 2) {
+                    int i = 0, k = e;
+                    while (k > i) {
+                        k -= i + 1;
+                        ++i;
+                    }
+                    sst.jtj[e] = gram[i * W + k];
+                } else {
+                    const int j = e - p * (p + 1) / 2;
+                    sst.jtr[j] = gram[p * W + j];
+                }
+            }
         }
         if (tid == 0) {
-            for (int j = 0; j < p; ++j) a.outc[(size_t)cand * a.kmax + j] = f.c[j];
-            a.outsse[cand] = best;
-            a.outstatus[cand] = status;
+            double loss = 0.0;
+            int bad = 0, skip = 0;
+            if (!init) {
+                for (int t = 0; t < a.ntiles; ++t) {
+                    const double *pp = pt + (size_t)t * FT_PART_STRIDE;
+                    loss += pp[FT_PART_LOSS];
+                    bad |= pp[FT_PART_BAD] != 0.0;
+                    if (ft_op_assembles(op)) skip |= pp[FT_PART_SKIP] != 0.0;
+                }
+            }
+            s_loss = loss;
+            s_bad = bad;
+            s_skip = skip;
+        }
+        __syncthreads();
+        if (tid == 0) ft_advance(a, sst, cand, p, s_loss, s_bad, s_skip, L, delta);
+        __syncthreads();
+        {
+            const double *src = reinterpret_cast<const double *>(&sst);
+            double *dst = reinterpret_cast<double *>(a.state + cand);
+            for (int i = tid; i < (int)(sizeof(FitState) / 8); i += FT_CTRL_T) dst[i] = src[i];
+        }
+        if (tid == 0 && sst.op != FOP_NONE) {
+            const int k = atomicAdd(&a.counts[nq * FOP_COUNT + sst.op], 1);
+            a.lists[((size_t)nq * FOP_COUNT + sst.op) * a.nprog + k] = cand;
         }
         __syncthreads();
     }
+}
+
+/* Clear the queue that step s fills and the work counters it consumes. */
+__global__ void ft_step_reset(FitArgs a, int q)
+{
+    const int t = threadIdx.x;
+    if (t < FOP_COUNT) {
+        a.counts[(q ^ 1) * FOP_COUNT + t] = 0;
+        a.work[q * FOP_COUNT + t] = 0;
+    }
+}
+
+/* Close every candidate that has not finished (a bound, never reached). */
+__global__ void ft_flush(FitArgs a)
+{
+    const int cand = blockIdx.x * blockDim.x + threadIdx.x;
+    if (cand >= a.nprog) return;
+    FitState &st = a.state[cand];
+    if (st.pc == PC_DONE) return;
+    if (a.metric == FM_IMPLICIT) {
+        if (!(st.best < st.start_best))
+            for (int j = 0; j < a.pcount[cand]; ++j) st.c[j] = st.start_c[j];
+        if (st.status != 7) st.status = st.improved ? 0 : 6;
+    } else {
+        st.pc = PC_END;
+    }
+    ft_finish(a, st, cand, a.pcount[cand]);
 }
 
 /* ---- gradients and the implicit score ------------------------------ */
@@ -1225,6 +1039,7 @@ __global__ void ft_implicit_finalize(int nprog, int ntiles, const double *partia
     }
 }
 
+
 /* ---- host side -------------------------------------------------------- */
 
 namespace {
@@ -1258,26 +1073,17 @@ bool validate_records(const uint32_t *rec, int m, int p, int v)
     return parents[m - 1] == 0;
 }
 
-struct FitBatchPrep {
-    std::vector<int> node_off, valid, order[4];
-    int mmax[4] = {1, 1, 1, 1};
-    int pmax[4] = {0, 0, 0, 0};
+struct FitPrep {
+    std::vector<int> node_off, valid;
+    int mmax = 1;
+    int pmax = 0;
 };
 
-int bucket_of(int m)
-{
-    if (m <= 16) return 0;
-    if (m <= 32) return 1;
-    if (m <= 64) return 2;
-    return 3;
-}
-
 void prep_batch(const unsigned int *off, const unsigned int *prog, const int *pcount, int nprog,
-                int v, FitBatchPrep &b)
+                int v, FitPrep &b)
 {
     b.node_off.resize(nprog + 1);
     b.valid.resize(nprog);
-    std::vector<double> cost(nprog);
     for (int i = 0; i <= nprog; ++i) b.node_off[i] = (int)(off[i] / 4);
     for (int i = 0; i < nprog; ++i) {
         const int m = b.node_off[i + 1] - b.node_off[i];
@@ -1285,65 +1091,74 @@ void prep_batch(const unsigned int *off, const unsigned int *prog, const int *pc
         const bool ok = (off[i] % 4 == 0) && p >= 0 && p <= FT_MAX_CONST &&
                         validate_records(prog + off[i], m, p, v);
         b.valid[i] = ok ? 1 : 0;
-        const int bk = bucket_of(m < 1 ? 1 : m);
-        b.order[bk].push_back(i);
-        b.mmax[bk] = std::max(b.mmax[bk], std::max(m, 1));
-        b.pmax[bk] = std::max(b.pmax[bk], std::max(p, 0));
-        cost[i] = (double)m * (1.0 + 0.05 * p);
+        if (ok) {
+            b.mmax = std::max(b.mmax, m);
+            b.pmax = std::max(b.pmax, p);
+        }
     }
-    for (int k = 0; k < 4; ++k)
-        std::stable_sort(b.order[k].begin(), b.order[k].end(),
-                         [&](int x, int y) { return cost[x] > cost[y]; });
 }
 
-int fit_occupancy(size_t smem)
+int occupancy(const void *fn, int threads, size_t smem)
 {
     int blocks = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, ft_kernel<FT_THREADS>, FT_THREADS,
-                                                      smem) != cudaSuccess) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, fn, threads, smem) != cudaSuccess) {
         cudaGetLastError();
         return 1;
     }
     return blocks < 1 ? 1 : blocks;
 }
 
-/* Launches the bucketed persistent fit on the context stream. `one_by_one`
-   launches one single-block kernel per candidate (the plain arm). */
-int launch_fit(RcCtx *c, FitArgs base, const FitBatchPrep &b, int *d_order, int *d_counters,
-               int nprog, bool one_by_one)
+/* Upper bound on the sweeps one candidate can request: the first assembly,
+   per LM iteration an assembly and up to three objective sweeps (L1 Armijo
+   halvings) or one, the f64 re-baseline and four polish steps of an
+   assembly and two objective sweeps; for the implicit arm one base sweep and
+   two per iteration. */
+int max_steps(int iters, int metric)
 {
-    int obase = 0;
-    for (int k = 0; k < 4; ++k) {
-        const int nb = (int)b.order[k].size();
-        if (nb == 0) continue;
-        FitArgs a = base;
-        a.mmax = b.mmax[k];
-        a.W = 4 * ((b.pmax[k] + 1 + 3) / 4);
-        const size_t smem = ft_layout(a.mmax, a.W, FT_THREADS).total;
-        if (cudaFuncSetAttribute(ft_kernel<FT_THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem) != cudaSuccess) {
-            cudaGetLastError();
-            return -1;
+    const int it = iters < 1 ? 1 : iters;
+    if (metric == FM_IMPLICIT) return 1 + 2 * it + 1;
+    const int per = metric == FM_ABSOLUTE ? 4 : 2;
+    return 2 + per * it + 1 + 12 + 1;
+}
+
+struct SweepLaunch {
+    const void *fn;
+    size_t smem;
+    int grid;
+};
+
+template <int OPK>
+SweepLaunch sweep_launch(RcCtx *c, int mmax, int Wmax)
+{
+    SweepLaunch s;
+    s.fn = (const void *)ft_sweep<OPK, FT_THREADS>;
+    s.smem = ft_sweep_smem(OPK, mmax, Wmax, FT_THREADS);
+    if (s.smem > 48 * 1024)
+        cudaFuncSetAttribute(s.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
+    s.grid = c->sm_count * occupancy(s.fn, FT_THREADS, s.smem);
+    return s;
+}
+
+/* Enqueue the whole fit on the context stream: init, the bounded steps, the
+   flush. */
+void enqueue_fit(cudaStream_t s_, int sm_count, const FitArgs &a, int steps,
+                 const SweepLaunch *sw, int nkinds)
+{
+    const int ctrl_grid = sm_count * 8;
+    ft_step_reset<<<1, 32, 0, s_>>>(a, 1);
+    cudaMemsetAsync(a.work + 1 * FOP_COUNT, 0, sizeof(int) * FOP_COUNT, s_);
+    ft_control<<<ctrl_grid, FT_CTRL_T, 0, s_>>>(a, 1, 1);
+    for (int s = 0; s < steps; ++s) {
+        const int q = s & 1;
+        ft_step_reset<<<1, 32, 0, s_>>>(a, q);
+        for (int k = 0; k < nkinds; ++k) {
+            const SweepLaunch &L = sw[k];
+            void *args[] = {(void *)&a, (void *)&q};
+            cudaLaunchKernel(L.fn, dim3(L.grid), dim3(FT_THREADS), args, L.smem, s_);
         }
-        if (one_by_one) {
-            for (int i = 0; i < nb; ++i) {
-                a.order = d_order + obase + i;
-                a.ncand = 1;
-                a.counter = d_counters + 8 + obase + i;
-                ft_kernel<FT_THREADS><<<1, FT_THREADS, smem, c->s>>>(a);
-            }
-        } else {
-            a.order = d_order + obase;
-            a.ncand = nb;
-            a.counter = d_counters + k;
-            int grid = c->sm_count * fit_occupancy(smem);
-            if (grid > nb) grid = nb;
-            ft_kernel<FT_THREADS><<<grid, FT_THREADS, smem, c->s>>>(a);
-        }
-        obase += nb;
+        ft_control<<<ctrl_grid, FT_CTRL_T, 0, s_>>>(a, q, 0);
     }
-    (void)nprog;
-    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+    ft_flush<<<(a.nprog + 127) / 128, 128, 0, s_>>>(a);
 }
 
 float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const int *pcount,
@@ -1352,7 +1167,7 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
 {
     (void)gauge;
     if (!c || !prog || !off || !pcount || !c0 || !outc || !outsse || !outstatus) return -1.0f;
-    if (nprog <= 0 || kmax <= 0 || kmax > FT_MAX_CONST) return -1.0f;
+    if (nprog <= 0 || kmax <= 0 || kmax > FT_MAX_CONST || c->n <= 0) return -1.0f;
     if (metric == FM_LOGISTIC && !c->has_tsign) return -1.0f;
     if (metric != FM_SQUARED && metric != FM_LOG_SQUASHED && metric != FM_ABSOLUTE &&
         metric != FM_LOGISTIC && metric != FM_IMPLICIT)
@@ -1363,11 +1178,10 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     RcStats *st = &c->stats;
     double t = rc_now_ms();
     if (rc_ensure_f64(c) != 0) return -1.0f;
-    FitBatchPrep b;
+    FitPrep b;
     prep_batch(off, prog, pcount, nprog, c->v, b);
-    std::vector<int> order;
-    order.reserve(nprog);
-    for (int k = 0; k < 4; ++k) order.insert(order.end(), b.order[k].begin(), b.order[k].end());
+    const int ntiles = (c->n + FT_TILE_ROWS - 1) / FT_TILE_ROWS;
+    const int Wmax = 4 * ((b.pmax + 1 + 3) / 4);
     const size_t words = off[nprog];
     size_t cur = 0;
     const size_t o_rec = rc_take(&cur, sizeof(uint32_t) * words);
@@ -1375,13 +1189,16 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     const size_t o_p = rc_take(&cur, sizeof(int) * nprog);
     const size_t o_c0 = rc_take(&cur, sizeof(double) * (size_t)nprog * kmax);
     const size_t o_valid = rc_take(&cur, sizeof(int) * nprog);
-    const size_t o_order = rc_take(&cur, sizeof(int) * nprog);
     const size_t in_end = rc_take(&cur, 0);
     const size_t o_c = rc_take(&cur, sizeof(double) * (size_t)nprog * kmax);
     const size_t o_sse = rc_take(&cur, sizeof(double) * nprog);
     const size_t o_status = rc_take(&cur, sizeof(int) * nprog);
     const size_t io_end = rc_take(&cur, 0);
-    const size_t o_cnt = rc_take(&cur, sizeof(int) * (8 + nprog));
+    const size_t o_state = rc_take(&cur, sizeof(FitState) * nprog);
+    const size_t o_part = rc_take(&cur, sizeof(double) * (size_t)nprog * ntiles * FT_PART_STRIDE);
+    const size_t o_lists = rc_take(&cur, sizeof(int) * 2 * FOP_COUNT * (size_t)nprog);
+    const size_t o_counts = rc_take(&cur, sizeof(int) * 2 * FOP_COUNT);
+    const size_t o_work = rc_take(&cur, sizeof(int) * 2 * FOP_COUNT);
     const size_t dev_end = rc_take(&cur, 0);
     if (rc_reserve(c, dev_end, io_end) != 0) return -1.0f;
     st->alloc_ms += rc_now_ms() - t;
@@ -1392,11 +1209,7 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     memcpy(host + o_p, pcount, sizeof(int) * nprog);
     memcpy(host + o_c0, c0, sizeof(double) * (size_t)nprog * kmax);
     memcpy(host + o_valid, b.valid.data(), sizeof(int) * nprog);
-    memcpy(host + o_order, order.data(), sizeof(int) * nprog);
-    /* outputs start as the inputs so untouched slots echo c0 */
     memcpy(host + o_c, c0, sizeof(double) * (size_t)nprog * kmax);
-    cudaMemcpyAsync(dev, host, io_end, cudaMemcpyHostToDevice, c->s);
-    cudaMemsetAsync(dev + o_cnt, 0, sizeof(int) * (8 + nprog), c->s);
     st->h2d_ms += rc_now_ms() - t;
     st->h2d_bytes += io_end;
 
@@ -1421,16 +1234,88 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     a.iters = iters;
     a.metric = metric;
     a.flags = flags;
+    a.ntiles = ntiles;
+    a.mmax = b.mmax;
+    a.Wmax = Wmax;
+    a.nprog = nprog;
+    a.state = reinterpret_cast<FitState *>(dev + o_state);
+    a.part = reinterpret_cast<double *>(dev + o_part);
+    a.lists = reinterpret_cast<int *>(dev + o_lists);
+    a.counts = reinterpret_cast<int *>(dev + o_counts);
+    a.work = reinterpret_cast<int *>(dev + o_work);
     a.outc = reinterpret_cast<double *>(dev + o_c);
     a.outsse = reinterpret_cast<double *>(dev + o_sse);
     a.outstatus = reinterpret_cast<int *>(dev + o_status);
+
+    SweepLaunch sw[4];
+    int nk = 0;
+    if (metric == FM_IMPLICIT) {
+        sw[nk] = sweep_launch<FOP_IJAC>(c, b.mmax, Wmax); ++nk;
+        sw[nk] = sweep_launch<FOP_ICOST>(c, b.mmax, Wmax); ++nk;
+    } else {
+        sw[nk] = sweep_launch<FOP_ASM32>(c, b.mmax, Wmax); ++nk;
+        sw[nk] = sweep_launch<FOP_LOSS32>(c, b.mmax, Wmax); ++nk;
+        if (!(flags & 1)) {
+            sw[nk] = sweep_launch<FOP_ASM64>(c, b.mmax, Wmax); ++nk;
+            sw[nk] = sweep_launch<FOP_LOSS64>(c, b.mmax, Wmax); ++nk;
+        }
+    }
+    const int steps = max_steps(iters, metric);
+
     t = rc_now_ms();
     cudaEventRecord(c->t0, c->s);
-    const int rc = launch_fit(c, a, b, reinterpret_cast<int *>(dev + o_order),
-                              reinterpret_cast<int *>(dev + o_cnt), nprog, mode == 1);
+    cudaMemcpyAsync(dev, host, io_end, cudaMemcpyHostToDevice, c->s);
+    bool ok = true;
+    if (mode == 1) {
+        /* plain arm: the same step kernels, one candidate per launch sequence */
+        for (int i = 0; i < nprog && ok; ++i) {
+            FitArgs one = a;
+            one.rec = a.rec;
+            one.nprog = 1;
+            one.node_off = a.node_off + i;
+            one.pcount = a.pcount + i;
+            one.c0 = a.c0 + (size_t)i * kmax;
+            one.valid = a.valid + i;
+            one.state = a.state + i;
+            one.part = a.part + (size_t)i * ntiles * FT_PART_STRIDE;
+            one.outc = a.outc + (size_t)i * kmax;
+            one.outsse = a.outsse + i;
+            one.outstatus = a.outstatus + i;
+            enqueue_fit(c->s, c->sm_count, one, steps, sw, nk);
+            ok = cudaGetLastError() == cudaSuccess;
+        }
+    } else {
+        char key[256];
+        snprintf(key, sizeof(key), "%p|%d|%d|%d|%d|%d|%d|%d|%d|%d|%zu", (void *)dev, nprog, kmax,
+                 ntiles, b.mmax, Wmax, iters, metric, flags, steps, io_end);
+        if (!c->fit_graph || c->fit_graph_key != key) {
+            if (c->fit_graph) {
+                cudaGraphExecDestroy(c->fit_graph);
+                c->fit_graph = nullptr;
+            }
+            cudaGraph_t g = nullptr;
+            cudaStream_t cap = nullptr;
+            cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
+            ok = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+            if (ok) {
+                enqueue_fit(cap, c->sm_count, a, steps, sw, nk);
+                ok = cudaStreamEndCapture(cap, &g) == cudaSuccess && g;
+            }
+            if (ok) ok = cudaGraphInstantiate(&c->fit_graph, g, 0) == cudaSuccess;
+            if (g) cudaGraphDestroy(g);
+            cudaStreamDestroy(cap);
+            if (!ok) {
+                cudaGetLastError();
+                c->fit_graph = nullptr;
+            } else {
+                c->fit_graph_key = key;
+            }
+        }
+        if (ok) ok = cudaGraphLaunch(c->fit_graph, c->s) == cudaSuccess;
+    }
     cudaEventRecord(c->t1, c->s);
     st->launch_ms += rc_now_ms() - t;
-    if (rc != 0) {
+    if (!ok || cudaGetLastError() != cudaSuccess) {
         cudaStreamSynchronize(c->s);
         cudaGetLastError();
         return -1.0f;
@@ -1489,7 +1374,7 @@ int rc_fit_kernel_info(int kmax, int *threads, int *smem_bytes, int *max_constan
     if (kmax > FT_MAX_CONST || kmax < 0) return -1;
     const int W = 4 * ((kmax + 1 + 3) / 4);
     *threads = FT_THREADS;
-    *smem_bytes = (int)ft_layout(FT_MAX_NODES_ABI, W, FT_THREADS).total;
+    *smem_bytes = (int)ft_sweep_smem(FOP_ASM32, FT_MAX_NODES_ABI, W, FT_THREADS);
     *max_constants = FT_MAX_CONST;
     return 0;
 }
@@ -1502,10 +1387,9 @@ int rc_grad_batch(void *ctx, const unsigned int *prog, const unsigned int *off, 
     if (!rc || !prog || !off || !pcount || !c || !value || !out) return -1;
     if (nprog <= 0 || kmax <= 0 || kmax > FT_MAX_CONST || (want != 1 && want != 2)) return -1;
     if (row0 < 0 || nrows <= 0 || row0 + nrows > rc->n) return -1;
-    FitBatchPrep b;
+    FitPrep b;
     prep_batch(off, prog, pcount, nprog, rc->v, b);
-    int mmax = 1;
-    for (int k = 0; k < 4; ++k) mmax = std::max(mmax, b.mmax[k]);
+    const int mmax = b.mmax;
     const int width = want == 1 ? kmax : rc->v;
     const size_t words = off[nprog];
     size_t cur = 0;
@@ -1568,10 +1452,9 @@ float rc_implicit_score_batch(void *ctx, const unsigned int *prog, const unsigne
     if (!rc || !prog || !off || !pcount || !c || !out || !status) return -1.0f;
     if (nprog <= 0 || kmax <= 0 || kmax > FT_MAX_CONST || rc->n <= 0) return -1.0f;
     RcStats *st = &rc->stats;
-    FitBatchPrep b;
+    FitPrep b;
     prep_batch(off, prog, pcount, nprog, rc->v, b);
-    int mmax = 1;
-    for (int k = 0; k < 4; ++k) mmax = std::max(mmax, b.mmax[k]);
+    const int mmax = b.mmax;
     const int T = 128;
     const int rows_per_tile = 16384;
     const int ntiles = (rc->n + rows_per_tile - 1) / rows_per_tile;

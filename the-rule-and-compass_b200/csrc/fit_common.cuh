@@ -1,0 +1,462 @@
+#pragma once
+/*
+ * Device building blocks of the batched fit: per-row forward and reverse
+ * sweeps over fit records (f32 and f64), the per-row objective pieces, the
+ * block reductions, the 4x4 register-blocked SYRK of the augmented Gram, the
+ * damped solves, and the implicit-metric residual.
+ *
+ * Semantics follow the reference's batched fit (my-version/src/cuda/eval.cu:
+ * 1106-2606) and the CPU fitter it stands in for (my-version/src/fit.rs:
+ * 1453-1827, :2534-2624, :3092-3170; my-version/src/implicit.rs:68-409).
+ */
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "rc_internal.h"
+#include "rc_ops.cuh"
+
+#define FT_MAX_CONST 20
+#define FT_MAX_NODES_ABI 96   /* the reference's plan cap (fit.rs:854) */
+#define FT_MAX_NODES 255      /* what this kernel accepts */
+#define FT_THREADS 128
+#define FT_L1_EPS 1e-6
+#define FT_LN_DET_FLOOR (-27.631021115928547)
+
+enum {
+    FM_SQUARED = 0, FM_LOG_SQUASHED = 1, FM_CORRELATION = 2, FM_CORRELATION_SIGNED = 3,
+    FM_ABSOLUTE = 4, FM_LOGISTIC = 5, FM_IMPLICIT = 6
+};
+
+
+/* ---- per-row sweeps ---------------------------------------------------- */
+
+/* f32 forward sweep of one row; `tp` is this thread's tape column (stride T). */
+template <int T>
+__device__ __forceinline__ float ft_fwd_f(const uint4 *rec, int m, const float *cols, int npad,
+                                          int row, const float *cf, float *tp)
+{
+    float val = 0.0f;
+    for (int i = 0; i < m; ++i) {
+        const uint4 r = rec[i];
+        if (r.x == OP_CONST) val = cf[r.w];
+        else if (r.x == OP_VAR) val = __ldg(cols + (size_t)r.w * npad + row);
+        else {
+            const float a = tp[r.y * T];
+            const float b = ft_op_binary(r.x) ? tp[r.z * T] : 0.0f;
+            val = ft_value_f(r.x, a, b);
+        }
+        tp[i * T] = val;
+    }
+    return val;
+}
+
+/* f64 forward sweep; `tp` has stride TS. */
+template <int TS>
+__device__ __forceinline__ double ft_fwd_d(const uint4 *rec, int m, const double *cols, int npad,
+                                           int row, const double *c, double *tp)
+{
+    double val = 0.0;
+    for (int i = 0; i < m; ++i) {
+        const uint4 r = rec[i];
+        if (r.x == OP_CONST) val = c[r.w];
+        else if (r.x == OP_VAR) val = __ldg(cols + (size_t)r.w * npad + row);
+        else {
+            const double a = tp[r.y * TS];
+            const double b = ft_op_binary(r.x) ? tp[r.z * TS] : 0.0;
+            val = ft_value_d(r.x, a, b);
+        }
+        tp[i * TS] = val;
+    }
+    return val;
+}
+
+/* f64 forward with the row's inputs given explicitly (implicit metric). */
+template <int TS>
+__device__ __forceinline__ double ft_fwd_d_x(const uint4 *rec, int m, const double *x,
+                                             const double *c, double *tp)
+{
+    double val = 0.0;
+    for (int i = 0; i < m; ++i) {
+        const uint4 r = rec[i];
+        if (r.x == OP_CONST) val = c[r.w];
+        else if (r.x == OP_VAR) val = x[r.w];
+        else {
+            const double a = tp[r.y * TS];
+            const double b = ft_op_binary(r.x) ? tp[r.z * TS] : 0.0;
+            val = ft_value_d(r.x, a, b);
+        }
+        tp[i * TS] = val;
+    }
+    return val;
+}
+
+/* Reverse sweep in place (f32). Adjoints of constants are written to
+   g[slot * gs] (f64), of inputs accumulated into ig[col * is] when ig != 0.
+   Every node of a fit-record tree has one parent, so a child's tape entry
+   switches from value to adjoint exactly when its parent is processed.
+   Mirrors eval.cu:1236-1317 (an adjoint of zero passes nothing). */
+template <int T>
+__device__ __forceinline__ void ft_bwd_f(const uint4 *rec, int m, float *tp, double *g, int gs,
+                                         float *ig, int is)
+{
+    tp[(m - 1) * T] = 1.0f;
+    for (int i = m - 1; i >= 0; --i) {
+        const uint4 r = rec[i];
+        const float a = tp[i * T];
+        if (r.x == OP_CONST) {
+            if (g) g[r.w * gs] += (double)a;
+            continue;
+        }
+        if (r.x == OP_VAR) {
+            if (ig) ig[r.w * is] += a;
+            continue;
+        }
+        const bool bin = ft_op_binary(r.x);
+        const float x = tp[r.y * T];
+        const float yv = bin ? tp[r.z * T] : 0.0f;
+        float c0 = 0.0f, c1 = 0.0f;
+        if (a != 0.0f && !(r.x == OP_POW && !(x > 0.0f))) {
+            float d0, d1;
+            ft_partials_f(r.x, x, yv, d0, d1);
+            c0 = a * d0;
+            c1 = a * d1;
+        }
+        tp[r.y * T] = c0;
+        if (bin) tp[r.z * T] = c1;
+    }
+}
+
+template <int TS>
+__device__ __forceinline__ void ft_bwd_d(const uint4 *rec, int m, double *tp, double *g, int gs,
+                                         double *ig, int is)
+{
+    tp[(m - 1) * TS] = 1.0;
+    for (int i = m - 1; i >= 0; --i) {
+        const uint4 r = rec[i];
+        const double a = tp[i * TS];
+        if (r.x == OP_CONST) {
+            if (g) g[r.w * gs] += a;
+            continue;
+        }
+        if (r.x == OP_VAR) {
+            if (ig) ig[r.w * is] += a;
+            continue;
+        }
+        const bool bin = ft_op_binary(r.x);
+        const double x = tp[r.y * TS];
+        const double yv = bin ? tp[r.z * TS] : 0.0;
+        double c0 = 0.0, c1 = 0.0;
+        if (a != 0.0 && !(r.x == OP_POW && !(x > 0.0))) {
+            double d0, d1;
+            ft_partials_d(r.x, x, yv, d0, d1);
+            c0 = a * d0;
+            c1 = a * d1;
+        }
+        tp[r.y * TS] = c0;
+        if (bin) tp[r.z * TS] = c1;
+    }
+}
+
+/* ---- objective pieces (eval.cu:638-693, 1492-1855) ------------------- */
+
+__device__ __forceinline__ float ft_row_loss_f(float r, int metric)
+{
+    if (metric == FM_LOG_SQUASHED) {
+        const float rr = r * r;
+        return isfinite(rr) ? log1pf(rr) : 2.0f * logf(fabsf(r));
+    }
+    if (metric == FM_ABSOLUTE) return fabsf(r);
+    return r * r;
+}
+
+__device__ __forceinline__ double ft_row_weight(double base, double r, int metric)
+{
+    if (metric == FM_LOG_SQUASHED) return base * 2.0 / (1.0 + r * r);
+    if (metric == FM_ABSOLUTE) return base / fmax(fabs(r), FT_L1_EPS);
+    return base;
+}
+
+__device__ __forceinline__ double ft_logistic_q(double u)
+{
+    double q;
+    if (u >= 0.0) q = 1.0 / (1.0 + exp(-u));
+    else {
+        const double e = exp(u);
+        q = e / (1.0 + e);
+    }
+    return fmin(1.0 - 1e-9, fmax(1e-9, q));
+}
+
+__device__ __forceinline__ double ft_softplus_neg(double u)
+{
+    const double a = fabs(u);
+    return (u < 0.0 ? -u : 0.0) + log1p(exp(-a));
+}
+
+/* ---- block reductions -------------------------------------------------- */
+
+template <int T>
+__device__ __forceinline__ double ft_block_sum(double v, double *red)
+{
+    const int tid = threadIdx.x;
+    red[tid] = v;
+    __syncthreads();
+    for (int st = T / 2; st > 0; st >>= 1) {
+        if (tid < st) red[tid] += red[tid + st];
+        __syncthreads();
+    }
+    const double total = red[0];
+    __syncthreads();
+    return total;
+}
+
+/* SYRK block assignment: the (W/4)x(W/4) block lower triangle of the
+   augmented Gram [J | r]^T [J | r] is split into nblk 4x4 blocks; thread t
+   owns block t % nblk and rows r == t / nblk (mod RG). */
+struct Syrk {
+    int nblk, RG, blk, rg, bi, bj;
+};
+
+template <int T>
+__device__ __forceinline__ Syrk ft_syrk_setup(int W)
+{
+    Syrk s;
+    const int nb = W / 4;
+    s.nblk = nb * (nb + 1) / 2;
+    s.RG = T / s.nblk;
+    if (s.RG < 1) s.RG = 1;
+    s.blk = threadIdx.x % s.nblk;
+    s.rg = threadIdx.x / s.nblk;
+    int b = s.blk, i = 0;
+    while (b > i) {
+        b -= i + 1;
+        ++i;
+    }
+    s.bi = i;
+    s.bj = b;
+    return s;
+}
+
+/* Accumulate rows [0, R) of the row buffer into this thread's block. */
+__device__ __forceinline__ void ft_syrk_chunk(const Syrk &s, const double *rows, int W, int R,
+                                              double acc[16])
+{
+    if (s.rg >= s.RG) return;
+    for (int r = s.rg; r < R; r += s.RG) {
+        const double *row = rows + (size_t)r * W;
+        const double2 a01 = *reinterpret_cast<const double2 *>(row + 4 * s.bi);
+        const double2 a23 = *reinterpret_cast<const double2 *>(row + 4 * s.bi + 2);
+        const double2 b01 = *reinterpret_cast<const double2 *>(row + 4 * s.bj);
+        const double2 b23 = *reinterpret_cast<const double2 *>(row + 4 * s.bj + 2);
+        const double av[4] = {a01.x, a01.y, a23.x, a23.y};
+        const double bv[4] = {b01.x, b01.y, b23.x, b23.y};
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i * 4 + j] = fma(av[i], bv[j], acc[i * 4 + j]);
+    }
+}
+
+/* Reduce the per-group partial blocks in ascending group order and unpack the
+   packed lower triangle J^T J (p(p+1)/2) and J^T r (p). */
+template <int T>
+__device__ __forceinline__ void ft_syrk_finish(const Syrk &s, double acc[16], double *part,
+                                               double *gram, int W, int p, double *jtj,
+                                               double *jtr)
+{
+    const int tid = threadIdx.x;
+    if (s.rg < s.RG) {
+#pragma unroll
+        for (int e = 0; e < 16; ++e) part[(s.rg * s.nblk + s.blk) * 16 + e] = acc[e];
+    }
+    __syncthreads();
+    for (int q = tid; q < s.nblk * 16; q += T) {
+        const int blk = q / 16, e = q % 16;
+        double sum = 0.0;
+        for (int g = 0; g < s.RG; ++g) sum += part[(g * s.nblk + blk) * 16 + e];
+        int b = blk, bi = 0;
+        while (b > bi) {
+            b -= bi + 1;
+            ++bi;
+        }
+        const int i = 4 * bi + e / 4, j = 4 * b + e % 4;
+        gram[i * W + j] = sum;
+    }
+    __syncthreads();
+    for (int q = tid; q < p * (p + 1) / 2 + p; q += T) {
+        if (q < p * (p + 1) / 2) {
+            int i = 0, k = q;
+            while (k > i) {
+                k -= i + 1;
+                ++i;
+            }
+            jtj[q] = gram[i * W + k];
+        } else {
+            const int j = q - p * (p + 1) / 2;
+            jtr[j] = gram[p * W + j];
+        }
+    }
+    __syncthreads();
+}
+
+/* ---- the damped solve (eval.cu:1873-1949 `ft_solve`) ----------------- */
+
+__device__ int ft_solve(const double *jtj, const double *jtr, double lambda, int p, double *delta,
+                        double *L)
+{
+    double dscale[FT_MAX_CONST];
+    for (int i = 0; i < p; ++i) {
+        const double aii = jtj[i * (i + 1) / 2 + i];
+        if (!(aii > 0.0) || !isfinite(aii)) return 1;
+        dscale[i] = sqrt(aii);
+    }
+    int rank_deficient = 0;
+    double sum_ln_L = 0.0;
+    int ok = 1;
+    for (int i = 0; i < p && ok; ++i) {
+        for (int j = 0; j <= i; ++j) {
+            double s = jtj[i * (i + 1) / 2 + j] / (dscale[i] * dscale[j]);
+            if (!isfinite(s)) return 1;
+            for (int k = 0; k < j; ++k) s -= L[i * p + k] * L[j * p + k];
+            if (i == j) {
+                if (!(s > 0.0) || !isfinite(s)) {
+                    ok = 0;
+                    break;
+                }
+                L[i * p + i] = sqrt(s);
+                sum_ln_L += 0.5 * log(s);
+            } else {
+                L[i * p + j] = s / L[j * p + j];
+            }
+        }
+    }
+    if (!ok) rank_deficient = 1;
+    else {
+        const double ln_det = 2.0 * sum_ln_L;
+        if (!isfinite(ln_det) || ln_det < FT_LN_DET_FLOOR) rank_deficient = 1;
+    }
+    for (int i = 0; i < p; ++i) {
+        for (int j = 0; j <= i; ++j) {
+            double s = jtj[i * (i + 1) / 2 + j] / (dscale[i] * dscale[j]);
+            if (i == j) s = s * (1.0 + lambda) + 1e-12;
+            for (int k = 0; k < j; ++k) s -= L[i * p + k] * L[j * p + k];
+            if (i == j) {
+                if (!(s > 1e-18) || !isfinite(s)) return 1;
+                L[i * p + i] = sqrt(s);
+            } else {
+                L[i * p + j] = s / L[j * p + j];
+            }
+        }
+    }
+    double rhs[FT_MAX_CONST];
+    for (int i = 0; i < p; ++i) rhs[i] = -jtr[i] / dscale[i];
+    for (int i = 0; i < p; ++i) {
+        double s = rhs[i];
+        for (int k = 0; k < i; ++k) s -= L[i * p + k] * rhs[k];
+        rhs[i] = s / L[i * p + i];
+    }
+    for (int i = p - 1; i >= 0; --i) {
+        double s = rhs[i];
+        for (int k = i + 1; k < p; ++k) s -= L[k * p + i] * delta[k];
+        delta[i] = s / L[i * p + i];
+    }
+    for (int i = 0; i < p; ++i) delta[i] /= dscale[i];
+    return rank_deficient ? 4 : 0;
+}
+
+/* Gaussian elimination with partial pivoting on (A + lambda diag A + 1e-12 I)
+   (implicit.rs:215-253). `M` is p x (p+1) scratch. Returns 0 or 1 (singular). */
+__device__ int ft_gauss_solve(const double *jtj, const double *jtr, double lambda, int p,
+                              double *delta, double *M)
+{
+    const int w = p + 1;
+    for (int i = 0; i < p; ++i) {
+        for (int j = 0; j < p; ++j) {
+            const int a = i > j ? i : j, b = i > j ? j : i;
+            M[i * w + j] = jtj[a * (a + 1) / 2 + b];
+        }
+        M[i * w + i] = M[i * w + i] * (1.0 + lambda) + 1e-12;
+        M[i * w + p] = -jtr[i];
+    }
+    for (int col = 0; col < p; ++col) {
+        int piv = col;
+        for (int r = col + 1; r < p; ++r)
+            if (fabs(M[r * w + col]) > fabs(M[piv * w + col])) piv = r;
+        if (fabs(M[piv * w + col]) < 1e-300) return 1;
+        if (piv != col)
+            for (int c = 0; c <= p; ++c) {
+                const double t = M[col * w + c];
+                M[col * w + c] = M[piv * w + c];
+                M[piv * w + c] = t;
+            }
+        for (int r = col + 1; r < p; ++r) {
+            const double f = M[r * w + col] / M[col * w + col];
+            if (f != 0.0)
+                for (int c = col; c <= p; ++c) M[r * w + c] -= f * M[col * w + c];
+        }
+    }
+    for (int i = p - 1; i >= 0; --i) {
+        double s = M[i * w + p];
+        for (int j = i + 1; j < p; ++j) s -= M[i * w + j] * delta[j];
+        delta[i] = s / M[i * w + i];
+    }
+    return 0;
+}
+
+/* ---- the implicit metric (implicit.rs:68-409) ---------------------------
+ * Per row: d = f / ||grad_x f|| (f64 forward + input adjoint); a row with a
+ * non-finite value or gradient, or a zero gradient norm, makes the whole
+ * evaluation undefined. The LM's Jacobian is central differences of d with
+ * h = 1e-6 (1 + |c_j|), exactly as the reference CPU arm. */
+
+#define FT_IMPLICIT_MAXV 16
+
+template <int TS>
+__device__ __forceinline__ bool ft_implicit_d(const uint4 *rec, int m, const double *x, int v,
+                                              const double *c, double *tp, double &d)
+{
+    const double fv = ft_fwd_d_x<TS>(rec, m, x, c, tp);
+    if (!isfinite(fv)) return false;
+    double ig[FT_IMPLICIT_MAXV];
+    for (int k = 0; k < FT_IMPLICIT_MAXV; ++k) ig[k] = 0.0;
+    /* input adjoint accumulated in registers: columns are < FT_IMPLICIT_MAXV */
+    tp[(m - 1) * TS] = 1.0;
+    for (int i = m - 1; i >= 0; --i) {
+        const uint4 r = rec[i];
+        const double a = tp[i * TS];
+        if (r.x == OP_CONST) continue;
+        if (r.x == OP_VAR) {
+#pragma unroll
+            for (int k = 0; k < FT_IMPLICIT_MAXV; ++k)
+                if ((int)r.w == k) ig[k] += a;
+            continue;
+        }
+        const bool bin = ft_op_binary(r.x);
+        const double xx = tp[r.y * TS];
+        const double yy = bin ? tp[r.z * TS] : 0.0;
+        double c0 = 0.0, c1 = 0.0;
+        if (a != 0.0 && !(r.x == OP_POW && !(xx > 0.0))) {
+            double d0, d1;
+            ft_partials_d(r.x, xx, yy, d0, d1);
+            c0 = a * d0;
+            c1 = a * d1;
+        }
+        tp[r.y * TS] = c0;
+        if (bin) tp[r.z * TS] = c1;
+    }
+    double nsq = 0.0;
+    for (int k = 0; k < FT_IMPLICIT_MAXV; ++k) {
+        if (k >= v) break;
+        if (!isfinite(ig[k])) return false;
+        nsq += ig[k] * ig[k];
+    }
+    const double norm = sqrt(nsq);
+    if (!(isfinite(norm) && norm > 0.0)) return false;
+    d = fv / norm;
+    return isfinite(d);
+}
+
+

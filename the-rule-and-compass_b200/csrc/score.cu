@@ -363,7 +363,8 @@ float rc_score_run(RcCtx *c, const uint32_t *words, const uint32_t *off, int wid
             obase += nb;
         }
         rc_score_finalize<<<(nprog + 127) / 128, 128, 0, c->s>>>(
-            nprog, d_ctiles, a.part, ntiles, a.bad, c->n, kmode, c->syy, d_out, d_status,
+            nprog, d_ctiles, a.part, ntiles, a.bad, c->n, (corr && pass == 1) ? mode : kmode,
+            c->syy, d_out, d_status,
             reinterpret_cast<float *>(dev + o_f32), reinterpret_cast<double *>(dev + o_pbar),
             reinterpret_cast<double *>(dev + o_pbarerr), d_nflag,
             track ? reinterpret_cast<int *>(dev + o_flagged) : nullptr);
@@ -406,7 +407,8 @@ float rc_score_run(RcCtx *c, const uint32_t *words, const uint32_t *off, int wid
             l.mode = kmode;
             rc_score64_kernel<LANE_T><<<grid, LANE_T, smem, c->s>>>(l);
             rc_score64_finalize<<<(nprog + 127) / 128, 128, 0, c->s>>>(
-                l.flagged, d_nflag, ntiles, l.part, nprog, ntiles, l.bad, c->n, kmode, c->syy,
+                l.flagged, d_nflag, ntiles, l.part, nprog, ntiles, l.bad, c->n,
+                (corr && pass == 1) ? mode : kmode, c->syy,
                 d_out, d_status, reinterpret_cast<double *>(dev + o_pbar64));
         }
     }
