@@ -40,6 +40,7 @@
 #include <vector>
 
 #include "fit_common.cuh"
+#include "fit_interp.cuh"
 
 #define FT_TILE_ROWS 4096
 #define FT_NBLK_MAX 21                     /* 4x4 blocks of a 24-wide augmented Gram */
@@ -89,6 +90,11 @@ struct FitArgs {
     int kmax;
     const double *c0;
     const int *valid;
+    const FIns *fins;      /* stack-machine translation of the records */
+    const int *fins_off;   /* [P+1] */
+    int fslots;            /* spill slots needed by the batch */
+    int ftape;             /* partial-tape slots needed by the batch */
+    int fmaxins;
     int iters, metric, flags;
     int ntiles;
     int mmax;
@@ -457,6 +463,198 @@ __global__ void __launch_bounds__(T) ft_sweep(FitArgs a, int q)
         else if (OPK == FOP_LOSS64) ft_tile_loss64<T>(a, rec, m, cd, tape64, red, r0, r1, pt);
         else if (OPK == FOP_IJAC) ft_tile_implicit<T, true>(a, rec, m, p, cd, tape64, rows, red, r0, r1, pt);
         else ft_tile_implicit<T, false>(a, rec, m, p, cd, tape64, rows, red, r0, r1, pt);
+        __syncthreads();
+    }
+}
+
+/* ---- four-rows-per-thread f32 sweeps -------------------------------- */
+
+/* SYRK over f32 Jacobian rows of stride Wp (values are f32-rounded, so f64
+   products of the widened values are exact). The lanes of a warp own
+   different blocks of the same row, so each scalar load touches one row:
+   one wavefront, broadcast where blocks share columns. */
+__device__ __forceinline__ void ft_syrk_chunk_f32(const Syrk &s, const float *rows, int Wp, int R,
+                                                  double acc[16])
+{
+    if (s.rg >= s.RG) return;
+    for (int r = s.rg; r < R; r += s.RG) {
+        const float *row = rows + (size_t)r * Wp;
+        double av[4], bv[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            av[c] = row[4 * s.bi + c];
+            bv[c] = row[4 * s.bj + c];
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i * 4 + j] = fma(av[i], bv[j], acc[i * 4 + j]);
+    }
+}
+
+/* Jacobian rows of the four-row sweep: 4T rows of Wmax + 1 floats (an odd
+   stride: thread t owns rows t, t+T, t+2T, t+3T, so its accesses to one
+   column fall in distinct banks across the warp). */
+__host__ __device__ inline size_t ft_sweep4_rows_bytes(int Wmax, int T)
+{
+    const size_t rows = sizeof(float) * 4 * (size_t)T * (Wmax + 1);
+    const size_t part = sizeof(double) * (size_t)T * 16;
+    return rows > part ? rows : part;
+}
+
+/* Shared memory of a four-row sweep: instructions, f32 constants, spill
+   slots, the partial tape and the Jacobian rows (assembly only), a
+   reduction buffer. */
+__host__ __device__ inline size_t ft_sweep4_smem(int opk, int maxins, int slots, int tape, int Wmax,
+                                                 int T)
+{
+    size_t s = 8 * (size_t)((maxins + 1) & ~1) + 128 + 16 * (size_t)(slots > 0 ? slots : 1) * T;
+    if (opk == FOP_ASM32) s += 16 * (size_t)(tape > 0 ? tape : 1) * T + ft_sweep4_rows_bytes(Wmax, T);
+    return s + 8 * (size_t)T;
+}
+
+template <int T>
+__device__ void ft_tile_asm32x4(const FitArgs &a, const FIns *ins, int nins, int p,
+                                const float *cf, float4 *stk, float4 *tape, float *rows,
+                                double *red, int r0, int r1, double *pt)
+{
+    const int tid = threadIdx.x;
+    const int W = 4 * ((p + 1 + 3) / 4);
+    const Syrk sy = ft_syrk_setup<T>(W);
+    double acc[16];
+#pragma unroll
+    for (int e = 0; e < 16; ++e) acc[e] = 0.0;
+    double loss = 0.0;
+    int bad = 0;
+    const int Wp = W + 1;
+    float *g = rows + (size_t)tid * Wp;
+    for (int base = r0; base < r1; base += 4 * T) {
+        const int row = base + 4 * tid;
+        for (int i = 0; i < 4; ++i)
+            for (int j = 0; j < W; ++j) g[(size_t)i * T * Wp + j] = 0.0f;
+        const float4 pv = fi_forward<T, true>(ins, cf, a.cols, a.npad, row, stk, tape, tid);
+        fi_reverse<T>(ins, nins, stk, tape, g, T * Wp, tid);
+        const float pr[4] = {pv.x, pv.y, pv.z, pv.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            float *gi = g + (size_t)i * T * Wp;
+            const int rr = row + i;
+            const double wr = (rr < r1 && a.w) ? a.w[rr] : 1.0;
+            if (!(rr < r1 && wr > 0.0)) {
+                for (int j = 0; j < W; ++j) gi[j] = 0.0f;
+                continue;
+            }
+            const float pred = pr[i];
+            const float r = pred - a.y[rr];
+            bool ok = isfinite(pred) && fabsf(pred) <= 1e30f && isfinite(r);
+            double sw, resp = (double)r, rowloss;
+            if (a.metric == FM_LOGISTIC) {
+                const double tt = a.tsign ? (double)a.tsign[rr] : 0.0;
+                const double u = tt * (double)pred;
+                if (!a.tsign || !isfinite(tt)) ok = false;
+                const double qq = ft_logistic_q(u);
+                sw = wr * qq * (1.0 - qq);
+                resp = -tt / qq;
+                rowloss = wr * ft_softplus_neg(u);
+            } else {
+                sw = ft_row_weight(wr, (double)r, a.metric);
+                rowloss = wr * (double)ft_row_loss_f(r, a.metric);
+            }
+            const float s = sqrtf((float)sw);
+            for (int j = 0; j < p; ++j)
+                if (!isfinite(gi[j])) ok = false;
+            for (int j = 0; j < p; ++j) gi[j] = ok ? s * gi[j] : 0.0f;
+            gi[p] = ok ? (float)(s * resp) : 0.0f;
+            for (int j = p + 1; j < W; ++j) gi[j] = 0.0f;
+            if (ok) loss += rowloss;
+            else bad = 1;
+        }
+        __syncthreads();
+        ft_syrk_chunk_f32(sy, rows, Wp, 4 * T, acc);
+        __syncthreads();
+    }
+    bad = __syncthreads_or(bad);
+    loss = ft_block_sum<T>(loss, red);
+    ft_tile_gram_out<T>(sy, acc, reinterpret_cast<double *>(rows), pt);
+    if (threadIdx.x == 0) {
+        pt[FT_PART_LOSS] = loss;
+        pt[FT_PART_BAD] = bad ? 1.0 : 0.0;
+        pt[FT_PART_SKIP] = 0.0;
+    }
+}
+
+template <int T>
+__device__ void ft_tile_loss32x4(const FitArgs &a, const FIns *ins, const float *cf, float4 *stk,
+                                 double *red, int r0, int r1, double *pt)
+{
+    const int tid = threadIdx.x;
+    double local = 0.0;
+    for (int row = r0 + 4 * tid; row < r1; row += 4 * T) {
+        const float4 pv = fi_forward<T, false>(ins, cf, a.cols, a.npad, row, stk, nullptr, tid);
+        const float pr[4] = {pv.x, pv.y, pv.z, pv.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int rr = row + i;
+            if (rr >= r1) continue;
+            const double wr = a.w ? a.w[rr] : 1.0;
+            if (wr <= 0.0) continue;
+            const float pred = pr[i];
+            const float r = pred - a.y[rr];
+            if (!isfinite(pred) || fabsf(pred) > 1e30f || !isfinite(r)) local += 1e30;
+            else if (a.metric == FM_LOGISTIC) {
+                const double tt = a.tsign ? (double)a.tsign[rr] : 0.0;
+                local += isfinite(tt) ? wr * ft_softplus_neg(tt * (double)pred) : 1e30;
+            } else if (a.metric == FM_SQUARED) local += wr * (double)r * (double)r;
+            else local += wr * (double)ft_row_loss_f(r, a.metric);
+        }
+    }
+    const double total = ft_block_sum<T>(local, red);
+    if (tid == 0) {
+        pt[FT_PART_LOSS] = total;
+        pt[FT_PART_BAD] = 0.0;
+    }
+}
+
+/* The f32 assembly / objective sweeps over the four-row interpreter. */
+template <int OPK, int T>
+__global__ void __launch_bounds__(T) ft_sweep4(FitArgs a, int q)
+{
+    extern __shared__ __align__(16) unsigned char sm[];
+    FIns *ins = reinterpret_cast<FIns *>(sm);
+    float *cf = reinterpret_cast<float *>(sm + 8 * (size_t)((a.fmaxins + 1) & ~1));
+    float4 *stk = reinterpret_cast<float4 *>(reinterpret_cast<unsigned char *>(cf) + 128);
+    float4 *tape = stk + (size_t)(a.fslots > 0 ? a.fslots : 1) * T;
+    float *rows = reinterpret_cast<float *>(tape + (OPK == FOP_ASM32 ? (size_t)(a.ftape > 0 ? a.ftape : 1) * T : 0));
+    double *red = reinterpret_cast<double *>(
+        reinterpret_cast<unsigned char *>(rows) + (OPK == FOP_ASM32 ? ft_sweep4_rows_bytes(a.Wmax, T) : 0));
+    __shared__ int s_item;
+    const int tid = threadIdx.x;
+    const int *list = a.lists + ((size_t)q * FOP_COUNT + OPK) * a.nprog;
+    const int total = a.counts[q * FOP_COUNT + OPK] * a.ntiles;
+    int *work = a.work + q * FOP_COUNT + OPK;
+    for (;;) {
+        if (tid == 0) s_item = atomicAdd(work, 1);
+        __syncthreads();
+        const int item = s_item;
+        __syncthreads();
+        if (item >= total) break;
+        const int cand = list[item / a.ntiles];
+        const int tile = item % a.ntiles;
+        const FitState *st = a.state + cand;
+        const int ib = a.fins_off[cand];
+        const int nins = a.fins_off[cand + 1] - ib;
+        const int p = a.pcount[cand];
+        const int sel = st->sel;
+        for (int i = tid; i < nins; i += T) ins[i] = a.fins[ib + i];
+        if (tid < p) cf[tid] = (float)(sel ? st->trial[tid] : st->c[tid]);
+        __syncthreads();
+        const int r0 = tile * FT_TILE_ROWS;
+        const int r1 = min(a.n, r0 + FT_TILE_ROWS);
+        double *pt = a.part + ((size_t)cand * a.ntiles + tile) * FT_PART_STRIDE;
+        if (OPK == FOP_ASM32)
+            ft_tile_asm32x4<T>(a, ins, nins, p, cf, stk, tape, rows, red, r0, r1, pt);
+        else
+            ft_tile_loss32x4<T>(a, ins, cf, stk, red, r0, r1, pt);
         __syncthreads();
     }
 }
@@ -1075,8 +1273,13 @@ bool validate_records(const uint32_t *rec, int m, int p, int v)
 
 struct FitPrep {
     std::vector<int> node_off, valid;
+    std::vector<FIns> fins;
+    std::vector<int> fins_off;
     int mmax = 1;
     int pmax = 0;
+    int fslots = 1;
+    int ftape = 1;
+    int fmaxins = 2;
 };
 
 void prep_batch(const unsigned int *off, const unsigned int *prog, const int *pcount, int nprog,
@@ -1096,6 +1299,27 @@ void prep_batch(const unsigned int *off, const unsigned int *prog, const int *pc
             b.pmax = std::max(b.pmax, p);
         }
     }
+    /* the four-row stack machine's translation (a tree not in stack order is
+       rejected as well) */
+    b.fins.clear();
+    b.fins_off.assign(nprog + 1, 0);
+    std::vector<FIns> one;
+    for (int i = 0; i < nprog; ++i) {
+        b.fins_off[i] = (int)b.fins.size();
+        if (!b.valid[i]) continue;
+        int ns = 0, nt = 0;
+        const int m = b.node_off[i + 1] - b.node_off[i];
+        if (!fi_decode(prog + off[i], m, one, &ns, &nt)) {
+            b.valid[i] = 0;
+            continue;
+        }
+        b.fins.insert(b.fins.end(), one.begin(), one.end());
+        b.fslots = std::max(b.fslots, ns);
+        b.ftape = std::max(b.ftape, nt);
+        b.fmaxins = std::max(b.fmaxins, (int)one.size());
+    }
+    b.fins_off[nprog] = (int)b.fins.size();
+    if (b.fins.empty()) b.fins.resize(1);
 }
 
 int occupancy(const void *fn, int threads, size_t smem)
@@ -1125,6 +1349,7 @@ struct SweepLaunch {
     const void *fn;
     size_t smem;
     int grid;
+    int threads;
 };
 
 template <int OPK>
@@ -1136,6 +1361,20 @@ SweepLaunch sweep_launch(RcCtx *c, int mmax, int Wmax)
     if (s.smem > 48 * 1024)
         cudaFuncSetAttribute(s.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
     s.grid = c->sm_count * occupancy(s.fn, FT_THREADS, s.smem);
+    s.threads = FT_THREADS;
+    return s;
+}
+
+template <int OPK, int T>
+SweepLaunch sweep4_launch(RcCtx *c, const FitPrep &b, int Wmax)
+{
+    SweepLaunch s;
+    s.fn = (const void *)ft_sweep4<OPK, T>;
+    s.smem = ft_sweep4_smem(OPK, b.fmaxins, b.fslots, b.ftape, Wmax, T);
+    if (s.smem > 48 * 1024)
+        cudaFuncSetAttribute(s.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
+    s.grid = c->sm_count * occupancy(s.fn, T, s.smem);
+    s.threads = T;
     return s;
 }
 
@@ -1154,7 +1393,7 @@ void enqueue_fit(cudaStream_t s_, int sm_count, const FitArgs &a, int steps,
         for (int k = 0; k < nkinds; ++k) {
             const SweepLaunch &L = sw[k];
             void *args[] = {(void *)&a, (void *)&q};
-            cudaLaunchKernel(L.fn, dim3(L.grid), dim3(FT_THREADS), args, L.smem, s_);
+            cudaLaunchKernel(L.fn, dim3(L.grid), dim3(L.threads), args, L.smem, s_);
         }
         ft_control<<<ctrl_grid, FT_CTRL_T, 0, s_>>>(a, q, 0);
     }
@@ -1189,6 +1428,8 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     const size_t o_p = rc_take(&cur, sizeof(int) * nprog);
     const size_t o_c0 = rc_take(&cur, sizeof(double) * (size_t)nprog * kmax);
     const size_t o_valid = rc_take(&cur, sizeof(int) * nprog);
+    const size_t o_fins = rc_take(&cur, sizeof(FIns) * b.fins.size());
+    const size_t o_finsoff = rc_take(&cur, sizeof(int) * (nprog + 1));
     const size_t in_end = rc_take(&cur, 0);
     const size_t o_c = rc_take(&cur, sizeof(double) * (size_t)nprog * kmax);
     const size_t o_sse = rc_take(&cur, sizeof(double) * nprog);
@@ -1209,6 +1450,8 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     memcpy(host + o_p, pcount, sizeof(int) * nprog);
     memcpy(host + o_c0, c0, sizeof(double) * (size_t)nprog * kmax);
     memcpy(host + o_valid, b.valid.data(), sizeof(int) * nprog);
+    memcpy(host + o_fins, b.fins.data(), sizeof(FIns) * b.fins.size());
+    memcpy(host + o_finsoff, b.fins_off.data(), sizeof(int) * (nprog + 1));
     memcpy(host + o_c, c0, sizeof(double) * (size_t)nprog * kmax);
     st->h2d_ms += rc_now_ms() - t;
     st->h2d_bytes += io_end;
@@ -1231,6 +1474,11 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     a.kmax = kmax;
     a.c0 = reinterpret_cast<const double *>(dev + o_c0);
     a.valid = reinterpret_cast<const int *>(dev + o_valid);
+    a.fins = reinterpret_cast<const FIns *>(dev + o_fins);
+    a.fins_off = reinterpret_cast<const int *>(dev + o_finsoff);
+    a.fslots = b.fslots;
+    a.ftape = b.ftape;
+    a.fmaxins = b.fmaxins;
     a.iters = iters;
     a.metric = metric;
     a.flags = flags;
@@ -1253,8 +1501,8 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
         sw[nk] = sweep_launch<FOP_IJAC>(c, b.mmax, Wmax); ++nk;
         sw[nk] = sweep_launch<FOP_ICOST>(c, b.mmax, Wmax); ++nk;
     } else {
-        sw[nk] = sweep_launch<FOP_ASM32>(c, b.mmax, Wmax); ++nk;
-        sw[nk] = sweep_launch<FOP_LOSS32>(c, b.mmax, Wmax); ++nk;
+        sw[nk] = sweep4_launch<FOP_ASM32, 64>(c, b, Wmax); ++nk;
+        sw[nk] = sweep4_launch<FOP_LOSS32, 128>(c, b, Wmax); ++nk;
         if (!(flags & 1)) {
             sw[nk] = sweep_launch<FOP_ASM64>(c, b.mmax, Wmax); ++nk;
             sw[nk] = sweep_launch<FOP_LOSS64>(c, b.mmax, Wmax); ++nk;
@@ -1276,6 +1524,7 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
             one.pcount = a.pcount + i;
             one.c0 = a.c0 + (size_t)i * kmax;
             one.valid = a.valid + i;
+            one.fins_off = a.fins_off + i;
             one.state = a.state + i;
             one.part = a.part + (size_t)i * ntiles * FT_PART_STRIDE;
             one.outc = a.outc + (size_t)i * kmax;
@@ -1286,8 +1535,9 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
         }
     } else {
         char key[256];
-        snprintf(key, sizeof(key), "%p|%d|%d|%d|%d|%d|%d|%d|%d|%d|%zu", (void *)dev, nprog, kmax,
-                 ntiles, b.mmax, Wmax, iters, metric, flags, steps, io_end);
+        snprintf(key, sizeof(key), "%p|%d|%d|%d|%d|%d|%d|%d|%d|%d|%zu|%d|%d|%d", (void *)dev, nprog,
+                 kmax, ntiles, b.mmax, Wmax, iters, metric, flags, steps, io_end, b.fslots, b.ftape,
+                 b.fmaxins);
         if (!c->fit_graph || c->fit_graph_key != key) {
             if (c->fit_graph) {
                 cudaGraphExecDestroy(c->fit_graph);
