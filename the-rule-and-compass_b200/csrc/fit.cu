@@ -37,6 +37,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "fit_common.cuh"
@@ -91,10 +92,13 @@ struct FitArgs {
     const double *c0;
     const int *valid;
     const FIns *fins;      /* stack-machine translation of the records */
-    const int *fins_off;   /* [P+1] */
+    const int *fins_off;   /* [P+1] start of [forward | reverse] */
+    const int4 *finfo;     /* [P] forward count, reverse count, active threads,
+                              spill slots | tape slots << 16 */
     int fslots;            /* spill slots needed by the batch */
     int ftape;             /* partial-tape slots needed by the batch */
-    int fmaxins;
+    int fmaxins;           /* longest forward + reverse list */
+    size_t asm_region;     /* f32 assembly region of the launch */
     int iters, metric, flags;
     int ntiles;
     int mmax;
@@ -153,193 +157,6 @@ __device__ __forceinline__ void ft_tile_gram_out(const Syrk &sy, const double ac
         pt[q] = s;
     }
     __syncthreads();
-}
-
-/* f32 assembly of one tile at the f32 constants `cf` (eval.cu:1692-1804). */
-template <int T>
-__device__ void ft_tile_asm32(const FitArgs &a, const uint4 *rec, int m, int p, const float *cf,
-                              float *tape, double *rows, double *red, int r0, int r1, double *pt)
-{
-    const int tid = threadIdx.x;
-    const int W = 4 * ((p + 1 + 3) / 4);
-    const Syrk sy = ft_syrk_setup<T>(W);
-    double acc[16];
-#pragma unroll
-    for (int e = 0; e < 16; ++e) acc[e] = 0.0;
-    double loss = 0.0;
-    int bad = 0;
-    float *tp = tape + tid;
-    double *myrow = rows + (size_t)tid * W;
-    for (int base = r0; base < r1; base += T) {
-        const int row = base + tid;
-        for (int j = 0; j < W; ++j) myrow[j] = 0.0;
-        const double wr = (row < r1 && a.w) ? a.w[row] : 1.0;
-        if (row < r1 && wr > 0.0) {
-            const float pred = ft_fwd_f<T>(rec, m, a.cols, a.npad, row, cf, tp);
-            const float r = pred - a.y[row];
-            bool ok = isfinite(pred) && fabsf(pred) <= 1e30f && isfinite(r);
-            ft_bwd_f<T>(rec, m, tp, myrow, 1, nullptr, 0);
-            double sw, resp = (double)r, rowloss;
-            if (a.metric == FM_LOGISTIC) {
-                const double tt = a.tsign ? (double)a.tsign[row] : 0.0;
-                const double u = tt * (double)pred;
-                if (!a.tsign || !isfinite(tt)) ok = false;
-                const double qq = ft_logistic_q(u);
-                sw = wr * qq * (1.0 - qq);
-                resp = -tt / qq;
-                rowloss = wr * ft_softplus_neg(u);
-            } else {
-                sw = ft_row_weight(wr, (double)r, a.metric);
-                rowloss = wr * (double)ft_row_loss_f(r, a.metric);
-            }
-            const float s = sqrtf((float)sw);
-            for (int j = 0; j < p; ++j)
-                if (!isfinite((float)myrow[j])) ok = false;
-            for (int j = 0; j < p; ++j) myrow[j] = ok ? (double)(s * (float)myrow[j]) : 0.0;
-            myrow[p] = ok ? (double)(float)(s * resp) : 0.0;
-            if (ok) loss += rowloss;
-            else bad = 1;
-        }
-        __syncthreads();
-        ft_syrk_chunk(sy, rows, W, T, acc);
-        __syncthreads();
-    }
-    bad = __syncthreads_or(bad);
-    loss = ft_block_sum<T>(loss, red);
-    ft_tile_gram_out<T>(sy, acc, rows, pt);
-    if (tid == 0) {
-        pt[FT_PART_LOSS] = loss;
-        pt[FT_PART_BAD] = bad ? 1.0 : 0.0;
-        pt[FT_PART_SKIP] = 0.0;
-    }
-}
-
-/* f64 assembly of one tile at the f64 constants `cd` (eval.cu:1492-1630):
-   T/2 rows per chunk, each with an f64 tape column. */
-template <int T>
-__device__ void ft_tile_asm64(const FitArgs &a, const uint4 *rec, int m, int p, const double *cd,
-                              double *tape64, double *rows, double *red, int r0, int r1,
-                              double *pt)
-{
-    constexpr int TS = T / 2;
-    const int tid = threadIdx.x;
-    const int W = 4 * ((p + 1 + 3) / 4);
-    const Syrk sy = ft_syrk_setup<T>(W);
-    double acc[16];
-#pragma unroll
-    for (int e = 0; e < 16; ++e) acc[e] = 0.0;
-    double loss = 0.0;
-    int bad = 0, skipped = 0;
-    double *tp = tape64 + tid;
-    double *myrow = rows + (size_t)tid * W;
-    for (int base = r0; base < r1; base += TS) {
-        const int row = base + tid;
-        if (tid < TS) {
-            for (int j = 0; j < W; ++j) myrow[j] = 0.0;
-            const double wr = (row < r1 && a.w) ? a.w[row] : 1.0;
-            if (row < r1 && wr > 0.0) {
-                const double pred = ft_fwd_d<TS>(rec, m, a.cols64, a.npad, row, cd, tp);
-                const double r = pred - a.y64[row];
-                bool ok = isfinite(pred) && isfinite(r);
-                ft_bwd_d<TS>(rec, m, tp, myrow, 1, nullptr, 0);
-                bool grad_ok = true;
-                for (int j = 0; j < p; ++j)
-                    if (!isfinite(myrow[j])) grad_ok = false;
-                double sw, resp = r, rho;
-                if (a.metric == FM_LOGISTIC) {
-                    const double tt = a.tsign64 ? a.tsign64[row] : 0.0;
-                    const double u = tt * pred;
-                    if (!a.tsign64 || !isfinite(tt)) ok = false;
-                    const double qq = ft_logistic_q(u);
-                    sw = wr * qq * (1.0 - qq);
-                    resp = -tt / qq;
-                    rho = ft_softplus_neg(u);
-                } else {
-                    sw = ft_row_weight(wr, r, a.metric);
-                    if (a.metric == FM_SQUARED) rho = r * r;
-                    else if (a.metric == FM_ABSOLUTE) rho = fabs(r);
-                    else rho = log1p(r * r);
-                }
-                const double s = sqrt(sw);
-                const bool use = ok && grad_ok;
-                for (int j = 0; j < p; ++j) myrow[j] = use ? s * myrow[j] : 0.0;
-                myrow[p] = use ? s * resp : 0.0;
-                if (ok) loss += wr * rho;
-                else bad = 1;
-                if (ok && !grad_ok) skipped = 1;
-            }
-        }
-        __syncthreads();
-        ft_syrk_chunk(sy, rows, W, TS, acc);
-        __syncthreads();
-    }
-    bad = __syncthreads_or(bad);
-    skipped = __syncthreads_or(skipped);
-    loss = ft_block_sum<T>(loss, red);
-    ft_tile_gram_out<T>(sy, acc, rows, pt);
-    if (tid == 0) {
-        pt[FT_PART_LOSS] = loss;
-        pt[FT_PART_BAD] = bad ? 1.0 : 0.0;
-        pt[FT_PART_SKIP] = skipped ? 1.0 : 0.0;
-    }
-}
-
-/* f32 objective of one tile (eval.cu:1808-1855). */
-template <int T>
-__device__ void ft_tile_loss32(const FitArgs &a, const uint4 *rec, int m, const float *cf,
-                               float *tape, double *red, int r0, int r1, double *pt)
-{
-    const int tid = threadIdx.x;
-    double local = 0.0;
-    float *tp = tape + tid;
-    for (int row = r0 + tid; row < r1; row += T) {
-        const double wr = a.w ? a.w[row] : 1.0;
-        if (wr <= 0.0) continue;
-        const float pred = ft_fwd_f<T>(rec, m, a.cols, a.npad, row, cf, tp);
-        const float r = pred - a.y[row];
-        if (!isfinite(pred) || fabsf(pred) > 1e30f || !isfinite(r)) local += 1e30;
-        else if (a.metric == FM_LOGISTIC) {
-            const double tt = a.tsign ? (double)a.tsign[row] : 0.0;
-            local += isfinite(tt) ? wr * ft_softplus_neg(tt * (double)pred) : 1e30;
-        } else if (a.metric == FM_SQUARED) local += wr * (double)r * (double)r;
-        else local += wr * (double)ft_row_loss_f(r, a.metric);
-    }
-    const double total = ft_block_sum<T>(local, red);
-    if (tid == 0) {
-        pt[FT_PART_LOSS] = total;
-        pt[FT_PART_BAD] = 0.0;
-    }
-}
-
-/* f64 objective of one tile (eval.cu:1634-1682), T/2 rows at a time. */
-template <int T>
-__device__ void ft_tile_loss64(const FitArgs &a, const uint4 *rec, int m, const double *cd,
-                               double *tape64, double *red, int r0, int r1, double *pt)
-{
-    constexpr int TS = T / 2;
-    const int tid = threadIdx.x;
-    double local = 0.0;
-    if (tid < TS) {
-        double *tp = tape64 + tid;
-        for (int row = r0 + tid; row < r1; row += TS) {
-            const double wr = a.w ? a.w[row] : 1.0;
-            if (wr <= 0.0) continue;
-            const double pred = ft_fwd_d<TS>(rec, m, a.cols64, a.npad, row, cd, tp);
-            const double r = pred - a.y64[row];
-            if (!isfinite(pred) || !isfinite(r)) local += 1e30;
-            else if (a.metric == FM_LOGISTIC) {
-                const double tt = a.tsign64 ? a.tsign64[row] : 0.0;
-                local += isfinite(tt) ? wr * ft_softplus_neg(tt * pred) : 1e30;
-            } else if (a.metric == FM_SQUARED) local += wr * r * r;
-            else if (a.metric == FM_ABSOLUTE) local += wr * fabs(r);
-            else local += wr * log1p(r * r);
-        }
-    }
-    const double total = ft_block_sum<T>(local, red);
-    if (tid == 0) {
-        pt[FT_PART_LOSS] = total;
-        pt[FT_PART_BAD] = 0.0;
-    }
 }
 
 /* Implicit metric of one tile (implicit.rs:156-174, :302-333): the cost
@@ -457,155 +274,321 @@ __global__ void __launch_bounds__(T) ft_sweep(FitArgs a, int q)
         const int r0 = tile * FT_TILE_ROWS;
         const int r1 = min(a.n, r0 + FT_TILE_ROWS);
         double *pt = a.part + ((size_t)cand * a.ntiles + tile) * FT_PART_STRIDE;
-        if (OPK == FOP_ASM32) ft_tile_asm32<T>(a, rec, m, p, cf, tape, rows, red, r0, r1, pt);
-        else if (OPK == FOP_ASM64) ft_tile_asm64<T>(a, rec, m, p, cd, tape64, rows, red, r0, r1, pt);
-        else if (OPK == FOP_LOSS32) ft_tile_loss32<T>(a, rec, m, cf, tape, red, r0, r1, pt);
-        else if (OPK == FOP_LOSS64) ft_tile_loss64<T>(a, rec, m, cd, tape64, red, r0, r1, pt);
-        else if (OPK == FOP_IJAC) ft_tile_implicit<T, true>(a, rec, m, p, cd, tape64, rows, red, r0, r1, pt);
+        if (OPK == FOP_IJAC) ft_tile_implicit<T, true>(a, rec, m, p, cd, tape64, rows, red, r0, r1, pt);
         else ft_tile_implicit<T, false>(a, rec, m, p, cd, tape64, rows, red, r0, r1, pt);
         __syncthreads();
     }
 }
 
-/* ---- four-rows-per-thread f32 sweeps -------------------------------- */
+/* ---- four-rows-per-thread sweeps ------------------------------------- */
 
-/* SYRK over f32 Jacobian rows of stride Wp (values are f32-rounded, so f64
-   products of the widened values are exact). The lanes of a warp own
-   different blocks of the same row, so each scalar load touches one row:
-   one wavefront, broadcast where blocks share columns. */
-__device__ __forceinline__ void ft_syrk_chunk_f32(const Syrk &s, const float *rows, int Wp, int R,
-                                                  double acc[16])
+#define FT_ASM_T 128
+#define FT_ASM_BUDGET (48 * 1024)
+
+/* Per-candidate shared region of an assembly sweep at A active threads:
+   spill slots and partial tape ([slot][A] 16-byte vectors), then the
+   Jacobian rows column-major ([W8][NR * A + 4], W8 = p + 1 rounded up to 8;
+   NR = 4 f32 or 2 f64 rows per thread). A column stride of 4 mod 32 words
+   (f32) or 4 mod 16 words (f64) keeps both the per-thread stores of the
+   reverse sweep and the tensor-core fragment loads bank-conflict free. The
+   size is that of the f64 layout, the larger of the two. */
+__host__ __device__ inline size_t ft_asm_region(int A, int slots, int tape, int W8)
 {
-    if (s.rg >= s.RG) return;
-    for (int r = s.rg; r < R; r += s.RG) {
-        const float *row = rows + (size_t)r * Wp;
-        double av[4], bv[4];
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            av[c] = row[4 * s.bi + c];
-            bv[c] = row[4 * s.bj + c];
-        }
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) acc[i * 4 + j] = fma(av[i], bv[j], acc[i * 4 + j]);
-    }
+    return 16 * (size_t)A * (size_t)(slots + tape) + 8 * (size_t)W8 * (2 * (size_t)A + 4);
 }
 
-/* Jacobian rows of the four-row sweep: 4T rows of Wmax + 1 floats (an odd
-   stride: thread t owns rows t, t+T, t+2T, t+3T, so its accesses to one
-   column fall in distinct banks across the warp). */
-__host__ __device__ inline size_t ft_sweep4_rows_bytes(int Wmax, int T)
+/* Active threads of a candidate: the most (128, 64 or 32) whose region fits
+   the fixed budget. It depends on the candidate alone, so its summation
+   order does not depend on the batch. */
+inline int ft_asm_threads(int slots, int tape, int p)
 {
-    const size_t rows = sizeof(float) * 4 * (size_t)T * (Wmax + 1);
-    const size_t part = sizeof(double) * (size_t)T * 16;
-    return rows > part ? rows : part;
+    const int W8 = 8 * ((p + 1 + 7) / 8);
+    int A = FT_ASM_T;
+    while (A > 32 && ft_asm_region(A, slots, tape, W8) > FT_ASM_BUDGET) A /= 2;
+    return A;
 }
 
-/* Shared memory of a four-row sweep: instructions, f32 constants, spill
-   slots, the partial tape and the Jacobian rows (assembly only), a
-   reduction buffer. */
-__host__ __device__ inline size_t ft_sweep4_smem(int opk, int maxins, int slots, int tape, int Wmax,
+__host__ __device__ inline bool ft_op_f64(int opk) { return opk == FOP_ASM64 || opk == FOP_LOSS64; }
+
+/* Shared memory of a four-row sweep: forward and reverse instructions,
+   constants, the assembly region (or the spill slots of an objective sweep),
+   a reduction buffer. */
+__host__ __device__ inline size_t ft_sweep4_smem(int opk, int maxins, int slots, size_t region,
                                                  int T)
 {
-    size_t s = 8 * (size_t)((maxins + 1) & ~1) + 128 + 16 * (size_t)(slots > 0 ? slots : 1) * T;
-    if (opk == FOP_ASM32) s += 16 * (size_t)(tape > 0 ? tape : 1) * T + ft_sweep4_rows_bytes(Wmax, T);
+    size_t s = 8 * (size_t)((maxins + 1) & ~1) + 8 * FT_MAX_CONST;
+    s += ft_op_assembles(opk) ? region : 16 * (size_t)(slots > 0 ? slots : 1) * T;
     return s + 8 * (size_t)T;
 }
 
-template <int T>
-__device__ void ft_tile_asm32x4(const FitArgs &a, const FIns *ins, int nins, int p,
-                                const float *cf, float4 *stk, float4 *tape, float *rows,
-                                double *red, int r0, int r1, double *pt)
+/* One row's place in an assembly, from its prediction (eval.cu:1692-1804
+   for f32, :1492-1630 for f64): whether it counts, whether it is usable, the
+   adjoint seed (its square-root IRLS/GN weight), the weighted residual and
+   its objective term. */
+struct FtRow {
+    bool use, ok;
+    float s_zero;
+    double seed, res, loss;
+};
+
+__device__ __forceinline__ FtRow ft_row_f32(const FitArgs &a, int rr, int r1, float pred)
 {
-    const int tid = threadIdx.x;
-    const int W = 4 * ((p + 1 + 3) / 4);
-    const Syrk sy = ft_syrk_setup<T>(W);
-    double acc[16];
-#pragma unroll
-    for (int e = 0; e < 16; ++e) acc[e] = 0.0;
-    double loss = 0.0;
-    int bad = 0;
-    const int Wp = W + 1;
-    float *g = rows + (size_t)tid * Wp;
-    for (int base = r0; base < r1; base += 4 * T) {
-        const int row = base + 4 * tid;
-        for (int i = 0; i < 4; ++i)
-            for (int j = 0; j < W; ++j) g[(size_t)i * T * Wp + j] = 0.0f;
-        const float4 pv = fi_forward<T, true>(ins, cf, a.cols, a.npad, row, stk, tape, tid);
-        fi_reverse<T>(ins, nins, stk, tape, g, T * Wp, tid);
-        const float pr[4] = {pv.x, pv.y, pv.z, pv.w};
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            float *gi = g + (size_t)i * T * Wp;
-            const int rr = row + i;
-            const double wr = (rr < r1 && a.w) ? a.w[rr] : 1.0;
-            if (!(rr < r1 && wr > 0.0)) {
-                for (int j = 0; j < W; ++j) gi[j] = 0.0f;
-                continue;
-            }
-            const float pred = pr[i];
-            const float r = pred - a.y[rr];
-            bool ok = isfinite(pred) && fabsf(pred) <= 1e30f && isfinite(r);
-            double sw, resp = (double)r, rowloss;
-            if (a.metric == FM_LOGISTIC) {
-                const double tt = a.tsign ? (double)a.tsign[rr] : 0.0;
-                const double u = tt * (double)pred;
-                if (!a.tsign || !isfinite(tt)) ok = false;
-                const double qq = ft_logistic_q(u);
-                sw = wr * qq * (1.0 - qq);
-                resp = -tt / qq;
-                rowloss = wr * ft_softplus_neg(u);
-            } else {
-                sw = ft_row_weight(wr, (double)r, a.metric);
-                rowloss = wr * (double)ft_row_loss_f(r, a.metric);
-            }
-            const float s = sqrtf((float)sw);
-            for (int j = 0; j < p; ++j)
-                if (!isfinite(gi[j])) ok = false;
-            for (int j = 0; j < p; ++j) gi[j] = ok ? s * gi[j] : 0.0f;
-            gi[p] = ok ? (float)(s * resp) : 0.0f;
-            for (int j = p + 1; j < W; ++j) gi[j] = 0.0f;
-            if (ok) loss += rowloss;
-            else bad = 1;
-        }
-        __syncthreads();
-        ft_syrk_chunk_f32(sy, rows, Wp, 4 * T, acc);
-        __syncthreads();
+    FtRow o;
+    const double wr = (rr < r1 && a.w) ? a.w[rr] : 1.0;
+    o.use = rr < r1 && wr > 0.0;
+    o.ok = false;
+    o.s_zero = 0.0f;
+    o.seed = 0.0;
+    o.res = 0.0;
+    o.loss = 0.0;
+    if (!o.use) return o;
+    const float r = pred - a.y[rr];
+    bool good = isfinite(pred) && fabsf(pred) <= 1e30f && isfinite(r);
+    double sw, resp = (double)r;
+    if (a.metric == FM_LOGISTIC) {
+        const double tt = a.tsign ? (double)a.tsign[rr] : 0.0;
+        const double u = tt * (double)pred;
+        if (!a.tsign || !isfinite(tt)) good = false;
+        const double qq = ft_logistic_q(u);
+        sw = wr * qq * (1.0 - qq);
+        resp = -tt / qq;
+        o.loss = wr * ft_softplus_neg(u);
+    } else {
+        sw = ft_row_weight(wr, (double)r, a.metric);
+        o.loss = wr * (double)ft_row_loss_f(r, a.metric);
     }
-    bad = __syncthreads_or(bad);
-    loss = ft_block_sum<T>(loss, red);
-    ft_tile_gram_out<T>(sy, acc, reinterpret_cast<double *>(rows), pt);
-    if (threadIdx.x == 0) {
-        pt[FT_PART_LOSS] = loss;
-        pt[FT_PART_BAD] = bad ? 1.0 : 0.0;
-        pt[FT_PART_SKIP] = 0.0;
+    const float s = sqrtf((float)sw);
+    o.ok = good;
+    if (good) {
+        o.seed = s > 0.0f ? s : 1.0f;
+        o.s_zero = s > 0.0f ? 0.0f : 1.0f;
+        o.res = (float)(s * resp);
+    }
+    return o;
+}
+
+__device__ __forceinline__ FtRow ft_row_f64(const FitArgs &a, int rr, int r1, double pred)
+{
+    FtRow o;
+    const double wr = (rr < r1 && a.w) ? a.w[rr] : 1.0;
+    o.use = rr < r1 && wr > 0.0;
+    o.ok = false;
+    o.s_zero = 0.0f;
+    o.seed = 0.0;
+    o.res = 0.0;
+    o.loss = 0.0;
+    if (!o.use) return o;
+    const double r = pred - a.y64[rr];
+    bool good = isfinite(pred) && isfinite(r);
+    double sw, resp = r, rho;
+    if (a.metric == FM_LOGISTIC) {
+        const double tt = a.tsign64 ? a.tsign64[rr] : 0.0;
+        const double u = tt * pred;
+        if (!a.tsign64 || !isfinite(tt)) good = false;
+        const double qq = ft_logistic_q(u);
+        sw = wr * qq * (1.0 - qq);
+        resp = -tt / qq;
+        rho = ft_softplus_neg(u);
+    } else {
+        sw = ft_row_weight(wr, r, a.metric);
+        if (a.metric == FM_SQUARED) rho = r * r;
+        else if (a.metric == FM_ABSOLUTE) rho = fabs(r);
+        else rho = log1p(r * r);
+    }
+    const double s = sqrt(sw);
+    o.ok = good;
+    o.loss = wr * rho;
+    if (good) {
+        o.seed = s > 0.0 ? s : 1.0;
+        o.s_zero = s > 0.0 ? 0.0f : 1.0f;
+        o.res = s * resp;
+    }
+    return o;
+}
+
+/* Fold the warp's NR * 32 rows of the column-major Jacobian into its
+   J^T J | J^T r blocks with f64 tensor-core MMAs (f32 values widen
+   exactly, so products are exact and sums f64). */
+template <int NB, typename V>
+__device__ __forceinline__ void ft_fold(const V *g, int R, int A, int w, int gid, int tig,
+                                        double (*acc)[2])
+{
+    constexpr int NR = FiV<V>::NR;
+#pragma unroll 4
+    for (int s = 0; s < 8 * NR; ++s) {
+        const int q = 4 * s + tig;
+        const int local = (q >> 5) * A + 32 * w + (q & 31);
+        double x[NB];
+#pragma unroll
+        for (int I = 0; I < NB; ++I) x[I] = (double)g[(size_t)(8 * I + gid) * R + local];
+        int b = 0;
+#pragma unroll
+        for (int I = 0; I < NB; ++I)
+#pragma unroll
+            for (int J = 0; J <= I; ++J, ++b) fi_dmma(acc[b][0], acc[b][1], x[I], x[J]);
     }
 }
 
-template <int T>
-__device__ void ft_tile_loss32x4(const FitArgs &a, const FIns *ins, const float *cf, float4 *stk,
-                                 double *red, int r0, int r1, double *pt)
+/* Assembly of one tile in f32 or f64: the forward sweep of the thread's
+   rows, the reverse sweep seeded with each row's square-root weight (so it
+   yields the weighted Jacobian row), the weighted residual as column p, and
+   the warp's rows folded into the augmented Gram matrix. Warps work
+   independently over their own rows; the tile's sum is a fixed-order sum
+   over warps, written in the packed 4x4-block layout the controller reads. */
+template <typename V, int T>
+__device__ void ft_tile_asm(const FitArgs &a, const FIns *fwd, const FIns *rev, int nr, int p,
+                            int A, int slots, int ntape, const V *cv, unsigned char *region,
+                            double *red, int r0, int r1, double *pt)
 {
+    using F = FiV<V>;
+    using V4 = typename F::V4;
+    constexpr int NR = F::NR;
+    constexpr bool F64 = sizeof(V) == 8;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, w = tid >> 5, gid = lane >> 2, tig = lane & 3;
+    const int NB = (p + 1 + 7) / 8;
+    const int W8 = 8 * NB, R = NR * A + 4;
+    V4 *stk = reinterpret_cast<V4 *>(region);
+    V4 *tape = stk + (size_t)slots * A;
+    V *g = reinterpret_cast<V *>(tape + (size_t)ntape * A);
+    const V *cols = F64 ? reinterpret_cast<const V *>(a.cols64) : reinterpret_cast<const V *>(a.cols);
+    for (int i = tid; i < W8 * R; i += T) g[i] = V(0);
+    __syncthreads();
+    double acc[6][2];
+#pragma unroll
+    for (int b = 0; b < 6; ++b) acc[b][0] = acc[b][1] = 0.0;
+    double loss = 0.0;
+    int bad = 0, skipped = 0;
+    if (tid < A) {
+        V *gt = g + tid;
+        for (int base = r0; base < r1; base += NR * A) {
+            const int row = base + NR * tid;
+            V pr[NR];
+            fi_forward<V, true>(fwd, cv, cols, a.npad, row, stk, tape, A, tid, pr);
+            FtRow rw[NR];
+            V seed[NR];
+            bool special = false;
+#pragma unroll
+            for (int i = 0; i < NR; ++i) {
+                rw[i] = F64 ? ft_row_f64(a, row + i, r1, (double)pr[i])
+                            : ft_row_f32(a, row + i, r1, (float)pr[i]);
+                seed[i] = (V)rw[i].seed;
+                special = special || rw[i].s_zero != 0.0f;
+            }
+            const bool fin = fi_reverse<V>(rev, nr, stk, tape, A, tid, gt, R, A, seed);
+            if (!fin || special) {
+                /* rare rows: a non-finite Jacobian entry (the row is dropped
+                   from the Jacobian; in f32 it counts as failed), or a zero
+                   weight (its entries are zero) */
+#pragma unroll
+                for (int i = 0; i < NR; ++i) {
+                    if (!rw[i].ok) continue;
+                    V *gi = gt + (size_t)i * A;
+                    bool rf = true;
+                    if (!fin)
+                        for (int j = 0; j < p; ++j) rf = rf && isfinite(gi[(size_t)j * R]);
+                    if (!rf || rw[i].s_zero != 0.0f)
+                        for (int j = 0; j < p; ++j) gi[(size_t)j * R] = V(0);
+                    if (!rf) {
+                        if (F64) {
+                            skipped = 1;
+                            rw[i].res = 0.0;
+                            rw[i].seed = 0.0; /* marks the row's residual column zero */
+                        } else {
+                            rw[i].ok = false;
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < NR; ++i) {
+                const bool jac = rw[i].ok && rw[i].seed != 0.0;
+                gt[(size_t)p * R + (size_t)i * A] = jac ? (V)rw[i].res : V(0);
+                if (rw[i].ok) loss += rw[i].loss;
+                else if (rw[i].use) bad = 1;
+            }
+            __syncwarp();
+            if (NB <= 1) ft_fold<1, V>(g, R, A, w, gid, tig, acc);
+            else if (NB == 2) ft_fold<2, V>(g, R, A, w, gid, tig, acc);
+            else ft_fold<3, V>(g, R, A, w, gid, tig, acc);
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    const int NBLK = NB * (NB + 1) / 2;
+    double *gb = reinterpret_cast<double *>(region);
+    if (tid < A) {
+        for (int b = 0; b < NBLK; ++b) {
+            gb[(size_t)(w * NBLK + b) * 64 + gid * 8 + 2 * tig] = acc[b][0];
+            gb[(size_t)(w * NBLK + b) * 64 + gid * 8 + 2 * tig + 1] = acc[b][1];
+        }
+    }
+    __syncthreads();
+    const int W = 4 * ((p + 1 + 3) / 4);
+    const int nb4 = W / 4, nblk4 = nb4 * (nb4 + 1) / 2, nw = A / 32;
+    for (int e = tid; e < nblk4 * 16; e += T) {
+        int b4 = e >> 4, bi = 0;
+        while (b4 > bi) {
+            b4 -= bi + 1;
+            ++bi;
+        }
+        const int rw4 = 4 * bi + ((e & 15) >> 2), cl = 4 * b4 + (e & 3);
+        const int I = rw4 >> 3, J = cl >> 3;
+        const int el = (I * (I + 1) / 2 + J) * 64 + (rw4 & 7) * 8 + (cl & 7);
+        double s = 0.0;
+        for (int v = 0; v < nw; ++v) s += gb[(size_t)v * NBLK * 64 + el];
+        pt[e] = s;
+    }
+    bad = __syncthreads_or(bad);
+    skipped = __syncthreads_or(skipped);
+    loss = ft_block_sum<T>(loss, red);
+    if (tid == 0) {
+        pt[FT_PART_LOSS] = loss;
+        pt[FT_PART_BAD] = bad ? 1.0 : 0.0;
+        pt[FT_PART_SKIP] = skipped ? 1.0 : 0.0;
+    }
+}
+
+/* Objective of one tile in f32 or f64 (eval.cu:1808-1855): the forward
+   sweep only; a row that is not finite costs 1e30. */
+template <typename V, int T>
+__device__ void ft_tile_loss(const FitArgs &a, const FIns *ins, const V *cv,
+                             typename FiV<V>::V4 *stk, double *red, int r0, int r1, double *pt)
+{
+    constexpr int NR = FiV<V>::NR;
+    constexpr bool F64 = sizeof(V) == 8;
+    const V *cols = F64 ? reinterpret_cast<const V *>(a.cols64) : reinterpret_cast<const V *>(a.cols);
     const int tid = threadIdx.x;
     double local = 0.0;
-    for (int row = r0 + 4 * tid; row < r1; row += 4 * T) {
-        const float4 pv = fi_forward<T, false>(ins, cf, a.cols, a.npad, row, stk, nullptr, tid);
-        const float pr[4] = {pv.x, pv.y, pv.z, pv.w};
+    for (int row = r0 + NR * tid; row < r1; row += NR * T) {
+        V pr[NR];
+        fi_forward<V, false>(ins, cv, cols, a.npad, row, stk, nullptr, T, tid, pr);
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
+        for (int i = 0; i < NR; ++i) {
             const int rr = row + i;
             if (rr >= r1) continue;
             const double wr = a.w ? a.w[rr] : 1.0;
             if (wr <= 0.0) continue;
-            const float pred = pr[i];
-            const float r = pred - a.y[rr];
-            if (!isfinite(pred) || fabsf(pred) > 1e30f || !isfinite(r)) local += 1e30;
-            else if (a.metric == FM_LOGISTIC) {
-                const double tt = a.tsign ? (double)a.tsign[rr] : 0.0;
-                local += isfinite(tt) ? wr * ft_softplus_neg(tt * (double)pred) : 1e30;
-            } else if (a.metric == FM_SQUARED) local += wr * (double)r * (double)r;
-            else local += wr * (double)ft_row_loss_f(r, a.metric);
+            if (F64) {
+                const double pred = (double)pr[i];
+                const double r = pred - a.y64[rr];
+                if (!isfinite(pred) || !isfinite(r)) local += 1e30;
+                else if (a.metric == FM_LOGISTIC) {
+                    const double tt = a.tsign64 ? a.tsign64[rr] : 0.0;
+                    local += isfinite(tt) ? wr * ft_softplus_neg(tt * pred) : 1e30;
+                } else if (a.metric == FM_SQUARED) local += wr * r * r;
+                else if (a.metric == FM_ABSOLUTE) local += wr * fabs(r);
+                else local += wr * log1p(r * r);
+            } else {
+                const float pred = (float)pr[i];
+                const float r = pred - a.y[rr];
+                if (!isfinite(pred) || fabsf(pred) > 1e30f || !isfinite(r)) local += 1e30;
+                else if (a.metric == FM_LOGISTIC) {
+                    const double tt = a.tsign ? (double)a.tsign[rr] : 0.0;
+                    local += isfinite(tt) ? wr * ft_softplus_neg(tt * (double)pred) : 1e30;
+                } else if (a.metric == FM_SQUARED) local += wr * (double)r * (double)r;
+                else local += wr * (double)ft_row_loss_f(r, a.metric);
+            }
         }
     }
     const double total = ft_block_sum<T>(local, red);
@@ -615,18 +598,21 @@ __device__ void ft_tile_loss32x4(const FitArgs &a, const FIns *ins, const float 
     }
 }
 
-/* The f32 assembly / objective sweeps over the four-row interpreter. */
+/* The assembly / objective sweeps (f32 and f64) over the four-row
+   interpreter: a persistent grid over the queued (candidate, tile) items. */
 template <int OPK, int T>
 __global__ void __launch_bounds__(T) ft_sweep4(FitArgs a, int q)
 {
+    using V = typename std::conditional<OPK == FOP_ASM64 || OPK == FOP_LOSS64, double, float>::type;
+    using V4 = typename FiV<V>::V4;
     extern __shared__ __align__(16) unsigned char sm[];
     FIns *ins = reinterpret_cast<FIns *>(sm);
-    float *cf = reinterpret_cast<float *>(sm + 8 * (size_t)((a.fmaxins + 1) & ~1));
-    float4 *stk = reinterpret_cast<float4 *>(reinterpret_cast<unsigned char *>(cf) + 128);
-    float4 *tape = stk + (size_t)(a.fslots > 0 ? a.fslots : 1) * T;
-    float *rows = reinterpret_cast<float *>(tape + (OPK == FOP_ASM32 ? (size_t)(a.ftape > 0 ? a.ftape : 1) * T : 0));
+    V *cv = reinterpret_cast<V *>(sm + 8 * (size_t)((a.fmaxins + 1) & ~1));
+    unsigned char *region = reinterpret_cast<unsigned char *>(sm + 8 * (size_t)((a.fmaxins + 1) & ~1) +
+                                                              8 * FT_MAX_CONST);
     double *red = reinterpret_cast<double *>(
-        reinterpret_cast<unsigned char *>(rows) + (OPK == FOP_ASM32 ? ft_sweep4_rows_bytes(a.Wmax, T) : 0));
+        region + (ft_op_assembles(OPK) ? a.asm_region
+                                       : 16 * (size_t)(a.fslots > 0 ? a.fslots : 1) * T));
     __shared__ int s_item;
     const int tid = threadIdx.x;
     const int *list = a.lists + ((size_t)q * FOP_COUNT + OPK) * a.nprog;
@@ -642,19 +628,22 @@ __global__ void __launch_bounds__(T) ft_sweep4(FitArgs a, int q)
         const int tile = item % a.ntiles;
         const FitState *st = a.state + cand;
         const int ib = a.fins_off[cand];
-        const int nins = a.fins_off[cand + 1] - ib;
+        const int4 info = a.finfo[cand];
+        const int nf = info.x, nr = info.y;
+        const int nins = ft_op_assembles(OPK) ? nf + nr : nf;
         const int p = a.pcount[cand];
         const int sel = st->sel;
         for (int i = tid; i < nins; i += T) ins[i] = a.fins[ib + i];
-        if (tid < p) cf[tid] = (float)(sel ? st->trial[tid] : st->c[tid]);
+        if (tid < p) cv[tid] = (V)(sel ? st->trial[tid] : st->c[tid]);
         __syncthreads();
         const int r0 = tile * FT_TILE_ROWS;
         const int r1 = min(a.n, r0 + FT_TILE_ROWS);
         double *pt = a.part + ((size_t)cand * a.ntiles + tile) * FT_PART_STRIDE;
-        if (OPK == FOP_ASM32)
-            ft_tile_asm32x4<T>(a, ins, nins, p, cf, stk, tape, rows, red, r0, r1, pt);
+        if (ft_op_assembles(OPK))
+            ft_tile_asm<V, T>(a, ins, ins + nf, nr, p, info.z, info.w & 0xffff, info.w >> 16, cv,
+                              region, red, r0, r1, pt);
         else
-            ft_tile_loss32x4<T>(a, ins, cf, stk, red, r0, r1, pt);
+            ft_tile_loss<V, T>(a, ins, cv, reinterpret_cast<V4 *>(region), red, r0, r1, pt);
         __syncthreads();
     }
 }
@@ -1142,6 +1131,47 @@ __global__ void __launch_bounds__(T) ft_grad_kernel(FitArgs a, int want, int row
     }
 }
 
+/* Constant gradients of rows [row0, row0 + nrows) through the same
+   four-row forward and reverse sweeps as the f32 assembly, with adjoint
+   seed 1: one warp per (candidate, 128-row tile), tiles aligned down to a
+   multiple of four rows. */
+__global__ void __launch_bounds__(32) ft_grad4_kernel(FitArgs a, int row0, int nrows, int ntiles,
+                                                      float *value, float *out)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int cand = blockIdx.x / ntiles;
+    const int tile = blockIdx.x % ntiles;
+    const int tid = threadIdx.x;
+    if (!a.valid[cand]) return;
+    const int4 info = a.finfo[cand];
+    const int nf = info.x, nr = info.y, slots = info.w & 0xffff, ntape = info.w >> 16;
+    const int p = a.pcount[cand];
+    FIns *ins = reinterpret_cast<FIns *>(smem);
+    float *cf = reinterpret_cast<float *>(smem + 8 * (size_t)((a.fmaxins + 1) & ~1));
+    float4 *stk = reinterpret_cast<float4 *>(cf + FT_MAX_CONST);
+    float4 *tape = stk + (size_t)slots * 32;
+    float *g = reinterpret_cast<float *>(tape + (size_t)ntape * 32);
+    const int R = 4 * 32 + 4;
+    const int ib = a.fins_off[cand];
+    for (int i = tid; i < nf + nr; i += 32) ins[i] = a.fins[ib + i];
+    if (tid < p) cf[tid] = (float)a.c0[(size_t)cand * a.kmax + tid];
+    for (int i = tid; i < p * R; i += 32) g[i] = 0.0f;
+    __syncwarp();
+    const int row = (row0 & ~3) + tile * 128 + 4 * tid;
+    if (row >= row0 + nrows || row >= a.n) return;
+    float pr[4], seed[4] = {1.0f, 1.0f, 1.0f, 1.0f};
+    fi_forward<float, true>(ins, cf, a.cols, a.npad, row, stk, tape, 32, tid, pr);
+    fi_reverse<float>(ins + nf, nr, stk, tape, 32, tid, g + tid, R, 32, seed);
+    for (int i = 0; i < 4; ++i) {
+        const int rr = row + i;
+        if (rr < row0 || rr >= row0 + nrows) continue;
+        const size_t o = (size_t)cand * nrows + (rr - row0);
+        value[o] = pr[i];
+        for (int j = 0; j < a.kmax; ++j)
+            out[o * a.kmax + j] = j < p ? g[(size_t)j * R + i * 32 + tid] : 0.0f;
+    }
+}
+
 /* Implicit score per (candidate, tile of rows): partial sums of w * d and w. */
 template <int T>
 __global__ void __launch_bounds__(T) ft_implicit_score_kernel(FitArgs a, int ntiles,
@@ -1275,6 +1305,8 @@ struct FitPrep {
     std::vector<int> node_off, valid;
     std::vector<FIns> fins;
     std::vector<int> fins_off;
+    std::vector<int4> finfo;
+    size_t asm_region = 0;
     int mmax = 1;
     int pmax = 0;
     int fslots = 1;
@@ -1303,20 +1335,27 @@ void prep_batch(const unsigned int *off, const unsigned int *prog, const int *pc
        rejected as well) */
     b.fins.clear();
     b.fins_off.assign(nprog + 1, 0);
-    std::vector<FIns> one;
+    b.finfo.assign(nprog, make_int4(0, 0, 32, 0));
+    b.asm_region = FT_ASM_BUDGET;
+    std::vector<FIns> fwd, rev;
     for (int i = 0; i < nprog; ++i) {
         b.fins_off[i] = (int)b.fins.size();
         if (!b.valid[i]) continue;
         int ns = 0, nt = 0;
         const int m = b.node_off[i + 1] - b.node_off[i];
-        if (!fi_decode(prog + off[i], m, one, &ns, &nt)) {
+        if (!fi_decode(prog + off[i], m, fwd, rev, &ns, &nt) || ns > 0xffff || nt > 0x7fff) {
             b.valid[i] = 0;
             continue;
         }
-        b.fins.insert(b.fins.end(), one.begin(), one.end());
+        b.fins.insert(b.fins.end(), fwd.begin(), fwd.end());
+        b.fins.insert(b.fins.end(), rev.begin(), rev.end());
+        const int A = ft_asm_threads(ns, nt, pcount[i]);
+        b.finfo[i] = make_int4((int)fwd.size(), (int)rev.size(), A, ns | (nt << 16));
+        b.asm_region = std::max(b.asm_region,
+                                ft_asm_region(A, ns, nt, 8 * ((pcount[i] + 1 + 7) / 8)));
         b.fslots = std::max(b.fslots, ns);
         b.ftape = std::max(b.ftape, nt);
-        b.fmaxins = std::max(b.fmaxins, (int)one.size());
+        b.fmaxins = std::max(b.fmaxins, (int)(fwd.size() + rev.size()));
     }
     b.fins_off[nprog] = (int)b.fins.size();
     if (b.fins.empty()) b.fins.resize(1);
@@ -1370,7 +1409,8 @@ SweepLaunch sweep4_launch(RcCtx *c, const FitPrep &b, int Wmax)
 {
     SweepLaunch s;
     s.fn = (const void *)ft_sweep4<OPK, T>;
-    s.smem = ft_sweep4_smem(OPK, b.fmaxins, b.fslots, b.ftape, Wmax, T);
+    (void)Wmax;
+    s.smem = ft_sweep4_smem(OPK, b.fmaxins, b.fslots, b.asm_region, T);
     if (s.smem > 48 * 1024)
         cudaFuncSetAttribute(s.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
     s.grid = c->sm_count * occupancy(s.fn, T, s.smem);
@@ -1430,6 +1470,7 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     const size_t o_valid = rc_take(&cur, sizeof(int) * nprog);
     const size_t o_fins = rc_take(&cur, sizeof(FIns) * b.fins.size());
     const size_t o_finsoff = rc_take(&cur, sizeof(int) * (nprog + 1));
+    const size_t o_finfo = rc_take(&cur, sizeof(int4) * nprog);
     const size_t in_end = rc_take(&cur, 0);
     const size_t o_c = rc_take(&cur, sizeof(double) * (size_t)nprog * kmax);
     const size_t o_sse = rc_take(&cur, sizeof(double) * nprog);
@@ -1452,6 +1493,7 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     memcpy(host + o_valid, b.valid.data(), sizeof(int) * nprog);
     memcpy(host + o_fins, b.fins.data(), sizeof(FIns) * b.fins.size());
     memcpy(host + o_finsoff, b.fins_off.data(), sizeof(int) * (nprog + 1));
+    memcpy(host + o_finfo, b.finfo.data(), sizeof(int4) * nprog);
     memcpy(host + o_c, c0, sizeof(double) * (size_t)nprog * kmax);
     st->h2d_ms += rc_now_ms() - t;
     st->h2d_bytes += io_end;
@@ -1476,6 +1518,8 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     a.valid = reinterpret_cast<const int *>(dev + o_valid);
     a.fins = reinterpret_cast<const FIns *>(dev + o_fins);
     a.fins_off = reinterpret_cast<const int *>(dev + o_finsoff);
+    a.finfo = reinterpret_cast<const int4 *>(dev + o_finfo);
+    a.asm_region = b.asm_region;
     a.fslots = b.fslots;
     a.ftape = b.ftape;
     a.fmaxins = b.fmaxins;
@@ -1501,11 +1545,11 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
         sw[nk] = sweep_launch<FOP_IJAC>(c, b.mmax, Wmax); ++nk;
         sw[nk] = sweep_launch<FOP_ICOST>(c, b.mmax, Wmax); ++nk;
     } else {
-        sw[nk] = sweep4_launch<FOP_ASM32, 64>(c, b, Wmax); ++nk;
+        sw[nk] = sweep4_launch<FOP_ASM32, FT_ASM_T>(c, b, Wmax); ++nk;
         sw[nk] = sweep4_launch<FOP_LOSS32, 128>(c, b, Wmax); ++nk;
         if (!(flags & 1)) {
-            sw[nk] = sweep_launch<FOP_ASM64>(c, b.mmax, Wmax); ++nk;
-            sw[nk] = sweep_launch<FOP_LOSS64>(c, b.mmax, Wmax); ++nk;
+            sw[nk] = sweep4_launch<FOP_ASM64, FT_ASM_T>(c, b, Wmax); ++nk;
+            sw[nk] = sweep4_launch<FOP_LOSS64, 128>(c, b, Wmax); ++nk;
         }
     }
     const int steps = max_steps(iters, metric);
@@ -1525,6 +1569,7 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
             one.c0 = a.c0 + (size_t)i * kmax;
             one.valid = a.valid + i;
             one.fins_off = a.fins_off + i;
+            one.finfo = a.finfo + i;
             one.state = a.state + i;
             one.part = a.part + (size_t)i * ntiles * FT_PART_STRIDE;
             one.outc = a.outc + (size_t)i * kmax;
@@ -1535,9 +1580,9 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
         }
     } else {
         char key[256];
-        snprintf(key, sizeof(key), "%p|%d|%d|%d|%d|%d|%d|%d|%d|%d|%zu|%d|%d|%d", (void *)dev, nprog,
-                 kmax, ntiles, b.mmax, Wmax, iters, metric, flags, steps, io_end, b.fslots, b.ftape,
-                 b.fmaxins);
+        snprintf(key, sizeof(key), "%p|%d|%d|%d|%d|%d|%d|%d|%d|%d|%zu|%d|%d|%d|%zu", (void *)dev,
+                 nprog, kmax, ntiles, b.mmax, Wmax, iters, metric, flags, steps, io_end, b.fslots,
+                 b.ftape, b.fmaxins, b.asm_region);
         if (!c->fit_graph || c->fit_graph_key != key) {
             if (c->fit_graph) {
                 cudaGraphExecDestroy(c->fit_graph);
@@ -1622,9 +1667,10 @@ int rc_fit_kernel_info(int kmax, int *threads, int *smem_bytes, int *max_constan
 {
     if (!threads || !smem_bytes || !max_constants) return -1;
     if (kmax > FT_MAX_CONST || kmax < 0) return -1;
-    const int W = 4 * ((kmax + 1 + 3) / 4);
-    *threads = FT_THREADS;
-    *smem_bytes = (int)ft_sweep_smem(FOP_ASM32, FT_MAX_NODES_ABI, W, FT_THREADS);
+    /* the f32 assembly sweep: its fixed region budget plus the instruction
+       lists of the largest accepted tree */
+    *threads = FT_ASM_T;
+    *smem_bytes = (int)ft_sweep4_smem(FOP_ASM32, 2 * FT_MAX_NODES_ABI + 1, 1, FT_ASM_BUDGET, FT_ASM_T);
     *max_constants = FT_MAX_CONST;
     return 0;
 }
@@ -1652,7 +1698,11 @@ int rc_grad_batch(void *ctx, const unsigned int *prog, const unsigned int *off, 
     const size_t o_val = rc_take(&cur, sizeof(float) * (size_t)nprog * nrows);
     const size_t o_out = rc_take(&cur, sizeof(float) * (size_t)nprog * nrows * width);
     const size_t io_end = rc_take(&cur, 0);
-    if (rc_reserve(rc, io_end, io_end) != 0) return -1;
+    const size_t o_fins = rc_take(&cur, sizeof(FIns) * b.fins.size());
+    const size_t o_finsoff = rc_take(&cur, sizeof(int) * (nprog + 1));
+    const size_t o_finfo = rc_take(&cur, sizeof(int4) * nprog);
+    const size_t dev_end = rc_take(&cur, 0);
+    if (rc_reserve(rc, dev_end, io_end) != 0) return -1;
     unsigned char *dev = rc->dev, *host = rc->host;
     memcpy(host + o_rec, prog, sizeof(uint32_t) * words);
     memcpy(host + o_noff, b.node_off.data(), sizeof(int) * (nprog + 1));
@@ -1674,6 +1724,30 @@ int rc_grad_batch(void *ctx, const unsigned int *prog, const unsigned int *off, 
     a.c0 = reinterpret_cast<const double *>(dev + o_c);
     a.valid = reinterpret_cast<const int *>(dev + o_valid);
     a.mmax = mmax;
+    if (want == 1) {
+        /* the four-row sweeps of the f32 assembly */
+        std::vector<unsigned char> stage(dev_end - io_end);
+        memcpy(stage.data() + (o_fins - io_end), b.fins.data(), sizeof(FIns) * b.fins.size());
+        memcpy(stage.data() + (o_finsoff - io_end), b.fins_off.data(), sizeof(int) * (nprog + 1));
+        memcpy(stage.data() + (o_finfo - io_end), b.finfo.data(), sizeof(int4) * nprog);
+        a.fins = reinterpret_cast<const FIns *>(dev + o_fins);
+        a.fins_off = reinterpret_cast<const int *>(dev + o_finsoff);
+        a.finfo = reinterpret_cast<const int4 *>(dev + o_finfo);
+        a.fmaxins = b.fmaxins;
+        cudaMemcpyAsync(dev + io_end, stage.data(), stage.size(), cudaMemcpyHostToDevice, rc->s);
+        const int ntiles = ((row0 + nrows) - (row0 & ~3) + 127) / 128;
+        const size_t smem = 8 * (size_t)((b.fmaxins + 1) & ~1) + 4 * FT_MAX_CONST +
+                            16 * 32 * (size_t)(b.fslots + b.ftape) +
+                            4 * (size_t)(b.pmax > 0 ? b.pmax : 1) * (4 * 32 + 4);
+        if (cudaFuncSetAttribute(ft_grad4_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem) != cudaSuccess) {
+            cudaGetLastError();
+            return -1;
+        }
+        ft_grad4_kernel<<<nprog * ntiles, 32, smem, rc->s>>>(
+            a, row0, nrows, ntiles, reinterpret_cast<float *>(dev + o_val),
+            reinterpret_cast<float *>(dev + o_out));
+    } else {
     const int T = 128;
     const int ntiles = (nrows + T - 1) / T;
     const size_t smem = sizeof(uint4) * mmax + sizeof(float) * FT_MAX_CONST +
@@ -1687,6 +1761,7 @@ int rc_grad_batch(void *ctx, const unsigned int *prog, const unsigned int *off, 
     ft_grad_kernel<128><<<nprog * ntiles, T, smem, rc->s>>>(
         a, want, row0, nrows, ntiles, reinterpret_cast<float *>(dev + o_val),
         reinterpret_cast<float *>(dev + o_out));
+    }
     cudaMemcpyAsync(host + in_end, dev + in_end, io_end - in_end, cudaMemcpyDeviceToHost, rc->s);
     if (rc_finish(rc) != 0) return -1;
     memcpy(value, host + o_val, sizeof(float) * (size_t)nprog * nrows);

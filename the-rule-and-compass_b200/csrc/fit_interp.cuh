@@ -7,17 +7,19 @@
  * like postfix bytecode. The host translates it once per batch into 8-byte
  * instructions: pushes of an input column or a constant slot, unary and
  * binary operators, and a binary operator fused with the push of its right
- * operand. The top of stack lives in registers (four rows per thread,
- * `float4`), deeper entries in shared-memory spill slots fixed at decode time.
+ * operand. The top of stack lives in registers (four rows per thread),
+ * deeper entries in shared-memory spill slots fixed at decode time.
  *
- * The reverse sweep walks the instructions backwards and is the mirror of the
- * forward stack machine: an operator's adjoint arrives on top of stack, its
- * children's adjoints leave through the same spill slot and top of stack
- * their values used, so no per-node value tape is needed. Only the local
- * partial derivatives of non-linear operators are kept, in a per-thread
- * shared-memory tape (one slot per partial). A zero adjoint passes nothing
- * to its operands, as the reference's adjoint does (eval.cu:1245-1246,
- * fit.rs:1479-1481).
+ * The reverse sweep is the mirror of the forward stack machine: an
+ * operator's adjoint arrives on top of stack, its children's adjoints leave
+ * through the same spill slot and top of stack their values used, so no
+ * per-node value tape is needed. It runs over a second instruction list in
+ * which every subtree without a constant is collapsed to the restore of the
+ * adjoint below it (or dropped), since nothing in it has a constant to
+ * differentiate. Only the local partials that lie on a path from a constant
+ * to the root are kept, in a per-thread shared-memory tape. A zero adjoint
+ * passes nothing to its operands, as the reference's adjoint does
+ * (eval.cu:1245-1246, fit.rs:1479-1481).
  */
 #pragma once
 
@@ -26,7 +28,7 @@
 #include "rc_ops.cuh"
 
 enum FiKind {
-    FI_PUSH_VAR = 0,   /* spill TOS to `spill`; TOS = x[imm] */
+    FI_PUSH_VAR = 0,   /* spill TOS to `spill`; TOS = x[imm]. Reverse: restore only */
     FI_PUSH_PARAM = 1, /* spill TOS; TOS = c[imm] */
     FI_UNARY = 2,      /* TOS = op(TOS) */
     FI_BIN_S = 3,      /* TOS = op(slot[arg], TOS) */
@@ -35,8 +37,15 @@ enum FiKind {
     FI_HALT = 6
 };
 
+/* Flag bits above the kind: the left (or only) / right operand's subtree
+   holds a constant, and a reverse store that adds to an earlier one. */
+#define FI_KIND_MASK 7u
+#define FI_HP_L 8u
+#define FI_HP_R 16u
+#define FI_ACC 32u
+
 struct FIns {
-    uint8_t kind;
+    uint8_t kind;  /* FiKind | flags */
     uint8_t op;
     uint8_t arg;   /* spill slot of the left operand (FI_BIN_S) */
     uint8_t spill; /* slot a push spills TOS to, 0xff when the stack was empty */
@@ -45,20 +54,28 @@ struct FIns {
 };
 static_assert(sizeof(FIns) == 8, "FIns is 8 bytes");
 
-/* Partials an operator keeps for the reverse sweep: none for linear ones. */
-__host__ __device__ inline int fi_npartials(unsigned op, bool binary)
+__host__ __device__ constexpr bool fi_nonlinear(unsigned op)
 {
-    if (op == OP_ADD || op == OP_SUB || op == OP_NEG) return 0;
-    return binary ? 2 : 1;
+    return op != OP_ADD && op != OP_SUB && op != OP_NEG;
 }
 
-/* Host translation of one fit-record program. Returns false when the records
-   are not a tree in stack (post-) order, which the device path rejects. */
-inline bool fi_decode(const uint32_t *rec, int m, std::vector<FIns> &out, int *nslots, int *ntape)
+/* Host translation of one fit-record program into the forward list `fwd`
+   (ending in HALT) and the reverse list `rev` (walked last to first).
+   Returns false when the records are not a tree in stack (post-) order,
+   which the device path rejects. */
+inline bool fi_decode(const uint32_t *rec, int m, std::vector<FIns> &fwd, std::vector<FIns> &rev,
+                      int *nslots, int *ntape)
 {
-    std::vector<int> stack;
+    struct Ent {
+        int rec, first;
+        bool hp;
+    };
+    std::vector<Ent> stack;
+    std::vector<int> lo(m, 0), hi(m, -1), kid0(m, -1), kid1(m, -1);
+    std::vector<char> hp(m, 0), fused(m, 0);
     int depth = 0, maxslot = -1, tape = 0;
-    out.clear();
+    fwd.clear();
+    rev.clear();
     for (int i = 0; i < m; ++i) {
         const uint32_t op = rec[4 * i], k0 = rec[4 * i + 1], k1 = rec[4 * i + 2],
                        slot = rec[4 * i + 3];
@@ -78,38 +95,61 @@ inline bool fi_decode(const uint32_t *rec, int m, std::vector<FIns> &out, int *n
                 maxslot = maxslot > depth - 1 ? maxslot : depth - 1;
             }
             ++depth;
-            stack.push_back(i);
-            out.push_back(in);
+            hp[i] = op == OP_CONST;
+            lo[i] = (int)fwd.size();
+            stack.push_back({i, (int)fwd.size(), op == OP_CONST});
+            fwd.push_back(in);
+            hi[i] = lo[i];
         } else if (ft_op_binary(op)) {
-            if (stack.size() < 2 || stack[stack.size() - 1] != (int)k1 ||
-                stack[stack.size() - 2] != (int)k0)
+            if (stack.size() < 2 || stack[stack.size() - 1].rec != (int)k1 ||
+                stack[stack.size() - 2].rec != (int)k0)
                 return false;
+            const Ent L = stack[stack.size() - 2], R = stack[stack.size() - 1];
             stack.pop_back();
-            stack.back() = i;
-            in.kind = FI_BIN_S;
+            const bool h = L.hp || R.hp;
+            hp[i] = h;
+            kid0[i] = (int)k0;
+            kid1[i] = (int)k1;
+            unsigned flags = 0;
+            int np = 0;
+            if (h) {
+                flags = (L.hp ? FI_HP_L : 0u) | (R.hp ? FI_HP_R : 0u);
+                if (fi_nonlinear(op)) np = (L.hp ? 1 : 0) + (R.hp ? 1 : 0);
+            }
+            in.kind = (uint8_t)(FI_BIN_S | flags);
             in.arg = (uint8_t)(depth - 2);
             --depth;
-            const int np = fi_npartials(op, true);
-            FIns &prev = out.back();
-            if ((prev.kind == FI_PUSH_VAR || prev.kind == FI_PUSH_PARAM) && prev.spill == in.arg) {
+            FIns &prev = fwd.back();
+            const unsigned pk = prev.kind & FI_KIND_MASK;
+            if ((pk == FI_PUSH_VAR || pk == FI_PUSH_PARAM) && prev.spill == in.arg) {
                 /* fuse "push right operand; op" */
-                prev.kind = prev.kind == FI_PUSH_VAR ? FI_BIN_V : FI_BIN_P;
+                prev.kind = (uint8_t)((pk == FI_PUSH_VAR ? FI_BIN_V : FI_BIN_P) | flags);
                 prev.op = (uint8_t)op;
                 prev.spill = 0xff;
                 prev.tape = (uint16_t)tape;
+                fused[k1] = 1;
             } else {
-                out.push_back(in);
+                fwd.push_back(in);
             }
             tape += np;
+            lo[i] = L.first;
+            hi[i] = (int)fwd.size() - 1;
+            stack.back() = {i, L.first, h};
         } else {
-            if (stack.empty() || stack.back() != (int)k0) return false;
-            stack.back() = i;
-            in.kind = FI_UNARY;
-            tape += fi_npartials(op, false);
-            out.push_back(in);
+            if (stack.empty() || stack.back().rec != (int)k0) return false;
+            const Ent C = stack.back();
+            hp[i] = C.hp;
+            kid0[i] = (int)k0;
+            in.kind = (uint8_t)(FI_UNARY | (C.hp ? FI_HP_L : 0u));
+            if (C.hp && fi_nonlinear(op)) ++tape;
+            lo[i] = C.first;
+            fwd.push_back(in);
+            hi[i] = (int)fwd.size() - 1;
+            stack.back() = {i, C.first, C.hp};
         }
+        if (tape > 0xfff0) return false;
     }
-    if (stack.size() != 1 || stack[0] != m - 1) return false;
+    if (stack.size() != 1 || stack[0].rec != m - 1) return false;
     FIns h;
     h.kind = FI_HALT;
     h.op = 0;
@@ -117,192 +157,334 @@ inline bool fi_decode(const uint32_t *rec, int m, std::vector<FIns> &out, int *n
     h.spill = 0xff;
     h.imm = 0;
     h.tape = (uint16_t)tape;
-    out.push_back(h);
+    fwd.push_back(h);
     *nslots = maxslot + 1;
     *ntape = tape;
+
+    /* reverse list: maximal constant-free subtrees below a node with a
+       constant become a restore of the adjoint below them (the left operand
+       of a binary), or vanish (the right operand: its operator hands the left
+       adjoint on directly; a fused leaf has no instruction of its own) */
+    const int nf = (int)fwd.size() - 1;
+    std::vector<int> skip_to(nf, -1);
+    std::vector<char> emit(nf, 0);
+    for (int i = 0; i < m; ++i) {
+        if (!hp[i]) continue;
+        const int kids[2] = {kid0[i], kid1[i]};
+        for (int s = 0; s < 2; ++s) {
+            const int k = kids[s];
+            if (k < 0 || hp[k] || fused[k] || hi[k] < lo[k]) continue;
+            skip_to[lo[k]] = hi[k];
+            emit[lo[k]] = (s == 0 && fwd[lo[k]].spill != 0xff) ? 1 : 0;
+        }
+    }
+    if (hp[m - 1]) {
+        for (int j = 0; j < nf;) {
+            if (skip_to[j] >= 0) {
+                if (emit[j]) {
+                    FIns r = fwd[j];
+                    r.kind = FI_PUSH_VAR;
+                    rev.push_back(r);
+                }
+                j = skip_to[j] + 1;
+            } else {
+                rev.push_back(fwd[j]);
+                ++j;
+            }
+        }
+    }
+    /* a constant slot met again (in reverse order) accumulates */
+    std::vector<char> seen(65536, 0);
+    for (int j = (int)rev.size() - 1; j >= 0; --j) {
+        const unsigned k = rev[j].kind & FI_KIND_MASK;
+        if (k == FI_PUSH_PARAM || k == FI_BIN_P) {
+            if (seen[rev[j].imm]) rev[j].kind |= FI_ACC;
+            seen[rev[j].imm] = 1;
+        }
+    }
     return true;
 }
 
-/* f32 local partials of one operator (ft_partials_f semantics). A `pow`
-   with a non-positive base passes nothing. */
-__device__ __forceinline__ void fi_partials(unsigned op, float x, float y, float r, float &d0,
-                                            float &d1)
+/* Local partials of one operator (ft_partials_f / ft_partials_d semantics,
+   with the operator's value `r` reused where it is the same expression). A
+   `pow` with a non-positive base passes nothing. */
+template <typename V>
+__device__ __forceinline__ void fi_partials(unsigned op, V x, V y, V r, V &d0, V &d1)
 {
-    d0 = 0.0f;
-    d1 = 0.0f;
+    d0 = V(0);
+    d1 = V(0);
     switch (op) {
         case OP_EXP: d0 = r; break;
-        case OP_LOG: d0 = 1.0f / x; break;
-        case OP_ABS: d0 = x >= 0.0f ? 1.0f : -1.0f; break;
-        case OP_SQRT: d0 = 1.0f / (2.0f * r); break;
-        case OP_SIN: d0 = cosf(x); break;
-        case OP_COS: d0 = -sinf(x); break;
+        case OP_LOG: d0 = V(1) / x; break;
+        case OP_ABS: d0 = x >= V(0) ? V(1) : V(-1); break;
+        case OP_SQRT: d0 = V(1) / (V(2) * r); break;
+        case OP_SIN: d0 = cos(x); break;
+        case OP_COS: d0 = -sin(x); break;
         case OP_TAN: {
-            const float t = cosf(x);
-            d0 = 1.0f / (t * t);
+            const V t = cos(x);
+            d0 = V(1) / (t * t);
         } break;
-        case OP_SINH: d0 = coshf(x); break;
-        case OP_COSH: d0 = sinhf(x); break;
-        case OP_TANH: d0 = 1.0f - r * r; break;
-        case OP_SIG: d0 = r * (1.0f - r); break;
-        case OP_GAUSS: d0 = (-2.0f * x) * r; break;
-        case OP_SQUARE: d0 = 2.0f * x; break;
-        case OP_CUBE: d0 = 3.0f * x * x; break;
-        case OP_ERF: d0 = 1.1283791670955126f * expf(-x * x); break;
-        case OP_ERFC: d0 = -1.1283791670955126f * expf(-x * x); break;
+        case OP_SINH: d0 = cosh(x); break;
+        case OP_COSH: d0 = sinh(x); break;
+        case OP_TANH: d0 = V(1) - r * r; break;
+        case OP_SIG: d0 = r * (V(1) - r); break;
+        case OP_GAUSS: d0 = (V(-2) * x) * r; break;
+        case OP_SQUARE: d0 = V(2) * x; break;
+        case OP_CUBE: d0 = V(3) * x * x; break;
+        case OP_ERF: d0 = V(1.1283791670955126) * exp(-x * x); break;
+        case OP_ERFC: d0 = V(-1.1283791670955126) * exp(-x * x); break;
         case OP_MUL: d0 = y; d1 = x; break;
-        case OP_DIV: d0 = 1.0f / y; d1 = -x / (y * y); break;
+        case OP_DIV: d0 = V(1) / y; d1 = -x / (y * y); break;
         case OP_POW:
-            if (x > 0.0f) {
-                d0 = y * powf(x, y - 1.0f);
-                d1 = r * logf(x);
+            if (x > V(0)) {
+                d0 = y * pow(x, y - V(1));
+                d1 = r * log(x);
             }
             break;
         default: break;
     }
 }
 
-__device__ __forceinline__ float fi_child(float a, float d) { return a == 0.0f ? 0.0f : a * d; }
+/* Row lanes of a thread: four f32 rows (float4) or two f64 rows
+   (double2), 16 bytes either way. */
+template <typename V>
+struct FiV;
+template <>
+struct FiV<float> {
+    using V4 = float4;
+    static constexpr int NR = 4;
+    __device__ __forceinline__ static void unpack(const float4 &x, float *v)
+    {
+        v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+    }
+    __device__ __forceinline__ static float4 pack(const float *v)
+    {
+        return make_float4(v[0], v[1], v[2], v[3]);
+    }
+    __device__ __forceinline__ static float value(unsigned op, float a, float b)
+    {
+        return ft_value_f(op, a, b);
+    }
+};
+template <>
+struct FiV<double> {
+    using V4 = double2;
+    static constexpr int NR = 2;
+    __device__ __forceinline__ static void unpack(const double2 &x, double *v)
+    {
+        v[0] = x.x; v[1] = x.y;
+    }
+    __device__ __forceinline__ static double2 pack(const double *v) { return make_double2(v[0], v[1]); }
+    __device__ __forceinline__ static double value(unsigned op, double a, double b)
+    {
+        return ft_value_d(op, a, b);
+    }
+};
 
-/* Forward sweep of four rows. Constants from `cf`, inputs from the columns
-   at `row` (16-byte aligned). With PARTIALS, every non-linear operator stores
-   its partials in `tape` ([slot][T] float4). */
-template <int T, bool PARTIALS>
-__device__ __forceinline__ float4 fi_forward(const FIns *__restrict__ prog, const float *cf,
-                                             const float *__restrict__ cols, int npad, int row,
-                                             float4 *stk, float4 *tape, int tid)
+template <typename V>
+__device__ __forceinline__ V fi_child(V a, V d)
 {
-    float t0 = 0.f, t1 = 0.f, t2 = 0.f, t3 = 0.f;
+    return a == V(0) ? V(0) : a * d;
+}
+
+/* One operator on the thread's rows: values, and with PARTIALS the
+   partials the instruction keeps. The operator is a compile-time constant in
+   each case, so the value and partial switches fold away. */
+#define FI_OPN(OPC)                                                                   \
+    case OPC: {                                                                       \
+        _Pragma("unroll") for (int i = 0; i < NR; ++i) r[i] = F::value(OPC, a[i], b[i]); \
+        if (PARTIALS && fi_nonlinear(OPC) && (kind & (FI_HP_L | FI_HP_R))) {          \
+            V pl[NR], pr[NR];                                                         \
+            _Pragma("unroll") for (int i = 0; i < NR; ++i)                            \
+                fi_partials<V>(OPC, a[i], b[i], r[i], pl[i], pr[i]);                  \
+            int ts = in.tape;                                                         \
+            if (kind & FI_HP_L) {                                                     \
+                tape[(size_t)ts * S + tid] = F::pack(pl);                             \
+                ++ts;                                                                 \
+            }                                                                         \
+            if (kind & FI_HP_R) tape[(size_t)ts * S + tid] = F::pack(pr);             \
+        }                                                                             \
+    } break;
+
+/* Forward sweep of the thread's rows (four f32 or two f64). Constants from
+   `cf`, inputs from the columns at `row` (16-byte aligned). Spill slots and
+   the tape are [slot][S] 16-byte vectors with this thread at `tid`. The
+   prediction of row i is left in out[i]. */
+template <typename V, bool PARTIALS>
+__device__ __forceinline__ void fi_forward(const FIns *__restrict__ prog, const V *cf,
+                                           const V *__restrict__ cols, int npad, int row,
+                                           typename FiV<V>::V4 *stk, typename FiV<V>::V4 *tape,
+                                           int S, int tid, V *out)
+{
+    using F = FiV<V>;
+    using V4 = typename F::V4;
+    constexpr int NR = F::NR;
+    V t[NR];
+#pragma unroll
+    for (int i = 0; i < NR; ++i) t[i] = V(0);
     for (int pc = 0; pc < 512; ++pc) {
         const FIns in = prog[pc];
         const unsigned kind = in.kind;
-        if (kind <= FI_PUSH_PARAM) {
-            if (in.spill != 0xff) stk[in.spill * T + tid] = make_float4(t0, t1, t2, t3);
-            if (kind == FI_PUSH_VAR) {
-                const float4 x = __ldg(reinterpret_cast<const float4 *>(
-                    cols + (size_t)in.imm * (size_t)npad + row));
-                t0 = x.x; t1 = x.y; t2 = x.z; t3 = x.w;
+        const unsigned k = kind & FI_KIND_MASK;
+        if (k <= FI_PUSH_PARAM) {
+            if (in.spill != 0xff) stk[(size_t)in.spill * S + tid] = F::pack(t);
+            if (k == FI_PUSH_VAR) {
+                F::unpack(__ldg(reinterpret_cast<const V4 *>(cols + (size_t)in.imm * (size_t)npad + row)), t);
             } else {
-                const float c = cf[in.imm];
-                t0 = c; t1 = c; t2 = c; t3 = c;
+                const V c = cf[in.imm];
+#pragma unroll
+                for (int i = 0; i < NR; ++i) t[i] = c;
             }
             continue;
         }
-        if (kind == FI_UNARY) {
-            const float r0 = ft_value_f(in.op, t0, 0.f), r1 = ft_value_f(in.op, t1, 0.f);
-            const float r2 = ft_value_f(in.op, t2, 0.f), r3 = ft_value_f(in.op, t3, 0.f);
-            if (PARTIALS && in.op != OP_NEG) {
-                float d, z;
-                float4 dd;
-                fi_partials(in.op, t0, 0.f, r0, d, z); dd.x = d;
-                fi_partials(in.op, t1, 0.f, r1, d, z); dd.y = d;
-                fi_partials(in.op, t2, 0.f, r2, d, z); dd.z = d;
-                fi_partials(in.op, t3, 0.f, r3, d, z); dd.w = d;
-                tape[in.tape * T + tid] = dd;
+        if (k == FI_HALT) break;
+        V a[NR], b[NR];
+        if (k == FI_BIN_S) {
+            F::unpack(stk[(size_t)in.arg * S + tid], a);
+#pragma unroll
+            for (int i = 0; i < NR; ++i) b[i] = t[i];
+        } else {
+#pragma unroll
+            for (int i = 0; i < NR; ++i) {
+                a[i] = t[i];
+                b[i] = V(0);
             }
-            t0 = r0; t1 = r1; t2 = r2; t3 = r3;
-            continue;
+            if (k == FI_BIN_V) {
+                F::unpack(__ldg(reinterpret_cast<const V4 *>(cols + (size_t)in.imm * (size_t)npad + row)), b);
+            } else if (k == FI_BIN_P) {
+                const V c = cf[in.imm];
+#pragma unroll
+                for (int i = 0; i < NR; ++i) b[i] = c;
+            }
         }
-        if (kind <= FI_BIN_P) {
-            float a0, a1, a2, a3, b0, b1, b2, b3;
-            if (kind == FI_BIN_S) {
-                const float4 a = stk[in.arg * T + tid];
-                a0 = a.x; a1 = a.y; a2 = a.z; a3 = a.w;
-                b0 = t0; b1 = t1; b2 = t2; b3 = t3;
-            } else {
-                a0 = t0; a1 = t1; a2 = t2; a3 = t3;
-                if (kind == FI_BIN_V) {
-                    const float4 x = __ldg(reinterpret_cast<const float4 *>(
-                        cols + (size_t)in.imm * (size_t)npad + row));
-                    b0 = x.x; b1 = x.y; b2 = x.z; b3 = x.w;
-                } else {
-                    const float c = cf[in.imm];
-                    b0 = c; b1 = c; b2 = c; b3 = c;
+        V r[NR];
+        switch (in.op) {
+            FI_OPN(OP_ADD) FI_OPN(OP_SUB) FI_OPN(OP_MUL) FI_OPN(OP_DIV) FI_OPN(OP_POW)
+            FI_OPN(OP_SIN) FI_OPN(OP_COS) FI_OPN(OP_TAN) FI_OPN(OP_EXP) FI_OPN(OP_LOG)
+            FI_OPN(OP_SQRT) FI_OPN(OP_ABS) FI_OPN(OP_TANH) FI_OPN(OP_SIG) FI_OPN(OP_SQUARE)
+            FI_OPN(OP_CUBE) FI_OPN(OP_NEG) FI_OPN(OP_GAUSS) FI_OPN(OP_SINH) FI_OPN(OP_COSH)
+            FI_OPN(OP_ERF) FI_OPN(OP_ERFC)
+            default:
+#pragma unroll
+                for (int i = 0; i < NR; ++i) r[i] = V(NAN);
+                break;
+        }
+#pragma unroll
+        for (int i = 0; i < NR; ++i) t[i] = r[i];
+    }
+#pragma unroll
+    for (int i = 0; i < NR; ++i) out[i] = t[i];
+}
+#undef FI_OPN
+
+/* Reverse sweep of the thread's rows over the reverse list (`nr` entries,
+   walked from the last). The adjoints start at the rows' seeds `a`.
+   Constant adjoints are stored to g[slot * R + i * A] for row i (`g` is
+   this thread's first row). Returns whether every stored value is
+   finite. */
+template <typename V>
+__device__ __forceinline__ bool fi_reverse(const FIns *__restrict__ rev, int nr,
+                                           typename FiV<V>::V4 *stk,
+                                           const typename FiV<V>::V4 *tape, int S, int tid, V *g,
+                                           int R, int A, V *a)
+{
+    using F = FiV<V>;
+    constexpr int NR = F::NR;
+    bool fin = true;
+    for (int pc = nr - 1; pc >= 0; --pc) {
+        const FIns in = rev[pc];
+        const unsigned kind = in.kind;
+        const unsigned k = kind & FI_KIND_MASK;
+        if (k <= FI_PUSH_PARAM) {
+            if (k == FI_PUSH_PARAM) {
+                V *gs = g + (size_t)in.imm * R;
+#pragma unroll
+                for (int i = 0; i < NR; ++i) {
+                    const V v = (kind & FI_ACC) ? a[i] + gs[i * A] : a[i];
+                    gs[i * A] = v;
+                    fin = fin && isfinite(v);
                 }
             }
-            const float r0 = ft_value_f(in.op, a0, b0), r1 = ft_value_f(in.op, a1, b1);
-            const float r2 = ft_value_f(in.op, a2, b2), r3 = ft_value_f(in.op, a3, b3);
-            if (PARTIALS && in.op != OP_ADD && in.op != OP_SUB) {
-                float4 p0, p1;
-                fi_partials(in.op, a0, b0, r0, p0.x, p1.x);
-                fi_partials(in.op, a1, b1, r1, p0.y, p1.y);
-                fi_partials(in.op, a2, b2, r2, p0.z, p1.z);
-                fi_partials(in.op, a3, b3, r3, p0.w, p1.w);
-                tape[in.tape * T + tid] = p0;
-                tape[(in.tape + 1) * T + tid] = p1;
-            }
-            t0 = r0; t1 = r1; t2 = r2; t3 = r3;
+            if (in.spill != 0xff) F::unpack(stk[(size_t)in.spill * S + tid], a);
             continue;
         }
-        break; /* FI_HALT */
+        if (k == FI_UNARY) {
+            if (in.op == OP_NEG) {
+#pragma unroll
+                for (int i = 0; i < NR; ++i) a[i] = -a[i];
+            } else {
+                V d[NR];
+                F::unpack(tape[(size_t)in.tape * S + tid], d);
+#pragma unroll
+                for (int i = 0; i < NR; ++i) a[i] = fi_child(a[i], d[i]);
+            }
+            continue;
+        }
+        /* binary: left adjoint l, right adjoint r, for the sides with a
+           constant */
+        V l[NR], r[NR];
+        if (in.op == OP_ADD || in.op == OP_SUB) {
+            const bool sub = in.op == OP_SUB;
+#pragma unroll
+            for (int i = 0; i < NR; ++i) {
+                l[i] = a[i];
+                r[i] = sub ? -a[i] : a[i];
+            }
+        } else {
+            int ts = in.tape;
+#pragma unroll
+            for (int i = 0; i < NR; ++i) l[i] = r[i] = V(0);
+            if (kind & FI_HP_L) {
+                V d[NR];
+                F::unpack(tape[(size_t)ts * S + tid], d);
+#pragma unroll
+                for (int i = 0; i < NR; ++i) l[i] = fi_child(a[i], d[i]);
+                ++ts;
+            }
+            if (kind & FI_HP_R) {
+                V d[NR];
+                F::unpack(tape[(size_t)ts * S + tid], d);
+#pragma unroll
+                for (int i = 0; i < NR; ++i) r[i] = fi_child(a[i], d[i]);
+            }
+        }
+        if (k == FI_BIN_S) {
+            if ((kind & FI_HP_L) && (kind & FI_HP_R)) {
+                /* the left adjoint waits in its spill slot while the right
+                   subtree is walked; that subtree's first push restores it */
+                stk[(size_t)in.arg * S + tid] = F::pack(l);
+#pragma unroll
+                for (int i = 0; i < NR; ++i) a[i] = r[i];
+            } else if (kind & FI_HP_R) {
+#pragma unroll
+                for (int i = 0; i < NR; ++i) a[i] = r[i];
+            } else {
+#pragma unroll
+                for (int i = 0; i < NR; ++i) a[i] = l[i];
+            }
+        } else {
+            if (k == FI_BIN_P) {
+                V *gs = g + (size_t)in.imm * R;
+#pragma unroll
+                for (int i = 0; i < NR; ++i) {
+                    const V v = (kind & FI_ACC) ? r[i] + gs[i * A] : r[i];
+                    gs[i * A] = v;
+                    fin = fin && isfinite(v);
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < NR; ++i) a[i] = l[i];
+        }
     }
-    return make_float4(t0, t1, t2, t3);
+    return fin;
 }
 
-/* Reverse sweep of four rows (the instructions of `prog`, `nins` of them
-   including HALT). Constant adjoints are accumulated into g[i * gs + slot]
-   (f32) for row i of the thread: `g` points at the thread's first row. */
-template <int T>
-__device__ __forceinline__ void fi_reverse(const FIns *__restrict__ prog, int nins, float4 *stk,
-                                           const float4 *tape, float *g, int gs, int tid)
+/* D = A * B + D for one 8x8x4 f64 tile (mma.sync; A row-major, B
+   column-major). Lane (g = lane / 4, t = lane % 4) holds A[g][t], B[t][g]
+   and D[g][2t], D[g][2t + 1]. */
+__device__ __forceinline__ void fi_dmma(double &d0, double &d1, double a, double b)
 {
-    float a0 = 1.f, a1 = 1.f, a2 = 1.f, a3 = 1.f;
-    float *g0 = g;
-    for (int pc = nins - 2; pc >= 0; --pc) {
-        const FIns in = prog[pc];
-        const unsigned kind = in.kind;
-        if (kind <= FI_PUSH_PARAM) {
-            if (kind == FI_PUSH_PARAM) {
-                g0[in.imm] += a0;
-                g0[gs + in.imm] += a1;
-                g0[2 * gs + in.imm] += a2;
-                g0[3 * gs + in.imm] += a3;
-            }
-            if (in.spill != 0xff) {
-                const float4 s = stk[in.spill * T + tid];
-                a0 = s.x; a1 = s.y; a2 = s.z; a3 = s.w;
-            }
-            continue;
-        }
-        if (kind == FI_UNARY) {
-            if (in.op == OP_NEG) {
-                a0 = -a0; a1 = -a1; a2 = -a2; a3 = -a3;
-            } else {
-                const float4 d = tape[in.tape * T + tid];
-                a0 = fi_child(a0, d.x); a1 = fi_child(a1, d.y);
-                a2 = fi_child(a2, d.z); a3 = fi_child(a3, d.w);
-            }
-            continue;
-        }
-        /* binary: left adjoint (x) and right adjoint (y) */
-        float l0, l1, l2, l3, r0, r1, r2, r3;
-        if (in.op == OP_ADD) {
-            l0 = a0; l1 = a1; l2 = a2; l3 = a3;
-            r0 = a0; r1 = a1; r2 = a2; r3 = a3;
-        } else if (in.op == OP_SUB) {
-            l0 = a0; l1 = a1; l2 = a2; l3 = a3;
-            r0 = -a0; r1 = -a1; r2 = -a2; r3 = -a3;
-        } else {
-            const float4 p0 = tape[in.tape * T + tid];
-            const float4 p1 = tape[(in.tape + 1) * T + tid];
-            l0 = fi_child(a0, p0.x); l1 = fi_child(a1, p0.y);
-            l2 = fi_child(a2, p0.z); l3 = fi_child(a3, p0.w);
-            r0 = fi_child(a0, p1.x); r1 = fi_child(a1, p1.y);
-            r2 = fi_child(a2, p1.z); r3 = fi_child(a3, p1.w);
-        }
-        if (kind == FI_BIN_S) {
-            /* the left operand's adjoint waits in its spill slot; the right
-               operand's subtree is next */
-            stk[in.arg * T + tid] = make_float4(l0, l1, l2, l3);
-            a0 = r0; a1 = r1; a2 = r2; a3 = r3;
-        } else {
-            if (kind == FI_BIN_P) {
-                g0[in.imm] += r0;
-                g0[gs + in.imm] += r1;
-                g0[2 * gs + in.imm] += r2;
-                g0[3 * gs + in.imm] += r3;
-            }
-            a0 = l0; a1 = l1; a2 = l2; a3 = l3;
-        }
-    }
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
 }
