@@ -42,6 +42,7 @@
 
 #include "fit_common.cuh"
 #include "fit_interp.cuh"
+#include "fit_prep.h"
 
 #define FT_TILE_ROWS 4096
 #define FT_NBLK_MAX 21                     /* 4x4 blocks of a 24-wide augmented Gram */
@@ -285,16 +286,25 @@ __global__ void __launch_bounds__(T) ft_sweep(FitArgs a, int q)
 #define FT_ASM_T 128
 #define FT_ASM_BUDGET (48 * 1024)
 
+/* Rows per thread of each sweep: the assemblies carry 8 bytes of rows per
+   thread (two f32 or one f64 row) to fit more threads beside their tapes;
+   the objective sweeps, which keep no tape, carry 16 (four f32 or two f64
+   rows). */
+#define FT_ASM32_NR 2
+#define FT_ASM64_NR 1
+#define FT_LOSS32_NR 4
+#define FT_LOSS64_NR 2
+
 /* Per-candidate shared region of an assembly sweep at A active threads:
-   spill slots and partial tape ([slot][A] 16-byte vectors), then the
-   Jacobian rows column-major ([W8][NR * A + 4], W8 = p + 1 rounded up to 8;
-   NR = 4 f32 or 2 f64 rows per thread). A column stride of 4 mod 32 words
-   (f32) or 4 mod 16 words (f64) keeps both the per-thread stores of the
-   reverse sweep and the tensor-core fragment loads bank-conflict free. The
-   size is that of the f64 layout, the larger of the two. */
+   spill slots and partial tape ([slot][A] 8-byte row vectors), then the
+   Jacobian rows column-major ([W8][NR * A + 4], W8 = p + 1 rounded up to 8).
+   A column stride of 4 mod 32 words (f32) or 4 mod 16 doubles (f64) keeps
+   both the per-thread stores of the reverse sweep and the tensor-core
+   fragment loads bank-conflict free. The size is that of the f64 layout,
+   the larger of the two. */
 __host__ __device__ inline size_t ft_asm_region(int A, int slots, int tape, int W8)
 {
-    return 16 * (size_t)A * (size_t)(slots + tape) + 8 * (size_t)W8 * (2 * (size_t)A + 4);
+    return 8 * (size_t)A * (size_t)(slots + tape) + 8 * (size_t)W8 * ((size_t)A + 4);
 }
 
 /* Active threads of a candidate: the most (128, 64 or 32) whose region fits
@@ -409,11 +419,10 @@ __device__ __forceinline__ FtRow ft_row_f64(const FitArgs &a, int rr, int r1, do
 /* Fold the warp's NR * 32 rows of the column-major Jacobian into its
    J^T J | J^T r blocks with f64 tensor-core MMAs (f32 values widen
    exactly, so products are exact and sums f64). */
-template <int NB, typename V>
+template <int NB, typename V, int NR>
 __device__ __forceinline__ void ft_fold(const V *g, int R, int A, int w, int gid, int tig,
                                         double (*acc)[2])
 {
-    constexpr int NR = FiV<V>::NR;
 #pragma unroll 4
     for (int s = 0; s < 8 * NR; ++s) {
         const int q = 4 * s + tig;
@@ -435,14 +444,13 @@ __device__ __forceinline__ void ft_fold(const V *g, int R, int A, int w, int gid
    the warp's rows folded into the augmented Gram matrix. Warps work
    independently over their own rows; the tile's sum is a fixed-order sum
    over warps, written in the packed 4x4-block layout the controller reads. */
-template <typename V, int T>
+template <typename V, int NR, int T>
 __device__ void ft_tile_asm(const FitArgs &a, const FIns *fwd, const FIns *rev, int nr, int p,
                             int A, int slots, int ntape, const V *cv, unsigned char *region,
                             double *red, int r0, int r1, double *pt)
 {
-    using F = FiV<V>;
+    using F = FiV<V, NR>;
     using V4 = typename F::V4;
-    constexpr int NR = F::NR;
     constexpr bool F64 = sizeof(V) == 8;
     const int tid = threadIdx.x;
     const int lane = tid & 31, w = tid >> 5, gid = lane >> 2, tig = lane & 3;
@@ -464,7 +472,7 @@ __device__ void ft_tile_asm(const FitArgs &a, const FIns *fwd, const FIns *rev, 
         for (int base = r0; base < r1; base += NR * A) {
             const int row = base + NR * tid;
             V pr[NR];
-            fi_forward<V, true>(fwd, cv, cols, a.npad, row, stk, tape, A, tid, pr);
+            fi_forward<V, NR, true>(fwd, cv, cols, a.npad, row, stk, tape, A, tid, pr);
             FtRow rw[NR];
             V seed[NR];
             bool special = false;
@@ -475,7 +483,7 @@ __device__ void ft_tile_asm(const FitArgs &a, const FIns *fwd, const FIns *rev, 
                 seed[i] = (V)rw[i].seed;
                 special = special || rw[i].s_zero != 0.0f;
             }
-            const bool fin = fi_reverse<V>(rev, nr, stk, tape, A, tid, gt, R, A, seed);
+            const bool fin = fi_reverse<V, NR>(rev, nr, stk, tape, A, tid, gt, R, A, seed);
             if (!fin || special) {
                 /* rare rows: a non-finite Jacobian entry (the row is dropped
                    from the Jacobian; in f32 it counts as failed), or a zero
@@ -508,9 +516,9 @@ __device__ void ft_tile_asm(const FitArgs &a, const FIns *fwd, const FIns *rev, 
                 else if (rw[i].use) bad = 1;
             }
             __syncwarp();
-            if (NB <= 1) ft_fold<1, V>(g, R, A, w, gid, tig, acc);
-            else if (NB == 2) ft_fold<2, V>(g, R, A, w, gid, tig, acc);
-            else ft_fold<3, V>(g, R, A, w, gid, tig, acc);
+            if (NB <= 1) ft_fold<1, V, NR>(g, R, A, w, gid, tig, acc);
+            else if (NB == 2) ft_fold<2, V, NR>(g, R, A, w, gid, tig, acc);
+            else ft_fold<3, V, NR>(g, R, A, w, gid, tig, acc);
             __syncwarp();
         }
     }
@@ -518,7 +526,9 @@ __device__ void ft_tile_asm(const FitArgs &a, const FIns *fwd, const FIns *rev, 
     const int NBLK = NB * (NB + 1) / 2;
     double *gb = reinterpret_cast<double *>(region);
     if (tid < A) {
-        for (int b = 0; b < NBLK; ++b) {
+#pragma unroll
+        for (int b = 0; b < 6; ++b) {
+            if (b >= NBLK) break;
             gb[(size_t)(w * NBLK + b) * 64 + gid * 8 + 2 * tig] = acc[b][0];
             gb[(size_t)(w * NBLK + b) * 64 + gid * 8 + 2 * tig + 1] = acc[b][1];
         }
@@ -551,18 +561,17 @@ __device__ void ft_tile_asm(const FitArgs &a, const FIns *fwd, const FIns *rev, 
 
 /* Objective of one tile in f32 or f64 (eval.cu:1808-1855): the forward
    sweep only; a row that is not finite costs 1e30. */
-template <typename V, int T>
+template <typename V, int NR, int T>
 __device__ void ft_tile_loss(const FitArgs &a, const FIns *ins, const V *cv,
-                             typename FiV<V>::V4 *stk, double *red, int r0, int r1, double *pt)
+                             typename FiV<V, NR>::V4 *stk, double *red, int r0, int r1, double *pt)
 {
-    constexpr int NR = FiV<V>::NR;
     constexpr bool F64 = sizeof(V) == 8;
     const V *cols = F64 ? reinterpret_cast<const V *>(a.cols64) : reinterpret_cast<const V *>(a.cols);
     const int tid = threadIdx.x;
     double local = 0.0;
     for (int row = r0 + NR * tid; row < r1; row += NR * T) {
         V pr[NR];
-        fi_forward<V, false>(ins, cv, cols, a.npad, row, stk, nullptr, T, tid, pr);
+        fi_forward<V, NR, false>(ins, cv, cols, a.npad, row, stk, nullptr, T, tid, pr);
 #pragma unroll
         for (int i = 0; i < NR; ++i) {
             const int rr = row + i;
@@ -604,7 +613,11 @@ template <int OPK, int T>
 __global__ void __launch_bounds__(T) ft_sweep4(FitArgs a, int q)
 {
     using V = typename std::conditional<OPK == FOP_ASM64 || OPK == FOP_LOSS64, double, float>::type;
-    using V4 = typename FiV<V>::V4;
+    constexpr int NR = OPK == FOP_ASM32    ? FT_ASM32_NR
+                       : OPK == FOP_ASM64  ? FT_ASM64_NR
+                       : OPK == FOP_LOSS32 ? FT_LOSS32_NR
+                                           : FT_LOSS64_NR;
+    using V4 = typename FiV<V, NR>::V4;
     extern __shared__ __align__(16) unsigned char sm[];
     FIns *ins = reinterpret_cast<FIns *>(sm);
     V *cv = reinterpret_cast<V *>(sm + 8 * (size_t)((a.fmaxins + 1) & ~1));
@@ -640,10 +653,10 @@ __global__ void __launch_bounds__(T) ft_sweep4(FitArgs a, int q)
         const int r1 = min(a.n, r0 + FT_TILE_ROWS);
         double *pt = a.part + ((size_t)cand * a.ntiles + tile) * FT_PART_STRIDE;
         if (ft_op_assembles(OPK))
-            ft_tile_asm<V, T>(a, ins, ins + nf, nr, p, info.z, info.w & 0xffff, info.w >> 16, cv,
-                              region, red, r0, r1, pt);
+            ft_tile_asm<V, NR, T>(a, ins, ins + nf, nr, p, info.z, info.w & 0xffff, info.w >> 16,
+                                  cv, region, red, r0, r1, pt);
         else
-            ft_tile_loss<V, T>(a, ins, cv, reinterpret_cast<V4 *>(region), red, r0, r1, pt);
+            ft_tile_loss<V, NR, T>(a, ins, cv, reinterpret_cast<V4 *>(region), red, r0, r1, pt);
         __syncthreads();
     }
 }
@@ -1131,13 +1144,15 @@ __global__ void __launch_bounds__(T) ft_grad_kernel(FitArgs a, int want, int row
     }
 }
 
-/* Constant gradients of rows [row0, row0 + nrows) through the same
-   four-row forward and reverse sweeps as the f32 assembly, with adjoint
-   seed 1: one warp per (candidate, 128-row tile), tiles aligned down to a
-   multiple of four rows. */
+/* Constant gradients of rows [row0, row0 + nrows) through the same forward
+   and reverse sweeps as the f32 assembly (FT_ASM32_NR rows per thread), with
+   adjoint seed 1: one warp per (candidate, 32 * FT_ASM32_NR-row tile), tiles
+   aligned down to a multiple of FT_ASM32_NR rows. */
 __global__ void __launch_bounds__(32) ft_grad4_kernel(FitArgs a, int row0, int nrows, int ntiles,
                                                       float *value, float *out)
 {
+    constexpr int NR = FT_ASM32_NR;
+    using V4 = FiV<float, NR>::V4;
     extern __shared__ __align__(16) unsigned char smem[];
     const int cand = blockIdx.x / ntiles;
     const int tile = blockIdx.x % ntiles;
@@ -1148,21 +1163,22 @@ __global__ void __launch_bounds__(32) ft_grad4_kernel(FitArgs a, int row0, int n
     const int p = a.pcount[cand];
     FIns *ins = reinterpret_cast<FIns *>(smem);
     float *cf = reinterpret_cast<float *>(smem + 8 * (size_t)((a.fmaxins + 1) & ~1));
-    float4 *stk = reinterpret_cast<float4 *>(cf + FT_MAX_CONST);
-    float4 *tape = stk + (size_t)slots * 32;
+    V4 *stk = reinterpret_cast<V4 *>(cf + FT_MAX_CONST);
+    V4 *tape = stk + (size_t)slots * 32;
     float *g = reinterpret_cast<float *>(tape + (size_t)ntape * 32);
-    const int R = 4 * 32 + 4;
+    const int R = NR * 32 + 4;
     const int ib = a.fins_off[cand];
     for (int i = tid; i < nf + nr; i += 32) ins[i] = a.fins[ib + i];
     if (tid < p) cf[tid] = (float)a.c0[(size_t)cand * a.kmax + tid];
     for (int i = tid; i < p * R; i += 32) g[i] = 0.0f;
     __syncwarp();
-    const int row = (row0 & ~3) + tile * 128 + 4 * tid;
+    const int row = (row0 & ~(NR - 1)) + tile * 32 * NR + NR * tid;
     if (row >= row0 + nrows || row >= a.n) return;
-    float pr[4], seed[4] = {1.0f, 1.0f, 1.0f, 1.0f};
-    fi_forward<float, true>(ins, cf, a.cols, a.npad, row, stk, tape, 32, tid, pr);
-    fi_reverse<float>(ins + nf, nr, stk, tape, 32, tid, g + tid, R, 32, seed);
-    for (int i = 0; i < 4; ++i) {
+    float pr[NR], seed[NR];
+    for (int i = 0; i < NR; ++i) seed[i] = 1.0f;
+    fi_forward<float, NR, true>(ins, cf, a.cols, a.npad, row, stk, tape, 32, tid, pr);
+    fi_reverse<float, NR>(ins + nf, nr, stk, tape, 32, tid, g + tid, R, 32, seed);
+    for (int i = 0; i < NR; ++i) {
         const int rr = row + i;
         if (rr < row0 || rr >= row0 + nrows) continue;
         const size_t o = (size_t)cand * nrows + (rr - row0);
@@ -1301,19 +1317,10 @@ bool validate_records(const uint32_t *rec, int m, int p, int v)
     return parents[m - 1] == 0;
 }
 
-struct FitPrep {
-    std::vector<int> node_off, valid;
-    std::vector<FIns> fins;
-    std::vector<int> fins_off;
-    std::vector<int4> finfo;
-    size_t asm_region = 0;
-    int mmax = 1;
-    int pmax = 0;
-    int fslots = 1;
-    int ftape = 1;
-    int fmaxins = 2;
-};
 
+}  // namespace
+
+/* Decode and check a batch of fit-record programs for the device sweeps. */
 void prep_batch(const unsigned int *off, const unsigned int *prog, const int *pcount, int nprog,
                 int v, FitPrep &b)
 {
@@ -1360,6 +1367,8 @@ void prep_batch(const unsigned int *off, const unsigned int *prog, const int *pc
     b.fins_off[nprog] = (int)b.fins.size();
     if (b.fins.empty()) b.fins.resize(1);
 }
+
+namespace {
 
 int occupancy(const void *fn, int threads, size_t smem)
 {
@@ -1735,10 +1744,11 @@ int rc_grad_batch(void *ctx, const unsigned int *prog, const unsigned int *off, 
         a.finfo = reinterpret_cast<const int4 *>(dev + o_finfo);
         a.fmaxins = b.fmaxins;
         cudaMemcpyAsync(dev + io_end, stage.data(), stage.size(), cudaMemcpyHostToDevice, rc->s);
-        const int ntiles = ((row0 + nrows) - (row0 & ~3) + 127) / 128;
+        constexpr int NR = FT_ASM32_NR;
+        const int ntiles = ((row0 + nrows) - (row0 & ~(NR - 1)) + 32 * NR - 1) / (32 * NR);
         const size_t smem = 8 * (size_t)((b.fmaxins + 1) & ~1) + 4 * FT_MAX_CONST +
-                            16 * 32 * (size_t)(b.fslots + b.ftape) +
-                            4 * (size_t)(b.pmax > 0 ? b.pmax : 1) * (4 * 32 + 4);
+                            4 * NR * 32 * (size_t)(b.fslots + b.ftape) +
+                            4 * (size_t)(b.pmax > 0 ? b.pmax : 1) * (NR * 32 + 4);
         if (cudaFuncSetAttribute(ft_grad4_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem) != cudaSuccess) {
             cudaGetLastError();

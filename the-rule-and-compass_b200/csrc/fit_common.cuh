@@ -304,7 +304,7 @@ __device__ __forceinline__ void ft_syrk_finish(const Syrk &s, double acc[16], do
 
 /* ---- the damped solve (eval.cu:1873-1949 `ft_solve`) ----------------- */
 
-__device__ int ft_solve(const double *jtj, const double *jtr, double lambda, int p, double *delta,
+__device__ inline int ft_solve(const double *jtj, const double *jtr, double lambda, int p, double *delta,
                         double *L)
 {
     double dscale[FT_MAX_CONST];
@@ -369,7 +369,7 @@ __device__ int ft_solve(const double *jtj, const double *jtr, double lambda, int
 
 /* Gaussian elimination with partial pivoting on (A + lambda diag A + 1e-12 I)
    (implicit.rs:215-253). `M` is p x (p+1) scratch. Returns 0 or 1 (singular). */
-__device__ int ft_gauss_solve(const double *jtj, const double *jtr, double lambda, int p,
+__device__ inline int ft_gauss_solve(const double *jtj, const double *jtr, double lambda, int p,
                               double *delta, double *M)
 {
     const int w = p + 1;

@@ -1,13 +1,14 @@
 /*
- * Four-rows-per-thread stack interpreter for fit records, forward and
- * reverse.
+ * Multi-row stack interpreter for fit records, forward and reverse: each
+ * thread carries NR rows (f32 or f64) through one decode of every
+ * instruction.
  *
  * A fit-record program (post-order records [op, kid0, kid1, slot],
  * my-version/src/fit.rs:985-1056) of a tree is evaluated on a stack exactly
  * like postfix bytecode. The host translates it once per batch into 8-byte
  * instructions: pushes of an input column or a constant slot, unary and
  * binary operators, and a binary operator fused with the push of its right
- * operand. The top of stack lives in registers (four rows per thread),
+ * operand. The top of stack lives in registers (NR rows per thread),
  * deeper entries in shared-memory spill slots fixed at decode time.
  *
  * The reverse sweep is the mirror of the forward stack machine: an
@@ -23,6 +24,7 @@
  */
 #pragma once
 
+#include <cstring>
 #include <vector>
 
 #include "rc_ops.cuh"
@@ -245,39 +247,45 @@ __device__ __forceinline__ void fi_partials(unsigned op, V x, V y, V r, V &d0, V
     }
 }
 
-/* Row lanes of a thread: four f32 rows (float4) or two f64 rows
-   (double2), 16 bytes either way. */
-template <typename V>
-struct FiV;
-template <>
-struct FiV<float> {
-    using V4 = float4;
-    static constexpr int NR = 4;
-    __device__ __forceinline__ static void unpack(const float4 &x, float *v)
+/* The rows a thread carries: NR values of type V, moved as one 4-, 8- or
+   16-byte vector (spill slots, tape, column loads). */
+template <typename V, int NR>
+struct FiV {
+    struct alignas(sizeof(V) * NR) V4 {
+        V v[NR];
+    };
+    __device__ __forceinline__ static void unpack(const V4 &x, V *v)
     {
-        v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+#pragma unroll
+        for (int i = 0; i < NR; ++i) v[i] = x.v[i];
     }
-    __device__ __forceinline__ static float4 pack(const float *v)
+    __device__ __forceinline__ static V4 pack(const V *v)
     {
-        return make_float4(v[0], v[1], v[2], v[3]);
+        V4 x;
+#pragma unroll
+        for (int i = 0; i < NR; ++i) x.v[i] = v[i];
+        return x;
     }
-    __device__ __forceinline__ static float value(unsigned op, float a, float b)
+    /* read-only load of NR consecutive column values */
+    __device__ __forceinline__ static void ldg(const V *p, V *v)
     {
-        return ft_value_f(op, a, b);
+        V4 x;
+        if constexpr (sizeof(V4) == 16) {
+            const float4 t = __ldg(reinterpret_cast<const float4 *>(p));
+            memcpy(&x, &t, 16);
+        } else if constexpr (sizeof(V4) == 8) {
+            const float2 t = __ldg(reinterpret_cast<const float2 *>(p));
+            memcpy(&x, &t, 8);
+        } else {
+            const float t = __ldg(reinterpret_cast<const float *>(p));
+            memcpy(&x, &t, 4);
+        }
+        unpack(x, v);
     }
-};
-template <>
-struct FiV<double> {
-    using V4 = double2;
-    static constexpr int NR = 2;
-    __device__ __forceinline__ static void unpack(const double2 &x, double *v)
+    __device__ __forceinline__ static V value(unsigned op, V a, V b)
     {
-        v[0] = x.x; v[1] = x.y;
-    }
-    __device__ __forceinline__ static double2 pack(const double *v) { return make_double2(v[0], v[1]); }
-    __device__ __forceinline__ static double value(unsigned op, double a, double b)
-    {
-        return ft_value_d(op, a, b);
+        if constexpr (sizeof(V) == 8) return ft_value_d(op, a, b);
+        else return ft_value_f(op, a, b);
     }
 };
 
@@ -306,19 +314,17 @@ __device__ __forceinline__ V fi_child(V a, V d)
         }                                                                             \
     } break;
 
-/* Forward sweep of the thread's rows (four f32 or two f64). Constants from
-   `cf`, inputs from the columns at `row` (16-byte aligned). Spill slots and
-   the tape are [slot][S] 16-byte vectors with this thread at `tid`. The
-   prediction of row i is left in out[i]. */
-template <typename V, bool PARTIALS>
+/* Forward sweep of the thread's NR rows. Constants from `cf`, inputs from
+   the columns at `row` (aligned to the row vector). Spill slots and the tape
+   are [slot][S] row vectors with this thread at `tid`. The prediction of
+   row i is left in out[i]. */
+template <typename V, int NR, bool PARTIALS>
 __device__ __forceinline__ void fi_forward(const FIns *__restrict__ prog, const V *cf,
                                            const V *__restrict__ cols, int npad, int row,
-                                           typename FiV<V>::V4 *stk, typename FiV<V>::V4 *tape,
-                                           int S, int tid, V *out)
+                                           typename FiV<V, NR>::V4 *stk,
+                                           typename FiV<V, NR>::V4 *tape, int S, int tid, V *out)
 {
-    using F = FiV<V>;
-    using V4 = typename F::V4;
-    constexpr int NR = F::NR;
+    using F = FiV<V, NR>;
     V t[NR];
 #pragma unroll
     for (int i = 0; i < NR; ++i) t[i] = V(0);
@@ -329,7 +335,7 @@ __device__ __forceinline__ void fi_forward(const FIns *__restrict__ prog, const 
         if (k <= FI_PUSH_PARAM) {
             if (in.spill != 0xff) stk[(size_t)in.spill * S + tid] = F::pack(t);
             if (k == FI_PUSH_VAR) {
-                F::unpack(__ldg(reinterpret_cast<const V4 *>(cols + (size_t)in.imm * (size_t)npad + row)), t);
+                F::ldg(cols + (size_t)in.imm * (size_t)npad + row, t);
             } else {
                 const V c = cf[in.imm];
 #pragma unroll
@@ -350,7 +356,7 @@ __device__ __forceinline__ void fi_forward(const FIns *__restrict__ prog, const 
                 b[i] = V(0);
             }
             if (k == FI_BIN_V) {
-                F::unpack(__ldg(reinterpret_cast<const V4 *>(cols + (size_t)in.imm * (size_t)npad + row)), b);
+                F::ldg(cols + (size_t)in.imm * (size_t)npad + row, b);
             } else if (k == FI_BIN_P) {
                 const V c = cf[in.imm];
 #pragma unroll
@@ -382,14 +388,13 @@ __device__ __forceinline__ void fi_forward(const FIns *__restrict__ prog, const 
    Constant adjoints are stored to g[slot * R + i * A] for row i (`g` is
    this thread's first row). Returns whether every stored value is
    finite. */
-template <typename V>
+template <typename V, int NR>
 __device__ __forceinline__ bool fi_reverse(const FIns *__restrict__ rev, int nr,
-                                           typename FiV<V>::V4 *stk,
-                                           const typename FiV<V>::V4 *tape, int S, int tid, V *g,
-                                           int R, int A, V *a)
+                                           typename FiV<V, NR>::V4 *stk,
+                                           const typename FiV<V, NR>::V4 *tape, int S, int tid,
+                                           V *g, int R, int A, V *a)
 {
-    using F = FiV<V>;
-    constexpr int NR = F::NR;
+    using F = FiV<V, NR>;
     bool fin = true;
     for (int pc = nr - 1; pc >= 0; --pc) {
         const FIns in = rev[pc];

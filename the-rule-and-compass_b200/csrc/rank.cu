@@ -1,10 +1,739 @@
 /*
- * Exact statistics: rank sums, order statistics, maximum scan, autotune.
+ * Exact statistics over f64 predictions: rank-correlation sums
+ * (eval.cu:2888-3133, :4093-4361), order statistics of |r|
+ * (eval.cu:4365-4520, :4743-4850) and the maximum-error scan
+ * (eval.cu:4522-4740).
+ *
+ * Rank sums. A (candidate, trial) segment's f64 predictions over all n rows
+ * become order-preserving u64 keys (-0 folded onto +0, anything not finite
+ * onto the largest key). A segmented LSD radix sort (8-bit digits, a pass
+ * whose digit is constant over a segment skipped) orders them with the row
+ * as payload. One pass over the sorted keys then gives every position q its
+ * run [i, j) of equal keys, twice its centred average rank A = i + j - n,
+ * and the exact sums sum A * B[row] and sum A^2 in 128-bit integers, B being
+ * the target's own A (computed once per context the same way). Integer sums
+ * do not depend on order, so the result is bit-identical to the CPU's
+ * `RankTarget::sums` (metrics.rs:1359-1416) for the same predictions.
+ *
+ * Order statistics sort the bit patterns of |pred - y| (non-negative, so
+ * they order like the values) and pick the median or average the
+ * interquartile window by rank. The maximum scan is an integer max over the
+ * same patterns with the lowest attaining row, plus the per-row feasibility
+ * interval of a level along one constant (reverse sweep for dr/dc).
  */
+#include <algorithm>
 #include <cstring>
+#include <limits>
+#include <vector>
 
+#include "fit_common.cuh"
+#include "fit_prep.h"
 #include "rc_internal.h"
 #include "rc_ops.cuh"
+
+typedef unsigned long long u64;
+
+#define RS_T 256                  /* sort / contribution threads */
+#define RS_ITEMS 16               /* keys per thread */
+#define RS_TILE (RS_T * RS_ITEMS) /* keys per tile */
+#define RS_WARPS (RS_T / 32)
+#define RK_T 256                  /* key threads (two rows each per step) */
+#define RK_TILE 8192              /* rows per key block */
+#define RK_WAVE_BYTES ((size_t)3 << 30)
+
+/* ---- keys -------------------------------------------------------------- */
+
+/* Order-preserving key of an f64 (eval.cu:2921-2928 semantics): -0 shares
+   +0's key, NaN is the largest key. */
+__device__ __forceinline__ u64 rk_key(double v)
+{
+    if (v == 0.0) v = 0.0;
+    if (isnan(v)) return ~0ULL;
+    u64 b = (u64)__double_as_longlong(v);
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ULL);
+}
+
+__device__ __forceinline__ u64 rk_abs_key(double r) { return (u64)__double_as_longlong(fabs(r)); }
+
+__device__ __forceinline__ double rk_key_abs_value(u64 k) { return __longlong_as_double((long long)k); }
+
+enum { RK_RANK = 0, RK_ABS = 1 };
+
+/* Keys of segments [seg0, seg0 + gridDim.x / tiles) over all rows: the f64
+   forward sweep of the segment's candidate at its constants
+   (c0[seg * kmax + slot]), two rows per thread. RK_RANK keys the
+   prediction; RK_ABS keys |pred - y| and flags a row whose prediction is
+   not finite or exceeds 1e30 (eval.cu:4388-4418). A non-finite key marks
+   the segment's status 2. */
+template <int MODE>
+__global__ void __launch_bounds__(RK_T) rk_keys(const FIns *fins, const int *fins_off,
+                                                const int4 *finfo, const int *valid,
+                                                const double *c0, int kmax, const double *cols,
+                                                const double *y, int npad, int n, int ntrials,
+                                                int seg0, int tiles, int maxins, u64 *keys,
+                                                unsigned int *rows, int *status)
+{
+    using V4 = FiV<double, 2>::V4;
+    extern __shared__ __align__(16) unsigned char sm[];
+    FIns *ins = reinterpret_cast<FIns *>(sm);
+    double *cv = reinterpret_cast<double *>(sm + 8 * (size_t)((maxins + 1) & ~1));
+    V4 *stk = reinterpret_cast<V4 *>(cv + FT_MAX_CONST);
+    const int ls = blockIdx.x / tiles;
+    const int seg = seg0 + ls;
+    const int tile = blockIdx.x % tiles;
+    const int cand = seg / ntrials;
+    const int tid = threadIdx.x;
+    const bool ok = valid[cand] != 0;
+    const int nf = finfo[cand].x;
+    if (ok) {
+        for (int i = tid; i < nf; i += RK_T) ins[i] = fins[fins_off[cand] + i];
+        if (tid < FT_MAX_CONST) cv[tid] = tid < kmax ? c0[(size_t)seg * kmax + tid] : 0.0;
+    }
+    __syncthreads();
+    const int r0 = tile * RK_TILE, r1 = min(n, r0 + RK_TILE);
+    u64 *kseg = keys + (size_t)ls * n;
+    unsigned int *rseg = rows ? rows + (size_t)ls * n : nullptr;
+    bool bad = !ok;
+    for (int row = r0 + 2 * tid; row < r1; row += 2 * RK_T) {
+        double pr[2] = {CUDART_NAN, CUDART_NAN};
+        if (ok) fi_forward<double, 2, false>(ins, cv, cols, npad, row, stk, nullptr, RK_T, tid, pr);
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const int rr = row + i;
+            if (rr >= r1) continue;
+            u64 k;
+            if (MODE == RK_RANK) {
+                if (!isfinite(pr[i])) {
+                    k = ~0ULL;
+                    bad = true;
+                } else {
+                    k = rk_key(pr[i]);
+                }
+            } else {
+                const double r = pr[i] - y[rr];
+                if (!isfinite(pr[i]) || fabs(pr[i]) > 1e30 || !isfinite(r)) {
+                    k = ~0ULL;
+                    bad = true;
+                } else {
+                    k = rk_abs_key(r);
+                }
+            }
+            kseg[rr] = k;
+            if (rseg) rseg[rr] = (unsigned int)rr;
+        }
+    }
+    if (__syncthreads_or(bad) && tid == 0) status[seg] = 2;
+}
+
+/* Keys of the target (one segment). */
+__global__ void rk_target_keys(const double *y, int n, u64 *keys, unsigned int *rows)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        keys[i] = rk_key(y[i]);
+        rows[i] = (unsigned int)i;
+    }
+}
+
+/* ---- segmented LSD radix sort ------------------------------------------ */
+
+/* Per tile, the counts of the 8-bit digit at `shift`: hist[seg][tile][256]. A
+   warp takes 32 consecutive keys per round and adds each distinct digit
+   once. */
+__global__ void __launch_bounds__(RS_T) rs_hist(const u64 *ka, const u64 *kb,
+                                                const unsigned char *par, int n, int ntiles,
+                                                int shift, unsigned int *hist)
+{
+    __shared__ unsigned int cnt[256];
+    const int seg = blockIdx.x / ntiles, tile = blockIdx.x % ntiles;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const u64 *src = (par[seg] ? kb : ka) + (size_t)seg * n;
+    cnt[tid] = 0;
+    __syncthreads();
+    const int base = tile * RS_TILE + w * (RS_TILE / RS_WARPS);
+    for (int r = 0; r < RS_TILE / RS_WARPS / 32; ++r) {
+        const int idx = base + 32 * r + lane;
+        const bool in = idx < n;
+        const unsigned d = in ? (unsigned)(src[idx] >> shift) & 255u : 256u;
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        if (in && lane == __ffs(peers) - 1) atomicAdd(&cnt[d], (unsigned)__popc(peers));
+    }
+    __syncthreads();
+    hist[((size_t)seg * ntiles + tile) * 256 + tid] = cnt[tid];
+}
+
+/* Per segment, turn the tile counts into each (tile, digit)'s first output
+   position (digit-major, then tile order), in place. A digit that holds all
+   n keys leaves the order unchanged: the segment skips this pass. */
+__global__ void __launch_bounds__(256) rs_scan(unsigned int *hist, int n, int ntiles,
+                                               unsigned char *skip)
+{
+    __shared__ unsigned int wsum[8];
+    const int seg = blockIdx.x, d = threadIdx.x, lane = d & 31, w = d >> 5;
+    unsigned int *h = hist + (size_t)seg * ntiles * 256;
+    unsigned int total = 0;
+    for (int t = 0; t < ntiles; ++t) total += h[(size_t)t * 256 + d];
+    /* exclusive scan of the 256 digit totals */
+    unsigned int x = total;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[w] = x;
+    const int all = __syncthreads_or(total == (unsigned)n);
+    unsigned int before = 0;
+    for (int k = 0; k < w; ++k) before += wsum[k];
+    unsigned int off = before + x - total;
+    if (d == 0) skip[seg] = all ? 1 : 0;
+    for (int t = 0; t < ntiles; ++t) {
+        const unsigned int c = h[(size_t)t * 256 + d];
+        h[(size_t)t * 256 + d] = off;
+        off += c;
+    }
+}
+
+/* Stable scatter of one pass. Warp w owns 512 consecutive keys of the tile
+   and ranks each key among the warp's earlier keys of the same digit
+   (match_any per round of 32); the warps' digit counts are then scanned in
+   warp order, so the output keeps the input order inside a digit. */
+template <bool VALS>
+__global__ void __launch_bounds__(RS_T) rs_scatter(u64 *ka, u64 *kb, unsigned int *va,
+                                                   unsigned int *vb, const unsigned char *par,
+                                                   const unsigned char *skip,
+                                                   const unsigned int *hist, int n, int ntiles,
+                                                   int shift)
+{
+    __shared__ unsigned int cnt[RS_WARPS][256];
+    __shared__ unsigned int goff[256];
+    const int seg = blockIdx.x / ntiles, tile = blockIdx.x % ntiles;
+    if (skip[seg]) return;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const size_t sb = (size_t)seg * n;
+    const bool p = par[seg] != 0;
+    const u64 *src = (p ? kb : ka) + sb;
+    u64 *dst = (p ? ka : kb) + sb;
+    const unsigned int *vsrc = VALS ? (p ? vb : va) + sb : nullptr;
+    unsigned int *vdst = VALS ? (p ? va : vb) + sb : nullptr;
+#pragma unroll
+    for (int k = 0; k < RS_WARPS; ++k) cnt[k][tid] = 0;
+    goff[tid] = hist[((size_t)seg * ntiles + tile) * 256 + tid];
+    __syncthreads();
+    constexpr int R = RS_TILE / RS_WARPS / 32;
+    const int base = tile * RS_TILE + w * (RS_TILE / RS_WARPS);
+    const unsigned lt = (1u << lane) - 1u;
+    u64 key[R];
+    unsigned int val[R];
+    unsigned short rk[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int idx = base + 32 * r + lane;
+        const bool in = idx < n;
+        key[r] = in ? src[idx] : 0ULL;
+        val[r] = (VALS && in) ? vsrc[idx] : 0u;
+        const unsigned d = in ? (unsigned)(key[r] >> shift) & 255u : 256u;
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        rk[r] = in ? (unsigned short)(cnt[w][d] + __popc(peers & lt)) : 0;
+        __syncwarp();
+        if (in && lane == __ffs(peers) - 1) cnt[w][d] += __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    {
+        unsigned int run = 0;
+#pragma unroll
+        for (int k = 0; k < RS_WARPS; ++k) {
+            const unsigned int c = cnt[k][tid];
+            cnt[k][tid] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int idx = base + 32 * r + lane;
+        if (idx >= n) continue;
+        const unsigned d = (unsigned)(key[r] >> shift) & 255u;
+        const unsigned int pos = goff[d] + cnt[w][d] + rk[r];
+        dst[pos] = key[r];
+        if (VALS) vdst[pos] = val[r];
+    }
+}
+
+/* After a pass: a segment that moved now lives in the other buffer. */
+__global__ void rs_flip(unsigned char *par, const unsigned char *skip, int nseg)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < nseg && !skip[s]) par[s] ^= 1;
+}
+
+struct RsBuffers {
+    u64 *ka, *kb;
+    unsigned int *va, *vb;
+    unsigned int *hist;
+    unsigned char *par, *skip;
+};
+
+/* Sort `nseg` segments of n keys (with row payloads when VALS) in place
+   across the two buffers; par[seg] tells which holds the result. */
+template <bool VALS>
+void rs_sort(const RsBuffers &b, int nseg, int n, cudaStream_t s)
+{
+    const int ntiles = (n + RS_TILE - 1) / RS_TILE;
+    const unsigned grid = (unsigned)nseg * (unsigned)ntiles;
+    cudaMemsetAsync(b.par, 0, nseg, s);
+    for (int pass = 0; pass < 8; ++pass) {
+        const int shift = 8 * pass;
+        rs_hist<<<grid, RS_T, 0, s>>>(b.ka, b.kb, b.par, n, ntiles, shift, b.hist);
+        rs_scan<<<nseg, 256, 0, s>>>(b.hist, n, ntiles, b.skip);
+        rs_scatter<VALS><<<grid, RS_T, 0, s>>>(b.ka, b.kb, b.va, b.vb, b.par, b.skip, b.hist, n,
+                                               ntiles, shift);
+        rs_flip<<<(nseg + 255) / 256, 256, 0, s>>>(b.par, b.skip, nseg);
+    }
+}
+
+/* ---- runs and exact sums ----------------------------------------------- */
+
+/* Block exclusive max (forward) of an int over the 256 threads. */
+__device__ __forceinline__ int rk_excl_max(int v, int *sh)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x = max(x, y);
+    }
+    if (lane == 31) sh[w] = x;
+    __syncthreads();
+    int before = -1;
+    for (int k = 0; k < w; ++k) before = max(before, sh[k]);
+    int ex = __shfl_up_sync(0xffffffffu, x, 1);
+    if (lane == 0) ex = -1;
+    __syncthreads();
+    return max(before, ex);
+}
+
+/* Block exclusive min from the right of an int over the 256 threads. */
+__device__ __forceinline__ int rk_excl_min_right(int v, int *sh)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_down_sync(0xffffffffu, x, o);
+        if (lane + o < 32) x = min(x, y);
+    }
+    if (lane == 0) sh[w] = x;
+    __syncthreads();
+    int after = 0x7fffffff;
+    for (int k = w + 1; k < RS_WARPS; ++k) after = min(after, sh[k]);
+    int ex = __shfl_down_sync(0xffffffffu, x, 1);
+    if (lane == 31) ex = 0x7fffffff;
+    __syncthreads();
+    return min(after, ex);
+}
+
+/* First index in [lo, hi) whose key is >= k (keys sorted). */
+__device__ int rk_lower(const u64 *keys, int lo, int hi, u64 k)
+{
+    while (lo < hi) {
+        const int mid = lo + ((hi - lo) >> 1);
+        if (keys[mid] < k) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+/* First index in [lo, hi) whose key is > k (keys sorted), or hi. */
+__device__ int rk_upper(const u64 *keys, int lo, int hi, u64 k)
+{
+    while (lo < hi) {
+        const int mid = lo + ((hi - lo) >> 1);
+        if (keys[mid] <= k) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+enum { RK_SUMS = 0, RK_FILL = 1 };
+
+/* One tile of a sorted segment: every position's run [i, j) (block scans
+   of the run starts inside the tile; a binary search for a run that crosses
+   the tile's edge), A = i + j - n, and the tile's exact partial sums.
+   RK_SUMS: part = (sum A * B[row], sum A^2). RK_FILL (the target): B[row] = A
+   and part = (0, sum A^2). */
+template <int MODE>
+__global__ void __launch_bounds__(RS_T) rk_runs(const u64 *ka, const u64 *kb,
+                                                const unsigned int *va, const unsigned int *vb,
+                                                const unsigned char *par, int n, int ntiles,
+                                                const long long *B, long long *Bout,
+                                                __int128 *part)
+{
+    __shared__ int sh[RS_WARPS];
+    __shared__ int s_left, s_right;
+    __shared__ __int128 red[RS_T];
+    const int seg = blockIdx.x / ntiles, tile = blockIdx.x % ntiles;
+    const int tid = threadIdx.x;
+    const size_t sb = (size_t)seg * n;
+    const bool p = par[seg] != 0;
+    const u64 *keys = (p ? kb : ka) + sb;
+    const unsigned int *vals = (p ? vb : va) + sb;
+    const int t0 = tile * RS_TILE, t1 = min(n, t0 + RS_TILE);
+    const int q0 = t0 + tid * RS_ITEMS;
+    u64 k[RS_ITEMS];
+    bool f[RS_ITEMS];
+    u64 prev = (q0 > 0 && q0 < t1) ? keys[q0 - 1] : 0ULL;
+    int last = -1, first = 0x7fffffff;
+#pragma unroll
+    for (int j = 0; j < RS_ITEMS; ++j) {
+        const int q = q0 + j;
+        const bool in = q < t1;
+        k[j] = in ? keys[q] : 0ULL;
+        f[j] = in && (q == 0 || k[j] != prev);
+        prev = k[j];
+        if (f[j]) {
+            last = q;
+            first = min(first, q);
+        }
+    }
+    if (tid == 0) {
+        /* the run holding the tile's first position may start earlier; the
+           one holding its last position may end later */
+        const u64 kf = keys[t0], kl = keys[t1 - 1];
+        s_left = (t0 > 0 && keys[t0 - 1] == kf) ? rk_lower(keys, 0, t0, kf) : t0;
+        s_right = (t1 < n && keys[t1] == kl) ? rk_upper(keys, t1, n, kl) : t1;
+    }
+    const int ex_start = rk_excl_max(last, sh);
+    const int ex_end = rk_excl_min_right(first, sh);
+    const int start0 = ex_start >= 0 ? ex_start : s_left;
+    int end = ex_end != 0x7fffffff ? ex_end : s_right;
+    int st[RS_ITEMS];
+    {
+        int cur = start0;
+#pragma unroll
+        for (int j = 0; j < RS_ITEMS; ++j) {
+            if (f[j]) cur = q0 + j;
+            st[j] = cur;
+        }
+    }
+    __int128 ab = 0, aa = 0;
+#pragma unroll
+    for (int j = RS_ITEMS - 1; j >= 0; --j) {
+        const int q = q0 + j;
+        if (q < t1) {
+            const long long A = (long long)st[j] + (long long)end - (long long)n;
+            const unsigned int row = vals[q];
+            aa += (__int128)A * A;
+            if (MODE == RK_SUMS) ab += (__int128)A * B[row];
+            else Bout[row] = A;
+            if (f[j]) end = q;
+        }
+    }
+    /* fixed-order block sums (integers: exact in any order) */
+    red[tid] = ab;
+    __syncthreads();
+    if (tid == 0) {
+        __int128 s = 0;
+        for (int i = 0; i < RS_T; ++i) s += red[i];
+        part[((size_t)seg * ntiles + tile) * 2 + 0] = s;
+    }
+    __syncthreads();
+    red[tid] = aa;
+    __syncthreads();
+    if (tid == 0) {
+        __int128 s = 0;
+        for (int i = 0; i < RS_T; ++i) s += red[i];
+        part[((size_t)seg * ntiles + tile) * 2 + 1] = s;
+    }
+}
+
+/* Per segment: the tile partials summed into two 128-bit values, written as
+   (hi, lo) u64 pairs at out[4 * seg ...] (two's complement). */
+__global__ void rk_final(const __int128 *part, int ntiles, int nseg, u64 *out)
+{
+    const int seg = blockIdx.x * blockDim.x + threadIdx.x;
+    if (seg >= nseg) return;
+    __int128 ab = 0, aa = 0;
+    for (int t = 0; t < ntiles; ++t) {
+        ab += part[((size_t)seg * ntiles + t) * 2 + 0];
+        aa += part[((size_t)seg * ntiles + t) * 2 + 1];
+    }
+    const unsigned __int128 uab = (unsigned __int128)ab, uaa = (unsigned __int128)aa;
+    out[(size_t)seg * 4 + 0] = (u64)(uab >> 64);
+    out[(size_t)seg * 4 + 1] = (u64)uab;
+    out[(size_t)seg * 4 + 2] = (u64)(uaa >> 64);
+    out[(size_t)seg * 4 + 3] = (u64)uaa;
+}
+
+/* ---- order statistics --------------------------------------------------- */
+
+#define OS_T 256
+
+/* Median (what 0) or interquartile mean (what 1) of a sorted segment of
+   |r| patterns (eval.cu:4436-4520 semantics): the middle value or the mean of
+   the two middle values; the mean of ranks [n/4, 3n/4) (all rows below four)
+   as a fixed 256-thread strided sum and tree. */
+__global__ void __launch_bounds__(OS_T) os_pick(const u64 *ka, const u64 *kb,
+                                                const unsigned char *par, int n, int seg0,
+                                                int nseg, int what, const int *status,
+                                                double *out)
+{
+    __shared__ double part[OS_T];
+    const int ls = blockIdx.x;
+    const int seg = seg0 + ls;
+    const int tid = threadIdx.x;
+    if (ls >= nseg) return;
+    if (status[seg] != 0) {
+        if (tid == 0) out[seg] = CUDART_NAN;
+        return;
+    }
+    const u64 *k = (par[ls] ? kb : ka) + (size_t)ls * n;
+    if (what == 0) {
+        if (tid == 0)
+            out[seg] = (n & 1) ? rk_key_abs_value(k[n / 2])
+                               : 0.5 * (rk_key_abs_value(k[n / 2 - 1]) + rk_key_abs_value(k[n / 2]));
+        return;
+    }
+    const int lo = n < 4 ? 0 : n / 4, hi = n < 4 ? n : (3 * n) / 4;
+    double s = 0.0;
+    for (int i = lo + tid; i < hi; i += OS_T) s += rk_key_abs_value(k[i]);
+    part[tid] = s;
+    __syncthreads();
+    for (int st = OS_T / 2; st > 0; st >>= 1) {
+        if (tid < st) part[tid] += part[tid + st];
+        __syncthreads();
+    }
+    if (tid == 0) out[seg] = part[0] / (double)(hi - lo);
+}
+
+/* ---- maximum-error scan ------------------------------------------------- */
+
+#define MX_T 256
+
+/* One block per segment (eval.cu:4522-4640 semantics): rows tid, tid + 256,
+   ...; the integer max of the |r| patterns with the lowest attaining row;
+   with a coordinate and a finite level t, the intersection of the per-row
+   intervals {delta : |r + b delta| <= t}, b = dr/dc from the reverse sweep,
+   where a row with b = 0 only vetoes (|r| > t). A row that is not finite
+   stops the thread and marks the segment. */
+__global__ void __launch_bounds__(MX_T) mx_scan(const FIns *fins, const int *fins_off,
+                                                const int4 *finfo, const int *valid,
+                                                const int *pcount, const double *c0, int kmax,
+                                                const int *coords, const double *levels,
+                                                const double *cols, const double *y, int npad,
+                                                int n, int ntrials, int maxins, RcMaxOut *out)
+{
+    using V4 = FiV<double, 1>::V4;
+    extern __shared__ __align__(16) unsigned char sm[];
+    __shared__ u64 skey[MX_T];
+    __shared__ int srow[MX_T];
+    __shared__ double slo[MX_T], shi[MX_T];
+    __shared__ int sbad[MX_T];
+    const int seg = blockIdx.x;
+    const int tid = threadIdx.x;
+    const int cand = seg / ntrials;
+    const int4 info = finfo[cand];
+    const int nf = info.x, nr = info.y, slots = info.w & 0xffff, ntape = info.w >> 16;
+    const int p = pcount[cand];
+    FIns *ins = reinterpret_cast<FIns *>(sm);
+    double *cv = reinterpret_cast<double *>(sm + 8 * (size_t)((maxins + 1) & ~1));
+    V4 *stk = reinterpret_cast<V4 *>(cv + FT_MAX_CONST);
+    V4 *tape = stk + (size_t)slots * MX_T;
+    double *g = reinterpret_cast<double *>(tape + (size_t)ntape * MX_T);
+    const bool ok = valid[cand] != 0;
+    if (ok) {
+        for (int i = tid; i < nf + nr; i += MX_T) ins[i] = fins[fins_off[cand] + i];
+        if (tid < FT_MAX_CONST) cv[tid] = tid < kmax ? c0[(size_t)seg * kmax + tid] : 0.0;
+    }
+    __syncthreads();
+    const int coord = (coords && p > 0 && coords[seg] >= 0 && coords[seg] < p) ? coords[seg] : -1;
+    const double level = levels ? levels[seg] : CUDART_NAN;
+    const bool want = coord >= 0 && isfinite(level) && level >= 0.0;
+    u64 mykey = 0ULL;
+    int myrow = 0x7fffffff;
+    double mylo = -CUDART_INF, myhi = CUDART_INF;
+    int mybad = ok ? 0 : 1;
+    for (int row = tid; ok && row < n; row += MX_T) {
+        double pr;
+        if (want) fi_forward<double, 1, true>(ins, cv, cols, npad, row, stk, tape, MX_T, tid, &pr);
+        else fi_forward<double, 1, false>(ins, cv, cols, npad, row, stk, nullptr, MX_T, tid, &pr);
+        const double r = pr - y[row];
+        if (!isfinite(pr) || fabs(pr) > 1e30 || !isfinite(r)) {
+            mybad |= 1;
+            break;
+        }
+        const u64 key = rk_abs_key(r);
+        if (key > mykey || (key == mykey && row < myrow)) {
+            mykey = key;
+            myrow = row;
+        }
+        if (want && (mybad & 2) == 0) {
+            for (int j = 0; j < p; ++j) g[(size_t)j * MX_T + tid] = 0.0;
+            double seed = 1.0;
+            fi_reverse<double, 1>(ins + nf, nr, stk, tape, MX_T, tid, g + tid, MX_T, MX_T, &seed);
+            const double b = g[(size_t)coord * MX_T + tid];
+            if (!isfinite(b)) {
+                mybad |= 1;
+                break;
+            }
+            if (b == 0.0) {
+                if (fabs(r) > level) mybad |= 2;
+            } else {
+                const double e1 = (-level - r) / b;
+                const double e2 = (level - r) / b;
+                mylo = fmax(mylo, fmin(e1, e2));
+                myhi = fmin(myhi, fmax(e1, e2));
+            }
+        }
+    }
+    skey[tid] = mykey;
+    srow[tid] = myrow;
+    slo[tid] = mylo;
+    shi[tid] = myhi;
+    sbad[tid] = mybad;
+    __syncthreads();
+    for (int st = MX_T / 2; st > 0; st >>= 1) {
+        if (tid < st) {
+            const int j = tid + st;
+            if (skey[j] > skey[tid] || (skey[j] == skey[tid] && srow[j] < srow[tid])) {
+                skey[tid] = skey[j];
+                srow[tid] = srow[j];
+            }
+            slo[tid] = fmax(slo[tid], slo[j]);
+            shi[tid] = fmin(shi[tid], shi[j]);
+            sbad[tid] |= sbad[j];
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        const int bad = sbad[0];
+        RcMaxOut o;
+        o.status = (bad & 1) ? 2 : 0;
+        o.vmax = (bad & 1) ? CUDART_NAN : rk_key_abs_value(skey[0]);
+        o.row = (bad & 1) ? -1 : srow[0];
+        o.lo = (bad & 2) ? CUDART_INF : slo[0];
+        o.hi = (bad & 2) ? -CUDART_INF : shi[0];
+        out[seg] = o;
+    }
+}
+
+/* ---- host side -------------------------------------------------------- */
+
+namespace {
+
+size_t rs_bytes(size_t keys, int nseg, int n, bool vals)
+{
+    const size_t ntiles = (size_t)((n + RS_TILE - 1) / RS_TILE);
+    size_t s = 2 * sizeof(u64) * keys + (vals ? 2 * sizeof(unsigned int) * keys : 0);
+    s += sizeof(unsigned int) * 256 * ntiles * (size_t)nseg + 2 * (size_t)nseg + 512;
+    s += 2 * sizeof(__int128) * ntiles * (size_t)nseg;
+    return s;
+}
+
+/* Carve the sort buffers for `nseg` segments of n keys from `base` at *cur. */
+RsBuffers rs_carve(unsigned char *base, size_t *cur, int nseg, int n, bool vals, __int128 **part)
+{
+    const size_t keys = (size_t)nseg * n;
+    const size_t ntiles = (size_t)((n + RS_TILE - 1) / RS_TILE);
+    RsBuffers b;
+    b.ka = reinterpret_cast<u64 *>(base + rc_take(cur, sizeof(u64) * keys));
+    b.kb = reinterpret_cast<u64 *>(base + rc_take(cur, sizeof(u64) * keys));
+    b.va = vals ? reinterpret_cast<unsigned int *>(base + rc_take(cur, sizeof(unsigned int) * keys))
+                : nullptr;
+    b.vb = vals ? reinterpret_cast<unsigned int *>(base + rc_take(cur, sizeof(unsigned int) * keys))
+                : nullptr;
+    b.hist = reinterpret_cast<unsigned int *>(
+        base + rc_take(cur, sizeof(unsigned int) * 256 * ntiles * (size_t)nseg));
+    b.par = base + rc_take(cur, (size_t)nseg);
+    b.skip = base + rc_take(cur, (size_t)nseg);
+    *part = reinterpret_cast<__int128 *>(base + rc_take(cur, 2 * sizeof(__int128) * ntiles * nseg));
+    return b;
+}
+
+/* B (the target's doubled centred ranks) and sum B^2, once per context. */
+int rk_prepare(RcCtx *c)
+{
+    if (c->rank_ready) return 0;
+    if (c->n <= 1) return -1;
+    if (rc_ensure_f64(c) != 0) return -1;
+    const int n = c->n;
+    if (!c->d_rank_b && cudaMalloc((void **)&c->d_rank_b, sizeof(long long) * (size_t)n) != cudaSuccess) {
+        cudaGetLastError();
+        c->d_rank_b = nullptr;
+        return -1;
+    }
+    size_t cur = 0;
+    const size_t o_out = rc_take(&cur, sizeof(u64) * 4);
+    const size_t io_end = rc_take(&cur, 0);
+    const size_t work = cur;
+    if (rc_reserve(c, work + rs_bytes((size_t)n, 1, n, true) + 4096, io_end) != 0) return -1;
+    __int128 *part = nullptr;
+    size_t wc = work;
+    const RsBuffers b = rs_carve(c->dev, &wc, 1, n, true, &part);
+    const int ntiles = (n + RS_TILE - 1) / RS_TILE;
+    rk_target_keys<<<(n + 255) / 256, 256, 0, c->s>>>(c->d_y64, n, b.ka, b.va);
+    rs_sort<true>(b, 1, n, c->s);
+    rk_runs<RK_FILL><<<ntiles, RS_T, 0, c->s>>>(b.ka, b.kb, b.va, b.vb, b.par, n, ntiles, nullptr,
+                                                c->d_rank_b, part);
+    rk_final<<<1, 32, 0, c->s>>>(part, ntiles, 1, reinterpret_cast<u64 *>(c->dev + o_out));
+    cudaMemcpyAsync(c->host + o_out, c->dev + o_out, sizeof(u64) * 4, cudaMemcpyDeviceToHost, c->s);
+    if (rc_finish(c) != 0) return -1;
+    /* sum A^2 of the target is sum B^2 */
+    const u64 *h = reinterpret_cast<const u64 *>(c->host + o_out);
+    c->rank_bb[0] = h[2];
+    c->rank_bb[1] = h[3];
+    c->rank_ready = 1;
+    return 0;
+}
+
+struct StatPrep {
+    FitPrep b;
+    size_t o_fins, o_finsoff, o_finfo, o_valid, o_p, o_c0, in_end;
+};
+
+/* Upload the decoded programs and the per-segment constants. */
+void stat_inputs(RcCtx *c, const unsigned int *prog, const unsigned int *off, const int *pcount,
+                 int nsets, int nsegs, int kmax, const double *c0, size_t *cur, StatPrep &sp)
+{
+    prep_batch(off, prog, pcount, nsets, c->v, sp.b);
+    sp.o_fins = rc_take(cur, sizeof(FIns) * sp.b.fins.size());
+    sp.o_finsoff = rc_take(cur, sizeof(int) * (nsets + 1));
+    sp.o_finfo = rc_take(cur, sizeof(int4) * nsets);
+    sp.o_valid = rc_take(cur, sizeof(int) * nsets);
+    sp.o_p = rc_take(cur, sizeof(int) * nsets);
+    sp.o_c0 = rc_take(cur, sizeof(double) * (size_t)nsegs * kmax);
+    sp.in_end = rc_take(cur, 0);
+}
+
+void stat_copy(RcCtx *c, const int *pcount, int nsets, int nsegs, int kmax, const double *c0,
+               const StatPrep &sp)
+{
+    unsigned char *h = c->host;
+    memcpy(h + sp.o_fins, sp.b.fins.data(), sizeof(FIns) * sp.b.fins.size());
+    memcpy(h + sp.o_finsoff, sp.b.fins_off.data(), sizeof(int) * (nsets + 1));
+    memcpy(h + sp.o_finfo, sp.b.finfo.data(), sizeof(int4) * nsets);
+    memcpy(h + sp.o_valid, sp.b.valid.data(), sizeof(int) * nsets);
+    memcpy(h + sp.o_p, pcount, sizeof(int) * nsets);
+    memcpy(h + sp.o_c0, c0, sizeof(double) * (size_t)nsegs * kmax);
+    cudaMemcpyAsync(c->dev, h, sp.in_end, cudaMemcpyHostToDevice, c->s);
+}
+
+size_t key_smem(const StatPrep &sp)
+{
+    return 8 * (size_t)((sp.b.fmaxins + 1) & ~1) + 8 * FT_MAX_CONST +
+           16 * (size_t)(sp.b.fslots > 0 ? sp.b.fslots : 1) * RK_T;
+}
+
+/* Segments per wave so that a wave's sort buffers stay within the budget. */
+int wave_segments(int nsegs, int n, bool vals)
+{
+    const size_t per = rs_bytes((size_t)n, 1, n, vals);
+    size_t w = RK_WAVE_BYTES / (per ? per : 1);
+    if (w < 1) w = 1;
+    return (int)std::min<size_t>(w, (size_t)nsegs);
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -12,33 +741,201 @@ float rc_rank_score_batch(void *ctx, const unsigned int *prog, const unsigned in
                           const int *pcount, int nsets, int ntrials, int kmax, const double *c0,
                           unsigned long long *out, int *out_status, unsigned long long *out_bb)
 {
-    (void)ctx; (void)prog; (void)off; (void)pcount; (void)nsets; (void)ntrials; (void)kmax;
-    (void)c0; (void)out; (void)out_status; (void)out_bb;
-    return -1.0f;
+    RcCtx *c = (RcCtx *)ctx;
+    if (!c || !prog || !off || !pcount || !c0 || !out || !out_status || !out_bb) return -1.0f;
+    if (nsets <= 0 || ntrials <= 0 || kmax <= 0 || kmax > FT_MAX_CONST) return -1.0f;
+    if (c->n <= 1) return -1.0f;
+    const int n = c->n;
+    const long long total = (long long)nsets * ntrials * (long long)n;
+    if (total > 0x7fffffffLL) return -1.0f;
+    if (rk_prepare(c) != 0) return -1.0f;
+    const int nsegs = nsets * ntrials;
+    StatPrep sp;
+    size_t cur = 0;
+    stat_inputs(c, prog, off, pcount, nsets, nsegs, kmax, c0, &cur, sp);
+    const size_t o_out = rc_take(&cur, sizeof(u64) * 4 * (size_t)nsegs);
+    const size_t o_status = rc_take(&cur, sizeof(int) * (size_t)nsegs);
+    const size_t io_end = rc_take(&cur, 0);
+    const int wseg = wave_segments(nsegs, n, true);
+    const size_t work = cur;
+    if (rc_reserve(c, work + rs_bytes((size_t)wseg * n, wseg, n, true) + 4096, io_end) != 0)
+        return -1.0f;
+    stat_copy(c, pcount, nsets, nsegs, kmax, c0, sp);
+    unsigned char *dev = c->dev;
+    int *d_status = reinterpret_cast<int *>(dev + o_status);
+    cudaMemsetAsync(d_status, 0, sizeof(int) * nsegs, c->s);
+    const size_t smem = key_smem(sp);
+    if (smem > 48 * 1024 &&
+        cudaFuncSetAttribute(rk_keys<RK_RANK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess)
+        return -1.0f;
+    const int ktiles = (n + RK_TILE - 1) / RK_TILE;
+    const int ntiles = (n + RS_TILE - 1) / RS_TILE;
+    cudaEventRecord(c->t0, c->s);
+    for (int s0 = 0; s0 < nsegs; s0 += wseg) {
+        const int ns = std::min(wseg, nsegs - s0);
+        size_t wc = work;
+        __int128 *part = nullptr;
+        const RsBuffers b = rs_carve(dev, &wc, ns, n, true, &part);
+        rk_keys<RK_RANK><<<(unsigned)ns * ktiles, RK_T, smem, c->s>>>(
+            reinterpret_cast<const FIns *>(dev + sp.o_fins),
+            reinterpret_cast<const int *>(dev + sp.o_finsoff),
+            reinterpret_cast<const int4 *>(dev + sp.o_finfo),
+            reinterpret_cast<const int *>(dev + sp.o_valid),
+            reinterpret_cast<const double *>(dev + sp.o_c0), kmax, c->d_cols64, c->d_y64, c->npad,
+            n, ntrials, s0, ktiles, sp.b.fmaxins, b.ka, b.va, d_status);
+        rs_sort<true>(b, ns, n, c->s);
+        rk_runs<RK_SUMS><<<(unsigned)ns * ntiles, RS_T, 0, c->s>>>(
+            b.ka, b.kb, b.va, b.vb, b.par, n, ntiles, c->d_rank_b, nullptr, part);
+        rk_final<<<(ns + 127) / 128, 128, 0, c->s>>>(part, ntiles, ns,
+                                                     reinterpret_cast<u64 *>(dev + o_out) + 4 * (size_t)s0);
+    }
+    cudaEventRecord(c->t1, c->s);
+    if (cudaGetLastError() != cudaSuccess) return -1.0f;
+    cudaMemcpyAsync(c->host + sp.in_end, dev + sp.in_end, io_end - sp.in_end,
+                    cudaMemcpyDeviceToHost, c->s);
+    if (rc_finish(c) != 0) return -1.0f;
+    memcpy(out, c->host + o_out, sizeof(u64) * 4 * (size_t)nsegs);
+    memcpy(out_status, c->host + o_status, sizeof(int) * (size_t)nsegs);
+    out_bb[0] = c->rank_bb[0];
+    out_bb[1] = c->rank_bb[1];
+    float ms = -1.0f;
+    cudaEventElapsedTime(&ms, c->t0, c->t1);
+    return ms;
 }
 
 int rc_rank_debug_b(void *ctx, long long *out)
 {
-    (void)ctx; (void)out;
-    return -1;
+    RcCtx *c = (RcCtx *)ctx;
+    if (!c || !out) return -1;
+    if (rk_prepare(c) != 0) return -1;
+    if (cudaMemcpy(out, c->d_rank_b, sizeof(long long) * (size_t)c->n, cudaMemcpyDeviceToHost) !=
+        cudaSuccess)
+        return -1;
+    return 0;
 }
 
 float rc_order_stat_score_batch(void *ctx, const unsigned int *prog, const unsigned int *off,
                                 const int *pcount, int nsets, int ntrials, int kmax,
                                 const double *c0, int what, double *out_value, int *out_status)
 {
-    (void)ctx; (void)prog; (void)off; (void)pcount; (void)nsets; (void)ntrials; (void)kmax;
-    (void)c0; (void)what; (void)out_value; (void)out_status;
-    return -1.0f;
+    RcCtx *c = (RcCtx *)ctx;
+    if (!c || !prog || !off || !pcount || !c0 || !out_value || !out_status) return -1.0f;
+    if (nsets <= 0 || ntrials <= 0 || kmax <= 0 || kmax > FT_MAX_CONST) return -1.0f;
+    if (what != 0 && what != 1) return -1.0f;
+    if (c->n <= 0) return -1.0f;
+    const int n = c->n;
+    const long long total = (long long)nsets * ntrials * (long long)n;
+    if (total > 0x7fffffffLL) return -1.0f;
+    if (rc_ensure_f64(c) != 0) return -1.0f;
+    const int nsegs = nsets * ntrials;
+    StatPrep sp;
+    size_t cur = 0;
+    stat_inputs(c, prog, off, pcount, nsets, nsegs, kmax, c0, &cur, sp);
+    const size_t o_val = rc_take(&cur, sizeof(double) * (size_t)nsegs);
+    const size_t o_status = rc_take(&cur, sizeof(int) * (size_t)nsegs);
+    const size_t io_end = rc_take(&cur, 0);
+    const int wseg = wave_segments(nsegs, n, false);
+    const size_t work = cur;
+    if (rc_reserve(c, work + rs_bytes((size_t)wseg * n, wseg, n, false) + 4096, io_end) != 0)
+        return -1.0f;
+    stat_copy(c, pcount, nsets, nsegs, kmax, c0, sp);
+    unsigned char *dev = c->dev;
+    int *d_status = reinterpret_cast<int *>(dev + o_status);
+    cudaMemsetAsync(d_status, 0, sizeof(int) * nsegs, c->s);
+    const size_t smem = key_smem(sp);
+    if (smem > 48 * 1024 &&
+        cudaFuncSetAttribute(rk_keys<RK_ABS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess)
+        return -1.0f;
+    const int ktiles = (n + RK_TILE - 1) / RK_TILE;
+    cudaEventRecord(c->t0, c->s);
+    for (int s0 = 0; s0 < nsegs; s0 += wseg) {
+        const int ns = std::min(wseg, nsegs - s0);
+        size_t wc = work;
+        __int128 *part = nullptr;
+        const RsBuffers b = rs_carve(dev, &wc, ns, n, false, &part);
+        rk_keys<RK_ABS><<<(unsigned)ns * ktiles, RK_T, smem, c->s>>>(
+            reinterpret_cast<const FIns *>(dev + sp.o_fins),
+            reinterpret_cast<const int *>(dev + sp.o_finsoff),
+            reinterpret_cast<const int4 *>(dev + sp.o_finfo),
+            reinterpret_cast<const int *>(dev + sp.o_valid),
+            reinterpret_cast<const double *>(dev + sp.o_c0), kmax, c->d_cols64, c->d_y64, c->npad,
+            n, ntrials, s0, ktiles, sp.b.fmaxins, b.ka, nullptr, d_status);
+        rs_sort<false>(b, ns, n, c->s);
+        os_pick<<<ns, OS_T, 0, c->s>>>(b.ka, b.kb, b.par, n, s0, ns, what, d_status,
+                                       reinterpret_cast<double *>(dev + o_val));
+    }
+    cudaEventRecord(c->t1, c->s);
+    if (cudaGetLastError() != cudaSuccess) return -1.0f;
+    cudaMemcpyAsync(c->host + sp.in_end, dev + sp.in_end, io_end - sp.in_end,
+                    cudaMemcpyDeviceToHost, c->s);
+    if (rc_finish(c) != 0) return -1.0f;
+    memcpy(out_value, c->host + o_val, sizeof(double) * (size_t)nsegs);
+    memcpy(out_status, c->host + o_status, sizeof(int) * (size_t)nsegs);
+    float ms = -1.0f;
+    cudaEventElapsedTime(&ms, c->t0, c->t1);
+    return ms;
 }
 
 float rc_max_scan_batch(void *ctx, const unsigned int *prog, const unsigned int *off,
                         const int *pcount, int nsets, int ntrials, int kmax, const double *c0,
                         const int *coords, const double *levels, RcMaxOut *out)
 {
-    (void)ctx; (void)prog; (void)off; (void)pcount; (void)nsets; (void)ntrials; (void)kmax;
-    (void)c0; (void)coords; (void)levels; (void)out;
-    return -1.0f;
+    RcCtx *c = (RcCtx *)ctx;
+    if (!c || !prog || !off || !pcount || !c0 || !out) return -1.0f;
+    if (nsets <= 0 || ntrials <= 0 || kmax <= 0 || kmax > FT_MAX_CONST) return -1.0f;
+    if (c->n <= 0) return -1.0f;
+    const int n = c->n;
+    const int nsegs = nsets * ntrials;
+    if ((long long)nsegs * (long long)n > 0x7fffffffLL) return -1.0f;
+    if (rc_ensure_f64(c) != 0) return -1.0f;
+    StatPrep sp;
+    size_t cur = 0;
+    stat_inputs(c, prog, off, pcount, nsets, nsegs, kmax, c0, &cur, sp);
+    const size_t o_coords = rc_take(&cur, sizeof(int) * (size_t)nsegs);
+    const size_t o_levels = rc_take(&cur, sizeof(double) * (size_t)nsegs);
+    const size_t in_end = rc_take(&cur, 0);
+    const size_t o_out = rc_take(&cur, sizeof(RcMaxOut) * (size_t)nsegs);
+    const size_t io_end = rc_take(&cur, 0);
+    if (rc_reserve(c, io_end, io_end) != 0) return -1.0f;
+    int *hc = reinterpret_cast<int *>(c->host + o_coords);
+    double *hl = reinterpret_cast<double *>(c->host + o_levels);
+    for (int s = 0; s < nsegs; ++s) {
+        hc[s] = coords ? coords[s] : -1;
+        hl[s] = (coords && levels) ? levels[s] : std::numeric_limits<double>::quiet_NaN();
+    }
+    stat_copy(c, pcount, nsets, nsegs, kmax, c0, sp);
+    cudaMemcpyAsync(c->dev + o_coords, c->host + o_coords, in_end - o_coords,
+                    cudaMemcpyHostToDevice, c->s);
+    unsigned char *dev = c->dev;
+    const int pmax = std::max(sp.b.pmax, 1);
+    const size_t smem = 8 * (size_t)((sp.b.fmaxins + 1) & ~1) + 8 * FT_MAX_CONST +
+                        8 * (size_t)MX_T * (sp.b.fslots + sp.b.ftape + pmax);
+    if (smem > 200 * 1024) return -1.0f;
+    if (smem > 48 * 1024 &&
+        cudaFuncSetAttribute(mx_scan, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess)
+        return -1.0f;
+    cudaEventRecord(c->t0, c->s);
+    mx_scan<<<nsegs, MX_T, smem, c->s>>>(
+        reinterpret_cast<const FIns *>(dev + sp.o_fins),
+        reinterpret_cast<const int *>(dev + sp.o_finsoff),
+        reinterpret_cast<const int4 *>(dev + sp.o_finfo),
+        reinterpret_cast<const int *>(dev + sp.o_valid), reinterpret_cast<const int *>(dev + sp.o_p),
+        reinterpret_cast<const double *>(dev + sp.o_c0), kmax,
+        reinterpret_cast<const int *>(dev + o_coords), reinterpret_cast<const double *>(dev + o_levels),
+        c->d_cols64, c->d_y64, c->npad, n, ntrials, sp.b.fmaxins,
+        reinterpret_cast<RcMaxOut *>(dev + o_out));
+    cudaEventRecord(c->t1, c->s);
+    if (cudaGetLastError() != cudaSuccess) return -1.0f;
+    cudaMemcpyAsync(c->host + o_out, dev + o_out, sizeof(RcMaxOut) * nsegs, cudaMemcpyDeviceToHost,
+                    c->s);
+    if (rc_finish(c) != 0) return -1.0f;
+    memcpy(out, c->host + o_out, sizeof(RcMaxOut) * (size_t)nsegs);
+    float ms = -1.0f;
+    cudaEventElapsedTime(&ms, c->t0, c->t1);
+    return ms;
 }
 
 int rc_autotune(void *ctx, const unsigned int *prog, const unsigned int *off, int nprog,

@@ -118,6 +118,12 @@ def _c(a, dt):
     return None if a is None else np.ascontiguousarray(a, dtype=dt)
 
 
+def _i128(hi, lo):
+    """Two's-complement 128-bit value from its (hi, lo) u64 halves."""
+    v = (int(hi) << 64) | int(lo)
+    return v - (1 << 128) if v >= 1 << 127 else v
+
+
 # Score objective codes (RC_SCORE_*, my-version/src/cuda/eval.cu:609-640).
 SCORE_SQUARED, SCORE_ABSOLUTE, SCORE_LOG_SQUASHED, SCORE_SIGNED, SCORE_MAXIMUM = 0, 1, 2, 3, 4
 SCORE_CORRELATION, SCORE_CORRELATION_SIGNED, SCORE_AIC, SCORE_AICC, SCORE_BIC = 5, 6, 7, 8, 9
@@ -284,6 +290,75 @@ class GpuEvaluator:
         if ms < 0:
             raise DeviceError("rc_implicit_score_batch failed")
         return out, status, ms
+
+    # -- exact statistics (my-version/src/gpu.rs:1986-2075, :2628-2838) ----
+    @staticmethod
+    def _segments(prog, off, pcount, c0, kmax, ntrials):
+        prog, off, pcount = _c(prog, np.uint32), _c(off, np.uint32), _c(pcount, np.int32)
+        nsets = len(off) - 1
+        c0 = _c(c0, np.float64).reshape(-1)
+        if c0.size != nsets * ntrials * kmax:
+            raise ValueError("c0 must hold nsets * ntrials * kmax constants")
+        return prog, off, pcount, c0, nsets
+
+    def rank_sums(self, prog, off, pcount, c0, kmax, ntrials=1):
+        """Exact rank sums per (set, trial) segment: a list of (ab, aa) Python
+        ints (None where status != 0), the statuses, sum B^2 and the ms."""
+        prog, off, pcount, c0, nsets = self._segments(prog, off, pcount, c0, kmax, ntrials)
+        nseg = nsets * ntrials
+        out = np.zeros(4 * nseg, np.uint64)
+        status = np.zeros(nseg, np.int32)
+        bb = np.zeros(2, np.uint64)
+        ms = lib().rc_rank_score_batch(self.ctx, _p(prog, ctypes.c_uint32),
+                                       _p(off, ctypes.c_uint32), _p(pcount, ctypes.c_int32),
+                                       nsets, ntrials, kmax, _p(c0, ctypes.c_double),
+                                       _p(out, ctypes.c_uint64), _p(status, ctypes.c_int32),
+                                       _p(bb, ctypes.c_uint64))
+        if ms < 0:
+            raise DeviceError("rc_rank_score_batch failed")
+        sums = []
+        for s in range(nseg):
+            if status[s] != 0:
+                sums.append(None)
+            else:
+                sums.append((_i128(out[4 * s], out[4 * s + 1]), _i128(out[4 * s + 2], out[4 * s + 3])))
+        return sums, status, _i128(bb[0], bb[1]), ms
+
+    def rank_target(self):
+        out = np.zeros(self.n, np.int64)
+        if lib().rc_rank_debug_b(self.ctx, _p(out, ctypes.c_int64)) != 0:
+            raise DeviceError("rc_rank_debug_b failed")
+        return out
+
+    def order_stat(self, prog, off, pcount, c0, kmax, what, ntrials=1):
+        """Exact median (what 0) or interquartile mean (what 1) of |r| per
+        segment, with statuses and the ms."""
+        prog, off, pcount, c0, nsets = self._segments(prog, off, pcount, c0, kmax, ntrials)
+        nseg = nsets * ntrials
+        val = np.zeros(nseg, np.float64)
+        status = np.zeros(nseg, np.int32)
+        ms = lib().rc_order_stat_score_batch(self.ctx, _p(prog, ctypes.c_uint32),
+                                             _p(off, ctypes.c_uint32), _p(pcount, ctypes.c_int32),
+                                             nsets, ntrials, kmax, _p(c0, ctypes.c_double), what,
+                                             _p(val, ctypes.c_double), _p(status, ctypes.c_int32))
+        if ms < 0:
+            raise DeviceError("rc_order_stat_score_batch failed")
+        return val, status, ms
+
+    def max_scan(self, prog, off, pcount, c0, kmax, ntrials=1, coords=None, levels=None):
+        """Exact max |r|, its lowest row and the level intervals per segment."""
+        prog, off, pcount, c0, nsets = self._segments(prog, off, pcount, c0, kmax, ntrials)
+        nseg = nsets * ntrials
+        out = (RcMaxOut * nseg)()
+        coords = _c(coords, np.int32)
+        levels = _c(levels, np.float64)
+        ms = lib().rc_max_scan_batch(self.ctx, _p(prog, ctypes.c_uint32), _p(off, ctypes.c_uint32),
+                                     _p(pcount, ctypes.c_int32), nsets, ntrials, kmax,
+                                     _p(c0, ctypes.c_double), _p(coords, ctypes.c_int32),
+                                     _p(levels, ctypes.c_double), out)
+        if ms < 0:
+            raise DeviceError("rc_max_scan_batch failed")
+        return [(o.vmax, o.row, o.lo, o.hi, o.status) for o in out], ms
 
     # -- telemetry -----------------------------------------------------
     def stats_begin(self):
