@@ -2,10 +2,16 @@
 
 Default workload (`--workload score`): batched evaluation + squared-error
 scoring of P = 4096 random expression programs over N = 1,048,576 rows x 5
-features (the batched-scoring configuration), metric expr*row evals/s.
-`--workload fit`: batched LM fit of P = 2048 candidates (1-20 constants,
-5-60 nodes, 20 iterations) over N = 262,144 rows x 8 features, metric fitted
-candidates/s.
+features (the batched-scoring configuration), metric expr*row evals/s. On one
+GPU the same line also carries, under "fit" and "rank", the second headline
+metric and the exact-statistics stage:
+  fit:  batched LM fit of P = 2048 candidates (1-20 constants, 5-60 nodes,
+        20 iterations) over N = 262,144 rows x 8 features, fitted
+        candidates/s, for the fused graph-replayed batch and for the plain
+        one-candidate-at-a-time form of the same steps (on a subset);
+  rank: exact rank-correlation sums of 64 candidates over N = 1,048,576 rows
+        x 10 features, candidate*rows/s.
+`--workload fit` makes the fit the primary line.
 
 One step is one pass of the hot path over the whole batch. `value` is
 device-timed with CUDA events on the library's stream (inputs resident in
@@ -224,6 +230,7 @@ def bench_score(args, rank, world, dev, pkg, W, flushbuf):
     dev_ms, wall = [], []
     import torch
     torch.cuda.synchronize()
+    n0 = ev.launch_count()
     with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clk:
         for _ in range(args.steps):
             flush_l2(flushbuf)
@@ -232,6 +239,7 @@ def bench_score(args, rank, world, dev, pkg, W, flushbuf):
             vals, status, ms = ev.score_batch(prog, off, 0, pcount)
             wall.append(time.perf_counter() - t0)
             dev_ms.append(ms)
+    launches = ev.launch_count() - n0
     stats = ev.last_stats()
     clocks = clk.summary()
     ev.close()
@@ -239,34 +247,125 @@ def bench_score(args, rank, world, dev, pkg, W, flushbuf):
     d2h = int(P * (8 + 4))
     return dict(P=P, N=N, dev_ms=dev_ms, wall=wall, alg_ops=alg_ops, clocks=clocks,
                 h2d=h2d, d2h=d2h, trees=trees, x=x, y=y, stats=stats,
-                launches_per_step=2, unit_count=float(P) * N)
+                launches=launches, unit_count=float(P) * N)
 
 
-def bench_fit(args, rank, world, dev, pkg, W, flushbuf):
-    P, N = args.P or 2048, args.N or 262144
+def fit_lane_ops(plans, N, iters):
+    """Algorithmic work of one fit in FP32-lane-op equivalents: per candidate,
+    iteration and row, 4.5 L FP32 ops (forward, reverse, trial forward;
+    L = records) plus p(p+1)/2 + p + 1 FP64 FMAs (Gram, rhs, loss) counted
+    twice (FP64 issues at half the FP32 rate)."""
+    fp32 = sum(4.5 * len(p.words) / 4 for p in plans) * iters * N
+    fp64 = sum(p.nconst * (p.nconst + 1) / 2 + p.nconst + 1 for p in plans) * iters * N
+    return fp32 + 2.0 * fp64
+
+
+def bench_fit(args, rank, world, dev, pkg, W, flushbuf, steps=None, warmup=None, plain=True):
+    P, N = (args.P if args.workload == "fit" and args.P else 2048), \
+        (args.N if args.workload == "fit" and args.N else 262144)
+    steps = args.steps if steps is None else steps
+    warmup = args.warmup if warmup is None else warmup
+    iters = 20
     trees, x, y = W.fit_workload(P, N, seed=rank)
     ev = pkg.GpuEvaluator(x.astype(np.float32).reshape(-1), N, x.shape[0], y.astype(np.float32))
     ev.set_fit_data(x.reshape(-1), y)
     plans = [pkg.gpu_fit_plan(t) for t in trees]
     prog, off, pcount, c0, gauge, kmax = pkg.pack_plans(plans)
-    for _ in range(args.warmup):
-        ev.fit_batch_fused(prog, off, pcount, c0, gauge, kmax, 20)
+    for _ in range(warmup):
+        ev.fit_batch_fused(prog, off, pcount, c0, gauge, kmax, iters)
     dev_ms, wall = [], []
     import torch
+    n0 = ev.launch_count()
     with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clk:
-        for _ in range(args.steps):
+        for _ in range(steps):
             flush_l2(flushbuf)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            _, _, st, ms = ev.fit_batch_fused(prog, off, pcount, c0, gauge, kmax, 20)
+            _, loss, st, ms = ev.fit_batch_fused(prog, off, pcount, c0, gauge, kmax, iters)
             wall.append(time.perf_counter() - t0)
             dev_ms.append(ms)
+    launches = ev.launch_count() - n0
     clocks = clk.summary()
+    out = dict(P=P, N=N, dev_ms=dev_ms, wall=wall, clocks=clocks, trees=trees, x=x, y=y,
+               launches=launches, unit_count=float(P),
+               lane_ops=fit_lane_ops(plans, N, iters),
+               status=np.bincount(st, minlength=9).tolist())
+    out["h2d"] = int(prog.nbytes + off.nbytes + pcount.nbytes + c0.nbytes + gauge.nbytes)
+    out["d2h"] = int(P * (kmax * 8 + 8 + 4))
+    if plain:
+        # the plain device form: the same step kernels, one candidate at a
+        # time, on a subset (its cost is linear in the candidate count)
+        S = min(32, P)
+        sp, so, spc, sc0, sg, _ = pkg.pack_plans(plans[:S], kmax)
+        ev.fit_batch_plain(sp, so, spc, sc0, sg, kmax, iters)
+        t0 = time.perf_counter()
+        _, ploss, pst, pms = ev.fit_batch_plain(sp, so, spc, sc0, sg, kmax, iters)
+        pwall = time.perf_counter() - t0
+        out["plain"] = {"value": S / (pms / 1e3), "unit": "candidates/s", "sample": S,
+                        "e2e": S / pwall,
+                        "same_losses": bool(np.array_equal(ploss.view(np.uint64),
+                                                           loss[:S].view(np.uint64)))}
     ev.close()
-    h2d = int(prog.nbytes + off.nbytes + pcount.nbytes + c0.nbytes + gauge.nbytes)
-    d2h = int(P * (kmax * 8 + 8 + 4))
-    return dict(P=P, N=N, dev_ms=dev_ms, wall=wall, clocks=clocks, h2d=h2d, d2h=d2h,
-                trees=trees, x=x, y=y, launches_per_step=4, unit_count=float(P))
+    return out
+
+
+def rank_data(n, seed=0):
+    """10 features (6 normal, 4 Student-t nu=3) and a heavy-tailed target
+    (y = 0.8 x0 / (1 + x1^2) + log(1 + |x3|) + 0.1 t3-noise)."""
+    rng = np.random.Generator(np.random.PCG64(seed + 5000))
+    x = np.concatenate([rng.standard_normal((6, n)), rng.standard_t(3.0, (4, n))])
+    y = 0.8 * x[0] / (1.0 + x[1] ** 2) + np.log1p(np.abs(x[3])) + 0.1 * rng.standard_t(3.0, n)
+    return x, y
+
+
+def bench_rank(args, rank, pkg, W, flushbuf, steps, warmup):
+    """Exact rank sums of 64 fit-style candidates over N = 1,048,576 rows."""
+    P, N = 64, 1 << 20
+    x, y = rank_data(N, seed=rank)
+    trees, _, _ = W.fit_workload(P, 16, seed=100 + rank, nvars=10)
+    ev = pkg.GpuEvaluator(x.astype(np.float32).reshape(-1), N, 10, y.astype(np.float32))
+    ev.set_fit_data(x.reshape(-1), y)
+    plans = [pkg.gpu_fit_plan(t) for t in trees]
+    prog, off, pcount, c0, gauge, kmax = pkg.pack_plans(plans)
+    ev.rank_target()
+    for _ in range(warmup):
+        ev.rank_sums(prog, off, pcount, c0, kmax)
+    import torch
+    dev_ms, wall = [], []
+    n0 = ev.launch_count()
+    for _ in range(steps):
+        flush_l2(flushbuf)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sums, status, bb, ms = ev.rank_sums(prog, off, pcount, c0, kmax)
+        wall.append(time.perf_counter() - t0)
+        dev_ms.append(ms)
+    launches = ev.launch_count() - n0
+    ev.close()
+    rows = float(P) * N
+    per = float(np.mean(dev_ms)) / 1e3
+    achieved = 32.0 * rows / per / 1e9
+    peak = load_peaks().get("hbm_gbs", 6650.0)
+    return {"metric": "rank_candidate_rows_per_s", "value": rows / per, "unit": "candidate*row/s",
+            "e2e": rows * steps / sum(wall), "ms_per_step": 1e3 * per, "launches": launches,
+            "finite_segments": int((status == 0).sum()),
+            "config": f"exact rank sums, P={P} candidates x 1 trial, N={N} rows x 10 features",
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "note": "algorithmic 32 B per candidate*row (f64 eval, 8 B key, 4 B "
+                                 "row, read back, 8 B gathered target rank) / event time; "
+                                 "peak = measured copy bandwidth (MEASURED_PEAKS.json)"}}
+
+
+def fit_roofline(r, peaks):
+    per = float(np.mean(r["dev_ms"])) / 1e3
+    achieved = r["lane_ops"] / per / 1e9
+    peak = 148 * 128 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e9
+    return {"bound": "fp32_issue", "achieved": achieved, "peak": peak, "unit": "Glane-op/s",
+            "frac": achieved / peak, "traffic": None,
+            "note": "sum over candidates of 20 iters x N x (4.5 L FP32 ops + 2 x (p(p+1)/2 + "
+                    "p + 1) FP64 FMAs), L = records, / event time of one fit; peak = 148 SMs x "
+                    "128 FP32 lanes x sm_max_mhz from MEASURED_PEAKS.json"}
 
 
 def main():
@@ -279,6 +378,8 @@ def main():
     ap.add_argument("--P", type=int, default=0)
     ap.add_argument("--N", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="skip the fit and rank measurements of the default line")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", 0))
@@ -332,7 +433,7 @@ def main():
                                f"features, squared error", "l2": "flushed between steps"}
         else:
             metric, unit = "fitted_candidates_per_s", "candidates/s"
-            roof = None
+            roof = fit_roofline(r, peaks)
             cfg = {"workload": f"batched LM fit, P={r['P']}, N={r['N']} rows x 8 features, "
                                f"20 iters, fused adjoint", "l2": "flushed between steps"}
         line = {"metric": metric, "value": value, "unit": unit, "n_gpus": world,
@@ -343,7 +444,11 @@ def main():
                 "clocks": r["clocks"],
                 "e2e": {"value": e2e, "unit": unit, "h2d_bytes_per_step": r["h2d"],
                         "d2h_bytes_per_step": r["d2h"]},
-                "gpu_launches": r["launches_per_step"] * args.steps}
+                "gpu_launches": r["launches"]}
+        if args.workload == "fit" and "plain" in r:
+            line["plain"] = r["plain"]
+            line["fused_over_plain"] = value / r["plain"]["value"]
+            line["fit_status_histogram"] = r["status"]
         if not args.no_cpu_baseline and world == 1:
             threads = os.cpu_count() or 1
             if args.workload == "score":
@@ -357,6 +462,18 @@ def main():
                                         "cores": threads, "kind": "port",
                                         "sample": "16 candidates x 16384 rows x 20 iters, "
                                                   "scaled linearly in rows"}
+        if args.workload == "score" and world == 1 and not args.no_secondary:
+            f = bench_fit(args, rank, world, local, pkg, W, flushbuf, steps=3, warmup=3)
+            fv = f["unit_count"] * len(f["dev_ms"]) / (sum(f["dev_ms"]) / 1e3)
+            line["fit"] = {
+                "metric": "fitted_candidates_per_s", "value": fv, "unit": "candidates/s",
+                "e2e": f["unit_count"] * len(f["wall"]) / sum(f["wall"]),
+                "ms_per_step": float(np.mean(f["dev_ms"])),
+                "config": f"batched LM fit, P={f['P']}, N={f['N']} rows x 8 features, 20 iters",
+                "plain": f["plain"], "fused_over_plain": fv / f["plain"]["value"],
+                "roofline": fit_roofline(f, peaks), "gpu_launches": f["launches"],
+                "status_histogram": f["status"], "clocks": f["clocks"]}
+            line["rank"] = bench_rank(args, rank, pkg, W, flushbuf, steps=3, warmup=3)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

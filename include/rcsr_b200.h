@@ -201,6 +201,10 @@ int rc_grad_batch(void *ctx, const unsigned int *prog, const unsigned int *off,
 float rc_implicit_score_batch(void *ctx, const unsigned int *prog, const unsigned int *off,
                               const int *pcount, int nprog, int kmax, const double *c,
                               double *out, int *status);
+/* Kernels this context has launched so far (a replayed fit graph counts its
+   kernel nodes). No counterpart in the reference: telemetry for callers that
+   check the device path really ran. Returns 0, or -1 on a null argument. */
+int rc_launch_count(void *ctx, unsigned long long *out);
 /* Autotune the scoring launch shape (candidates per work item, rows per work
    item) for this context's (N, feature count) and the length buckets of the
    staged program batch; the choice is cached per (N, V, bucket) and, when

@@ -6,6 +6,7 @@ non-finite -> +inf / status 2, composition-free bits, the device stack guard,
 and the f32-vs-f64 SSE agreement (relative error < 1e-4), plus a seeded
 random batch with the benchmark's tree distribution.
 """
+import importlib
 import math
 
 import numpy as np
@@ -244,3 +245,29 @@ def test_ill_conditioned_candidates_are_rescored_in_f64(pkg, E, O):
             if not cpu_bad:
                 assert abs(vals[k] - want) <= 1e-4 * abs(want) + 1e-12, (kind, k, vals[k], want)
     ev.close()
+
+
+def test_autotune_keeps_scores_bit_identical(pkg, tmp_path):
+    W = importlib.import_module("the-rule-and-compass_b200.workloads")
+    trees, x, y = W.scoring_workload(300, 50000, seed=7)
+    ev = pkg.GpuEvaluator(x.reshape(-1), 50000, 5, y)
+    pop = pkg.Population(trees)
+    prog, off = pop.programs()
+    pc = np.zeros(len(trees), np.int32)
+    before, st0, _ = ev.score_batch(prog, off, 0, pc)
+    path = str(tmp_path / "tune.txt")
+    k = ev.autotune(prog, off, path)
+    assert k >= 1
+    lines = open(path).read().split()
+    assert len(lines) == 4 * k and lines[0] == "50000" and lines[1] == "5"
+    after, st1, _ = ev.score_batch(prog, off, 0, pc)
+    assert np.array_equal(st0, st1)
+    assert np.array_equal(before.view(np.uint64), after.view(np.uint64))
+    # a second context reads the table instead of timing again
+    ev2 = pkg.GpuEvaluator(x.reshape(-1), 50000, 5, y)
+    assert ev2.autotune(prog, off, path) == k
+    n0 = ev.launch_count()
+    ev.score_batch(prog, off, 0, pc)
+    assert ev.launch_count() > n0
+    ev.close()
+    ev2.close()

@@ -107,6 +107,7 @@ int rc_ensure_f64(RcCtx *c)
         }
         c->alloc_calls++;
         if (total)
+            c->launches += 1;
             rc_cast_kernel<<<(unsigned)((total + 255) / 256), 256, 0, c->s>>>(c->d_cols, c->d_cols64,
                                                                              (long long)total);
     }
@@ -117,6 +118,7 @@ int rc_ensure_f64(RcCtx *c)
             return -1;
         }
         c->alloc_calls++;
+        c->launches += 1;
         rc_cast_kernel<<<(c->npad + 255) / 256, 256, 0, c->s>>>(c->d_y, c->d_y64, c->npad);
     }
     return cudaGetLastError() == cudaSuccess ? 0 : -1;

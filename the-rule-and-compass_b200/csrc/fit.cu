@@ -1429,8 +1429,8 @@ SweepLaunch sweep4_launch(RcCtx *c, const FitPrep &b, int Wmax)
 
 /* Enqueue the whole fit on the context stream: init, the bounded steps, the
    flush. */
-void enqueue_fit(cudaStream_t s_, int sm_count, const FitArgs &a, int steps,
-                 const SweepLaunch *sw, int nkinds)
+unsigned long long enqueue_fit(cudaStream_t s_, int sm_count, const FitArgs &a, int steps,
+                               const SweepLaunch *sw, int nkinds)
 {
     const int ctrl_grid = sm_count * 8;
     ft_step_reset<<<1, 32, 0, s_>>>(a, 1);
@@ -1447,6 +1447,7 @@ void enqueue_fit(cudaStream_t s_, int sm_count, const FitArgs &a, int steps,
         ft_control<<<ctrl_grid, FT_CTRL_T, 0, s_>>>(a, q, 0);
     }
     ft_flush<<<(a.nprog + 127) / 128, 128, 0, s_>>>(a);
+    return 3ULL + (unsigned long long)steps * (2ULL + (unsigned long long)nkinds);
 }
 
 float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const int *pcount,
@@ -1584,7 +1585,7 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
             one.outc = a.outc + (size_t)i * kmax;
             one.outsse = a.outsse + i;
             one.outstatus = a.outstatus + i;
-            enqueue_fit(c->s, c->sm_count, one, steps, sw, nk);
+            c->launches += enqueue_fit(c->s, c->sm_count, one, steps, sw, nk);
             ok = cudaGetLastError() == cudaSuccess;
         }
     } else {
@@ -1602,7 +1603,7 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
             cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
             ok = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
             if (ok) {
-                enqueue_fit(cap, c->sm_count, a, steps, sw, nk);
+                c->fit_graph_kernels = enqueue_fit(cap, c->sm_count, a, steps, sw, nk);
                 ok = cudaStreamEndCapture(cap, &g) == cudaSuccess && g;
             }
             if (ok) ok = cudaGraphInstantiate(&c->fit_graph, g, 0) == cudaSuccess;
@@ -1616,6 +1617,7 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
             }
         }
         if (ok) ok = cudaGraphLaunch(c->fit_graph, c->s) == cudaSuccess;
+        if (ok) c->launches += c->fit_graph_kernels;
     }
     cudaEventRecord(c->t1, c->s);
     st->launch_ms += rc_now_ms() - t;
@@ -1754,6 +1756,7 @@ int rc_grad_batch(void *ctx, const unsigned int *prog, const unsigned int *off, 
             cudaGetLastError();
             return -1;
         }
+        rc->launches += 1;
         ft_grad4_kernel<<<nprog * ntiles, 32, smem, rc->s>>>(
             a, row0, nrows, ntiles, reinterpret_cast<float *>(dev + o_val),
             reinterpret_cast<float *>(dev + o_out));
@@ -1768,6 +1771,7 @@ int rc_grad_batch(void *ctx, const unsigned int *prog, const unsigned int *off, 
         cudaGetLastError();
         return -1;
     }
+    rc->launches += 1;
     ft_grad_kernel<128><<<nprog * ntiles, T, smem, rc->s>>>(
         a, want, row0, nrows, ntiles, reinterpret_cast<float *>(dev + o_val),
         reinterpret_cast<float *>(dev + o_out));
@@ -1841,6 +1845,7 @@ float rc_implicit_score_batch(void *ctx, const unsigned int *prog, const unsigne
         return -1.0f;
     }
     cudaEventRecord(rc->t0, rc->s);
+    rc->launches += 2;
     ft_implicit_score_kernel<128><<<nprog * ntiles, T, smem, rc->s>>>(
         a, ntiles, rows_per_tile, reinterpret_cast<double *>(dev + o_part),
         reinterpret_cast<int *>(dev + o_bad));

@@ -276,7 +276,7 @@ struct RsBuffers {
 /* Sort `nseg` segments of n keys (with row payloads when VALS) in place
    across the two buffers; par[seg] tells which holds the result. */
 template <bool VALS>
-void rs_sort(const RsBuffers &b, int nseg, int n, cudaStream_t s)
+unsigned long long rs_sort(const RsBuffers &b, int nseg, int n, cudaStream_t s)
 {
     const int ntiles = (n + RS_TILE - 1) / RS_TILE;
     const unsigned grid = (unsigned)nseg * (unsigned)ntiles;
@@ -289,6 +289,7 @@ void rs_sort(const RsBuffers &b, int nseg, int n, cudaStream_t s)
                                                ntiles, shift);
         rs_flip<<<(nseg + 255) / 256, 256, 0, s>>>(b.par, b.skip, nseg);
     }
+    return 32;
 }
 
 /* ---- runs and exact sums ----------------------------------------------- */
@@ -672,7 +673,7 @@ int rk_prepare(RcCtx *c)
     const RsBuffers b = rs_carve(c->dev, &wc, 1, n, true, &part);
     const int ntiles = (n + RS_TILE - 1) / RS_TILE;
     rk_target_keys<<<(n + 255) / 256, 256, 0, c->s>>>(c->d_y64, n, b.ka, b.va);
-    rs_sort<true>(b, 1, n, c->s);
+    c->launches += 3 + rs_sort<true>(b, 1, n, c->s);
     rk_runs<RK_FILL><<<ntiles, RS_T, 0, c->s>>>(b.ka, b.kb, b.va, b.vb, b.par, n, ntiles, nullptr,
                                                 c->d_rank_b, part);
     rk_final<<<1, 32, 0, c->s>>>(part, ntiles, 1, reinterpret_cast<u64 *>(c->dev + o_out));
@@ -784,7 +785,7 @@ float rc_rank_score_batch(void *ctx, const unsigned int *prog, const unsigned in
             reinterpret_cast<const int *>(dev + sp.o_valid),
             reinterpret_cast<const double *>(dev + sp.o_c0), kmax, c->d_cols64, c->d_y64, c->npad,
             n, ntrials, s0, ktiles, sp.b.fmaxins, b.ka, b.va, d_status);
-        rs_sort<true>(b, ns, n, c->s);
+        c->launches += 3 + rs_sort<true>(b, ns, n, c->s);
         rk_runs<RK_SUMS><<<(unsigned)ns * ntiles, RS_T, 0, c->s>>>(
             b.ka, b.kb, b.va, b.vb, b.par, n, ntiles, c->d_rank_b, nullptr, part);
         rk_final<<<(ns + 127) / 128, 128, 0, c->s>>>(part, ntiles, ns,
@@ -862,7 +863,7 @@ float rc_order_stat_score_batch(void *ctx, const unsigned int *prog, const unsig
             reinterpret_cast<const int *>(dev + sp.o_valid),
             reinterpret_cast<const double *>(dev + sp.o_c0), kmax, c->d_cols64, c->d_y64, c->npad,
             n, ntrials, s0, ktiles, sp.b.fmaxins, b.ka, nullptr, d_status);
-        rs_sort<false>(b, ns, n, c->s);
+        c->launches += 2 + rs_sort<false>(b, ns, n, c->s);
         os_pick<<<ns, OS_T, 0, c->s>>>(b.ka, b.kb, b.par, n, s0, ns, what, d_status,
                                        reinterpret_cast<double *>(dev + o_val));
     }
@@ -918,6 +919,7 @@ float rc_max_scan_batch(void *ctx, const unsigned int *prog, const unsigned int 
             cudaSuccess)
         return -1.0f;
     cudaEventRecord(c->t0, c->s);
+    c->launches += 1;
     mx_scan<<<nsegs, MX_T, smem, c->s>>>(
         reinterpret_cast<const FIns *>(dev + sp.o_fins),
         reinterpret_cast<const int *>(dev + sp.o_finsoff),
@@ -938,11 +940,13 @@ float rc_max_scan_batch(void *ctx, const unsigned int *prog, const unsigned int 
     return ms;
 }
 
-int rc_autotune(void *ctx, const unsigned int *prog, const unsigned int *off, int nprog,
-                const char *path)
+int rc_launch_count(void *ctx, unsigned long long *out)
 {
-    (void)ctx; (void)prog; (void)off; (void)nprog; (void)path;
-    return -1;
+    RcCtx *c = (RcCtx *)ctx;
+    if (!c || !out) return -1;
+    *out = c->launches;
+    return 0;
 }
+
 
 }  // extern "C"

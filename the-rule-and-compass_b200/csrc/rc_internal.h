@@ -130,6 +130,10 @@ struct RcCtx {
     /* cached CUDA graph of the fused fit for a repeated batch shape */
     cudaGraphExec_t fit_graph;
     std::string fit_graph_key;
+    unsigned long long fit_graph_kernels; /* kernel nodes in one replay */
+
+    /* kernels this context has launched (graph replays count their nodes) */
+    unsigned long long launches;
 };
 
 double rc_now_ms();

@@ -27,6 +27,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <fstream>
 #include <mutex>
 #include <numeric>
 #include <vector>
@@ -360,8 +361,10 @@ float rc_score_run(RcCtx *c, const uint32_t *words, const uint32_t *off, int wid
             int grid = c->sm_count * occupancy_blocks(fn, T, smem);
             if (grid > a.nitems) grid = a.nitems;
             launch_score_kernel(T, track, grid, smem, c->s, a);
+            c->launches += 1;
             obase += nb;
         }
+        c->launches += 1;
         rc_score_finalize<<<(nprog + 127) / 128, 128, 0, c->s>>>(
             nprog, d_ctiles, a.part, ntiles, a.bad, c->n, (corr && pass == 1) ? mode : kmode,
             c->syy, d_out, d_status,
@@ -405,6 +408,7 @@ float rc_score_run(RcCtx *c, const uint32_t *words, const uint32_t *off, int wid
             if (pass == 1) cudaMemsetAsync(dev + o_bad64, 0, sizeof(int) * nprog, c->s);
             l.counter = d_cnt + 4 + pass;
             l.mode = kmode;
+            c->launches += 2;
             rc_score64_kernel<LANE_T><<<grid, LANE_T, smem, c->s>>>(l);
             rc_score64_finalize<<<(nprog + 127) / 128, 128, 0, c->s>>>(
                 l.flagged, d_nflag, ntiles, l.part, nprog, ntiles, l.bad, c->n,
@@ -630,6 +634,7 @@ extern "C" int rc_pool_hash(void *ctx, int which, int nprog, int width, unsigned
     size_t cur = 0;
     const size_t o = rc_take(&cur, sizeof(unsigned long long) * nprog);
     if (rc_reserve(c, cur, cur) != 0) return -1;
+    c->launches += 1;
     rc_hash_kernel<<<(nprog + 127) / 128, 128, 0, c->s>>>(
         c->d_pool[b], width, nprog, reinterpret_cast<unsigned long long *>(c->dev + o));
     cudaMemcpyAsync(c->host + o, c->dev + o, sizeof(unsigned long long) * nprog,
@@ -934,4 +939,83 @@ extern "C" int rc_score_batch_noalloc(const float *cols, const float *y, int n, 
         return -1;
     }
     return 0;
+}
+
+/* ---- launch-shape autotuner ------------------------------------------- */
+
+/* Candidates per work item (the group G) for each length bucket, chosen by
+   timing the scorer on the caller's batch: per bucket, every G in
+   {1, 2, 4, 8, 16, 32} is run three times after a warm-up on that bucket's
+   programs and the fastest median kept in the context. With a path, entries
+   for this (N, V) are read first (a bucket found there is not re-timed) and
+   the table is written back as lines "n v bucket group". */
+extern "C" int rc_autotune(void *ctx, const unsigned int *prog, const unsigned int *off, int nprog,
+                           const char *path)
+{
+    RcCtx *c = (RcCtx *)ctx;
+    if (!c || !prog || !off || nprog <= 0) return -1;
+    std::vector<int> have(2, 0);
+    std::vector<std::string> keep;
+    if (path) {
+        std::ifstream in(path);
+        long long n, v;
+        int b, g;
+        std::string line;
+        while (std::getline(in, line)) {
+            if (sscanf(line.c_str(), "%lld %lld %d %d", &n, &v, &b, &g) != 4) continue;
+            if (n == c->n && v == c->v && b >= 0 && b < 2 && g >= 1 && g <= 32) {
+                c->tune[b] = std::make_pair(g, 0);
+                have[b] = 1;
+            } else {
+                keep.push_back(line);
+            }
+        }
+    }
+    /* split the batch by bucket */
+    std::vector<uint32_t> words[2], offs[2];
+    offs[0].push_back(0);
+    offs[1].push_back(0);
+    std::vector<RcIns> tmp(RC_MAX_INS);
+    for (int i = 0; i < nprog; ++i) {
+        int ns = 0;
+        const int cnt = rc_decode_postfix(prog + off[i], off[i + 1] - off[i], c->v, tmp.data(), &ns);
+        if (cnt <= 0) continue;
+        const int b = ns <= RC_SHALLOW_SLOTS ? 0 : 1;
+        words[b].insert(words[b].end(), prog + off[i], prog + off[i + 1]);
+        offs[b].push_back((uint32_t)words[b].size());
+    }
+    for (int b = 0; b < 2; ++b) {
+        const int nb = (int)offs[b].size() - 1;
+        if (nb == 0 || have[b]) continue;
+        std::vector<double> out(nb);
+        std::vector<int> status(nb), pc(nb, 0);
+        std::vector<float> f32(nb);
+        int best_g = 8;
+        float best = 1e30f;
+        for (int g = 1; g <= 32; g *= 2) {
+            c->tune[b] = std::make_pair(g, 0);
+            float t[4];
+            bool ok = true;
+            for (int r = 0; r < 4 && ok; ++r) {
+                t[r] = rc_score_run(c, words[b].data(), offs[b].data(), 0, nb, SM_SQUARED, pc.data(),
+                                    out.data(), status.data(), f32.data(), nullptr);
+                ok = t[r] >= 0.0f;
+            }
+            if (!ok) continue;
+            std::sort(t + 1, t + 4);
+            if (t[2] < best) {
+                best = t[2];
+                best_g = g;
+            }
+        }
+        c->tune[b] = std::make_pair(best_g, 0);
+    }
+    if (path) {
+        std::ofstream o(path, std::ios::trunc);
+        for (const std::string &l : keep) o << l << "\n";
+        for (const auto &kv : c->tune)
+            o << c->n << " " << c->v << " " << kv.first << " " << kv.second.first << "\n";
+        if (!o) return -1;
+    }
+    return (int)c->tune.size();
 }

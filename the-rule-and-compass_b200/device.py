@@ -70,6 +70,7 @@ SIGNATURES = {
     "rc_fit_kernel_info": (ci, [ci, i32p, i32p, i32p]),
     "rc_rank_score_batch": (cf, [cvp, u32p, u32p, i32p, ci, ci, ci, f64p, u64p, i32p, u64p]),
     "rc_rank_debug_b": (ci, [cvp, i64p]),
+    "rc_launch_count": (ci, [cvp, u64p]),
     "rc_order_stat_score_batch": (cf, [cvp, u32p, u32p, i32p, ci, ci, ci, f64p, ci, f64p,
                                        i32p]),
     "rc_max_scan_batch": (cf, [cvp, u32p, u32p, i32p, ci, ci, ci, f64p, i32p, f64p,
@@ -368,6 +369,24 @@ class GpuEvaluator:
         s = RcStats()
         lib().rc_last_stats(self.ctx, ctypes.byref(s))
         return s
+
+    def autotune(self, prog, off, path=None):
+        """Time the scorer's candidates-per-item choice per length bucket on
+        this batch; returns the number of cached entries."""
+        prog, off = _c(prog, np.uint32), _c(off, np.uint32)
+        p = path.encode() if path else None
+        k = lib().rc_autotune(self.ctx, _p(prog, ctypes.c_uint32), _p(off, ctypes.c_uint32),
+                              len(off) - 1, p)
+        if k < 0:
+            raise DeviceError("rc_autotune failed")
+        return k
+
+    def launch_count(self):
+        """Kernels launched on this context so far."""
+        out = np.zeros(1, np.uint64)
+        if lib().rc_launch_count(self.ctx, _p(out, ctypes.c_uint64)) != 0:
+            raise DeviceError("rc_launch_count failed")
+        return int(out[0])
 
     def arena_report(self):
         r = RcArenaReport()
