@@ -320,7 +320,8 @@ def rank_data(n, seed=0):
 
 def bench_rank(args, rank, pkg, W, flushbuf, steps, warmup):
     """Exact rank sums of 64 fit-style candidates over N = 1,048,576 rows."""
-    P, N = 64, 1 << 20
+    P = args.P if args.workload == "rank" and args.P else 64
+    N = args.N if args.workload == "rank" and args.N else 1 << 20
     x, y = rank_data(N, seed=rank)
     trees, _, _ = W.fit_workload(P, 16, seed=100 + rank, nvars=10)
     ev = pkg.GpuEvaluator(x.astype(np.float32).reshape(-1), N, 10, y.astype(np.float32))
@@ -374,7 +375,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="score", choices=["score", "fit"])
+    ap.add_argument("--workload", default="score", choices=["score", "fit", "rank"])
     ap.add_argument("--P", type=int, default=0)
     ap.add_argument("--N", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -401,10 +402,25 @@ def main():
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
+    if args.workload == "rank":
+        # the exact-statistics stage alone (one GPU): the line bench_rank makes
+        r = bench_rank(args, rank, pkg, W, flushbuf, args.steps, args.warmup)
+        if rank == 0:
+            r.update({"n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                      "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                      "dtype": "f64 eval, integer sums", "data": "synthetic",
+                      "gpu_launches": r.pop("launches"),
+                      "e2e": {"value": r["e2e"], "unit": r["unit"], "h2d_bytes_per_step": None,
+                              "d2h_bytes_per_step": None},
+                      "config": {"workload": r["config"], "l2": "flushed between steps"}})
+            print(json.dumps(r), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return
     if args.workload == "score":
         r = bench_score(args, rank, world, local, pkg, W, flushbuf)
     else:
-        r = bench_fit(args, rank, world, local, pkg, W, flushbuf)
+        r = bench_fit(args, rank, world, local, pkg, W, flushbuf, plain=not args.no_secondary)
     torch.cuda.synchronize()
 
     dev_s = sum(r["dev_ms"]) / 1e3

@@ -150,12 +150,18 @@ __global__ void __launch_bounds__(RS_T) rs_hist(const u64 *ka, const u64 *kb,
     cnt[tid] = 0;
     __syncthreads();
     const int base = tile * RS_TILE + w * (RS_TILE / RS_WARPS);
-    for (int r = 0; r < RS_TILE / RS_WARPS / 32; ++r) {
+    constexpr int R = RS_TILE / RS_WARPS / 32;
+    unsigned dg[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        /* all loads first, so each thread has R in flight */
         const int idx = base + 32 * r + lane;
-        const bool in = idx < n;
-        const unsigned d = in ? (unsigned)(src[idx] >> shift) & 255u : 256u;
-        const unsigned peers = __match_any_sync(0xffffffffu, d);
-        if (in && lane == __ffs(peers) - 1) atomicAdd(&cnt[d], (unsigned)__popc(peers));
+        dg[r] = idx < n ? (unsigned)(src[idx] >> shift) & 255u : 256u;
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const unsigned peers = __match_any_sync(0xffffffffu, dg[r]);
+        if (dg[r] < 256u && lane == __ffs(peers) - 1) atomicAdd(&cnt[dg[r]], (unsigned)__popc(peers));
     }
     __syncthreads();
     hist[((size_t)seg * ntiles + tile) * 256 + tid] = cnt[tid];
@@ -195,16 +201,28 @@ __global__ void __launch_bounds__(256) rs_scan(unsigned int *hist, int n, int nt
 /* Stable scatter of one pass. Warp w owns 512 consecutive keys of the tile
    and ranks each key among the warp's earlier keys of the same digit
    (match_any per round of 32); the warps' digit counts are then scanned in
-   warp order, so the output keeps the input order inside a digit. */
+   warp order, so the output keeps the input order inside a digit. The tile
+   is first reordered by digit in shared memory, so that consecutive threads
+   write consecutive addresses of each digit's output run. */
 template <bool VALS>
-__global__ void __launch_bounds__(RS_T) rs_scatter(u64 *ka, u64 *kb, unsigned int *va,
-                                                   unsigned int *vb, const unsigned char *par,
-                                                   const unsigned char *skip,
-                                                   const unsigned int *hist, int n, int ntiles,
-                                                   int shift)
+__host__ __device__ constexpr size_t rs_scatter_smem()
 {
+    return sizeof(u64) * RS_TILE + (VALS ? 2 * sizeof(unsigned int) * RS_TILE : 0);
+}
+
+template <bool VALS>
+__global__ void __launch_bounds__(RS_T, 3) rs_scatter(u64 *ka, u64 *kb, unsigned int *va,
+                                                      unsigned int *vb, const unsigned char *par,
+                                                      const unsigned char *skip,
+                                                      const unsigned int *hist, int n, int ntiles,
+                                                      int shift)
+{
+    extern __shared__ __align__(16) unsigned char sm[];
+    u64 *skey = reinterpret_cast<u64 *>(sm);
+    unsigned int *sval_in = reinterpret_cast<unsigned int *>(skey + RS_TILE);
+    unsigned int *sval = sval_in + RS_TILE;
     __shared__ unsigned int cnt[RS_WARPS][256];
-    __shared__ unsigned int goff[256];
+    __shared__ unsigned int goff[256], lstart[256], wsum[RS_WARPS];
     const int seg = blockIdx.x / ntiles, tile = blockIdx.x % ntiles;
     if (skip[seg]) return;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
@@ -217,19 +235,25 @@ __global__ void __launch_bounds__(RS_T) rs_scatter(u64 *ka, u64 *kb, unsigned in
 #pragma unroll
     for (int k = 0; k < RS_WARPS; ++k) cnt[k][tid] = 0;
     goff[tid] = hist[((size_t)seg * ntiles + tile) * 256 + tid];
-    __syncthreads();
     constexpr int R = RS_TILE / RS_WARPS / 32;
-    const int base = tile * RS_TILE + w * (RS_TILE / RS_WARPS);
+    const int t0 = tile * RS_TILE;
+    const int wb = w * (RS_TILE / RS_WARPS);
+    const int count = min(RS_TILE, n - t0);
     const unsigned lt = (1u << lane) - 1u;
     u64 key[R];
-    unsigned int val[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        /* all loads first, so each thread has R in flight */
+        const int li = wb + 32 * r + lane;
+        const bool in = li < count;
+        key[r] = in ? src[t0 + li] : 0ULL;
+        if (VALS && in) sval_in[li] = vsrc[t0 + li];
+    }
+    __syncthreads();
     unsigned short rk[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-        const int idx = base + 32 * r + lane;
-        const bool in = idx < n;
-        key[r] = in ? src[idx] : 0ULL;
-        val[r] = (VALS && in) ? vsrc[idx] : 0u;
+        const bool in = wb + 32 * r + lane < count;
         const unsigned d = in ? (unsigned)(key[r] >> shift) & 255u : 256u;
         const unsigned peers = __match_any_sync(0xffffffffu, d);
         rk[r] = in ? (unsigned short)(cnt[w][d] + __popc(peers & lt)) : 0;
@@ -238,24 +262,43 @@ __global__ void __launch_bounds__(RS_T) rs_scatter(u64 *ka, u64 *kb, unsigned in
         __syncwarp();
     }
     __syncthreads();
-    {
-        unsigned int run = 0;
+    /* per digit: warp prefixes, the digit's tile total, its start in the
+       digit-ordered tile */
+    unsigned int tot = 0;
 #pragma unroll
-        for (int k = 0; k < RS_WARPS; ++k) {
-            const unsigned int c = cnt[k][tid];
-            cnt[k][tid] = run;
-            run += c;
-        }
+    for (int k = 0; k < RS_WARPS; ++k) {
+        const unsigned int c = cnt[k][tid];
+        cnt[k][tid] = tot;
+        tot += c;
     }
+    unsigned int x = tot;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[w] = x;
+    __syncthreads();
+    unsigned int before = 0;
+    for (int k = 0; k < w; ++k) before += wsum[k];
+    lstart[tid] = before + x - tot;
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-        const int idx = base + 32 * r + lane;
-        if (idx >= n) continue;
+        const int li = wb + 32 * r + lane;
+        if (li >= count) continue;
         const unsigned d = (unsigned)(key[r] >> shift) & 255u;
-        const unsigned int pos = goff[d] + cnt[w][d] + rk[r];
-        dst[pos] = key[r];
-        if (VALS) vdst[pos] = val[r];
+        const unsigned int lp = lstart[d] + cnt[w][d] + rk[r];
+        skey[lp] = key[r];
+        if (VALS) sval[lp] = sval_in[li];
+    }
+    __syncthreads();
+    for (int i = tid; i < count; i += RS_T) {
+        const u64 k = skey[i];
+        const unsigned d = (unsigned)(k >> shift) & 255u;
+        const unsigned int pos = goff[d] + (unsigned)i - lstart[d];
+        dst[pos] = k;
+        if (VALS) vdst[pos] = sval[i];
     }
 }
 
@@ -279,14 +322,16 @@ template <bool VALS>
 unsigned long long rs_sort(const RsBuffers &b, int nseg, int n, cudaStream_t s)
 {
     const int ntiles = (n + RS_TILE - 1) / RS_TILE;
+    cudaFuncSetAttribute(rs_scatter<VALS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)rs_scatter_smem<VALS>());
     const unsigned grid = (unsigned)nseg * (unsigned)ntiles;
     cudaMemsetAsync(b.par, 0, nseg, s);
     for (int pass = 0; pass < 8; ++pass) {
         const int shift = 8 * pass;
         rs_hist<<<grid, RS_T, 0, s>>>(b.ka, b.kb, b.par, n, ntiles, shift, b.hist);
         rs_scan<<<nseg, 256, 0, s>>>(b.hist, n, ntiles, b.skip);
-        rs_scatter<VALS><<<grid, RS_T, 0, s>>>(b.ka, b.kb, b.va, b.vb, b.par, b.skip, b.hist, n,
-                                               ntiles, shift);
+        rs_scatter<VALS><<<grid, RS_T, rs_scatter_smem<VALS>(), s>>>(
+            b.ka, b.kb, b.va, b.vb, b.par, b.skip, b.hist, n, ntiles, shift);
         rs_flip<<<(nseg + 255) / 256, 256, 0, s>>>(b.par, b.skip, nseg);
     }
     return 32;
