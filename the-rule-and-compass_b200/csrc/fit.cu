@@ -54,14 +54,15 @@
 
 enum {
     FOP_NONE = 0, FOP_ASM32 = 1, FOP_ASM64 = 2, FOP_LOSS32 = 3, FOP_LOSS64 = 4,
-    FOP_IJAC = 5, FOP_ICOST = 6, FOP_COUNT = 7
+    FOP_IJAC = 5, FOP_ICOST = 6, FOP_CASM = 7, FOP_CSCORE = 8, FOP_COUNT = 9
 };
 
 enum {
     PC_INIT = 0, PC_AFTER_FIRST_ASM, PC_ROUND, PC_ITER, PC_AFTER_ASM, PC_SOLVE,
     PC_AFTER_TRIAL, PC_REBASE, PC_AFTER_REBASE, PC_POLISH, PC_AFTER_PASM, PC_AFTER_PTRIAL,
     PC_END, PC_I_INIT, PC_I_AFTER_BASE, PC_I_ITER, PC_I_AFTER_JAC, PC_I_AFTER_TRIAL, PC_I_END,
-    PC_DONE
+    PC_C_INIT, PC_C_SCORE_ONLY, PC_C_AFTER_FIRST, PC_C_ITER, PC_C_AFTER_ASM, PC_C_SOLVE,
+    PC_C_AFTER_TRIAL, PC_C_POLISH, PC_C_AFTER_PASM, PC_C_AFTER_PTRIAL, PC_C_END, PC_DONE
 };
 
 /* Per-candidate LM state, resident in device memory between steps. */
@@ -72,6 +73,7 @@ struct FitState {
     double jtj[FT_NTRI];
     double jtr[FT_MAX_CONST];
     double lambda, best, start_best;
+    double rho, svar, syy; /* correlation arm: moments of the last assembly */
     int pc, op, sel;
     int status, round, it, half, pit;
     int assembled, improved, rank, skip, start;
@@ -91,6 +93,7 @@ struct FitArgs {
     const int *pcount;
     int kmax;
     const double *c0;
+    const int *gauge;      /* [2P] correlation gauge pair (scale, offset), -1 = none */
     const int *valid;
     const FIns *fins;      /* stack-machine translation of the records */
     const int *fins_off;   /* [P+1] start of [forward | reverse] */
@@ -119,7 +122,15 @@ struct FitArgs {
 
 __host__ __device__ inline bool ft_op_assembles(int opk)
 {
-    return opk == FOP_ASM32 || opk == FOP_ASM64 || opk == FOP_IJAC;
+    return opk == FOP_ASM32 || opk == FOP_ASM64 || opk == FOP_IJAC || opk == FOP_CASM;
+}
+
+/* Columns of a sweep's augmented Gram: the Jacobian and the residual, or for
+   the correlation assembly the Jacobian and the weighted 1, f and y
+   (eval.cu:1959-2063 moments). */
+__host__ __device__ inline int ft_gram_cols(int opk, int p)
+{
+    return p + (opk == FOP_CASM ? 3 : 1);
 }
 
 __host__ __device__ inline size_t ft_rows_bytes(int Wmax, int T)
@@ -310,9 +321,9 @@ __host__ __device__ inline size_t ft_asm_region(int A, int slots, int tape, int 
 /* Active threads of a candidate: the most (128, 64 or 32) whose region fits
    the fixed budget. It depends on the candidate alone, so its summation
    order does not depend on the batch. */
-inline int ft_asm_threads(int slots, int tape, int p)
+inline int ft_asm_threads(int slots, int tape, int ncols)
 {
-    const int W8 = 8 * ((p + 1 + 7) / 8);
+    const int W8 = 8 * ((ncols + 7) / 8);
     int A = FT_ASM_T;
     while (A > 32 && ft_asm_region(A, slots, tape, W8) > FT_ASM_BUDGET) A /= 2;
     return A;
@@ -339,7 +350,32 @@ struct FtRow {
     bool use, ok;
     float s_zero;
     double seed, res, loss;
+    double c1, c2; /* correlation: the weighted prediction and target columns */
 };
+
+/* A row of the correlation assembly (eval.cu:2031-2047): the reverse sweep
+   is seeded with sqrt(w), and the extra columns carry sqrt(w), sqrt(w) f and
+   sqrt(w) y, so the augmented Gram holds every weighted moment the objective
+   needs. A row whose prediction or target is not finite fails the
+   assembly. */
+__device__ __forceinline__ FtRow ft_row_corr(const FitArgs &a, int rr, int r1, float pred)
+{
+    FtRow o;
+    const double wr = (rr < r1 && a.w) ? a.w[rr] : 1.0;
+    o.use = rr < r1 && wr > 0.0;
+    o.ok = false;
+    o.s_zero = 0.0f;
+    o.seed = o.res = o.loss = o.c1 = o.c2 = 0.0;
+    if (!o.use) return o;
+    const float t = a.y[rr];
+    if (!(isfinite(pred) && fabsf(pred) <= 1e30f && isfinite(t))) return o;
+    const float s = sqrtf((float)wr);
+    o.ok = true;
+    o.seed = s;
+    o.c1 = s * pred;
+    o.c2 = s * t;
+    return o;
+}
 
 __device__ __forceinline__ FtRow ft_row_f32(const FitArgs &a, int rr, int r1, float pred)
 {
@@ -444,7 +480,7 @@ __device__ __forceinline__ void ft_fold(const V *g, int R, int A, int w, int gid
    the warp's rows folded into the augmented Gram matrix. Warps work
    independently over their own rows; the tile's sum is a fixed-order sum
    over warps, written in the packed 4x4-block layout the controller reads. */
-template <typename V, int NR, int T>
+template <typename V, int NR, int T, bool CORR>
 __device__ void ft_tile_asm(const FitArgs &a, const FIns *fwd, const FIns *rev, int nr, int p,
                             int A, int slots, int ntape, const V *cv, unsigned char *region,
                             double *red, int r0, int r1, double *pt)
@@ -454,7 +490,8 @@ __device__ void ft_tile_asm(const FitArgs &a, const FIns *fwd, const FIns *rev, 
     constexpr bool F64 = sizeof(V) == 8;
     const int tid = threadIdx.x;
     const int lane = tid & 31, w = tid >> 5, gid = lane >> 2, tig = lane & 3;
-    const int NB = (p + 1 + 7) / 8;
+    const int ncols = p + (CORR ? 3 : 1);
+    const int NB = (ncols + 7) / 8;
     const int W8 = 8 * NB, R = NR * A + 4;
     V4 *stk = reinterpret_cast<V4 *>(region);
     V4 *tape = stk + (size_t)slots * A;
@@ -478,8 +515,9 @@ __device__ void ft_tile_asm(const FitArgs &a, const FIns *fwd, const FIns *rev, 
             bool special = false;
 #pragma unroll
             for (int i = 0; i < NR; ++i) {
-                rw[i] = F64 ? ft_row_f64(a, row + i, r1, (double)pr[i])
-                            : ft_row_f32(a, row + i, r1, (float)pr[i]);
+                rw[i] = CORR  ? ft_row_corr(a, row + i, r1, (float)pr[i])
+                        : F64 ? ft_row_f64(a, row + i, r1, (double)pr[i])
+                              : ft_row_f32(a, row + i, r1, (float)pr[i]);
                 seed[i] = (V)rw[i].seed;
                 special = special || rw[i].s_zero != 0.0f;
             }
@@ -498,7 +536,7 @@ __device__ void ft_tile_asm(const FitArgs &a, const FIns *fwd, const FIns *rev, 
                     if (!rf || rw[i].s_zero != 0.0f)
                         for (int j = 0; j < p; ++j) gi[(size_t)j * R] = V(0);
                     if (!rf) {
-                        if (F64) {
+                        if (F64 && !CORR) {
                             skipped = 1;
                             rw[i].res = 0.0;
                             rw[i].seed = 0.0; /* marks the row's residual column zero */
@@ -510,8 +548,15 @@ __device__ void ft_tile_asm(const FitArgs &a, const FIns *fwd, const FIns *rev, 
             }
 #pragma unroll
             for (int i = 0; i < NR; ++i) {
-                const bool jac = rw[i].ok && rw[i].seed != 0.0;
-                gt[(size_t)p * R + (size_t)i * A] = jac ? (V)rw[i].res : V(0);
+                if (CORR) {
+                    const bool ok = rw[i].ok;
+                    gt[(size_t)p * R + (size_t)i * A] = ok ? (V)rw[i].seed : V(0);
+                    gt[(size_t)(p + 1) * R + (size_t)i * A] = ok ? (V)rw[i].c1 : V(0);
+                    gt[(size_t)(p + 2) * R + (size_t)i * A] = ok ? (V)rw[i].c2 : V(0);
+                } else {
+                    const bool jac = rw[i].ok && rw[i].seed != 0.0;
+                    gt[(size_t)p * R + (size_t)i * A] = jac ? (V)rw[i].res : V(0);
+                }
                 if (rw[i].ok) loss += rw[i].loss;
                 else if (rw[i].use) bad = 1;
             }
@@ -534,7 +579,7 @@ __device__ void ft_tile_asm(const FitArgs &a, const FIns *fwd, const FIns *rev, 
         }
     }
     __syncthreads();
-    const int W = 4 * ((p + 1 + 3) / 4);
+    const int W = 4 * ((ncols + 3) / 4);
     const int nb4 = W / 4, nblk4 = nb4 * (nb4 + 1) / 2, nw = A / 32;
     for (int e = tid; e < nblk4 * 16; e += T) {
         int b4 = e >> 4, bi = 0;
@@ -607,16 +652,60 @@ __device__ void ft_tile_loss(const FitArgs &a, const FIns *ins, const V *cv,
     }
 }
 
+/* The weighted moments of one tile for the correlation trial score
+   (eval.cu:2170-2214): W, sum w f, sum w f^2, sum w f y, sum w y,
+   sum w y^2 in f64 from the f32 forward sweep, in pt[0..5]. A row whose
+   prediction or target is not finite marks the tile bad, which rejects the
+   trial. */
+template <int NR, int T>
+__device__ void ft_tile_corr_score(const FitArgs &a, const FIns *ins, const float *cv,
+                                   typename FiV<float, NR>::V4 *stk, double *red, int r0, int r1,
+                                   double *pt)
+{
+    const int tid = threadIdx.x;
+    double m[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    int bad = 0;
+    for (int row = r0 + NR * tid; row < r1; row += NR * T) {
+        float pr[NR];
+        fi_forward<float, NR, false>(ins, cv, a.cols, a.npad, row, stk, nullptr, T, tid, pr);
+#pragma unroll
+        for (int i = 0; i < NR; ++i) {
+            const int rr = row + i;
+            if (rr >= r1) continue;
+            const double wr = a.w ? a.w[rr] : 1.0;
+            if (wr <= 0.0) continue;
+            const double f = (double)pr[i], t = (double)a.y[rr];
+            if (!isfinite(f) || fabs(f) > 1e30 || !isfinite(t)) {
+                bad = 1;
+                continue;
+            }
+            m[0] += wr;
+            m[1] += wr * f;
+            m[2] += wr * f * f;
+            m[3] += wr * f * t;
+            m[4] += wr * t;
+            m[5] += wr * t * t;
+        }
+    }
+    bad = __syncthreads_or(bad);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        const double s = ft_block_sum<T>(m[k], red);
+        if (tid == 0) pt[k] = s;
+    }
+    if (tid == 0) pt[FT_PART_BAD] = bad ? 1.0 : 0.0;
+}
+
 /* The assembly / objective sweeps (f32 and f64) over the four-row
    interpreter: a persistent grid over the queued (candidate, tile) items. */
 template <int OPK, int T>
 __global__ void __launch_bounds__(T) ft_sweep4(FitArgs a, int q)
 {
     using V = typename std::conditional<OPK == FOP_ASM64 || OPK == FOP_LOSS64, double, float>::type;
-    constexpr int NR = OPK == FOP_ASM32    ? FT_ASM32_NR
-                       : OPK == FOP_ASM64  ? FT_ASM64_NR
-                       : OPK == FOP_LOSS32 ? FT_LOSS32_NR
-                                           : FT_LOSS64_NR;
+    constexpr int NR = (OPK == FOP_ASM32 || OPK == FOP_CASM) ? FT_ASM32_NR
+                       : OPK == FOP_ASM64                      ? FT_ASM64_NR
+                       : (OPK == FOP_LOSS32 || OPK == FOP_CSCORE) ? FT_LOSS32_NR
+                                                                  : FT_LOSS64_NR;
     using V4 = typename FiV<V, NR>::V4;
     extern __shared__ __align__(16) unsigned char sm[];
     FIns *ins = reinterpret_cast<FIns *>(sm);
@@ -653,8 +742,12 @@ __global__ void __launch_bounds__(T) ft_sweep4(FitArgs a, int q)
         const int r1 = min(a.n, r0 + FT_TILE_ROWS);
         double *pt = a.part + ((size_t)cand * a.ntiles + tile) * FT_PART_STRIDE;
         if (ft_op_assembles(OPK))
-            ft_tile_asm<V, NR, T>(a, ins, ins + nf, nr, p, info.z, info.w & 0xffff, info.w >> 16,
-                                  cv, region, red, r0, r1, pt);
+            ft_tile_asm<V, NR, T, OPK == FOP_CASM>(a, ins, ins + nf, nr, p, info.z, info.w & 0xffff,
+                                                   info.w >> 16, cv, region, red, r0, r1, pt);
+        else if (OPK == FOP_CSCORE)
+            ft_tile_corr_score<NR, T>(a, ins, reinterpret_cast<const float *>(cv),
+                                      reinterpret_cast<typename FiV<float, NR>::V4 *>(region), red,
+                                      r0, r1, pt);
         else
             ft_tile_loss<V, NR, T>(a, ins, cv, reinterpret_cast<V4 *>(region), red, r0, r1, pt);
         __syncthreads();
@@ -662,6 +755,94 @@ __global__ void __launch_bounds__(T) ft_sweep4(FitArgs a, int q)
 }
 
 /* ---- the per-candidate controller --------------------------------------- */
+
+/* ---- correlation objective (eval.cu:1959-2262) ----------------------- */
+
+/* From the assembled augmented Gram (columns: the p Jacobian columns,
+   sqrt(w), sqrt(w) f, sqrt(w) y; lower triangle, row stride W): rho, the
+   variances, the gradient of rho in st.jtr and its Gauss-Newton curvature in
+   st.jtj (eval.cu:2118-2160). Returns the objective 1 - |rho| (1 - rho when
+   signed); bad marks a non-finite result. */
+__device__ double ft_corr_moments(const double *gram, int W, int p, int metric, FitState &st,
+                                  int &bad)
+{
+    auto G = [&](int i, int j) { return gram[i * W + j]; };
+    const double Wt = G(p, p);
+    const double sum_f = G(p + 1, p), sum_f2 = G(p + 1, p + 1), sum_ft = G(p + 2, p + 1);
+    const double sum_t = G(p + 2, p), sum_t2 = G(p + 2, p + 2);
+    double sff = 0.0, syy = 0.0, rho = 0.0;
+    bool ident = true;
+    if (Wt > 0.0) {
+        const double mf = sum_f / Wt, mt = sum_t / Wt;
+        sff = sum_f2 - Wt * mf * mf;
+        syy = sum_t2 - Wt * mt * mt;
+        const double sft = sum_ft - Wt * mf * mt;
+        if (sff > 0.0 && syy > 0.0) {
+            rho = sft / sqrt(sff * syy);
+            const double root = sqrt(sff * syy);
+            double av[FT_MAX_CONST], gbar[FT_MAX_CONST];
+            for (int j = 0; j < p; ++j) {
+                gbar[j] = G(p, j) / Wt;
+                av[j] = G(p + 1, j) - Wt * gbar[j] * mf;
+                const double bj = G(p + 2, j) - Wt * gbar[j] * mt;
+                st.jtr[j] = bj / root - rho * av[j] / sff;
+            }
+            int k = 0;
+            for (int i = 0; i < p; ++i)
+                for (int j = 0; j <= i; ++j, ++k) {
+                    const double centred = G(i, j) - Wt * gbar[i] * gbar[j];
+                    st.jtj[k] = (centred - av[i] * av[j] / sff) / sff;
+                }
+            ident = false;
+        }
+    }
+    if (ident) {
+        int k = 0;
+        for (int i = 0; i < p; ++i) {
+            st.jtr[i] = 0.0;
+            for (int j = 0; j <= i; ++j, ++k) st.jtj[k] = i == j ? 1.0 : 0.0;
+        }
+    }
+    st.svar = sff;
+    st.syy = syy;
+    st.rho = rho;
+    const double score = metric == FM_CORRELATION_SIGNED ? 1.0 - rho : 1.0 - fabs(rho);
+    bad = (!isfinite(score) || !isfinite(sff) || !isfinite(syy)) ? 1 : 0;
+    return score;
+}
+
+/* The value-only objective from the six weighted sums (eval.cu:2226-2234). */
+__device__ double ft_corr_trial(const double *m, int metric)
+{
+    const double Wt = m[0];
+    if (!(Wt > 0.0)) return 1e30;
+    const double mf = m[1] / Wt, mt = m[4] / Wt;
+    const double sff = m[2] - Wt * mf * mf;
+    const double syy = m[5] - Wt * mt * mt;
+    const double sft = m[3] - Wt * mf * mt;
+    if (!(sff > 0.0) || !(syy > 0.0)) return 1.0;
+    const double rho = sft / sqrt(sff * syy);
+    return metric == FM_CORRELATION_SIGNED ? 1.0 - rho : 1.0 - fabs(rho);
+}
+
+/* Turn the rho gradient into the objective's (L = 1 - sigma rho, so the
+   damped solve with jtr = dL steps along -H^-1 dL) and freeze the gauge
+   slots: zero right-hand side, identity row and column (eval.cu:2239-2258).
+   Applied in place to the assembled system before every solve, as the
+   reference does. */
+__device__ void ft_corr_mask(FitState &st, int p, int metric, const int *g)
+{
+    const double sigma = metric == FM_CORRELATION_SIGNED ? 1.0 : (st.rho >= 0.0 ? 1.0 : -1.0);
+    for (int j = 0; j < p; ++j) st.jtr[j] = -sigma * st.jtr[j];
+    for (int i = 0; i < p; ++i) {
+        const bool gi = g[0] == i || g[1] == i;
+        for (int j = 0; j <= i; ++j) {
+            const bool gj = g[0] == j || g[1] == j;
+            if (gi || gj) st.jtj[i * (i + 1) / 2 + j] = i == j ? 1.0 : 0.0;
+        }
+        if (gi) st.jtr[i] = 0.0;
+    }
+}
 
 /* Status labels of a finished fit (eval.cu:2583-2600), then the outputs. */
 __device__ void ft_finish(const FitArgs &a, FitState &st, int cand, int p)
@@ -677,6 +858,11 @@ __device__ void ft_finish(const FitArgs &a, FitState &st, int cand, int p)
             else if (st.rank) status = 4;
             else if (!st.improved && a.iters > 0) status = 6;
         }
+    }
+    if (st.pc == PC_C_END) {
+        /* a finite correlation answer is returned as is (eval.cu:2430-2440) */
+        if (status == 1 || status == 2) status = !st.start ? 7 : (st.improved ? 5 : 6);
+        else if (status == 0 && st.rank) status = 4;
     }
     for (int j = 0; j < p; ++j) a.outc[(size_t)cand * a.kmax + j] = st.c[j];
     a.outsse[cand] = st.best;
@@ -714,6 +900,10 @@ __device__ void ft_advance(const FitArgs &a, FitState &st, int cand, int p, doub
                 }
                 if (a.metric == FM_IMPLICIT) {
                     st.pc = PC_I_INIT;
+                    break;
+                }
+                if (a.metric == FM_CORRELATION || a.metric == FM_CORRELATION_SIGNED) {
+                    st.pc = PC_C_INIT;
                     break;
                 }
                 if (iters <= 0) {
@@ -884,6 +1074,150 @@ __device__ void ft_advance(const FitArgs &a, FitState &st, int cand, int p, doub
             case PC_END:
                 ft_finish(a, st, cand, p);
                 return;
+            /* ---- correlation metric (eval.cu:2316-2440) ---- */
+            case PC_C_INIT: {
+                const int *g = a.gauge + 2 * cand;
+                const int gs = g[0], go = g[1];
+                if (gs >= 0 && gs < p && isfinite(st.c[gs]) && st.c[gs] != 0.0)
+                    st.c[gs] = st.c[gs] > 0.0 ? 1.0 : -1.0;
+                if (go >= 0 && go < p) st.c[go] = 0.0;
+                st.best = 1.0;
+                st.op = iters > 0 ? FOP_CASM : FOP_CSCORE;
+                st.sel = 0;
+                st.pc = iters > 0 ? PC_C_AFTER_FIRST : PC_C_SCORE_ONLY;
+                return;
+            }
+            case PC_C_SCORE_ONLY:
+                st.best = rl;
+                st.pc = PC_C_END;
+                break;
+            case PC_C_AFTER_FIRST:
+                st.start = rb ? 0 : 1;
+                st.assembled = 1;
+                if (rb) {
+                    st.status = 2;
+                    st.pc = PC_C_END;
+                } else if (!(st.svar > 0.0) || !(st.syy > 0.0)) {
+                    st.best = 1.0;
+                    st.pc = PC_C_END;
+                } else if (st.svar < 1e-24 * st.syy) {
+                    st.status = 1;
+                    st.pc = PC_C_END;
+                } else {
+                    st.best = rl;
+                    st.lambda = 1e-3;
+                    st.it = 0;
+                    st.pc = PC_C_ITER;
+                }
+                break;
+            case PC_C_ITER:
+                if (!(st.it < iters && st.status == 0)) {
+                    st.pit = 0;
+                    st.pc = PC_C_POLISH;
+                    break;
+                }
+                if (!st.assembled) {
+                    st.op = FOP_CASM;
+                    st.sel = 0;
+                    st.pc = PC_C_AFTER_ASM;
+                    return;
+                }
+                st.pc = PC_C_SOLVE;
+                break;
+            case PC_C_AFTER_ASM:
+                st.assembled = 1;
+                if (rb) {
+                    st.status = 2;
+                    st.pc = PC_C_END;
+                    break;
+                }
+                if (st.svar < 1e-24 * st.syy) {
+                    st.status = 1;
+                    st.pc = PC_C_END;
+                    break;
+                }
+                st.pc = PC_C_SOLVE;
+                break;
+            case PC_C_SOLVE: {
+                ft_corr_mask(st, p, a.metric, a.gauge + 2 * cand);
+                const int sv = ft_solve(st.jtj, st.jtr, st.lambda, p, delta, L);
+                if (sv == 1) {
+                    st.status = 1;
+                    st.pc = PC_C_END;
+                    break;
+                }
+                if (sv == 4) st.rank = 1;
+                for (int j = 0; j < p; ++j) st.trial[j] = fmin(1e6, fmax(-1e6, st.c[j] + delta[j]));
+                st.op = FOP_CSCORE;
+                st.sel = 1;
+                st.pc = PC_C_AFTER_TRIAL;
+                return;
+            }
+            case PC_C_AFTER_TRIAL:
+                if (rl < st.best) {
+                    for (int j = 0; j < p; ++j) st.c[j] = st.trial[j];
+                    st.best = rl;
+                    st.lambda = fmax(st.lambda / 8.0, 1e-12);
+                    st.assembled = 0;
+                    st.improved = 1;
+                    if (st.best <= 0.0) {
+                        st.pit = 0;
+                        st.pc = PC_C_POLISH;
+                        break;
+                    }
+                } else {
+                    st.lambda *= 6.0;
+                    if (st.lambda > 1e9) {
+                        st.pit = 0;
+                        st.pc = PC_C_POLISH;
+                        break;
+                    }
+                }
+                st.it++;
+                st.pc = PC_C_ITER;
+                break;
+            case PC_C_POLISH:
+                if (!(st.pit < 4 && st.status == 0 && st.best > 0.0)) {
+                    st.pc = PC_C_END;
+                    break;
+                }
+                st.op = FOP_CASM;
+                st.sel = 0;
+                st.pc = PC_C_AFTER_PASM;
+                return;
+            case PC_C_AFTER_PASM: {
+                if (rb) {
+                    st.status = 2;
+                    st.pc = PC_C_END;
+                    break;
+                }
+                ft_corr_mask(st, p, a.metric, a.gauge + 2 * cand);
+                const int sv = ft_solve(st.jtj, st.jtr, 0.0, p, delta, L);
+                if (sv == 1) {
+                    st.pc = PC_C_END;
+                    break;
+                }
+                if (sv == 4) st.rank = 1;
+                for (int j = 0; j < p; ++j) st.trial[j] = fmin(1e6, fmax(-1e6, st.c[j] + delta[j]));
+                st.op = FOP_CSCORE;
+                st.sel = 1;
+                st.pc = PC_C_AFTER_PTRIAL;
+                return;
+            }
+            case PC_C_AFTER_PTRIAL:
+                if (rl < st.best) {
+                    for (int j = 0; j < p; ++j) st.c[j] = st.trial[j];
+                    st.best = rl;
+                    st.improved = 1;
+                    st.pit++;
+                    st.pc = PC_C_POLISH;
+                } else {
+                    st.pc = PC_C_END;
+                }
+                break;
+            case PC_C_END:
+                ft_finish(a, st, cand, p);
+                return;
             /* ---- implicit metric ---- */
             case PC_I_INIT:
                 for (int j = 0; j < p; ++j) st.start_c[j] = st.c[j];
@@ -1017,8 +1351,8 @@ __global__ void __launch_bounds__(FT_CTRL_T) ft_control(FitArgs a, int q, int in
         __syncthreads();
         if (init && tid == 0) sst.pc = PC_INIT;
         const double *pt = a.part + (size_t)cand * a.ntiles * FT_PART_STRIDE;
+        const int W = 4 * ((ft_gram_cols(op, p) + 3) / 4);
         if (!init && ft_op_assembles(op)) {
-            const int W = 4 * ((p + 1 + 3) / 4);
             const int nb = W / 4;
             const int nblk = nb * (nb + 1) / 2;
             for (int e = tid; e < nblk * 16; e += FT_CTRL_T) {
@@ -1032,7 +1366,7 @@ __global__ void __launch_bounds__(FT_CTRL_T) ft_control(FitArgs a, int q, int in
                 gram[(4 * bi + ((e & 15) >> 2)) * W + 4 * b + (e & 3)] = s;
             }
             __syncthreads();
-            for (int e = tid; e < p * (p + 1) / 2 + p; e += FT_CTRL_T) {
+            for (int e = tid; op != FOP_CASM && e < p * (p + 1) / 2 + p; e += FT_CTRL_T) {
                 if (e < p * (p + 1) / 2) {
                     int i = 0, k = e;
                     while (k > i) {
@@ -1055,6 +1389,16 @@ __global__ void __launch_bounds__(FT_CTRL_T) ft_control(FitArgs a, int q, int in
                     loss += pp[FT_PART_LOSS];
                     bad |= pp[FT_PART_BAD] != 0.0;
                     if (ft_op_assembles(op)) skip |= pp[FT_PART_SKIP] != 0.0;
+                }
+                if (op == FOP_CASM) {
+                    int cb = 0;
+                    loss = ft_corr_moments(gram, W, p, a.metric, sst, cb);
+                    bad |= cb;
+                } else if (op == FOP_CSCORE) {
+                    double m[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+                    for (int t = 0; t < a.ntiles; ++t)
+                        for (int k = 0; k < 6; ++k) m[k] += pt[(size_t)t * FT_PART_STRIDE + k];
+                    loss = bad ? INFINITY : ft_corr_trial(m, a.metric);
                 }
             }
             s_loss = loss;
@@ -1322,7 +1666,7 @@ bool validate_records(const uint32_t *rec, int m, int p, int v)
 
 /* Decode and check a batch of fit-record programs for the device sweeps. */
 void prep_batch(const unsigned int *off, const unsigned int *prog, const int *pcount, int nprog,
-                int v, FitPrep &b)
+                int v, FitPrep &b, int extra_cols)
 {
     b.node_off.resize(nprog + 1);
     b.valid.resize(nprog);
@@ -1356,10 +1700,11 @@ void prep_batch(const unsigned int *off, const unsigned int *prog, const int *pc
         }
         b.fins.insert(b.fins.end(), fwd.begin(), fwd.end());
         b.fins.insert(b.fins.end(), rev.begin(), rev.end());
-        const int A = ft_asm_threads(ns, nt, pcount[i]);
+        const int ncols = pcount[i] + 1 + extra_cols;
+        const int A = ft_asm_threads(ns, nt, ncols);
         b.finfo[i] = make_int4((int)fwd.size(), (int)rev.size(), A, ns | (nt << 16));
         b.asm_region = std::max(b.asm_region,
-                                ft_asm_region(A, ns, nt, 8 * ((pcount[i] + 1 + 7) / 8)));
+                                ft_asm_region(A, ns, nt, 8 * ((ncols + 7) / 8)));
         b.fslots = std::max(b.fslots, ns);
         b.ftape = std::max(b.ftape, nt);
         b.fmaxins = std::max(b.fmaxins, (int)(fwd.size() + rev.size()));
@@ -1389,6 +1734,9 @@ int max_steps(int iters, int metric)
 {
     const int it = iters < 1 ? 1 : iters;
     if (metric == FM_IMPLICIT) return 1 + 2 * it + 1;
+    /* correlation: the first assembly, per iteration an assembly and a trial,
+       four polish assemblies and trials */
+    if (metric == FM_CORRELATION || metric == FM_CORRELATION_SIGNED) return 2 + 2 * it + 8 + 2;
     const int per = metric == FM_ABSOLUTE ? 4 : 2;
     return 2 + per * it + 1 + 12 + 1;
 }
@@ -1454,13 +1802,14 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
               int nprog, int kmax, const double *c0, const int *gauge, int iters, int metric,
               int flags, double *outc, double *outsse, int *outstatus, int mode)
 {
-    (void)gauge;
     if (!c || !prog || !off || !pcount || !c0 || !outc || !outsse || !outstatus) return -1.0f;
     if (nprog <= 0 || kmax <= 0 || kmax > FT_MAX_CONST || c->n <= 0) return -1.0f;
     if (metric == FM_LOGISTIC && !c->has_tsign) return -1.0f;
+    const bool corr = metric == FM_CORRELATION || metric == FM_CORRELATION_SIGNED;
     if (metric != FM_SQUARED && metric != FM_LOG_SQUASHED && metric != FM_ABSOLUTE &&
-        metric != FM_LOGISTIC && metric != FM_IMPLICIT)
+        metric != FM_LOGISTIC && metric != FM_IMPLICIT && !corr)
         return -1.0f;
+    if (corr && !gauge) return -1.0f;
     if (metric == FM_IMPLICIT && c->v > FT_IMPLICIT_MAXV) return -1.0f;
     for (int i = 0; i < nprog; ++i)
         if (pcount[i] < 0 || pcount[i] > kmax) return -1.0f;
@@ -1468,7 +1817,7 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     double t = rc_now_ms();
     if (rc_ensure_f64(c) != 0) return -1.0f;
     FitPrep b;
-    prep_batch(off, prog, pcount, nprog, c->v, b);
+    prep_batch(off, prog, pcount, nprog, c->v, b, corr ? 2 : 0);
     const int ntiles = (c->n + FT_TILE_ROWS - 1) / FT_TILE_ROWS;
     const int Wmax = 4 * ((b.pmax + 1 + 3) / 4);
     const size_t words = off[nprog];
@@ -1478,6 +1827,7 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     const size_t o_p = rc_take(&cur, sizeof(int) * nprog);
     const size_t o_c0 = rc_take(&cur, sizeof(double) * (size_t)nprog * kmax);
     const size_t o_valid = rc_take(&cur, sizeof(int) * nprog);
+    const size_t o_gauge = rc_take(&cur, sizeof(int) * 2 * (size_t)nprog);
     const size_t o_fins = rc_take(&cur, sizeof(FIns) * b.fins.size());
     const size_t o_finsoff = rc_take(&cur, sizeof(int) * (nprog + 1));
     const size_t o_finfo = rc_take(&cur, sizeof(int4) * nprog);
@@ -1501,6 +1851,8 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     memcpy(host + o_p, pcount, sizeof(int) * nprog);
     memcpy(host + o_c0, c0, sizeof(double) * (size_t)nprog * kmax);
     memcpy(host + o_valid, b.valid.data(), sizeof(int) * nprog);
+    if (gauge) memcpy(host + o_gauge, gauge, sizeof(int) * 2 * (size_t)nprog);
+    else memset(host + o_gauge, 0xff, sizeof(int) * 2 * (size_t)nprog);
     memcpy(host + o_fins, b.fins.data(), sizeof(FIns) * b.fins.size());
     memcpy(host + o_finsoff, b.fins_off.data(), sizeof(int) * (nprog + 1));
     memcpy(host + o_finfo, b.finfo.data(), sizeof(int4) * nprog);
@@ -1526,6 +1878,7 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     a.kmax = kmax;
     a.c0 = reinterpret_cast<const double *>(dev + o_c0);
     a.valid = reinterpret_cast<const int *>(dev + o_valid);
+    a.gauge = reinterpret_cast<const int *>(dev + o_gauge);
     a.fins = reinterpret_cast<const FIns *>(dev + o_fins);
     a.fins_off = reinterpret_cast<const int *>(dev + o_finsoff);
     a.finfo = reinterpret_cast<const int4 *>(dev + o_finfo);
@@ -1554,6 +1907,9 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     if (metric == FM_IMPLICIT) {
         sw[nk] = sweep_launch<FOP_IJAC>(c, b.mmax, Wmax); ++nk;
         sw[nk] = sweep_launch<FOP_ICOST>(c, b.mmax, Wmax); ++nk;
+    } else if (corr) {
+        sw[nk] = sweep4_launch<FOP_CASM, FT_ASM_T>(c, b, Wmax); ++nk;
+        sw[nk] = sweep4_launch<FOP_CSCORE, 128>(c, b, Wmax); ++nk;
     } else {
         sw[nk] = sweep4_launch<FOP_ASM32, FT_ASM_T>(c, b, Wmax); ++nk;
         sw[nk] = sweep4_launch<FOP_LOSS32, 128>(c, b, Wmax); ++nk;
@@ -1578,6 +1934,7 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
             one.pcount = a.pcount + i;
             one.c0 = a.c0 + (size_t)i * kmax;
             one.valid = a.valid + i;
+            one.gauge = a.gauge + 2 * (size_t)i;
             one.fins_off = a.fins_off + i;
             one.finfo = a.finfo + i;
             one.state = a.state + i;

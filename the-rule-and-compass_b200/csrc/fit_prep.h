@@ -25,6 +25,7 @@ struct FitPrep {
 };
 
 /* Validate and translate `nprog` programs (`off` in words); a rejected
-   program has valid[i] = 0 and no instructions. */
+   program has valid[i] = 0 and no instructions. `extra_cols` widens the
+   assembly's Gram beyond p + 1 columns (the correlation moments use 2). */
 void prep_batch(const unsigned int *off, const unsigned int *prog, const int *pcount, int nprog,
-                int v, FitPrep &b);
+                int v, FitPrep &b, int extra_cols = 0);
