@@ -205,3 +205,35 @@ def test_jacobian_matches_central_differences_and_the_cpu_adjoint(pkg, E, O):
             checked += 1
     assert checked > 50
     ev.close()
+
+
+def test_logistic_fit_reaches_the_log_loss_optimum(pkg, E):
+    """Metric 5 (the device logistic arm, eval.cu:589-604 code LOGISTIC): a
+    logit model a*x + b fitted to labels drawn from sigmoid(2x - 0.5) reaches
+    the minimum of sum softplus(-t * pred) (t = +-1 labels) that a
+    general-purpose optimiser finds, and reports that objective."""
+    from scipy.optimize import minimize
+    rng = np.random.Generator(np.random.PCG64(21))
+    n = 5000
+    x = rng.uniform(-3.0, 3.0, n)
+    lab = (rng.uniform(size=n) < 1.0 / (1.0 + np.exp(-(2.0 * x - 0.5)))).astype(np.float64)
+    t = 2.0 * lab - 1.0
+    ev = pkg.GpuEvaluator(x.astype(np.float32), n, 1, lab.astype(np.float32))
+    ev.set_fit_data(x.astype(np.float32).astype(np.float64), lab)
+    ev.set_fit_sign(t)
+    tree = E.node(E.ADD, [E.node(E.MUL, [E.constant(0.3), E.input(0)]), E.constant(0.1)])
+    plan = pkg.gpu_fit_plan(tree)
+    c, loss, status, _ = ev.fit_plans([plan], 20, metric=5)
+    assert status[0] in (0, 5, 6)
+    x64 = x.astype(np.float32).astype(np.float64)
+
+    def obj(v):
+        u = t * (v[0] * x64 + v[1])
+        return np.sum(np.logaddexp(0.0, -u))
+
+    cc = plan.apply(tree, c[0][: plan.nconst]).constants()
+    got = obj(cc)
+    assert abs(loss[0] - got) <= 1e-9 * got
+    ref = minimize(obj, [0.3, 0.1], method="BFGS", options={"gtol": 1e-10})
+    assert got <= ref.fun * (1 + 1e-7), (got, ref.fun)
+    ev.close()

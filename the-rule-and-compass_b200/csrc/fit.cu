@@ -465,7 +465,7 @@ __device__ __forceinline__ void ft_fold(const V *g, int R, int A, int w, int gid
         const int local = (q >> 5) * A + 32 * w + (q & 31);
         double x[NB];
 #pragma unroll
-        for (int I = 0; I < NB; ++I) x[I] = (double)g[(size_t)(8 * I + gid) * R + local];
+        for (int I = 0; I < NB; ++I) x[I] = (double)g[(8 * I + gid) * R + local];
         int b = 0;
 #pragma unroll
         for (int I = 0; I < NB; ++I)
@@ -494,8 +494,8 @@ __device__ void ft_tile_asm(const FitArgs &a, const FIns *fwd, const FIns *rev, 
     const int NB = (ncols + 7) / 8;
     const int W8 = 8 * NB, R = NR * A + 4;
     V4 *stk = reinterpret_cast<V4 *>(region);
-    V4 *tape = stk + (size_t)slots * A;
-    V *g = reinterpret_cast<V *>(tape + (size_t)ntape * A);
+    V4 *tape = stk + slots * A;
+    V *g = reinterpret_cast<V *>(tape + ntape * A);
     const V *cols = F64 ? reinterpret_cast<const V *>(a.cols64) : reinterpret_cast<const V *>(a.cols);
     for (int i = tid; i < W8 * R; i += T) g[i] = V(0);
     __syncthreads();
@@ -529,12 +529,12 @@ __device__ void ft_tile_asm(const FitArgs &a, const FIns *fwd, const FIns *rev, 
 #pragma unroll
                 for (int i = 0; i < NR; ++i) {
                     if (!rw[i].ok) continue;
-                    V *gi = gt + (size_t)i * A;
+                    V *gi = gt + i * A;
                     bool rf = true;
                     if (!fin)
-                        for (int j = 0; j < p; ++j) rf = rf && isfinite(gi[(size_t)j * R]);
+                        for (int j = 0; j < p; ++j) rf = rf && isfinite(gi[j * R]);
                     if (!rf || rw[i].s_zero != 0.0f)
-                        for (int j = 0; j < p; ++j) gi[(size_t)j * R] = V(0);
+                        for (int j = 0; j < p; ++j) gi[j * R] = V(0);
                     if (!rf) {
                         if (F64 && !CORR) {
                             skipped = 1;
@@ -550,12 +550,12 @@ __device__ void ft_tile_asm(const FitArgs &a, const FIns *fwd, const FIns *rev, 
             for (int i = 0; i < NR; ++i) {
                 if (CORR) {
                     const bool ok = rw[i].ok;
-                    gt[(size_t)p * R + (size_t)i * A] = ok ? (V)rw[i].seed : V(0);
-                    gt[(size_t)(p + 1) * R + (size_t)i * A] = ok ? (V)rw[i].c1 : V(0);
-                    gt[(size_t)(p + 2) * R + (size_t)i * A] = ok ? (V)rw[i].c2 : V(0);
+                    gt[p * R + i * A] = ok ? (V)rw[i].seed : V(0);
+                    gt[(p + 1) * R + i * A] = ok ? (V)rw[i].c1 : V(0);
+                    gt[(p + 2) * R + i * A] = ok ? (V)rw[i].c2 : V(0);
                 } else {
                     const bool jac = rw[i].ok && rw[i].seed != 0.0;
-                    gt[(size_t)p * R + (size_t)i * A] = jac ? (V)rw[i].res : V(0);
+                    gt[p * R + i * A] = jac ? (V)rw[i].res : V(0);
                 }
                 if (rw[i].ok) loss += rw[i].loss;
                 else if (rw[i].use) bad = 1;
@@ -574,8 +574,8 @@ __device__ void ft_tile_asm(const FitArgs &a, const FIns *fwd, const FIns *rev, 
 #pragma unroll
         for (int b = 0; b < 6; ++b) {
             if (b >= NBLK) break;
-            gb[(size_t)(w * NBLK + b) * 64 + gid * 8 + 2 * tig] = acc[b][0];
-            gb[(size_t)(w * NBLK + b) * 64 + gid * 8 + 2 * tig + 1] = acc[b][1];
+            gb[(w * NBLK + b) * 64 + gid * 8 + 2 * tig] = acc[b][0];
+            gb[(w * NBLK + b) * 64 + gid * 8 + 2 * tig + 1] = acc[b][1];
         }
     }
     __syncthreads();
@@ -591,7 +591,7 @@ __device__ void ft_tile_asm(const FitArgs &a, const FIns *fwd, const FIns *rev, 
         const int I = rw4 >> 3, J = cl >> 3;
         const int el = (I * (I + 1) / 2 + J) * 64 + (rw4 & 7) * 8 + (cl & 7);
         double s = 0.0;
-        for (int v = 0; v < nw; ++v) s += gb[(size_t)v * NBLK * 64 + el];
+        for (int v = 0; v < nw; ++v) s += gb[v * NBLK * 64 + el];
         pt[e] = s;
     }
     bad = __syncthreads_or(bad);

@@ -307,10 +307,10 @@ __device__ __forceinline__ V fi_child(V a, V d)
                 fi_partials<V>(OPC, a[i], b[i], r[i], pl[i], pr[i]);                  \
             int ts = in.tape;                                                         \
             if (kind & FI_HP_L) {                                                     \
-                tape[(size_t)ts * S + tid] = F::pack(pl);                             \
+                tape[ts * S + tid] = F::pack(pl);                             \
                 ++ts;                                                                 \
             }                                                                         \
-            if (kind & FI_HP_R) tape[(size_t)ts * S + tid] = F::pack(pr);             \
+            if (kind & FI_HP_R) tape[ts * S + tid] = F::pack(pr);             \
         }                                                                             \
     } break;
 
@@ -333,7 +333,7 @@ __device__ __forceinline__ void fi_forward(const FIns *__restrict__ prog, const 
         const unsigned kind = in.kind;
         const unsigned k = kind & FI_KIND_MASK;
         if (k <= FI_PUSH_PARAM) {
-            if (in.spill != 0xff) stk[(size_t)in.spill * S + tid] = F::pack(t);
+            if (in.spill != 0xff) stk[in.spill * S + tid] = F::pack(t);
             if (k == FI_PUSH_VAR) {
                 F::ldg(cols + (size_t)in.imm * (size_t)npad + row, t);
             } else {
@@ -346,7 +346,7 @@ __device__ __forceinline__ void fi_forward(const FIns *__restrict__ prog, const 
         if (k == FI_HALT) break;
         V a[NR], b[NR];
         if (k == FI_BIN_S) {
-            F::unpack(stk[(size_t)in.arg * S + tid], a);
+            F::unpack(stk[in.arg * S + tid], a);
 #pragma unroll
             for (int i = 0; i < NR; ++i) b[i] = t[i];
         } else {
@@ -366,7 +366,42 @@ __device__ __forceinline__ void fi_forward(const FIns *__restrict__ prog, const 
         V r[NR];
         switch (in.op) {
             FI_OPN(OP_ADD) FI_OPN(OP_SUB) FI_OPN(OP_MUL) FI_OPN(OP_DIV) FI_OPN(OP_POW)
-            FI_OPN(OP_SIN) FI_OPN(OP_COS) FI_OPN(OP_TAN) FI_OPN(OP_EXP) FI_OPN(OP_LOG)
+            case OP_SIN:
+            case OP_COS:
+                if (sizeof(V) == 4 && PARTIALS && (kind & FI_HP_L)) {
+                    /* one f32 sincosf gives the value and the partial (its
+                       results equal sinf / cosf bit for bit on B200) */
+                    V pl[NR];
+                    const bool is_sin = in.op == OP_SIN;
+#pragma unroll
+                    for (int i = 0; i < NR; ++i) {
+                        float s, c;
+                        sincosf((float)a[i], &s, &c);
+                        r[i] = is_sin ? s : c;
+                        pl[i] = is_sin ? c : -s;
+                    }
+                    tape[in.tape * S + tid] = F::pack(pl);
+                } else if (in.op == OP_SIN) {
+#pragma unroll
+                    for (int i = 0; i < NR; ++i) r[i] = F::value(OP_SIN, a[i], b[i]);
+                    if (PARTIALS && (kind & FI_HP_L)) {
+                        V pl[NR];
+#pragma unroll
+                        for (int i = 0; i < NR; ++i) pl[i] = cos(a[i]);
+                        tape[in.tape * S + tid] = F::pack(pl);
+                    }
+                } else {
+#pragma unroll
+                    for (int i = 0; i < NR; ++i) r[i] = F::value(OP_COS, a[i], b[i]);
+                    if (PARTIALS && (kind & FI_HP_L)) {
+                        V pl[NR];
+#pragma unroll
+                        for (int i = 0; i < NR; ++i) pl[i] = -sin(a[i]);
+                        tape[in.tape * S + tid] = F::pack(pl);
+                    }
+                }
+                break;
+            FI_OPN(OP_TAN) FI_OPN(OP_EXP) FI_OPN(OP_LOG)
             FI_OPN(OP_SQRT) FI_OPN(OP_ABS) FI_OPN(OP_TANH) FI_OPN(OP_SIG) FI_OPN(OP_SQUARE)
             FI_OPN(OP_CUBE) FI_OPN(OP_NEG) FI_OPN(OP_GAUSS) FI_OPN(OP_SINH) FI_OPN(OP_COSH)
             FI_OPN(OP_ERF) FI_OPN(OP_ERFC)
@@ -402,7 +437,7 @@ __device__ __forceinline__ bool fi_reverse(const FIns *__restrict__ rev, int nr,
         const unsigned k = kind & FI_KIND_MASK;
         if (k <= FI_PUSH_PARAM) {
             if (k == FI_PUSH_PARAM) {
-                V *gs = g + (size_t)in.imm * R;
+                V *gs = g + in.imm * R;
 #pragma unroll
                 for (int i = 0; i < NR; ++i) {
                     const V v = (kind & FI_ACC) ? a[i] + gs[i * A] : a[i];
@@ -410,7 +445,7 @@ __device__ __forceinline__ bool fi_reverse(const FIns *__restrict__ rev, int nr,
                     fin = fin && isfinite(v);
                 }
             }
-            if (in.spill != 0xff) F::unpack(stk[(size_t)in.spill * S + tid], a);
+            if (in.spill != 0xff) F::unpack(stk[in.spill * S + tid], a);
             continue;
         }
         if (k == FI_UNARY) {
@@ -419,7 +454,7 @@ __device__ __forceinline__ bool fi_reverse(const FIns *__restrict__ rev, int nr,
                 for (int i = 0; i < NR; ++i) a[i] = -a[i];
             } else {
                 V d[NR];
-                F::unpack(tape[(size_t)in.tape * S + tid], d);
+                F::unpack(tape[in.tape * S + tid], d);
 #pragma unroll
                 for (int i = 0; i < NR; ++i) a[i] = fi_child(a[i], d[i]);
             }
@@ -441,14 +476,14 @@ __device__ __forceinline__ bool fi_reverse(const FIns *__restrict__ rev, int nr,
             for (int i = 0; i < NR; ++i) l[i] = r[i] = V(0);
             if (kind & FI_HP_L) {
                 V d[NR];
-                F::unpack(tape[(size_t)ts * S + tid], d);
+                F::unpack(tape[ts * S + tid], d);
 #pragma unroll
                 for (int i = 0; i < NR; ++i) l[i] = fi_child(a[i], d[i]);
                 ++ts;
             }
             if (kind & FI_HP_R) {
                 V d[NR];
-                F::unpack(tape[(size_t)ts * S + tid], d);
+                F::unpack(tape[ts * S + tid], d);
 #pragma unroll
                 for (int i = 0; i < NR; ++i) r[i] = fi_child(a[i], d[i]);
             }
@@ -457,7 +492,7 @@ __device__ __forceinline__ bool fi_reverse(const FIns *__restrict__ rev, int nr,
             if ((kind & FI_HP_L) && (kind & FI_HP_R)) {
                 /* the left adjoint waits in its spill slot while the right
                    subtree is walked; that subtree's first push restores it */
-                stk[(size_t)in.arg * S + tid] = F::pack(l);
+                stk[in.arg * S + tid] = F::pack(l);
 #pragma unroll
                 for (int i = 0; i < NR; ++i) a[i] = r[i];
             } else if (kind & FI_HP_R) {
@@ -469,7 +504,7 @@ __device__ __forceinline__ bool fi_reverse(const FIns *__restrict__ rev, int nr,
             }
         } else {
             if (k == FI_BIN_P) {
-                V *gs = g + (size_t)in.imm * R;
+                V *gs = g + in.imm * R;
 #pragma unroll
                 for (int i = 0; i < NR; ++i) {
                     const V v = (kind & FI_ACC) ? r[i] + gs[i * A] : r[i];
