@@ -103,6 +103,14 @@ struct FitArgs {
     int ftape;             /* partial-tape slots needed by the batch */
     int fmaxins;           /* longest forward + reverse list */
     size_t asm_region;     /* f32 assembly region of the launch */
+    const int2 *fcinfo;    /* [P] cached forward count (after the reverse list),
+                              first cache column */
+    float *cache;          /* [columns][npad] values of constant-free subtrees */
+    const FIns *sub_fins;  /* forward lists of the cached subtrees */
+    const int *sub_off;    /* [nsub + 1] */
+    const int *sub_col;    /* [nsub] */
+    int nsub;
+    int sub_slots, sub_maxins;
     int iters, metric, flags;
     int ntiles;
     int mmax;
@@ -483,7 +491,7 @@ __device__ __forceinline__ void ft_fold(const V *g, int R, int A, int w, int gid
 template <typename V, int NR, int T, bool CORR>
 __device__ void ft_tile_asm(const FitArgs &a, const FIns *fwd, const FIns *rev, int nr, int p,
                             int A, int slots, int ntape, const V *cv, unsigned char *region,
-                            double *red, int r0, int r1, double *pt)
+                            double *red, int r0, int r1, double *pt, const V *ccols)
 {
     using F = FiV<V, NR>;
     using V4 = typename F::V4;
@@ -509,7 +517,7 @@ __device__ void ft_tile_asm(const FitArgs &a, const FIns *fwd, const FIns *rev, 
         for (int base = r0; base < r1; base += NR * A) {
             const int row = base + NR * tid;
             V pr[NR];
-            fi_forward<V, NR, true>(fwd, cv, cols, a.npad, row, stk, tape, A, tid, pr);
+            fi_forward<V, NR, true>(fwd, cv, cols, a.npad, row, stk, tape, A, tid, pr, ccols);
             FtRow rw[NR];
             V seed[NR];
             bool special = false;
@@ -608,7 +616,8 @@ __device__ void ft_tile_asm(const FitArgs &a, const FIns *fwd, const FIns *rev, 
    sweep only; a row that is not finite costs 1e30. */
 template <typename V, int NR, int T>
 __device__ void ft_tile_loss(const FitArgs &a, const FIns *ins, const V *cv,
-                             typename FiV<V, NR>::V4 *stk, double *red, int r0, int r1, double *pt)
+                             typename FiV<V, NR>::V4 *stk, double *red, int r0, int r1, double *pt,
+                             const V *ccols)
 {
     constexpr bool F64 = sizeof(V) == 8;
     const V *cols = F64 ? reinterpret_cast<const V *>(a.cols64) : reinterpret_cast<const V *>(a.cols);
@@ -616,7 +625,7 @@ __device__ void ft_tile_loss(const FitArgs &a, const FIns *ins, const V *cv,
     double local = 0.0;
     for (int row = r0 + NR * tid; row < r1; row += NR * T) {
         V pr[NR];
-        fi_forward<V, NR, false>(ins, cv, cols, a.npad, row, stk, nullptr, T, tid, pr);
+        fi_forward<V, NR, false>(ins, cv, cols, a.npad, row, stk, nullptr, T, tid, pr, ccols);
 #pragma unroll
         for (int i = 0; i < NR; ++i) {
             const int rr = row + i;
@@ -660,14 +669,14 @@ __device__ void ft_tile_loss(const FitArgs &a, const FIns *ins, const V *cv,
 template <int NR, int T>
 __device__ void ft_tile_corr_score(const FitArgs &a, const FIns *ins, const float *cv,
                                    typename FiV<float, NR>::V4 *stk, double *red, int r0, int r1,
-                                   double *pt)
+                                   double *pt, const float *ccols)
 {
     const int tid = threadIdx.x;
     double m[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     int bad = 0;
     for (int row = r0 + NR * tid; row < r1; row += NR * T) {
         float pr[NR];
-        fi_forward<float, NR, false>(ins, cv, a.cols, a.npad, row, stk, nullptr, T, tid, pr);
+        fi_forward<float, NR, false>(ins, cv, a.cols, a.npad, row, stk, nullptr, T, tid, pr, ccols);
 #pragma unroll
         for (int i = 0; i < NR; ++i) {
             const int rr = row + i;
@@ -731,11 +740,20 @@ __global__ void __launch_bounds__(T) ft_sweep4(FitArgs a, int q)
         const FitState *st = a.state + cand;
         const int ib = a.fins_off[cand];
         const int4 info = a.finfo[cand];
-        const int nf = info.x, nr = info.y;
-        const int nins = ft_op_assembles(OPK) ? nf + nr : nf;
+        const int nr = info.y;
+        /* f32 sweeps run the cached forward list (constant-free subtrees read
+           from the cache), the f64 polish the full one */
+        constexpr bool CACHED = sizeof(V) == 4;
+        const int2 fc = CACHED ? a.fcinfo[cand] : make_int2(info.x, 0);
+        const int nf = fc.x;
+        const FIns *fsrc = a.fins + ib + (CACHED ? info.x + nr : 0);
+        const V *ccols = CACHED ? reinterpret_cast<const V *>(a.cache) + (size_t)fc.y * a.npad
+                                : nullptr;
         const int p = a.pcount[cand];
         const int sel = st->sel;
-        for (int i = tid; i < nins; i += T) ins[i] = a.fins[ib + i];
+        for (int i = tid; i < nf; i += T) ins[i] = fsrc[i];
+        if (ft_op_assembles(OPK))
+            for (int i = tid; i < nr; i += T) ins[nf + i] = a.fins[ib + info.x + i];
         if (tid < p) cv[tid] = (V)(sel ? st->trial[tid] : st->c[tid]);
         __syncthreads();
         const int r0 = tile * FT_TILE_ROWS;
@@ -743,14 +761,43 @@ __global__ void __launch_bounds__(T) ft_sweep4(FitArgs a, int q)
         double *pt = a.part + ((size_t)cand * a.ntiles + tile) * FT_PART_STRIDE;
         if (ft_op_assembles(OPK))
             ft_tile_asm<V, NR, T, OPK == FOP_CASM>(a, ins, ins + nf, nr, p, info.z, info.w & 0xffff,
-                                                   info.w >> 16, cv, region, red, r0, r1, pt);
+                                                   info.w >> 16, cv, region, red, r0, r1, pt, ccols);
         else if (OPK == FOP_CSCORE)
             ft_tile_corr_score<NR, T>(a, ins, reinterpret_cast<const float *>(cv),
                                       reinterpret_cast<typename FiV<float, NR>::V4 *>(region), red,
-                                      r0, r1, pt);
+                                      r0, r1, pt, reinterpret_cast<const float *>(ccols));
         else
-            ft_tile_loss<V, NR, T>(a, ins, cv, reinterpret_cast<V4 *>(region), red, r0, r1, pt);
+            ft_tile_loss<V, NR, T>(a, ins, cv, reinterpret_cast<V4 *>(region), red, r0, r1, pt,
+                                   ccols);
         __syncthreads();
+    }
+}
+
+/* Values of the cached constant-free subtrees over all rows, once per fit:
+   one block per (subtree, 4096-row tile), four rows per thread, the same
+   f32 forward sweep the other kinds run (so a cached value is bit-identical
+   to the value a full forward sweep computes). */
+#define FT_FILL_T 128
+__global__ void __launch_bounds__(FT_FILL_T) ft_cache_fill(FitArgs a)
+{
+    using V4 = FiV<float, 4>::V4;
+    extern __shared__ __align__(16) unsigned char sm[];
+    FIns *ins = reinterpret_cast<FIns *>(sm);
+    V4 *stk = reinterpret_cast<V4 *>(sm + 8 * (size_t)((a.sub_maxins + 1) & ~1));
+    const int s = blockIdx.x / a.ntiles, tile = blockIdx.x % a.ntiles;
+    const int tid = threadIdx.x;
+    const int b = a.sub_off[s], ni = a.sub_off[s + 1] - b;
+    for (int i = tid; i < ni; i += FT_FILL_T) ins[i] = a.sub_fins[b + i];
+    __syncthreads();
+    const int r0 = tile * FT_TILE_ROWS, r1 = min(a.n, r0 + FT_TILE_ROWS);
+    float *out = a.cache + (size_t)a.sub_col[s] * a.npad;
+    for (int row = r0 + 4 * tid; row < r1; row += 4 * FT_FILL_T) {
+        float pr[4];
+        fi_forward<float, 4, false>(ins, nullptr, a.cols, a.npad, row, stk, nullptr, FT_FILL_T, tid,
+                                    pr);
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            if (row + i < r1) out[row + i] = pr[i];
     }
 }
 
@@ -1666,7 +1713,7 @@ bool validate_records(const uint32_t *rec, int m, int p, int v)
 
 /* Decode and check a batch of fit-record programs for the device sweeps. */
 void prep_batch(const unsigned int *off, const unsigned int *prog, const int *pcount, int nprog,
-                int v, FitPrep &b, int extra_cols)
+                int v, FitPrep &b, int extra_cols, size_t cache_bytes_per_col, size_t cache_cap)
 {
     b.node_off.resize(nprog + 1);
     b.valid.resize(nprog);
@@ -1688,18 +1735,67 @@ void prep_batch(const unsigned int *off, const unsigned int *prog, const int *pc
     b.fins_off.assign(nprog + 1, 0);
     b.finfo.assign(nprog, make_int4(0, 0, 32, 0));
     b.asm_region = FT_ASM_BUDGET;
-    std::vector<FIns> fwd, rev;
+    const bool caching = cache_bytes_per_col > 0;
+    b.fcinfo.assign(nprog, make_int2(0, 0));
+    b.sub_fins.clear();
+    b.sub_off.assign(1, 0);
+    b.sub_col.clear();
+    b.sub_cand_off.assign(nprog + 1, 0);
+    b.ncache = 0;
+    std::vector<FIns> fwd, rev, fwdc, sf, sr;
+    std::vector<std::vector<uint32_t>> subs;
     for (int i = 0; i < nprog; ++i) {
         b.fins_off[i] = (int)b.fins.size();
+        b.sub_cand_off[i] = (int)b.sub_col.size();
         if (!b.valid[i]) continue;
         int ns = 0, nt = 0;
         const int m = b.node_off[i + 1] - b.node_off[i];
-        if (!fi_decode(prog + off[i], m, fwd, rev, &ns, &nt) || ns > 0xffff || nt > 0x7fff) {
+        if (!fi_decode(prog + off[i], m, fwd, rev, &ns, &nt, caching ? &fwdc : nullptr,
+                       caching ? &subs : nullptr) ||
+            ns > 0xffff || nt > 0x7fff) {
             b.valid[i] = 0;
             continue;
         }
         b.fins.insert(b.fins.end(), fwd.begin(), fwd.end());
         b.fins.insert(b.fins.end(), rev.begin(), rev.end());
+        if (caching) {
+            /* the cached list (or the full one again past the cap) */
+            const bool fits = (size_t)(b.ncache + (int)subs.size()) * cache_bytes_per_col <= cache_cap;
+            bool ok = fits && !subs.empty();
+            std::vector<FIns> cand_sub;
+            std::vector<int> cand_off;
+            int smax = 0, imax = 0;
+            for (size_t s = 0; ok && s < subs.size(); ++s) {
+                int a2 = 0, b2 = 0;
+                if (!fi_decode(subs[s].data(), (int)(subs[s].size() / 4), sf, sr, &a2, &b2)) {
+                    ok = false;
+                    break;
+                }
+                cand_off.push_back((int)cand_sub.size());
+                cand_sub.insert(cand_sub.end(), sf.begin(), sf.end());
+                smax = std::max(smax, a2);
+                imax = std::max(imax, (int)sf.size());
+            }
+            const std::vector<FIns> &use = ok ? fwdc : fwd;
+            b.fins.insert(b.fins.end(), use.begin(), use.end());
+            b.fcinfo[i] = make_int2((int)use.size(), ok ? b.ncache : 0);
+            if (ok) {
+                const int base = (int)b.sub_fins.size();
+                for (size_t s = 0; s < subs.size(); ++s) {
+                    b.sub_col.push_back(b.ncache + (int)s);
+                    b.sub_off.push_back(base + (s + 1 < subs.size() ? cand_off[s + 1]
+                                                                    : (int)cand_sub.size()));
+                }
+                b.sub_fins.insert(b.sub_fins.end(), cand_sub.begin(), cand_sub.end());
+                b.ncache += (int)subs.size();
+                b.sub_slots = std::max(b.sub_slots, smax);
+                b.sub_maxins = std::max(b.sub_maxins, imax);
+            }
+        } else {
+            /* no cache: the f32 list is the full one again */
+            b.fins.insert(b.fins.end(), fwd.begin(), fwd.end());
+            b.fcinfo[i] = make_int2((int)fwd.size(), 0);
+        }
         const int ncols = pcount[i] + 1 + extra_cols;
         const int A = ft_asm_threads(ns, nt, ncols);
         b.finfo[i] = make_int4((int)fwd.size(), (int)rev.size(), A, ns | (nt << 16));
@@ -1710,7 +1806,10 @@ void prep_batch(const unsigned int *off, const unsigned int *prog, const int *pc
         b.fmaxins = std::max(b.fmaxins, (int)(fwd.size() + rev.size()));
     }
     b.fins_off[nprog] = (int)b.fins.size();
+    b.sub_cand_off[nprog] = (int)b.sub_col.size();
     if (b.fins.empty()) b.fins.resize(1);
+    if (b.sub_fins.empty()) b.sub_fins.resize(1);
+    if (b.sub_col.empty()) b.sub_col.resize(1);
 }
 
 namespace {
@@ -1781,6 +1880,13 @@ unsigned long long enqueue_fit(cudaStream_t s_, int sm_count, const FitArgs &a, 
                                const SweepLaunch *sw, int nkinds)
 {
     const int ctrl_grid = sm_count * 8;
+    unsigned long long k = 0;
+    if (a.nsub > 0) {
+        const size_t smem = 8 * (size_t)((a.sub_maxins + 1) & ~1) +
+                            16 * (size_t)(a.sub_slots > 0 ? a.sub_slots : 1) * FT_FILL_T;
+        ft_cache_fill<<<(unsigned)a.nsub * (unsigned)a.ntiles, FT_FILL_T, smem, s_>>>(a);
+        k = 1;
+    }
     ft_step_reset<<<1, 32, 0, s_>>>(a, 1);
     cudaMemsetAsync(a.work + 1 * FOP_COUNT, 0, sizeof(int) * FOP_COUNT, s_);
     ft_control<<<ctrl_grid, FT_CTRL_T, 0, s_>>>(a, 1, 1);
@@ -1795,7 +1901,7 @@ unsigned long long enqueue_fit(cudaStream_t s_, int sm_count, const FitArgs &a, 
         ft_control<<<ctrl_grid, FT_CTRL_T, 0, s_>>>(a, q, 0);
     }
     ft_flush<<<(a.nprog + 127) / 128, 128, 0, s_>>>(a);
-    return 3ULL + (unsigned long long)steps * (2ULL + (unsigned long long)nkinds);
+    return k + 3ULL + (unsigned long long)steps * (2ULL + (unsigned long long)nkinds);
 }
 
 float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const int *pcount,
@@ -1817,7 +1923,15 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     double t = rc_now_ms();
     if (rc_ensure_f64(c) != 0) return -1.0f;
     FitPrep b;
-    prep_batch(off, prog, pcount, nprog, c->v, b, corr ? 2 : 0);
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        cudaGetLastError();
+        free_b = 0;
+    }
+    const size_t cache_cap = std::min<size_t>((size_t)16 << 30, free_b / 3);
+    const bool use_cache = metric != FM_IMPLICIT;
+    prep_batch(off, prog, pcount, nprog, c->v, b, corr ? 2 : 0,
+               use_cache ? sizeof(float) * (size_t)c->npad : 0, cache_cap);
     const int ntiles = (c->n + FT_TILE_ROWS - 1) / FT_TILE_ROWS;
     const int Wmax = 4 * ((b.pmax + 1 + 3) / 4);
     const size_t words = off[nprog];
@@ -1831,6 +1945,10 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     const size_t o_fins = rc_take(&cur, sizeof(FIns) * b.fins.size());
     const size_t o_finsoff = rc_take(&cur, sizeof(int) * (nprog + 1));
     const size_t o_finfo = rc_take(&cur, sizeof(int4) * nprog);
+    const size_t o_fcinfo = rc_take(&cur, sizeof(int2) * nprog);
+    const size_t o_subf = rc_take(&cur, sizeof(FIns) * b.sub_fins.size());
+    const size_t o_suboff = rc_take(&cur, sizeof(int) * b.sub_off.size());
+    const size_t o_subcol = rc_take(&cur, sizeof(int) * b.sub_col.size());
     const size_t in_end = rc_take(&cur, 0);
     const size_t o_c = rc_take(&cur, sizeof(double) * (size_t)nprog * kmax);
     const size_t o_sse = rc_take(&cur, sizeof(double) * nprog);
@@ -1841,6 +1959,7 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     const size_t o_lists = rc_take(&cur, sizeof(int) * 2 * FOP_COUNT * (size_t)nprog);
     const size_t o_counts = rc_take(&cur, sizeof(int) * 2 * FOP_COUNT);
     const size_t o_work = rc_take(&cur, sizeof(int) * 2 * FOP_COUNT);
+    const size_t o_cache = rc_take(&cur, sizeof(float) * (size_t)c->npad * (size_t)b.ncache);
     const size_t dev_end = rc_take(&cur, 0);
     if (rc_reserve(c, dev_end, io_end) != 0) return -1.0f;
     st->alloc_ms += rc_now_ms() - t;
@@ -1856,6 +1975,10 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     memcpy(host + o_fins, b.fins.data(), sizeof(FIns) * b.fins.size());
     memcpy(host + o_finsoff, b.fins_off.data(), sizeof(int) * (nprog + 1));
     memcpy(host + o_finfo, b.finfo.data(), sizeof(int4) * nprog);
+    memcpy(host + o_fcinfo, b.fcinfo.data(), sizeof(int2) * nprog);
+    memcpy(host + o_subf, b.sub_fins.data(), sizeof(FIns) * b.sub_fins.size());
+    memcpy(host + o_suboff, b.sub_off.data(), sizeof(int) * b.sub_off.size());
+    memcpy(host + o_subcol, b.sub_col.data(), sizeof(int) * b.sub_col.size());
     memcpy(host + o_c, c0, sizeof(double) * (size_t)nprog * kmax);
     st->h2d_ms += rc_now_ms() - t;
     st->h2d_bytes += io_end;
@@ -1882,6 +2005,14 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     a.fins = reinterpret_cast<const FIns *>(dev + o_fins);
     a.fins_off = reinterpret_cast<const int *>(dev + o_finsoff);
     a.finfo = reinterpret_cast<const int4 *>(dev + o_finfo);
+    a.fcinfo = reinterpret_cast<const int2 *>(dev + o_fcinfo);
+    a.cache = reinterpret_cast<float *>(dev + o_cache);
+    a.sub_fins = reinterpret_cast<const FIns *>(dev + o_subf);
+    a.sub_off = reinterpret_cast<const int *>(dev + o_suboff);
+    a.sub_col = reinterpret_cast<const int *>(dev + o_subcol);
+    a.nsub = (int)b.sub_off.size() - 1;
+    a.sub_slots = b.sub_slots;
+    a.sub_maxins = b.sub_maxins;
     a.asm_region = b.asm_region;
     a.fslots = b.fslots;
     a.ftape = b.ftape;
@@ -1937,6 +2068,10 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
             one.gauge = a.gauge + 2 * (size_t)i;
             one.fins_off = a.fins_off + i;
             one.finfo = a.finfo + i;
+            one.fcinfo = a.fcinfo + i;
+            one.sub_off = a.sub_off + b.sub_cand_off[i];
+            one.sub_col = a.sub_col + b.sub_cand_off[i];
+            one.nsub = b.sub_cand_off[i + 1] - b.sub_cand_off[i];
             one.state = a.state + i;
             one.part = a.part + (size_t)i * ntiles * FT_PART_STRIDE;
             one.outc = a.outc + (size_t)i * kmax;
@@ -1950,6 +2085,9 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
         snprintf(key, sizeof(key), "%p|%d|%d|%d|%d|%d|%d|%d|%d|%d|%zu|%d|%d|%d|%zu", (void *)dev,
                  nprog, kmax, ntiles, b.mmax, Wmax, iters, metric, flags, steps, io_end, b.fslots,
                  b.ftape, b.fmaxins, b.asm_region);
+        const size_t kl = strlen(key);
+        snprintf(key + kl, sizeof(key) - kl, "|%d|%d|%d|%d", b.ncache, a.nsub, b.sub_slots,
+                 b.sub_maxins);
         if (!c->fit_graph || c->fit_graph_key != key) {
             if (c->fit_graph) {
                 cudaGraphExecDestroy(c->fit_graph);

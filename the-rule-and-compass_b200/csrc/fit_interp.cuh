@@ -32,11 +32,12 @@
 enum FiKind {
     FI_PUSH_VAR = 0,   /* spill TOS to `spill`; TOS = x[imm]. Reverse: restore only */
     FI_PUSH_PARAM = 1, /* spill TOS; TOS = c[imm] */
-    FI_UNARY = 2,      /* TOS = op(TOS) */
-    FI_BIN_S = 3,      /* TOS = op(slot[arg], TOS) */
-    FI_BIN_V = 4,      /* TOS = op(TOS, x[imm]) */
-    FI_BIN_P = 5,      /* TOS = op(TOS, c[imm]) */
-    FI_HALT = 6
+    FI_PUSH_CACHE = 2, /* spill TOS; TOS = cached column imm of the candidate */
+    FI_UNARY = 3,      /* TOS = op(TOS) */
+    FI_BIN_S = 4,      /* TOS = op(slot[arg], TOS) */
+    FI_BIN_V = 5,      /* TOS = op(TOS, x[imm]) */
+    FI_BIN_P = 6,      /* TOS = op(TOS, c[imm]) */
+    FI_HALT = 7
 };
 
 /* Flag bits above the kind: the left (or only) / right operand's subtree
@@ -64,16 +65,23 @@ __host__ __device__ constexpr bool fi_nonlinear(unsigned op)
 /* Host translation of one fit-record program into the forward list `fwd`
    (ending in HALT) and the reverse list `rev` (walked last to first).
    Returns false when the records are not a tree in stack (post-) order,
-   which the device path rejects. */
+   which the device path rejects.
+
+   With `fwdc`, also the forward list in which every maximal constant-free
+   subtree of two or more instructions is replaced by one push of a cached
+   column (its values over all rows do not depend on the constants, so they
+   are computed once per fit), and in `subs` the records of each such
+   subtree, renumbered as a program of its own, in cache-column order. */
 inline bool fi_decode(const uint32_t *rec, int m, std::vector<FIns> &fwd, std::vector<FIns> &rev,
-                      int *nslots, int *ntape)
+                      int *nslots, int *ntape, std::vector<FIns> *fwdc = nullptr,
+                      std::vector<std::vector<uint32_t>> *subs = nullptr)
 {
     struct Ent {
         int rec, first;
         bool hp;
     };
     std::vector<Ent> stack;
-    std::vector<int> lo(m, 0), hi(m, -1), kid0(m, -1), kid1(m, -1);
+    std::vector<int> lo(m, 0), hi(m, -1), kid0(m, -1), kid1(m, -1), first_rec(m, 0);
     std::vector<char> hp(m, 0), fused(m, 0);
     int depth = 0, maxslot = -1, tape = 0;
     fwd.clear();
@@ -98,6 +106,7 @@ inline bool fi_decode(const uint32_t *rec, int m, std::vector<FIns> &fwd, std::v
             }
             ++depth;
             hp[i] = op == OP_CONST;
+            first_rec[i] = i;
             lo[i] = (int)fwd.size();
             stack.push_back({i, (int)fwd.size(), op == OP_CONST});
             fwd.push_back(in);
@@ -112,6 +121,7 @@ inline bool fi_decode(const uint32_t *rec, int m, std::vector<FIns> &fwd, std::v
             hp[i] = h;
             kid0[i] = (int)k0;
             kid1[i] = (int)k1;
+            first_rec[i] = first_rec[k0];
             unsigned flags = 0;
             int np = 0;
             if (h) {
@@ -142,6 +152,7 @@ inline bool fi_decode(const uint32_t *rec, int m, std::vector<FIns> &fwd, std::v
             const Ent C = stack.back();
             hp[i] = C.hp;
             kid0[i] = (int)k0;
+            first_rec[i] = first_rec[k0];
             in.kind = (uint8_t)(FI_UNARY | (C.hp ? FI_HP_L : 0u));
             if (C.hp && fi_nonlinear(op)) ++tape;
             lo[i] = C.first;
@@ -203,6 +214,56 @@ inline bool fi_decode(const uint32_t *rec, int m, std::vector<FIns> &fwd, std::v
             if (seen[rev[j].imm]) rev[j].kind |= FI_ACC;
             seen[rev[j].imm] = 1;
         }
+    }
+    if (fwdc) {
+        /* cacheable: constant-free, its own instructions (not a fused leaf),
+           two or more of them, and its parent has a constant (or it is the
+           whole tree) */
+        std::vector<int> parent(m, -1);
+        for (int i = 0; i < m; ++i) {
+            if (kid0[i] >= 0) parent[kid0[i]] = i;
+            if (kid1[i] >= 0) parent[kid1[i]] = i;
+        }
+        std::vector<int> start_of(nf, -1);
+        for (int k = 0; k < m; ++k) {
+            if (hp[k] || fused[k] || hi[k] - lo[k] < 1) continue;
+            if (parent[k] >= 0 && !hp[parent[k]]) continue;
+            start_of[lo[k]] = k;
+        }
+        fwdc->clear();
+        if (subs) subs->clear();
+        int col = 0;
+        for (int j = 0; j < nf;) {
+            const int k = start_of[j];
+            if (k < 0) {
+                fwdc->push_back(fwd[j]);
+                ++j;
+                continue;
+            }
+            FIns c = fwd[j];
+            c.kind = FI_PUSH_CACHE;
+            c.op = 0;
+            c.arg = 0;
+            c.imm = (uint16_t)col++;
+            c.tape = 0;
+            fwdc->push_back(c);
+            if (subs) {
+                const int b = first_rec[k];
+                std::vector<uint32_t> s(4 * (size_t)(k - b + 1));
+                for (int r = b; r <= k; ++r) {
+                    const uint32_t op = rec[4 * r];
+                    const bool leaf = op == OP_CONST || op == OP_VAR;
+                    const bool bin = !leaf && ft_op_binary(op);
+                    s[4 * (r - b) + 0] = op;
+                    s[4 * (r - b) + 1] = leaf ? rec[4 * r + 1] : rec[4 * r + 1] - (uint32_t)b;
+                    s[4 * (r - b) + 2] = bin ? rec[4 * r + 2] - (uint32_t)b : rec[4 * r + 2];
+                    s[4 * (r - b) + 3] = rec[4 * r + 3];
+                }
+                subs->push_back(std::move(s));
+            }
+            j = hi[k] + 1;
+        }
+        fwdc->push_back(fwd[nf]);
     }
     return true;
 }
@@ -315,14 +376,16 @@ __device__ __forceinline__ V fi_child(V a, V d)
     } break;
 
 /* Forward sweep of the thread's NR rows. Constants from `cf`, inputs from
-   the columns at `row` (aligned to the row vector). Spill slots and the tape
-   are [slot][S] row vectors with this thread at `tid`. The prediction of
-   row i is left in out[i]. */
+   the columns at `row` (aligned to the row vector), cached subtree values
+   from `ccols` (same stride). Spill slots and the tape are [slot][S] row
+   vectors with this thread at `tid`. The prediction of row i is left in
+   out[i]. */
 template <typename V, int NR, bool PARTIALS>
 __device__ __forceinline__ void fi_forward(const FIns *__restrict__ prog, const V *cf,
                                            const V *__restrict__ cols, int npad, int row,
                                            typename FiV<V, NR>::V4 *stk,
-                                           typename FiV<V, NR>::V4 *tape, int S, int tid, V *out)
+                                           typename FiV<V, NR>::V4 *tape, int S, int tid, V *out,
+                                           const V *__restrict__ ccols = nullptr)
 {
     using F = FiV<V, NR>;
     V t[NR];
@@ -332,10 +395,12 @@ __device__ __forceinline__ void fi_forward(const FIns *__restrict__ prog, const 
         const FIns in = prog[pc];
         const unsigned kind = in.kind;
         const unsigned k = kind & FI_KIND_MASK;
-        if (k <= FI_PUSH_PARAM) {
+        if (k <= FI_PUSH_CACHE) {
             if (in.spill != 0xff) stk[in.spill * S + tid] = F::pack(t);
             if (k == FI_PUSH_VAR) {
                 F::ldg(cols + (size_t)in.imm * (size_t)npad + row, t);
+            } else if (k == FI_PUSH_CACHE) {
+                F::ldg(ccols + (size_t)in.imm * (size_t)npad + row, t);
             } else {
                 const V c = cf[in.imm];
 #pragma unroll
@@ -435,7 +500,7 @@ __device__ __forceinline__ bool fi_reverse(const FIns *__restrict__ rev, int nr,
         const FIns in = rev[pc];
         const unsigned kind = in.kind;
         const unsigned k = kind & FI_KIND_MASK;
-        if (k <= FI_PUSH_PARAM) {
+        if (k <= FI_PUSH_CACHE) {
             if (k == FI_PUSH_PARAM) {
                 V *gs = g + in.imm * R;
 #pragma unroll

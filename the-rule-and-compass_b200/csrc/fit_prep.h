@@ -22,10 +22,25 @@ struct FitPrep {
     int fslots = 1;                   /* most spill slots */
     int ftape = 1;                    /* most tape slots */
     int fmaxins = 2;                  /* longest forward + reverse list */
+
+    /* constant-free subtree cache (requested by prep_batch's cache_npad) */
+    std::vector<int2> fcinfo;         /* per candidate: cached forward count (the list
+                                         follows the reverse list), first cache column */
+    std::vector<FIns> sub_fins;       /* forward lists of the cached subtrees */
+    std::vector<int> sub_off;         /* [nsub + 1] */
+    std::vector<int> sub_col;         /* [nsub] cache column of each subtree */
+    std::vector<int> sub_cand_off;    /* [P + 1] first subtree of each candidate */
+    int ncache = 0;                   /* cache columns */
+    int sub_slots = 1;                /* most spill slots of a subtree program */
+    int sub_maxins = 2;               /* longest subtree program */
 };
 
 /* Validate and translate `nprog` programs (`off` in words); a rejected
    program has valid[i] = 0 and no instructions. `extra_cols` widens the
-   assembly's Gram beyond p + 1 columns (the correlation moments use 2). */
+   assembly's Gram beyond p + 1 columns (the correlation moments use 2).
+   With cache_bytes_per_col > 0, constant-free subtrees are cached (columns of
+   that many bytes) while the total stays within cache_cap bytes; later
+   candidates keep their full forward list. */
 void prep_batch(const unsigned int *off, const unsigned int *prog, const int *pcount, int nprog,
-                int v, FitPrep &b, int extra_cols = 0);
+                int v, FitPrep &b, int extra_cols = 0, size_t cache_bytes_per_col = 0,
+                size_t cache_cap = 0);
