@@ -11,9 +11,9 @@
  *    consecutive rows at once, so one warp-uniform dispatch drives four rows
  *    and deeper stack entries live in fixed per-thread shared-memory slots;
  *  - a work item is (a group of G candidates of similar length, a tile of
- *    rows): the tile's feature rows are staged once in shared memory and
- *    reused by all G candidates, which divides the L2 traffic of the feature
- *    matrix by G;
+ *    rows); each warp runs one candidate over all of its rows of the tile
+ *    (features read from L2, where the whole matrix stays resident) and
+ *    reduces once, and a hard failure ends the warp's rows of that candidate;
  *  - items are handed out by an atomic counter over groups ordered by
  *    decreasing program length (longest first), so uneven lengths do not
  *    leave a tail;
@@ -246,7 +246,8 @@ float rc_score_run(RcCtx *c, const uint32_t *words, const uint32_t *off, int wid
         });
     }
     const int Tb[2] = {256, 64};
-    const int staged = (c->v + 1) <= stage_limit_cols() + 1 ? 1 : 0;
+    /* the scoring kernel reads features from L2; nothing is staged */
+    const int staged = 0;
     const int ntiles = std::max(1, (c->n + TILE_ROWS - 1) / TILE_ROWS);
     std::vector<int> cand_tiles(nprog, ntiles);
     std::vector<int> order;

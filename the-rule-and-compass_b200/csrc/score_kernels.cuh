@@ -529,7 +529,6 @@ __global__ void __launch_bounds__(T) rc_score_kernel(ScoreArgs a)
     constexpr int NW = T / 32;
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
-    float4 *xs = reinterpret_cast<float4 *>(smem_raw);
     float4 *stk = reinterpret_cast<float4 *>(smem_raw + ScoreSmem<T>::xs_bytes(a.v, a.staged));
     uint2 *estk = reinterpret_cast<uint2 *>(stk + a.nslots * T);
     double *swarp = reinterpret_cast<double *>(estk + a.nslots * T);
@@ -557,31 +556,26 @@ __global__ void __launch_bounds__(T) rc_score_kernel(ScoreArgs a)
             for (int q = tid; q < e - b; q += T) sprog[c * a.maxins + q] = a.ins[b + q];
             if (skip_bad && *((volatile int *)(a.bad + cand))) skipmask |= 1u << c;
         }
-        for (int q = tid; q < gcount * NW * 4; q += T) swarp[q] = mode == SM_MAXIMUM ? 0.0 : 0.0;
-        if (tid == 0) s_bad = skipmask;
+        for (int q = tid; q < gcount * NW * 4; q += T) swarp[q] = 0.0;
+        if (tid == 0) s_bad = 0;
         __syncthreads();
 
-        for (int s = 0; s < a.subtiles; ++s) {
-            const int row0 = (tile * a.subtiles + s) * SUB;
-            if (row0 >= a.n) break;
-            const int myrow = row0 + 4 * tid;
-            const float4 yv4 = __ldg(reinterpret_cast<const float4 *>(a.y + myrow));
-            if (a.staged) {
-                for (int k = 0; k < a.v; ++k) {
-                    xs[k * T + tid] = __ldg(reinterpret_cast<const float4 *>(
-                        a.cols + (size_t)k * (size_t)a.npad + (size_t)myrow));
-                }
-            }
-            __syncthreads();
-            for (int c = 0; c < gcount; ++c) {
-                /* a candidate already known to be a hard failure skips its rows */
-                if (skip_bad && (*((volatile unsigned *)&s_bad) & (1u << c))) continue;
-                const int cand = a.order[cbase + c];
+        /* each warp runs one candidate over all of the tile's rows before its
+           single reduction; the features come straight from L2 */
+        for (int c = 0; c < gcount; ++c) {
+            /* a candidate already known to be a hard failure skips its rows */
+            if (skip_bad && (skipmask & (1u << c))) continue;
+            const int cand = a.order[cbase + c];
+            double a0 = 0.0, a1 = 0.0, e0 = 0.0, e1 = 0.0;
+            int bad = 0;
+            for (int s = 0; s < a.subtiles; ++s) {
+                const int row0 = (tile * a.subtiles + s) * SUB;
+                if (row0 >= a.n) break;
+                const int myrow = row0 + 4 * tid;
                 float4 p, pe;
-                rc_run<T, TRACK>(sprog + c * a.maxins, xs, a.staged != 0, a.cols, a.npad, myrow,
-                                 stk, estk, tid, p, pe);
-                double a0 = 0.0, a1 = 0.0, e0 = 0.0, e1 = 0.0;
-                int bad = 0;
+                rc_run<T, TRACK>(sprog + c * a.maxins, nullptr, false, a.cols, a.npad, myrow, stk,
+                                 estk, tid, p, pe);
+                const float4 yv4 = __ldg(reinterpret_cast<const float4 *>(a.y + myrow));
                 const float pr[4] = {p.x, p.y, p.z, p.w};
                 const float pq[4] = {pe.x, pe.y, pe.z, pe.w};
                 const float yy[4] = {yv4.x, yv4.y, yv4.z, yv4.w};
@@ -592,35 +586,32 @@ __global__ void __launch_bounds__(T) rc_score_kernel(ScoreArgs a)
                         rc_accumulate(a, mode, pr[i], pq[i], yy[i], row, cand, a0, a1, e0, e1,
                                       bad);
                 }
-                if (mode == SM_PREDICT) continue;
-                if (mode == SM_MAXIMUM) {
-                    a0 = rc_warp_max(a0);
-                    e0 = rc_warp_max(e0);
-                } else {
-                    a0 = rc_warp_sum(a0);
-                    if (TRACK) e0 = rc_warp_sum(e0);
-                    if (mode == SM_CORR_PASS2 || (mode >= SM_LOG_LOSS && mode <= SM_HINGE_SQUARED)) {
-                        a1 = rc_warp_sum(a1);
-                        if (TRACK) e1 = rc_warp_sum(e1);
-                    }
-                }
-                const unsigned anybad = __any_sync(0xffffffffu, bad);
-                if (lane == 0) {
-                    double *sw = swarp + (c * NW + warp) * 4;
-                    if (mode == SM_MAXIMUM) {
-                        sw[0] = fmax(sw[0], a0);
-                        sw[2] = fmax(sw[2], e0);
-                    } else {
-                        sw[0] += a0;
-                        sw[1] += a1;
-                        sw[2] += e0;
-                        sw[3] += e1;
-                    }
-                    if (anybad) atomicOr(&s_bad, 1u << c);
+                /* a hard failure ends this warp's rows of the candidate */
+                if (skip_bad && __any_sync(0xffffffffu, bad)) break;
+            }
+            if (mode == SM_PREDICT) continue;
+            if (mode == SM_MAXIMUM) {
+                a0 = rc_warp_max(a0);
+                e0 = rc_warp_max(e0);
+            } else {
+                a0 = rc_warp_sum(a0);
+                if (TRACK) e0 = rc_warp_sum(e0);
+                if (mode == SM_CORR_PASS2 || (mode >= SM_LOG_LOSS && mode <= SM_HINGE_SQUARED)) {
+                    a1 = rc_warp_sum(a1);
+                    if (TRACK) e1 = rc_warp_sum(e1);
                 }
             }
-            __syncthreads();
+            const unsigned anybad = __any_sync(0xffffffffu, bad);
+            if (lane == 0) {
+                double *sw = swarp + (c * NW + warp) * 4;
+                sw[0] = a0;
+                sw[1] = a1;
+                sw[2] = e0;
+                sw[3] = e1;
+                if (anybad) atomicOr(&s_bad, 1u << c);
+            }
         }
+        __syncthreads();
 
         /* Warps in ascending order: one partial per (candidate, tile). */
         if (tid < gcount * 4 && mode != SM_PREDICT) {
