@@ -7,6 +7,7 @@ librcsr_b200.so and checks that it exports every function include/rcsr_b200.h
 declares.
 """
 import ctypes
+import importlib
 import os
 import re
 
@@ -118,3 +119,27 @@ def test_fit_kernel_info_contract(pkg):
     assert L.rc_fit_kernel_info(20, ctypes.byref(t), ctypes.byref(s), ctypes.byref(m)) == 0
     assert m.value == 20 and t.value > 0 and s.value > 0
     assert L.rc_fit_kernel_info(21, ctypes.byref(t), ctypes.byref(s), ctypes.byref(m)) == -1
+
+
+def test_fit_admission_rules(pkg):
+    """search.rs:3006-3074: admission_count and select_promoted."""
+    H = importlib.import_module("the-rule-and-compass_b200.host")
+    assert H.admission_count(100, 1000) == 32
+    assert H.admission_count(200, 1000) == 50
+    assert H.admission_count(20, 1000) == 20
+    assert H.admission_count(1000, 1 << 20) == 1000
+    assert H.admission_count(0, 10) == 1
+    rng = np.random.Generator(np.random.PCG64(5))
+    pops = [40, 200, 7]
+    pending = [(i, j) for i, p in enumerate(pops) for j in range(p) if rng.uniform() < 0.8]
+    err = np.round(rng.uniform(0, 1, len(pending)), 1)      # many ties
+    cx = rng.integers(1, 5, len(pending)).astype(float)       # ties too
+    hc = rng.uniform(size=len(pending)) < 0.9
+    for rows in (1000, 1 << 20):
+        got = H.select_promoted(pops, pending, err, cx, hc, rows)
+        want = []
+        for i, p in enumerate(pops):
+            ranked = sorted([(err[k], cx[k], j) for k, (ii, j) in enumerate(pending)
+                             if ii == i and hc[k]])
+            want += [(i, j) for _, _, j in ranked[: H.admission_count(p, rows)]]
+        assert got == sorted(want)

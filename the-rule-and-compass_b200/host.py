@@ -40,6 +40,14 @@ def lib():
                                    P(ctypes.c_uint32), ctypes.c_int, P(ctypes.c_double),
                                    ctypes.c_int, P(ctypes.c_int32), P(ctypes.c_int),
                                    ctypes.c_int]
+        L.rch_admission_count.restype = ctypes.c_int
+        L.rch_admission_count.argtypes = [ctypes.c_int, ctypes.c_longlong]
+        L.rch_select_promoted.restype = ctypes.c_int
+        L.rch_select_promoted.argtypes = [ctypes.c_int, P(ctypes.c_int32), ctypes.c_int,
+                                          P(ctypes.c_int32), P(ctypes.c_int32),
+                                          P(ctypes.c_double), P(ctypes.c_double),
+                                          P(ctypes.c_uint8), ctypes.c_longlong,
+                                          P(ctypes.c_int32), P(ctypes.c_int32), ctypes.c_int]
         _lib = L
     return _lib
 
@@ -170,3 +178,31 @@ def pack_plans(plans, kmax=None):
         c0[i, : p.nconst] = p.c0
     gauge = np.concatenate([p.gauge for p in plans]).astype(np.int32)
     return prog, off, pcount, c0, gauge, kmax
+
+
+def admission_count(island_pop, train_rows):
+    """Offspring of one island admitted to the fitted batch
+    (my-version/src/search.rs:3006-3031)."""
+    return lib().rch_admission_count(int(island_pop), int(train_rows))
+
+
+def select_promoted(island_pop, pending, error, complexity, has_constants, train_rows):
+    """The (island, index) pairs promoted to the fitted batch
+    (my-version/src/search.rs:3033-3074). `pending` is a list of (island,
+    index); `error`, `complexity` and `has_constants` are aligned with it."""
+    isl = np.asarray([p[0] for p in pending], np.int32)
+    idx = np.asarray([p[1] for p in pending], np.int32)
+    pops = np.asarray(island_pop, np.int32)
+    err = np.ascontiguousarray(error, np.float64)
+    cx = np.ascontiguousarray(complexity, np.float64)
+    hc = np.ascontiguousarray(has_constants, np.uint8)
+    oi = np.zeros(max(len(pending), 1), np.int32)
+    oj = np.zeros(max(len(pending), 1), np.int32)
+    k = lib().rch_select_promoted(len(pops), _p(pops, ctypes.c_int32), len(pending),
+                                  _p(isl, ctypes.c_int32), _p(idx, ctypes.c_int32),
+                                  _p(err, ctypes.c_double), _p(cx, ctypes.c_double),
+                                  _p(hc, ctypes.c_uint8), int(train_rows),
+                                  _p(oi, ctypes.c_int32), _p(oj, ctypes.c_int32), len(oi))
+    if k < 0:
+        raise RuntimeError("rch_select_promoted failed")
+    return list(zip(oi[:k].tolist(), oj[:k].tolist()))

@@ -15,6 +15,7 @@
  * device opcodes, 64..66 the inverse hyperbolics. Exposed through a small C
  * API (rch_*) for the Python package and the benchmark.
  */
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -269,6 +270,67 @@ int rch_fit_plan(const int *ops, const double *vals, int nn, uint32_t *words, in
     }
     *nconst = f.nconst;
     return m;
+}
+
+/* my-version/src/search.rs:3006-3031 `admission_count`: how many of an
+   island's offspring enter the fitted batch. From 2^20 training rows every
+   candidate with constants; below, a quarter of the island floored at 32 and
+   capped at the island size. */
+int rch_admission_count(int island_pop, long long train_rows)
+{
+    if (island_pop < 1) island_pop = 1;
+    if (train_rows >= (1LL << 20)) return island_pop;
+    int k = island_pop / 4;
+    if (k < 32) k = 32;
+    if (k > island_pop) k = island_pop;
+    return k < 1 ? 1 : k;
+}
+
+/* search.rs:3033-3074 `select_promoted`: per island, the pending offspring
+   that have constants, ranked by screened error, then complexity, then
+   population index; the best admission_count(island_pop) of each island are
+   promoted. The result is (island, index) pairs in ascending order. Errors
+   are compared with NaN treated as larger than every number (a total order;
+   screening reports +inf, not NaN, for a failed candidate). Returns the count,
+   or -1 when `cap` is too small. */
+int rch_select_promoted(int nislands, const int *island_pop, int npending, const int *pend_island,
+                        const int *pend_index, const double *error, const double *complexity,
+                        const unsigned char *has_constants, long long train_rows, int *out_island,
+                        int *out_index, int cap)
+{
+    struct Cand {
+        int j;
+        double err, cx;
+    };
+    auto key_lt = [](double a, double b) {
+        const bool na = std::isnan(a), nb = std::isnan(b);
+        if (na || nb) return !na && nb;
+        return a < b;
+    };
+    std::vector<std::pair<int, int>> out;
+    for (int i = 0; i < nislands; ++i) {
+        std::vector<Cand> ranked;
+        for (int k = 0; k < npending; ++k)
+            if (pend_island[k] == i && has_constants[k])
+                ranked.push_back({pend_index[k], error[k], complexity[k]});
+        std::stable_sort(ranked.begin(), ranked.end(), [&](const Cand &a, const Cand &b) {
+            if (key_lt(a.err, b.err)) return true;
+            if (key_lt(b.err, a.err)) return false;
+            if (key_lt(a.cx, b.cx)) return true;
+            if (key_lt(b.cx, a.cx)) return false;
+            return a.j < b.j;
+        });
+        const int take = std::min<int>(rch_admission_count(island_pop[i], train_rows),
+                                       (int)ranked.size());
+        for (int q = 0; q < take; ++q) out.push_back({i, ranked[q].j});
+    }
+    std::sort(out.begin(), out.end());
+    if ((int)out.size() > cap) return -1;
+    for (size_t q = 0; q < out.size(); ++q) {
+        out_island[q] = out[q].first;
+        out_index[q] = out[q].second;
+    }
+    return (int)out.size();
 }
 
 }  /* extern "C" */
