@@ -271,3 +271,58 @@ def test_autotune_keeps_scores_bit_identical(pkg, tmp_path):
     assert ev.launch_count() > n0
     ev.close()
     ev2.close()
+
+
+def _fnv1a(words):
+    h = 0xcbf29ce484222325
+    for w in words:
+        h ^= int(w)
+        h = (h * 0x100000001b3) & 0xFFFFFFFFFFFFFFFF
+        if w == 255:
+            break
+    return h
+
+
+def test_fixed_width_pool_matches_the_packed_batch(pkg):
+    """rc_pool_reserve/upload/score/eval/hash (eval.cu:3514-3874): a
+    fixed-width pool scores and evaluates exactly like the packed batch, and
+    its hash is genome::postfix_hash (FNV-1a over the words up to HALT,
+    my-version/src/genome.rs:43-52)."""
+    import ctypes
+    D = importlib.import_module("the-rule-and-compass_b200.device")
+    W = importlib.import_module("the-rule-and-compass_b200.workloads")
+    trees, x, y = W.scoring_workload(96, 20000, seed=11)
+    ev = pkg.GpuEvaluator(x.reshape(-1), 20000, 5, y)
+    prog, off = pkg.Population(trees).programs()
+    P = len(off) - 1
+    width = int(np.max(np.diff(off))) + 3
+    pool = np.full((P, width), 255, np.uint32)
+    for i in range(P):
+        pool[i, : off[i + 1] - off[i]] = prog[off[i]:off[i + 1]]
+    flat = np.ascontiguousarray(pool.reshape(-1))
+    L = D.lib()
+    assert L.rc_pool_reserve(ev.ctx, P, width) == 0
+    pc = np.zeros(P, np.int32)
+    want, wst, _ = ev.score_batch(prog, off, 0, pc)
+    wev, _ = ev.eval_batch(prog, off, 0)
+    for which in (0, 1):
+        assert L.rc_pool_upload(ev.ctx, which, flat.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+                                P) == 0
+        out = np.zeros(P, np.float64)
+        st = np.zeros(P, np.int32)
+        ms = L.rc_pool_score(ev.ctx, which, P, width, 0,
+                             pc.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                             out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                             st.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)))
+        assert ms >= 0
+        assert np.array_equal(st, wst)
+        assert np.array_equal(out.view(np.uint64), want.view(np.uint64))
+        f = np.zeros(P, np.float32)
+        assert L.rc_pool_eval(ev.ctx, which, P, width,
+                              f.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), 0) >= 0
+        assert np.array_equal(f.view(np.uint32), wev.view(np.uint32))
+        h = np.zeros(P, np.uint64)
+        assert L.rc_pool_hash(ev.ctx, which, P, width,
+                              h.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))) == 0
+        assert [int(v) for v in h] == [_fnv1a(pool[i]) for i in range(P)]
+    ev.close()
