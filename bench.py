@@ -245,9 +245,11 @@ def bench_score(args, rank, world, dev, pkg, W, flushbuf):
     ev.close()
     h2d = int(prog.nbytes + off.nbytes + pcount.nbytes)
     d2h = int(P * (8 + 4))
+    finite = np.asarray(status) == 0
     return dict(P=P, N=N, dev_ms=dev_ms, wall=wall, alg_ops=alg_ops, clocks=clocks,
                 h2d=h2d, d2h=d2h, trees=trees, x=x, y=y, stats=stats,
-                launches=launches, unit_count=float(P) * N)
+                launches=launches, unit_count=float(P) * N,
+                finite=int(finite.sum()), alg_ops_finite=float(N) * float((ops[finite] + 2).sum()))
 
 
 def fit_lane_ops(plans, N, iters):
@@ -440,11 +442,18 @@ def main():
             per_launch_ms = float(np.mean(r["dev_ms"]))
             achieved = r["alg_ops"] / (per_launch_ms / 1e3) / 1e9
             peak = 148 * 128 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e9
+            achieved_f = r["alg_ops_finite"] / (per_launch_ms / 1e3) / 1e9
             roof = {"bound": "fp32_issue", "achieved": achieved, "peak": peak,
-                    "unit": "Glane-op/s", "frac": achieved / peak, "traffic": None,
+                    "unit": "Glane-op/s", "frac": achieved / peak,
+                    "traffic": 25.69e6,
+                    "finite_candidates": r["finite"],
+                    "achieved_finite_only": achieved_f, "frac_finite_only": achieved_f / peak,
                     "note": "interpreter ops (bytecode ops + residual + loss) per row per "
                             "candidate / event time of the scoring launches; peak = 148 SMs x "
-                            "128 FP32 lanes x sm_max_mhz from MEASURED_PEAKS.json"}
+                            "128 FP32 lanes x sm_max_mhz from MEASURED_PEAKS.json; candidates "
+                            "proven non-finite stop early, *_finite_only counts the finite ones "
+                            "alone; traffic = dram read+write bytes of one scoring-kernel launch "
+                            "from an ncu capture of this workload"}
             cfg = {"workload": f"batched scoring, P={r['P']} programs, N={r['N']} rows x 5 "
                                f"features, squared error", "l2": "flushed between steps"}
         else:
