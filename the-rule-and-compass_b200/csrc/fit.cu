@@ -303,7 +303,7 @@ __global__ void __launch_bounds__(T) ft_sweep(FitArgs a, int q)
 /* ---- four-rows-per-thread sweeps ------------------------------------- */
 
 #define FT_ASM_T 128
-#define FT_ASM_BUDGET (48 * 1024)
+#define FT_ASM_BUDGET (40 * 1024)
 
 /* Rows per thread of each sweep: the assemblies carry 8 bytes of rows per
    thread (two f32 or one f64 row) to fit more threads beside their tapes;
