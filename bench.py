@@ -3,15 +3,20 @@
 Default workload (`--workload score`): batched evaluation + squared-error
 scoring of P = 4096 random expression programs over N = 1,048,576 rows x 5
 features (the batched-scoring configuration), metric expr*row evals/s. On one
-GPU the same line also carries, under "fit" and "rank", the second headline
-metric and the exact-statistics stage:
-  fit:  batched LM fit of P = 2048 candidates (1-20 constants, 5-60 nodes,
-        20 iterations) over N = 262,144 rows x 8 features, fitted
-        candidates/s, for the fused graph-replayed batch and for the plain
-        one-candidate-at-a-time form of the same steps (on a subset);
-  rank: exact rank-correlation sums of 64 candidates over N = 1,048,576 rows
-        x 10 features, candidate*rows/s.
-`--workload fit` makes the fit the primary line.
+GPU the same line also carries the other configurations:
+  fit:      batched LM fit of P = 2048 candidates (1-20 constants, 5-60
+            nodes, 20 iterations) over N = 262,144 rows x 8 features, fitted
+            candidates/s, for the fused graph-replayed batch and for the plain
+            one-candidate-per-launch form of the same steps (on a seeded
+            random sample of the batch);
+  fit_1m:   the same fit distribution at N = 1,048,576 rows;
+  implicit: |f|/||grad f|| scoring of P = 1024 candidates of f(x, y, d1, d2)
+            over N = 1,048,576 rows through the fused input adjoint, and the
+            LM fit of those with constants;
+  c5:       one island's generation (P = 1000) over N = 4,194,304 rows x 10
+            heavy-tailed features: the L1 IRLS fit and the exact
+            rank-correlation sums.
+`--workload fit|implicit|c5|rank` makes one of them the primary line.
 
 One step is one pass of the hot path over the whole batch. `value` is
 device-timed with CUDA events on the library's stream (inputs resident in
@@ -262,102 +267,221 @@ def fit_lane_ops(plans, N, iters):
     return fp32 + 2.0 * fp64
 
 
-def bench_fit(args, rank, world, dev, pkg, W, flushbuf, steps=None, warmup=None, plain=True):
-    P, N = (args.P if args.workload == "fit" and args.P else 2048), \
-        (args.N if args.workload == "fit" and args.N else 262144)
-    steps = args.steps if steps is None else steps
-    warmup = args.warmup if warmup is None else warmup
-    iters = 20
-    trees, x, y = W.fit_workload(P, N, seed=rank)
+def fit_setup(pkg, W, case, P, N, seed):
+    """The evaluator, fit plans and label of one fit configuration:
+      c3:  1-20 constants, 5-60 nodes over N rows x 8 features ~U(-2,2),
+           y = 1.7 exp(-x0^2/2) cos(2.3 x1) + 0.4 x2 + noise; squared error;
+      c5:  1-20 constants over N rows x 10 heavy-tailed features,
+           y = 0.8 x0/(1+x1^2) + log(1+|x3|) + 0.1 t3 noise; absolute error
+           (L1 IRLS with true-MAE acceptance)."""
+    if case == "c3":
+        trees, x, y = W.fit_workload(P, N, seed=seed)
+        metric, what = 0, f"batched LM fit (squared), P={P}, N={N} rows x 8 features, 20 iters"
+    else:
+        x, y = W.heavy_tail_data(N, seed=seed)
+        trees, _, _ = W.fit_workload(P, 16, seed=7 + seed, nvars=10)
+        metric = 4
+        what = (f"batched L1 IRLS fit (absolute), P={P}, N={N} rows x 10 heavy-tailed "
+                f"features, 20 iters")
     ev = pkg.GpuEvaluator(x.astype(np.float32).reshape(-1), N, x.shape[0], y.astype(np.float32))
     ev.set_fit_data(x.reshape(-1), y)
     plans = [pkg.gpu_fit_plan(t) for t in trees]
+    return ev, plans, trees, x, y, metric, what
+
+
+def time_fit(pkg, ev, plans, metric, N, steps, warmup, flushbuf, plain_n, seed):
+    """Fused fits of the whole batch (graph-replayed), timed per step on the
+    device and end to end; then the plain one-candidate-per-launch form on a
+    seeded random sample of the same candidates (its cost is linear in the
+    candidate count), whose losses must equal the fused ones bit for bit."""
+    import torch
+    iters = 20
+    P = len(plans)
     prog, off, pcount, c0, gauge, kmax = pkg.pack_plans(plans)
     for _ in range(warmup):
-        ev.fit_batch_fused(prog, off, pcount, c0, gauge, kmax, iters)
+        ev.fit_batch_fused(prog, off, pcount, c0, gauge, kmax, iters, metric)
     dev_ms, wall = [], []
-    import torch
     n0 = ev.launch_count()
     with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clk:
         for _ in range(steps):
             flush_l2(flushbuf)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            _, loss, st, ms = ev.fit_batch_fused(prog, off, pcount, c0, gauge, kmax, iters)
+            _, loss, st, ms = ev.fit_batch_fused(prog, off, pcount, c0, gauge, kmax, iters,
+                                                 metric)
             wall.append(time.perf_counter() - t0)
             dev_ms.append(ms)
     launches = ev.launch_count() - n0
-    clocks = clk.summary()
-    out = dict(P=P, N=N, dev_ms=dev_ms, wall=wall, clocks=clocks, trees=trees, x=x, y=y,
-               launches=launches, unit_count=float(P),
-               lane_ops=fit_lane_ops(plans, N, iters),
-               status=np.bincount(st, minlength=9).tolist())
-    out["h2d"] = int(prog.nbytes + off.nbytes + pcount.nbytes + c0.nbytes + gauge.nbytes)
-    out["d2h"] = int(P * (kmax * 8 + 8 + 4))
-    if plain:
-        # the plain device form: the same step kernels, one candidate at a
-        # time, on a subset (its cost is linear in the candidate count)
-        S = min(32, P)
-        sp, so, spc, sc0, sg, _ = pkg.pack_plans(plans[:S], kmax)
-        ev.fit_batch_plain(sp, so, spc, sc0, sg, kmax, iters)
+    out = dict(P=P, N=N, dev_ms=dev_ms, wall=wall, clocks=clk.summary(), launches=launches,
+               unit_count=float(P), status=np.bincount(st, minlength=9).tolist(),
+               h2d=int(prog.nbytes + off.nbytes + pcount.nbytes + c0.nbytes + gauge.nbytes),
+               d2h=int(P * (kmax * 8 + 8 + 4)))
+    if metric in (0, 4):
+        out["lane_ops"] = fit_lane_ops(plans, N, iters)
+    if plain_n:
+        rng = np.random.Generator(np.random.PCG64(seed + 77))
+        idx = np.sort(rng.choice(P, size=min(plain_n, P), replace=False))
+        sp, so, spc, sc0, sg, _ = pkg.pack_plans([plans[i] for i in idx], kmax)
+        w = pkg.pack_plans([plans[i] for i in idx[:2]], kmax)
+        ev.fit_batch_plain(w[0], w[1], w[2], w[3], w[4], kmax, iters, metric)
+        torch.cuda.synchronize()
         t0 = time.perf_counter()
-        _, ploss, pst, pms = ev.fit_batch_plain(sp, so, spc, sc0, sg, kmax, iters)
+        _, ploss, pst, pms = ev.fit_batch_plain(sp, so, spc, sc0, sg, kmax, iters, metric)
         pwall = time.perf_counter() - t0
-        out["plain"] = {"value": S / (pms / 1e3), "unit": "candidates/s", "sample": S,
-                        "e2e": S / pwall,
+        out["plain"] = {"value": len(idx) / (pms / 1e3), "unit": "candidates/s",
+                        "sample": f"{len(idx)} candidates drawn at random (seeded) from the "
+                                  f"batch, one launch sequence each",
+                        "e2e": len(idx) / pwall,
                         "same_losses": bool(np.array_equal(ploss.view(np.uint64),
-                                                           loss[:S].view(np.uint64)))}
-    ev.close()
+                                                           loss[idx].view(np.uint64)))}
     return out
 
 
-def rank_data(n, seed=0):
-    """10 features (6 normal, 4 Student-t nu=3) and a heavy-tailed target
-    (y = 0.8 x0 / (1 + x1^2) + log(1 + |x3|) + 0.1 t3-noise)."""
-    rng = np.random.Generator(np.random.PCG64(seed + 5000))
-    x = np.concatenate([rng.standard_normal((6, n)), rng.standard_t(3.0, (4, n))])
-    y = 0.8 * x[0] / (1.0 + x[1] ** 2) + np.log1p(np.abs(x[3])) + 0.1 * rng.standard_t(3.0, n)
-    return x, y
+def fit_summary(r, peaks, what):
+    """The fit block of a JSON line."""
+    fv = r["unit_count"] * len(r["dev_ms"]) / (sum(r["dev_ms"]) / 1e3)
+    d = {"metric": "fitted_candidates_per_s", "value": fv, "unit": "candidates/s",
+         "e2e": r["unit_count"] * len(r["wall"]) / sum(r["wall"]),
+         "ms_per_step": float(np.mean(r["dev_ms"])), "steps": len(r["dev_ms"]),
+         "config": what, "gpu_launches": r["launches"], "status_histogram": r["status"],
+         "clocks": r["clocks"]}
+    if "plain" in r:
+        d["plain"] = r["plain"]
+        d["fused_over_plain"] = fv / r["plain"]["value"]
+    d["roofline"] = fit_roofline(r, peaks) if "lane_ops" in r else None
+    return d
 
 
-def bench_rank(args, rank, pkg, W, flushbuf, steps, warmup):
-    """Exact rank sums of 64 fit-style candidates over N = 1,048,576 rows."""
-    P = args.P if args.workload == "rank" and args.P else 64
-    N = args.N if args.workload == "rank" and args.N else 1 << 20
-    x, y = rank_data(N, seed=rank)
-    trees, _, _ = W.fit_workload(P, 16, seed=100 + rank, nvars=10)
-    ev = pkg.GpuEvaluator(x.astype(np.float32).reshape(-1), N, 10, y.astype(np.float32))
-    ev.set_fit_data(x.reshape(-1), y)
-    plans = [pkg.gpu_fit_plan(t) for t in trees]
-    prog, off, pcount, c0, gauge, kmax = pkg.pack_plans(plans)
-    ev.rank_target()
-    for _ in range(warmup):
-        ev.rank_sums(prog, off, pcount, c0, kmax)
+def bench_fit(args, rank, world, dev, pkg, W, flushbuf, steps=None, warmup=None, plain=True,
+              N=None):
+    P = args.P if args.workload == "fit" and args.P else 2048
+    N = N or (args.N if args.workload == "fit" and args.N else 262144)
+    steps = args.steps if steps is None else steps
+    warmup = args.warmup if warmup is None else warmup
+    ev, plans, trees, x, y, metric, what = fit_setup(pkg, W, "c3", P, N, rank)
+    out = time_fit(pkg, ev, plans, metric, N, steps, warmup, flushbuf, 64 if plain else 0, rank)
+    ev.close()
+    out.update(trees=trees, x=x, y=y, what=what)
+    return out
+
+
+def bench_implicit(args, rank, pkg, W, flushbuf, steps, warmup, fit_steps, fit_warmup):
+    """The implicit metric (P = 1024 candidates of f(x, y, d1, d2) on a noisy
+    unit circle with two distractors, length 3-40, 0-6 constants;
+    N = 1,048,576 rows): scoring |f|/||grad f|| through the fused input
+    adjoint (candidate*rows/s), and the LM fit of the candidates that hold
+    constants."""
     import torch
+    P = args.P if args.workload == "implicit" and args.P else 1024
+    N = args.N if args.workload == "implicit" and args.N else 1 << 20
+    trees, cols = W.implicit_workload(P, N, seed=rank)
+    ev = pkg.GpuEvaluator(cols.astype(np.float32).reshape(-1), N, 4, np.zeros(N, np.float32))
+    ev.set_fit_data(cols.reshape(-1), np.zeros(N))
+    splans = [pkg.gpu_fit_plan(t, allow_no_constants=True) for t in trees]
+    prog, off, pcount, c0, gauge, kmax = pkg.pack_plans(splans)
+    for _ in range(warmup):
+        ev.implicit_score(prog, off, pcount, c0, kmax)
     dev_ms, wall = [], []
     n0 = ev.launch_count()
     for _ in range(steps):
         flush_l2(flushbuf)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        sums, status, bb, ms = ev.rank_sums(prog, off, pcount, c0, kmax)
+        vals, status, ms = ev.implicit_score(prog, off, pcount, c0, kmax)
+        wall.append(time.perf_counter() - t0)
+        dev_ms.append(ms)
+    rows = float(P) * N
+    score = {"metric": "implicit_score_candidate_rows_per_s",
+             "value": rows * steps / (sum(dev_ms) / 1e3), "unit": "candidate*row/s",
+             "e2e": rows * steps / sum(wall), "ms_per_step": float(np.mean(dev_ms)),
+             "gpu_launches": ev.launch_count() - n0,
+             "finite_candidates": int((status == 0).sum()),
+             "config": f"implicit |f|/||grad f|| scoring, P={P}, N={N} rows x 4 inputs"}
+    fplans = [pkg.gpu_fit_plan(t) for t in trees if t.constants()]
+    fit = time_fit(pkg, ev, fplans, 6, N, fit_steps, fit_warmup, flushbuf, 16, rank)
+    ev.close()
+    what = (f"implicit |f|/||grad f|| LM fit (exact Jacobian from the input adjoint), the "
+            f"{fit['P']} of P={P} candidates with constants, N={N} rows, 20 iters")
+    return score, fit, what
+
+
+def rank_stage(pkg, ev, plans, N, flushbuf, steps, warmup):
+    """Exact rank sums of every plan's predictions against the resident
+    target: candidate*rows/s and the HBM roofline of 32 algorithmic bytes per
+    candidate*row."""
+    import torch
+    P = len(plans)
+    # one call holds at most 2^31 - 1 candidate*rows (the ABI's limit, as in
+    # the reference); larger batches go in chunks, as its binding does
+    per_call = max(1, 0x7FFFFFFF // N)
+    chunks = [pkg.pack_plans(plans[s:s + per_call]) for s in range(0, P, per_call)]
+
+    def run():
+        ms, st = 0.0, []
+        for cp, co, cc, c0_, _, km in chunks:
+            _, s, _, m = ev.rank_sums(cp, co, cc, c0_, km)
+            ms += m
+            st.append(s)
+        return np.concatenate(st), ms
+
+    ev.rank_target()
+    for _ in range(warmup):
+        run()
+    dev_ms, wall = [], []
+    n0 = ev.launch_count()
+    for _ in range(steps):
+        flush_l2(flushbuf)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        status, ms = run()
         wall.append(time.perf_counter() - t0)
         dev_ms.append(ms)
     launches = ev.launch_count() - n0
-    ev.close()
     rows = float(P) * N
     per = float(np.mean(dev_ms)) / 1e3
     achieved = 32.0 * rows / per / 1e9
     peak = load_peaks().get("hbm_gbs", 6650.0)
     return {"metric": "rank_candidate_rows_per_s", "value": rows / per, "unit": "candidate*row/s",
             "e2e": rows * steps / sum(wall), "ms_per_step": 1e3 * per, "launches": launches,
+            "h2d": int(sum(c[0].nbytes + c[1].nbytes + c[2].nbytes + c[3].nbytes
+                           for c in chunks)),
+            "d2h": int(P * (4 * 8 + 4) + 16 * len(chunks)), "calls_per_step": len(chunks),
             "finite_segments": int((status == 0).sum()),
-            "config": f"exact rank sums, P={P} candidates x 1 trial, N={N} rows x 10 features",
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None,
                          "note": "algorithmic 32 B per candidate*row (f64 eval, 8 B key, 4 B "
                                  "row, read back, 8 B gathered target rank) / event time; "
                                  "peak = measured copy bandwidth (MEASURED_PEAKS.json)"}}
+
+
+def bench_rank(args, rank, pkg, W, flushbuf, steps, warmup):
+    """Exact rank sums of P fit-style candidates (default 64) over N rows
+    (default 1,048,576) x 10 heavy-tailed features."""
+    P = args.P if args.workload == "rank" and args.P else 64
+    N = args.N if args.workload == "rank" and args.N else 1 << 20
+    x, y = W.heavy_tail_data(N, seed=rank)
+    trees, _, _ = W.fit_workload(P, 16, seed=100 + rank, nvars=10)
+    ev = pkg.GpuEvaluator(x.astype(np.float32).reshape(-1), N, 10, y.astype(np.float32))
+    ev.set_fit_data(x.reshape(-1), y)
+    r = rank_stage(pkg, ev, [pkg.gpu_fit_plan(t) for t in trees], N, flushbuf, steps, warmup)
+    ev.close()
+    r["config"] = f"exact rank sums, P={P} candidates x 1 trial, N={N} rows x 10 features"
+    return r
+
+
+def bench_c5(args, rank, pkg, W, flushbuf, steps, warmup, fit_steps, fit_warmup):
+    """The heavy-tailed configuration (N = 4,194,304 rows x 10 features, one
+    island's generation of P = 1000 candidates): the L1 IRLS fit and the exact
+    rank-correlation sums of the same candidates."""
+    P = args.P if args.workload == "c5" and args.P else 1000
+    N = args.N if args.workload == "c5" and args.N else 1 << 22
+    ev, plans, trees, x, y, metric, what = fit_setup(pkg, W, "c5", P, N, rank)
+    fit = time_fit(pkg, ev, plans, metric, N, fit_steps, fit_warmup, flushbuf, 16, rank)
+    rk = rank_stage(pkg, ev, plans, N, flushbuf, steps, warmup)
+    rk["config"] = (f"exact rank-correlation sums, P={P} candidates x 1 trial, N={N} rows x "
+                    f"10 heavy-tailed features")
+    ev.close()
+    return fit, what, rk
 
 
 def fit_roofline(r, peaks):
@@ -371,18 +495,36 @@ def fit_roofline(r, peaks):
                     "128 FP32 lanes x sm_max_mhz from MEASURED_PEAKS.json"}
 
 
+def single_gpu_line(args, world, r, metric, unit, what, extra):
+    """The JSON line of a one-GPU workload whose numbers come from a fit or
+    rank block."""
+    line = {"metric": metric, "value": r["value"], "unit": unit, "n_gpus": world,
+            "steps": r.get("steps", args.steps), "warmup": args.warmup,
+            "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 rows, f64 sums", "data": "synthetic",
+            "config": {"workload": what, "l2": "flushed between steps"},
+            "roofline": r.get("roofline"), "clocks": r.get("clocks"),
+            "e2e": {"value": r["e2e"], "unit": unit, "h2d_bytes_per_step": r.get("h2d"),
+                    "d2h_bytes_per_step": r.get("d2h")},
+            "gpu_launches": r.get("gpu_launches", r.get("launches"))}
+    line.update(extra)
+    return line
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="score", choices=["score", "fit", "rank"])
+    ap.add_argument("--workload", default="score",
+                    choices=["score", "fit", "rank", "implicit", "c5"])
     ap.add_argument("--P", type=int, default=0)
     ap.add_argument("--N", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true",
-                    help="skip the fit and rank measurements of the default line")
+                    help="skip the fit, implicit and heavy-tailed measurements of the "
+                         "default line")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", 0))
@@ -400,23 +542,41 @@ def main():
     pkg = importlib.import_module(PKG)
     W = importlib.import_module(PKG + ".workloads")
     flushbuf = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    peaks = load_peaks()
 
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    if args.workload == "rank":
-        # the exact-statistics stage alone (one GPU): the line bench_rank makes
-        r = bench_rank(args, rank, pkg, W, flushbuf, args.steps, args.warmup)
+    if args.workload in ("rank", "implicit", "c5"):
+        # one-GPU stages: each rank measures its own copy; rank 0 reports
+        if args.workload == "rank":
+            r = bench_rank(args, rank, pkg, W, flushbuf, args.steps, args.warmup)
+            line = single_gpu_line(args, world, r, r["metric"], r["unit"], r.pop("config"),
+                                   {"dtype": "f64 eval, integer sums"})
+        elif args.workload == "implicit":
+            score, fit, what = bench_implicit(args, rank, pkg, W, flushbuf, args.steps,
+                                              args.warmup, args.steps, args.warmup)
+            fs = fit_summary(fit, peaks, what)
+            line = single_gpu_line(args, world, fs, fs["metric"], fs["unit"], what,
+                                   {"dtype": "f64", "implicit_score": score,
+                                    "plain": fs.get("plain"),
+                                    "fused_over_plain": fs.get("fused_over_plain"),
+                                    "fit_status_histogram": fs["status_histogram"]})
+            line["h2d"] = fit["h2d"]
+        else:
+            fit, what, rk = bench_c5(args, rank, pkg, W, flushbuf, args.steps, args.warmup,
+                                     args.steps, args.warmup)
+            fs = fit_summary(fit, peaks, what)
+            fs["h2d"], fs["d2h"] = fit["h2d"], fit["d2h"]
+            line = single_gpu_line(args, world, fs, fs["metric"], fs["unit"], what,
+                                   {"plain": fs.get("plain"),
+                                    "fused_over_plain": fs.get("fused_over_plain"),
+                                    "fit_status_histogram": fs["status_histogram"],
+                                    "rank": rk})
         if rank == 0:
-            r.update({"n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-                      "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                      "dtype": "f64 eval, integer sums", "data": "synthetic",
-                      "gpu_launches": r.pop("launches"),
-                      "e2e": {"value": r["e2e"], "unit": r["unit"], "h2d_bytes_per_step": None,
-                              "d2h_bytes_per_step": None},
-                      "config": {"workload": r["config"], "l2": "flushed between steps"}})
-            print(json.dumps(r), flush=True)
+            print(json.dumps(line), flush=True)
         if world > 1:
+            dist.barrier()
             dist.destroy_process_group()
         return
     if args.workload == "score":
@@ -435,7 +595,6 @@ def main():
     units = r["unit_count"] * args.steps * world
     value = units / dev_s
     e2e = units / wall_s
-    peaks = load_peaks()
     if rank == 0:
         if args.workload == "score":
             metric, unit = "expr_row_evals_per_s", "expr*row/s"
@@ -459,8 +618,7 @@ def main():
         else:
             metric, unit = "fitted_candidates_per_s", "candidates/s"
             roof = fit_roofline(r, peaks)
-            cfg = {"workload": f"batched LM fit, P={r['P']}, N={r['N']} rows x 8 features, "
-                               f"20 iters, fused adjoint", "l2": "flushed between steps"}
+            cfg = {"workload": r["what"] + ", fused adjoint", "l2": "flushed between steps"}
         line = {"metric": metric, "value": value, "unit": unit, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": 1e3 * dev_s / args.steps, "higher_is_better": True,
@@ -489,16 +647,15 @@ def main():
                                                   "scaled linearly in rows"}
         if args.workload == "score" and world == 1 and not args.no_secondary:
             f = bench_fit(args, rank, world, local, pkg, W, flushbuf, steps=3, warmup=3)
-            fv = f["unit_count"] * len(f["dev_ms"]) / (sum(f["dev_ms"]) / 1e3)
-            line["fit"] = {
-                "metric": "fitted_candidates_per_s", "value": fv, "unit": "candidates/s",
-                "e2e": f["unit_count"] * len(f["wall"]) / sum(f["wall"]),
-                "ms_per_step": float(np.mean(f["dev_ms"])),
-                "config": f"batched LM fit, P={f['P']}, N={f['N']} rows x 8 features, 20 iters",
-                "plain": f["plain"], "fused_over_plain": fv / f["plain"]["value"],
-                "roofline": fit_roofline(f, peaks), "gpu_launches": f["launches"],
-                "status_histogram": f["status"], "clocks": f["clocks"]}
-            line["rank"] = bench_rank(args, rank, pkg, W, flushbuf, steps=3, warmup=3)
+            line["fit"] = fit_summary(f, peaks, f["what"])
+            f = bench_fit(args, rank, world, local, pkg, W, flushbuf, steps=2, warmup=3,
+                          N=1 << 20)
+            line["fit_1m"] = fit_summary(f, peaks, f["what"])
+            del f
+            score, fit, what = bench_implicit(args, rank, pkg, W, flushbuf, 3, 3, 1, 1)
+            line["implicit"] = {"score": score, "fit": fit_summary(fit, peaks, what)}
+            fit, what, rk = bench_c5(args, rank, pkg, W, flushbuf, 3, 3, 1, 1)
+            line["c5"] = {"absolute_fit": fit_summary(fit, peaks, what), "rank": rk}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

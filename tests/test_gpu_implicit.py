@@ -103,3 +103,32 @@ def test_implicit_fit_on_noisy_circle_tracks_the_cpu_fit(pkg, E, O):
     for a, b in zip(plan.apply(t, c[0]).constants(), cpu_tree.constants()):
         assert abs(a - b) <= 1e-5 * (1 + abs(b))
     ev.close()
+
+
+def test_implicit_fit_batch_tracks_the_cpu_fit(pkg, O):
+    """A seeded batch of the implicit workload (f(x, y, d1, d2) with 1-6
+    constants). The device's Jacobian is exact (forward-over-reverse through
+    the input adjoint) where the CPU takes central differences, so the two LM
+    trajectories agree to rounding on most candidates and part ways only on
+    a few non-convex ones."""
+    W = importlib.import_module("the-rule-and-compass_b200.workloads")
+    trees, cols = W.implicit_workload(96, 4096, seed=11)
+    ev = evaluator(pkg, cols)
+    fit_trees = [t for t in trees if t.constants()]
+    plans = [pkg.gpu_fit_plan(t) for t in fit_trees]
+    c, loss, status, _ = ev.fit_plans(plans, 20, metric=6)
+    assert set(np.unique(status)) <= {0, 6, 7}, status
+    rel = []
+    for k, t in enumerate(fit_trees):
+        cpu, _ = O.implicit_fit(t, cols.reshape(-1), 4096, 4, 20)
+        assert math.isinf(cpu) == math.isinf(loss[k]), (k, loss[k], cpu)
+        if math.isinf(cpu):
+            continue
+        rel.append((loss[k] - cpu) / max(abs(cpu), 1e-300))
+    rel = np.asarray(rel)
+    assert len(rel) >= 60
+    assert np.median(np.abs(rel)) <= 1e-9, np.median(np.abs(rel))
+    assert np.mean(np.abs(rel) <= 1e-6) >= 0.6, rel
+    assert np.mean(rel <= 1e-6) >= 0.85, rel        # no worse than the CPU fit
+    assert rel.max() <= 0.1, rel.max()
+    ev.close()

@@ -60,7 +60,8 @@ enum {
 enum {
     PC_INIT = 0, PC_AFTER_FIRST_ASM, PC_ROUND, PC_ITER, PC_AFTER_ASM, PC_SOLVE,
     PC_AFTER_TRIAL, PC_REBASE, PC_AFTER_REBASE, PC_POLISH, PC_AFTER_PASM, PC_AFTER_PTRIAL,
-    PC_END, PC_I_INIT, PC_I_AFTER_BASE, PC_I_ITER, PC_I_AFTER_JAC, PC_I_AFTER_TRIAL, PC_I_END,
+    PC_END, PC_I_INIT, PC_I_AFTER_BASE, PC_I_ITER, PC_I_AFTER_JAC, PC_I_SOLVE, PC_I_AFTER_TRIAL,
+    PC_I_END,
     PC_C_INIT, PC_C_SCORE_ONLY, PC_C_AFTER_FIRST, PC_C_ITER, PC_C_AFTER_ASM, PC_C_SOLVE,
     PC_C_AFTER_TRIAL, PC_C_POLISH, PC_C_AFTER_PASM, PC_C_AFTER_PTRIAL, PC_C_END, PC_DONE
 };
@@ -153,7 +154,8 @@ __host__ __device__ inline size_t ft_rows_bytes(int Wmax, int T)
    the assembling kinds, and a reduction buffer. */
 __host__ __device__ inline size_t ft_sweep_smem(int opk, int mmax, int Wmax, int T)
 {
-    size_t s = 16 * (size_t)mmax + 16 * FT_MAX_CONST + 4 * (size_t)mmax * T;
+    size_t s = 16 * (size_t)mmax + 16 * FT_MAX_CONST +
+               4 * (size_t)mmax * T * (opk == FOP_IJAC ? 2 : 1);
     if (ft_op_assembles(opk)) s += ft_rows_bytes(Wmax, T);
     return s + 8 * (size_t)T;
 }
@@ -180,12 +182,14 @@ __device__ __forceinline__ void ft_tile_gram_out(const Syrk &sy, const double ac
 }
 
 /* Implicit metric of one tile (implicit.rs:156-174, :302-333): the cost
-   sum w d^2 at `cd`, and with `jac` the central-difference Jacobian rows of
-   sqrt(w) d and their J^T J / J^T r. An undefined row marks the tile bad. */
+   sum w d^2 at `cd`, and with JAC the Jacobian rows of sqrt(w) d (exact,
+   forward-over-reverse, where the reference takes central differences
+   with h = 1e-6 (1 + |c_j|)) and their J^T J / J^T r. An undefined row
+   marks the tile bad. `tan64` is the second f64 tape of the Jacobian. */
 template <int T, bool JAC>
 __device__ void ft_tile_implicit(const FitArgs &a, const uint4 *rec, int m, int p,
-                                 const double *cd, double *tape64, double *rows, double *red,
-                                 int r0, int r1, double *pt)
+                                 const double *cd, double *tape64, double *tan64, double *rows,
+                                 double *red, int r0, int r1, double *pt)
 {
     constexpr int TS = T / 2;
     const int tid = threadIdx.x;
@@ -199,7 +203,6 @@ __device__ void ft_tile_implicit(const FitArgs &a, const uint4 *rec, int m, int 
     double *tp = tape64 + tid;
     double *myrow = rows + (size_t)tid * W;
     double x[FT_IMPLICIT_MAXV];
-    double cp[FT_MAX_CONST];
     for (int base = r0; base < r1; base += TS) {
         const int row = base + tid;
         if (tid < TS) {
@@ -211,30 +214,18 @@ __device__ void ft_tile_implicit(const FitArgs &a, const uint4 *rec, int m, int 
                 for (int k = 0; k < FT_IMPLICIT_MAXV; ++k)
                     x[k] = k < a.v ? a.cols64[(size_t)k * a.npad + row] : 0.0;
                 double d;
-                if (!ft_implicit_d<TS>(rec, m, x, a.v, cd, tp, d)) bad = 1;
-                else {
-                    const double sw = sqrt(wr);
+                const double sw = sqrt(wr);
+                const bool ok = JAC ? ft_implicit_jac<TS>(rec, m, x, a.v, cd, p, sw, tp,
+                                                          tan64 + tid, d, myrow)
+                                    : ft_implicit_d<TS>(rec, m, x, a.v, cd, tp, d);
+                if (!ok) {
+                    bad = 1;
+                    if (JAC)
+                        for (int j = 0; j < p; ++j) myrow[j] = 0.0;
+                } else {
                     const double r = sw * d;
                     cost += r * r;
-                    if (JAC) {
-                        for (int j = 0; j < p; ++j) cp[j] = cd[j];
-                        for (int j = 0; j < p && !bad; ++j) {
-                            const double h = 1e-6 * (1.0 + fabs(cd[j]));
-                            double dp, dm;
-                            cp[j] = cd[j] + h;
-                            const bool okp = ft_implicit_d<TS>(rec, m, x, a.v, cp, tp, dp);
-                            cp[j] = cd[j] - h;
-                            const bool okm = ft_implicit_d<TS>(rec, m, x, a.v, cp, tp, dm);
-                            cp[j] = cd[j];
-                            if (!okp || !okm) {
-                                bad = 1;
-                                break;
-                            }
-                            myrow[j] = (sw * dp - sw * dm) / (2.0 * h);
-                            if (!isfinite(myrow[j])) bad = 1;
-                        }
-                        myrow[p] = r;
-                    }
+                    if (JAC) myrow[p] = r;
                 }
             }
         }
@@ -264,7 +255,8 @@ __global__ void __launch_bounds__(T) ft_sweep(FitArgs a, int q)
     float *cf = reinterpret_cast<float *>(cd + FT_MAX_CONST);
     float *tape = cf + 2 * FT_MAX_CONST;
     double *tape64 = reinterpret_cast<double *>(tape);
-    double *rows = reinterpret_cast<double *>(tape + (size_t)a.mmax * T);
+    double *tan64 = reinterpret_cast<double *>(tape + (size_t)a.mmax * T);
+    double *rows = reinterpret_cast<double *>(tape + (size_t)a.mmax * T * (OPK == FOP_IJAC ? 2 : 1));
     double *red = rows + (ft_op_assembles(OPK) ? ft_rows_bytes(a.Wmax, T) / 8 : 0);
     __shared__ int s_item;
     const int tid = threadIdx.x;
@@ -294,8 +286,10 @@ __global__ void __launch_bounds__(T) ft_sweep(FitArgs a, int q)
         const int r0 = tile * FT_TILE_ROWS;
         const int r1 = min(a.n, r0 + FT_TILE_ROWS);
         double *pt = a.part + ((size_t)cand * a.ntiles + tile) * FT_PART_STRIDE;
-        if (OPK == FOP_IJAC) ft_tile_implicit<T, true>(a, rec, m, p, cd, tape64, rows, red, r0, r1, pt);
-        else ft_tile_implicit<T, false>(a, rec, m, p, cd, tape64, rows, red, r0, r1, pt);
+        if (OPK == FOP_IJAC)
+            ft_tile_implicit<T, true>(a, rec, m, p, cd, tape64, tan64, rows, red, r0, r1, pt);
+        else
+            ft_tile_implicit<T, false>(a, rec, m, p, cd, tape64, tan64, rows, red, r0, r1, pt);
         __syncthreads();
     }
 }
@@ -1289,15 +1283,26 @@ __device__ void ft_advance(const FitArgs &a, FitState &st, int cand, int p, doub
                     st.pc = PC_I_END;
                     break;
                 }
-                st.op = FOP_IJAC;
-                st.sel = 0;
-                st.pc = PC_I_AFTER_JAC;
-                return;
-            case PC_I_AFTER_JAC: {
+                /* the reference recomputes the residuals and Jacobian at an
+                   unchanged point after a rejected or singular step; the
+                   system kept from the last assembly is the same one */
+                if (!st.assembled) {
+                    st.op = FOP_IJAC;
+                    st.sel = 0;
+                    st.pc = PC_I_AFTER_JAC;
+                    return;
+                }
+                st.pc = PC_I_SOLVE;
+                break;
+            case PC_I_AFTER_JAC:
                 if (rb) {
                     st.pc = PC_I_END;
                     break;
                 }
+                st.assembled = 1;
+                st.pc = PC_I_SOLVE;
+                break;
+            case PC_I_SOLVE: {
                 const int sv = ft_gauss_solve(st.jtj, st.jtr, st.lambda, p, delta, L);
                 if (sv != 0) {
                     st.lambda *= 6.0;
@@ -1318,6 +1323,7 @@ __device__ void ft_advance(const FitArgs &a, FitState &st, int cand, int p, doub
                     for (int j = 0; j < p; ++j) st.c[j] = st.trial[j];
                     st.lambda = fmax(st.lambda / 8.0, 1e-12);
                     st.improved = 1;
+                    st.assembled = 0;
                     st.pc = st.best == 0.0 ? PC_I_END : PC_I_ITER;
                 } else {
                     st.lambda *= 6.0;

@@ -406,6 +406,91 @@ __device__ inline int ft_gauss_solve(const double *jtj, const double *jtr, doubl
     return 0;
 }
 
+/* First and second local partials of one node (f64): d0, d1 as
+   ft_partials_d, and d00 = d2 node / da2, d01 = d2 node / da db,
+   d11 = d2 node / db2. A `pow` with a non-positive base passes nothing. */
+__device__ __forceinline__ void ft_partials2_d(unsigned op, double x, double y, double &d0,
+                                               double &d1, double &d00, double &d01,
+                                               double &d11)
+{
+    d0 = d1 = d00 = d01 = d11 = 0.0;
+    switch (op) {
+        case OP_NEG: d0 = -1.0; break;
+        case OP_EXP: d0 = exp(x); d00 = d0; break;
+        case OP_LOG: d0 = 1.0 / x; d00 = -d0 * d0; break;
+        case OP_ABS: d0 = x >= 0.0 ? 1.0 : -1.0; break;
+        case OP_SQRT: {
+            const double s = sqrt(x);
+            d0 = 1.0 / (2.0 * s);
+            d00 = -d0 / (2.0 * x);
+        } break;
+        case OP_SIN: {
+            double s, c;
+            sincos(x, &s, &c);
+            d0 = c;
+            d00 = -s;
+        } break;
+        case OP_COS: {
+            double s, c;
+            sincos(x, &s, &c);
+            d0 = -s;
+            d00 = -c;
+        } break;
+        case OP_TAN: {
+            double s, c;
+            sincos(x, &s, &c);
+            d0 = 1.0 / (c * c);
+            d00 = 2.0 * s / (c * c * c);
+        } break;
+        case OP_SINH: d0 = cosh(x); d00 = sinh(x); break;
+        case OP_COSH: d0 = sinh(x); d00 = cosh(x); break;
+        case OP_TANH: {
+            const double t = tanh(x);
+            d0 = 1.0 - t * t;
+            d00 = -2.0 * t * d0;
+        } break;
+        case OP_SIG: {
+            const double s = 1.0 / (1.0 + exp(-x));
+            d0 = s * (1.0 - s);
+            d00 = d0 * (1.0 - 2.0 * s);
+        } break;
+        case OP_GAUSS: {
+            const double e = exp(-x * x);
+            d0 = (-2.0 * x) * e;
+            d00 = (4.0 * x * x - 2.0) * e;
+        } break;
+        case OP_SQUARE: d0 = 2.0 * x; d00 = 2.0; break;
+        case OP_CUBE: d0 = 3.0 * x * x; d00 = 6.0 * x; break;
+        case OP_ERF: d0 = 1.1283791670955126 * exp(-x * x); d00 = -2.0 * x * d0; break;
+        case OP_ERFC: d0 = -1.1283791670955126 * exp(-x * x); d00 = -2.0 * x * d0; break;
+        case OP_ADD: d0 = 1.0; d1 = 1.0; break;
+        case OP_SUB: d0 = 1.0; d1 = -1.0; break;
+        case OP_MUL: d0 = y; d1 = x; d01 = 1.0; break;
+        case OP_DIV: {
+            const double iy = 1.0 / y;
+            d0 = iy;
+            d1 = -x / (y * y);
+            d01 = -iy * iy;
+            d11 = 2.0 * x * iy * iy * iy;
+        } break;
+        case OP_POW:
+            if (x > 0.0) {
+                const double lx = log(x), pm1 = pow(x, y - 1.0), pw = pow(x, y);
+                d0 = y * pm1;
+                d1 = pw * lx;
+                d00 = y * (y - 1.0) * pow(x, y - 2.0);
+                d01 = pm1 * (1.0 + y * lx);
+                d11 = pw * lx * lx;
+            }
+            break;
+        default: break;
+    }
+}
+
+/* a * d with a zero factor passing nothing (an adjoint or tangent of zero
+   does not meet an infinite partial). */
+__device__ __forceinline__ double ft_mul0(double a, double d) { return a == 0.0 ? 0.0 : a * d; }
+
 /* ---- the implicit metric (implicit.rs:68-409) ---------------------------
  * Per row: d = f / ||grad_x f|| (f64 forward + input adjoint); a row with a
  * non-finite value or gradient, or a zero gradient norm, makes the whole
@@ -457,6 +542,133 @@ __device__ __forceinline__ bool ft_implicit_d(const uint4 *rec, int m, const dou
     if (!(isfinite(norm) && norm > 0.0)) return false;
     d = fv / norm;
     return isfinite(d);
+}
+
+/* The implicit residual of one row and its exact Jacobian row (f64):
+   d = f / ||g||, g = grad_x f, and for each constant
+     dd/dc_j = (df/dc_j) / ||g|| - f (g . dg/dc_j) / ||g||^3,
+   where g . dg/dc_j = d/dc_j (grad_x f . v) at v = g held fixed, a
+   Hessian-vector product of f. Four sweeps over the records:
+   1. forward values (tape `vt`);
+   2. reverse in place: the input adjoint g and df/dc (into jrow);
+   3. forward again, values and tangents along x' = g (tapes `vt`, `tt`);
+   4. reverse of the tangent: each node's slots switch from (value,
+      tangent) to (adjoint u, second-order adjoint w) when its parent is
+      processed; a constant's w is g . dg/dc_j.
+   jrow[j] receives sqrt(w_row) dd/dc_j for j < p. Returns false when the
+   row is undefined (non-finite value, gradient or Jacobian entry, or a
+   zero gradient): the same rows ft_implicit_d rejects, plus a non-finite
+   Jacobian entry. */
+template <int TS>
+__device__ bool ft_implicit_jac(const uint4 *rec, int m, const double *x, int v, const double *c,
+                                int p, double sw, double *vt, double *tt, double &d, double *jrow)
+{
+    const double fv = ft_fwd_d_x<TS>(rec, m, x, c, vt);
+    if (!isfinite(fv)) return false;
+    for (int j = 0; j < p; ++j) jrow[j] = 0.0;
+    double ig[FT_IMPLICIT_MAXV];
+#pragma unroll
+    for (int k = 0; k < FT_IMPLICIT_MAXV; ++k) ig[k] = 0.0;
+    vt[(m - 1) * TS] = 1.0;
+    for (int i = m - 1; i >= 0; --i) {
+        const uint4 r = rec[i];
+        const double a = vt[i * TS];
+        if (r.x == OP_CONST) {
+            jrow[r.w] += a;
+            continue;
+        }
+        if (r.x == OP_VAR) {
+#pragma unroll
+            for (int k = 0; k < FT_IMPLICIT_MAXV; ++k)
+                if ((int)r.w == k) ig[k] += a;
+            continue;
+        }
+        const bool bin = ft_op_binary(r.x);
+        const double xx = vt[r.y * TS];
+        const double yy = bin ? vt[r.z * TS] : 0.0;
+        double c0 = 0.0, c1 = 0.0;
+        if (a != 0.0 && !(r.x == OP_POW && !(xx > 0.0))) {
+            double d0, d1;
+            ft_partials_d(r.x, xx, yy, d0, d1);
+            c0 = a * d0;
+            c1 = a * d1;
+        }
+        vt[r.y * TS] = c0;
+        if (bin) vt[r.z * TS] = c1;
+    }
+    double nsq = 0.0;
+    for (int k = 0; k < FT_IMPLICIT_MAXV; ++k) {
+        if (k >= v) break;
+        if (!isfinite(ig[k])) return false;
+        nsq += ig[k] * ig[k];
+    }
+    const double norm = sqrt(nsq);
+    if (!(isfinite(norm) && norm > 0.0)) return false;
+    d = fv / norm;
+    if (!isfinite(d)) return false;
+    /* 3: values and tangents along x' = g */
+    for (int i = 0; i < m; ++i) {
+        const uint4 r = rec[i];
+        double val, tan = 0.0;
+        if (r.x == OP_CONST) val = c[r.w];
+        else if (r.x == OP_VAR) {
+            val = x[r.w];
+#pragma unroll
+            for (int k = 0; k < FT_IMPLICIT_MAXV; ++k)
+                if ((int)r.w == k) tan = ig[k];
+        } else {
+            const bool bin = ft_op_binary(r.x);
+            const double a = vt[r.y * TS], ta = tt[r.y * TS];
+            const double b = bin ? vt[r.z * TS] : 0.0, tb = bin ? tt[r.z * TS] : 0.0;
+            val = ft_value_d(r.x, a, b);
+            if (!(r.x == OP_POW && !(a > 0.0)) && (ta != 0.0 || tb != 0.0)) {
+                double d0, d1;
+                ft_partials_d(r.x, a, b, d0, d1);
+                tan = ft_mul0(ta, d0) + ft_mul0(tb, d1);
+            }
+        }
+        vt[i * TS] = val;
+        tt[i * TS] = tan;
+    }
+    /* 4: reverse of the tangent; u = first-order adjoint, w = second */
+    const double s1 = sw / norm, s3 = sw * fv / (norm * norm * norm);
+    for (int j = 0; j < p; ++j) jrow[j] *= s1;
+    vt[(m - 1) * TS] = 1.0;
+    tt[(m - 1) * TS] = 0.0;
+    for (int i = m - 1; i >= 0; --i) {
+        const uint4 r = rec[i];
+        const double u = vt[i * TS], w = tt[i * TS];
+        if (r.x == OP_CONST) {
+            jrow[r.w] -= ft_mul0(w, s3);
+            continue;
+        }
+        if (r.x == OP_VAR) continue;
+        const bool bin = ft_op_binary(r.x);
+        const double a = vt[r.y * TS], ta = tt[r.y * TS];
+        const double b = bin ? vt[r.z * TS] : 0.0, tb = bin ? tt[r.z * TS] : 0.0;
+        double u0 = 0.0, u1 = 0.0, w0 = 0.0, w1 = 0.0;
+        if ((u != 0.0 || w != 0.0) && !(r.x == OP_POW && !(a > 0.0))) {
+            double d0, d1, d00, d01, d11;
+            ft_partials2_d(r.x, a, b, d0, d1, d00, d01, d11);
+            if (u != 0.0) {
+                u0 = u * d0;
+                u1 = u * d1;
+            }
+            const double h0 = ft_mul0(ta, d00) + ft_mul0(tb, d01);
+            const double h1 = ft_mul0(ta, d01) + ft_mul0(tb, d11);
+            w0 = ft_mul0(w, d0) + ft_mul0(u, h0);
+            w1 = ft_mul0(w, d1) + ft_mul0(u, h1);
+        }
+        vt[r.y * TS] = u0;
+        tt[r.y * TS] = w0;
+        if (bin) {
+            vt[r.z * TS] = u1;
+            tt[r.z * TS] = w1;
+        }
+    }
+    for (int j = 0; j < p; ++j)
+        if (!isfinite(jrow[j])) return false;
+    return true;
 }
 
 
