@@ -6,9 +6,9 @@
  *
  * Rank sums. A (candidate, trial) segment's f64 predictions over all n rows
  * become order-preserving u64 keys (-0 folded onto +0, anything not finite
- * onto the largest key). A segmented LSD radix sort (8-bit digits, a pass
- * whose digit is constant over a segment skipped) orders them with the row
- * as payload. One pass over the sorted keys then gives every position q its
+ * onto the largest key). A segmented LSD radix sort (8-bit digits, one
+ * kernel per pass with decoupled look-back, a pass whose digit is constant
+ * over a segment skipped) orders them with the row as payload. One pass over the sorted keys then gives every position q its
  * run [i, j) of equal keys, twice its centred average rank A = i + j - n,
  * and the exact sums sum A * B[row] and sum A^2 in 128-bit integers, B being
  * the target's own A (computed once per context the same way). Integer sums
@@ -134,88 +134,133 @@ __global__ void rk_target_keys(const double *y, int n, u64 *keys, unsigned int *
     }
 }
 
-/* ---- segmented LSD radix sort ------------------------------------------ */
+/* ---- segmented LSD radix sort (one sweep per digit) ---------------------
+ * Keys are u64, 8-bit digits, up to eight passes. One read of the keys first
+ * counts every digit of every pass per segment (rs_count); rs_prep turns the
+ * counts into each digit's first output position, marks the passes whose
+ * digit is constant over a segment (they leave the order unchanged and are
+ * skipped) and which buffer ends up holding each segment. A pass is then one
+ * kernel (rs_pass): every tile ranks its keys by digit, publishes its digit
+ * counts, adds up its predecessors' counts by decoupled look-back over the
+ * published words, and writes its keys to their final places of the pass.
+ * Tiles take increasing tickets per pass (segments interleaved), so every
+ * tile a tile waits on has started before it; each wait is bounded, and a
+ * wait that gives up raises a flag that stops every other wait and every
+ * write, and fails the call. */
 
-/* Per tile, the counts of the 8-bit digit at `shift`: hist[seg][tile][256]. A
-   warp takes 32 consecutive keys per round and adds each distinct digit
-   once. */
-__global__ void __launch_bounds__(RS_T) rs_hist(const u64 *ka, const u64 *kb,
-                                                const unsigned char *par, int n, int ntiles,
-                                                int shift, unsigned int *hist)
+#define RS_PASSES 8
+#define RS_ST_AGG 1ULL    /* published word: the tile's own counts */
+#define RS_ST_PREFIX 2ULL /* published word: counts of this and every earlier tile */
+#define RS_SPIN_LIMIT (1u << 22)
+
+/* A published look-back word: kind in bits 62-63, pass tag (1-8) in bits
+   32-39, the count in bits 0-31. Words of another pass read as unpublished. */
+__device__ __forceinline__ u64 rs_word(u64 kind, int pass, unsigned int v)
 {
-    __shared__ unsigned int cnt[256];
-    const int seg = blockIdx.x / ntiles, tile = blockIdx.x % ntiles;
-    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    const u64 *src = (par[seg] ? kb : ka) + (size_t)seg * n;
-    cnt[tid] = 0;
-    __syncthreads();
-    const int base = tile * RS_TILE + w * (RS_TILE / RS_WARPS);
-    constexpr int R = RS_TILE / RS_WARPS / 32;
-    unsigned dg[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        /* all loads first, so each thread has R in flight */
-        const int idx = base + 32 * r + lane;
-        dg[r] = idx < n ? (unsigned)(src[idx] >> shift) & 255u : 256u;
-    }
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const unsigned peers = __match_any_sync(0xffffffffu, dg[r]);
-        if (dg[r] < 256u && lane == __ffs(peers) - 1) atomicAdd(&cnt[dg[r]], (unsigned)__popc(peers));
-    }
-    __syncthreads();
-    hist[((size_t)seg * ntiles + tile) * 256 + tid] = cnt[tid];
+    return (kind << 62) | ((u64)(pass + 1) << 32) | (u64)v;
 }
 
-/* Per segment, turn the tile counts into each (tile, digit)'s first output
-   position (digit-major, then tile order), in place. A digit that holds all
-   n keys leaves the order unchanged: the segment skips this pass. */
-__global__ void __launch_bounds__(256) rs_scan(unsigned int *hist, int n, int ntiles,
-                                               unsigned char *skip)
+/* Per segment, the counts of all eight digits: count[seg][pass][256]. A
+   block counts RS_COUNT_TILES tiles in shared memory before adding to the
+   segment's totals. */
+#define RS_COUNT_TILES 8
+__global__ void __launch_bounds__(RS_T) rs_count(const u64 *keys, int n, int nblk,
+                                                 unsigned int *count)
+{
+    __shared__ unsigned int cnt[RS_PASSES][256];
+    const int seg = blockIdx.x / nblk, blk = blockIdx.x % nblk;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const u64 *src = keys + (size_t)seg * n;
+#pragma unroll
+    for (int d = 0; d < RS_PASSES; ++d) cnt[d][tid] = 0;
+    __syncthreads();
+    const long long r0 = (long long)blk * RS_COUNT_TILES * RS_TILE;
+    const long long r1 = min((long long)n, r0 + (long long)RS_COUNT_TILES * RS_TILE);
+    for (long long c = r0; c < r1; c += 4 * RS_T) {
+        /* four loads in flight per thread; every lane takes part in the
+           warp votes, out-of-range ones with no digit */
+        u64 k[4];
+        bool in[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const long long idx = c + i * RS_T + tid;
+            in[i] = idx < r1;
+            k[i] = in[i] ? src[idx] : 0ULL;
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int d = 0; d < RS_PASSES; ++d) {
+                const unsigned dg = in[i] ? (unsigned)(k[i] >> (8 * d)) & 255u : 256u;
+                /* a digit the whole warp shares (a constant segment, the
+                   exponent bytes) is one add; the exponent bytes take few
+                   values, so they are grouped; mantissa bytes scatter over
+                   the bins and add one by one */
+                if (__all_sync(0xffffffffu, dg == __shfl_sync(0xffffffffu, dg, 0))) {
+                    if (lane == 0 && dg < 256u) atomicAdd(&cnt[d][dg], 32u);
+                } else if (d >= 6) {
+                    const unsigned peers = __match_any_sync(0xffffffffu, dg);
+                    if (dg < 256u && lane == __ffs(peers) - 1)
+                        atomicAdd(&cnt[d][dg], (unsigned)__popc(peers));
+                } else if (dg < 256u) {
+                    atomicAdd(&cnt[d][dg], 1u);
+                }
+            }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int d = 0; d < RS_PASSES; ++d)
+        if (cnt[d][tid]) atomicAdd(&count[((size_t)seg * RS_PASSES + d) * 256 + tid], cnt[d][tid]);
+}
+
+/* Per segment: digit counts -> first output positions (in place), the mask
+   of skipped passes, and the buffer that holds the sorted keys. */
+__global__ void __launch_bounds__(256) rs_prep(unsigned int *count, int n, unsigned char *skip,
+                                               unsigned char *par)
 {
     __shared__ unsigned int wsum[8];
     const int seg = blockIdx.x, d = threadIdx.x, lane = d & 31, w = d >> 5;
-    unsigned int *h = hist + (size_t)seg * ntiles * 256;
-    unsigned int total = 0;
-    for (int t = 0; t < ntiles; ++t) total += h[(size_t)t * 256 + d];
-    /* exclusive scan of the 256 digit totals */
-    unsigned int x = total;
+    unsigned mask = 0;
+    for (int pass = 0; pass < RS_PASSES; ++pass) {
+        unsigned int *h = count + ((size_t)seg * RS_PASSES + pass) * 256;
+        const unsigned int total = h[d];
+        unsigned int x = total;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const unsigned int y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) wsum[w] = x;
+        const int all = __syncthreads_or(total == (unsigned)n);
+        unsigned int before = 0;
+        for (int k = 0; k < w; ++k) before += wsum[k];
+        h[d] = before + x - total;
+        if (all) mask |= 1u << pass;
+        __syncthreads();
     }
-    if (lane == 31) wsum[w] = x;
-    const int all = __syncthreads_or(total == (unsigned)n);
-    unsigned int before = 0;
-    for (int k = 0; k < w; ++k) before += wsum[k];
-    unsigned int off = before + x - total;
-    if (d == 0) skip[seg] = all ? 1 : 0;
-    for (int t = 0; t < ntiles; ++t) {
-        const unsigned int c = h[(size_t)t * 256 + d];
-        h[(size_t)t * 256 + d] = off;
-        off += c;
+    if (d == 0) {
+        skip[seg] = (unsigned char)mask;
+        par[seg] = (unsigned char)(__popc(~mask & 0xffu) & 1);
     }
 }
 
-/* Stable scatter of one pass. Warp w owns 512 consecutive keys of the tile
-   and ranks each key among the warp's earlier keys of the same digit
-   (match_any per round of 32); the warps' digit counts are then scanned in
-   warp order, so the output keeps the input order inside a digit. The tile
-   is first reordered by digit in shared memory, so that consecutive threads
+/* One pass over every segment's tiles. Warp w ranks its keys among the
+   warp's earlier keys of the same digit (match_any per round of 32); the
+   warps' counts are scanned in warp order, so the pass is stable. The tile
+   is reordered by digit in shared memory first, so that consecutive threads
    write consecutive addresses of each digit's output run. */
 template <bool VALS>
-__host__ __device__ constexpr size_t rs_scatter_smem()
+__host__ __device__ constexpr size_t rs_pass_smem()
 {
     return sizeof(u64) * RS_TILE + (VALS ? 2 * sizeof(unsigned int) * RS_TILE : 0);
 }
 
 template <bool VALS>
-__global__ void __launch_bounds__(RS_T, 3) rs_scatter(u64 *ka, u64 *kb, unsigned int *va,
-                                                      unsigned int *vb, const unsigned char *par,
-                                                      const unsigned char *skip,
-                                                      const unsigned int *hist, int n, int ntiles,
-                                                      int shift)
+__global__ void __launch_bounds__(RS_T, 3) rs_pass(u64 *ka, u64 *kb, unsigned int *va,
+                                                   unsigned int *vb, const unsigned char *skip,
+                                                   const unsigned int *goff_all, u64 *state,
+                                                   int *ticket, int *abort_flag, int n,
+                                                   int ntiles, int pass)
 {
     extern __shared__ __align__(16) unsigned char sm[];
     u64 *skey = reinterpret_cast<u64 *>(sm);
@@ -223,18 +268,25 @@ __global__ void __launch_bounds__(RS_T, 3) rs_scatter(u64 *ka, u64 *kb, unsigned
     unsigned int *sval = sval_in + RS_TILE;
     __shared__ unsigned int cnt[RS_WARPS][256];
     __shared__ unsigned int goff[256], lstart[256], wsum[RS_WARPS];
-    const int seg = blockIdx.x / ntiles, tile = blockIdx.x % ntiles;
-    if (skip[seg]) return;
+    __shared__ int s_ticket;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    if (tid == 0) s_ticket = atomicAdd(ticket + pass, 1);
+    __syncthreads();
+    /* segments interleave in ticket order, so the tiles in flight spread
+       over the segments and each look-back chain stays short */
+    const int nseg = (int)(gridDim.x / (unsigned)ntiles);
+    const int seg = s_ticket % nseg, tile = s_ticket / nseg;
+    const unsigned mask = skip[seg];
+    if (mask & (1u << pass)) return;
+    const int shift = 8 * pass;
+    const bool p = (__popc(~mask & ((1u << pass) - 1u)) & 1) != 0;
     const size_t sb = (size_t)seg * n;
-    const bool p = par[seg] != 0;
     const u64 *src = (p ? kb : ka) + sb;
     u64 *dst = (p ? ka : kb) + sb;
     const unsigned int *vsrc = VALS ? (p ? vb : va) + sb : nullptr;
     unsigned int *vdst = VALS ? (p ? va : vb) + sb : nullptr;
 #pragma unroll
     for (int k = 0; k < RS_WARPS; ++k) cnt[k][tid] = 0;
-    goff[tid] = hist[((size_t)seg * ntiles + tile) * 256 + tid];
     constexpr int R = RS_TILE / RS_WARPS / 32;
     const int t0 = tile * RS_TILE;
     const int wb = w * (RS_TILE / RS_WARPS);
@@ -243,7 +295,6 @@ __global__ void __launch_bounds__(RS_T, 3) rs_scatter(u64 *ka, u64 *kb, unsigned
     u64 key[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-        /* all loads first, so each thread has R in flight */
         const int li = wb + 32 * r + lane;
         const bool in = li < count;
         key[r] = in ? src[t0 + li] : 0ULL;
@@ -262,8 +313,7 @@ __global__ void __launch_bounds__(RS_T, 3) rs_scatter(u64 *ka, u64 *kb, unsigned
         __syncwarp();
     }
     __syncthreads();
-    /* per digit: warp prefixes, the digit's tile total, its start in the
-       digit-ordered tile */
+    /* per digit (thread tid): warp prefixes and the tile's count */
     unsigned int tot = 0;
 #pragma unroll
     for (int k = 0; k < RS_WARPS; ++k) {
@@ -271,6 +321,33 @@ __global__ void __launch_bounds__(RS_T, 3) rs_scatter(u64 *ka, u64 *kb, unsigned
         cnt[k][tid] = tot;
         tot += c;
     }
+    /* publish, then look back over the earlier tiles of the segment */
+    volatile u64 *st = reinterpret_cast<volatile u64 *>(state) + (size_t)seg * ntiles * 256;
+    st[(size_t)tile * 256 + tid] = rs_word(tile == 0 ? RS_ST_PREFIX : RS_ST_AGG, pass, tot);
+    unsigned int excl = 0;
+    bool failed = false;
+    for (int j = tile - 1; j >= 0 && !failed; --j) {
+        unsigned spins = 0, ns = 8;
+        u64 v;
+        for (;;) {
+            v = st[(size_t)j * 256 + tid];
+            if ((int)((v >> 32) & 0xffu) == pass + 1 && (v >> 62) != 0) break;
+            if (++spins > RS_SPIN_LIMIT || *(volatile int *)abort_flag) {
+                atomicExch(abort_flag, 1);
+                failed = true;
+                break;
+            }
+            __nanosleep(ns);
+            if (ns < 256) ns <<= 1;
+        }
+        if (failed) break;
+        excl += (unsigned int)v;
+        if ((v >> 62) == RS_ST_PREFIX) break;
+    }
+    if (tile > 0 && !failed)
+        st[(size_t)tile * 256 + tid] = rs_word(RS_ST_PREFIX, pass, excl + tot);
+    goff[tid] = goff_all[((size_t)seg * RS_PASSES + pass) * 256 + tid] + excl;
+    /* the tile's digit starts in the digit-ordered tile */
     unsigned int x = tot;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -282,7 +359,7 @@ __global__ void __launch_bounds__(RS_T, 3) rs_scatter(u64 *ka, u64 *kb, unsigned
     unsigned int before = 0;
     for (int k = 0; k < w; ++k) before += wsum[k];
     lstart[tid] = before + x - tot;
-    __syncthreads();
+    if (__syncthreads_or(failed)) return;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int li = wb + 32 * r + lane;
@@ -297,44 +374,46 @@ __global__ void __launch_bounds__(RS_T, 3) rs_scatter(u64 *ka, u64 *kb, unsigned
         const u64 k = skey[i];
         const unsigned d = (unsigned)(k >> shift) & 255u;
         const unsigned int pos = goff[d] + (unsigned)i - lstart[d];
+        if (pos >= (unsigned)n) {
+            atomicExch(abort_flag, 1);
+            continue;
+        }
         dst[pos] = k;
         if (VALS) vdst[pos] = sval[i];
     }
 }
 
-/* After a pass: a segment that moved now lives in the other buffer. */
-__global__ void rs_flip(unsigned char *par, const unsigned char *skip, int nseg)
-{
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s < nseg && !skip[s]) par[s] ^= 1;
-}
-
 struct RsBuffers {
     u64 *ka, *kb;
     unsigned int *va, *vb;
-    unsigned int *hist;
+    unsigned int *count; /* [nseg][8][256] digit counts, then first positions */
+    u64 *state;          /* [nseg][ntiles][256] look-back words */
+    int *ticket;         /* [8] per-pass tile tickets */
     unsigned char *par, *skip;
 };
 
-/* Sort `nseg` segments of n keys (with row payloads when VALS) in place
-   across the two buffers; par[seg] tells which holds the result. */
+/* Sort `nseg` segments of n keys (with row payloads when VALS) across the
+   two buffers; par[seg] tells which holds the result. Returns the number of
+   kernels launched. A look-back that gave up, or a position out of range,
+   sets *abort_flag (which the caller zeroes once and checks after). */
 template <bool VALS>
-unsigned long long rs_sort(const RsBuffers &b, int nseg, int n, cudaStream_t s)
+unsigned long long rs_sort(const RsBuffers &b, int nseg, int n, int *abort_flag, cudaStream_t s)
 {
     const int ntiles = (n + RS_TILE - 1) / RS_TILE;
-    cudaFuncSetAttribute(rs_scatter<VALS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)rs_scatter_smem<VALS>());
+    const int nblk = (ntiles + RS_COUNT_TILES - 1) / RS_COUNT_TILES;
+    cudaFuncSetAttribute(rs_pass<VALS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)rs_pass_smem<VALS>());
+    cudaMemsetAsync(b.count, 0, sizeof(unsigned int) * RS_PASSES * 256 * (size_t)nseg, s);
+    cudaMemsetAsync(b.state, 0, sizeof(u64) * 256 * (size_t)ntiles * (size_t)nseg, s);
+    cudaMemsetAsync(b.ticket, 0, sizeof(int) * RS_PASSES, s);
+    rs_count<<<(unsigned)nseg * (unsigned)nblk, RS_T, 0, s>>>(b.ka, n, nblk, b.count);
+    rs_prep<<<nseg, 256, 0, s>>>(b.count, n, b.skip, b.par);
     const unsigned grid = (unsigned)nseg * (unsigned)ntiles;
-    cudaMemsetAsync(b.par, 0, nseg, s);
-    for (int pass = 0; pass < 8; ++pass) {
-        const int shift = 8 * pass;
-        rs_hist<<<grid, RS_T, 0, s>>>(b.ka, b.kb, b.par, n, ntiles, shift, b.hist);
-        rs_scan<<<nseg, 256, 0, s>>>(b.hist, n, ntiles, b.skip);
-        rs_scatter<VALS><<<grid, RS_T, rs_scatter_smem<VALS>(), s>>>(
-            b.ka, b.kb, b.va, b.vb, b.par, b.skip, b.hist, n, ntiles, shift);
-        rs_flip<<<(nseg + 255) / 256, 256, 0, s>>>(b.par, b.skip, nseg);
-    }
-    return 32;
+    for (int pass = 0; pass < RS_PASSES; ++pass)
+        rs_pass<VALS><<<grid, RS_T, rs_pass_smem<VALS>(), s>>>(
+            b.ka, b.kb, b.va, b.vb, b.skip, b.count, b.state, b.ticket, abort_flag, n, ntiles,
+            pass);
+    return 2 + RS_PASSES;
 }
 
 /* ---- runs and exact sums ----------------------------------------------- */
@@ -671,7 +750,9 @@ size_t rs_bytes(size_t keys, int nseg, int n, bool vals)
 {
     const size_t ntiles = (size_t)((n + RS_TILE - 1) / RS_TILE);
     size_t s = 2 * sizeof(u64) * keys + (vals ? 2 * sizeof(unsigned int) * keys : 0);
-    s += sizeof(unsigned int) * 256 * ntiles * (size_t)nseg + 2 * (size_t)nseg + 512;
+    s += sizeof(unsigned int) * RS_PASSES * 256 * (size_t)nseg;
+    s += sizeof(u64) * 256 * ntiles * (size_t)nseg;
+    s += 2 * (size_t)nseg + sizeof(int) * RS_PASSES + 8 * 256;
     s += 2 * sizeof(__int128) * ntiles * (size_t)nseg;
     return s;
 }
@@ -688,8 +769,10 @@ RsBuffers rs_carve(unsigned char *base, size_t *cur, int nseg, int n, bool vals,
                 : nullptr;
     b.vb = vals ? reinterpret_cast<unsigned int *>(base + rc_take(cur, sizeof(unsigned int) * keys))
                 : nullptr;
-    b.hist = reinterpret_cast<unsigned int *>(
-        base + rc_take(cur, sizeof(unsigned int) * 256 * ntiles * (size_t)nseg));
+    b.count = reinterpret_cast<unsigned int *>(
+        base + rc_take(cur, sizeof(unsigned int) * RS_PASSES * 256 * (size_t)nseg));
+    b.state = reinterpret_cast<u64 *>(base + rc_take(cur, sizeof(u64) * 256 * ntiles * (size_t)nseg));
+    b.ticket = reinterpret_cast<int *>(base + rc_take(cur, sizeof(int) * RS_PASSES));
     b.par = base + rc_take(cur, (size_t)nseg);
     b.skip = base + rc_take(cur, (size_t)nseg);
     *part = reinterpret_cast<__int128 *>(base + rc_take(cur, 2 * sizeof(__int128) * ntiles * nseg));
@@ -710,20 +793,24 @@ int rk_prepare(RcCtx *c)
     }
     size_t cur = 0;
     const size_t o_out = rc_take(&cur, sizeof(u64) * 4);
+    const size_t o_abort = rc_take(&cur, sizeof(int));
     const size_t io_end = rc_take(&cur, 0);
     const size_t work = cur;
     if (rc_reserve(c, work + rs_bytes((size_t)n, 1, n, true) + 4096, io_end) != 0) return -1;
+    int *d_abort = reinterpret_cast<int *>(c->dev + o_abort);
+    cudaMemsetAsync(d_abort, 0, sizeof(int), c->s);
     __int128 *part = nullptr;
     size_t wc = work;
     const RsBuffers b = rs_carve(c->dev, &wc, 1, n, true, &part);
     const int ntiles = (n + RS_TILE - 1) / RS_TILE;
     rk_target_keys<<<(n + 255) / 256, 256, 0, c->s>>>(c->d_y64, n, b.ka, b.va);
-    c->launches += 3 + rs_sort<true>(b, 1, n, c->s);
+    c->launches += 3 + rs_sort<true>(b, 1, n, d_abort, c->s);
     rk_runs<RK_FILL><<<ntiles, RS_T, 0, c->s>>>(b.ka, b.kb, b.va, b.vb, b.par, n, ntiles, nullptr,
                                                 c->d_rank_b, part);
     rk_final<<<1, 32, 0, c->s>>>(part, ntiles, 1, reinterpret_cast<u64 *>(c->dev + o_out));
-    cudaMemcpyAsync(c->host + o_out, c->dev + o_out, sizeof(u64) * 4, cudaMemcpyDeviceToHost, c->s);
+    cudaMemcpyAsync(c->host + o_out, c->dev + o_out, io_end - o_out, cudaMemcpyDeviceToHost, c->s);
     if (rc_finish(c) != 0) return -1;
+    if (*reinterpret_cast<const int *>(c->host + o_abort) != 0) return -1;
     /* sum A^2 of the target is sum B^2 */
     const u64 *h = reinterpret_cast<const u64 *>(c->host + o_out);
     c->rank_bb[0] = h[2];
@@ -801,6 +888,7 @@ float rc_rank_score_batch(void *ctx, const unsigned int *prog, const unsigned in
     stat_inputs(c, prog, off, pcount, nsets, nsegs, kmax, c0, &cur, sp);
     const size_t o_out = rc_take(&cur, sizeof(u64) * 4 * (size_t)nsegs);
     const size_t o_status = rc_take(&cur, sizeof(int) * (size_t)nsegs);
+    const size_t o_abort = rc_take(&cur, sizeof(int));
     const size_t io_end = rc_take(&cur, 0);
     const int wseg = wave_segments(nsegs, n, true);
     const size_t work = cur;
@@ -809,7 +897,9 @@ float rc_rank_score_batch(void *ctx, const unsigned int *prog, const unsigned in
     stat_copy(c, pcount, nsets, nsegs, kmax, c0, sp);
     unsigned char *dev = c->dev;
     int *d_status = reinterpret_cast<int *>(dev + o_status);
+    int *d_abort = reinterpret_cast<int *>(dev + o_abort);
     cudaMemsetAsync(d_status, 0, sizeof(int) * nsegs, c->s);
+    cudaMemsetAsync(d_abort, 0, sizeof(int), c->s);
     const size_t smem = key_smem(sp);
     if (smem > 48 * 1024 &&
         cudaFuncSetAttribute(rk_keys<RK_RANK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -830,7 +920,7 @@ float rc_rank_score_batch(void *ctx, const unsigned int *prog, const unsigned in
             reinterpret_cast<const int *>(dev + sp.o_valid),
             reinterpret_cast<const double *>(dev + sp.o_c0), kmax, c->d_cols64, c->d_y64, c->npad,
             n, ntrials, s0, ktiles, sp.b.fmaxins, b.ka, b.va, d_status);
-        c->launches += 3 + rs_sort<true>(b, ns, n, c->s);
+        c->launches += 3 + rs_sort<true>(b, ns, n, d_abort, c->s);
         rk_runs<RK_SUMS><<<(unsigned)ns * ntiles, RS_T, 0, c->s>>>(
             b.ka, b.kb, b.va, b.vb, b.par, n, ntiles, c->d_rank_b, nullptr, part);
         rk_final<<<(ns + 127) / 128, 128, 0, c->s>>>(part, ntiles, ns,
@@ -841,6 +931,7 @@ float rc_rank_score_batch(void *ctx, const unsigned int *prog, const unsigned in
     cudaMemcpyAsync(c->host + sp.in_end, dev + sp.in_end, io_end - sp.in_end,
                     cudaMemcpyDeviceToHost, c->s);
     if (rc_finish(c) != 0) return -1.0f;
+    if (*reinterpret_cast<const int *>(c->host + o_abort) != 0) return -1.0f;
     memcpy(out, c->host + o_out, sizeof(u64) * 4 * (size_t)nsegs);
     memcpy(out_status, c->host + o_status, sizeof(int) * (size_t)nsegs);
     out_bb[0] = c->rank_bb[0];
@@ -880,6 +971,7 @@ float rc_order_stat_score_batch(void *ctx, const unsigned int *prog, const unsig
     stat_inputs(c, prog, off, pcount, nsets, nsegs, kmax, c0, &cur, sp);
     const size_t o_val = rc_take(&cur, sizeof(double) * (size_t)nsegs);
     const size_t o_status = rc_take(&cur, sizeof(int) * (size_t)nsegs);
+    const size_t o_abort = rc_take(&cur, sizeof(int));
     const size_t io_end = rc_take(&cur, 0);
     const int wseg = wave_segments(nsegs, n, false);
     const size_t work = cur;
@@ -888,7 +980,9 @@ float rc_order_stat_score_batch(void *ctx, const unsigned int *prog, const unsig
     stat_copy(c, pcount, nsets, nsegs, kmax, c0, sp);
     unsigned char *dev = c->dev;
     int *d_status = reinterpret_cast<int *>(dev + o_status);
+    int *d_abort = reinterpret_cast<int *>(dev + o_abort);
     cudaMemsetAsync(d_status, 0, sizeof(int) * nsegs, c->s);
+    cudaMemsetAsync(d_abort, 0, sizeof(int), c->s);
     const size_t smem = key_smem(sp);
     if (smem > 48 * 1024 &&
         cudaFuncSetAttribute(rk_keys<RK_ABS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -908,7 +1002,7 @@ float rc_order_stat_score_batch(void *ctx, const unsigned int *prog, const unsig
             reinterpret_cast<const int *>(dev + sp.o_valid),
             reinterpret_cast<const double *>(dev + sp.o_c0), kmax, c->d_cols64, c->d_y64, c->npad,
             n, ntrials, s0, ktiles, sp.b.fmaxins, b.ka, nullptr, d_status);
-        c->launches += 2 + rs_sort<false>(b, ns, n, c->s);
+        c->launches += 2 + rs_sort<false>(b, ns, n, d_abort, c->s);
         os_pick<<<ns, OS_T, 0, c->s>>>(b.ka, b.kb, b.par, n, s0, ns, what, d_status,
                                        reinterpret_cast<double *>(dev + o_val));
     }
@@ -917,6 +1011,7 @@ float rc_order_stat_score_batch(void *ctx, const unsigned int *prog, const unsig
     cudaMemcpyAsync(c->host + sp.in_end, dev + sp.in_end, io_end - sp.in_end,
                     cudaMemcpyDeviceToHost, c->s);
     if (rc_finish(c) != 0) return -1.0f;
+    if (*reinterpret_cast<const int *>(c->host + o_abort) != 0) return -1.0f;
     memcpy(out_value, c->host + o_val, sizeof(double) * (size_t)nsegs);
     memcpy(out_status, c->host + o_status, sizeof(int) * (size_t)nsegs);
     float ms = -1.0f;
