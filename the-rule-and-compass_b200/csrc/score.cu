@@ -278,6 +278,7 @@ float rc_score_run(RcCtx *c, const uint32_t *words, const uint32_t *off, int wid
     const size_t o_pbarerr = rc_take(&cur, sizeof(double) * nprog);
     const size_t o_pbar64 = rc_take(&cur, sizeof(double) * nprog);
     const size_t o_flagged = rc_take(&cur, sizeof(int) * nprog);
+    const size_t o_badrow = rc_take(&cur, track && !corr ? sizeof(int) * nprog : 0);
     const size_t o_part64 = rc_take(&cur, track ? 2 * sizeof(double) * (size_t)nprog * ntiles : 0);
     const size_t o_pred = rc_take(&cur, pred_out ? sizeof(float) * (size_t)nprog * c->n : 0);
     const size_t dev_end = rc_take(&cur, 0);
@@ -295,6 +296,7 @@ float rc_score_run(RcCtx *c, const uint32_t *words, const uint32_t *off, int wid
     memcpy(host + o_ctiles, cand_tiles.data(), sizeof(int) * nprog);
     cudaMemcpyAsync(dev, host, in_end, cudaMemcpyHostToDevice, c->s);
     cudaMemsetAsync(dev + o_bad, 0, o_zero_end - o_bad, c->s);
+    if (track && !corr) cudaMemsetAsync(dev + o_badrow, 0x7f, sizeof(int) * nprog, c->s);
     st->h2d_ms += rc_now_ms() - t;
     st->h2d_bytes += in_end;
 
@@ -319,6 +321,7 @@ float rc_score_run(RcCtx *c, const uint32_t *words, const uint32_t *off, int wid
     a.ntiles = ntiles;
     a.part = reinterpret_cast<double *>(dev + o_part);
     a.bad = reinterpret_cast<int *>(dev + o_bad);
+    a.badrow = track && !corr ? reinterpret_cast<int *>(dev + o_badrow) : nullptr;
     a.pred = pred_out ? reinterpret_cast<float *>(dev + o_pred) : nullptr;
     a.pbar = reinterpret_cast<const double *>(dev + o_pbar);
     a.pbar_err = reinterpret_cast<const double *>(dev + o_pbarerr);
@@ -404,6 +407,18 @@ float rc_score_run(RcCtx *c, const uint32_t *words, const uint32_t *off, int wid
         }
         const int grid = c->sm_count *
                          occupancy_blocks((const void *)rc_score64_kernel<LANE_T>, LANE_T, smem);
+        if (a.badrow) {
+            /* the f32 failure rows first: most failures are confirmed there */
+            l.mode = mode;
+            const size_t csmem = (size_t)max_slots * 32 * 16 + RC_MAX_INS * sizeof(RcIns);
+            if (set_smem((const void *)rc_badrow_check<32>, csmem) != 0) {
+                st->failed = 1;
+                cudaStreamSynchronize(c->s);
+                return -1.0f;
+            }
+            rc_badrow_check<32><<<nprog, 32, csmem, c->s>>>(l, a.badrow);
+            c->launches += 1;
+        }
         for (int pass = 0; pass < passes; ++pass) {
             const int kmode = corr ? (pass == 0 ? SM_CORR_PASS1 : SM_CORR_PASS2) : mode;
             if (pass == 1) cudaMemsetAsync(dev + o_bad64, 0, sizeof(int) * nprog, c->s);

@@ -405,6 +405,7 @@ struct ScoreArgs {
     int nprog;
     int ptiles;
     int *bad;             /* [P] */
+    int *badrow;          /* [P] or null: first 4-row group of a hard failure */
     float *pred;          /* SM_PREDICT: [P][n] */
     const double *pbar;   /* SM_CORR_PASS2: per-candidate mean prediction */
     const double *pbar_err;
@@ -586,8 +587,14 @@ __global__ void __launch_bounds__(T) rc_score_kernel(ScoreArgs a)
                         rc_accumulate(a, mode, pr[i], pq[i], yy[i], row, cand, a0, a1, e0, e1,
                                       bad);
                 }
-                /* a hard failure ends this warp's rows of the candidate */
-                if (skip_bad && __any_sync(0xffffffffu, bad)) break;
+                /* a hard failure ends this warp's rows of the candidate; the
+                   lowest failing 4-row group is kept for the f64 re-check */
+                if (skip_bad && __any_sync(0xffffffffu, bad)) {
+                    const int grp = __reduce_min_sync(0xffffffffu,
+                                                      bad ? (unsigned)myrow : 0x7fffffffu);
+                    if (a.badrow && lane == 0) atomicMin(a.badrow + cand, grp);
+                    break;
+                }
             }
             if (mode == SM_PREDICT) continue;
             if (mode == SM_MAXIMUM) {
@@ -880,17 +887,27 @@ __global__ void __launch_bounds__(T) rc_score64_kernel(Score64Args a)
     double2 *stk = reinterpret_cast<double2 *>(smem_raw);
     RcIns *sprog = reinterpret_cast<RcIns *>(stk + a.nslots * T);
     double *red = reinterpret_cast<double *>(sprog + RC_MAX_INS);
-    __shared__ int s_item;
+    __shared__ int s_item, s_known;
     const int tid = threadIdx.x;
     const int SUB = 2 * T;
     const int subtiles = RC_TILE_ROWS / SUB;
     const int mode = a.mode;
     for (;;) {
-        if (tid == 0) s_item = atomicAdd(a.counter, 1);
+        const int total = *a.nflag * a.ntiles;
+        if (tid == 0) {
+            s_item = atomicAdd(a.counter, 1);
+            s_known = s_item < total ? *((volatile int *)(a.bad + a.flagged[s_item / a.ntiles]))
+                                     : 0;
+        }
         __syncthreads();
         const int item = s_item;
-        const int total = *a.nflag * a.ntiles;
         if (item >= total) break;
+        /* a candidate already shown non-finite needs no more rows (its
+           partial sums are not read) */
+        if (s_known) {
+            __syncthreads();
+            continue;
+        }
         const int cand = a.flagged[item / a.ntiles];
         const int tile = item % a.ntiles;
         const int b = a.ins_off[cand], e = a.ins_off[cand + 1];
@@ -958,6 +975,48 @@ __global__ void __launch_bounds__(T) rc_score64_kernel(Score64Args a)
             __syncthreads();
         }
     }
+}
+
+/* A row's hard failure in the f64 lane (the rule of rc_score64_kernel): a
+   prediction that is not finite or beyond 1e30, and for the classification
+   objectives an invalid weight or label. */
+__device__ __forceinline__ bool rc_row64_bad(const Score64Args &a, double v, int row)
+{
+    if (a.mode >= SM_LOG_LOSS && a.mode <= SM_HINGE_SQUARED) {
+        const double wi = a.w ? a.w[row] : 1.0;
+        if (!isfinite(wi) || wi < 0.0) return true;
+        if (wi == 0.0) return false;
+        const double t = a.tsign ? (double)a.tsign[row] : CUDART_NAN;
+        return !isfinite(t) || !isfinite(v) || fabs(v) > 1e30;
+    }
+    return !isfinite(v) || fabs(v) > 1e30;
+}
+
+/* Before the f64 lane: each flagged candidate that failed in f32 has its
+   failing 4-row group evaluated in f64 first (one warp per candidate, two
+   lanes with two rows each). A failure there is a failure of the whole
+   candidate in f64, exactly what the lane's scan would find, so the lane
+   skips it; otherwise the lane scans all rows as before. */
+template <int T>
+__global__ void __launch_bounds__(T) rc_badrow_check(Score64Args a, const int *badrow)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2 *stk = reinterpret_cast<double2 *>(smem_raw);
+    RcIns *sprog = reinterpret_cast<RcIns *>(stk + a.nslots * T);
+    const int k = blockIdx.x, tid = threadIdx.x;
+    if (k >= *a.nflag) return;
+    const int cand = a.flagged[k];
+    const int r = badrow[cand];
+    if (r < 0 || r >= a.n) return;
+    const int b = a.ins_off[cand], e = a.ins_off[cand + 1];
+    for (int q = tid; q < e - b; q += T) sprog[q] = a.ins[b + q];
+    __syncthreads();
+    if (tid >= 2) return;
+    const int myrow = r + 2 * tid;
+    const double2 p = rc_run_d<T>(sprog, a.cols, a.npad, myrow, stk, tid);
+    const bool b0 = myrow < a.n && rc_row64_bad(a, p.x, myrow);
+    const bool b1 = myrow + 1 < a.n && rc_row64_bad(a, p.y, myrow + 1);
+    if (b0 || b1) atomicOr(a.bad + cand, 1);
 }
 
 /* Overwrite the flagged candidates' results with the f64 lane's. */
