@@ -115,6 +115,25 @@ float rc_pool_score(void *ctx, int which, int nprog, int width, int kind, const 
                     double *out, int *status);
 /* eval.cu:3864 rc_pool_hash: FNV-1a of each slot up to and including HALT. */
 int rc_pool_hash(void *ctx, int which, int nprog, int width, unsigned long long *out);
+/* The next generation of the fixed-width pool, on the device
+   (postfix.rs:511-567 Variation::next_generation_with_front with the engine
+   of postfix.rs:438-973 and genome.rs:43-302; the reference runs this on the
+   host). Parents: pool `which`, islands*pop slots of `width` (<= 128) words
+   with their errors err[islands*pop] (host). Children go to pool which ^ 1.
+   ops: nops (opcode, arity) pairs in the engine's table order; restart:
+   [islands] or NULL; front: nfront programs packed by front_off[nfront+1]
+   (words), drawn with probability front_p. Outputs (host, each nullable):
+   len/cost [islands*pop] u16, hash u64, err f64 (the island's elite keeps its
+   parent's error, every other slot NaN), words [islands*pop*width]. Returns
+   kernel ms >= 0, or -1 (bad arguments, a parent slot that is not a valid
+   program, or no pool of this width reserved). */
+float rc_pool_vary(void *ctx, int which, int islands, int pop, int width, const double *err,
+                   int nvars, int max_complexity, unsigned int seed, unsigned int gen,
+                   int init_depth, int dedup, const unsigned int *ops, int nops,
+                   const unsigned char *restart, const unsigned int *front,
+                   const unsigned int *front_off, int nfront, double front_p,
+                   unsigned short *out_len, unsigned short *out_cost,
+                   unsigned long long *out_hash, double *out_err, unsigned int *out_words);
 /* eval.cu:3438 rc_predict: raw P x N predictions, row-major, no 1e30 rule. */
 int rc_predict(void *ctx, const unsigned int *prog, const unsigned int *off, int nprog,
                float *out);

@@ -33,14 +33,17 @@ def build() -> str:
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB_PATH) or (
-                os.path.getmtime(LIB_PATH) < os.path.getmtime(os.path.join(HERE, "oracle.cpp"))):
+        if not os.path.exists(LIB_PATH) or any(
+                os.path.getmtime(LIB_PATH) < os.path.getmtime(os.path.join(HERE, f))
+                for f in ("oracle.cpp", "variation.cpp")):
             build()
         L = ctypes.CDLL(LIB_PATH)
         P = ctypes.POINTER
         i32p, f64p, f32p, u64p, i64p = (P(ctypes.c_int32), P(ctypes.c_double), P(ctypes.c_float),
                                         P(ctypes.c_uint64), P(ctypes.c_int64))
         ci, cd = ctypes.c_int, ctypes.c_double
+        u32, u32p = ctypes.c_uint32, P(ctypes.c_uint32)
+        u8p, u16p = P(ctypes.c_uint8), P(ctypes.c_uint16)
         sig = {
             "or_tree_ok": (ci, [i32p, f64p, ci]),
             "or_predict": (ci, [i32p, f64p, ci, f64p, ci, ci, f64p]),
@@ -55,6 +58,13 @@ def lib():
             "or_rank_sums": (ci, [f64p, f64p, ci, u64p]),
             "or_centred_ranks_doubled": (ci, [f64p, ci, i64p]),
             "or_erf": (cd, [cd]),
+            "orv_philox": (None, [u32, u32, u32, u32, u32, ci, u32p]),
+            "orv_hash": (ctypes.c_uint64, [u32p, ci]),
+            "orv_spans": (ci, [u32p, ci]),
+            "orv_random_arena": (None, [ci, ci, ci, u32, ci, u32p, ci, u32, ci, ci, u32p]),
+            "orv_next_generation": (ci, [ci, ci, ci, u32, ci, ci, u32p, ci, ci, ci, u32p, f64p,
+                                         u32, u8p, u32p, u32p, ci, cd, u32p, u16p, u16p, u64p,
+                                         f64p]),
             "or_erfc": (cd, [cd]),
         }
         for name, (res, args) in sig.items():
@@ -209,3 +219,69 @@ def erf(x):
 
 def erfc(x):
     return lib().or_erfc(float(x))
+
+
+# ---- flat postfix variation (oracle/variation.cpp) --------------------------
+
+def philox(seed, island, gen, slot, n=1, draw=0):
+    """The first n Philox4x32-10 outputs at (seed, island, gen, slot, draw)."""
+    out = np.zeros(4 * n, np.uint32)
+    lib().orv_philox(seed, island, gen, slot, draw, n, _ptr(out, ctypes.c_uint32))
+    return out.reshape(n, 4)
+
+
+def postfix_hash(words):
+    w = np.ascontiguousarray(words, np.uint32)
+    return int(lib().orv_hash(_ptr(w, ctypes.c_uint32), len(w)))
+
+
+def spans_count(words):
+    """Node count of the strict postfix parse, or -1 when malformed."""
+    w = np.ascontiguousarray(words, np.uint32)
+    return int(lib().orv_spans(_ptr(w, ctypes.c_uint32), len(w)))
+
+
+def _ops(ops):
+    return np.ascontiguousarray(np.asarray(ops, np.uint32).reshape(-1, 2))
+
+
+def random_arena(width, nvars, max_complexity, ops, rng_seed, depth, count):
+    """Parents as the reference's tests draw them: consecutive random
+    programs from the generator at (rng_seed, 0, 0, 0); [count, width]."""
+    o = _ops(ops)
+    out = np.zeros(count * width, np.uint32)
+    lib().orv_random_arena(width, nvars, max_complexity, 0, 3, _ptr(o, ctypes.c_uint32), len(o),
+                           rng_seed, depth, count, _ptr(out, ctypes.c_uint32))
+    return out.reshape(count, width)
+
+
+def next_generation(words, err, islands, pop, width, nvars, max_complexity, seed, gen, ops,
+                    init_depth=3, dedup=True, restart=None, front=None, front_p=0.0):
+    """Variation::next_generation_with_front on the CPU. Returns
+    (words [islands*pop, width], len, cost, hash, err)."""
+    o = _ops(ops)
+    w = np.ascontiguousarray(words, np.uint32).reshape(-1)
+    e = np.ascontiguousarray(err, np.float64)
+    r = None if restart is None else np.ascontiguousarray(restart, np.uint8)
+    fw, fo, nf = None, None, 0
+    if front:
+        fo = np.zeros(len(front) + 1, np.uint32)
+        fo[1:] = np.cumsum([len(f) for f in front])
+        fw = np.ascontiguousarray(np.concatenate([np.asarray(f, np.uint32) for f in front]))
+        nf = len(front)
+    n = islands * pop
+    ow = np.zeros(n * width, np.uint32)
+    ol = np.zeros(n, np.uint16)
+    oc = np.zeros(n, np.uint16)
+    oh = np.zeros(n, np.uint64)
+    oe = np.zeros(n, np.float64)
+    rc = lib().orv_next_generation(width, nvars, max_complexity, seed, init_depth, int(dedup),
+                                   _ptr(o, ctypes.c_uint32), len(o), islands, pop,
+                                   _ptr(w, ctypes.c_uint32), _ptr(e, ctypes.c_double), gen,
+                                   _ptr(r, ctypes.c_uint8), _ptr(fw, ctypes.c_uint32),
+                                   _ptr(fo, ctypes.c_uint32), nf, front_p,
+                                   _ptr(ow, ctypes.c_uint32), _ptr(ol, ctypes.c_uint16),
+                                   _ptr(oc, ctypes.c_uint16), _ptr(oh, ctypes.c_uint64),
+                                   _ptr(oe, ctypes.c_double))
+    assert rc == 0, "parents are not valid postfix programs"
+    return ow.reshape(n, width), ol, oc, oh, oe

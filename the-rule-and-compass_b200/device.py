@@ -65,6 +65,9 @@ SIGNATURES = {
     "rc_pool_eval": (cf, [cvp, ci, ci, ci, f32p, ci]),
     "rc_pool_score": (cf, [cvp, ci, ci, ci, ci, i32p, f64p, i32p]),
     "rc_pool_hash": (ci, [cvp, ci, ci, ci, u64p]),
+    "rc_pool_vary": (cf, [cvp, ci, ci, ci, ci, f64p, ci, ci, ctypes.c_uint, ctypes.c_uint, ci, ci,
+                          u32p, ci, P(ctypes.c_uint8), u32p, u32p, ci, ctypes.c_double,
+                          P(ctypes.c_uint16), P(ctypes.c_uint16), u64p, f64p, u32p]),
     "rc_predict": (ci, [cvp, u32p, u32p, ci, f32p]),
     "rc_fit_batch": (cf, [cvp, u32p, u32p, i32p, ci, ci, f64p, i32p, ci, ci, f64p, f64p, i32p]),
     "rc_fit_kernel_info": (ci, [ci, i32p, i32p, i32p]),
@@ -400,3 +403,59 @@ def device_count() -> int:
 
 def device_name() -> str:
     return lib().rc_device_name().decode()
+
+
+class GenomePool:
+    """The device's double-buffered fixed-width program pool (`rc_pool_*`,
+    eval.cu:3514-3874) of islands x pop slots, with the next generation built
+    on the device (`rc_pool_vary`, postfix.rs:511-567)."""
+
+    def __init__(self, ev, islands, pop, width):
+        self.ev, self.islands, self.pop, self.width = ev, islands, pop, width
+        if lib().rc_pool_reserve(ev.ctx, islands * pop, width) != 0:
+            raise DeviceError("rc_pool_reserve failed")
+
+    def upload(self, which, words):
+        w = np.ascontiguousarray(words, np.uint32).reshape(-1)
+        assert w.size == self.islands * self.pop * self.width
+        if lib().rc_pool_upload(self.ev.ctx, which, _p(w, ctypes.c_uint32),
+                                self.islands * self.pop) != 0:
+            raise DeviceError("rc_pool_upload failed")
+
+    def hash(self, which):
+        out = np.zeros(self.islands * self.pop, np.uint64)
+        if lib().rc_pool_hash(self.ev.ctx, which, self.islands * self.pop, self.width,
+                              _p(out, ctypes.c_uint64)) != 0:
+            raise DeviceError("rc_pool_hash failed")
+        return out
+
+    def vary(self, which, err, gen, nvars, max_complexity, seed, ops, init_depth=3, dedup=True,
+             restart=None, front=None, front_p=0.0, words=True):
+        """Children of pool `which` into pool `which ^ 1`. Returns
+        (words [islands*pop, width] or None, len, cost, hash, err, ms)."""
+        n = self.islands * self.pop
+        e = np.ascontiguousarray(err, np.float64)
+        o = np.ascontiguousarray(np.asarray(ops, np.uint32).reshape(-1))
+        r = None if restart is None else np.ascontiguousarray(restart, np.uint8)
+        fw = fo = None
+        nf = 0
+        if front:
+            fo = np.zeros(len(front) + 1, np.uint32)
+            fo[1:] = np.cumsum([len(f) for f in front])
+            fw = np.ascontiguousarray(np.concatenate([np.asarray(f, np.uint32) for f in front]))
+            nf = len(front)
+        ol = np.zeros(n, np.uint16)
+        oc = np.zeros(n, np.uint16)
+        oh = np.zeros(n, np.uint64)
+        oe = np.zeros(n, np.float64)
+        ow = np.zeros(n * self.width, np.uint32) if words else None
+        ms = lib().rc_pool_vary(self.ev.ctx, which, self.islands, self.pop, self.width,
+                                _p(e, ctypes.c_double), nvars, max_complexity, seed, gen,
+                                init_depth, int(dedup), _p(o, ctypes.c_uint32), len(o) // 2,
+                                _p(r, ctypes.c_uint8), _p(fw, ctypes.c_uint32),
+                                _p(fo, ctypes.c_uint32), nf, front_p, _p(ol, ctypes.c_uint16),
+                                _p(oc, ctypes.c_uint16), _p(oh, ctypes.c_uint64),
+                                _p(oe, ctypes.c_double), _p(ow, ctypes.c_uint32))
+        if ms < 0:
+            raise DeviceError("rc_pool_vary failed")
+        return (None if ow is None else ow.reshape(n, self.width)), ol, oc, oh, oe, ms

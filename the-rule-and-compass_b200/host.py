@@ -206,3 +206,16 @@ def select_promoted(island_pop, pending, error, complexity, has_constants, train
     if k < 0:
         raise RuntimeError("rch_select_promoted failed")
     return list(zip(oi[:k].tolist(), oj[:k].tolist()))
+
+
+# Op::default_set() (my-version/src/expr.rs:392-398) through postfix_opcode
+# (my-version/src/gpu.rs:447-494): the variation engine's (opcode, arity)
+# table, in table order.
+DEFAULT_VARIATION_OPS = ((17, 1), (9, 1), (10, 1), (12, 1), (11, 1), (6, 1), (7, 1), (8, 1),
+                         (21, 1), (22, 1), (13, 1), (14, 1), (18, 1), (15, 1), (16, 1),
+                         (2, 2), (3, 2), (4, 2), (5, 2), (20, 2), (32, 3))
+
+
+def width_for(max_complexity):
+    """Fixed slot width for a maximum complexity (genome.rs:35-37)."""
+    return max(2 * max_complexity + 4, 8)
