@@ -15,8 +15,11 @@ GPU the same line also carries the other configurations:
             LM fit of those with constants;
   c5:       one island's generation (P = 1000) over N = 4,194,304 rows x 10
             heavy-tailed features: the L1 IRLS fit and the exact
-            rank-correlation sums.
-`--workload fit|implicit|c5|rank` makes one of them the primary line.
+            rank-correlation sums;
+  vary:     the next generation of a 16 x 1000 program pool built on the
+            device (tournament, crossover, mutation, hashing, dedup),
+            children/s beside the CPU restatement of the reference engine.
+`--workload fit|implicit|c5|rank|vary` makes one of them the primary line.
 
 One step is one pass of the hot path over the whole batch. `value` is
 device-timed with CUDA events on the library's stream (inputs resident in
@@ -484,6 +487,62 @@ def bench_c5(args, rank, pkg, W, flushbuf, steps, warmup, fit_steps, fit_warmup)
     return fit, what, rk
 
 
+def bench_vary(args, rank, pkg, flushbuf, steps, warmup):
+    """One generation of the device variation (rc_pool_vary): 16 islands x
+    1000 slots of width 64 (max complexity 30, 10 inputs, the default
+    operator set), parents drawn as the reference's tests draw them, seeded
+    errors. children/s from the library's events around the call, e2e from
+    the wall clock of the call with host buffers (errors in; lengths, node
+    counts, hashes, errors and the child programs out), beside the CPU
+    restatement of the reference engine on one thread."""
+    islands = args.P if args.workload == "vary" and args.P else 16
+    pop, width, nvars, mc = 1000, 64, 10, 30
+    n = islands * pop
+    ops = pkg.DEFAULT_VARIATION_OPS
+    err = np.array([((i * 7919) % 10007) / 10007.0 for i in range(n)])
+    x = np.linspace(-1.0, 1.0, 64, dtype=np.float32)
+    ev = pkg.GpuEvaluator(np.stack([x, x]).reshape(-1), 64, 2, x)
+    pool = pkg.GenomePool(ev, islands, pop, width)
+    # parents: a restarted (random) population built by the device into pool 1
+    seed_words = np.full((n, width), 255, np.uint32)
+    seed_words[:, 0], seed_words[:, 1] = 1, 0
+    pool.upload(0, seed_words)
+    words = pool.vary(0, err, 0, nvars, mc, 5 + rank, ops, restart=[1] * islands)[0]
+    for g in range(warmup):
+        pool.vary(1, err, 1 + g, nvars, mc, 77, ops)
+    dev_ms, wall = [], []
+    n0 = ev.launch_count()
+    import torch
+    for g in range(steps):
+        flush_l2(flushbuf)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = pool.vary(1, err, 1 + g, nvars, mc, 77, ops)
+        wall.append(time.perf_counter() - t0)
+        dev_ms.append(out[5])
+    launches = ev.launch_count() - n0
+    # the CPU baseline and checker: the reference engine restated on the CPU
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    t0 = time.perf_counter()
+    ref = O.next_generation(words, err, islands, pop, width, nvars, mc, 77, steps, ops)
+    cpu_s = time.perf_counter() - t0
+    same = bool(np.array_equal(out[0], ref[0]) and np.array_equal(out[3], ref[3]))
+    ev.close()
+    n = float(n)
+    per = float(np.mean(dev_ms)) / 1e3
+    return {"metric": "children_per_s", "value": n / per, "unit": "children/s",
+            "e2e": n * steps / sum(wall), "ms_per_step": 1e3 * per, "launches": launches,
+            "h2d": int(err.nbytes), "d2h": int(n * (2 + 2 + 8 + 8 + 4 * width)),
+            "same_as_cpu": same,
+            "cpu_baseline": {"value": n / cpu_s, "unit": "children/s", "cores": 1,
+                             "kind": "port",
+                             "sample": "the last timed generation, CPU restatement of the "
+                                       "reference engine (sequential, as the reference)"},
+            "config": f"device variation, {islands} islands x {pop} slots, width {width}, "
+                      f"max complexity {mc}, {nvars} inputs, default operator set, dedup on"}
+
+
 def fit_roofline(r, peaks):
     per = float(np.mean(r["dev_ms"])) / 1e3
     achieved = r["lane_ops"] / per / 1e9
@@ -518,7 +577,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="score",
-                    choices=["score", "fit", "rank", "implicit", "c5"])
+                    choices=["score", "fit", "rank", "implicit", "c5", "vary"])
     ap.add_argument("--P", type=int, default=0)
     ap.add_argument("--N", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -547,9 +606,14 @@ def main():
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    if args.workload in ("rank", "implicit", "c5"):
+    if args.workload in ("rank", "implicit", "c5", "vary"):
         # one-GPU stages: each rank measures its own copy; rank 0 reports
-        if args.workload == "rank":
+        if args.workload == "vary":
+            r = bench_vary(args, rank, pkg, flushbuf, args.steps, args.warmup)
+            line = single_gpu_line(args, world, r, r["metric"], r["unit"], r.pop("config"),
+                                   {"dtype": "u32 words, integer", "cpu_baseline": r["cpu_baseline"],
+                                    "same_as_cpu": r["same_as_cpu"]})
+        elif args.workload == "rank":
             r = bench_rank(args, rank, pkg, W, flushbuf, args.steps, args.warmup)
             line = single_gpu_line(args, world, r, r["metric"], r["unit"], r.pop("config"),
                                    {"dtype": "f64 eval, integer sums"})
@@ -656,6 +720,7 @@ def main():
             line["implicit"] = {"score": score, "fit": fit_summary(fit, peaks, what)}
             fit, what, rk = bench_c5(args, rank, pkg, W, flushbuf, 3, 3, 1, 1)
             line["c5"] = {"absolute_fit": fit_summary(fit, peaks, what), "rank": rk}
+            line["vary"] = bench_vary(args, rank, pkg, flushbuf, 5, 3)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

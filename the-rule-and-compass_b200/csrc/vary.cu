@@ -28,7 +28,7 @@
 #include "rc_internal.h"
 #include "vary_gen.cuh"
 
-#define RV_K 2   /* attempts per slot computed on the device */
+#define RV_K 3   /* attempts per slot computed on the device */
 #define RV_T 128
 
 namespace {
