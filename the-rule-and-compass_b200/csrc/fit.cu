@@ -1585,58 +1585,96 @@ __global__ void __launch_bounds__(32) ft_grad4_kernel(FitArgs a, int row0, int n
     }
 }
 
-/* Implicit score per (candidate, tile of rows): partial sums of w * d and w. */
-template <int T>
-__global__ void __launch_bounds__(T) ft_implicit_score_kernel(FitArgs a, int ntiles,
-                                                               int rows_per_tile,
-                                                               double *partial, int *bad)
+/* Implicit score per (candidate, tile of rows) on the four-row stack
+   machine: each thread carries NR rows through the forward sweep (partials
+   on input paths kept) and the input-adjoint reverse sweep (fi_reverse_x),
+   then d = |f| / ||grad_x f|| per row (implicit.rs:68-104, the zero-gradient
+   guard included); partial sums of w * d and w. A row with a non-finite
+   weight, value, gradient or distance marks the candidate bad. */
+template <int T, int NR>
+__global__ void __launch_bounds__(T) ft_implicit_score_x(
+    const FIns *__restrict__ fins, const int *__restrict__ fins_off, const int4 *__restrict__ info,
+    const int *__restrict__ valid, const double *__restrict__ c, int kmax,
+    const float *__restrict__ cols, int npad, int n, int v, const double *__restrict__ w,
+    int ntiles, int rows_per_tile, int maxins, int slots, int ntape, double *partial, int *bad)
 {
+    using F = FiV<float, NR>;
+    using V4 = typename F::V4;
     extern __shared__ __align__(16) unsigned char smem[];
     const int cand = blockIdx.x / ntiles;
     const int tile = blockIdx.x % ntiles;
     const int tid = threadIdx.x;
-    uint4 *rec = reinterpret_cast<uint4 *>(smem);
-    float *cf = reinterpret_cast<float *>(rec + a.mmax);
-    float *tape = cf + FT_MAX_CONST;
-    float *ig = tape + (size_t)a.mmax * T;
-    double *red = reinterpret_cast<double *>(ig + (size_t)a.v * T);
-    const int nb = a.node_off[cand];
-    const int m = a.node_off[cand + 1] - nb;
-    const int p = a.pcount[cand];
-    for (int i = tid; i < m; i += T) rec[i] = a.rec[nb + i];
-    if (tid < p) cf[tid] = (float)a.c0[(size_t)cand * a.kmax + tid];
-    __syncthreads();
+    FIns *ins = reinterpret_cast<FIns *>(smem);
+    float *cf = reinterpret_cast<float *>(smem + 8 * (size_t)((maxins + 1) & ~1));
+    V4 *stk = reinterpret_cast<V4 *>(cf + FT_MAX_CONST);
+    V4 *tape = stk + (size_t)(slots > 0 ? slots : 1) * T;
+    V4 *ig = tape + (size_t)(ntape > 0 ? ntape : 1) * T;
+    double *red = reinterpret_cast<double *>(ig + (size_t)v * T);
+    int isbad = !valid[cand];
     double sum = 0.0, wsum = 0.0;
-    int isbad = !a.valid[cand];
     const int r0 = tile * rows_per_tile;
-    const int r1 = min(a.n, r0 + rows_per_tile);
+    const int r1 = min(n, r0 + rows_per_tile);
     if (!isbad) {
-        for (int row = r0 + tid; row < r1; row += T) {
-            const double wr = a.w ? a.w[row] : 1.0;
-            if (!isfinite(wr) || wr < 0.0) {
+        const int4 in4 = info[cand];
+        const int nf = in4.x, nr = in4.y;
+        const int ib = fins_off[cand];
+        for (int i = tid; i < nf + nr; i += T) ins[i] = fins[ib + i];
+        if (tid < kmax) cf[tid] = (float)c[(size_t)cand * kmax + tid];
+        __syncthreads();
+        for (int row = r0 + NR * tid; row < r1; row += NR * T) {
+            float pr[NR];
+            fi_forward<float, NR, true>(ins, cf, cols, npad, row, stk, tape, T, tid, pr);
+            for (int k = 0; k < v; ++k) {
+                float z[NR];
+#pragma unroll
+                for (int i = 0; i < NR; ++i) z[i] = 0.0f;
+                ig[k * T + tid] = F::pack(z);
+            }
+            float a[NR];
+#pragma unroll
+            for (int i = 0; i < NR; ++i) a[i] = 1.0f;
+            fi_reverse_x<float, NR>(ins + nf, nr, stk, tape, T, tid, ig, a);
+            double nsq[NR];
+            bool gfin[NR];
+#pragma unroll
+            for (int i = 0; i < NR; ++i) {
+                nsq[i] = 0.0;
+                gfin[i] = true;
+            }
+            for (int k = 0; k < v; ++k) {
+                float g[NR];
+                F::unpack(ig[k * T + tid], g);
+#pragma unroll
+                for (int i = 0; i < NR; ++i) {
+                    gfin[i] = gfin[i] && isfinite(g[i]);
+                    nsq[i] += (double)g[i] * (double)g[i];
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < NR; ++i) {
+                const int rr = row + i;
+                if (rr >= r1) continue;
+                const double wr = w ? w[rr] : 1.0;
+                if (!isfinite(wr) || wr < 0.0) {
+                    isbad = 1;
+                    continue;
+                }
+                if (wr == 0.0) continue;
+                const double norm = sqrt(nsq[i]);
+                const bool ok = isfinite(pr[i]) && gfin[i] && isfinite(norm) && norm > 0.0;
+                const double d = ok ? fabs((double)pr[i]) / norm : 0.0;
+                if (!ok || !isfinite(d)) {
+                    isbad = 1;
+                    continue;
+                }
+                sum += wr * d;
+                wsum += wr;
+            }
+            /* an infeasible candidate's sums are not read: stop its rows */
+            if (__any_sync(0xffffffffu, isbad) || *((volatile int *)(bad + cand))) {
                 isbad = 1;
-                continue;
+                break;
             }
-            if (wr == 0.0) continue;
-            const float fv = ft_fwd_f<T>(rec, m, a.cols, a.npad, row, cf, tape + tid);
-            for (int k = 0; k < a.v; ++k) ig[k * T + tid] = 0.0f;
-            ft_bwd_f<T>(rec, m, tape + tid, nullptr, 0, ig + tid, T);
-            double nsq = 0.0;
-            bool ok = isfinite(fv);
-            for (int k = 0; k < a.v; ++k) {
-                const double gk = (double)ig[k * T + tid];
-                if (!isfinite(gk)) ok = false;
-                nsq += gk * gk;
-            }
-            const double norm = sqrt(nsq);
-            if (!(isfinite(norm) && norm > 0.0)) ok = false;
-            const double d = ok ? fabs((double)fv) / norm : 0.0;
-            if (!ok || !isfinite(d)) {
-                isbad = 1;
-                continue;
-            }
-            sum += wr * d;
-            wsum += wr;
         }
     }
     const int anybad = __syncthreads_or(isbad);
@@ -2291,18 +2329,42 @@ float rc_implicit_score_batch(void *ctx, const unsigned int *prog, const unsigne
     RcCtx *rc = (RcCtx *)ctx;
     if (!rc || !prog || !off || !pcount || !c || !out || !status) return -1.0f;
     if (nprog <= 0 || kmax <= 0 || kmax > FT_MAX_CONST || rc->n <= 0) return -1.0f;
+    if (rc->v > FT_IMPLICIT_MAXV) return -1.0f;
     RcStats *st = &rc->stats;
     FitPrep b;
     prep_batch(off, prog, pcount, nprog, rc->v, b);
-    const int mmax = b.mmax;
+    /* the input-mode translation: partials and pruning along input paths */
+    std::vector<FIns> xfins, fwd, rev;
+    std::vector<int> xoff(nprog + 1, 0);
+    std::vector<int4> xinfo(nprog, make_int4(0, 0, 0, 0));
+    int slots = 1, ntape = 1, maxins = 2;
+    for (int i = 0; i < nprog; ++i) {
+        xoff[i] = (int)xfins.size();
+        if (!b.valid[i]) continue;
+        int ns = 0, nt = 0;
+        const int m = b.node_off[i + 1] - b.node_off[i];
+        if (!fi_decode(prog + off[i], m, fwd, rev, &ns, &nt, nullptr, nullptr, true) ||
+            ns > 0xffff || nt > 0x7fff) {
+            b.valid[i] = 0;
+            continue;
+        }
+        xfins.insert(xfins.end(), fwd.begin(), fwd.end());
+        xfins.insert(xfins.end(), rev.begin(), rev.end());
+        xinfo[i] = make_int4((int)fwd.size(), (int)rev.size(), ns, nt);
+        slots = std::max(slots, ns);
+        ntape = std::max(ntape, nt);
+        maxins = std::max(maxins, (int)(fwd.size() + rev.size()));
+    }
+    xoff[nprog] = (int)xfins.size();
+    if (xfins.empty()) xfins.resize(1);
     const int T = 128;
+    constexpr int NR = 2;
     const int rows_per_tile = 16384;
     const int ntiles = (rc->n + rows_per_tile - 1) / rows_per_tile;
-    const size_t words = off[nprog];
     size_t cur = 0;
-    const size_t o_rec = rc_take(&cur, sizeof(uint32_t) * words);
-    const size_t o_noff = rc_take(&cur, sizeof(int) * (nprog + 1));
-    const size_t o_p = rc_take(&cur, sizeof(int) * nprog);
+    const size_t o_fins = rc_take(&cur, sizeof(FIns) * xfins.size());
+    const size_t o_xoff = rc_take(&cur, sizeof(int) * (nprog + 1));
+    const size_t o_info = rc_take(&cur, sizeof(int4) * nprog);
     const size_t o_c = rc_take(&cur, sizeof(double) * (size_t)nprog * kmax);
     const size_t o_valid = rc_take(&cur, sizeof(int) * nprog);
     const size_t in_end = rc_take(&cur, 0);
@@ -2315,41 +2377,31 @@ float rc_implicit_score_batch(void *ctx, const unsigned int *prog, const unsigne
     if (rc_reserve(rc, dev_end, io_end) != 0) return -1.0f;
     unsigned char *dev = rc->dev, *host = rc->host;
     double t = rc_now_ms();
-    memcpy(host + o_rec, prog, sizeof(uint32_t) * words);
-    memcpy(host + o_noff, b.node_off.data(), sizeof(int) * (nprog + 1));
-    memcpy(host + o_p, pcount, sizeof(int) * nprog);
+    memcpy(host + o_fins, xfins.data(), sizeof(FIns) * xfins.size());
+    memcpy(host + o_xoff, xoff.data(), sizeof(int) * (nprog + 1));
+    memcpy(host + o_info, xinfo.data(), sizeof(int4) * nprog);
     memcpy(host + o_c, c, sizeof(double) * (size_t)nprog * kmax);
     memcpy(host + o_valid, b.valid.data(), sizeof(int) * nprog);
     cudaMemcpyAsync(dev, host, in_end, cudaMemcpyHostToDevice, rc->s);
     cudaMemsetAsync(dev + o_bad, 0, sizeof(int) * nprog, rc->s);
     st->h2d_ms += rc_now_ms() - t;
-    FitArgs a;
-    memset(&a, 0, sizeof(a));
-    a.cols = rc->d_cols;
-    a.w = rc->d_w64;
-    a.n = rc->n;
-    a.npad = rc->npad;
-    a.v = rc->v;
-    a.rec = reinterpret_cast<const uint4 *>(dev + o_rec);
-    a.node_off = reinterpret_cast<const int *>(dev + o_noff);
-    a.pcount = reinterpret_cast<const int *>(dev + o_p);
-    a.kmax = kmax;
-    a.c0 = reinterpret_cast<const double *>(dev + o_c);
-    a.valid = reinterpret_cast<const int *>(dev + o_valid);
-    a.mmax = mmax;
-    const size_t smem = sizeof(uint4) * mmax + sizeof(float) * FT_MAX_CONST +
-                        sizeof(float) * (size_t)mmax * T + sizeof(float) * (size_t)rc->v * T +
-                        sizeof(double) * T + 64;
-    if (cudaFuncSetAttribute(ft_implicit_score_kernel<128>,
+    using V4 = FiV<float, NR>::V4;
+    const size_t smem = 8 * (size_t)((maxins + 1) & ~1) + sizeof(float) * FT_MAX_CONST +
+                        sizeof(V4) * (size_t)(slots + ntape + rc->v) * T + sizeof(double) * T;
+    if (smem > 48 * 1024 &&
+        cudaFuncSetAttribute(ft_implicit_score_x<128, NR>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
         cudaGetLastError();
         return -1.0f;
     }
     cudaEventRecord(rc->t0, rc->s);
     rc->launches += 2;
-    ft_implicit_score_kernel<128><<<nprog * ntiles, T, smem, rc->s>>>(
-        a, ntiles, rows_per_tile, reinterpret_cast<double *>(dev + o_part),
-        reinterpret_cast<int *>(dev + o_bad));
+    ft_implicit_score_x<128, NR><<<nprog * ntiles, T, smem, rc->s>>>(
+        reinterpret_cast<const FIns *>(dev + o_fins), reinterpret_cast<const int *>(dev + o_xoff),
+        reinterpret_cast<const int4 *>(dev + o_info), reinterpret_cast<const int *>(dev + o_valid),
+        reinterpret_cast<const double *>(dev + o_c), kmax, rc->d_cols, rc->npad, rc->n, rc->v,
+        rc->d_w64, ntiles, rows_per_tile, maxins, slots, ntape,
+        reinterpret_cast<double *>(dev + o_part), reinterpret_cast<int *>(dev + o_bad));
     ft_implicit_finalize<<<(nprog + 127) / 128, 128, 0, rc->s>>>(
         nprog, ntiles, reinterpret_cast<const double *>(dev + o_part),
         reinterpret_cast<const int *>(dev + o_bad), reinterpret_cast<double *>(dev + o_out),

@@ -71,11 +71,19 @@ __host__ __device__ constexpr bool fi_nonlinear(unsigned op)
    subtree of two or more instructions is replaced by one push of a cached
    column (its values over all rows do not depend on the constants, so they
    are computed once per fit), and in `subs` the records of each such
-   subtree, renumbered as a program of its own, in cache-column order. */
+   subtree, renumbered as a program of its own, in cache-column order.
+
+   With `inputs`, the lists differentiate with respect to the inputs instead
+   of the constants: the partials kept and the subtrees pruned are those on
+   and off paths from an input leaf, a pruned left operand is restored by a
+   push of kind FI_PUSH_CACHE, and the reverse sweep's input leaves (pushes
+   and fused operands of kind FI_PUSH_VAR / FI_BIN_V) add their adjoints to
+   the input's gradient (fi_reverse_x). No cached list is made. */
 inline bool fi_decode(const uint32_t *rec, int m, std::vector<FIns> &fwd, std::vector<FIns> &rev,
                       int *nslots, int *ntape, std::vector<FIns> *fwdc = nullptr,
-                      std::vector<std::vector<uint32_t>> *subs = nullptr)
+                      std::vector<std::vector<uint32_t>> *subs = nullptr, bool inputs = false)
 {
+    const uint32_t leaf_op = inputs ? OP_VAR : OP_CONST;
     struct Ent {
         int rec, first;
         bool hp;
@@ -105,10 +113,10 @@ inline bool fi_decode(const uint32_t *rec, int m, std::vector<FIns> &fwd, std::v
                 maxslot = maxslot > depth - 1 ? maxslot : depth - 1;
             }
             ++depth;
-            hp[i] = op == OP_CONST;
+            hp[i] = op == leaf_op;
             first_rec[i] = i;
             lo[i] = (int)fwd.size();
-            stack.push_back({i, (int)fwd.size(), op == OP_CONST});
+            stack.push_back({i, (int)fwd.size(), op == leaf_op});
             fwd.push_back(in);
             hi[i] = lo[i];
         } else if (ft_op_binary(op)) {
@@ -196,7 +204,7 @@ inline bool fi_decode(const uint32_t *rec, int m, std::vector<FIns> &fwd, std::v
             if (skip_to[j] >= 0) {
                 if (emit[j]) {
                     FIns r = fwd[j];
-                    r.kind = FI_PUSH_VAR;
+                    r.kind = inputs ? FI_PUSH_CACHE : FI_PUSH_VAR;
                     rev.push_back(r);
                 }
                 j = skip_to[j] + 1;
@@ -215,6 +223,7 @@ inline bool fi_decode(const uint32_t *rec, int m, std::vector<FIns> &fwd, std::v
             seen[rev[j].imm] = 1;
         }
     }
+    if (inputs) return true;
     if (fwdc) {
         /* cacheable: constant-free, its own instructions (not a fused leaf),
            two or more of them, and its parent has a constant (or it is the
@@ -582,6 +591,96 @@ __device__ __forceinline__ bool fi_reverse(const FIns *__restrict__ rev, int nr,
         }
     }
     return fin;
+}
+
+/* Reverse sweep of the thread's rows over an input-mode reverse list (see
+   fi_decode): the same stack machine as fi_reverse, seeded with a[], whose
+   input leaves add their adjoints to the thread's gradient rows
+   ig[col * S + tid] (zeroed by the caller). Constants receive nothing. */
+template <typename V, int NR>
+__device__ __forceinline__ void fi_reverse_x(const FIns *__restrict__ rev, int nr,
+                                             typename FiV<V, NR>::V4 *stk,
+                                             const typename FiV<V, NR>::V4 *tape, int S, int tid,
+                                             typename FiV<V, NR>::V4 *ig, V *a)
+{
+    using F = FiV<V, NR>;
+    for (int pc = nr - 1; pc >= 0; --pc) {
+        const FIns in = rev[pc];
+        const unsigned kind = in.kind;
+        const unsigned k = kind & FI_KIND_MASK;
+        if (k <= FI_PUSH_CACHE) {
+            if (k == FI_PUSH_VAR) {
+                V gv[NR];
+                F::unpack(ig[in.imm * S + tid], gv);
+#pragma unroll
+                for (int i = 0; i < NR; ++i) gv[i] += a[i];
+                ig[in.imm * S + tid] = F::pack(gv);
+            }
+            if (in.spill != 0xff) F::unpack(stk[in.spill * S + tid], a);
+            continue;
+        }
+        if (k == FI_UNARY) {
+            if (in.op == OP_NEG) {
+#pragma unroll
+                for (int i = 0; i < NR; ++i) a[i] = -a[i];
+            } else {
+                V d[NR];
+                F::unpack(tape[in.tape * S + tid], d);
+#pragma unroll
+                for (int i = 0; i < NR; ++i) a[i] = fi_child(a[i], d[i]);
+            }
+            continue;
+        }
+        V l[NR], r[NR];
+        if (in.op == OP_ADD || in.op == OP_SUB) {
+            const bool sub = in.op == OP_SUB;
+#pragma unroll
+            for (int i = 0; i < NR; ++i) {
+                l[i] = a[i];
+                r[i] = sub ? -a[i] : a[i];
+            }
+        } else {
+            int ts = in.tape;
+#pragma unroll
+            for (int i = 0; i < NR; ++i) l[i] = r[i] = V(0);
+            if (kind & FI_HP_L) {
+                V d[NR];
+                F::unpack(tape[ts * S + tid], d);
+#pragma unroll
+                for (int i = 0; i < NR; ++i) l[i] = fi_child(a[i], d[i]);
+                ++ts;
+            }
+            if (kind & FI_HP_R) {
+                V d[NR];
+                F::unpack(tape[ts * S + tid], d);
+#pragma unroll
+                for (int i = 0; i < NR; ++i) r[i] = fi_child(a[i], d[i]);
+            }
+        }
+        if (k == FI_BIN_S) {
+            if ((kind & FI_HP_L) && (kind & FI_HP_R)) {
+                stk[in.arg * S + tid] = F::pack(l);
+#pragma unroll
+                for (int i = 0; i < NR; ++i) a[i] = r[i];
+            } else if (kind & FI_HP_R) {
+#pragma unroll
+                for (int i = 0; i < NR; ++i) a[i] = r[i];
+            } else {
+#pragma unroll
+                for (int i = 0; i < NR; ++i) a[i] = l[i];
+            }
+        } else {
+            if (k == FI_BIN_V) {
+                V gv[NR];
+                F::unpack(ig[in.imm * S + tid], gv);
+#pragma unroll
+                for (int i = 0; i < NR; ++i) gv[i] += r[i];
+                ig[in.imm * S + tid] = F::pack(gv);
+            }
+#pragma unroll
+            for (int i = 0; i < NR; ++i) a[i] = l[i];
+        }
+    }
 }
 
 /* D = A * B + D for one 8x8x4 f64 tile (mma.sync; A row-major, B
