@@ -149,13 +149,16 @@ __host__ __device__ inline size_t ft_rows_bytes(int Wmax, int T)
     return rows > part ? rows : part;
 }
 
-/* Dynamic shared memory of a sweep kernel: records, constants (f64 and f32),
-   the tape (f32 [node][T], or f64 [node][T/2]), the Jacobian row buffer for
-   the assembling kinds, and a reduction buffer. */
+/* Threads of the implicit sweeps: every thread carries one row. */
+#define FT_ITHREADS 64
+
+/* Dynamic shared memory of an implicit sweep kernel: records, constants
+   (f64 and f32), the f64 tape ([node][T]; two for the Jacobian), the
+   Jacobian row buffer for the assembling kind, and a reduction buffer. */
 __host__ __device__ inline size_t ft_sweep_smem(int opk, int mmax, int Wmax, int T)
 {
     size_t s = 16 * (size_t)mmax + 16 * FT_MAX_CONST +
-               4 * (size_t)mmax * T * (opk == FOP_IJAC ? 2 : 1);
+               8 * (size_t)mmax * T * (opk == FOP_IJAC ? 2 : 1);
     if (ft_op_assembles(opk)) s += ft_rows_bytes(Wmax, T);
     return s + 8 * (size_t)T;
 }
@@ -191,7 +194,7 @@ __device__ void ft_tile_implicit(const FitArgs &a, const uint4 *rec, int m, int 
                                  const double *cd, double *tape64, double *tan64, double *rows,
                                  double *red, int r0, int r1, double *pt)
 {
-    constexpr int TS = T / 2;
+    constexpr int TS = T;
     const int tid = threadIdx.x;
     const int W = 4 * ((p + 1 + 3) / 4);
     const Syrk sy = ft_syrk_setup<T>(W);
@@ -255,8 +258,8 @@ __global__ void __launch_bounds__(T) ft_sweep(FitArgs a, int q)
     float *cf = reinterpret_cast<float *>(cd + FT_MAX_CONST);
     float *tape = cf + 2 * FT_MAX_CONST;
     double *tape64 = reinterpret_cast<double *>(tape);
-    double *tan64 = reinterpret_cast<double *>(tape + (size_t)a.mmax * T);
-    double *rows = reinterpret_cast<double *>(tape + (size_t)a.mmax * T * (OPK == FOP_IJAC ? 2 : 1));
+    double *tan64 = tape64 + (size_t)a.mmax * T;
+    double *rows = tape64 + (size_t)a.mmax * T * (OPK == FOP_IJAC ? 2 : 1);
     double *red = rows + (ft_op_assembles(OPK) ? ft_rows_bytes(a.Wmax, T) / 8 : 0);
     __shared__ int s_item;
     const int tid = threadIdx.x;
@@ -1895,12 +1898,12 @@ template <int OPK>
 SweepLaunch sweep_launch(RcCtx *c, int mmax, int Wmax)
 {
     SweepLaunch s;
-    s.fn = (const void *)ft_sweep<OPK, FT_THREADS>;
-    s.smem = ft_sweep_smem(OPK, mmax, Wmax, FT_THREADS);
+    s.fn = (const void *)ft_sweep<OPK, FT_ITHREADS>;
+    s.smem = ft_sweep_smem(OPK, mmax, Wmax, FT_ITHREADS);
     if (s.smem > 48 * 1024)
         cudaFuncSetAttribute(s.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
-    s.grid = c->sm_count * occupancy(s.fn, FT_THREADS, s.smem);
-    s.threads = FT_THREADS;
+    s.grid = c->sm_count * occupancy(s.fn, FT_ITHREADS, s.smem);
+    s.threads = FT_ITHREADS;
     return s;
 }
 
