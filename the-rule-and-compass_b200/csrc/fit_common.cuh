@@ -53,26 +53,6 @@ __device__ __forceinline__ float ft_fwd_f(const uint4 *rec, int m, const float *
     return val;
 }
 
-/* f64 forward sweep; `tp` has stride TS. */
-template <int TS>
-__device__ __forceinline__ double ft_fwd_d(const uint4 *rec, int m, const double *cols, int npad,
-                                           int row, const double *c, double *tp)
-{
-    double val = 0.0;
-    for (int i = 0; i < m; ++i) {
-        const uint4 r = rec[i];
-        if (r.x == OP_CONST) val = c[r.w];
-        else if (r.x == OP_VAR) val = __ldg(cols + (size_t)r.w * npad + row);
-        else {
-            const double a = tp[r.y * TS];
-            const double b = ft_op_binary(r.x) ? tp[r.z * TS] : 0.0;
-            val = ft_value_d(r.x, a, b);
-        }
-        tp[i * TS] = val;
-    }
-    return val;
-}
-
 /* f64 forward with the row's inputs given explicitly (implicit metric). */
 template <int TS>
 __device__ __forceinline__ double ft_fwd_d_x(const uint4 *rec, int m, const double *x,
