@@ -143,6 +143,17 @@ def postfix_ops(prog, off):
 # CPU baseline: the oracle on a bounded sample, parallel over candidates.
 # ---------------------------------------------------------------------------
 
+def cpu_model():
+    """The host CPU's model name (Linux /proc/cpuinfo), or None."""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def cpu_score_baseline(trees, x, y, n_rows, n_cand, threads):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
@@ -216,7 +227,7 @@ def run_reference(args, rank, world):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": cfg,
             "cpu_baseline": {"value": value, "unit": unit, "cores": threads, "kind": "port",
-                             "sample": sample},
+                             "cpu_model": cpu_model(), "sample": sample},
             "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -700,13 +711,17 @@ def main():
             threads = os.cpu_count() or 1
             if args.workload == "score":
                 v, dt = cpu_score_baseline(r["trees"], r["x"], r["y"], 1 << 16, 64, threads)
+                v1, _ = cpu_score_baseline(r["trees"], r["x"], r["y"], 1 << 16, 8, 1)
                 line["cpu_baseline"] = {"value": v, "unit": unit, "cores": threads,
-                                        "kind": "port",
-                                        "sample": "64 programs x 65536 rows, f64 oracle"}
+                                        "kind": "port", "cpu_model": cpu_model(),
+                                        "value_1_thread": v1,
+                                        "sample": "64 programs x 65536 rows, f64 oracle "
+                                                  "(single thread: 8 programs)"}
             else:
                 v, dt = cpu_fit_baseline(r["trees"], r["x"], r["y"], 1 << 14, 16, 20, threads)
                 line["cpu_baseline"] = {"value": v * (1 << 14) / r["N"], "unit": unit,
                                         "cores": threads, "kind": "port",
+                                        "cpu_model": cpu_model(),
                                         "sample": "16 candidates x 16384 rows x 20 iters, "
                                                   "scaled linearly in rows"}
         if args.workload == "score" and world == 1 and not args.no_secondary:
