@@ -112,6 +112,10 @@ struct FitArgs {
     const int *sub_col;    /* [nsub] */
     int nsub;
     int sub_slots, sub_maxins;
+    const FIns *xfins;     /* implicit metric: input-mode lists [forward | reverse] */
+    const int *xfins_off;  /* [P + 1] */
+    const int4 *xinfo;     /* forward count, reverse count, spill slots, tape slots */
+    int xmaxins, xslots, xtape;
     int iters, metric, flags;
     int ntiles;
     int mmax;
@@ -248,11 +252,110 @@ __device__ void ft_tile_implicit(const FitArgs &a, const uint4 *rec, int m, int 
     }
 }
 
+/* The implicit cost of one tile, sum w d^2 with d = f / ||grad_x f||
+   (implicit.rs:156-174), on the stack machine: f64, one row per thread, the
+   forward sweep keeping partials on input paths and the input-adjoint
+   reverse sweep (fi_reverse_x). Row for row the same values, checks and
+   summation order as ft_implicit_d over the records. */
+template <int T>
+__device__ void ft_tile_icost_x(const FitArgs &a, const FIns *fwd, int nf, int nr,
+                                const double *cd, FiV<double, 1>::V4 *stk,
+                                FiV<double, 1>::V4 *tape, FiV<double, 1>::V4 *ig, double *red,
+                                int r0, int r1, double *pt)
+{
+    const int tid = threadIdx.x;
+    double cost = 0.0;
+    int bad = 0;
+    for (int base = r0; base < r1; base += T) {
+        const int row = base + tid;
+        double fv;
+        fi_forward<double, 1, true>(fwd, cd, a.cols64, a.npad, row, stk, tape, T, tid, &fv);
+        if (row >= r1) continue;
+        const double wr = a.w ? a.w[row] : 1.0;
+        if (!(isfinite(wr) && wr >= 0.0)) {
+            bad = 1;
+            continue;
+        }
+        if (wr == 0.0) continue;
+        if (!isfinite(fv)) {
+            bad = 1;
+            continue;
+        }
+        for (int k = 0; k < a.v; ++k) ig[k * T + tid].v[0] = 0.0;
+        double seed = 1.0;
+        fi_reverse_x<double, 1>(fwd + nf, nr, stk, tape, T, tid, ig, &seed);
+        double nsq = 0.0;
+        bool ok = true;
+        for (int k = 0; k < a.v; ++k) {
+            const double g = ig[k * T + tid].v[0];
+            if (!isfinite(g)) ok = false;
+            nsq += g * g;
+        }
+        const double norm = sqrt(nsq);
+        if (!ok || !(isfinite(norm) && norm > 0.0)) {
+            bad = 1;
+            continue;
+        }
+        const double d = fv / norm;
+        if (!isfinite(d)) {
+            bad = 1;
+            continue;
+        }
+        const double r = sqrt(wr) * d;
+        cost += r * r;
+    }
+    bad = __syncthreads_or(bad);
+    cost = ft_block_sum<T>(cost, red);
+    if (tid == 0) {
+        pt[FT_PART_LOSS] = cost;
+        pt[FT_PART_BAD] = bad ? 1.0 : 0.0;
+        pt[FT_PART_SKIP] = 0.0;
+    }
+}
+
 /* One sweep kind over every queued (candidate, tile) item of step parity q. */
 template <int OPK, int T>
 __global__ void __launch_bounds__(T) ft_sweep(FitArgs a, int q)
 {
     extern __shared__ __align__(16) unsigned char sm[];
+    if constexpr (OPK == FOP_ICOST) {
+        /* [instructions | constants | spill slots | tape | input gradients | reduction] */
+        using V4 = FiV<double, 1>::V4;
+        FIns *ins = reinterpret_cast<FIns *>(sm);
+        double *cd = reinterpret_cast<double *>(sm + 8 * (size_t)((a.xmaxins + 1) & ~1));
+        V4 *stk = reinterpret_cast<V4 *>(cd + FT_MAX_CONST);
+        V4 *tape = stk + (size_t)a.xslots * T;
+        V4 *ig = tape + (size_t)a.xtape * T;
+        double *red = reinterpret_cast<double *>(ig + (size_t)a.v * T);
+        __shared__ int s_item;
+        const int tid = threadIdx.x;
+        const int *list = a.lists + ((size_t)q * FOP_COUNT + OPK) * a.nprog;
+        const int total = a.counts[q * FOP_COUNT + OPK] * a.ntiles;
+        int *work = a.work + q * FOP_COUNT + OPK;
+        for (;;) {
+            if (tid == 0) s_item = atomicAdd(work, 1);
+            __syncthreads();
+            const int item = s_item;
+            __syncthreads();
+            if (item >= total) break;
+            const int cand = list[item / a.ntiles];
+            const int tile = item % a.ntiles;
+            const FitState *st = a.state + cand;
+            const int4 info = a.xinfo[cand];
+            const int ib = a.xfins_off[cand];
+            const int p = a.pcount[cand];
+            const int sel = st->sel;
+            for (int i = tid; i < info.x + info.y; i += T) ins[i] = a.xfins[ib + i];
+            if (tid < p) cd[tid] = sel ? st->trial[tid] : st->c[tid];
+            __syncthreads();
+            const int r0 = tile * FT_TILE_ROWS;
+            const int r1 = min(a.n, r0 + FT_TILE_ROWS);
+            double *pt = a.part + ((size_t)cand * a.ntiles + tile) * FT_PART_STRIDE;
+            ft_tile_icost_x<T>(a, ins, info.x, info.y, cd, stk, tape, ig, red, r0, r1, pt);
+            __syncthreads();
+        }
+        return;
+    }
     uint4 *rec = reinterpret_cast<uint4 *>(sm);
     double *cd = reinterpret_cast<double *>(sm + 16 * (size_t)a.mmax);
     float *cf = reinterpret_cast<float *>(cd + FT_MAX_CONST);
@@ -1894,6 +1997,58 @@ struct SweepLaunch {
     int threads;
 };
 
+/* Input-mode translation (fi_decode with `inputs`) of every valid candidate:
+   [forward | reverse] per candidate, counts and slot sizes in info. A
+   candidate it cannot translate becomes invalid. */
+struct XPrep {
+    std::vector<FIns> fins;
+    std::vector<int> off;
+    std::vector<int4> info;
+    int slots = 1, tape = 1, maxins = 2;
+};
+
+void prep_inputs(const unsigned int *off, const unsigned int *prog, int nprog,
+                 const std::vector<int> &node_off, std::vector<int> &valid, XPrep &x)
+{
+    std::vector<FIns> fwd, rev;
+    x.fins.clear();
+    x.off.assign(nprog + 1, 0);
+    x.info.assign(nprog, make_int4(0, 0, 0, 0));
+    for (int i = 0; i < nprog; ++i) {
+        x.off[i] = (int)x.fins.size();
+        if (!valid[i]) continue;
+        int ns = 0, nt = 0;
+        const int m = node_off[i + 1] - node_off[i];
+        if (!fi_decode(prog + off[i], m, fwd, rev, &ns, &nt, nullptr, nullptr, true) ||
+            ns > 0xffff || nt > 0x7fff) {
+            valid[i] = 0;
+            continue;
+        }
+        x.fins.insert(x.fins.end(), fwd.begin(), fwd.end());
+        x.fins.insert(x.fins.end(), rev.begin(), rev.end());
+        x.info[i] = make_int4((int)fwd.size(), (int)rev.size(), ns, nt);
+        x.slots = std::max(x.slots, ns);
+        x.tape = std::max(x.tape, nt);
+        x.maxins = std::max(x.maxins, (int)(fwd.size() + rev.size()));
+    }
+    x.off[nprog] = (int)x.fins.size();
+    if (x.fins.empty()) x.fins.resize(1);
+}
+
+/* The implicit cost sweep on the stack machine. */
+SweepLaunch icost_launch(RcCtx *c, const XPrep &x)
+{
+    SweepLaunch s;
+    s.fn = (const void *)ft_sweep<FOP_ICOST, FT_ITHREADS>;
+    s.smem = 8 * (size_t)((x.maxins + 1) & ~1) + 8 * FT_MAX_CONST +
+             8 * (size_t)FT_ITHREADS * (x.slots + x.tape + c->v) + 8 * (size_t)FT_ITHREADS;
+    if (s.smem > 48 * 1024)
+        cudaFuncSetAttribute(s.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
+    s.grid = c->sm_count * occupancy(s.fn, FT_ITHREADS, s.smem);
+    s.threads = FT_ITHREADS;
+    return s;
+}
+
 template <int OPK>
 SweepLaunch sweep_launch(RcCtx *c, int mmax, int Wmax)
 {
@@ -1979,6 +2134,9 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     const bool use_cache = metric != FM_IMPLICIT;
     prep_batch(off, prog, pcount, nprog, c->v, b, corr ? 2 : 0,
                use_cache ? sizeof(float) * (size_t)c->npad : 0, cache_cap);
+    XPrep xp;
+    if (metric == FM_IMPLICIT) prep_inputs(off, prog, nprog, b.node_off, b.valid, xp);
+    else xp.fins.resize(1);
     const int ntiles = (c->n + FT_TILE_ROWS - 1) / FT_TILE_ROWS;
     const int Wmax = 4 * ((b.pmax + 1 + 3) / 4);
     const size_t words = off[nprog];
@@ -1996,6 +2154,9 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     const size_t o_subf = rc_take(&cur, sizeof(FIns) * b.sub_fins.size());
     const size_t o_suboff = rc_take(&cur, sizeof(int) * b.sub_off.size());
     const size_t o_subcol = rc_take(&cur, sizeof(int) * b.sub_col.size());
+    const size_t o_xfins = rc_take(&cur, sizeof(FIns) * xp.fins.size());
+    const size_t o_xoff = rc_take(&cur, sizeof(int) * xp.off.size());
+    const size_t o_xinfo = rc_take(&cur, sizeof(int4) * xp.info.size());
     const size_t in_end = rc_take(&cur, 0);
     const size_t o_c = rc_take(&cur, sizeof(double) * (size_t)nprog * kmax);
     const size_t o_sse = rc_take(&cur, sizeof(double) * nprog);
@@ -2026,6 +2187,9 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     memcpy(host + o_subf, b.sub_fins.data(), sizeof(FIns) * b.sub_fins.size());
     memcpy(host + o_suboff, b.sub_off.data(), sizeof(int) * b.sub_off.size());
     memcpy(host + o_subcol, b.sub_col.data(), sizeof(int) * b.sub_col.size());
+    memcpy(host + o_xfins, xp.fins.data(), sizeof(FIns) * xp.fins.size());
+    if (!xp.off.empty()) memcpy(host + o_xoff, xp.off.data(), sizeof(int) * xp.off.size());
+    if (!xp.info.empty()) memcpy(host + o_xinfo, xp.info.data(), sizeof(int4) * xp.info.size());
     memcpy(host + o_c, c0, sizeof(double) * (size_t)nprog * kmax);
     st->h2d_ms += rc_now_ms() - t;
     st->h2d_bytes += io_end;
@@ -2060,6 +2224,12 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     a.nsub = (int)b.sub_off.size() - 1;
     a.sub_slots = b.sub_slots;
     a.sub_maxins = b.sub_maxins;
+    a.xfins = reinterpret_cast<const FIns *>(dev + o_xfins);
+    a.xfins_off = reinterpret_cast<const int *>(dev + o_xoff);
+    a.xinfo = reinterpret_cast<const int4 *>(dev + o_xinfo);
+    a.xmaxins = xp.maxins;
+    a.xslots = xp.slots;
+    a.xtape = xp.tape;
     a.asm_region = b.asm_region;
     a.fslots = b.fslots;
     a.ftape = b.ftape;
@@ -2084,7 +2254,7 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     int nk = 0;
     if (metric == FM_IMPLICIT) {
         sw[nk] = sweep_launch<FOP_IJAC>(c, b.mmax, Wmax); ++nk;
-        sw[nk] = sweep_launch<FOP_ICOST>(c, b.mmax, Wmax); ++nk;
+        sw[nk] = icost_launch(c, xp); ++nk;
     } else if (corr) {
         sw[nk] = sweep4_launch<FOP_CASM, FT_ASM_T>(c, b, Wmax); ++nk;
         sw[nk] = sweep4_launch<FOP_CSCORE, 128>(c, b, Wmax); ++nk;
@@ -2114,6 +2284,8 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
             one.valid = a.valid + i;
             one.gauge = a.gauge + 2 * (size_t)i;
             one.fins_off = a.fins_off + i;
+            one.xfins_off = a.xfins_off + i;
+            one.xinfo = a.xinfo + i;
             one.finfo = a.finfo + i;
             one.fcinfo = a.fcinfo + i;
             one.sub_off = a.sub_off + b.sub_cand_off[i];
@@ -2133,8 +2305,8 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
                  nprog, kmax, ntiles, b.mmax, Wmax, iters, metric, flags, steps, io_end, b.fslots,
                  b.ftape, b.fmaxins, b.asm_region);
         const size_t kl = strlen(key);
-        snprintf(key + kl, sizeof(key) - kl, "|%d|%d|%d|%d", b.ncache, a.nsub, b.sub_slots,
-                 b.sub_maxins);
+        snprintf(key + kl, sizeof(key) - kl, "|%d|%d|%d|%d|%d|%d|%d", b.ncache, a.nsub,
+                 b.sub_slots, b.sub_maxins, xp.maxins, xp.slots, xp.tape);
         if (!c->fit_graph || c->fit_graph_key != key) {
             if (c->fit_graph) {
                 cudaGraphExecDestroy(c->fit_graph);
@@ -2337,29 +2509,12 @@ float rc_implicit_score_batch(void *ctx, const unsigned int *prog, const unsigne
     FitPrep b;
     prep_batch(off, prog, pcount, nprog, rc->v, b);
     /* the input-mode translation: partials and pruning along input paths */
-    std::vector<FIns> xfins, fwd, rev;
-    std::vector<int> xoff(nprog + 1, 0);
-    std::vector<int4> xinfo(nprog, make_int4(0, 0, 0, 0));
-    int slots = 1, ntape = 1, maxins = 2;
-    for (int i = 0; i < nprog; ++i) {
-        xoff[i] = (int)xfins.size();
-        if (!b.valid[i]) continue;
-        int ns = 0, nt = 0;
-        const int m = b.node_off[i + 1] - b.node_off[i];
-        if (!fi_decode(prog + off[i], m, fwd, rev, &ns, &nt, nullptr, nullptr, true) ||
-            ns > 0xffff || nt > 0x7fff) {
-            b.valid[i] = 0;
-            continue;
-        }
-        xfins.insert(xfins.end(), fwd.begin(), fwd.end());
-        xfins.insert(xfins.end(), rev.begin(), rev.end());
-        xinfo[i] = make_int4((int)fwd.size(), (int)rev.size(), ns, nt);
-        slots = std::max(slots, ns);
-        ntape = std::max(ntape, nt);
-        maxins = std::max(maxins, (int)(fwd.size() + rev.size()));
-    }
-    xoff[nprog] = (int)xfins.size();
-    if (xfins.empty()) xfins.resize(1);
+    XPrep xp;
+    prep_inputs(off, prog, nprog, b.node_off, b.valid, xp);
+    std::vector<FIns> &xfins = xp.fins;
+    std::vector<int> &xoff = xp.off;
+    std::vector<int4> &xinfo = xp.info;
+    const int slots = xp.slots, ntape = xp.tape, maxins = xp.maxins;
     const int T = 128;
     constexpr int NR = 2;
     const int rows_per_tile = 16384;
