@@ -219,3 +219,101 @@ DEFAULT_VARIATION_OPS = ((17, 1), (9, 1), (10, 1), (12, 1), (11, 1), (6, 1), (7,
 def width_for(max_complexity):
     """Fixed slot width for a maximum complexity (genome.rs:35-37)."""
     return max(2 * max_complexity + 4, 8)
+
+
+# ---- the run-level fit ledger ------------------------------------------------
+
+# Labels of the finite device answers (my-version/src/search.rs:2939-2948).
+STATUS_LABELS = {4: "rank_deficient", 5: "recovered", 6: "no_improvement", 7: "start_unusable",
+                 8: "recovered_skipped"}
+
+
+def fit_status_usable(status):
+    """Statuses that carry a finite answer the search may keep
+    (my-version/src/fit/gpu.rs:103-105)."""
+    return int(status) in (0, 4, 5, 6, 7, 8)
+
+
+def status_fallback_cause(status):
+    """The CPU-fallback cause of a device status (search.rs:2952-2959)."""
+    return {1: "ill_conditioned", 2: "non_finite", 3: "rank_declined"}.get(int(status),
+                                                                         "unsupported_plan")
+
+
+def _jnum(v):
+    """A number as the reference's ledger prints it (Rust's shortest
+    round-trip decimal, no exponent; null when not finite)."""
+    v = float(v)
+    if not np.isfinite(v):
+        return "null"
+    return np.format_float_positional(v, unique=True, trim="-")
+
+
+def _jmap(d):
+    return ",".join('"%s":%d' % (k, d[k]) for k in sorted(d))
+
+
+class FitLedger:
+    """The `gpu.fit` run-record of the reference's `--json` output
+    (my-version/src/main.rs:995-1010) and its accounting
+    (search.rs:2040-2120): candidates screened, offered to the fit arm,
+    answered on the device, sent to the exact CPU arm by cause, device
+    answers by status label, finalist refits, and the fit stage's times."""
+
+    def __init__(self, strategy="gpu"):
+        self.strategy = strategy
+        self.screened = self.attempts = self.gpu = self.fallback = self.refits = 0
+        self.fallback_by_cause = {}
+        self.status_by_label = {}
+        self.seconds = self.host_seconds = self.fallback_seconds = 0.0
+        self.fallback_bounded = self.fallback_workers = self.fallback_max = 0
+
+    def note_fallback(self, cause):
+        self.fallback += 1
+        self.fallback_by_cause[cause] = self.fallback_by_cause.get(cause, 0) + 1
+
+    def record_batch(self, trees, constants, status, ms):
+        """One fit batch of `trees` with the device's `constants` [P][kmax],
+        `status` [P] and kernel `ms` (negative: the launch failed). A tree
+        without constants is not offered; a tree the plan rejects falls back
+        as `too_many_constants` or `unsupported_plan`; a planned tree is a
+        device answer when its status is usable and its constants finite,
+        else a fallback by its status (`non_finite` for a non-finite
+        constant). Trees that were planned are in `constants` order."""
+        planned = []
+        for t in trees:
+            try:
+                gpu_fit_plan(t)
+                planned.append(t)
+                self.attempts += 1
+            except GpuFitReject as r:
+                if r.label == "no_constants":
+                    continue
+                self.attempts += 1
+                self.note_fallback("too_many_constants" if r.label == "too_many_constants"
+                                   else "unsupported_plan")
+        if ms < 0:
+            for _ in planned:
+                self.note_fallback("launch")
+            return
+        self.seconds += ms / 1e3
+        for k in range(len(planned)):
+            s = int(status[k])
+            finite = bool(np.all(np.isfinite(constants[k])))
+            if fit_status_usable(s) and finite:
+                self.gpu += 1
+                if s in STATUS_LABELS:
+                    lab = STATUS_LABELS[s]
+                    self.status_by_label[lab] = self.status_by_label.get(lab, 0) + 1
+            else:
+                self.note_fallback("non_finite" if not finite else status_fallback_cause(s))
+
+    def to_json(self):
+        return ('"fit":{"strategy":"%s","screened":%d,"attempts":%d,"gpu":%d,"fallback":%d,'
+                '"fallback_by_cause":{%s},"status_by_label":{%s},"refits":%d,"seconds":%s,'
+                '"host_seconds":%s,"fallback_seconds":%s,"fallback_bounded":%d,'
+                '"fallback_workers":%d,"fallback_max":%d}' % (
+                    self.strategy, self.screened, self.attempts, self.gpu, self.fallback,
+                    _jmap(self.fallback_by_cause), _jmap(self.status_by_label), self.refits,
+                    _jnum(self.seconds), _jnum(self.host_seconds), _jnum(self.fallback_seconds),
+                    self.fallback_bounded, self.fallback_workers, self.fallback_max))
