@@ -122,7 +122,7 @@ int rc_pool_hash(void *ctx, int which, int nprog, int width, unsigned long long 
    with their errors err[islands*pop] (host). Children go to pool which ^ 1.
    ops: nops (opcode, arity) pairs in the engine's table order; restart:
    [islands] or NULL; front: nfront programs packed by front_off[nfront+1]
-   (words), drawn with probability front_p. Outputs (host, each nullable):
+   (words, each 2..width long), drawn with probability front_p. Outputs (host, each nullable):
    len/cost [islands*pop] u16, hash u64, err f64 (the island's elite keeps its
    parent's error, every other slot NaN), words [islands*pop*width]. Returns
    kernel ms >= 0, or -1 (bad arguments, a parent slot that is not a valid

@@ -195,8 +195,12 @@ extern "C" float rc_pool_vary(void *ctx, int which, int islands, int pop, int wi
     cfg.nfront = front_p > 0.0 ? nfront : 0;
     cfg.front_p = front_p;
     const size_t nfw = cfg.nfront > 0 ? front_off[cfg.nfront] : 0;
+    /* a front program must fit a slot, as FrontParents::from_front keeps only
+       those (postfix.rs:369-383); the engine's buffers hold one slot */
     for (int f = 0; f < cfg.nfront; ++f)
-        if (front_off[f + 1] < front_off[f]) return -1.0f;
+        if (front_off[f + 1] < front_off[f] || front_off[f + 1] - front_off[f] > (unsigned)width ||
+            front_off[f + 1] - front_off[f] < 2)
+            return -1.0f;
 
     /* layout: inputs [err | restart | front | front_off], parent metadata,
        items, their programs, host programs and choices */
