@@ -107,6 +107,7 @@ struct FitArgs {
     const int2 *fcinfo;    /* [P] cached forward count (after the reverse list),
                               first cache column */
     float *cache;          /* [columns][npad] values of constant-free subtrees */
+    double *cache64;       /* the same columns in f64 for the polish, or null */
     const FIns *sub_fins;  /* forward lists of the cached subtrees */
     const int *sub_off;    /* [nsub + 1] */
     const int *sub_col;    /* [nsub] */
@@ -843,12 +844,15 @@ __global__ void __launch_bounds__(T) ft_sweep4(FitArgs a, int q)
         const int nr = info.y;
         /* f32 sweeps run the cached forward list (constant-free subtrees read
            from the cache), the f64 polish the full one */
-        constexpr bool CACHED = sizeof(V) == 4;
+        const bool CACHED = sizeof(V) == 4 || a.cache64 != nullptr;
         const int2 fc = CACHED ? a.fcinfo[cand] : make_int2(info.x, 0);
         const int nf = fc.x;
         const FIns *fsrc = a.fins + ib + (CACHED ? info.x + nr : 0);
-        const V *ccols = CACHED ? reinterpret_cast<const V *>(a.cache) + (size_t)fc.y * a.npad
-                                : nullptr;
+        const V *ccols =
+            !CACHED ? nullptr
+                    : (sizeof(V) == 4 ? reinterpret_cast<const V *>(a.cache)
+                                      : reinterpret_cast<const V *>(a.cache64)) +
+                          (size_t)fc.y * a.npad;
         const int p = a.pcount[cand];
         const int sel = st->sel;
         for (int i = tid; i < nf; i += T) ins[i] = fsrc[i];
@@ -897,6 +901,32 @@ __global__ void __launch_bounds__(FT_FILL_T) ft_cache_fill(FitArgs a)
                                     pr);
 #pragma unroll
         for (int i = 0; i < 4; ++i)
+            if (row + i < r1) out[row + i] = pr[i];
+    }
+}
+
+/* The f64 twin of ft_cache_fill for the polish sweeps (two rows per
+   thread). The subtrees are the same programs, so each column holds exactly
+   the values the f64 sweeps would compute inline. */
+__global__ void __launch_bounds__(FT_FILL_T) ft_cache_fill64(FitArgs a)
+{
+    using V4 = FiV<double, 2>::V4;
+    extern __shared__ __align__(16) unsigned char sm[];
+    FIns *ins = reinterpret_cast<FIns *>(sm);
+    V4 *stk = reinterpret_cast<V4 *>(sm + 8 * (size_t)((a.sub_maxins + 1) & ~1));
+    const int s = blockIdx.x / a.ntiles, tile = blockIdx.x % a.ntiles;
+    const int tid = threadIdx.x;
+    const int b = a.sub_off[s], ni = a.sub_off[s + 1] - b;
+    for (int i = tid; i < ni; i += FT_FILL_T) ins[i] = a.sub_fins[b + i];
+    __syncthreads();
+    const int r0 = tile * FT_TILE_ROWS, r1 = min(a.n, r0 + FT_TILE_ROWS);
+    double *out = a.cache64 + (size_t)a.sub_col[s] * a.npad;
+    for (int row = r0 + 2 * tid; row < r1; row += 2 * FT_FILL_T) {
+        double pr[2];
+        fi_forward<double, 2, false>(ins, nullptr, a.cols64, a.npad, row, stk, nullptr, FT_FILL_T,
+                                     tid, pr);
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
             if (row + i < r1) out[row + i] = pr[i];
     }
 }
@@ -2088,6 +2118,10 @@ unsigned long long enqueue_fit(cudaStream_t s_, int sm_count, const FitArgs &a, 
                             16 * (size_t)(a.sub_slots > 0 ? a.sub_slots : 1) * FT_FILL_T;
         ft_cache_fill<<<(unsigned)a.nsub * (unsigned)a.ntiles, FT_FILL_T, smem, s_>>>(a);
         k = 1;
+        if (a.cache64) {
+            ft_cache_fill64<<<(unsigned)a.nsub * (unsigned)a.ntiles, FT_FILL_T, smem, s_>>>(a);
+            k = 2;
+        }
     }
     ft_step_reset<<<1, 32, 0, s_>>>(a, 1);
     cudaMemsetAsync(a.work + 1 * FOP_COUNT, 0, sizeof(int) * FOP_COUNT, s_);
@@ -2130,7 +2164,7 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
         cudaGetLastError();
         free_b = 0;
     }
-    const size_t cache_cap = std::min<size_t>((size_t)16 << 30, free_b / 3);
+    const size_t cache_cap = std::min<size_t>((size_t)48 << 30, free_b / 3);
     const bool use_cache = metric != FM_IMPLICIT;
     prep_batch(off, prog, pcount, nprog, c->v, b, corr ? 2 : 0,
                use_cache ? sizeof(float) * (size_t)c->npad : 0, cache_cap);
@@ -2168,6 +2202,11 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     const size_t o_counts = rc_take(&cur, sizeof(int) * 2 * FOP_COUNT);
     const size_t o_work = rc_take(&cur, sizeof(int) * 2 * FOP_COUNT);
     const size_t o_cache = rc_take(&cur, sizeof(float) * (size_t)c->npad * (size_t)b.ncache);
+    /* the f64 twin of the cache for the polish, when it fits the same cap */
+    const bool use64 = use_cache && b.ncache > 0 && !(flags & 1) &&
+                       sizeof(double) * (size_t)c->npad * (size_t)b.ncache <= cache_cap;
+    const size_t o_cache64 =
+        rc_take(&cur, use64 ? sizeof(double) * (size_t)c->npad * (size_t)b.ncache : 0);
     const size_t dev_end = rc_take(&cur, 0);
     if (rc_reserve(c, dev_end, io_end) != 0) return -1.0f;
     st->alloc_ms += rc_now_ms() - t;
@@ -2218,6 +2257,7 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     a.finfo = reinterpret_cast<const int4 *>(dev + o_finfo);
     a.fcinfo = reinterpret_cast<const int2 *>(dev + o_fcinfo);
     a.cache = reinterpret_cast<float *>(dev + o_cache);
+    a.cache64 = use64 ? reinterpret_cast<double *>(dev + o_cache64) : nullptr;
     a.sub_fins = reinterpret_cast<const FIns *>(dev + o_subf);
     a.sub_off = reinterpret_cast<const int *>(dev + o_suboff);
     a.sub_col = reinterpret_cast<const int *>(dev + o_subcol);
@@ -2305,8 +2345,8 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
                  nprog, kmax, ntiles, b.mmax, Wmax, iters, metric, flags, steps, io_end, b.fslots,
                  b.ftape, b.fmaxins, b.asm_region);
         const size_t kl = strlen(key);
-        snprintf(key + kl, sizeof(key) - kl, "|%d|%d|%d|%d|%d|%d|%d", b.ncache, a.nsub,
-                 b.sub_slots, b.sub_maxins, xp.maxins, xp.slots, xp.tape);
+        snprintf(key + kl, sizeof(key) - kl, "|%d|%d|%d|%d|%d|%d|%d|%d", b.ncache, a.nsub,
+                 b.sub_slots, b.sub_maxins, xp.maxins, xp.slots, xp.tape, use64 ? 1 : 0);
         if (!c->fit_graph || c->fit_graph_key != key) {
             if (c->fit_graph) {
                 cudaGraphExecDestroy(c->fit_graph);
