@@ -530,8 +530,9 @@ __device__ __forceinline__ bool ft_implicit_d(const uint4 *rec, int m, const dou
    where g . dg/dc_j = d/dc_j (grad_x f . v) at v = g held fixed, a
    Hessian-vector product of f. Four sweeps over the records:
    1. forward values (tape `vt`);
-   2. reverse in place: the input adjoint g and df/dc (into jrow);
-   3. forward again, values and tangents along x' = g (tapes `vt`, `tt`);
+   2. reverse: the input adjoint g and df/dc (into jrow), each node's
+      adjoint in `tt` (the values in `vt` stay);
+   3. forward tangents along x' = g over the stored values (into `tt`);
    4. reverse of the tangent: each node's slots switch from (value,
       tangent) to (adjoint u, second-order adjoint w) when its parent is
       processed; a constant's w is g . dg/dc_j.
@@ -549,10 +550,10 @@ __device__ bool ft_implicit_jac(const uint4 *rec, int m, const double *x, int v,
     double ig[FT_IMPLICIT_MAXV];
 #pragma unroll
     for (int k = 0; k < FT_IMPLICIT_MAXV; ++k) ig[k] = 0.0;
-    vt[(m - 1) * TS] = 1.0;
+    tt[(m - 1) * TS] = 1.0;
     for (int i = m - 1; i >= 0; --i) {
         const uint4 r = rec[i];
-        const double a = vt[i * TS];
+        const double a = tt[i * TS];
         if (r.x == OP_CONST) {
             jrow[r.w] += a;
             continue;
@@ -573,8 +574,8 @@ __device__ bool ft_implicit_jac(const uint4 *rec, int m, const double *x, int v,
             c0 = a * d0;
             c1 = a * d1;
         }
-        vt[r.y * TS] = c0;
-        if (bin) vt[r.z * TS] = c1;
+        tt[r.y * TS] = c0;
+        if (bin) tt[r.z * TS] = c1;
     }
     double nsq = 0.0;
     for (int k = 0; k < FT_IMPLICIT_MAXV; ++k) {
@@ -586,28 +587,25 @@ __device__ bool ft_implicit_jac(const uint4 *rec, int m, const double *x, int v,
     if (!(isfinite(norm) && norm > 0.0)) return false;
     d = fv / norm;
     if (!isfinite(d)) return false;
-    /* 3: values and tangents along x' = g */
+    /* 3: tangents along x' = g over the stored values (a node's adjoint in
+       tt is replaced by its tangent; its children's are tangents already) */
     for (int i = 0; i < m; ++i) {
         const uint4 r = rec[i];
-        double val, tan = 0.0;
-        if (r.x == OP_CONST) val = c[r.w];
-        else if (r.x == OP_VAR) {
-            val = x[r.w];
+        double tan = 0.0;
+        if (r.x == OP_VAR) {
 #pragma unroll
             for (int k = 0; k < FT_IMPLICIT_MAXV; ++k)
                 if ((int)r.w == k) tan = ig[k];
-        } else {
+        } else if (r.x != OP_CONST) {
             const bool bin = ft_op_binary(r.x);
             const double a = vt[r.y * TS], ta = tt[r.y * TS];
             const double b = bin ? vt[r.z * TS] : 0.0, tb = bin ? tt[r.z * TS] : 0.0;
-            val = ft_value_d(r.x, a, b);
             if (!(r.x == OP_POW && !(a > 0.0)) && (ta != 0.0 || tb != 0.0)) {
                 double d0, d1;
                 ft_partials_d(r.x, a, b, d0, d1);
                 tan = ft_mul0(ta, d0) + ft_mul0(tb, d1);
             }
         }
-        vt[i * TS] = val;
         tt[i * TS] = tan;
     }
     /* 4: reverse of the tangent; u = first-order adjoint, w = second */
