@@ -531,7 +531,8 @@ __device__ __forceinline__ bool ft_implicit_d(const uint4 *rec, int m, const dou
    Hessian-vector product of f. Four sweeps over the records:
    1. forward values (tape `vt`);
    2. reverse: the input adjoint g and df/dc (into jrow), each node's
-      adjoint in `tt` (the values in `vt` stay);
+      adjoint in `tt` (the values in `vt` stay); once a unary node's
+      adjoint is consumed, its slot keeps the node's partial;
    3. forward tangents along x' = g over the stored values (into `tt`);
    4. reverse of the tangent: each node's slots switch from (value,
       tangent) to (adjoint u, second-order adjoint w) when its parent is
@@ -566,7 +567,16 @@ __device__ bool ft_implicit_jac(const uint4 *rec, int m, const double *x, int v,
         }
         const bool bin = ft_op_binary(r.x);
         const double xx = vt[r.y * TS];
-        const double yy = bin ? vt[r.z * TS] : 0.0;
+        if (!bin) {
+            /* a unary node's own partial goes to its (now consumed) slot for
+               the tangent pass */
+            double d0, d1;
+            ft_partials_d(r.x, xx, 0.0, d0, d1);
+            tt[r.y * TS] = a != 0.0 ? a * d0 : 0.0;
+            tt[i * TS] = d0;
+            continue;
+        }
+        const double yy = vt[r.z * TS];
         double c0 = 0.0, c1 = 0.0;
         if (a != 0.0 && !(r.x == OP_POW && !(xx > 0.0))) {
             double d0, d1;
@@ -575,7 +585,7 @@ __device__ bool ft_implicit_jac(const uint4 *rec, int m, const double *x, int v,
             c1 = a * d1;
         }
         tt[r.y * TS] = c0;
-        if (bin) tt[r.z * TS] = c1;
+        tt[r.z * TS] = c1;
     }
     double nsq = 0.0;
     for (int k = 0; k < FT_IMPLICIT_MAXV; ++k) {
@@ -596,10 +606,13 @@ __device__ bool ft_implicit_jac(const uint4 *rec, int m, const double *x, int v,
 #pragma unroll
             for (int k = 0; k < FT_IMPLICIT_MAXV; ++k)
                 if ((int)r.w == k) tan = ig[k];
-        } else if (r.x != OP_CONST) {
-            const bool bin = ft_op_binary(r.x);
+        } else if (r.x == OP_CONST) {
+        } else if (!ft_op_binary(r.x)) {
+            const double ta = tt[r.y * TS];
+            if (ta != 0.0) tan = ft_mul0(ta, tt[i * TS]) + 0.0;
+        } else {
             const double a = vt[r.y * TS], ta = tt[r.y * TS];
-            const double b = bin ? vt[r.z * TS] : 0.0, tb = bin ? tt[r.z * TS] : 0.0;
+            const double b = vt[r.z * TS], tb = tt[r.z * TS];
             if (!(r.x == OP_POW && !(a > 0.0)) && (ta != 0.0 || tb != 0.0)) {
                 double d0, d1;
                 ft_partials_d(r.x, a, b, d0, d1);
