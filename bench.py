@@ -19,7 +19,8 @@ GPU the same line also carries the other configurations:
   vary:     the next generation of a 16 x 1000 program pool built on the
             device (tournament, crossover, mutation, hashing, dedup),
             children/s beside the CPU restatement of the reference engine.
-`--workload fit|implicit|c5|rank|vary` makes one of them the primary line.
+`--workload fit|implicit|c5|rank|vary` makes one of them the primary line;
+`--workload refit` times the exact f64 finalist refit on the host cores alone.
 
 One step is one pass of the hot path over the whole batch. `value` is
 device-timed with CUDA events on the library's stream (inputs resident in
@@ -181,6 +182,48 @@ def cpu_fit_baseline(trees, x, y, n_rows, n_cand, iters, threads):
     dt = time.perf_counter() - t0
     # per-candidate cost grows linearly in rows: scale to the full row count
     return n_cand / dt, dt
+
+
+def bench_refit(pkg, W, P=16, N=1 << 18, iters=20, port_sample=2):
+    """The exact f64 finalist refit on the host cores (host/refit.cpp): P
+    finalists of the fit workload's tree distribution at N rows x 8 features,
+    `iters` LM iterations, squared error, all host threads; beside it the
+    oracle's row-at-a-time restatement of the reference's refit (the port),
+    single-threaded on the first `port_sample` finalists, with the product's
+    own single-thread time on the same sample and a bit-for-bit comparison of
+    the two on it."""
+    trees, x, y = W.fit_workload(P, N, seed=7)
+    v = x.shape[0]
+    x64 = np.ascontiguousarray(x, np.float64).reshape(-1)
+    y64 = np.ascontiguousarray(y, np.float64)
+    threads = os.cpu_count() or 1
+    warm = np.ascontiguousarray(x64.reshape(v, N)[:, :4096]).reshape(-1)
+    pkg.refit_finalists_exact(trees[:1], warm, y64[:4096], 2)
+    t0 = time.perf_counter()
+    loss, _ = pkg.refit_finalists_exact(trees, x64, y64, iters, "squared", threads=threads)
+    dt = time.perf_counter() - t0
+    sample = trees[:port_sample]
+    t0 = time.perf_counter()
+    own, _ = pkg.refit_finalists_exact(sample, x64, y64, iters, "squared", threads=1)
+    dt1 = time.perf_counter() - t0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.lib()
+    t0 = time.perf_counter()
+    port = [O.fit(t, x64, N, v, y64, iters)[0] for t in sample]
+    dtp = time.perf_counter() - t0
+    same = bool(np.array_equal(np.asarray(port, np.float64).view(np.uint64),
+                               own.view(np.uint64)))
+    return {"metric": "refit_finalists_per_s", "value": P / dt, "unit": "finalists/s",
+            "threads": threads, "s": dt, "value_1_thread": port_sample / dt1,
+            "config": {"workload": f"exact f64 finalist refit, {P} finalists of the fit "
+                                   f"workload's trees, N={N} rows x {v} features, {iters} LM "
+                                   f"iterations, squared error"},
+            "cpu_baseline": {"value": port_sample / dtp, "unit": "finalists/s", "cores": 1,
+                             "kind": "port", "cpu_model": cpu_model(),
+                             "sample": f"the first {port_sample} finalists, row-at-a-time "
+                                       f"f64 oracle, one thread"},
+            "same_bits_as_port": same}
 
 
 # ---------------------------------------------------------------------------
@@ -588,7 +631,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="score",
-                    choices=["score", "fit", "rank", "implicit", "c5", "vary"])
+                    choices=["score", "fit", "rank", "implicit", "c5", "vary", "refit"])
     ap.add_argument("--P", type=int, default=0)
     ap.add_argument("--N", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -601,6 +644,14 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", 1))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.workload == "refit":
+        # host cores only: no device work
+        if rank == 0:
+            r = bench_refit(importlib.import_module(PKG),
+                            importlib.import_module(PKG + ".workloads"),
+                            P=args.P or 16, N=args.N or (1 << 18))
+            print(json.dumps(r), flush=True)
+        return
 
     import torch
     import torch.distributed as dist
@@ -736,6 +787,8 @@ def main():
             fit, what, rk = bench_c5(args, rank, pkg, W, flushbuf, 3, 3, 1, 1)
             line["c5"] = {"absolute_fit": fit_summary(fit, peaks, what), "rank": rk}
             line["vary"] = bench_vary(args, rank, pkg, flushbuf, 5, 3)
+            if not args.no_cpu_baseline:
+                line["refit"] = bench_refit(pkg, W)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

@@ -737,7 +737,13 @@ bool gn_trial(const Flat &f, const Rows &x, const double *y, const double *w,
     std::vector<double> step;
     if (!solve(ne.jtj, rhs, lambda, k, step)) return false;
     trial.resize(k);
-    for (int i = 0; i < k; ++i) trial[i] = std::min(1e6, std::max(-1e6, c[i] + step[i]));
+    for (int i = 0; i < k; ++i) {
+        /* Rust's f64::clamp: a NaN stays NaN */
+        double t = c[i] + step[i];
+        if (t < -1e6) t = -1e6;
+        if (t > 1e6) t = 1e6;
+        trial[i] = t;
+    }
     tsse = sse(f, x, y, w, trial.data(), v);
     return true;
 }

@@ -113,6 +113,16 @@ def test_library_exports_every_declared_symbol(pkg):
     assert sorted(dev.SIGNATURES) == names
 
 
+def test_host_library_exports_every_refit_symbol(pkg):
+    """include/rcsr_refit.h is served by librcsr_host.so (no GPU needed)."""
+    src = open(os.path.join(ROOT, "include", "rcsr_refit.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = sorted(set(re.findall(r"\b(rch_[a-z0-9_]+)\s*\(", src)))
+    assert names == ["rch_refit_finalists", "rch_soa_eval", "rch_soa_sse"]
+    lib = ctypes.CDLL(os.path.join(ROOT, "the-rule-and-compass_b200", "librcsr_host.so"))
+    assert all(hasattr(lib, n) for n in names)
+
+
 def test_fit_kernel_info_contract(pkg):
     L = pkg.cuda_lib()
     t, s, m = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()

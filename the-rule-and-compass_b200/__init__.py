@@ -9,3 +9,4 @@ from . import expr, host  # noqa: F401
 from .device import GpuEvaluator, GenomePool, DeviceError, lib as cuda_lib  # noqa: F401
 from .host import compile_program, gpu_fit_plan, Population, pack_plans  # noqa: F401
 from .host import DEFAULT_VARIATION_OPS, width_for, FitLedger  # noqa: F401
+from .host import refit_finalists_exact, soa_eval, soa_sse  # noqa: F401

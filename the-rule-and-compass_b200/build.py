@@ -2,7 +2,8 @@
 
 - `librcsr_b200.so`: the CUDA C-ABI library (csrc/*.cu), compiled for sm_100a
   only, one object per translation unit in parallel, then linked.
-- `librcsr_host.so`: the host-side compiler (host/rcsr_host.cpp).
+- `librcsr_host.so`: the host-side compiler (host/rcsr_host.cpp) and the
+  exact f64 finalist refit (host/refit.cpp).
 
 Run `python the-rule-and-compass_b200/build.py` or call `build()`.
 """
@@ -70,9 +71,15 @@ def build_cuda(verbose_ptxas=False):
 
 
 def build_host():
-    src = os.path.join(HERE, "host", "rcsr_host.cpp")
-    if _stale(HOST_LIB, [src]):
-        cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-Wall", "-o", HOST_LIB, src]
+    """The host library: the compiler (rcsr_host.cpp) and the exact f64
+    finalist refit (refit.cpp). -ffp-contract=off keeps every f64 operation
+    a separately rounded IEEE operation, which the refit's bit-identity with
+    the reference's CPU path relies on."""
+    srcs = [os.path.join(HERE, "host", f) for f in ("rcsr_host.cpp", "refit.cpp")]
+    deps = srcs + [os.path.join(INCLUDE, "rcsr_refit.h")]
+    if _stale(HOST_LIB, deps):
+        cmd = ["g++", "-O3", "-std=c++17", "-ffp-contract=off", "-fPIC", "-shared", "-pthread",
+               "-Wall", "-I" + INCLUDE, "-o", HOST_LIB, *srcs]
         subprocess.run(cmd, check=True)
     return HOST_LIB
 

@@ -48,6 +48,20 @@ def lib():
                                           P(ctypes.c_double), P(ctypes.c_double),
                                           P(ctypes.c_uint8), ctypes.c_longlong,
                                           P(ctypes.c_int32), P(ctypes.c_int32), ctypes.c_int]
+        L.rch_refit_finalists.restype = ctypes.c_int
+        L.rch_refit_finalists.argtypes = [P(ctypes.c_int32), P(ctypes.c_double), P(ctypes.c_int32),
+                                          ctypes.c_int, P(ctypes.c_double), ctypes.c_int64,
+                                          ctypes.c_int, P(ctypes.c_double), P(ctypes.c_double),
+                                          ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                          P(ctypes.c_double)]
+        L.rch_soa_eval.restype = ctypes.c_int
+        L.rch_soa_eval.argtypes = [P(ctypes.c_int32), P(ctypes.c_double), ctypes.c_int,
+                                   P(ctypes.c_double), ctypes.c_int64, ctypes.c_int,
+                                   P(ctypes.c_double)]
+        L.rch_soa_sse.restype = ctypes.c_double
+        L.rch_soa_sse.argtypes = [P(ctypes.c_int32), P(ctypes.c_double), ctypes.c_int,
+                                  P(ctypes.c_double), ctypes.c_int64, ctypes.c_int,
+                                  P(ctypes.c_double)]
         _lib = L
     return _lib
 
@@ -317,3 +331,77 @@ class FitLedger:
                     _jmap(self.fallback_by_cause), _jmap(self.status_by_label), self.refits,
                     _jnum(self.seconds), _jnum(self.host_seconds), _jnum(self.fallback_seconds),
                     self.fallback_bounded, self.fallback_workers, self.fallback_max))
+
+
+# ---- the exact f64 finalist refit (host/refit.cpp) ---------------------------
+
+REFIT_METRICS = {"squared": 0, "absolute": 1, "log_squashed": 2, "aic": 7, "aicc": 8, "bic": 9}
+
+
+def _cols64(cols, n):
+    c = np.ascontiguousarray(cols, np.float64)
+    nvars = c.size // n if n else 0
+    return c, nvars
+
+
+def refit_finalists_exact(trees, cols, y, iters, metric="squared", w=None, threads=0):
+    """`refit_finalists_exact` (fit/gpu.rs:666-687) for the least-squares
+    family (`fit_lm`) and the absolute / log-squashed IRLS arms, on the host
+    cores. `cols` is column-major f64 [nvars][n]. Returns (objective per
+    finalist, refit trees); the inputs are not modified. Raises ValueError for
+    a metric this refit does not cover."""
+    code = REFIT_METRICS.get(metric, metric)
+    y = np.ascontiguousarray(y, np.float64)
+    n = len(y)
+    c, nvars = _cols64(cols, n)
+    wv = None if w is None else np.ascontiguousarray(w, np.float64)
+    ops, vals, off = [], [], [0]
+    for t in trees:
+        o, v = t.prefix()
+        ops.append(np.asarray(o, np.int32))
+        vals.append(np.asarray(v, np.float64))
+        off.append(off[-1] + len(o))
+    ops = np.ascontiguousarray(np.concatenate(ops) if ops else np.zeros(1, np.int32), np.int32)
+    vals = np.ascontiguousarray(np.concatenate(vals) if vals else np.zeros(1), np.float64)
+    off = np.asarray(off, np.int32)
+    loss = np.zeros(max(len(trees), 1), np.float64)
+    rc = lib().rch_refit_finalists(_p(ops, ctypes.c_int32), _p(vals, ctypes.c_double),
+                                   _p(off, ctypes.c_int32), len(trees), _p(c, ctypes.c_double),
+                                   n, nvars, _p(y, ctypes.c_double),
+                                   None if wv is None else _p(wv, ctypes.c_double), int(iters),
+                                   int(code), int(threads), _p(loss, ctypes.c_double))
+    if rc == -2:
+        raise ValueError(f"the exact refit does not cover metric {metric!r}")
+    if rc != 0:
+        raise ValueError(f"rch_refit_finalists rejected its arguments ({rc})")
+    out = []
+    for i, t in enumerate(trees):
+        u = t.clone()
+        u.set_prefix_values(vals[off[i]:off[i + 1]])
+        out.append(u)
+    return loss[:len(trees)], out
+
+
+def soa_eval(tree, cols, n):
+    """Predictions of `tree` over n rows (`eval_soa::eval_batch`)."""
+    o, v = tree.prefix()
+    o = np.ascontiguousarray(o, np.int32)
+    v = np.ascontiguousarray(v, np.float64)
+    c, nvars = _cols64(cols, n)
+    out = np.empty(max(n, 1), np.float64)
+    rc = lib().rch_soa_eval(_p(o, ctypes.c_int32), _p(v, ctypes.c_double), len(o),
+                            _p(c, ctypes.c_double), n, nvars, _p(out, ctypes.c_double))
+    if rc != 0:
+        raise ValueError("malformed tree")
+    return out[:n]
+
+
+def soa_sse(tree, cols, y):
+    """The raw SSE of `tree` (`eval_soa::sse`)."""
+    o, v = tree.prefix()
+    o = np.ascontiguousarray(o, np.int32)
+    v = np.ascontiguousarray(v, np.float64)
+    y = np.ascontiguousarray(y, np.float64)
+    c, nvars = _cols64(cols, len(y))
+    return lib().rch_soa_sse(_p(o, ctypes.c_int32), _p(v, ctypes.c_double), len(o),
+                             _p(c, ctypes.c_double), len(y), nvars, _p(y, ctypes.c_double))
