@@ -405,3 +405,134 @@ def soa_sse(tree, cols, y):
     c, nvars = _cols64(cols, len(y))
     return lib().rch_soa_sse(_p(o, ctypes.c_int32), _p(v, ctypes.c_double), len(o),
                              _p(c, ctypes.c_double), len(y), nvars, _p(y, ctypes.c_double))
+
+
+# ---- the checkpoint's backend identity ---------------------------------------
+#
+# A run on this library is a `gpu` run: its checkpoint records `backend gpu`
+# and `error_kind f32_proxy` (the saved errors are the f32 device scores), and
+# a resume onto the other backend is refused unless explicitly allowed
+# (checkpoint.rs:89-160, :525-550, :1133-1175; provenance.rs:13-85). The
+# device name is the library's own `rc_device_name`.
+
+BACKENDS = ("cpu", "gpu", "unknown")
+
+
+class CheckpointMismatch(Exception):
+    """A resume the reference refuses (exit code 3, input error)."""
+
+
+def parse_backend(s: str) -> str:
+    """`Backend::parse` (checkpoint.rs:108-117)."""
+    if s not in BACKENDS:
+        raise ValueError(f"backend must be 'cpu', 'gpu' or 'unknown', got '{s}'")
+    return s
+
+
+def error_kind_for_backend(backend: str) -> str:
+    """`ErrorKind::for_backend` (checkpoint.rs:153-160): what the saved
+    errors are."""
+    return {"gpu": "f32_proxy", "cpu": "f64", "unknown": "unknown"}[parse_backend(backend)]
+
+
+def check_backend(saved: str, current: str, allow_change: bool = False) -> None:
+    """`Checkpoint::check_backend` (checkpoint.rs:1133-1151): a checkpoint
+    from before the record (`unknown`) is not checked."""
+    if saved == "unknown":
+        return
+    if saved != current and not allow_change:
+        raise CheckpointMismatch(
+            f"checkpoint backend mismatch: saved run used '{saved}', this run uses "
+            f"'{current}'; pass --allow-backend-change to resume across backends (the "
+            f"trajectory and reported errors will differ)")
+
+
+def backend_change_note(saved: str, current: str):
+    """The stderr line of an allowed backend change (main.rs:4196-4206), or
+    None when there is no change to report."""
+    if saved == "unknown" or saved == current:
+        return None
+    return f"# checkpoint: backend changed {saved} -> {current} (allowed by --allow-backend-change)"
+
+
+class BuildIdentity:
+    """`provenance::BuildIdentity` (provenance.rs:13-85): what produced a
+    saved state. For a `gpu` run `device` is `rc_device_name()` and `driver`
+    the driver version; a CPU run records `cpu` / `n/a`."""
+
+    FIELDS = ("version", "commit", "binary_sha256", "device", "driver", "threads")
+
+    def __init__(self, version, commit, binary_sha256, device, driver, threads):
+        self.version, self.commit, self.binary_sha256 = version, commit, binary_sha256
+        self.device, self.driver, self.threads = device, driver, int(threads)
+
+    @classmethod
+    def current(cls, gpu: bool, version="unknown", commit="unknown", binary_sha256="unknown"):
+        device, driver = device_identity(gpu)
+        return cls(version, commit, binary_sha256, device, driver, os.cpu_count() or 1)
+
+    def differences(self, now: "BuildIdentity"):
+        """Every differing field as `name: saved A -> current B`; device and
+        driver only when both runs used the GPU."""
+        out = []
+
+        def cmp(name, a, b):
+            if a != b:
+                out.append(f"{name}: saved {a} -> current {b}")
+        cmp("version", self.version, now.version)
+        cmp("commit", self.commit, now.commit)
+        cmp("binary_sha256", self.binary_sha256, now.binary_sha256)
+        if self.device != "cpu" and now.device != "cpu":
+            cmp("device", self.device, now.device)
+            cmp("driver", self.driver, now.driver)
+        cmp("threads", str(self.threads), str(now.threads))
+        return out
+
+    def records(self):
+        """The `build ...` lines of a checkpoint (checkpoint.rs:543-550)."""
+        return [f"build {k} {getattr(self, k)}" for k in self.FIELDS]
+
+
+def check_identity(saved, current: BuildIdentity, allow_change: bool = False) -> None:
+    """`Checkpoint::check_identity` (checkpoint.rs:1156-1175); `saved` None
+    is a checkpoint written before the identity existed."""
+    if saved is None:
+        return
+    diff = saved.differences(current)
+    if not diff or allow_change:
+        return
+    raise CheckpointMismatch(
+        f"checkpoint build identity mismatch ({'; '.join(diff)}); pass "
+        f"--allow-build-change to resume under a different binary, device or thread count "
+        f"(the trajectory may differ)")
+
+
+def device_identity(gpu: bool):
+    """`manifest::device_info` (manifest.rs:358-389) without the CUDA
+    version: (device, driver)."""
+    if not gpu:
+        return "cpu", "n/a"
+    from . import device as _device
+    name = _device.device_name()
+    driver = "unknown"
+    try:
+        import subprocess
+        r = subprocess.run(["nvidia-smi"], capture_output=True, text=True, timeout=30)
+        if r.returncode == 0:
+            for line in r.stdout.splitlines():
+                if "Driver Version:" in line:
+                    driver = line.split("Driver Version:")[1].split()[0]
+                    break
+    except (OSError, subprocess.SubprocessError):
+        pass
+    return name, driver
+
+
+def checkpoint_backend_records(identity: BuildIdentity = None):
+    """The identity lines a checkpoint of a run on this library carries:
+    `backend gpu`, `error_kind f32_proxy` and, with an identity, its
+    `build ...` lines (checkpoint.rs:533, :542-550)."""
+    lines = ["backend gpu", f"error_kind {error_kind_for_backend('gpu')}"]
+    if identity is not None:
+        lines += identity.records()
+    return lines
