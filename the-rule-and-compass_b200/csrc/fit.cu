@@ -54,7 +54,7 @@
 
 enum {
     FOP_NONE = 0, FOP_ASM32 = 1, FOP_ASM64 = 2, FOP_LOSS32 = 3, FOP_LOSS64 = 4,
-    FOP_IJAC = 5, FOP_ICOST = 6, FOP_CASM = 7, FOP_CSCORE = 8, FOP_COUNT = 9
+    FOP_IJAC = 5, FOP_ICOST = 6, FOP_CASM = 7, FOP_CSCORE = 8, FOP_IJACS = 9, FOP_COUNT = 10
 };
 
 enum {
@@ -120,6 +120,8 @@ struct FitArgs {
     int iters, metric, flags;
     int ntiles;
     int mmax;
+    int ijac_small;        /* implicit: programs of at most this many records take the
+                              short Jacobian launch (FOP_IJACS); 0: one launch */
     int Wmax;
     int nprog;
     FitState *state;
@@ -136,8 +138,11 @@ struct FitArgs {
 
 __host__ __device__ inline bool ft_op_assembles(int opk)
 {
-    return opk == FOP_ASM32 || opk == FOP_ASM64 || opk == FOP_IJAC || opk == FOP_CASM;
+    return opk == FOP_ASM32 || opk == FOP_ASM64 || opk == FOP_IJAC || opk == FOP_CASM ||
+           opk == FOP_IJACS;
 }
+
+__host__ __device__ inline bool ft_op_ijac(int opk) { return opk == FOP_IJAC || opk == FOP_IJACS; }
 
 /* Columns of a sweep's augmented Gram: the Jacobian and the residual, or for
    the correlation assembly the Jacobian and the weighted 1, f and y
@@ -163,7 +168,7 @@ __host__ __device__ inline size_t ft_rows_bytes(int Wmax, int T)
 __host__ __device__ inline size_t ft_sweep_smem(int opk, int mmax, int Wmax, int T)
 {
     size_t s = 16 * (size_t)mmax + 16 * FT_MAX_CONST +
-               8 * (size_t)mmax * T * (opk == FOP_IJAC ? 2 : 1);
+               8 * (size_t)mmax * T * (ft_op_ijac(opk) ? 2 : 1);
     if (ft_op_assembles(opk)) s += ft_rows_bytes(Wmax, T);
     return s + 8 * (size_t)T;
 }
@@ -357,13 +362,15 @@ __global__ void __launch_bounds__(T) ft_sweep(FitArgs a, int q)
         }
         return;
     }
+    /* the short Jacobian launch is laid out for its own record bound */
+    const int mcap = OPK == FOP_IJACS ? a.ijac_small : a.mmax;
     uint4 *rec = reinterpret_cast<uint4 *>(sm);
-    double *cd = reinterpret_cast<double *>(sm + 16 * (size_t)a.mmax);
+    double *cd = reinterpret_cast<double *>(sm + 16 * (size_t)mcap);
     float *cf = reinterpret_cast<float *>(cd + FT_MAX_CONST);
     float *tape = cf + 2 * FT_MAX_CONST;
     double *tape64 = reinterpret_cast<double *>(tape);
-    double *tan64 = tape64 + (size_t)a.mmax * T;
-    double *rows = tape64 + (size_t)a.mmax * T * (OPK == FOP_IJAC ? 2 : 1);
+    double *tan64 = tape64 + (size_t)mcap * T;
+    double *rows = tape64 + (size_t)mcap * T * (ft_op_ijac(OPK) ? 2 : 1);
     double *red = rows + (ft_op_assembles(OPK) ? ft_rows_bytes(a.Wmax, T) / 8 : 0);
     __shared__ int s_item;
     const int tid = threadIdx.x;
@@ -393,7 +400,7 @@ __global__ void __launch_bounds__(T) ft_sweep(FitArgs a, int q)
         const int r0 = tile * FT_TILE_ROWS;
         const int r1 = min(a.n, r0 + FT_TILE_ROWS);
         double *pt = a.part + ((size_t)cand * a.ntiles + tile) * FT_PART_STRIDE;
-        if (OPK == FOP_IJAC)
+        if (ft_op_ijac(OPK))
             ft_tile_implicit<T, true>(a, rec, m, p, cd, tape64, tan64, rows, red, r0, r1, pt);
         else
             ft_tile_implicit<T, false>(a, rec, m, p, cd, tape64, tan64, rows, red, r0, r1, pt);
@@ -1423,7 +1430,10 @@ __device__ void ft_advance(const FitArgs &a, FitState &st, int cand, int p, doub
                    unchanged point after a rejected or singular step; the
                    system kept from the last assembly is the same one */
                 if (!st.assembled) {
-                    st.op = FOP_IJAC;
+                    st.op = (a.ijac_small > 0 &&
+                             a.node_off[cand + 1] - a.node_off[cand] <= a.ijac_small)
+                                ? FOP_IJACS
+                                : FOP_IJAC;
                     st.sel = 0;
                     st.pc = PC_I_AFTER_JAC;
                     return;
@@ -2092,6 +2102,52 @@ SweepLaunch sweep_launch(RcCtx *c, int mmax, int Wmax)
     return s;
 }
 
+/* The record bound of the short Jacobian launch: the Jacobian sweep keeps
+   two f64 tapes per row in shared memory, sized for the longest program of
+   the launch, so one launch sized for the batch's longest program runs the
+   short ones at that program's occupancy. Estimate each split's time as the
+   records swept over the resident blocks each launch allows and take the
+   best, if it saves at least 5 %; 0 keeps one launch. The split depends on
+   the batch, but a candidate's arithmetic does not depend on which launch
+   runs it. */
+int ijac_split(RcCtx *c, const FitPrep &b, int Wmax)
+{
+    const void *fn = (const void *)ft_sweep<FOP_IJACS, FT_ITHREADS>;
+    /* occupancy queries up to the largest layout the split can choose */
+    const size_t smax = ft_sweep_smem(FOP_IJAC, b.mmax, Wmax, FT_ITHREADS);
+    if (smax > 48 * 1024 &&
+        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax) !=
+            cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    std::vector<int> ms;
+    for (size_t i = 0; i + 1 < b.node_off.size(); ++i)
+        if (b.valid[i]) ms.push_back(b.node_off[i + 1] - b.node_off[i]);
+    if (ms.size() < 2) return 0;
+    std::sort(ms.begin(), ms.end());
+    auto occ = [&](int m) {
+        return (double)occupancy(fn, FT_ITHREADS, ft_sweep_smem(FOP_IJAC, m, Wmax, FT_ITHREADS));
+    };
+    double total = 0.0;
+    for (int m : ms) total += m;
+    const double big = occ(b.mmax);
+    const double one = total / big;
+    double best = one, below = 0.0;
+    int pick = 0;
+    for (size_t i = 0; i < ms.size(); ++i) {
+        below += ms[i];
+        if (ms[i] >= b.mmax) break;
+        if (i + 1 < ms.size() && ms[i + 1] == ms[i]) continue;
+        const double cost = below / occ(ms[i]) + (total - below) / big;
+        if (cost < best) {
+            best = cost;
+            pick = ms[i];
+        }
+    }
+    return best <= 0.95 * one ? pick : 0;
+}
+
 template <int OPK, int T>
 SweepLaunch sweep4_launch(RcCtx *c, const FitPrep &b, int Wmax)
 {
@@ -2293,6 +2349,10 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     SweepLaunch sw[4];
     int nk = 0;
     if (metric == FM_IMPLICIT) {
+        a.ijac_small = ijac_split(c, b, Wmax);
+        if (a.ijac_small > 0) {
+            sw[nk] = sweep_launch<FOP_IJACS>(c, a.ijac_small, Wmax); ++nk;
+        }
         sw[nk] = sweep_launch<FOP_IJAC>(c, b.mmax, Wmax); ++nk;
         sw[nk] = icost_launch(c, xp); ++nk;
     } else if (corr) {
@@ -2345,8 +2405,9 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
                  nprog, kmax, ntiles, b.mmax, Wmax, iters, metric, flags, steps, io_end, b.fslots,
                  b.ftape, b.fmaxins, b.asm_region);
         const size_t kl = strlen(key);
-        snprintf(key + kl, sizeof(key) - kl, "|%d|%d|%d|%d|%d|%d|%d|%d", b.ncache, a.nsub,
-                 b.sub_slots, b.sub_maxins, xp.maxins, xp.slots, xp.tape, use64 ? 1 : 0);
+        snprintf(key + kl, sizeof(key) - kl, "|%d|%d|%d|%d|%d|%d|%d|%d|%d", b.ncache, a.nsub,
+                 b.sub_slots, b.sub_maxins, xp.maxins, xp.slots, xp.tape, use64 ? 1 : 0,
+                 a.ijac_small);
         if (!c->fit_graph || c->fit_graph_key != key) {
             if (c->fit_graph) {
                 cudaGraphExecDestroy(c->fit_graph);
