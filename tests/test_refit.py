@@ -160,3 +160,25 @@ def test_soa_evaluator_covers_every_operator(pkg, E, O):
         kids = [E.input(0), E.input(1), E.input(0)][:ar]
         t = E.node(op, kids)
         assert _same(pkg.host.soa_eval(t, xs, n), O.predict(t, xs, n, 2)), op
+
+
+@pytest.mark.parametrize("metric,code", [("squared", 0), ("absolute", 1)])
+def test_a_refit_split_over_threads_is_bit_identical(pkg, O, metric, code):
+    """Fewer finalists than threads and enough rows: each refit's passes are
+    split by rows over a team of threads (two chunks of rows here), with the
+    sums still taken in row order; the result equals the one-thread refit
+    and the oracle's row walk bit for bit, zero weights included."""
+    trees, x, y = _W().fit_workload(3, 70000, seed=21)
+    v, n = x.shape
+    rng = np.random.default_rng(8)
+    w = rng.uniform(0.5, 1.5, n)
+    w[rng.random(n) < 0.05] = 0.0
+    xs = np.ascontiguousarray(x, np.float64).reshape(-1)
+    one, t1 = pkg.host.refit_finalists_exact(trees, xs, y, 4, metric, w=w, threads=1)
+    team, t6 = pkg.host.refit_finalists_exact(trees, xs, y, 4, metric, w=w, threads=6)
+    assert _same(one, team)
+    for k, t in enumerate(trees):
+        assert _same(t1[k].constants(), t6[k].constants())
+        want, ref = O.fit(t, xs, n, v, y, 4, metric=code, w=w)
+        assert _same(team[k], want), (k, team[k], want)
+        assert _same(t6[k].constants(), ref.constants())

@@ -79,7 +79,7 @@ def build_host():
     deps = srcs + [os.path.join(INCLUDE, "rcsr_refit.h")]
     if _stale(HOST_LIB, deps):
         cmd = ["g++", "-O3", "-std=c++17", "-ffp-contract=off", "-fPIC", "-shared", "-pthread",
-               "-Wall", "-I" + INCLUDE, "-o", HOST_LIB, *srcs]
+               "-fopenmp", "-Wall", "-I" + INCLUDE, "-o", HOST_LIB, *srcs]
         subprocess.run(cmd, check=True)
     return HOST_LIB
 

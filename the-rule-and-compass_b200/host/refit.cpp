@@ -15,8 +15,11 @@
  * same f64 operation as the row walk and every sum is taken in the same order,
  * so the refit is bit-identical to the reference's; only the loop nest
  * differs (the node switch is taken once per block, and the element-wise
- * arithmetic vectorises). Finalists are independent and are refit on a pool
- * of threads.
+ * arithmetic vectorises). Finalists run concurrently on teams of threads:
+ * one thread each when there are at least as many finalists as threads,
+ * otherwise a finalist's passes are split by rows over its team (rows
+ * block-parallel, then every sum in row order on one thread). The thread
+ * count never changes a bit.
  *
  * The evaluator has the reference's two sets of domain rules: the tree
  * evaluator's (`expr::eval`, which `eval_soa.rs:273-380` mirrors: guarded
@@ -40,6 +43,8 @@
 #include <limits>
 #include <thread>
 #include <vector>
+
+#include <omp.h>
 
 namespace {
 
@@ -587,17 +592,45 @@ void backward(const Prog &p, int nb, const double *V, double *A, double *G)
 
 /* ---- the LM arm (fit.rs:1686-1827, :2318-2336, :2534-2624) ------------------ */
 
+/* One thread's sweep buffers. */
 struct Work {
     std::vector<double> V, A, G;
-    Plan plan;
-    bool planned = false;
     explicit Work(const Prog &p)
         : V((size_t)std::max(p.size(), 1) * RB), A((size_t)std::max(p.size(), 1) * RB),
           G((size_t)std::max((int)p.cpos.size(), 1) * RB)
     {
     }
+};
+
+/* Rows per chunk of a pass that runs on several threads. */
+constexpr int64_t CH = 256 * RB;
+
+/* The threads one refit runs on: a Work per thread, the refit's subtree
+   cache, and with more than one thread the chunk buffer of weighted
+   residuals (and Jacobian rows, [row][k + 1]) plus per-block failure flags.
+   A pass on several threads computes rows block-parallel and then takes
+   every sum in row order on the calling thread, so the bits do not depend
+   on the thread count. */
+struct Team {
+    int nt = 1;
+    std::vector<Work> wk;
+    Plan plan;
+    bool planned = false;
+    std::vector<double> rows;
+    std::vector<char> bad;
+    Team(const Prog &p, int threads) : nt(std::max(threads, 1))
+    {
+        wk.reserve(nt);
+        for (int t = 0; t < nt; ++t) wk.emplace_back(p);
+        if (nt > 1) {
+            rows.assign((size_t)CH * (size_t)(p.cpos.size() + 1), 0.0);
+            bad.assign((size_t)(CH / RB), 0);
+        }
+    }
     const Plan *flat_plan() const { return planned ? &plan : nullptr; }
 };
+
+inline int thread_index() { return omp_get_thread_num(); }
 
 bool transcendental(int op)
 {
@@ -615,10 +648,10 @@ bool transcendental(int op)
    Subtrees are taken by evaluation cost (a library function counts 8, other
    interior nodes 1). A subtree occupies the post-order range ending at its
    root. */
-void plan_cache(const Prog &p, const Data &d, size_t cap, Work &wk)
+void plan_cache(const Prog &p, const Data &d, size_t cap, Team &tm)
 {
     const int m = p.size();
-    wk.planned = false;
+    tm.planned = false;
     if (d.n == 0 || p.cpos.empty()) return;
     std::vector<int> parent(m, -1), span(m, 1), cost(m, 0);
     for (int i = 0; i < m; ++i) {
@@ -637,7 +670,7 @@ void plan_cache(const Prog &p, const Data &d, size_t cap, Work &wk)
     const size_t fit = cap / (sizeof(double) * (size_t)d.n);
     if (front.size() > fit) front.resize(fit);
     if (front.empty()) return;
-    Plan &pl = wk.plan;
+    Plan &pl = tm.plan;
     /* fill: evaluate only the chosen subtrees, block by block */
     Plan fill;
     fill.mode.assign(m, NODE_SKIP);
@@ -654,31 +687,69 @@ void plan_cache(const Prog &p, const Data &d, size_t cap, Work &wk)
         pl.col[r] = (int)f;
     }
     pl.cache.assign(front.size() * (size_t)d.n, 0.0);
-    for (int64_t r0 = 0; r0 < d.n; r0 += RB) {
+    const int64_t nblk = (d.n + RB - 1) / RB;
+#pragma omp parallel for num_threads(tm.nt) schedule(static) if (tm.nt > 1)
+    for (int64_t b = 0; b < nblk; ++b) {
+        Work &wk = tm.wk[tm.nt > 1 ? thread_index() : 0];
+        const int64_t r0 = b * RB;
         const int nb = (int)std::min<int64_t>(RB, d.n - r0);
         forward<false>(p, d, r0, nb, nullptr, wk.V.data(), &fill);
         for (size_t f = 0; f < front.size(); ++f)
             std::memcpy(pl.cache.data() + f * (size_t)d.n + r0,
                         wk.V.data() + (size_t)front[f] * RB, sizeof(double) * (size_t)nb);
     }
-    wk.planned = true;
+    tm.planned = true;
 }
 
 /* Weighted SSE at constants c (fit.rs:1732-1762): +inf on the first
    non-finite weighted residual. */
-double sse(const Prog &p, const Data &d, const double *w, const double *c, Work &wk)
+double sse(const Prog &p, const Data &d, const double *w, const double *c, Team &tm)
 {
     double s = 0.0;
-    const double *root = wk.V.data() + (size_t)p.root * RB;
-    for (int64_t r0 = 0; r0 < d.n; r0 += RB) {
-        const int nb = (int)std::min<int64_t>(RB, d.n - r0);
-        forward<false>(p, d, r0, nb, c, wk.V.data(), wk.flat_plan());
-        for (int r = 0; r < nb; ++r) {
-            const double sw = w ? w[r0 + r] : 1.0;
-            if (sw == 0.0) continue;
-            const double res = std::sqrt(sw) * (root[r] - d.y[r0 + r]);
-            if (!std::isfinite(res)) return INF;
-            s += res * res;
+    if (tm.nt == 1) {
+        Work &wk = tm.wk[0];
+        const double *root = wk.V.data() + (size_t)p.root * RB;
+        for (int64_t r0 = 0; r0 < d.n; r0 += RB) {
+            const int nb = (int)std::min<int64_t>(RB, d.n - r0);
+            forward<false>(p, d, r0, nb, c, wk.V.data(), tm.flat_plan());
+            for (int r = 0; r < nb; ++r) {
+                const double sw = w ? w[r0 + r] : 1.0;
+                if (sw == 0.0) continue;
+                const double res = std::sqrt(sw) * (root[r] - d.y[r0 + r]);
+                if (!std::isfinite(res)) return INF;
+                s += res * res;
+            }
+        }
+        return s;
+    }
+    double *R = tm.rows.data();
+    for (int64_t c0 = 0; c0 < d.n; c0 += CH) {
+        const int64_t nc = std::min<int64_t>(CH, d.n - c0);
+        const int nblk = (int)((nc + RB - 1) / RB);
+#pragma omp parallel for num_threads(tm.nt) schedule(static)
+        for (int b = 0; b < nblk; ++b) {
+            Work &wk = tm.wk[thread_index()];
+            const int64_t r0 = c0 + (int64_t)b * RB;
+            const int nb = (int)std::min<int64_t>(RB, d.n - r0);
+            forward<false>(p, d, r0, nb, c, wk.V.data(), tm.flat_plan());
+            const double *root = wk.V.data() + (size_t)p.root * RB;
+            char fail = 0;
+            for (int r = 0; r < nb; ++r) {
+                const double sw = w ? w[r0 + r] : 1.0;
+                double res = 0.0;
+                if (sw != 0.0) {
+                    res = std::sqrt(sw) * (root[r] - d.y[r0 + r]);
+                    if (!std::isfinite(res)) fail = 1;
+                }
+                R[r0 - c0 + r] = res;
+            }
+            tm.bad[b] = fail;
+        }
+        for (int b = 0; b < nblk; ++b)
+            if (tm.bad[b]) return INF;
+        for (int64_t r = 0; r < nc; ++r) {
+            if (w && w[c0 + r] == 0.0) continue;
+            s += R[r] * R[r];
         }
     }
     return s;
@@ -713,21 +784,109 @@ bool accumulate(int nb, int k, const double *w, const double *y, const double *p
     return true;
 }
 
+/* Rows [i0, i1) of J^T W J and J^T W r over a chunk of weighted rows
+   ([row][k + 1]: the Jacobian row, then the residual), in row order. Four
+   rows at a time: each accumulator is loaded once, takes the four rows'
+   products one after the other (the same additions in the same order as
+   row by row) and is stored once. A skipped (zero-weight) row is all zeros
+   and adds exact zeros, which leave every accumulator unchanged (none of
+   them can be -0). */
+__attribute__((target_clones("avx512f", "avx2", "default")))
+void accumulate_rows(int64_t nc, int k, int i0, int i1, const double *rows, double *jtj,
+                     double *jtr)
+{
+    const int k1 = k + 1;
+    int64_t r = 0;
+    for (; r + 4 <= nc; r += 4) {
+        const double *g0 = rows + (size_t)r * k1, *g1 = g0 + k1, *g2 = g1 + k1, *g3 = g2 + k1;
+        for (int i = i0; i < i1; ++i) {
+            double t = jtr[i];
+            t += g0[i] * g0[k];
+            t += g1[i] * g1[k];
+            t += g2[i] * g2[k];
+            t += g3[i] * g3[k];
+            jtr[i] = t;
+            const double a0 = g0[i], a1 = g1[i], a2 = g2[i], a3 = g3[i];
+            double *row = jtj + (size_t)i * k;
+            for (int j = 0; j <= i; ++j) {
+                double v = row[j];
+                v += a0 * g0[j];
+                v += a1 * g1[j];
+                v += a2 * g2[j];
+                v += a3 * g3[j];
+                row[j] = v;
+            }
+        }
+    }
+    for (; r < nc; ++r) {
+        const double *g = rows + (size_t)r * k1;
+        const double res = g[k];
+        for (int i = i0; i < i1; ++i) {
+            jtr[i] += g[i] * res;
+            double *row = jtj + (size_t)i * k;
+            const double gi = g[i];
+            for (int j = 0; j <= i; ++j) row[j] += gi * g[j];
+        }
+    }
+}
+
 /* J^T W J (lower triangle, then mirrored) and J^T W r at c, rows in order
    (fit.rs:1774-1827). False on a non-finite residual or Jacobian entry. */
 bool normal_equations(const Prog &p, const Data &d, const double *w, const double *c, int k,
-                      Work &wk, std::vector<double> &jtj, std::vector<double> &jtr)
+                      Team &tm, std::vector<double> &jtj, std::vector<double> &jtr)
 {
     jtj.assign((size_t)k * k, 0.0);
     jtr.assign(k, 0.0);
-    const double *root = wk.V.data() + (size_t)p.root * RB;
-    for (int64_t r0 = 0; r0 < d.n; r0 += RB) {
-        const int nb = (int)std::min<int64_t>(RB, d.n - r0);
-        forward<false>(p, d, r0, nb, c, wk.V.data(), wk.flat_plan());
-        backward(p, nb, wk.V.data(), wk.A.data(), wk.G.data());
-        if (!accumulate(nb, k, w ? w + r0 : nullptr, d.y + r0, root, wk.G.data(), jtj.data(),
-                        jtr.data()))
-            return false;
+    if (tm.nt == 1) {
+        Work &wk = tm.wk[0];
+        const double *root = wk.V.data() + (size_t)p.root * RB;
+        for (int64_t r0 = 0; r0 < d.n; r0 += RB) {
+            const int nb = (int)std::min<int64_t>(RB, d.n - r0);
+            forward<false>(p, d, r0, nb, c, wk.V.data(), tm.flat_plan());
+            backward(p, nb, wk.V.data(), wk.A.data(), wk.G.data());
+            if (!accumulate(nb, k, w ? w + r0 : nullptr, d.y + r0, root, wk.G.data(), jtj.data(),
+                            jtr.data()))
+                return false;
+        }
+    } else {
+        const int k1 = k + 1;
+        double *R = tm.rows.data();
+        for (int64_t c0 = 0; c0 < d.n; c0 += CH) {
+            const int64_t nc = std::min<int64_t>(CH, d.n - c0);
+            const int nblk = (int)((nc + RB - 1) / RB);
+#pragma omp parallel for num_threads(tm.nt) schedule(static)
+            for (int b = 0; b < nblk; ++b) {
+                Work &wk = tm.wk[thread_index()];
+                const int64_t r0 = c0 + (int64_t)b * RB;
+                const int nb = (int)std::min<int64_t>(RB, d.n - r0);
+                forward<false>(p, d, r0, nb, c, wk.V.data(), tm.flat_plan());
+                backward(p, nb, wk.V.data(), wk.A.data(), wk.G.data());
+                const double *root = wk.V.data() + (size_t)p.root * RB;
+                char fail = 0;
+                for (int r = 0; r < nb; ++r) {
+                    double *g = R + (size_t)(r0 - c0 + r) * k1;
+                    const double sw = w ? w[r0 + r] : 1.0;
+                    if (sw == 0.0) {
+                        for (int j = 0; j < k1; ++j) g[j] = 0.0;
+                        continue;
+                    }
+                    const double sq = std::sqrt(sw);
+                    const double res = sq * (root[r] - d.y[r0 + r]);
+                    if (!std::isfinite(res)) fail = 1;
+                    for (int j = 0; j < k; ++j) {
+                        g[j] = sq * wk.G[(size_t)j * RB + r];
+                        if (!std::isfinite(g[j])) fail = 1;
+                    }
+                    g[k] = res;
+                }
+                tm.bad[b] = fail;
+            }
+            for (int b = 0; b < nblk; ++b)
+                if (tm.bad[b]) return false;
+            /* the sums stay on this thread: split across threads, each would
+               stream the whole chunk, which costs more than it saves */
+            accumulate_rows(nc, k, 0, k, R, jtj.data(), jtr.data());
+        }
     }
     for (int i = 0; i < k; ++i)
         for (int j = 0; j < i; ++j) jtj[(size_t)j * k + i] = jtj[(size_t)i * k + j];
@@ -778,34 +937,34 @@ inline double clamp_c(double v)
    (fit.rs:2318-2336). */
 bool gn_trial(const Prog &p, const Data &d, const double *w, const std::vector<double> &c,
               double lambda, int k, const std::vector<double> &jtj, const std::vector<double> &jtr,
-              Work &wk, std::vector<double> &trial, double &tsse)
+              Team &tm, std::vector<double> &trial, double &tsse)
 {
     std::vector<double> rhs(k), step;
     for (int i = 0; i < k; ++i) rhs[i] = -jtr[i];
     if (!damped_solve(jtj, rhs, lambda, k, step)) return false;
     trial.resize(k);
     for (int i = 0; i < k; ++i) trial[i] = clamp_c(c[i] + step[i]);
-    tsse = sse(p, d, w, trial.data(), wk);
+    tsse = sse(p, d, w, trial.data(), tm);
     return true;
 }
 
 /* `fit_lm` (fit.rs:2534-2624): returns the weighted SSE at the best
    constants, which it leaves in c. */
 double fit_lm(const Prog &p, const Data &d, const double *w, int iters, std::vector<double> &c,
-              Work &wk)
+              Team &tm)
 {
     const int k = (int)p.cpos.size();
-    if (k == 0 || d.n == 0) return sse(p, d, w, nullptr, wk);
-    if (iters == 0) return sse(p, d, w, c.data(), wk);
+    if (k == 0 || d.n == 0) return sse(p, d, w, nullptr, tm);
+    if (iters == 0) return sse(p, d, w, c.data(), tm);
     std::vector<double> best_c = c, jtj, jtr, trial;
-    double best = sse(p, d, w, c.data(), wk);
+    double best = sse(p, d, w, c.data(), tm);
     double lambda = 1e-3;
     bool have = false;
     for (int it = 0; it < std::max(iters, 1); ++it) {
-        if (!have) have = normal_equations(p, d, w, c.data(), k, wk, jtj, jtr);
+        if (!have) have = normal_equations(p, d, w, c.data(), k, tm, jtj, jtr);
         if (!have) break;
         double tsse;
-        if (!gn_trial(p, d, w, c, lambda, k, jtj, jtr, wk, trial, tsse)) break;
+        if (!gn_trial(p, d, w, c, lambda, k, jtj, jtr, tm, trial, tsse)) break;
         if (tsse < best) {
             c = trial;
             best = tsse;
@@ -821,9 +980,9 @@ double fit_lm(const Prog &p, const Data &d, const double *w, int iters, std::vec
     /* the undamped Gauss-Newton polish */
     for (int it = 0; it < 4; ++it) {
         if (best == 0.0) break;
-        if (!normal_equations(p, d, w, best_c.data(), k, wk, jtj, jtr)) break;
+        if (!normal_equations(p, d, w, best_c.data(), k, tm, jtj, jtr)) break;
         double tsse;
-        if (!gn_trial(p, d, w, best_c, 0.0, k, jtj, jtr, wk, trial, tsse)) break;
+        if (!gn_trial(p, d, w, best_c, 0.0, k, jtj, jtr, tm, trial, tsse)) break;
         if (tsse < best) {
             best_c = trial;
             best = tsse;
@@ -837,13 +996,16 @@ double fit_lm(const Prog &p, const Data &d, const double *w, int iters, std::vec
 
 /* ---- predictions and scores ------------------------------------------------ */
 
-void predict(const Prog &p, const Data &d, const double *c, Work &wk, double *out)
+void predict(const Prog &p, const Data &d, const double *c, Team &tm, double *out)
 {
-    const double *root = wk.V.data() + (size_t)p.root * RB;
-    for (int64_t r0 = 0; r0 < d.n; r0 += RB) {
+    const int64_t nblk = (d.n + RB - 1) / RB;
+#pragma omp parallel for num_threads(tm.nt) schedule(static) if (tm.nt > 1)
+    for (int64_t b = 0; b < nblk; ++b) {
+        Work &wk = tm.wk[tm.nt > 1 ? thread_index() : 0];
+        const int64_t r0 = b * RB;
         const int nb = (int)std::min<int64_t>(RB, d.n - r0);
         forward<true>(p, d, r0, nb, c, wk.V.data());
-        std::memcpy(out + r0, root, sizeof(double) * (size_t)nb);
+        std::memcpy(out + r0, wk.V.data() + (size_t)p.root * RB, sizeof(double) * (size_t)nb);
     }
 }
 
@@ -884,7 +1046,7 @@ double score(const double *pred, const Data &d, int metric)
    weights from the current residuals, a short weighted LM, kept only while
    the configured objective falls; then one longer weighted LM at the final
    weights, kept if it improves. */
-double irls(const Prog &p, const Data &d, int iters, int metric, std::vector<double> &c, Work &wk)
+double irls(const Prog &p, const Data &d, int iters, int metric, std::vector<double> &c, Team &tm)
 {
     const int64_t n = d.n;
     std::vector<double> pred((size_t)std::max<int64_t>(n, 1)), wts((size_t)std::max<int64_t>(n, 1));
@@ -899,20 +1061,20 @@ double irls(const Prog &p, const Data &d, int iters, int metric, std::vector<dou
             wts[i] = base > 0.0 ? base * std::max(weight_of(r), 0.0) : 0.0;
         }
     };
-    predict(p, d, c.data(), wk, pred.data());
+    predict(p, d, c.data(), tm, pred.data());
     double best = score(pred.data(), d, metric);
     if (!std::isfinite(best)) return best;
     const int rounds = iters < 1 ? 1 : (iters > 4 ? 4 : iters);
     const int inner = std::max(iters / rounds, 1);
     std::vector<double> trial;
     for (int round = 0; round < rounds; ++round) {
-        predict(p, d, c.data(), wk, pred.data());
+        predict(p, d, c.data(), tm, pred.data());
         for (int64_t i = 0; i < n; ++i)
             if (!std::isfinite(pred[i] - d.y[i])) return best;
         set_weights();
         trial = c;
-        fit_lm(p, d, wts.data(), inner, trial, wk);
-        predict(p, d, trial.data(), wk, pred.data());
+        fit_lm(p, d, wts.data(), inner, trial, tm);
+        predict(p, d, trial.data(), tm, pred.data());
         const double s = score(pred.data(), d, metric);
         if (std::isfinite(s) && s < best) {
             best = s;
@@ -921,14 +1083,14 @@ double irls(const Prog &p, const Data &d, int iters, int metric, std::vector<dou
             break;
         }
     }
-    predict(p, d, c.data(), wk, pred.data());
+    predict(p, d, c.data(), tm, pred.data());
     bool all = true;
     for (int64_t i = 0; i < n; ++i) all = all && std::isfinite(pred[i]);
     if (all) {
         set_weights();
         trial = c;
-        fit_lm(p, d, wts.data(), std::max(iters, 4), trial, wk);
-        predict(p, d, trial.data(), wk, pred.data());
+        fit_lm(p, d, wts.data(), std::max(iters, 4), trial, tm);
+        predict(p, d, trial.data(), tm, pred.data());
         const double s = score(pred.data(), d, metric);
         if (std::isfinite(s) && s < best) {
             best = s;
@@ -946,24 +1108,24 @@ bool covered(int metric)
 
 /* One finalist: `fit_weighted_metric` for the covered metrics. */
 double refit_one(const int *ops, double *vals, int nn, const Data &d, int iters, int metric,
-                 size_t cache_cap)
+                 size_t cache_cap, int threads)
 {
     Prog p;
     if (!load(ops, vals, nn, p)) return NaN;
     std::vector<double> c(p.cpos.size());
     for (size_t s = 0; s < c.size(); ++s) c[s] = vals[p.cpos[s]];
-    Work wk(p);
-    if (iters > 0) plan_cache(p, d, cache_cap, wk);
+    Team tm(p, threads);
+    if (iters > 0) plan_cache(p, d, cache_cap, tm);
     const bool lsq = metric != MT_ABSOLUTE && metric != MT_LOG_SQUASHED;
     double r;
     if (lsq) {
-        r = fit_lm(p, d, d.w, iters, c, wk);
+        r = fit_lm(p, d, d.w, iters, c, tm);
     } else if (iters == 0) {
         std::vector<double> pred((size_t)std::max<int64_t>(d.n, 1));
-        predict(p, d, c.data(), wk, pred.data());
+        predict(p, d, c.data(), tm, pred.data());
         r = score(pred.data(), d, metric);
     } else {
-        r = irls(p, d, iters, metric, c, wk);
+        r = irls(p, d, iters, metric, c, tm);
     }
     for (size_t s = 0; s < c.size(); ++s) vals[p.cpos[s]] = c[s];
     return r;
@@ -985,9 +1147,16 @@ int rch_refit_finalists(const int32_t *ops, double *vals, const int32_t *tree_of
         if (tree_off[t + 1] < tree_off[t]) return -1;
     const Data d{cols, n, nvars, y, w};
     int nt = threads > 0 ? threads : (int)std::thread::hardware_concurrency();
-    nt = std::max(1, std::min(nt, ntrees));
+    nt = std::max(1, nt);
+    /* Teams of `team` threads refit finalists concurrently: with at least as
+       many finalists as threads every refit runs on one thread; with fewer,
+       each refit splits its passes by rows over its team (its sums stay in
+       row order). Few rows do not pay for a team. The bits are the same
+       either way. */
+    const int team = n >= 16384 ? std::max(1, nt / ntrees) : 1;
+    const int teams = std::max(1, std::min(ntrees, nt / team));
     /* the subtree caches of the fits in flight share 2 GiB */
-    const size_t cap = std::max<size_t>((size_t)16 << 20, ((size_t)2 << 30) / (size_t)nt);
+    const size_t cap = std::max<size_t>((size_t)16 << 20, ((size_t)2 << 30) / (size_t)teams);
     /* largest first (nodes x (constants + 1)), so the pool ends together */
     std::vector<int> order(ntrees);
     std::vector<long> work(ntrees);
@@ -1003,15 +1172,15 @@ int rch_refit_finalists(const int32_t *ops, double *vals, const int32_t *tree_of
         for (int q = next.fetch_add(1); q < ntrees; q = next.fetch_add(1)) {
             const int t = order[q];
             const int b = tree_off[t], e = tree_off[t + 1];
-            loss[t] = refit_one(ops + b, vals + b, e - b, d, iters, metric, cap);
+            loss[t] = refit_one(ops + b, vals + b, e - b, d, iters, metric, cap, team);
         }
     };
-    if (nt == 1) {
+    if (teams == 1) {
         worker();
     } else {
         std::vector<std::thread> pool;
-        pool.reserve(nt);
-        for (int i = 0; i < nt; ++i) pool.emplace_back(worker);
+        pool.reserve(teams);
+        for (int i = 0; i < teams; ++i) pool.emplace_back(worker);
         for (std::thread &th : pool) th.join();
     }
     return 0;
@@ -1025,8 +1194,8 @@ int rch_soa_eval(const int32_t *ops, const double *vals, int nn, const double *c
     Prog p;
     if (!ops || !vals || nn <= 0 || !load(ops, vals, nn, p)) return -1;
     const Data d{cols, n, nvars, nullptr, nullptr};
-    Work wk(p);
-    predict(p, d, nullptr, wk, out);
+    Team tm(p, 1);
+    predict(p, d, nullptr, tm, out);
     return 0;
 }
 
