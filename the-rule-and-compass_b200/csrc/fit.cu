@@ -411,7 +411,9 @@ __global__ void __launch_bounds__(T) ft_sweep(FitArgs a, int q)
 /* ---- four-rows-per-thread sweeps ------------------------------------- */
 
 #define FT_ASM_T 128
+#ifndef FT_ASM_BUDGET
 #define FT_ASM_BUDGET (40 * 1024)
+#endif
 
 /* Rows per thread of each sweep: the assemblies carry 8 bytes of rows per
    thread (two f32 or one f64 row) to fit more threads beside their tapes;
@@ -2400,7 +2402,7 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
             ok = cudaGetLastError() == cudaSuccess;
         }
     } else {
-        char key[256];
+        char key[512];
         snprintf(key, sizeof(key), "%p|%d|%d|%d|%d|%d|%d|%d|%d|%d|%zu|%d|%d|%d|%zu", (void *)dev,
                  nprog, kmax, ntiles, b.mmax, Wmax, iters, metric, flags, steps, io_end, b.fslots,
                  b.ftape, b.fmaxins, b.asm_region);
