@@ -122,6 +122,8 @@ struct FitArgs {
     int mmax;
     int ijac_small;        /* implicit: programs of at most this many records take the
                               short Jacobian launch (FOP_IJACS); 0: one launch */
+    int ijac_tape;         /* internal-node tape slots of the Jacobian launch */
+    int ijac_tape_small;   /* ... and of the short one */
     int Wmax;
     int nprog;
     FitState *state;
@@ -162,15 +164,14 @@ __host__ __device__ inline size_t ft_rows_bytes(int Wmax, int T)
 /* Threads of the implicit sweeps: every thread carries one row. */
 #define FT_ITHREADS 64
 
-/* Dynamic shared memory of an implicit sweep kernel: records, constants
-   (f64 and f32), the f64 tape ([node][T]; two for the Jacobian), the
-   Jacobian row buffer for the assembling kind, and a reduction buffer. */
-__host__ __device__ inline size_t ft_sweep_smem(int opk, int mmax, int Wmax, int T)
+/* Dynamic shared memory of an exact-Jacobian sweep: the compact records
+   and their reference scratch for `mrec` records, the constants, the two
+   f64 tapes ([slot][T], `tcap` internal-node slots each), the Jacobian row
+   buffer and a reduction buffer. */
+__host__ __device__ inline size_t ft_ijac_smem(int mrec, int tcap, int Wmax, int T)
 {
-    size_t s = 16 * (size_t)mmax + 16 * FT_MAX_CONST +
-               8 * (size_t)mmax * T * (ft_op_ijac(opk) ? 2 : 1);
-    if (ft_op_assembles(opk)) s += ft_rows_bytes(Wmax, T);
-    return s + 8 * (size_t)T;
+    return 16 * (size_t)mrec + 16 * (size_t)((mrec + 3) / 4) + 8 * (size_t)FT_MAX_CONST +
+           16 * (size_t)tcap * T + ft_rows_bytes(Wmax, T) + 8 * (size_t)T;
 }
 
 /* Fixed-order reduction of the per-thread SYRK blocks over the row groups,
@@ -195,12 +196,13 @@ __device__ __forceinline__ void ft_tile_gram_out(const Syrk &sy, const double ac
 }
 
 /* Implicit metric of one tile (implicit.rs:156-174, :302-333): the cost
-   sum w d^2 at `cd`, and with JAC the Jacobian rows of sqrt(w) d (exact,
+   sum w d^2 at `cd`, the Jacobian rows of sqrt(w) d (exact,
    forward-over-reverse, where the reference takes central differences
    with h = 1e-6 (1 + |c_j|)) and their J^T J / J^T r. An undefined row
-   marks the tile bad. `tan64` is the second f64 tape of the Jacobian. */
-template <int T, bool JAC>
-__device__ void ft_tile_implicit(const FitArgs &a, const uint4 *rec, int m, int p,
+   marks the tile bad. `rec` holds the ni compact records of ij_compact;
+   `tape64` and `tan64` are the two f64 tapes. */
+template <int T>
+__device__ void ft_tile_implicit(const FitArgs &a, const uint4 *rec, int ni, int p,
                                  const double *cd, double *tape64, double *tan64, double *rows,
                                  double *red, int r0, int r1, double *pt)
 {
@@ -219,8 +221,7 @@ __device__ void ft_tile_implicit(const FitArgs &a, const uint4 *rec, int m, int 
     for (int base = r0; base < r1; base += TS) {
         const int row = base + tid;
         if (tid < TS) {
-            if (JAC)
-                for (int j = 0; j < W; ++j) myrow[j] = 0.0;
+            for (int j = 0; j < W; ++j) myrow[j] = 0.0;
             const double wr = (row < r1 && a.w) ? a.w[row] : 1.0;
             if (row < r1 && !(isfinite(wr) && wr >= 0.0)) bad = 1;
             else if (row < r1 && wr > 0.0) {
@@ -228,29 +229,25 @@ __device__ void ft_tile_implicit(const FitArgs &a, const uint4 *rec, int m, int 
                     x[k] = k < a.v ? a.cols64[(size_t)k * a.npad + row] : 0.0;
                 double d;
                 const double sw = sqrt(wr);
-                const bool ok = JAC ? ft_implicit_jac<TS>(rec, m, x, a.v, cd, p, sw, tp,
-                                                          tan64 + tid, d, myrow)
-                                    : ft_implicit_d<TS>(rec, m, x, a.v, cd, tp, d);
+                const bool ok =
+                    ft_implicit_jac<TS>(rec, ni, x, a.v, cd, p, sw, tp, tan64 + tid, d, myrow);
                 if (!ok) {
                     bad = 1;
-                    if (JAC)
-                        for (int j = 0; j < p; ++j) myrow[j] = 0.0;
+                    for (int j = 0; j < p; ++j) myrow[j] = 0.0;
                 } else {
                     const double r = sw * d;
                     cost += r * r;
-                    if (JAC) myrow[p] = r;
+                    myrow[p] = r;
                 }
             }
         }
-        if (JAC) {
-            __syncthreads();
-            ft_syrk_chunk(sy, rows, W, TS, acc);
-            __syncthreads();
-        }
+        __syncthreads();
+        ft_syrk_chunk(sy, rows, W, TS, acc);
+        __syncthreads();
     }
     bad = __syncthreads_or(bad);
     cost = ft_block_sum<T>(cost, red);
-    if (JAC) ft_tile_gram_out<T>(sy, acc, rows, pt);
+    ft_tile_gram_out<T>(sy, acc, rows, pt);
     if (tid == 0) {
         pt[FT_PART_LOSS] = cost;
         pt[FT_PART_BAD] = bad ? 1.0 : 0.0;
@@ -319,12 +316,14 @@ __device__ void ft_tile_icost_x(const FitArgs &a, const FIns *fwd, int nf, int n
     }
 }
 
-/* One sweep kind over every queued (candidate, tile) item of step parity q. */
+/* The implicit cost sweep over every queued (candidate, tile) item of step
+   parity q. */
 template <int OPK, int T>
 __global__ void __launch_bounds__(T) ft_sweep(FitArgs a, int q)
 {
     extern __shared__ __align__(16) unsigned char sm[];
-    if constexpr (OPK == FOP_ICOST) {
+    static_assert(OPK == FOP_ICOST, "ft_sweep runs the cost kind");
+    {
         /* [instructions | constants | spill slots | tape | input gradients | reduction] */
         using V4 = FiV<double, 1>::V4;
         FIns *ins = reinterpret_cast<FIns *>(sm);
@@ -360,19 +359,27 @@ __global__ void __launch_bounds__(T) ft_sweep(FitArgs a, int q)
             ft_tile_icost_x<T>(a, ins, info.x, info.y, cd, stk, tape, ig, red, r0, r1, pt);
             __syncthreads();
         }
-        return;
     }
-    /* the short Jacobian launch is laid out for its own record bound */
+}
+
+/* The exact-Jacobian sweep (FOP_IJAC, or FOP_IJACS for the short programs)
+   over every queued (candidate, tile) item of step parity q: eight 64-thread
+   blocks per SM fit beside the compact tapes, so registers are held to
+   that. The short launch is laid out for its own record and tape bounds. */
+template <int OPK, int T>
+__global__ void __launch_bounds__(T, 8) ft_jac_sweep(FitArgs a, int q)
+{
+    extern __shared__ __align__(16) unsigned char sm[];
     const int mcap = OPK == FOP_IJACS ? a.ijac_small : a.mmax;
+    const int tcap = OPK == FOP_IJACS ? a.ijac_tape_small : a.ijac_tape;
     uint4 *rec = reinterpret_cast<uint4 *>(sm);
-    double *cd = reinterpret_cast<double *>(sm + 16 * (size_t)mcap);
-    float *cf = reinterpret_cast<float *>(cd + FT_MAX_CONST);
-    float *tape = cf + 2 * FT_MAX_CONST;
-    double *tape64 = reinterpret_cast<double *>(tape);
-    double *tan64 = tape64 + (size_t)mcap * T;
-    double *rows = tape64 + (size_t)mcap * T * (ft_op_ijac(OPK) ? 2 : 1);
-    double *red = rows + (ft_op_assembles(OPK) ? ft_rows_bytes(a.Wmax, T) / 8 : 0);
-    __shared__ int s_item;
+    unsigned *refs = reinterpret_cast<unsigned *>(sm + 16 * (size_t)mcap);
+    double *cd = reinterpret_cast<double *>(sm + 16 * (size_t)mcap + 16 * (size_t)((mcap + 3) / 4));
+    double *tape64 = cd + FT_MAX_CONST;
+    double *tan64 = tape64 + (size_t)tcap * T;
+    double *rows = tan64 + (size_t)tcap * T;
+    double *red = rows + ft_rows_bytes(a.Wmax, T) / 8;
+    __shared__ int s_item, s_ni;
     const int tid = threadIdx.x;
     const int *list = a.lists + ((size_t)q * FOP_COUNT + OPK) * a.nprog;
     const int total = a.counts[q * FOP_COUNT + OPK] * a.ntiles;
@@ -391,19 +398,14 @@ __global__ void __launch_bounds__(T) ft_sweep(FitArgs a, int q)
         const int p = a.pcount[cand];
         const int sel = st->sel;
         for (int i = tid; i < m; i += T) rec[i] = a.rec[nb + i];
-        if (tid < p) {
-            const double cv = sel ? st->trial[tid] : st->c[tid];
-            cd[tid] = cv;
-            cf[tid] = (float)cv;
-        }
+        if (tid < p) cd[tid] = sel ? st->trial[tid] : st->c[tid];
+        __syncthreads();
+        if (tid == 0) s_ni = ij_compact(rec, m, refs);
         __syncthreads();
         const int r0 = tile * FT_TILE_ROWS;
         const int r1 = min(a.n, r0 + FT_TILE_ROWS);
         double *pt = a.part + ((size_t)cand * a.ntiles + tile) * FT_PART_STRIDE;
-        if (ft_op_ijac(OPK))
-            ft_tile_implicit<T, true>(a, rec, m, p, cd, tape64, tan64, rows, red, r0, r1, pt);
-        else
-            ft_tile_implicit<T, false>(a, rec, m, p, cd, tape64, tan64, rows, red, r0, r1, pt);
+        ft_tile_implicit<T>(a, rec, s_ni, p, cd, tape64, tan64, rows, red, r0, r1, pt);
         __syncthreads();
     }
 }
@@ -1909,6 +1911,7 @@ void prep_batch(const unsigned int *off, const unsigned int *prog, const int *pc
 {
     b.node_off.resize(nprog + 1);
     b.valid.resize(nprog);
+    b.ninternal.assign(nprog, 0);
     for (int i = 0; i <= nprog; ++i) b.node_off[i] = (int)(off[i] / 4);
     for (int i = 0; i < nprog; ++i) {
         const int m = b.node_off[i + 1] - b.node_off[i];
@@ -1919,6 +1922,12 @@ void prep_batch(const unsigned int *off, const unsigned int *prog, const int *pc
         if (ok) {
             b.mmax = std::max(b.mmax, m);
             b.pmax = std::max(b.pmax, p);
+            int ni = 0;
+            for (int r = 0; r < m; ++r) {
+                const uint32_t op = prog[off[i] + 4 * r];
+                ni += op != OP_CONST && op != OP_VAR;
+            }
+            b.ninternal[i] = ni;
         }
     }
     /* the four-row stack machine's translation (a tree not in stack order is
@@ -2092,11 +2101,11 @@ SweepLaunch icost_launch(RcCtx *c, const XPrep &x)
 }
 
 template <int OPK>
-SweepLaunch sweep_launch(RcCtx *c, int mmax, int Wmax)
+SweepLaunch sweep_launch(RcCtx *c, int mrec, int tcap, int Wmax)
 {
     SweepLaunch s;
-    s.fn = (const void *)ft_sweep<OPK, FT_ITHREADS>;
-    s.smem = ft_sweep_smem(OPK, mmax, Wmax, FT_ITHREADS);
+    s.fn = (const void *)ft_jac_sweep<OPK, FT_ITHREADS>;
+    s.smem = ft_ijac_smem(mrec, tcap, Wmax, FT_ITHREADS);
     if (s.smem > 48 * 1024)
         cudaFuncSetAttribute(s.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
     s.grid = c->sm_count * occupancy(s.fn, FT_ITHREADS, s.smem);
@@ -2104,50 +2113,66 @@ SweepLaunch sweep_launch(RcCtx *c, int mmax, int Wmax)
     return s;
 }
 
-/* The record bound of the short Jacobian launch: the Jacobian sweep keeps
-   two f64 tapes per row in shared memory, sized for the longest program of
-   the launch, so one launch sized for the batch's longest program runs the
-   short ones at that program's occupancy. Estimate each split's time as the
-   records swept over the resident blocks each launch allows and take the
-   best, if it saves at least 5 %; 0 keeps one launch. The split depends on
-   the batch, but a candidate's arithmetic does not depend on which launch
-   runs it. */
-int ijac_split(RcCtx *c, const FitPrep &b, int Wmax)
+/* The tape bound of the Jacobian launch (the most internal nodes of the
+   batch) and the record and tape bounds of the short launch. The sweep
+   keeps two f64 tapes per row in shared memory, one slot per internal
+   node, sized for the largest program of the launch, so one launch sized
+   for the batch runs the short programs at the largest one's occupancy.
+   Each split (programs of at most t records to the short launch) is
+   estimated as the internal nodes swept over the resident blocks each
+   launch allows; the best is kept if it saves at least 5 %, else `small`
+   is 0 and one launch serves all. The split depends on the batch, but a
+   candidate's arithmetic does not depend on which launch runs it. */
+struct IjacSplit {
+    int tape = 1, small = 0, tape_small = 1;
+};
+
+IjacSplit ijac_split(RcCtx *c, const FitPrep &b, int Wmax)
 {
-    const void *fn = (const void *)ft_sweep<FOP_IJACS, FT_ITHREADS>;
+    IjacSplit out;
+    std::vector<std::pair<int, int>> ms; /* (records, internal nodes) */
+    for (size_t i = 0; i + 1 < b.node_off.size(); ++i)
+        if (b.valid[i]) {
+            ms.emplace_back(b.node_off[i + 1] - b.node_off[i], b.ninternal[i]);
+            out.tape = std::max(out.tape, b.ninternal[i]);
+        }
+    if (ms.size() < 2) return out;
+    const void *fn = (const void *)ft_jac_sweep<FOP_IJACS, FT_ITHREADS>;
     /* occupancy queries up to the largest layout the split can choose */
-    const size_t smax = ft_sweep_smem(FOP_IJAC, b.mmax, Wmax, FT_ITHREADS);
+    const size_t smax = ft_ijac_smem(b.mmax, out.tape, Wmax, FT_ITHREADS);
     if (smax > 48 * 1024 &&
         cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax) !=
             cudaSuccess) {
         cudaGetLastError();
-        return 0;
+        return out;
     }
-    std::vector<int> ms;
-    for (size_t i = 0; i + 1 < b.node_off.size(); ++i)
-        if (b.valid[i]) ms.push_back(b.node_off[i + 1] - b.node_off[i]);
-    if (ms.size() < 2) return 0;
     std::sort(ms.begin(), ms.end());
-    auto occ = [&](int m) {
-        return (double)occupancy(fn, FT_ITHREADS, ft_sweep_smem(FOP_IJAC, m, Wmax, FT_ITHREADS));
+    auto occ = [&](int mrec, int tcap) {
+        return (double)occupancy(fn, FT_ITHREADS, ft_ijac_smem(mrec, tcap, Wmax, FT_ITHREADS));
     };
     double total = 0.0;
-    for (int m : ms) total += m;
-    const double big = occ(b.mmax);
+    for (const auto &e : ms) total += e.second + 1;
+    const double big = occ(b.mmax, out.tape);
     const double one = total / big;
     double best = one, below = 0.0;
-    int pick = 0;
+    int tmax = 1;
     for (size_t i = 0; i < ms.size(); ++i) {
-        below += ms[i];
-        if (ms[i] >= b.mmax) break;
-        if (i + 1 < ms.size() && ms[i + 1] == ms[i]) continue;
-        const double cost = below / occ(ms[i]) + (total - below) / big;
+        below += ms[i].second + 1;
+        tmax = std::max(tmax, ms[i].second);
+        if (ms[i].first >= b.mmax) break;
+        if (i + 1 < ms.size() && ms[i + 1].first == ms[i].first) continue;
+        const double cost = below / occ(ms[i].first, tmax) + (total - below) / big;
         if (cost < best) {
             best = cost;
-            pick = ms[i];
+            out.small = ms[i].first;
+            out.tape_small = tmax;
         }
     }
-    return best <= 0.95 * one ? pick : 0;
+    if (!(best <= 0.95 * one)) {
+        out.small = 0;
+        out.tape_small = 1;
+    }
+    return out;
 }
 
 template <int OPK, int T>
@@ -2351,11 +2376,14 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     SweepLaunch sw[4];
     int nk = 0;
     if (metric == FM_IMPLICIT) {
-        a.ijac_small = ijac_split(c, b, Wmax);
+        const IjacSplit js = ijac_split(c, b, Wmax);
+        a.ijac_small = js.small;
+        a.ijac_tape = js.tape;
+        a.ijac_tape_small = js.tape_small;
         if (a.ijac_small > 0) {
-            sw[nk] = sweep_launch<FOP_IJACS>(c, a.ijac_small, Wmax); ++nk;
+            sw[nk] = sweep_launch<FOP_IJACS>(c, a.ijac_small, a.ijac_tape_small, Wmax); ++nk;
         }
-        sw[nk] = sweep_launch<FOP_IJAC>(c, b.mmax, Wmax); ++nk;
+        sw[nk] = sweep_launch<FOP_IJAC>(c, b.mmax, a.ijac_tape, Wmax); ++nk;
         sw[nk] = icost_launch(c, xp); ++nk;
     } else if (corr) {
         sw[nk] = sweep4_launch<FOP_CASM, FT_ASM_T>(c, b, Wmax); ++nk;
@@ -2407,9 +2435,9 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
                  nprog, kmax, ntiles, b.mmax, Wmax, iters, metric, flags, steps, io_end, b.fslots,
                  b.ftape, b.fmaxins, b.asm_region);
         const size_t kl = strlen(key);
-        snprintf(key + kl, sizeof(key) - kl, "|%d|%d|%d|%d|%d|%d|%d|%d|%d", b.ncache, a.nsub,
-                 b.sub_slots, b.sub_maxins, xp.maxins, xp.slots, xp.tape, use64 ? 1 : 0,
-                 a.ijac_small);
+        snprintf(key + kl, sizeof(key) - kl, "|%d|%d|%d|%d|%d|%d|%d|%d|%d|%d|%d", b.ncache,
+                 a.nsub, b.sub_slots, b.sub_maxins, xp.maxins, xp.slots, xp.tape, use64 ? 1 : 0,
+                 a.ijac_small, a.ijac_tape, a.ijac_tape_small);
         if (!c->fit_graph || c->fit_graph_key != key) {
             if (c->fit_graph) {
                 cudaGraphExecDestroy(c->fit_graph);

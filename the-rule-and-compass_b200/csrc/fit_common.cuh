@@ -524,6 +524,74 @@ __device__ __forceinline__ bool ft_implicit_d(const uint4 *rec, int m, const dou
     return isfinite(d);
 }
 
+/* Child references of the compact records the Jacobian sweep runs over:
+   an internal node's tape slot, or a tagged leaf (an input column or a
+   constant slot) whose value and tangent are read from the row's inputs,
+   the constants and the input gradient instead of being taped. */
+#define IJ_LEAF 0x80000000u
+#define IJ_CONST 0x40000000u
+#define IJ_INDEX 0x0000ffffu
+
+/* Compact a candidate's fit records in place for the Jacobian sweep: the
+   internal nodes only, in post-order (record k is tape slot k), each child
+   a tape slot or a tagged leaf; `ref` is scratch for m entries. Run by one
+   thread. Returns the number of internal records (0 for a lone leaf). */
+__device__ __forceinline__ int ij_compact(uint4 *rec, int m, unsigned *ref)
+{
+    int k = 0;
+    for (int i = 0; i < m; ++i) {
+        const uint4 r = rec[i];
+        if (r.x == OP_CONST) {
+            ref[i] = IJ_LEAF | IJ_CONST | r.w;
+        } else if (r.x == OP_VAR) {
+            ref[i] = IJ_LEAF | r.w;
+        } else {
+            rec[k] = make_uint4(r.x, ref[r.y], ft_op_binary(r.x) ? ref[r.z] : 0u, 0u);
+            ref[i] = (unsigned)k++;
+        }
+    }
+    return k;
+}
+
+template <int TS>
+__device__ __forceinline__ double ij_val(unsigned ref, const double *vt, const double *x,
+                                         const double *c)
+{
+    if (ref & IJ_LEAF) return (ref & IJ_CONST) ? c[ref & IJ_INDEX] : x[ref & IJ_INDEX];
+    return vt[ref * TS];
+}
+
+/* A leaf's tangent along x' = g: g[col] for an input, 0 for a constant. */
+template <int TS>
+__device__ __forceinline__ double ij_tan(unsigned ref, const double *tt,
+                                         const double (&ig)[FT_IMPLICIT_MAXV])
+{
+    if (!(ref & IJ_LEAF)) return tt[ref * TS];
+    if (ref & IJ_CONST) return 0.0;
+    double t = 0.0;
+#pragma unroll
+    for (int k = 0; k < FT_IMPLICIT_MAXV; ++k)
+        if ((int)(ref & IJ_INDEX) == k) t = ig[k];
+    return t;
+}
+
+/* Hand a first-order adjoint to a child: an internal child's tape slot, a
+   constant's Jacobian entry, an input's gradient. */
+template <int TS>
+__device__ __forceinline__ void ij_put(unsigned ref, double v, double *tt, double *jrow,
+                                       double (&ig)[FT_IMPLICIT_MAXV])
+{
+    if (!(ref & IJ_LEAF)) {
+        tt[ref * TS] = v;
+    } else if (ref & IJ_CONST) {
+        jrow[ref & IJ_INDEX] += v;
+    } else {
+#pragma unroll
+        for (int k = 0; k < FT_IMPLICIT_MAXV; ++k)
+            if ((int)(ref & IJ_INDEX) == k) ig[k] += v;
+    }
+}
+
 /* The implicit residual of one row and its exact Jacobian row (f64):
    d = f / ||g||, g = grad_x f, and for each constant
      dd/dc_j = (df/dc_j) / ||g|| - f (g . dg/dc_j) / ||g||^3,
@@ -540,43 +608,48 @@ __device__ __forceinline__ bool ft_implicit_d(const uint4 *rec, int m, const dou
    jrow[j] receives sqrt(w_row) dd/dc_j for j < p. Returns false when the
    row is undefined (non-finite value, gradient or Jacobian entry, or a
    zero gradient): the same rows ft_implicit_d rejects, plus a non-finite
-   Jacobian entry. */
+   Jacobian entry. The sweeps run over the compact records of ij_compact:
+   only internal nodes own tape slots (about half of a tree's nodes), so
+   both tapes take half the shared memory; a leaf's adjoint is applied to
+   its gradient entry when its parent is processed (for an input shared by
+   several leaves that changes the order of its gradient's additions, not
+   the sum's meaning). */
 template <int TS>
-__device__ bool ft_implicit_jac(const uint4 *rec, int m, const double *x, int v, const double *c,
+__device__ bool ft_implicit_jac(const uint4 *ir, int ni, const double *x, int v, const double *c,
                                 int p, double sw, double *vt, double *tt, double &d, double *jrow)
 {
-    const double fv = ft_fwd_d_x<TS>(rec, m, x, c, vt);
+    /* a lone constant has no gradient; a lone input holds no constant */
+    if (ni == 0) return false;
+    /* 1: values of the internal nodes */
+    double fv = 0.0;
+    for (int k = 0; k < ni; ++k) {
+        const uint4 r = ir[k];
+        const double a = ij_val<TS>(r.y, vt, x, c);
+        const double b = ft_op_binary(r.x) ? ij_val<TS>(r.z, vt, x, c) : 0.0;
+        fv = ft_value_d(r.x, a, b);
+        vt[k * TS] = fv;
+    }
     if (!isfinite(fv)) return false;
     for (int j = 0; j < p; ++j) jrow[j] = 0.0;
     double ig[FT_IMPLICIT_MAXV];
 #pragma unroll
     for (int k = 0; k < FT_IMPLICIT_MAXV; ++k) ig[k] = 0.0;
-    tt[(m - 1) * TS] = 1.0;
-    for (int i = m - 1; i >= 0; --i) {
-        const uint4 r = rec[i];
-        const double a = tt[i * TS];
-        if (r.x == OP_CONST) {
-            jrow[r.w] += a;
-            continue;
-        }
-        if (r.x == OP_VAR) {
-#pragma unroll
-            for (int k = 0; k < FT_IMPLICIT_MAXV; ++k)
-                if ((int)r.w == k) ig[k] += a;
-            continue;
-        }
-        const bool bin = ft_op_binary(r.x);
-        const double xx = vt[r.y * TS];
-        if (!bin) {
+    /* 2: reverse; a leaf's adjoint goes straight to its gradient entry */
+    tt[(ni - 1) * TS] = 1.0;
+    for (int k = ni - 1; k >= 0; --k) {
+        const uint4 r = ir[k];
+        const double a = tt[k * TS];
+        const double xx = ij_val<TS>(r.y, vt, x, c);
+        if (!ft_op_binary(r.x)) {
             /* a unary node's own partial goes to its (now consumed) slot for
                the tangent pass */
             double d0, d1;
             ft_partials_d(r.x, xx, 0.0, d0, d1);
-            tt[r.y * TS] = a != 0.0 ? a * d0 : 0.0;
-            tt[i * TS] = d0;
+            ij_put<TS>(r.y, a != 0.0 ? a * d0 : 0.0, tt, jrow, ig);
+            tt[k * TS] = d0;
             continue;
         }
-        const double yy = vt[r.z * TS];
+        const double yy = ij_val<TS>(r.z, vt, x, c);
         double c0 = 0.0, c1 = 0.0;
         if (a != 0.0 && !(r.x == OP_POW && !(xx > 0.0))) {
             double d0, d1;
@@ -584,8 +657,8 @@ __device__ bool ft_implicit_jac(const uint4 *rec, int m, const double *x, int v,
             c0 = a * d0;
             c1 = a * d1;
         }
-        tt[r.y * TS] = c0;
-        tt[r.z * TS] = c1;
+        ij_put<TS>(r.y, c0, tt, jrow, ig);
+        ij_put<TS>(r.z, c1, tt, jrow, ig);
     }
     double nsq = 0.0;
     for (int k = 0; k < FT_IMPLICIT_MAXV; ++k) {
@@ -599,44 +672,36 @@ __device__ bool ft_implicit_jac(const uint4 *rec, int m, const double *x, int v,
     if (!isfinite(d)) return false;
     /* 3: tangents along x' = g over the stored values (a node's adjoint in
        tt is replaced by its tangent; its children's are tangents already) */
-    for (int i = 0; i < m; ++i) {
-        const uint4 r = rec[i];
+    for (int k = 0; k < ni; ++k) {
+        const uint4 r = ir[k];
         double tan = 0.0;
-        if (r.x == OP_VAR) {
-#pragma unroll
-            for (int k = 0; k < FT_IMPLICIT_MAXV; ++k)
-                if ((int)r.w == k) tan = ig[k];
-        } else if (r.x == OP_CONST) {
-        } else if (!ft_op_binary(r.x)) {
-            const double ta = tt[r.y * TS];
-            if (ta != 0.0) tan = ft_mul0(ta, tt[i * TS]) + 0.0;
+        if (!ft_op_binary(r.x)) {
+            const double ta = ij_tan<TS>(r.y, tt, ig);
+            if (ta != 0.0) tan = ft_mul0(ta, tt[k * TS]) + 0.0;
         } else {
-            const double a = vt[r.y * TS], ta = tt[r.y * TS];
-            const double b = vt[r.z * TS], tb = tt[r.z * TS];
+            const double a = ij_val<TS>(r.y, vt, x, c), ta = ij_tan<TS>(r.y, tt, ig);
+            const double b = ij_val<TS>(r.z, vt, x, c), tb = ij_tan<TS>(r.z, tt, ig);
             if (!(r.x == OP_POW && !(a > 0.0)) && (ta != 0.0 || tb != 0.0)) {
                 double d0, d1;
                 ft_partials_d(r.x, a, b, d0, d1);
                 tan = ft_mul0(ta, d0) + ft_mul0(tb, d1);
             }
         }
-        tt[i * TS] = tan;
+        tt[k * TS] = tan;
     }
-    /* 4: reverse of the tangent; u = first-order adjoint, w = second */
+    /* 4: reverse of the tangent; u = first-order adjoint, w = second; a
+       constant's w is g . dg/dc_j */
     const double s1 = sw / norm, s3 = sw * fv / (norm * norm * norm);
     for (int j = 0; j < p; ++j) jrow[j] *= s1;
-    vt[(m - 1) * TS] = 1.0;
-    tt[(m - 1) * TS] = 0.0;
-    for (int i = m - 1; i >= 0; --i) {
-        const uint4 r = rec[i];
-        const double u = vt[i * TS], w = tt[i * TS];
-        if (r.x == OP_CONST) {
-            jrow[r.w] -= ft_mul0(w, s3);
-            continue;
-        }
-        if (r.x == OP_VAR) continue;
+    vt[(ni - 1) * TS] = 1.0;
+    tt[(ni - 1) * TS] = 0.0;
+    for (int k = ni - 1; k >= 0; --k) {
+        const uint4 r = ir[k];
+        const double u = vt[k * TS], w = tt[k * TS];
         const bool bin = ft_op_binary(r.x);
-        const double a = vt[r.y * TS], ta = tt[r.y * TS];
-        const double b = bin ? vt[r.z * TS] : 0.0, tb = bin ? tt[r.z * TS] : 0.0;
+        const double a = ij_val<TS>(r.y, vt, x, c), ta = ij_tan<TS>(r.y, tt, ig);
+        const double b = bin ? ij_val<TS>(r.z, vt, x, c) : 0.0;
+        const double tb = bin ? ij_tan<TS>(r.z, tt, ig) : 0.0;
         double u0 = 0.0, u1 = 0.0, w0 = 0.0, w1 = 0.0;
         if ((u != 0.0 || w != 0.0) && !(r.x == OP_POW && !(a > 0.0))) {
             double d0, d1, d00, d01, d11;
@@ -650,11 +715,19 @@ __device__ bool ft_implicit_jac(const uint4 *rec, int m, const double *x, int v,
             w0 = ft_mul0(w, d0) + ft_mul0(u, h0);
             w1 = ft_mul0(w, d1) + ft_mul0(u, h1);
         }
-        vt[r.y * TS] = u0;
-        tt[r.y * TS] = w0;
+        if (!(r.y & IJ_LEAF)) {
+            vt[r.y * TS] = u0;
+            tt[r.y * TS] = w0;
+        } else if (r.y & IJ_CONST) {
+            jrow[r.y & IJ_INDEX] -= ft_mul0(w0, s3);
+        }
         if (bin) {
-            vt[r.z * TS] = u1;
-            tt[r.z * TS] = w1;
+            if (!(r.z & IJ_LEAF)) {
+                vt[r.z * TS] = u1;
+                tt[r.z * TS] = w1;
+            } else if (r.z & IJ_CONST) {
+                jrow[r.z & IJ_INDEX] -= ft_mul0(w1, s3);
+            }
         }
     }
     for (int j = 0; j < p; ++j)

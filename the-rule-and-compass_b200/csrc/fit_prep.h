@@ -12,6 +12,7 @@
 
 struct FitPrep {
     std::vector<int> node_off, valid; /* record offsets [P+1]; 1 = accepted */
+    std::vector<int> ninternal;       /* per candidate: records that are not leaves */
     std::vector<FIns> fins;           /* per candidate: forward list | reverse list */
     std::vector<int> fins_off;        /* [P+1] */
     std::vector<int4> finfo;          /* forward count, reverse count, assembly threads,
