@@ -258,8 +258,9 @@ __device__ void ft_tile_implicit(const FitArgs &a, const uint4 *rec, int ni, int
 /* The implicit cost of one tile, sum w d^2 with d = f / ||grad_x f||
    (implicit.rs:156-174), on the stack machine: f64, one row per thread, the
    forward sweep keeping partials on input paths and the input-adjoint
-   reverse sweep (fi_reverse_x). Row for row the same values, checks and
-   summation order as ft_implicit_d over the records. */
+   reverse sweep (fi_reverse_x). A row with a non-finite value or input
+   gradient, or a zero gradient norm, marks the tile undefined
+   (implicit.rs:156-174). */
 template <int T>
 __device__ void ft_tile_icost_x(const FitArgs &a, const FIns *fwd, int nf, int nr,
                                 const double *cd, FiV<double, 1>::V4 *stk,

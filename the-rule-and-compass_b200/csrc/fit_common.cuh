@@ -53,26 +53,6 @@ __device__ __forceinline__ float ft_fwd_f(const uint4 *rec, int m, const float *
     return val;
 }
 
-/* f64 forward with the row's inputs given explicitly (implicit metric). */
-template <int TS>
-__device__ __forceinline__ double ft_fwd_d_x(const uint4 *rec, int m, const double *x,
-                                             const double *c, double *tp)
-{
-    double val = 0.0;
-    for (int i = 0; i < m; ++i) {
-        const uint4 r = rec[i];
-        if (r.x == OP_CONST) val = c[r.w];
-        else if (r.x == OP_VAR) val = x[r.w];
-        else {
-            const double a = tp[r.y * TS];
-            const double b = ft_op_binary(r.x) ? tp[r.z * TS] : 0.0;
-            val = ft_value_d(r.x, a, b);
-        }
-        tp[i * TS] = val;
-    }
-    return val;
-}
-
 /* Reverse sweep in place (f32). Adjoints of constants are written to
    g[slot * gs] (f64), of inputs accumulated into ig[col * is] when ig != 0.
    Every node of a fit-record tree has one parent, so a child's tape entry
@@ -474,55 +454,11 @@ __device__ __forceinline__ double ft_mul0(double a, double d) { return a == 0.0 
 /* ---- the implicit metric (implicit.rs:68-409) ---------------------------
  * Per row: d = f / ||grad_x f|| (f64 forward + input adjoint); a row with a
  * non-finite value or gradient, or a zero gradient norm, makes the whole
- * evaluation undefined. The LM's Jacobian is central differences of d with
- * h = 1e-6 (1 + |c_j|), exactly as the reference CPU arm. */
+ * evaluation undefined. The LM's Jacobian is exact (below) where the
+ * reference CPU arm takes central differences of d with h = 1e-6 (1 +
+ * |c_j|). */
 
 #define FT_IMPLICIT_MAXV 16
-
-template <int TS>
-__device__ __forceinline__ bool ft_implicit_d(const uint4 *rec, int m, const double *x, int v,
-                                              const double *c, double *tp, double &d)
-{
-    const double fv = ft_fwd_d_x<TS>(rec, m, x, c, tp);
-    if (!isfinite(fv)) return false;
-    double ig[FT_IMPLICIT_MAXV];
-    for (int k = 0; k < FT_IMPLICIT_MAXV; ++k) ig[k] = 0.0;
-    /* input adjoint accumulated in registers: columns are < FT_IMPLICIT_MAXV */
-    tp[(m - 1) * TS] = 1.0;
-    for (int i = m - 1; i >= 0; --i) {
-        const uint4 r = rec[i];
-        const double a = tp[i * TS];
-        if (r.x == OP_CONST) continue;
-        if (r.x == OP_VAR) {
-#pragma unroll
-            for (int k = 0; k < FT_IMPLICIT_MAXV; ++k)
-                if ((int)r.w == k) ig[k] += a;
-            continue;
-        }
-        const bool bin = ft_op_binary(r.x);
-        const double xx = tp[r.y * TS];
-        const double yy = bin ? tp[r.z * TS] : 0.0;
-        double c0 = 0.0, c1 = 0.0;
-        if (a != 0.0 && !(r.x == OP_POW && !(xx > 0.0))) {
-            double d0, d1;
-            ft_partials_d(r.x, xx, yy, d0, d1);
-            c0 = a * d0;
-            c1 = a * d1;
-        }
-        tp[r.y * TS] = c0;
-        if (bin) tp[r.z * TS] = c1;
-    }
-    double nsq = 0.0;
-    for (int k = 0; k < FT_IMPLICIT_MAXV; ++k) {
-        if (k >= v) break;
-        if (!isfinite(ig[k])) return false;
-        nsq += ig[k] * ig[k];
-    }
-    const double norm = sqrt(nsq);
-    if (!(isfinite(norm) && norm > 0.0)) return false;
-    d = fv / norm;
-    return isfinite(d);
-}
 
 /* Child references of the compact records the Jacobian sweep runs over:
    an internal node's tape slot, or a tagged leaf (an input column or a
@@ -607,7 +543,7 @@ __device__ __forceinline__ void ij_put(unsigned ref, double v, double *tt, doubl
       processed; a constant's w is g . dg/dc_j.
    jrow[j] receives sqrt(w_row) dd/dc_j for j < p. Returns false when the
    row is undefined (non-finite value, gradient or Jacobian entry, or a
-   zero gradient): the same rows ft_implicit_d rejects, plus a non-finite
+   zero gradient): the rows the cost sweep rejects, plus a non-finite
    Jacobian entry. The sweeps run over the compact records of ij_compact:
    only internal nodes own tape slots (about half of a tree's nodes), so
    both tapes take half the shared memory; a leaf's adjoint is applied to
