@@ -248,15 +248,18 @@ __global__ void __launch_bounds__(256) rs_prep(unsigned int *count, int n, unsig
    warp's earlier keys of the same digit (match_any per round of 32); the
    warps' counts are scanned in warp order, so the pass is stable. The tile
    is reordered by digit in shared memory first, so that consecutive threads
-   write consecutive addresses of each digit's output run. */
+   write consecutive addresses of each digit's output run. Keys and then row
+   payloads go through the same 32 KB stage: between the two, each thread
+   keeps its keys' slots in the digit-ordered tile and the output positions
+   of the slots it wrote, so four blocks share an SM. */
 template <bool VALS>
 __host__ __device__ constexpr size_t rs_pass_smem()
 {
-    return sizeof(u64) * RS_TILE + (VALS ? 2 * sizeof(unsigned int) * RS_TILE : 0);
+    return sizeof(u64) * RS_TILE;
 }
 
 template <bool VALS>
-__global__ void __launch_bounds__(RS_T, 3) rs_pass(u64 *ka, u64 *kb, unsigned int *va,
+__global__ void __launch_bounds__(RS_T, 4) rs_pass(u64 *ka, u64 *kb, unsigned int *va,
                                                    unsigned int *vb, const unsigned char *skip,
                                                    const unsigned int *goff_all, u64 *state,
                                                    int *ticket, int *abort_flag, int n,
@@ -264,10 +267,9 @@ __global__ void __launch_bounds__(RS_T, 3) rs_pass(u64 *ka, u64 *kb, unsigned in
 {
     extern __shared__ __align__(16) unsigned char sm[];
     u64 *skey = reinterpret_cast<u64 *>(sm);
-    unsigned int *sval_in = reinterpret_cast<unsigned int *>(skey + RS_TILE);
-    unsigned int *sval = sval_in + RS_TILE;
+    unsigned int *sval = reinterpret_cast<unsigned int *>(sm);
     __shared__ unsigned int cnt[RS_WARPS][256];
-    __shared__ unsigned int goff[256], lstart[256], wsum[RS_WARPS];
+    __shared__ unsigned int gdelta[256], wsum[RS_WARPS];
     __shared__ int s_ticket;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     if (tid == 0) s_ticket = atomicAdd(ticket + pass, 1);
@@ -288,6 +290,7 @@ __global__ void __launch_bounds__(RS_T, 3) rs_pass(u64 *ka, u64 *kb, unsigned in
 #pragma unroll
     for (int k = 0; k < RS_WARPS; ++k) cnt[k][tid] = 0;
     constexpr int R = RS_TILE / RS_WARPS / 32;
+    static_assert(R == RS_ITEMS, "a thread stages as many keys as it writes");
     const int t0 = tile * RS_TILE;
     const int wb = w * (RS_TILE / RS_WARPS);
     const int count = min(RS_TILE, n - t0);
@@ -296,20 +299,22 @@ __global__ void __launch_bounds__(RS_T, 3) rs_pass(u64 *ka, u64 *kb, unsigned in
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int li = wb + 32 * r + lane;
-        const bool in = li < count;
-        key[r] = in ? src[t0 + li] : 0ULL;
-        if (VALS && in) sval_in[li] = vsrc[t0 + li];
+        key[r] = li < count ? src[t0 + li] : 0ULL;
     }
     __syncthreads();
-    unsigned short rk[R];
+    /* rank of key r among the tile's earlier keys of its digit, two 16-bit
+       halves per register (ranks and slots are below RS_TILE) */
+    unsigned int rk[R / 2];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const bool in = wb + 32 * r + lane < count;
         const unsigned d = in ? (unsigned)(key[r] >> shift) & 255u : 256u;
         const unsigned peers = __match_any_sync(0xffffffffu, d);
-        rk[r] = in ? (unsigned short)(cnt[w][d] + __popc(peers & lt)) : 0;
+        const unsigned int base = in ? cnt[w][d] : 0u;
+        const unsigned int rr = base + __popc(peers & lt);
+        rk[r / 2] = (r & 1) ? (rk[r / 2] | (rr << 16)) : rr;
         __syncwarp();
-        if (in && lane == __ffs(peers) - 1) cnt[w][d] += __popc(peers);
+        if (in && lane == __ffs(peers) - 1) cnt[w][d] = base + __popc(peers);
         __syncwarp();
     }
     __syncthreads();
@@ -321,9 +326,40 @@ __global__ void __launch_bounds__(RS_T, 3) rs_pass(u64 *ka, u64 *kb, unsigned in
         cnt[k][tid] = tot;
         tot += c;
     }
-    /* publish, then look back over the earlier tiles of the segment */
+    /* publish the tile's counts at once, for the tiles that look back on it */
     volatile u64 *st = reinterpret_cast<volatile u64 *>(state) + (size_t)seg * ntiles * 256;
     st[(size_t)tile * 256 + tid] = rs_word(tile == 0 ? RS_ST_PREFIX : RS_ST_AGG, pass, tot);
+    /* the tile's digit starts in the digit-ordered tile */
+    unsigned int x = tot;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[w] = x;
+    __syncthreads();
+    unsigned int before = 0;
+    for (int k = 0; k < w; ++k) before += wsum[k];
+    /* digit tid starts at ls in the digit-ordered tile; cnt[k][tid] becomes
+       the slot of warp k's first key of that digit */
+    const unsigned int ls = before + x - tot;
+#pragma unroll
+    for (int k = 0; k < RS_WARPS; ++k) cnt[k][tid] += ls;
+    /* slot i of digit d goes to gdelta[d] + i (mod 2^32), once the earlier
+       tiles' counts (excl) are added below */
+    gdelta[tid] = goff_all[((size_t)seg * RS_PASSES + pass) * 256 + tid] - ls;
+    __syncthreads();
+    /* keys into the stage; key r's rank becomes its slot there (< count) */
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int li = wb + 32 * r + lane;
+        if (li >= count) continue;
+        const unsigned d = (unsigned)(key[r] >> shift) & 255u;
+        const unsigned int lp = cnt[w][d] + ((rk[r / 2] >> (16 * (r & 1))) & 0xffffu);
+        skey[lp] = key[r];
+        rk[r / 2] = (r & 1) ? ((rk[r / 2] & 0xffffu) | (lp << 16)) : ((rk[r / 2] & 0xffff0000u) | lp);
+    }
+    /* look back over the earlier tiles of the segment */
     unsigned int excl = 0;
     bool failed = false;
     for (int j = tile - 1; j >= 0 && !failed; --j) {
@@ -346,41 +382,36 @@ __global__ void __launch_bounds__(RS_T, 3) rs_pass(u64 *ka, u64 *kb, unsigned in
     }
     if (tile > 0 && !failed)
         st[(size_t)tile * 256 + tid] = rs_word(RS_ST_PREFIX, pass, excl + tot);
-    goff[tid] = goff_all[((size_t)seg * RS_PASSES + pass) * 256 + tid] + excl;
-    /* the tile's digit starts in the digit-ordered tile */
-    unsigned int x = tot;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const unsigned int y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
-    }
-    if (lane == 31) wsum[w] = x;
-    __syncthreads();
-    unsigned int before = 0;
-    for (int k = 0; k < w; ++k) before += wsum[k];
-    lstart[tid] = before + x - tot;
+    gdelta[tid] += excl;
     if (__syncthreads_or(failed)) return;
+    /* slot i = tid + k * RS_T leaves for its output position pos[k] */
+    unsigned int pos[RS_ITEMS];
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const int li = wb + 32 * r + lane;
-        if (li >= count) continue;
-        const unsigned d = (unsigned)(key[r] >> shift) & 255u;
-        const unsigned int lp = lstart[d] + cnt[w][d] + rk[r];
-        skey[lp] = key[r];
-        if (VALS) sval[lp] = sval_in[li];
-    }
-    __syncthreads();
-    for (int i = tid; i < count; i += RS_T) {
-        const u64 k = skey[i];
-        const unsigned d = (unsigned)(k >> shift) & 255u;
-        const unsigned int pos = goff[d] + (unsigned)i - lstart[d];
-        if (pos >= (unsigned)n) {
+    for (int k = 0; k < RS_ITEMS; ++k) {
+        const int i = tid + k * RS_T;
+        pos[k] = 0xffffffffu;
+        if (i >= count) continue;
+        const u64 kk = skey[i];
+        const unsigned d = (unsigned)(kk >> shift) & 255u;
+        const unsigned int q = gdelta[d] + (unsigned)i;
+        if (q >= (unsigned)n) {
             atomicExch(abort_flag, 1);
             continue;
         }
-        dst[pos] = k;
-        if (VALS) vdst[pos] = sval[i];
+        dst[q] = kk;
+        pos[k] = q;
     }
+    if (!VALS) return;
+    __syncthreads(); /* every key has left the stage */
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int li = wb + 32 * r + lane;
+        if (li < count) sval[(rk[r / 2] >> (16 * (r & 1))) & 0xffffu] = vsrc[t0 + li];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < RS_ITEMS; ++k)
+        if (pos[k] != 0xffffffffu) vdst[pos[k]] = sval[tid + k * RS_T];
 }
 
 struct RsBuffers {
