@@ -160,6 +160,22 @@ __device__ __forceinline__ u64 rs_word(u64 kind, int pass, unsigned int v)
     return (kind << 62) | ((u64)(pass + 1) << 32) | (u64)v;
 }
 
+/* Lanes of the warp holding the same 9-bit label (a digit, or 256 for a lane
+   with no key): one ballot per bit, each lane keeping the lanes that agree
+   with it on that bit. The same mask as __match_any_sync on the label, from
+   nine votes. */
+__device__ __forceinline__ unsigned rs_peers(unsigned d)
+{
+    unsigned m = 0xffffffffu;
+#pragma unroll
+    for (int b = 0; b < 9; ++b) {
+        const bool bit = (d >> b) & 1u;
+        const unsigned v = __ballot_sync(0xffffffffu, bit);
+        m &= bit ? v : ~v;
+    }
+    return m;
+}
+
 /* Per segment, the counts of all eight digits: count[seg][pass][256]. A
    block counts RS_COUNT_TILES tiles in shared memory before adding to the
    segment's totals. */
@@ -199,7 +215,7 @@ __global__ void __launch_bounds__(RS_T) rs_count(const u64 *keys, int n, int nbl
                 if (__all_sync(0xffffffffu, dg == __shfl_sync(0xffffffffu, dg, 0))) {
                     if (lane == 0 && dg < 256u) atomicAdd(&cnt[d][dg], 32u);
                 } else if (d >= 6) {
-                    const unsigned peers = __match_any_sync(0xffffffffu, dg);
+                    const unsigned peers = rs_peers(dg);
                     if (dg < 256u && lane == __ffs(peers) - 1)
                         atomicAdd(&cnt[d][dg], (unsigned)__popc(peers));
                 } else if (dg < 256u) {
@@ -245,7 +261,7 @@ __global__ void __launch_bounds__(256) rs_prep(unsigned int *count, int n, unsig
 }
 
 /* One pass over every segment's tiles. Warp w ranks its keys among the
-   warp's earlier keys of the same digit (match_any per round of 32); the
+   warp's earlier keys of the same digit (a peer mask per round of 32); the
    warps' counts are scanned in warp order, so the pass is stable. The tile
    is reordered by digit in shared memory first, so that consecutive threads
    write consecutive addresses of each digit's output run. Keys and then row
@@ -309,7 +325,7 @@ __global__ void __launch_bounds__(RS_T, 4) rs_pass(u64 *ka, u64 *kb, unsigned in
     for (int r = 0; r < R; ++r) {
         const bool in = wb + 32 * r + lane < count;
         const unsigned d = in ? (unsigned)(key[r] >> shift) & 255u : 256u;
-        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        const unsigned peers = rs_peers(d);
         const unsigned int base = in ? cnt[w][d] : 0u;
         const unsigned int rr = base + __popc(peers & lt);
         rk[r / 2] = (r & 1) ? (rk[r / 2] | (rr << 16)) : rr;
