@@ -215,7 +215,10 @@ __global__ void __launch_bounds__(RS_T) rs_count(const u64 *keys, int n, int nbl
                 if (__all_sync(0xffffffffu, dg == __shfl_sync(0xffffffffu, dg, 0))) {
                     if (lane == 0 && dg < 256u) atomicAdd(&cnt[d][dg], 32u);
                 } else if (d >= 6) {
-                    const unsigned peers = rs_peers(dg);
+                    /* match_any here: this kernel is bound by its shared-memory
+                       atomics, and the ballots' extra instructions cost more
+                       than the match saves */
+                    const unsigned peers = __match_any_sync(0xffffffffu, dg);
                     if (dg < 256u && lane == __ffs(peers) - 1)
                         atomicAdd(&cnt[d][dg], (unsigned)__popc(peers));
                 } else if (dg < 256u) {
