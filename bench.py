@@ -547,8 +547,9 @@ def bench_vary(args, rank, pkg, flushbuf, steps, warmup):
     operator set), parents drawn as the reference's tests draw them, seeded
     errors. children/s from the library's events around the call, e2e from
     the wall clock of the call with host buffers (errors in; lengths, node
-    counts, hashes, errors and the child programs out), beside the CPU
-    restatement of the reference engine on one thread."""
+    counts, hashes, errors and the child programs out; pinned and reused
+    across generations, as a generation loop would keep them), beside the
+    CPU restatement of the reference engine on one thread."""
     islands = args.P if args.workload == "vary" and args.P else 16
     pop, width, nvars, mc = 1000, 64, 10, 30
     n = islands * pop
@@ -562,16 +563,25 @@ def bench_vary(args, rank, pkg, flushbuf, steps, warmup):
     seed_words[:, 0], seed_words[:, 1] = 1, 0
     pool.upload(0, seed_words)
     words = pool.vary(0, err, 0, nvars, mc, 5 + rank, ops, restart=[1] * islands)[0]
+    import torch
+
+    def pinned(count, dt):
+        b = torch.empty(count * np.dtype(dt).itemsize, dtype=torch.uint8, pin_memory=True)
+        return b.numpy().view(dt)
+
+    err_h = pinned(n, np.float64)
+    err_h[:] = err
+    outbuf = (pinned(n * width, np.uint32), pinned(n, np.uint16), pinned(n, np.uint16),
+              pinned(n, np.uint64), pinned(n, np.float64))
     for g in range(warmup):
-        pool.vary(1, err, 1 + g, nvars, mc, 77, ops)
+        pool.vary(1, err_h, 1 + g, nvars, mc, 77, ops, out=outbuf)
     dev_ms, wall = [], []
     n0 = ev.launch_count()
-    import torch
     for g in range(steps):
         flush_l2(flushbuf)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        out = pool.vary(1, err, 1 + g, nvars, mc, 77, ops)
+        out = pool.vary(1, err_h, 1 + g, nvars, mc, 77, ops, out=outbuf)
         wall.append(time.perf_counter() - t0)
         dev_ms.append(out[5])
     launches = ev.launch_count() - n0

@@ -430,9 +430,13 @@ class GenomePool:
         return out
 
     def vary(self, which, err, gen, nvars, max_complexity, seed, ops, init_depth=3, dedup=True,
-             restart=None, front=None, front_p=0.0, words=True):
+             restart=None, front=None, front_p=0.0, words=True, out=None):
         """Children of pool `which` into pool `which ^ 1`. Returns
-        (words [islands*pop, width] or None, len, cost, hash, err, ms)."""
+        (words [islands*pop, width] or None, len, cost, hash, err, ms).
+        `out` may hold caller-owned result arrays (words or None, len u16,
+        cost u16, hash u64, err f64, each C-contiguous with islands*pop rows),
+        for example in pinned memory reused across generations; they are
+        filled and returned in place of fresh ones."""
         n = self.islands * self.pop
         e = np.ascontiguousarray(err, np.float64)
         o = np.ascontiguousarray(np.asarray(ops, np.uint32).reshape(-1))
@@ -444,11 +448,22 @@ class GenomePool:
             fo[1:] = np.cumsum([len(f) for f in front])
             fw = np.ascontiguousarray(np.concatenate([np.asarray(f, np.uint32) for f in front]))
             nf = len(front)
-        ol = np.zeros(n, np.uint16)
-        oc = np.zeros(n, np.uint16)
-        oh = np.zeros(n, np.uint64)
-        oe = np.zeros(n, np.float64)
-        ow = np.zeros(n * self.width, np.uint32) if words else None
+        if out is not None:
+            ow, ol, oc, oh, oe = out
+            for a, dt, m in ((ol, np.uint16, n), (oc, np.uint16, n), (oh, np.uint64, n),
+                             (oe, np.float64, n), (ow, np.uint32, n * self.width)):
+                if a is None and dt is np.uint32:
+                    continue
+                if a.dtype != dt or a.size != m or not a.flags.c_contiguous:
+                    raise ValueError("vary: out arrays must be C-contiguous words u32 "
+                                     "[n*width], len u16, cost u16, hash u64, err f64 [n]")
+            ow = None if ow is None else ow.reshape(-1)
+        else:
+            ol = np.zeros(n, np.uint16)
+            oc = np.zeros(n, np.uint16)
+            oh = np.zeros(n, np.uint64)
+            oe = np.zeros(n, np.float64)
+            ow = np.zeros(n * self.width, np.uint32) if words else None
         ms = lib().rc_pool_vary(self.ev.ctx, which, self.islands, self.pop, self.width,
                                 _p(e, ctypes.c_double), nvars, max_complexity, seed, gen,
                                 init_depth, int(dedup), _p(o, ctypes.c_uint32), len(o) // 2,
