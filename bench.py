@@ -116,6 +116,14 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+# The scoring CPU sample (the oracle's timed baseline and the parity check):
+# the first programs and rows of the timed workload.
+SCORE_SAMPLE_PROGS, SCORE_SAMPLE_ROWS = 64, 1 << 16
+# DRAM bytes (read + write) of one launch of the f32 scoring kernel on the
+# P = 4096, N = 1,048,576 workload, from ncu (profiles/rc_score_kernel_P4096_N1M.md).
+SCORE_TRAFFIC = 25.69e6
+
+
 def flush_l2(buf):
     """Write a buffer larger than the 126 MB L2 between timed steps."""
     if buf is not None:
@@ -155,18 +163,83 @@ def cpu_model():
     return None
 
 
-def cpu_score_baseline(trees, x, y, n_rows, n_cand, threads):
+def f32_constants(t):
+    """The tree with its constants rounded to f32, as the device's postfix
+    words carry them (gpu.rs:354)."""
+    t32 = t.clone()
+    t32.set_constants([float(np.float32(c)) for c in t.constants()])
+    return t32
+
+
+def cpu_score_baseline(trees, x, y, n_rows, n_cand, threads, want_values=False):
+    """The oracle's squared-error score (metrics::score_weighted over
+    expr::eval) of the first `n_cand` programs (constants as the device sees
+    them) on the first `n_rows` rows, parallel over candidates; returns
+    (expr*row/s, seconds[, values])."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     O.lib()
     x64 = np.ascontiguousarray(x[:, :n_rows].astype(np.float64)).reshape(-1)
     y64 = y[:n_rows].astype(np.float64)
-    sample = trees[:n_cand]
+    sample = [f32_constants(t) for t in trees[:n_cand]]
     t0 = time.perf_counter()
     with cf.ThreadPoolExecutor(max_workers=threads) as ex:
-        list(ex.map(lambda t: O.score(t, x64, n_rows, x.shape[0], y64, O.SQUARED), sample))
+        vals = list(ex.map(lambda t: O.score(t, x64, n_rows, x.shape[0], y64, O.SQUARED),
+                           sample))
     dt = time.perf_counter() - t0
+    if want_values:
+        return n_cand * n_rows / dt, dt, np.asarray(vals)
     return n_cand * n_rows / dt, dt
+
+
+def score_parity(pkg, trees, x, y, n_rows, oracle_vals):
+    """Device scores of the oracle's sample (the first len(oracle_vals)
+    programs on the first n_rows rows of the timed workload) against the
+    oracle: the largest relative error over candidates finite in both, and
+    how many candidates differ in their non-finite classification (device
+    status != 0 against a non-finite oracle value)."""
+    k = len(oracle_vals)
+    xs = np.ascontiguousarray(x[:, :n_rows])
+    ev = pkg.GpuEvaluator(xs.reshape(-1), n_rows, x.shape[0], np.ascontiguousarray(y[:n_rows]))
+    prog, off = pkg.Population(trees[:k]).programs()
+    vals, status, _ = ev.score_batch(prog, off, 0)
+    ev.close()
+    fin_cpu = np.isfinite(oracle_vals)
+    fin_dev = np.asarray(status) == 0
+    both = fin_cpu & fin_dev
+    rel = np.abs(vals[both] - oracle_vals[both]) / np.maximum(np.abs(oracle_vals[both]), 1e-300)
+    return {"checked": int(k), "rows": int(n_rows), "finite": int(both.sum()),
+            "max_rel_err": float(rel.max()) if rel.size else 0.0,
+            "nonfinite_mismatch": int((fin_cpu != fin_dev).sum()),
+            "bar": "relative error <= 1e-4 (gpu.rs:3349-3369), identical non-finite class",
+            "oracle": "f64 CPU restatement of expr::eval + metrics::score_weighted"}
+
+
+def cpu_fit_sample(trees, x, y, N, n_rows, n_cand, threads, metric=0, kind="fit", iters=20):
+    """The oracle's CPU fit (fit_weighted_metric: fit_lm, or irls_fit for the
+    absolute metric; implicit::fit for kind="implicit") of the first `n_cand`
+    candidates on the first `n_rows` rows, parallel over candidates; the rate
+    in candidates/s is scaled linearly in rows to the full N."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.lib()
+    v = x.shape[0]
+    x64 = np.ascontiguousarray(np.asarray(x, np.float64)[:, :n_rows]).reshape(-1)
+    y64 = None if y is None else np.ascontiguousarray(np.asarray(y, np.float64)[:n_rows])
+    sample = trees[:n_cand]
+    if kind == "implicit":
+        fn = lambda t: O.implicit_fit(t, x64, n_rows, v, iters)  # noqa: E731
+    else:
+        om = {0: O.SQUARED, 4: O.ABSOLUTE, 1: O.LOG_SQUASHED}[metric]
+        fn = lambda t: O.fit(t, x64, n_rows, v, y64, iters, om)  # noqa: E731
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+        list(ex.map(fn, sample))
+    dt = time.perf_counter() - t0
+    return {"value": n_cand / dt * n_rows / N, "unit": "candidates/s", "cores": threads,
+            "kind": "port", "cpu_model": cpu_model(),
+            "sample": f"the first {n_cand} candidates x the first {n_rows} rows, {iters} "
+                      f"iterations, f64 oracle, rate scaled linearly in rows to N={N}"}
 
 
 def cpu_fit_baseline(trees, x, y, n_rows, n_cand, iters, threads):
@@ -237,25 +310,29 @@ def run_reference(args, rank, world):
     W = importlib.import_module(PKG + ".workloads")
     threads = os.cpu_count() or 1
     if args.workload == "score":
-        P, N = 4096, 1 << 20
-        trees, x, y = W.scoring_workload(256, 1 << 16, seed=0)
-        n_rows, n_cand = 1 << 16, 64
+        # the repo arm's workload (seed 0): its first programs and rows
+        P, N = args.P or 4096, args.N or (1 << 20)
+        trees, x, y = W.scoring_workload(P, N, seed=0)
+        n_rows, n_cand = SCORE_SAMPLE_ROWS, SCORE_SAMPLE_PROGS
         metric, unit = "expr_row_evals_per_s", "expr*row/s"
         fn = lambda: cpu_score_baseline(trees, x, y, n_rows, n_cand, threads)  # noqa: E731
-        sample = f"{n_cand} programs x {n_rows} rows of the P={P}, N={N} workload per step"
-        cfg = {"workload": "batched scoring, P=4096 programs, N=1048576 rows x 5 features",
-               "metric_kind": "squared"}
+        sample = (f"the first {n_cand} programs x the first {n_rows} rows of the P={P}, N={N} "
+                  f"workload per step")
+        cfg = {"workload": f"batched scoring, P={P} programs, N={N} rows x 5 features, "
+                           f"squared error", "l2": "flushed between steps"}
     else:
-        trees, x, y = W.fit_workload(64, 1 << 14, seed=0)
+        P, N = args.P or 2048, args.N or 262144
+        trees, x, y = W.fit_workload(P, N, seed=0)
         n_rows, n_cand = 1 << 14, 16
         metric, unit = "fitted_candidates_per_s", "candidates/s"
 
         def fn():
             v, dt = cpu_fit_baseline(trees, x, y, n_rows, n_cand, 20, threads)
-            return v * n_rows / 262144.0, dt
-        sample = (f"{n_cand} candidates x {n_rows} rows x 20 LM iterations, scaled linearly "
-                  f"to N=262144")
-        cfg = {"workload": "batched LM fit, P=2048, N=262144 rows x 8 features, 20 iters"}
+            return v * n_rows / float(N), dt
+        sample = (f"the first {n_cand} candidates x the first {n_rows} rows x 20 LM iterations "
+                  f"per step, scaled linearly to N={N}")
+        cfg = {"workload": f"batched LM fit (squared), P={P}, N={N} rows x 8 features, 20 "
+                           f"iters, fused adjoint", "l2": "flushed between steps"}
     for _ in range(args.warmup):
         fn()
     vals, total = [], 0.0
@@ -289,7 +366,7 @@ def bench_score(args, rank, world, dev, pkg, W, flushbuf):
     # warm-up
     for _ in range(args.warmup):
         ev.score_batch(prog, off, 0, pcount)
-    dev_ms, wall = [], []
+    dev_ms, wall, prof = [], [], []
     import torch
     torch.cuda.synchronize()
     n0 = ev.launch_count()
@@ -301,6 +378,7 @@ def bench_score(args, rank, world, dev, pkg, W, flushbuf):
             vals, status, ms = ev.score_batch(prog, off, 0, pcount)
             wall.append(time.perf_counter() - t0)
             dev_ms.append(ms)
+            prof.append(ev.score_profile())
     launches = ev.launch_count() - n0
     stats = ev.last_stats()
     clocks = clk.summary()
@@ -309,19 +387,33 @@ def bench_score(args, rank, world, dev, pkg, W, flushbuf):
     d2h = int(P * (8 + 4))
     finite = np.asarray(status) == 0
     return dict(P=P, N=N, dev_ms=dev_ms, wall=wall, alg_ops=alg_ops, clocks=clocks,
-                h2d=h2d, d2h=d2h, trees=trees, x=x, y=y, stats=stats,
+                h2d=h2d, d2h=d2h, trees=trees, x=x, y=y, stats=stats, prof=prof,
                 launches=launches, unit_count=float(P) * N,
                 finite=int(finite.sum()), alg_ops_finite=float(N) * float((ops[finite] + 2).sum()))
 
 
-def fit_lane_ops(plans, N, iters):
-    """Algorithmic work of one fit in FP32-lane-op equivalents: per candidate,
-    iteration and row, 4.5 L FP32 ops (forward, reverse, trial forward;
-    L = records) plus p(p+1)/2 + p + 1 FP64 FMAs (Gram, rhs, loss) counted
-    twice (FP64 issues at half the FP32 rate)."""
-    fp32 = sum(4.5 * len(p.words) / 4 for p in plans) * iters * N
-    fp64 = sum(p.nconst * (p.nconst + 1) / 2 + p.nconst + 1 for p in plans) * iters * N
-    return fp32 + 2.0 * fp64
+def fit_lane_ops(plans, sweeps, N, metric):
+    """Algorithmic work of one fit in FP32-lane-op equivalents, from the
+    sweeps each candidate actually ran (the device's per-candidate counts):
+    per row, an f32 assembly is the forward (L) and reverse (2.5 L) sweeps
+    plus G = p(p+1)/2 + p + 1 f64 FMAs of the Gram fold (each counted twice:
+    FP64 issues at half the FP32 rate), an f32 objective sweep L + 2, and the
+    f64 sweeps the same work at twice the cost; the implicit Jacobian is four
+    passes (7 L) plus G, its cost sweep the forward and input adjoint (3.5 L)
+    plus the norm and the division. L = the candidate's records."""
+    tot = 0.0
+    for pl, sw in zip(plans, sweeps):
+        L = len(pl.words) / 4.0
+        p = pl.nconst
+        G = p * (p + 1) / 2.0 + p + 1 + (2 if metric in (2, 3) else 0) * (p + 2)
+        a32, l32, a64, l64 = (float(q) for q in sw)
+        if metric == 6:
+            per = 2.0 * a64 * (7.0 * L + G) + 2.0 * l64 * (3.5 * L + 6.0)
+        else:
+            per = (a32 * (3.5 * L + 2.0 * G) + l32 * (L + 2.0) +
+                   2.0 * a64 * (3.5 * L + G) + 2.0 * l64 * (L + 2.0))
+        tot += per
+    return tot * N
 
 
 def fit_setup(pkg, W, case, P, N, seed):
@@ -369,12 +461,13 @@ def time_fit(pkg, ev, plans, metric, N, steps, warmup, flushbuf, plain_n, seed):
             wall.append(time.perf_counter() - t0)
             dev_ms.append(ms)
     launches = ev.launch_count() - n0
+    sweeps = ev.fit_sweeps(P)
     out = dict(P=P, N=N, dev_ms=dev_ms, wall=wall, clocks=clk.summary(), launches=launches,
                unit_count=float(P), status=np.bincount(st, minlength=9).tolist(),
                h2d=int(prog.nbytes + off.nbytes + pcount.nbytes + c0.nbytes + gauge.nbytes),
-               d2h=int(P * (kmax * 8 + 8 + 4)))
-    if metric in (0, 4):
-        out["lane_ops"] = fit_lane_ops(plans, N, iters)
+               d2h=int(P * (kmax * 8 + 8 + 4)), loss=loss, status_list=st,
+               sweeps_mean=sweeps.mean(0).tolist(),
+               lane_ops=fit_lane_ops(plans, sweeps, N, metric))
     if plain_n:
         rng = np.random.Generator(np.random.PCG64(seed + 77))
         idx = np.sort(rng.choice(P, size=min(plain_n, P), replace=False))
@@ -401,23 +494,63 @@ def fit_summary(r, peaks, what):
          "e2e": r["unit_count"] * len(r["wall"]) / sum(r["wall"]),
          "ms_per_step": float(np.mean(r["dev_ms"])), "steps": len(r["dev_ms"]),
          "config": what, "gpu_launches": r["launches"], "status_histogram": r["status"],
-         "clocks": r["clocks"]}
+         "sweeps_per_candidate": r["sweeps_mean"], "clocks": r["clocks"]}
+    for k in ("status_histogram_reference_mode", "status57_classified", "cpu_baseline"):
+        if k in r:
+            d[k] = r[k]
     if "plain" in r:
         d["plain"] = r["plain"]
         d["fused_over_plain"] = fv / r["plain"]["value"]
-    d["roofline"] = fit_roofline(r, peaks) if "lane_ops" in r else None
+    d["roofline"] = fit_roofline(r, peaks)
     return d
 
 
+def fit_reference_mode(pkg, ev, plans, metric, trees, x, y, r, threads):
+    """The same batch once more with the f64 rescue off (flags bit 1: the
+    reference kernel's behaviour, stopping at an f32-only failure), untimed;
+    every status 5 / 7 of either run is classified on the CPU: `f32_only` when
+    the oracle's f64 normal equations (fit.rs:1774-1827) are finite at the
+    returned constants, `genuine` otherwise."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.lib()
+    prog, off, pcount, c0, gauge, kmax = pkg.pack_plans(plans)
+    c_ref, _, st_ref, _ = ev.fit_batch_fused(prog, off, pcount, c0, gauge, kmax, 20, metric, 2)
+    c_res, _, st_res, _ = ev.fit_batch_fused(prog, off, pcount, c0, gauge, kmax, 20, metric, 0)
+    v, n = x.shape
+    cols = np.ascontiguousarray(x, np.float64).reshape(-1)
+    y64 = np.ascontiguousarray(y, np.float64)
+
+    def classify(args):
+        k, cc = args
+        at = plans[k].apply(trees[k], cc[k][: plans[k].nconst])
+        return "f32_only" if O.normal_equations_ok(at, cols, n, v, y64) else "genuine"
+
+    out = {}
+    for tag, cc, st in (("rescue_on", c_res, st_res), ("reference_mode", c_ref, st_ref)):
+        ks = [k for k in range(len(plans)) if st[k] in (5, 7)]
+        with cf.ThreadPoolExecutor(threads) as ex:
+            cls = list(ex.map(classify, [(k, cc) for k in ks]))
+        out[tag] = {"f32_only": cls.count("f32_only"), "genuine": cls.count("genuine")}
+    r["status_histogram_reference_mode"] = np.bincount(st_ref, minlength=9).tolist()
+    r["status57_classified"] = out
+    return out
+
+
 def bench_fit(args, rank, world, dev, pkg, W, flushbuf, steps=None, warmup=None, plain=True,
-              N=None):
+              N=None, classify=False, cpu=False):
     P = args.P if args.workload == "fit" and args.P else 2048
     N = N or (args.N if args.workload == "fit" and args.N else 262144)
     steps = args.steps if steps is None else steps
     warmup = args.warmup if warmup is None else warmup
     ev, plans, trees, x, y, metric, what = fit_setup(pkg, W, "c3", P, N, rank)
     out = time_fit(pkg, ev, plans, metric, N, steps, warmup, flushbuf, 64 if plain else 0, rank)
+    threads = os.cpu_count() or 1
+    if classify:
+        fit_reference_mode(pkg, ev, plans, metric, trees, x, y, out, threads)
     ev.close()
+    if cpu and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_fit_sample(trees, x, y, N, 1 << 14, 16, threads)
     out.update(trees=trees, x=x, y=y, what=what)
     return out
 
@@ -448,15 +581,48 @@ def bench_implicit(args, rank, pkg, W, flushbuf, steps, warmup, fit_steps, fit_w
         wall.append(time.perf_counter() - t0)
         dev_ms.append(ms)
     rows = float(P) * N
+    peaks = load_peaks()
+    peak = 148 * 128 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e9
+    fin = np.asarray(status) == 0
+    # U_grad per candidate*row: forward L, input adjoint 2.5 L, the norm of
+    # the 4-input gradient and the division
+    ugrad = float(N) * sum(3.5 * len(pl.words) / 4.0 + 4.0 + 2.0
+                           for pl, f in zip(splans, fin) if f)
+    per = float(np.mean(dev_ms)) / 1e3
     score = {"metric": "implicit_score_candidate_rows_per_s",
              "value": rows * steps / (sum(dev_ms) / 1e3), "unit": "candidate*row/s",
              "e2e": rows * steps / sum(wall), "ms_per_step": float(np.mean(dev_ms)),
              "gpu_launches": ev.launch_count() - n0,
-             "finite_candidates": int((status == 0).sum()),
+             "finite_candidates": int(fin.sum()),
+             "roofline": {"bound": "fp32_issue", "achieved": ugrad / per / 1e9, "peak": peak,
+                          "unit": "Glane-op/s", "frac": ugrad / per / 1e9 / peak,
+                          "traffic": None,
+                          "note": "finite candidates x N x (3.5 L + 4 + 2) lane-ops (forward, "
+                                  "input adjoint, gradient norm, division; L = records) / "
+                                  "event time of the scoring call; infeasible candidates stop "
+                                  "at their first bad row and are not counted"},
              "config": f"implicit |f|/||grad f|| scoring, P={P}, N={N} rows x 4 inputs"}
     fplans = [pkg.gpu_fit_plan(t) for t in trees if t.constants()]
+    ftrees = [t for t in trees if t.constants()]
     fit = time_fit(pkg, ev, fplans, 6, N, fit_steps, fit_warmup, flushbuf, 16, rank)
     ev.close()
+    if not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        O.lib()
+        nr, nc = 1 << 16, 64
+        c64 = np.ascontiguousarray(cols[:, :nr]).reshape(-1)
+        t0 = time.perf_counter()
+        with cf.ThreadPoolExecutor(threads) as ex:
+            list(ex.map(lambda t: O.implicit_score(t, c64, nr, 4), trees[:nc]))
+        dt = time.perf_counter() - t0
+        score["cpu_baseline"] = {"value": nc * nr / dt, "unit": "candidate*row/s",
+                                 "cores": threads, "kind": "port", "cpu_model": cpu_model(),
+                                 "sample": f"the first {nc} candidates x the first {nr} rows, "
+                                           f"implicit::score restated in f64"}
+        fit["cpu_baseline"] = cpu_fit_sample(ftrees, cols, None, N, 1 << 14, 16, threads,
+                                             kind="implicit")
     what = (f"implicit |f|/||grad f|| LM fit (exact Jacobian from the input adjoint), the "
             f"{fit['P']} of P={P} candidates with constants, N={N} rows, 20 iters")
     return score, fit, what
@@ -538,7 +704,31 @@ def bench_c5(args, rank, pkg, W, flushbuf, steps, warmup, fit_steps, fit_warmup)
     rk["config"] = (f"exact rank-correlation sums, P={P} candidates x 1 trial, N={N} rows x "
                     f"10 heavy-tailed features")
     ev.close()
+    if not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        fit["cpu_baseline"] = cpu_fit_sample(trees, x, y, N, 1 << 14, 16, threads, metric=4)
+        rk["cpu_baseline"] = cpu_rank_sample(trees, x, y, 4, threads)
     return fit, what, rk
+
+
+def cpu_rank_sample(trees, x, y, n_cand, threads):
+    """The oracle's exact rank sums (expr::eval predictions, then
+    RankTarget::sums: sort, average ranks, i128 sums) of the first `n_cand`
+    candidates over all rows, parallel over candidates: candidate*rows/s."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.lib()
+    v, n = x.shape
+    cols = np.ascontiguousarray(x, np.float64).reshape(-1)
+    y64 = np.ascontiguousarray(y, np.float64)
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(threads) as ex:
+        list(ex.map(lambda t: O.rank_sums(O.predict(t, cols, n, v), y64), trees[:n_cand]))
+    dt = time.perf_counter() - t0
+    return {"value": n_cand * float(n) / dt, "unit": "candidate*row/s", "cores": threads,
+            "kind": "port", "cpu_model": cpu_model(),
+            "sample": f"the first {n_cand} candidates over all {n} rows, f64 oracle "
+                      f"(expr::eval + RankTarget::sums)"}
 
 
 def bench_vary(args, rank, pkg, flushbuf, steps, warmup):
@@ -612,10 +802,70 @@ def fit_roofline(r, peaks):
     achieved = r["lane_ops"] / per / 1e9
     peak = 148 * 128 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e9
     return {"bound": "fp32_issue", "achieved": achieved, "peak": peak, "unit": "Glane-op/s",
-            "frac": achieved / peak, "traffic": None,
-            "note": "sum over candidates of 20 iters x N x (4.5 L FP32 ops + 2 x (p(p+1)/2 + "
-                    "p + 1) FP64 FMAs), L = records, / event time of one fit; peak = 148 SMs x "
-                    "128 FP32 lanes x sm_max_mhz from MEASURED_PEAKS.json"}
+            "frac": achieved / peak, "traffic": r.get("traffic"),
+            "note": "the sweeps each candidate ran (device counts) x N x their per-row "
+                    "FP32-lane-op equivalents (f32 assembly 3.5 L + 2 G, f32 objective L + 2, "
+                    "f64 sweeps twice the f32 cost; G = p(p+1)/2 + p + 1 FMAs of the Gram "
+                    "fold), L = records, / CUDA-event time of the whole fused fit (the graph "
+                    "of all its kernels); peak = 148 SMs x 128 FP32 lanes x sm_max_mhz "
+                    "(MEASURED_PEAKS.json)"}
+
+
+def _cpu(block):
+    cb = block.get("cpu_baseline")
+    return None if cb is None else cb["value"]
+
+
+def secondary(args, rank, world, local, pkg, W, flushbuf, peaks, line):
+    """The other configurations on the default line: nested blocks with the
+    detail, and their headline numbers as top-level keys (so a record that
+    keeps only top-level scalars still has them)."""
+    f = bench_fit(args, rank, world, local, pkg, W, flushbuf, steps=3, warmup=3, classify=True,
+                  cpu=True)
+    fs = line["fit"] = fit_summary(f, peaks, f["what"])
+    cls = fs.get("status57_classified", {})
+    line.update(fit_fused=fs["value"], fit_fused_e2e=fs["e2e"],
+                fit_plain=fs["plain"]["value"], fused_over_plain=fs["fused_over_plain"],
+                fit_same_losses=fs["plain"]["same_losses"],
+                fit_roofline_frac=fs["roofline"]["frac"], fit_cpu_baseline=_cpu(fs),
+                fit_status_histogram=fs["status_histogram"],
+                fit_status_histogram_reference_mode=fs.get("status_histogram_reference_mode"),
+                fit_f32_only_failures=cls.get("rescue_on", {}).get("f32_only"),
+                fit_f32_only_failures_reference_mode=cls.get("reference_mode", {}).get("f32_only"))
+    f = bench_fit(args, rank, world, local, pkg, W, flushbuf, steps=2, warmup=3, N=1 << 20,
+                  cpu=True)
+    fs = line["fit_1m"] = fit_summary(f, peaks, f["what"])
+    line.update(fit_1m_fused=fs["value"], fit_1m_fused_e2e=fs["e2e"],
+                fit_1m_plain=fs["plain"]["value"], fused_over_plain_1m=fs["fused_over_plain"],
+                fit_1m_same_losses=fs["plain"]["same_losses"],
+                fit_1m_roofline_frac=fs["roofline"]["frac"], fit_1m_cpu_baseline=_cpu(fs),
+                fit_1m_status_histogram=fs["status_histogram"])
+    del f
+    score, fit, what = bench_implicit(args, rank, pkg, W, flushbuf, 3, 3, 1, 1)
+    fs = fit_summary(fit, peaks, what)
+    line["implicit"] = {"score": score, "fit": fs}
+    line.update(implicit_score=score["value"], implicit_score_e2e=score["e2e"],
+                implicit_score_roofline_frac=score["roofline"]["frac"],
+                implicit_score_cpu_baseline=_cpu(score),
+                implicit_fit_fused=fs["value"], implicit_fit_plain=fs["plain"]["value"],
+                implicit_fused_over_plain=fs["fused_over_plain"],
+                implicit_fit_roofline_frac=fs["roofline"]["frac"],
+                implicit_fit_cpu_baseline=_cpu(fs))
+    fit, what, rk = bench_c5(args, rank, pkg, W, flushbuf, 3, 3, 1, 1)
+    fs = fit_summary(fit, peaks, what)
+    line["c5"] = {"absolute_fit": fs, "rank": rk}
+    line.update(c5_fit_fused=fs["value"], c5_fit_plain=fs["plain"]["value"],
+                c5_fused_over_plain=fs["fused_over_plain"],
+                c5_fit_roofline_frac=fs["roofline"]["frac"], c5_fit_cpu_baseline=_cpu(fs),
+                c5_rank=rk["value"], c5_rank_e2e=rk["e2e"],
+                c5_rank_roofline_frac=rk["roofline"]["frac"], c5_rank_cpu_baseline=_cpu(rk))
+    vy = line["vary"] = bench_vary(args, rank, pkg, flushbuf, 5, 3)
+    line.update(vary_children=vy["value"], vary_children_e2e=vy["e2e"],
+                vary_same_as_cpu=vy["same_as_cpu"], vary_cpu_baseline=_cpu(vy))
+    if not args.no_cpu_baseline:
+        rf = line["refit"] = bench_refit(pkg, W)
+        line.update(refit_finalists=rf["value"], refit_cpu_baseline=_cpu(rf),
+                    refit_same_bits=rf["same_bits_as_port"])
 
 
 def single_gpu_line(args, world, r, metric, unit, what, extra):
@@ -734,21 +984,28 @@ def main():
     if rank == 0:
         if args.workload == "score":
             metric, unit = "expr_row_evals_per_s", "expr*row/s"
-            per_launch_ms = float(np.mean(r["dev_ms"]))
-            achieved = r["alg_ops"] / (per_launch_ms / 1e3) / 1e9
+            pr = r["prof"]
+            ms_f32 = float(np.mean([q["ms_f32"] for q in pr]))
+            ops_f32 = float(np.mean([q["ops_f32"] for q in pr]))
+            rows_f32 = float(np.mean([q["rows_f32"] for q in pr]))
+            rows_f64 = float(np.mean([q["rows_f64"] for q in pr]))
             peak = 148 * 128 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e9
-            achieved_f = r["alg_ops_finite"] / (per_launch_ms / 1e3) / 1e9
+            achieved = ops_f32 / (ms_f32 / 1e3) / 1e9
+            achieved_all = r["alg_ops"] / (ms_f32 / 1e3) / 1e9
             roof = {"bound": "fp32_issue", "achieved": achieved, "peak": peak,
-                    "unit": "Glane-op/s", "frac": achieved / peak,
-                    "traffic": 25.69e6,
+                    "unit": "Glane-op/s", "frac": achieved / peak, "traffic": SCORE_TRAFFIC,
+                    "kernel": "rc_score_kernel<256,true> (the f32 scoring launches)",
+                    "kernel_ms": ms_f32,
+                    "rest_ms": float(np.mean([q["ms_rest"] for q in pr])),
+                    "achieved_if_all_rows": achieved_all, "frac_if_all_rows": achieved_all / peak,
                     "finite_candidates": r["finite"],
-                    "achieved_finite_only": achieved_f, "frac_finite_only": achieved_f / peak,
-                    "note": "interpreter ops (bytecode ops + residual + loss) per row per "
-                            "candidate / event time of the scoring launches; peak = 148 SMs x "
-                            "128 FP32 lanes x sm_max_mhz from MEASURED_PEAKS.json; candidates "
-                            "proven non-finite stop early, *_finite_only counts the finite ones "
-                            "alone; traffic = dram read+write bytes of one scoring-kernel launch "
-                            "from an ncu capture of this workload"}
+                    "note": "lane-ops the interpreter actually ran (rows it evaluated x (postfix "
+                            "ops + residual + loss) of their candidate, counted by the kernel) / "
+                            "CUDA-event time of the f32 scoring launches on the library's "
+                            "stream; *_if_all_rows charges every candidate all N rows; peak = "
+                            "148 SMs x 128 FP32 lanes x sm_max_mhz (MEASURED_PEAKS.json); "
+                            "traffic = dram read+write bytes of one scoring-kernel launch (ncu, "
+                            "profiles/rc_score_kernel_P4096_N1M.md)"}
             cfg = {"workload": f"batched scoring, P={r['P']} programs, N={r['N']} rows x 5 "
                                f"features, squared error", "l2": "flushed between steps"}
         else:
@@ -764,6 +1021,12 @@ def main():
                 "e2e": {"value": e2e, "unit": unit, "h2d_bytes_per_step": r["h2d"],
                         "d2h_bytes_per_step": r["d2h"]},
                 "gpu_launches": r["launches"]}
+        if args.workload == "score":
+            # work actually done: a candidate stops at its first hard failure
+            line["value_evaluated"] = rows_f32 * world * args.steps / dev_s
+            line["rows_evaluated_per_step"] = rows_f32
+            line["rows_f64_rescored_per_step"] = rows_f64
+            line["candidates_finite"] = r["finite"]
         if args.workload == "fit" and "plain" in r:
             line["plain"] = r["plain"]
             line["fused_over_plain"] = value / r["plain"]["value"]
@@ -771,13 +1034,18 @@ def main():
         if not args.no_cpu_baseline and world == 1:
             threads = os.cpu_count() or 1
             if args.workload == "score":
-                v, dt = cpu_score_baseline(r["trees"], r["x"], r["y"], 1 << 16, 64, threads)
-                v1, _ = cpu_score_baseline(r["trees"], r["x"], r["y"], 1 << 16, 8, 1)
+                v, dt, ovals = cpu_score_baseline(r["trees"], r["x"], r["y"], SCORE_SAMPLE_ROWS,
+                                                  SCORE_SAMPLE_PROGS, threads, want_values=True)
+                v1, _ = cpu_score_baseline(r["trees"], r["x"], r["y"], SCORE_SAMPLE_ROWS, 8, 1)
                 line["cpu_baseline"] = {"value": v, "unit": unit, "cores": threads,
                                         "kind": "port", "cpu_model": cpu_model(),
                                         "value_1_thread": v1,
-                                        "sample": "64 programs x 65536 rows, f64 oracle "
-                                                  "(single thread: 8 programs)"}
+                                        "sample": f"the first {SCORE_SAMPLE_PROGS} programs x "
+                                                  f"the first {SCORE_SAMPLE_ROWS} rows of the "
+                                                  f"timed workload, f64 oracle (single thread: "
+                                                  f"8 programs)"}
+                line["parity"] = score_parity(pkg, r["trees"], r["x"], r["y"],
+                                              SCORE_SAMPLE_ROWS, ovals)
             else:
                 v, dt = cpu_fit_baseline(r["trees"], r["x"], r["y"], 1 << 14, 16, 20, threads)
                 line["cpu_baseline"] = {"value": v * (1 << 14) / r["N"], "unit": unit,
@@ -785,20 +1053,11 @@ def main():
                                         "cpu_model": cpu_model(),
                                         "sample": "16 candidates x 16384 rows x 20 iters, "
                                                   "scaled linearly in rows"}
+        if args.workload == "score" and "parity" in line:
+            line["parity_max_rel_err"] = line["parity"]["max_rel_err"]
+            line["parity_nonfinite_mismatch"] = line["parity"]["nonfinite_mismatch"]
         if args.workload == "score" and world == 1 and not args.no_secondary:
-            f = bench_fit(args, rank, world, local, pkg, W, flushbuf, steps=3, warmup=3)
-            line["fit"] = fit_summary(f, peaks, f["what"])
-            f = bench_fit(args, rank, world, local, pkg, W, flushbuf, steps=2, warmup=3,
-                          N=1 << 20)
-            line["fit_1m"] = fit_summary(f, peaks, f["what"])
-            del f
-            score, fit, what = bench_implicit(args, rank, pkg, W, flushbuf, 3, 3, 1, 1)
-            line["implicit"] = {"score": score, "fit": fit_summary(fit, peaks, what)}
-            fit, what, rk = bench_c5(args, rank, pkg, W, flushbuf, 3, 3, 1, 1)
-            line["c5"] = {"absolute_fit": fit_summary(fit, peaks, what), "rank": rk}
-            line["vary"] = bench_vary(args, rank, pkg, flushbuf, 5, 3)
-            if not args.no_cpu_baseline:
-                line["refit"] = bench_refit(pkg, W)
+            secondary(args, rank, world, local, pkg, W, flushbuf, peaks, line)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

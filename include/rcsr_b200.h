@@ -188,14 +188,19 @@ int rc_unified(void);
 
 /* ---- additive entry points (no counterpart in the reference ABI) ----- */
 
-/* Batched LM with the fused forward+adjoint sweep: one persistent launch per
-   node-count bucket runs every LM iteration of every candidate on the device,
-   fed by a cost-ordered work queue; the whole batch (upload, launches,
-   download) is replayed from a cached CUDA graph when the batch shape repeats.
-   Arguments, outputs and status codes are rc_fit_batch's; metric adds
-   6 = implicit (minimises sum w (f/|grad_x f|)^2 with a central-difference
-   constant Jacobian over the fused input-adjoint sweep). flags: bit 0 skips
-   the f64 polish. */
+/* Batched LM with the fused forward+adjoint sweep: every LM iteration of
+   every candidate runs on the device as a fixed sequence of steps (persistent
+   sweeps over (candidate, 4,096-row tile) work items, then a control kernel
+   that reduces, solves and queues each candidate's next sweep), captured once
+   as a CUDA graph per batch shape and replayed. Arguments, outputs and status
+   codes are rc_fit_batch's; metric adds 6 = implicit (minimises
+   sum w (f/|grad_x f|)^2 with an exact forward-over-reverse constant
+   Jacobian). flags: bit 0 skips the f64 re-baseline and polish; bit 1 turns
+   off the f64 rescue (by default a candidate whose f32 assembly meets a
+   non-finite row is re-assembled in f64 at the same constants and, when that
+   is finite, continues its LM in f64, as the CPU fit would; with the bit set
+   it stops there as the reference kernel does). rc_fit_batch and
+   rc_fit_batch_plain run with flags 0. */
 float rc_fit_batch_fused(void *ctx, const unsigned int *prog, const unsigned int *off,
                          const int *pcount, int nprog, int kmax, const double *c0,
                          const int *gauge, int iters, int metric, int flags, double *outc,
@@ -207,6 +212,13 @@ float rc_fit_batch_plain(void *ctx, const unsigned int *prog, const unsigned int
                          const int *pcount, int nprog, int kmax, const double *c0,
                          const int *gauge, int iters, int metric, double *outc,
                          double *outsse, int *outstatus);
+/* Sweeps each candidate of the context's last fit ran (valid until the next
+   call on the context), out[4 * cand + k]: k = 0 f32 assembly sweeps, 1 f32
+   objective sweeps, 2 f64 assembly sweeps (implicit: Jacobian sweeps), 3 f64
+   objective sweeps (implicit: cost sweeps); the correlation arm's assembly
+   and trial sweeps count as 0 and 1. Returns 0, or -1 when the last call was
+   not a fit of nprog candidates. No counterpart in the reference ABI. */
+int rc_last_fit_sweeps(void *ctx, int nprog, int *out);
 /* Per-row gradients of fit-record programs from the fused adjoint sweep, over
    rows [row0, row0 + nrows): want = 1 writes d f / d c_j (f32,
    out[(cand * nrows + r) * kmax + j]); want = 2 writes d f / d x_k
@@ -231,6 +243,17 @@ int rc_launch_count(void *ctx, unsigned long long *out);
    of cached entries, or -1. */
 int rc_autotune(void *ctx, const unsigned int *prog, const unsigned int *off, int nprog,
                 const char *path);
+
+/* Profile of the context's last scoring call (rc_score_batch, rc_eval,
+   rc_pool_score, ...): device ms of the f32 scoring kernels and of the rest
+   (finalize, the f64 rescore lane), the rows each interpreter actually
+   evaluated (a candidate stops at its first hard failure), and the same rows
+   weighted by their program's postfix ops + 2 (algorithmic lane-ops). Any
+   pointer may be NULL. Returns 0, or -1 before the first scoring call. No
+   counterpart in the reference ABI. */
+int rc_last_score_profile(void *ctx, float *ms_f32, float *ms_rest,
+                          unsigned long long *rows_f32, unsigned long long *rows_f64,
+                          unsigned long long *ops_f32, unsigned long long *ops_f64);
 
 /* Scoring for callers that cannot allocate device memory. No counterpart in
    the reference: it exists for host applications whose device memory is

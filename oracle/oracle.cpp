@@ -748,8 +748,19 @@ bool gn_trial(const Flat &f, const Rows &x, const double *y, const double *w,
     return true;
 }
 
+/* How the LM loop of `fit_lm` ended, for comparing the device's status
+   labels with the CPU's (the reference's CPU fit returns no status; this
+   records which of its `break`s was taken). */
+struct LmTrace {
+    int stop = 0;      /* 0 iterations / lambda / zero loss; 1 solve failed; 2 normal
+                          equations not finite */
+    int improved = 0;  /* an accepted step (LM or polish) */
+    int start_ok = 1;  /* the starting loss was finite */
+};
+
 /* fit.rs:2534-2624: `fit_lm`, the historical LM arm. */
-double fit_lm(Node &tree, const Rows &x, const double *y, const double *w, int iters)
+double fit_lm(Node &tree, const Rows &x, const double *y, const double *w, int iters,
+              LmTrace *trace = nullptr)
 {
     Flat f = flatten(tree);
     int k = f.nconst;
@@ -762,6 +773,7 @@ double fit_lm(Node &tree, const Rows &x, const double *y, const double *w, int i
     std::vector<double> best_c = c;
     if (iters == 0) return sse(f, x, y, w, c.data(), v);
     double best_sse = sse(f, x, y, w, c.data(), v);
+    if (trace) trace->start_ok = std::isfinite(best_sse) ? 1 : 0;
     double lambda = 1e-3;
     bool have = false;
     Normal ne;
@@ -770,11 +782,18 @@ double fit_lm(Node &tree, const Rows &x, const double *y, const double *w, int i
         if (!have) {
             have = normal_equations(f, x, y, w, c.data(), k, v, adj, grad, ne);
         }
-        if (!have) break;
+        if (!have) {
+            if (trace) trace->stop = 2;
+            break;
+        }
         std::vector<double> trial;
         double tsse;
-        if (!gn_trial(f, x, y, w, c, lambda, k, ne, v, trial, tsse)) break;
+        if (!gn_trial(f, x, y, w, c, lambda, k, ne, v, trial, tsse)) {
+            if (trace) trace->stop = 1;
+            break;
+        }
         if (tsse < best_sse) {
+            if (trace) trace->improved = 1;
             c = trial;
             best_sse = tsse;
             best_c = c;
@@ -794,6 +813,7 @@ double fit_lm(Node &tree, const Rows &x, const double *y, const double *w, int i
         double tsse;
         if (!gn_trial(f, x, y, w, best_c, 0.0, k, n2, v, trial, tsse)) break;
         if (tsse < best_sse) {
+            if (trace) trace->improved = 1;
             best_c = trial;
             best_sse = tsse;
         } else {
@@ -977,9 +997,121 @@ double score_unweighted(const double *pred, const double *y, int n, int m, int k
     }
 }
 
-/* metrics.rs:985-1075: `score_weighted` (regression block). */
+/* --- classification objectives (metrics.rs:1467-1579, :705-763) --------- */
+enum {
+    M_LOG_LOSS = 10, M_BRIER = 11, M_HINGE_SIGMOID = 12, M_HINGE_ORDINARY = 13,
+    M_HINGE_SQUARED = 14
+};
+
+/* metrics.rs:1534-1542: the stable logistic. */
+double sigmoid_stable(double x)
+{
+    if (x >= 0.0) return 1.0 / (1.0 + std::exp(-x));
+    const double e = std::exp(x);
+    return e / (1.0 + e);
+}
+
+/* metrics.rs:1547-1550: ln(1 + exp(-u)) as max(-u, 0) + ln_1p(exp(-|u|)). */
+double softplus_neg(double u)
+{
+    const double a = std::fabs(u);
+    return std::fmax(-u, 0.0) + std::log1p(std::exp(-a));
+}
+
+/* metrics.rs:1553-1579: one row, p the logit, l in {0, 1}. */
+double classification_row_loss(double p, double l, int m)
+{
+    const double t = 2.0 * l - 1.0;
+    const double u = t * p;
+    switch (m) {
+        case M_LOG_LOSS: return softplus_neg(u);
+        case M_BRIER: {
+            const double d = sigmoid_stable(p) - l;
+            return d * d;
+        }
+        case M_HINGE_SIGMOID: {
+            const double sg = 2.0 * sigmoid_stable(p) - 1.0;
+            return std::fmax(1.0 - t * sg, 0.0);
+        }
+        case M_HINGE_ORDINARY: return std::fmax(1.0 - u, 0.0);
+        case M_HINGE_SQUARED: {
+            const double h = std::fmax(1.0 - u, 0.0);
+            return h * h;
+        }
+        default: return NaN;
+    }
+}
+
+/* metrics.rs:1467-1475 `binary_labels` (w == NULL) and :1511-1532
+   `binary_labels_weighted`: l = [y > (min + max) / 2] over the positive-weight
+   rows. Returns false when a positive-weight target is not finite or none
+   exists. */
+bool binary_labels(const double *y, const double *w, int n, std::vector<double> &l)
+{
+    double lo = INF, hi = -INF;
+    for (int i = 0; i < n; ++i) {
+        if (w && !(w[i] > 0.0)) continue;
+        if (w && !std::isfinite(y[i])) return false;
+        lo = std::fmin(lo, y[i]);
+        hi = std::fmax(hi, y[i]);
+    }
+    if (w && (!std::isfinite(lo) || !std::isfinite(hi))) return false;
+    const double mid = 0.5 * (lo + hi);
+    l.assign(n, 0.0);
+    for (int i = 0; i < n; ++i) l[i] = ((!w || w[i] > 0.0) && y[i] > mid) ? 1.0 : 0.0;
+    return true;
+}
+
+/* metrics.rs:705-763 `score_native_weighted`, classification branch: the
+   weighted mean row loss; `*status` 0 ok, 2 a non-finite prediction (in a
+   positive-weight row) or unusable target, 4 all-zero weights, 1 invalid
+   weights. */
+double score_classification(const double *pred, const double *y, const double *w, int n, int m,
+                            int *status)
+{
+    *status = 1;
+    if (n == 0) return INF;
+    if (w) {
+        double total = 0.0;
+        for (int i = 0; i < n; ++i) {
+            if (!std::isfinite(w[i]) || w[i] < 0.0) return INF;
+            total += w[i];
+        }
+        if (!(total > 0.0)) {
+            *status = 4;
+            return INF;
+        }
+    }
+    for (int i = 0; i < n; ++i)
+        if ((!w || w[i] > 0.0) && !std::isfinite(pred[i])) {
+            *status = 2;
+            return INF;
+        }
+    double denom = 0.0;
+    if (w)
+        for (int i = 0; i < n; ++i) denom += w[i];
+    else
+        denom = (double)n;
+    std::vector<double> l;
+    if (!binary_labels(y, w, n, l)) {
+        *status = 2;
+        return INF;
+    }
+    double sum = 0.0;
+    for (int i = 0; i < n; ++i)
+        if (!w || w[i] > 0.0) sum += (w ? w[i] : 1.0) * classification_row_loss(pred[i], l[i], m);
+    *status = 0;
+    return sum / denom;
+}
+
+/* metrics.rs:985-1075: `score_weighted` (regression block); the
+   classification codes go to `score_native_weighted`'s branch. */
 double score_weighted(const double *pred, const double *y, const double *w, int n, int m, int k)
 {
+    if (m >= M_LOG_LOSS && m <= M_HINGE_SQUARED) {
+        int st = 0;
+        return score_classification(pred, y, w, n, m, &st);
+    }
     if (!w) return score_unweighted(pred, y, n, m, k);
     if (n == 0) return INF;
     double total = 0.0;
@@ -1474,6 +1606,132 @@ int or_centred_ranks_doubled(const double *v, int n, int64_t *out)
     std::vector<int64_t> a;
     if (!centred_ranks_doubled(v, n, a)) return -1;
     std::memcpy(out, a.data(), sizeof(int64_t) * (size_t)n);
+    return 0;
+}
+
+/* fit_lm (fit.rs:2534-2624) with how its LM loop ended: label[0] = 0 when it
+   ran out of iterations, lambda or loss, 1 when a damped solve failed, 2 when
+   the normal equations were not finite; label[1] = an accepted step;
+   label[2] = a finite starting loss. Constants are written back. */
+double or_fit_lm_traced(const int *op, double *val, int nn, const double *cols, int n, int v,
+                        const double *y, const double *w, int iters, int *label)
+{
+    Node t;
+    if (!load_tree(op, val, nn, t)) return NaN;
+    Rows x{cols, n, v};
+    LmTrace tr;
+    double r = fit_lm(t, x, y, w, iters, &tr);
+    label[0] = tr.stop;
+    label[1] = tr.improved;
+    label[2] = tr.start_ok;
+    int pos = 0;
+    store_tree(t, val, pos);
+    return r;
+}
+
+/* The tree's constants in the flat evaluator's slot order (fit.rs:1068-1196
+   `flatten`, the order proposals and `write_constants` use). Returns the
+   count, or -1. */
+int or_flat_constants(const int *op, const double *val, int nn, double *out)
+{
+    Node t;
+    if (!load_tree(op, val, nn, t)) return -1;
+    Flat f = flatten(t);
+    for (size_t i = 0; i < f.op.size(); ++i)
+        if (f.cslot[i] >= 0) out[f.cslot[i]] = f.val[i];
+    return f.nconst;
+}
+
+/* Whether fit.rs's `normal_equations` (fit.rs:1774-1827) are finite at the
+   tree's constants: 1 finite, 0 not, -1 for a bad tree. */
+int or_normal_equations_ok(const int *op, const double *val, int nn, const double *cols, int n,
+                           int v, const double *y, const double *w)
+{
+    Node t;
+    if (!load_tree(op, val, nn, t)) return -1;
+    Rows x{cols, n, v};
+    Flat f = flatten(t);
+    const int k = f.nconst;
+    const size_t m = f.op.size();
+    std::vector<double> c(k), vv(std::max<size_t>(m, 1)), adj(m), grad(k);
+    for (size_t i = 0; i < m; ++i)
+        if (f.cslot[i] >= 0) c[f.cslot[i]] = f.val[i];
+    Normal ne;
+    return normal_equations(f, x, y, w, c.data(), k, vv, adj, grad, ne) ? 1 : 0;
+}
+
+/* fit/gpu.rs:245-317 `verify_proposal` for the metrics the device fit
+   serves here (squared, absolute, log-squashed; the signed projection and
+   the rank family are not restated): apply the proposal to a clone and
+   accept it only when it is finite and no worse than the starting constants,
+   on the weighted SSE of the flat evaluator for squared (fit.rs `sse`) and on
+   the configured objective otherwise. Returns 0 (accepted, the constants are
+   written into `val` and `*value` is the proposal's exact objective) or 1
+   (rejected, `val` untouched). */
+int or_verify_proposal(const int *op, double *val, int nn, const double *cols, int n, int v,
+                       const double *y, const double *w, int metric, const double *proposal,
+                       int np, double *value)
+{
+    Node t;
+    if (!load_tree(op, val, nn, t)) return 1;
+    Rows x{cols, n, v};
+    Flat f = flatten(t);
+    if (np != f.nconst) return 1;
+    for (int i = 0; i < np; ++i)
+        if (!std::isfinite(proposal[i])) return 1;
+    std::vector<double> c0(f.nconst);
+    for (size_t i = 0; i < f.op.size(); ++i)
+        if (f.cslot[i] >= 0) c0[f.cslot[i]] = f.val[i];
+    Node trial = t;
+    int slot = 0;
+    write_constants(trial, proposal, slot);
+    double start, cand;
+    if (metric == M_SQUARED) {
+        std::vector<double> vv(std::max<size_t>(f.op.size(), 1));
+        start = sse(f, x, y, w, c0.data(), vv);
+        cand = sse(f, x, y, w, proposal, vv);
+    } else {
+        start = metric_score(t, x, y, w, metric);
+        cand = metric_score(trial, x, y, w, metric);
+    }
+    if (!std::isfinite(cand) || !std::isfinite(start) || cand > start) return 1;
+    int pos = 0;
+    store_tree(trial, val, pos);
+    *value = cand;
+    return 0;
+}
+
+/* fit/gpu.rs:176-213 `fit_batch_verified`, one tree: a missing proposal
+   (np < 0: the device status was not usable or a constant not finite) or a
+   rejected one falls back on the exact CPU fit from the starting constants
+   (`fit_weighted_metric`). Returns the tree's score; *state = 0 device
+   answer accepted, 1 rejected (CPU fit), 2 no proposal (CPU fit). */
+double or_fit_verified(const int *op, double *val, int nn, const double *cols, int n, int v,
+                       const double *y, const double *w, int iters, int metric,
+                       const double *proposal, int np, int *state)
+{
+    double value = NaN;
+    if (np >= 0) {
+        if (or_verify_proposal(op, val, nn, cols, n, v, y, w, metric, proposal, np, &value) ==
+            0) {
+            *state = 0;
+            return value;
+        }
+        *state = 1;
+    } else {
+        *state = 2;
+    }
+    return or_fit(op, val, nn, cols, n, v, y, w, iters, metric);
+}
+
+/* The binary labels a classification objective derives from y
+   (metrics.rs:1467-1532): out[i] = 1 or 0. Returns 0, or -1 when the
+   weighted rule has no usable target. */
+int or_binary_labels(const double *y, const double *w, int n, double *out)
+{
+    std::vector<double> l;
+    if (!binary_labels(y, w, n, l)) return -1;
+    std::memcpy(out, l.data(), sizeof(double) * (size_t)n);
     return 0;
 }
 

@@ -20,6 +20,7 @@ LIB_PATH = os.path.join(HERE, "liboracle.so")
 SQUARED, ABSOLUTE, LOG_SQUASHED, SIGNED, MAXIMUM = 0, 1, 2, 3, 4
 CORRELATION, CORRELATION_SIGNED, AIC, AICC, BIC = 5, 6, 7, 8, 9
 MEDIAN, INTERQUARTILE = 15, 16
+LOG_LOSS, BRIER, HINGE_SIGMOID, HINGE_ORDINARY, HINGE_SQUARED = 10, 11, 12, 13, 14
 RANK_CORRELATION, RANK_CORRELATION_SIGNED = 20, 21
 
 _lib = None
@@ -58,6 +59,14 @@ def lib():
             "or_rank_sums": (ci, [f64p, f64p, ci, u64p]),
             "or_centred_ranks_doubled": (ci, [f64p, ci, i64p]),
             "or_erf": (cd, [cd]),
+            "or_fit_lm_traced": (cd, [i32p, f64p, ci, f64p, ci, ci, f64p, f64p, ci, i32p]),
+            "or_flat_constants": (ci, [i32p, f64p, ci, f64p]),
+            "or_binary_labels": (ci, [f64p, f64p, ci, f64p]),
+            "or_normal_equations_ok": (ci, [i32p, f64p, ci, f64p, ci, ci, f64p, f64p]),
+            "or_verify_proposal": (ci, [i32p, f64p, ci, f64p, ci, ci, f64p, f64p, ci, f64p, ci,
+                                        f64p]),
+            "or_fit_verified": (cd, [i32p, f64p, ci, f64p, ci, ci, f64p, f64p, ci, ci, f64p, ci,
+                                     i32p]),
             "orv_philox": (None, [u32, u32, u32, u32, u32, ci, u32p]),
             "orv_hash": (ctypes.c_uint64, [u32p, ci]),
             "orv_spans": (ci, [u32p, ci]),
@@ -139,6 +148,80 @@ def fit(t, cols, n, v, y, iters, metric=SQUARED, w=None):
     out = t.clone()
     out.set_prefix_values(vals)
     return r, out
+
+
+def fit_lm_traced(t, cols, n, v, y, iters, w=None):
+    """fit::fit_lm with how its loop ended; returns (sse, fitted tree,
+    (stop, improved, start_ok)), stop 0 = ran out of iterations / lambda /
+    loss, 1 = a damped solve failed, 2 = the normal equations were not
+    finite."""
+    ops, vals = _tree(t)
+    c = _cols(cols)
+    y = np.ascontiguousarray(y, np.float64)
+    w = None if w is None else np.ascontiguousarray(w, np.float64)
+    lab = np.zeros(3, np.int32)
+    r = lib().or_fit_lm_traced(_ptr(ops, ctypes.c_int32), _ptr(vals, ctypes.c_double), len(ops),
+                               _ptr(c, ctypes.c_double), n, v, _ptr(y, ctypes.c_double),
+                               _ptr(w, ctypes.c_double), iters, _ptr(lab, ctypes.c_int32))
+    out = t.clone()
+    out.set_prefix_values(vals)
+    return r, out, tuple(int(q) for q in lab)
+
+
+def binary_labels(y, w=None):
+    """metrics::binary_labels(_weighted): l = [y > (min + max) / 2]."""
+    y = np.ascontiguousarray(y, np.float64)
+    w = None if w is None else np.ascontiguousarray(w, np.float64)
+    out = np.zeros(len(y), np.float64)
+    rc = lib().or_binary_labels(_ptr(y, ctypes.c_double), _ptr(w, ctypes.c_double), len(y),
+                                _ptr(out, ctypes.c_double))
+    return None if rc != 0 else out
+
+
+def flat_constants(t):
+    """The tree's constants in the flat evaluator's slot order."""
+    ops, vals = _tree(t)
+    out = np.zeros(max(len(ops), 1), np.float64)
+    k = lib().or_flat_constants(_ptr(ops, ctypes.c_int32), _ptr(vals, ctypes.c_double), len(ops),
+                                _ptr(out, ctypes.c_double))
+    assert k >= 0
+    return out[:k].copy()
+
+
+def normal_equations_ok(t, cols, n, v, y, w=None):
+    """Whether fit.rs `normal_equations` are finite at the tree's constants."""
+    ops, vals = _tree(t)
+    c = _cols(cols)
+    y = np.ascontiguousarray(y, np.float64)
+    w = None if w is None else np.ascontiguousarray(w, np.float64)
+    return lib().or_normal_equations_ok(_ptr(ops, ctypes.c_int32), _ptr(vals, ctypes.c_double),
+                                        len(ops), _ptr(c, ctypes.c_double), n, v,
+                                        _ptr(y, ctypes.c_double), _ptr(w, ctypes.c_double)) == 1
+
+
+def fit_verified(t, cols, n, v, y, iters, proposal, metric=SQUARED, w=None):
+    """fit::gpu::fit_batch_verified for one tree: `proposal` (constants in
+    flat slot order, or None when the device gave no usable answer) goes
+    through verify_proposal; a rejected or missing one falls back on the CPU
+    fit. Returns (score, tree, state) with state 0 = device answer accepted,
+    1 = rejected, 2 = no proposal."""
+    ops, vals = _tree(t)
+    c = _cols(cols)
+    y = np.ascontiguousarray(y, np.float64)
+    w = None if w is None else np.ascontiguousarray(w, np.float64)
+    if proposal is None:
+        prop, npr = None, -1
+    else:
+        prop = np.ascontiguousarray(proposal, np.float64)
+        npr = len(prop)
+    st = np.zeros(1, np.int32)
+    r = lib().or_fit_verified(_ptr(ops, ctypes.c_int32), _ptr(vals, ctypes.c_double), len(ops),
+                              _ptr(c, ctypes.c_double), n, v, _ptr(y, ctypes.c_double),
+                              _ptr(w, ctypes.c_double), iters, metric,
+                              _ptr(prop, ctypes.c_double), npr, _ptr(st, ctypes.c_int32))
+    out = t.clone()
+    out.set_prefix_values(vals)
+    return r, out, int(st[0])
 
 
 def flat_sse(t, cols, n, v, y, w=None):

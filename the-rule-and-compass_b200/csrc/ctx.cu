@@ -34,6 +34,9 @@ size_t rc_take(size_t *cur, size_t bytes)
 
 int rc_reserve(RcCtx *c, size_t dev_bytes, size_t host_bytes)
 {
+    /* every call reuses the region: the last fit's state is gone */
+    c->fit_state = nullptr;
+    c->fit_state_n = 0;
     if (dev_bytes < 256) dev_bytes = 256;
     if (host_bytes < 256) host_bytes = 256;
     if (dev_bytes > c->dev_bytes) {
@@ -196,7 +199,9 @@ void *rc_create(const float *cols, int n, int v, const float *y)
     if (c->sm_count <= 0) c->sm_count = 1;
     if (cudaStreamCreateWithFlags(&c->s, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&c->t0) != cudaSuccess || cudaEventCreate(&c->t1) != cudaSuccess ||
-        cudaEventCreateWithFlags(&c->ev_done, cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventCreateWithFlags(&c->ev_done, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreate(&c->sp[0]) != cudaSuccess || cudaEventCreate(&c->sp[1]) != cudaSuccess ||
+        cudaEventCreate(&c->sp[2]) != cudaSuccess) {
         cudaGetLastError();
         delete c;
         return nullptr;
@@ -242,6 +247,8 @@ void rc_destroy(void *ctx)
     if (c->t0) cudaEventDestroy(c->t0);
     if (c->t1) cudaEventDestroy(c->t1);
     if (c->ev_done) cudaEventDestroy(c->ev_done);
+    for (int i = 0; i < 3; ++i)
+        if (c->sp[i]) cudaEventDestroy(c->sp[i]);
     if (c->s) cudaStreamDestroy(c->s);
     delete c;
 }

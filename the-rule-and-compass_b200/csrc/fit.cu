@@ -34,6 +34,7 @@
  */
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -75,10 +76,59 @@ struct FitState {
     double jtr[FT_MAX_CONST];
     double lambda, best, start_best;
     double rho, svar, syy; /* correlation arm: moments of the last assembly */
+    double req_lambda;     /* damping of the requested solve */
     int pc, op, sel;
     int status, round, it, half, pit;
     int assembled, improved, rank, skip, start;
+    int req, sv;           /* solve request (FT_REQ_*) and the answered label */
+    int f64;               /* 0: f32 sweeps; 1: switched to f64 sweeps after an f32-only
+                              failure, loss not yet re-baselined; 2: f64, re-baselined */
+    int nsw[4];            /* sweeps run: f32 assembly, f32 objective, f64 assembly, f64
+                              objective (correlation and implicit kinds count in their
+                              class: CASM / CSCORE as f32, IJAC / ICOST as f64) */
 };
+
+/* Fit flags of rc_fit_batch_fused. */
+#define FT_FLAG_NO_POLISH 1 /* skip the f64 re-baseline and polish */
+#define FT_FLAG_NO_RESCUE 2 /* keep the reference kernel's f32-only failures */
+
+/* The controller's thread 0 runs the state machine; a damped solve is
+   handed to warp 0 (ft_solve_warp) by a request in the state, and the state
+   machine resumes at the same state with the answer. */
+enum { FT_REQ_NONE = 0, FT_REQ_SOLVE = 1, FT_REQ_DONE = 2 };
+
+__device__ __forceinline__ void ft_request_solve(FitState &st, double lambda)
+{
+    st.req = FT_REQ_SOLVE;
+    st.req_lambda = lambda;
+    st.op = FOP_NONE;
+}
+
+/* The answer to the last request (and clears it). */
+__device__ __forceinline__ int ft_take_solve(FitState &st)
+{
+    st.req = FT_REQ_NONE;
+    return st.sv;
+}
+
+/* The f64 rescue of an f32 assembly that failed. The f32 sweep marks a row
+   bad when its prediction, residual or Jacobian entry is not finite (or the
+   prediction exceeds 1e30) in f32, where the CPU fit's f64 arithmetic may
+   well be finite (an exp beyond 88, a square of a denominator below 1e-19).
+   Instead of stopping there (status 2, reported 5 or 7, as the reference
+   kernel does), the candidate's assembly is re-run in f64 at the same
+   constants, and from then on every sweep of its LM runs in f64: it stops
+   only where the CPU fit's normal equations would stop too (a non-finite
+   f64 residual or Jacobian entry). Returns true when the f64 assembly was
+   queued (the state is re-entered with its outputs). */
+__device__ __forceinline__ bool ft_rescue(int flags, FitState &st, int rb)
+{
+    if (!rb || st.f64 || (flags & FT_FLAG_NO_RESCUE)) return false;
+    st.f64 = 1;
+    st.op = FOP_ASM64;
+    st.sel = 0;
+    return true;
+}
 
 struct FitArgs {
     const float *cols;
@@ -1076,6 +1126,9 @@ __device__ void ft_advance(const FitArgs &a, FitState &st, int cand, int p, doub
         switch (st.pc) {
             case PC_INIT:
                 st.lambda = 1e-3;
+                st.req = FT_REQ_NONE;
+                st.f64 = 0;
+                st.nsw[0] = st.nsw[1] = st.nsw[2] = st.nsw[3] = 0;
                 st.status = 0;
                 st.best = 0.0;
                 st.rank = st.skip = st.improved = st.start = 0;
@@ -1104,6 +1157,13 @@ __device__ void ft_advance(const FitArgs &a, FitState &st, int cand, int p, doub
                 st.pc = PC_AFTER_FIRST_ASM;
                 return;
             case PC_AFTER_FIRST_ASM:
+                if (ft_rescue(a.flags, st, rb)) return;
+                /* in f64 a row skipped for a non-finite Jacobian entry fails
+                   the assembly, as it fails the CPU's normal equations */
+                if (st.f64) {
+                    rb = rb || rs;
+                    st.f64 = 2;
+                }
                 st.best = rl;
                 st.start = rb ? 0 : 1;
                 st.assembled = 1;
@@ -1131,7 +1191,7 @@ __device__ void ft_advance(const FitArgs &a, FitState &st, int cand, int p, doub
                     break;
                 }
                 if (!st.assembled) {
-                    st.op = FOP_ASM32;
+                    st.op = st.f64 ? FOP_ASM64 : FOP_ASM32;
                     st.sel = 0;
                     st.pc = PC_AFTER_ASM;
                     return;
@@ -1139,6 +1199,8 @@ __device__ void ft_advance(const FitArgs &a, FitState &st, int cand, int p, doub
                 st.pc = PC_SOLVE;
                 break;
             case PC_AFTER_ASM:
+                if (ft_rescue(a.flags, st, rb)) return;
+                if (st.f64) rb = rb || rs;
                 st.assembled = 1;
                 if (rb) {
                     st.status = 2;
@@ -1146,10 +1208,19 @@ __device__ void ft_advance(const FitArgs &a, FitState &st, int cand, int p, doub
                     st.pc = PC_ROUND;
                     break;
                 }
+                if (st.f64 == 1) {
+                    /* just switched: the loss to beat is the f64 one */
+                    st.best = rl;
+                    st.f64 = 2;
+                }
                 st.pc = PC_SOLVE;
                 break;
             case PC_SOLVE: {
-                const int sv = ft_solve(st.jtj, st.jtr, st.lambda, p, delta, L);
+                if (st.req != FT_REQ_DONE) {
+                    ft_request_solve(st, st.lambda);
+                    return;
+                }
+                const int sv = ft_take_solve(st);
                 if (sv == 1) {
                     st.status = 1;
                     st.round++;
@@ -1159,7 +1230,7 @@ __device__ void ft_advance(const FitArgs &a, FitState &st, int cand, int p, doub
                 if (sv == 4) st.rank = 1;
                 for (int j = 0; j < p; ++j) st.trial[j] = fmin(1e6, fmax(-1e6, st.c[j] + delta[j]));
                 st.half = 0;
-                st.op = FOP_LOSS32;
+                st.op = st.f64 ? FOP_LOSS64 : FOP_LOSS32;
                 st.sel = 1;
                 st.pc = PC_AFTER_TRIAL;
                 return;
@@ -1170,7 +1241,7 @@ __device__ void ft_advance(const FitArgs &a, FitState &st, int cand, int p, doub
                 if (irls && st.half < 2 && !(tsse < st.best)) {
                     for (int j = 0; j < p; ++j) st.trial[j] = st.c[j] + 0.5 * (st.trial[j] - st.c[j]);
                     st.half++;
-                    st.op = FOP_LOSS32;
+                    st.op = st.f64 ? FOP_LOSS64 : FOP_LOSS32;
                     st.sel = 1;
                     return;
                 }
@@ -1198,7 +1269,7 @@ __device__ void ft_advance(const FitArgs &a, FitState &st, int cand, int p, doub
                 break;
             }
             case PC_REBASE:
-                if (st.status == 0 && !(a.flags & 1)) {
+                if (st.status == 0 && !(a.flags & FT_FLAG_NO_POLISH)) {
                     st.op = FOP_LOSS64;
                     st.sel = 0;
                     st.pc = PC_AFTER_REBASE;
@@ -1221,13 +1292,17 @@ __device__ void ft_advance(const FitArgs &a, FitState &st, int cand, int p, doub
                 st.pc = PC_AFTER_PASM;
                 return;
             case PC_AFTER_PASM: {
-                if (rs) st.skip = 1;
-                if (rb) {
-                    st.status = 2;
-                    st.pc = PC_END;
-                    break;
+                if (st.req != FT_REQ_DONE) {
+                    if (rs) st.skip = 1;
+                    if (rb) {
+                        st.status = 2;
+                        st.pc = PC_END;
+                        break;
+                    }
+                    ft_request_solve(st, 0.0);
+                    return;
                 }
-                const int sv = ft_solve(st.jtj, st.jtr, 0.0, p, delta, L);
+                const int sv = ft_take_solve(st);
                 if (sv == 1) {
                     st.pc = PC_END;
                     break;
@@ -1328,8 +1403,12 @@ __device__ void ft_advance(const FitArgs &a, FitState &st, int cand, int p, doub
                 st.pc = PC_C_SOLVE;
                 break;
             case PC_C_SOLVE: {
-                ft_corr_mask(st, p, a.metric, a.gauge + 2 * cand);
-                const int sv = ft_solve(st.jtj, st.jtr, st.lambda, p, delta, L);
+                if (st.req != FT_REQ_DONE) {
+                    ft_corr_mask(st, p, a.metric, a.gauge + 2 * cand);
+                    ft_request_solve(st, st.lambda);
+                    return;
+                }
+                const int sv = ft_take_solve(st);
                 if (sv == 1) {
                     st.status = 1;
                     st.pc = PC_C_END;
@@ -1375,13 +1454,17 @@ __device__ void ft_advance(const FitArgs &a, FitState &st, int cand, int p, doub
                 st.pc = PC_C_AFTER_PASM;
                 return;
             case PC_C_AFTER_PASM: {
-                if (rb) {
-                    st.status = 2;
-                    st.pc = PC_C_END;
-                    break;
+                if (st.req != FT_REQ_DONE) {
+                    if (rb) {
+                        st.status = 2;
+                        st.pc = PC_C_END;
+                        break;
+                    }
+                    ft_corr_mask(st, p, a.metric, a.gauge + 2 * cand);
+                    ft_request_solve(st, 0.0);
+                    return;
                 }
-                ft_corr_mask(st, p, a.metric, a.gauge + 2 * cand);
-                const int sv = ft_solve(st.jtj, st.jtr, 0.0, p, delta, L);
+                const int sv = ft_take_solve(st);
                 if (sv == 1) {
                     st.pc = PC_C_END;
                     break;
@@ -1610,7 +1693,29 @@ __global__ void __launch_bounds__(FT_CTRL_T) ft_control(FitArgs a, int q, int in
             s_skip = skip;
         }
         __syncthreads();
-        if (tid == 0) ft_advance(a, sst, cand, p, s_loss, s_bad, s_skip, L, delta);
+        /* the state machine on thread 0; a solve it requests runs on warp 0
+           and the state machine resumes (at most one solve per step) */
+        for (int round = 0; round < 4; ++round) {
+            if (tid == 0) ft_advance(a, sst, cand, p, s_loss, s_bad, s_skip, L, delta);
+            __syncthreads();
+            if (sst.req != FT_REQ_SOLVE) break;
+            if (tid < 32) {
+                const int sv = ft_solve_warp(sst.jtj, sst.jtr, sst.req_lambda, p, delta);
+                if (tid == 0) {
+                    sst.sv = sv;
+                    sst.req = FT_REQ_DONE;
+                }
+            }
+            __syncthreads();
+        }
+        if (tid == 0 && sst.op != FOP_NONE) {
+            const int op = sst.op;
+            const int k = (op == FOP_ASM32 || op == FOP_CASM)      ? 0
+                          : (op == FOP_LOSS32 || op == FOP_CSCORE) ? 1
+                          : (op == FOP_ASM64 || ft_op_ijac(op))     ? 2
+                                                                    : 3;
+            sst.nsw[k]++;
+        }
         __syncthreads();
         {
             const double *src = reinterpret_cast<const double *>(&sst);
@@ -2039,7 +2144,8 @@ int max_steps(int iters, int metric)
        four polish assemblies and trials */
     if (metric == FM_CORRELATION || metric == FM_CORRELATION_SIGNED) return 2 + 2 * it + 8 + 2;
     const int per = metric == FM_ABSOLUTE ? 4 : 2;
-    return 2 + per * it + 1 + 12 + 1;
+    /* + 1: the f64 re-assembly of an f32-only failure (once per fit) */
+    return 2 + per * it + 1 + 12 + 1 + 1;
 }
 
 struct SweepLaunch {
@@ -2392,7 +2498,9 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     } else {
         sw[nk] = sweep4_launch<FOP_ASM32, FT_ASM_T>(c, b, Wmax); ++nk;
         sw[nk] = sweep4_launch<FOP_LOSS32, 128>(c, b, Wmax); ++nk;
-        if (!(flags & 1)) {
+        /* the f64 sweeps serve the polish and the f64 rescue */
+        if ((flags & (FT_FLAG_NO_POLISH | FT_FLAG_NO_RESCUE)) !=
+            (FT_FLAG_NO_POLISH | FT_FLAG_NO_RESCUE)) {
             sw[nk] = sweep4_launch<FOP_ASM64, FT_ASM_T>(c, b, Wmax); ++nk;
             sw[nk] = sweep4_launch<FOP_LOSS64, 128>(c, b, Wmax); ++nk;
         }
@@ -2484,6 +2592,9 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     cudaEventElapsedTime(&ms, c->t0, c->t1);
     st->kernel_ms = ms;
     st->batch = nprog;
+    c->fit_state = dev + o_state;
+    c->fit_state_n = nprog;
+    c->fit_state_stride = sizeof(FitState);
     c->warm = 1;
     c->batches++;
     return ms;
@@ -2518,6 +2629,24 @@ float rc_fit_batch_plain(void *ctx, const unsigned int *prog, const unsigned int
 {
     return fit_run((RcCtx *)ctx, prog, off, pcount, nprog, kmax, c0, gauge, iters, metric, 0, outc,
                    outsse, outstatus, 1);
+}
+
+/* Sweeps each candidate of the context's last fit ran, out[4 * cand + k]:
+   k = 0 f32 assemblies, 1 f32 objective sweeps, 2 f64 assemblies (implicit
+   Jacobians), 3 f64 objective sweeps (implicit costs). Returns 0, or -1 when
+   no fit of nprog candidates is the last call's. */
+int rc_last_fit_sweeps(void *ctx, int nprog, int *out)
+{
+    RcCtx *c = (RcCtx *)ctx;
+    if (!c || !out || !c->fit_state || nprog != c->fit_state_n) return -1;
+    const size_t off = offsetof(FitState, nsw);
+    if (cudaMemcpy2DAsync(out, 4 * sizeof(int), c->fit_state + off, c->fit_state_stride,
+                          4 * sizeof(int), (size_t)nprog, cudaMemcpyDeviceToHost,
+                          c->s) != cudaSuccess) {
+        cudaGetLastError();
+        return -1;
+    }
+    return rc_finish(c);
 }
 
 int rc_fit_kernel_info(int kmax, int *threads, int *smem_bytes, int *max_constants)

@@ -3,7 +3,8 @@
  * Device building blocks of the batched fit: per-row forward and reverse
  * sweeps over fit records (f32 and f64), the per-row objective pieces, the
  * block reductions, the 4x4 register-blocked SYRK of the augmented Gram, the
- * damped solves, and the implicit-metric residual.
+ * damped solves (a warp-cooperative Cholesky and the implicit arm's Gaussian
+ * elimination), and the implicit-metric residual.
  *
  * Semantics follow the reference's batched fit (my-version/src/cuda/eval.cu:
  * 1106-2606) and the CPU fitter it stands in for (my-version/src/fit.rs:
@@ -262,69 +263,106 @@ __device__ __forceinline__ void ft_syrk_finish(const Syrk &s, double acc[16], do
     __syncthreads();
 }
 
-/* ---- the damped solve (eval.cu:1873-1949 `ft_solve`) ----------------- */
+/* ---- the damped solve on one warp --------------------------------------
 
-__device__ inline int ft_solve(const double *jtj, const double *jtr, double lambda, int p, double *delta,
-                        double *L)
+   The step of one LM iteration solves (S + lambda diag S + 1e-12 I) u = -D^-1 g
+   for the Jacobi-equilibrated normal matrix S = D^-1 (J^T J) D^-1,
+   D = sqrt(diag J^T J), and returns delta = D^-1 u. The answer and its labels
+   are the reference's (eval.cu:1873-1949, fit.rs:1686-1760): 1 when a diagonal
+   entry of J^T J is not positive and finite, a scaled entry is not finite, or
+   the damped factor breaks down (pivot <= 1e-18); 4 (rank deficient, the step
+   is still returned) when the undamped factor of S breaks down or
+   ln det S < ln 1e-12; else 0.
+
+   Layout: lane i (< p) keeps row i of both Cholesky factors of S, the
+   undamped one (for the rank label) and the damped one (for the step), in
+   registers. Column k of both factors is one step: each lane at or below the
+   diagonal finishes its entry (i, k) from the k entries of its own row and
+   lane k's row, which arrive by shuffles; the pivot is then broadcast from
+   lane k. The triangular solves are columns too: lane k finishes its unknown
+   and broadcasts it; the forward pass updates the lanes below with their own
+   row entry, the backward pass with lane k's row entry. Every lane of the
+   warp calls this with the same arguments; lanes >= p follow the same
+   uniform branches. */
+
+#define FT_FULL_MASK 0xffffffffu
+
+__device__ __forceinline__ int ft_solve_warp(const double *jtj, const double *jtr, double lambda,
+                                             int p, double *delta)
 {
-    double dscale[FT_MAX_CONST];
-    for (int i = 0; i < p; ++i) {
-        const double aii = jtj[i * (i + 1) / 2 + i];
-        if (!(aii > 0.0) || !isfinite(aii)) return 1;
-        dscale[i] = sqrt(aii);
+    const int lane = threadIdx.x & 31;
+    const bool mine = lane < p;
+    const double aii = mine ? jtj[lane * (lane + 1) / 2 + lane] : 1.0;
+    if (__any_sync(FT_FULL_MASK, !(aii > 0.0) || !isfinite(aii))) return 1;
+    const double di = sqrt(aii);
+
+    double u[FT_MAX_CONST], l[FT_MAX_CONST];
+    bool nonfinite = false;
+#pragma unroll
+    for (int j = 0; j < FT_MAX_CONST; ++j) {
+        const double dj = __shfl_sync(FT_FULL_MASK, di, j);
+        double sij = 0.0;
+        if (mine && j <= lane) {
+            sij = jtj[lane * (lane + 1) / 2 + j] / (di * dj);
+            nonfinite = nonfinite || !isfinite(sij);
+        }
+        u[j] = sij;
+        l[j] = sij;
     }
-    int rank_deficient = 0;
-    double sum_ln_L = 0.0;
-    int ok = 1;
-    for (int i = 0; i < p && ok; ++i) {
-        for (int j = 0; j <= i; ++j) {
-            double s = jtj[i * (i + 1) / 2 + j] / (dscale[i] * dscale[j]);
-            if (!isfinite(s)) return 1;
-            for (int k = 0; k < j; ++k) s -= L[i * p + k] * L[j * p + k];
-            if (i == j) {
-                if (!(s > 0.0) || !isfinite(s)) {
-                    ok = 0;
-                    break;
-                }
-                L[i * p + i] = sqrt(s);
-                sum_ln_L += 0.5 * log(s);
-            } else {
-                L[i * p + j] = s / L[j * p + j];
-            }
+    if (__any_sync(FT_FULL_MASK, nonfinite)) return 1;
+
+    bool broke = false; /* the undamped factor broke down */
+    double lndet = 0.0; /* ln det S from the undamped pivots, summed on every lane */
+#pragma unroll
+    for (int k = 0; k < FT_MAX_CONST; ++k) {
+        if (k >= p) break;
+        double su = u[k], sd = l[k];
+        if (lane == k) sd = sd * (1.0 + lambda) + 1e-12;
+#pragma unroll
+        for (int m = 0; m < k; ++m) {
+            su -= u[m] * __shfl_sync(FT_FULL_MASK, u[m], k);
+            sd -= l[m] * __shfl_sync(FT_FULL_MASK, l[m], k);
+        }
+        const double pu = __shfl_sync(FT_FULL_MASK, su, k);
+        const double pd = __shfl_sync(FT_FULL_MASK, sd, k);
+        if (!(pd > 1e-18) || !isfinite(pd)) return 1;
+        if (!broke && (!(pu > 0.0) || !isfinite(pu))) broke = true;
+        if (!broke) lndet += log(pu);
+        const double ru = broke ? 1.0 : sqrt(pu), rd = sqrt(pd);
+        if (lane == k) {
+            u[k] = ru;
+            l[k] = rd;
+        } else if (lane > k) {
+            u[k] = su / ru;
+            l[k] = sd / rd;
         }
     }
-    if (!ok) rank_deficient = 1;
-    else {
-        const double ln_det = 2.0 * sum_ln_L;
-        if (!isfinite(ln_det) || ln_det < FT_LN_DET_FLOOR) rank_deficient = 1;
+    const int label = (broke || !isfinite(lndet) || lndet < FT_LN_DET_FLOOR) ? 4 : 0;
+
+    /* forward: L y = -D^-1 g */
+    double yv = mine ? -jtr[lane] / di : 0.0;
+#pragma unroll
+    for (int k = 0; k < FT_MAX_CONST; ++k) {
+        if (k >= p) break;
+        if (lane == k) yv = yv / l[k];
+        const double yk = __shfl_sync(FT_FULL_MASK, yv, k);
+        if (lane > k) yv -= l[k] * yk;
     }
-    for (int i = 0; i < p; ++i) {
-        for (int j = 0; j <= i; ++j) {
-            double s = jtj[i * (i + 1) / 2 + j] / (dscale[i] * dscale[j]);
-            if (i == j) s = s * (1.0 + lambda) + 1e-12;
-            for (int k = 0; k < j; ++k) s -= L[i * p + k] * L[j * p + k];
-            if (i == j) {
-                if (!(s > 1e-18) || !isfinite(s)) return 1;
-                L[i * p + i] = sqrt(s);
-            } else {
-                L[i * p + j] = s / L[j * p + j];
-            }
+    /* backward: L^T x = y; lane k's row holds column k of L^T */
+#pragma unroll
+    for (int k = FT_MAX_CONST - 1; k >= 0; --k) {
+        if (k >= p) continue;
+        if (lane == k) yv = yv / l[k];
+        const double xk = __shfl_sync(FT_FULL_MASK, yv, k);
+#pragma unroll
+        for (int j = 0; j < k; ++j) {
+            const double lkj = __shfl_sync(FT_FULL_MASK, l[j], k);
+            if (lane == j) yv -= lkj * xk;
         }
     }
-    double rhs[FT_MAX_CONST];
-    for (int i = 0; i < p; ++i) rhs[i] = -jtr[i] / dscale[i];
-    for (int i = 0; i < p; ++i) {
-        double s = rhs[i];
-        for (int k = 0; k < i; ++k) s -= L[i * p + k] * rhs[k];
-        rhs[i] = s / L[i * p + i];
-    }
-    for (int i = p - 1; i >= 0; --i) {
-        double s = rhs[i];
-        for (int k = i + 1; k < p; ++k) s -= L[k * p + i] * delta[k];
-        delta[i] = s / L[i * p + i];
-    }
-    for (int i = 0; i < p; ++i) delta[i] /= dscale[i];
-    return rank_deficient ? 4 : 0;
+    if (mine) delta[lane] = yv / di;
+    __syncwarp();
+    return label;
 }
 
 /* Gaussian elimination with partial pivoting on (A + lambda diag A + 1e-12 I)

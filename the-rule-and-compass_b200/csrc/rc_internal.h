@@ -134,6 +134,20 @@ struct RcCtx {
 
     /* kernels this context has launched (graph replays count their nodes) */
     unsigned long long launches;
+
+    /* the last fit's per-candidate state, in the device region (for
+       rc_last_fit_sweeps; valid until the region is reused) */
+    unsigned char *fit_state;
+    int fit_state_n;
+    size_t fit_state_stride;
+
+    /* profile of the last scoring call (rc_last_score_profile): events
+       around the f32 scoring kernels and the f64 lane, rows evaluated */
+    cudaEvent_t sp[3];
+    unsigned long long prof_rows[2];
+    unsigned long long prof_ops[2];
+    float prof_ms[2];
+    int prof_valid;
 };
 
 double rc_now_ms();

@@ -28,6 +28,7 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <map>
 #include <mutex>
 #include <numeric>
 #include <vector>
@@ -185,14 +186,29 @@ void launch_score_kernel(int T, bool track, int grid, size_t smem, cudaStream_t 
     }
 }
 
+/* Raise a kernel's dynamic shared-memory limit to at least `smem` on the
+   current device. The limit only ever grows: every path that launches the
+   kernel shares it, and lowering it for a small launch would make a larger
+   launch on another path fail. */
 int set_smem(const void *fn, size_t smem)
 {
     if (smem <= 48 * 1024) return 0;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return -1;
+    }
+    static std::mutex mu;
+    static std::map<std::pair<const void *, int>, size_t> raised;
+    std::lock_guard<std::mutex> lock(mu);
+    size_t &cur = raised[std::make_pair(fn, dev)];
+    if (smem <= cur) return 0;
     if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess) {
         cudaGetLastError();
         return -1;
     }
+    cur = smem;
     return 0;
 }
 
@@ -200,7 +216,6 @@ size_t lane_smem(int nslots) { return (size_t)nslots * LANE_T * 16 + RC_MAX_INS 
 
 }  // namespace
 
-static int stage_limit_cols() { return 15; }
 
 float rc_score_run(RcCtx *c, const uint32_t *words, const uint32_t *off, int width, int nprog,
                    int mode, const int *pcount, double *out, int *status, float *out_f32,
@@ -216,11 +231,17 @@ float rc_score_run(RcCtx *c, const uint32_t *words, const uint32_t *off, int wid
     ins.reserve((size_t)nprog * 16);
     std::vector<int> ins_off(nprog + 1, 0);
     std::vector<int> nslots(nprog, 0);
+    std::vector<int> opw(nprog, 0);
     std::vector<RcIns> local;
     for (int p = 0; p < nprog; ++p) {
         size_t b = width > 0 ? (size_t)p * (size_t)width : off[p];
         size_t e = width > 0 ? b + (size_t)width : off[p + 1];
         if (e < b) e = b;
+        /* algorithmic ops of a row: postfix ops (a push counts one) + residual + loss */
+        int ops = 0;
+        for (size_t q = b; q < e && words[q] != OP_HALT; ++ops)
+            q += (words[q] == OP_CONST || words[q] == OP_VAR) ? 2 : 1;
+        opw[p] = ops + 2;
         local.resize(std::max<size_t>(e - b, 1) + 1);
         int ns = 0;
         const int cnt = rc_decode_postfix(words + b, e - b, c->v, local.data(), &ns);
@@ -264,10 +285,12 @@ float rc_score_run(RcCtx *c, const uint32_t *words, const uint32_t *off, int wid
     const size_t o_insoff = rc_take(&cur, sizeof(int) * (nprog + 1));
     const size_t o_order = rc_take(&cur, sizeof(int) * nprog);
     const size_t o_ctiles = rc_take(&cur, sizeof(int) * nprog);
+    const size_t o_opw = rc_take(&cur, sizeof(int) * nprog);
     const size_t in_end = rc_take(&cur, 0);
     const size_t o_out = rc_take(&cur, sizeof(double) * nprog);
     const size_t o_status = rc_take(&cur, sizeof(int) * nprog);
     const size_t o_f32 = rc_take(&cur, sizeof(float) * nprog);
+    const size_t o_rows = rc_take(&cur, 4 * sizeof(unsigned long long));
     const size_t io_end = rc_take(&cur, 0);
     const size_t o_part = rc_take(&cur, 4 * sizeof(double) * (size_t)nprog * ntiles);
     const size_t o_bad = rc_take(&cur, sizeof(int) * nprog);
@@ -294,8 +317,11 @@ float rc_score_run(RcCtx *c, const uint32_t *words, const uint32_t *off, int wid
     memcpy(host + o_insoff, ins_off.data(), sizeof(int) * (nprog + 1));
     memcpy(host + o_order, order.data(), sizeof(int) * nprog);
     memcpy(host + o_ctiles, cand_tiles.data(), sizeof(int) * nprog);
+    memcpy(host + o_opw, opw.data(), sizeof(int) * nprog);
     cudaMemcpyAsync(dev, host, in_end, cudaMemcpyHostToDevice, c->s);
     cudaMemsetAsync(dev + o_bad, 0, o_zero_end - o_bad, c->s);
+    cudaMemsetAsync(dev + o_rows, 0, 4 * sizeof(unsigned long long), c->s);
+    unsigned long long *d_rows = reinterpret_cast<unsigned long long *>(dev + o_rows);
     if (track && !corr) cudaMemsetAsync(dev + o_badrow, 0x7f, sizeof(int) * nprog, c->s);
     st->h2d_ms += rc_now_ms() - t;
     st->h2d_bytes += in_end;
@@ -322,6 +348,8 @@ float rc_score_run(RcCtx *c, const uint32_t *words, const uint32_t *off, int wid
     a.part = reinterpret_cast<double *>(dev + o_part);
     a.bad = reinterpret_cast<int *>(dev + o_bad);
     a.badrow = track && !corr ? reinterpret_cast<int *>(dev + o_badrow) : nullptr;
+    a.rows = d_rows;
+    a.opw = reinterpret_cast<const int *>(dev + o_opw);
     a.pred = pred_out ? reinterpret_cast<float *>(dev + o_pred) : nullptr;
     a.pbar = reinterpret_cast<const double *>(dev + o_pbar);
     a.pbar_err = reinterpret_cast<const double *>(dev + o_pbarerr);
@@ -330,6 +358,7 @@ float rc_score_run(RcCtx *c, const uint32_t *words, const uint32_t *off, int wid
 
     t = rc_now_ms();
     cudaEventRecord(c->t0, c->s);
+    cudaEventRecord(c->sp[0], c->s);
     const int passes = corr ? 2 : 1;
     for (int pass = 0; pass < passes; ++pass) {
         const int kmode = corr ? (pass == 0 ? SM_CORR_PASS1 : SM_CORR_PASS2) : mode;
@@ -368,6 +397,7 @@ float rc_score_run(RcCtx *c, const uint32_t *words, const uint32_t *off, int wid
             c->launches += 1;
             obase += nb;
         }
+        if (pass == passes - 1) cudaEventRecord(c->sp[1], c->s);
         c->launches += 1;
         rc_score_finalize<<<(nprog + 127) / 128, 128, 0, c->s>>>(
             nprog, d_ctiles, a.part, ntiles, a.bad, c->n, (corr && pass == 1) ? mode : kmode,
@@ -399,6 +429,8 @@ float rc_score_run(RcCtx *c, const uint32_t *words, const uint32_t *off, int wid
         l.bad = reinterpret_cast<int *>(dev + o_bad64);
         l.pbar = reinterpret_cast<const double *>(dev + o_pbar64);
         l.ybar = c->ybar;
+        l.rows = d_rows + 1;
+        l.opw = a.opw;
         const size_t smem = lane_smem(max_slots);
         if (set_smem((const void *)rc_score64_kernel<LANE_T>, smem) != 0) {
             st->failed = 1;
@@ -432,6 +464,7 @@ float rc_score_run(RcCtx *c, const uint32_t *words, const uint32_t *off, int wid
                 d_out, d_status, reinterpret_cast<double *>(dev + o_pbar64));
         }
     }
+    cudaEventRecord(c->sp[2], c->s);
     cudaEventRecord(c->t1, c->s);
     st->launch_ms += rc_now_ms() - t;
     if (cudaGetLastError() != cudaSuccess) {
@@ -458,6 +491,12 @@ float rc_score_run(RcCtx *c, const uint32_t *words, const uint32_t *off, int wid
     st->d2h_bytes += io_end - in_end;
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, c->t0, c->t1);
+    memcpy(c->prof_rows, host + o_rows, sizeof(c->prof_rows));
+    memcpy(c->prof_ops, host + o_rows + 2 * sizeof(unsigned long long), sizeof(c->prof_ops));
+    c->prof_ms[0] = c->prof_ms[1] = 0.0f;
+    cudaEventElapsedTime(&c->prof_ms[0], c->sp[0], c->sp[1]);
+    cudaEventElapsedTime(&c->prof_ms[1], c->sp[1], c->sp[2]);
+    c->prof_valid = 1;
     st->kernel_ms = ms;
     st->batch = nprog;
     st->wall_ms = rc_now_ms() - (c->batch_start_ms > 0 ? c->batch_start_ms : t_begin);
@@ -693,7 +732,7 @@ __global__ void rc_noalloc_decode(const unsigned int *__restrict__ prog,
                                   const unsigned int *__restrict__ off, int nprog, int v,
                                   RcIns *__restrict__ ins, int *__restrict__ ins_off,
                                   int *__restrict__ order, int *__restrict__ cand_tiles,
-                                  int *__restrict__ deep, int ntiles)
+                                  int *__restrict__ deep, int *__restrict__ ins_len, int ntiles)
 {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p > nprog) return;
@@ -765,6 +804,7 @@ __global__ void rc_noalloc_decode(const unsigned int *__restrict__ prog,
         out[n++] = in;
         if (halted) break;
     }
+    ins_len[p] = n;
     if (!ok || !halted || maxslot + 1 > RC_SHALLOW_SLOTS) {
         deep[p] = ok && halted ? 1 : 0;
         RcIns bad;
@@ -774,6 +814,7 @@ __global__ void rc_noalloc_decode(const unsigned int *__restrict__ prog,
         bad.spill = 0xff;
         bad.imm = 0;
         out[0] = bad;
+        ins_len[p] = 1;
     }
 }
 
@@ -814,11 +855,6 @@ extern "C" int rc_score_batch_noalloc(const float *cols, const float *y, int n, 
         fprintf(stderr, "rc_score_batch_noalloc: kind %d unsupported (0..4 only)\n", kind);
         return -3;
     }
-    if (v + 1 > stage_limit_cols() + 1) {
-        fprintf(stderr, "rc_score_batch_noalloc: %d columns exceed the staged limit %d\n", v,
-                stage_limit_cols());
-        return -3;
-    }
     const long long need_rows = ((long long)n + SUB - 1) / SUB * SUB;
     if ((long long)ld < need_rows || (ld % 4) != 0 || ((uintptr_t)cols % 16) != 0 ||
         ((uintptr_t)y % 16) != 0) {
@@ -840,6 +876,7 @@ extern "C" int rc_score_batch_noalloc(const float *cols, const float *y, int n, 
     const size_t o_order = rc_take(&cur, sizeof(int) * (size_t)nprog);
     const size_t o_ctiles = rc_take(&cur, sizeof(int) * (size_t)nprog);
     const size_t o_deep = rc_take(&cur, sizeof(int) * (size_t)nprog);
+    const size_t o_len = rc_take(&cur, sizeof(int) * (size_t)nprog);
     const size_t o_part = rc_take(&cur, 4 * sizeof(double) * (size_t)nprog * ntiles);
     const size_t o_part64 = rc_take(&cur, 2 * sizeof(double) * (size_t)nprog * ntiles);
     const size_t o_flagged = rc_take(&cur, sizeof(int) * (size_t)nprog);
@@ -857,7 +894,8 @@ extern "C" int rc_score_batch_noalloc(const float *cols, const float *y, int n, 
     }
     const int G = 8;
     const int group = G < nprog ? G : nprog;
-    const size_t smem = ScoreSmem<256>::total(v, 1, RC_SHALLOW_SLOTS, group, RC_MAX_INS);
+    /* features are read from global memory (L2), nothing is staged */
+    const size_t smem = ScoreSmem<256>::total(v, 0, RC_SHALLOW_SLOTS, group, RC_MAX_INS);
     const size_t lsmem = lane_smem(RC_SHALLOW_SLOTS);
     NoallocDevice *d = &g_noalloc[dev];
     {
@@ -871,8 +909,7 @@ extern "C" int rc_score_batch_noalloc(const float *cols, const float *y, int n, 
                 cudaGetLastError();
                 return -1;
             }
-            const size_t maxsmem =
-                ScoreSmem<256>::total(stage_limit_cols(), 1, RC_SHALLOW_SLOTS, G, RC_MAX_INS);
+            const size_t maxsmem = ScoreSmem<256>::total(0, 0, RC_SHALLOW_SLOTS, G, RC_MAX_INS);
             if (set_smem((const void *)rc_score_kernel<256, true>, maxsmem) != 0 ||
                 set_smem((const void *)rc_score64_kernel<LANE_T>, lsmem) != 0)
                 return -1;
@@ -887,13 +924,21 @@ extern "C" int rc_score_batch_noalloc(const float *cols, const float *y, int n, 
             d->ready = 1;
         }
     }
+    /* the limits only grow, and another path may have launched these
+       kernels since; raising them again is a no-op when already high enough */
+    if (set_smem((const void *)rc_score_kernel<256, true>, smem) != 0 ||
+        set_smem((const void *)rc_score64_kernel<LANE_T>, lsmem) != 0) {
+        fprintf(stderr, "rc_score_batch_noalloc: cannot raise the shared-memory limit\n");
+        return -1;
+    }
     cudaStream_t s = (cudaStream_t)stream;
     unsigned char *sc = d->scratch;
     cudaMemsetAsync(sc + o_bad, 0, o_zero_end - o_bad, s);
     rc_noalloc_decode<<<(nprog + 1 + 127) / 128, 128, 0, s>>>(
         prog, off, nprog, v, reinterpret_cast<RcIns *>(sc + o_ins),
         reinterpret_cast<int *>(sc + o_insoff), reinterpret_cast<int *>(sc + o_order),
-        reinterpret_cast<int *>(sc + o_ctiles), reinterpret_cast<int *>(sc + o_deep), ntiles);
+        reinterpret_cast<int *>(sc + o_ctiles), reinterpret_cast<int *>(sc + o_deep),
+        reinterpret_cast<int *>(sc + o_len), ntiles);
     int *cnt = reinterpret_cast<int *>(sc + o_cnt);
     ScoreArgs a;
     memset(&a, 0, sizeof(a));
@@ -902,9 +947,10 @@ extern "C" int rc_score_batch_noalloc(const float *cols, const float *y, int n, 
     a.n = n;
     a.npad = ld;
     a.v = v;
-    a.staged = 1;
+    a.staged = 0;
     a.ins = reinterpret_cast<const RcIns *>(sc + o_ins);
     a.ins_off = reinterpret_cast<const int *>(sc + o_insoff);
+    a.ins_len = reinterpret_cast<const int *>(sc + o_len);
     a.order = reinterpret_cast<const int *>(sc + o_order);
     a.ncand = nprog;
     a.group = group;
@@ -922,6 +968,16 @@ extern "C" int rc_score_batch_noalloc(const float *cols, const float *y, int n, 
     int grid = d->sm_count * d->grid_per_sm;
     if (grid > a.nitems) grid = a.nitems;
     rc_score_kernel<256, true><<<grid, T, smem, s>>>(a);
+    {
+        /* a failed scoring launch must not let the finalize kernels write
+           stale scratch into the caller's outputs */
+        const cudaError_t le = cudaGetLastError();
+        if (le != cudaSuccess) {
+            fprintf(stderr, "rc_score_batch_noalloc: scoring launch failed: %s\n",
+                    cudaGetErrorString(le));
+            return -1;
+        }
+    }
     rc_score_finalize<<<(nprog + 127) / 128, 128, 0, s>>>(
         nprog, reinterpret_cast<const int *>(sc + o_ctiles), a.part, ntiles, a.bad, n, kind, 0.0,
         out, status, nullptr, nullptr, nullptr, cnt + 8, reinterpret_cast<int *>(sc + o_flagged));
@@ -954,6 +1010,28 @@ extern "C" int rc_score_batch_noalloc(const float *cols, const float *y, int n, 
         fprintf(stderr, "rc_score_batch_noalloc: launch failed: %s\n", cudaGetErrorString(e));
         return -1;
     }
+    return 0;
+}
+
+/* Profile of the context's last scoring call: device ms of the f32 scoring
+   kernels (from the first scoring launch to the end of the last one) and of
+   everything after them (finalize, the f64 lane and its finalize), and the
+   rows each interpreter evaluated (a candidate stops at its first hard
+   failure, so these can be below candidates x rows), and those rows weighted
+   by their candidate's postfix ops + 2 (the algorithmic lane-ops). */
+extern "C" int rc_last_score_profile(void *ctx, float *ms_f32, float *ms_rest,
+                                     unsigned long long *rows_f32,
+                                     unsigned long long *rows_f64,
+                                     unsigned long long *ops_f32, unsigned long long *ops_f64)
+{
+    RcCtx *c = (RcCtx *)ctx;
+    if (!c || !c->prof_valid) return -1;
+    if (ms_f32) *ms_f32 = c->prof_ms[0];
+    if (ms_rest) *ms_rest = c->prof_ms[1];
+    if (rows_f32) *rows_f32 = c->prof_rows[0];
+    if (rows_f64) *rows_f64 = c->prof_rows[1];
+    if (ops_f32) *ops_f32 = c->prof_ops[0];
+    if (ops_f64) *ops_f64 = c->prof_ops[1];
     return 0;
 }
 

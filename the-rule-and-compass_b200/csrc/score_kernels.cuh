@@ -392,6 +392,7 @@ struct ScoreArgs {
     int staged;
     const RcIns *ins;
     const int *ins_off;
+    const int *ins_len;   /* [P] instructions per program, or null: ins_off[p + 1] - ins_off[p] */
     const int *order;     /* candidate ids of this bucket, longest first */
     int ncand;            /* candidates in this bucket */
     int group;            /* candidates per work item */
@@ -406,6 +407,9 @@ struct ScoreArgs {
     int ptiles;
     int *bad;             /* [P] */
     int *badrow;          /* [P] or null: first 4-row group of a hard failure */
+    unsigned long long *rows; /* or null: [0] += rows the interpreter evaluated,
+                                 [2] += those rows x (ops + 2) of their candidate */
+    const int *opw;           /* [P] postfix ops + 2 per candidate (with rows) */
     float *pred;          /* SM_PREDICT: [P][n] */
     const double *pbar;   /* SM_CORR_PASS2: per-candidate mean prediction */
     const double *pbar_err;
@@ -536,6 +540,7 @@ __global__ void __launch_bounds__(T) rc_score_kernel(ScoreArgs a)
     RcIns *sprog = reinterpret_cast<RcIns *>(swarp + a.group * NW * 4);
     __shared__ int s_item;
     __shared__ unsigned s_bad;
+    __shared__ unsigned long long s_rows, s_ops;
     const int SUB = T * 4;
     const int mode = a.mode;
     const bool skip_bad = rc_mode_tracks(mode);
@@ -553,12 +558,17 @@ __global__ void __launch_bounds__(T) rc_score_kernel(ScoreArgs a)
         unsigned skipmask = 0;
         for (int c = 0; c < gcount; ++c) {
             const int cand = a.order[cbase + c];
-            const int b = a.ins_off[cand], e = a.ins_off[cand + 1];
+            const int b = a.ins_off[cand];
+            const int e = a.ins_len ? b + a.ins_len[cand] : a.ins_off[cand + 1];
             for (int q = tid; q < e - b; q += T) sprog[c * a.maxins + q] = a.ins[b + q];
             if (skip_bad && *((volatile int *)(a.bad + cand))) skipmask |= 1u << c;
         }
         for (int q = tid; q < gcount * NW * 4; q += T) swarp[q] = 0.0;
-        if (tid == 0) s_bad = 0;
+        if (tid == 0) {
+            s_bad = 0;
+            s_rows = 0;
+            s_ops = 0;
+        }
         __syncthreads();
 
         /* each warp runs one candidate over all of the tile's rows before its
@@ -569,10 +579,12 @@ __global__ void __launch_bounds__(T) rc_score_kernel(ScoreArgs a)
             const int cand = a.order[cbase + c];
             double a0 = 0.0, a1 = 0.0, e0 = 0.0, e1 = 0.0;
             int bad = 0;
+            int wrows = 0; /* rows of this warp the candidate was evaluated on */
             for (int s = 0; s < a.subtiles; ++s) {
                 const int row0 = (tile * a.subtiles + s) * SUB;
                 if (row0 >= a.n) break;
                 const int myrow = row0 + 4 * tid;
+                wrows += max(0, min(128, a.n - (row0 + 128 * warp)));
                 float4 p, pe;
                 rc_run<T, TRACK>(sprog + c * a.maxins, nullptr, false, a.cols, a.npad, myrow, stk,
                                  estk, tid, p, pe);
@@ -595,6 +607,10 @@ __global__ void __launch_bounds__(T) rc_score_kernel(ScoreArgs a)
                     if (a.badrow && lane == 0) atomicMin(a.badrow + cand, grp);
                     break;
                 }
+            }
+            if (a.rows && lane == 0 && wrows > 0) {
+                atomicAdd(&s_rows, (unsigned long long)wrows);
+                atomicAdd(&s_ops, (unsigned long long)wrows * (unsigned long long)a.opw[cand]);
             }
             if (mode == SM_PREDICT) continue;
             if (mode == SM_MAXIMUM) {
@@ -631,6 +647,10 @@ __global__ void __launch_bounds__(T) rc_score_kernel(ScoreArgs a)
             }
             a.part[((size_t)q * a.nprog + cand) * a.ptiles + tile] = s;
             if (q == 0 && (s_bad & (1u << c)) && !(skipmask & (1u << c))) atomicOr(&a.bad[cand], 1);
+        }
+        if (a.rows && tid == 0 && s_rows) {
+            atomicAdd(a.rows, s_rows);
+            atomicAdd(a.rows + 2, s_ops);
         }
         __syncthreads();
     }
@@ -878,6 +898,9 @@ struct Score64Args {
     const double *pbar;
     double ybar;
     int mode;
+    unsigned long long *rows; /* or null: [0] += rows the f64 lane evaluated,
+                                 [2] += those rows x (ops + 2) */
+    const int *opw;
 };
 
 template <int T>
@@ -915,10 +938,12 @@ __global__ void __launch_bounds__(T) rc_score64_kernel(Score64Args a)
         __syncthreads();
         double a0 = 0.0, a1 = 0.0;
         int bad = 0;
+        int trows = 0;
         for (int s = 0; s < subtiles; ++s) {
             const int row0 = (tile * subtiles + s) * SUB;
             if (row0 >= a.n) break;
             if (*((volatile int *)(a.bad + cand))) break;
+            trows += min(SUB, a.n - row0);
             const int myrow = row0 + 2 * tid;
             const double2 p = rc_run_d<T>(sprog, a.cols, a.npad, myrow, stk, tid);
             const double pr[2] = {p.x, p.y};
@@ -961,6 +986,10 @@ __global__ void __launch_bounds__(T) rc_score64_kernel(Score64Args a)
                 }
             }
             if (bad) atomicOr(a.bad + cand, 1);
+        }
+        if (a.rows && tid == 0 && trows > 0) {
+            atomicAdd(a.rows, (unsigned long long)trows);
+            atomicAdd(a.rows + 2, (unsigned long long)trows * (unsigned long long)a.opw[cand]);
         }
         /* fixed-order block trees */
         for (int q = 0; q < 2; ++q) {

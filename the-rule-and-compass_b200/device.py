@@ -74,6 +74,9 @@ SIGNATURES = {
     "rc_rank_score_batch": (cf, [cvp, u32p, u32p, i32p, ci, ci, ci, f64p, u64p, i32p, u64p]),
     "rc_rank_debug_b": (ci, [cvp, i64p]),
     "rc_launch_count": (ci, [cvp, u64p]),
+    "rc_last_fit_sweeps": (ci, [cvp, ci, ctypes.POINTER(ctypes.c_int32)]),
+    "rc_last_score_profile": (ci, [cvp, ctypes.POINTER(ctypes.c_float),
+                                   ctypes.POINTER(ctypes.c_float), u64p, u64p, u64p, u64p]),
     "rc_order_stat_score_batch": (cf, [cvp, u32p, u32p, i32p, ci, ci, ci, f64p, ci, f64p,
                                        i32p]),
     "rc_max_scan_batch": (cf, [cvp, u32p, u32p, i32p, ci, ci, ci, f64p, i32p, f64p,
@@ -390,6 +393,30 @@ class GpuEvaluator:
         if lib().rc_launch_count(self.ctx, _p(out, ctypes.c_uint64)) != 0:
             raise DeviceError("rc_launch_count failed")
         return int(out[0])
+
+    def fit_sweeps(self, nprog):
+        """Sweeps per candidate of the last fit: int32 [P][4] (f32 assembly,
+        f32 objective, f64 assembly, f64 objective)."""
+        out = np.zeros((nprog, 4), np.int32)
+        if lib().rc_last_fit_sweeps(self.ctx, nprog, _p(out, ctypes.c_int32)) != 0:
+            raise DeviceError("rc_last_fit_sweeps failed")
+        return out
+
+    def score_profile(self):
+        """Profile of the last scoring call: dict with the device ms of the
+        f32 scoring kernels (`ms_f32`) and of the rest (`ms_rest`), the rows
+        the f32 interpreter and the f64 lane evaluated (`rows_f32`,
+        `rows_f64`) and those rows x (postfix ops + 2) (`ops_f32`,
+        `ops_f64`)."""
+        ms = np.zeros(2, np.float32)
+        q = np.zeros(4, np.uint64)
+        if lib().rc_last_score_profile(self.ctx, _p(ms[0:1], ctypes.c_float),
+                                       _p(ms[1:2], ctypes.c_float), _p(q[0:1], ctypes.c_uint64),
+                                       _p(q[1:2], ctypes.c_uint64), _p(q[2:3], ctypes.c_uint64),
+                                       _p(q[3:4], ctypes.c_uint64)) != 0:
+            raise DeviceError("rc_last_score_profile failed")
+        return {"ms_f32": float(ms[0]), "ms_rest": float(ms[1]), "rows_f32": int(q[0]),
+                "rows_f64": int(q[1]), "ops_f32": int(q[2]), "ops_f64": int(q[3])}
 
     def arena_report(self):
         r = RcArenaReport()
