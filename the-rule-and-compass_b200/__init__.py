@@ -10,3 +10,4 @@ from .device import GpuEvaluator, GenomePool, DeviceError, lib as cuda_lib  # no
 from .host import compile_program, gpu_fit_plan, Population, pack_plans  # noqa: F401
 from .host import DEFAULT_VARIATION_OPS, width_for, FitLedger  # noqa: F401
 from .host import refit_finalists_exact, soa_eval, soa_sse  # noqa: F401
+from .search import GenerationLoop  # noqa: F401

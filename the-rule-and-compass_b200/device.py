@@ -449,6 +449,19 @@ class GenomePool:
                                 self.islands * self.pop) != 0:
             raise DeviceError("rc_pool_upload failed")
 
+    def score(self, which, kind=0, pcount=None):
+        """Score every slot of pool `which` (rc_pool_score): (values f64,
+        status i32, ms)."""
+        n = self.islands * self.pop
+        pc = _c(pcount if pcount is not None else np.zeros(n), np.int32)
+        out = np.zeros(n, np.float64)
+        st = np.zeros(n, np.int32)
+        ms = lib().rc_pool_score(self.ev.ctx, which, n, self.width, kind, _p(pc, ctypes.c_int32),
+                                 _p(out, ctypes.c_double), _p(st, ctypes.c_int32))
+        if ms < 0:
+            raise DeviceError("rc_pool_score failed")
+        return out, st, ms
+
     def hash(self, which):
         out = np.zeros(self.islands * self.pop, np.uint64)
         if lib().rc_pool_hash(self.ev.ctx, which, self.islands * self.pop, self.width,

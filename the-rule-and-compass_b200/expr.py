@@ -146,3 +146,38 @@ def from_prefix(ops, vals) -> Node:
     if pos != len(ops):
         raise ValueError("trailing nodes in prefix arrays")
     return t
+
+
+def from_postfix(words) -> Node:
+    """The tree of one postfix program (the words `gpu::emit` writes,
+    my-version/src/gpu.rs:320-438, and the device's variation engine builds):
+    `[CONST, f32 bits]`, `[VAR, index]`, operator words, up to HALT. A
+    constant's value is its f32 word widened to f64. Raises ValueError for a
+    program that is not one well-formed expression."""
+    w = np.asarray(words, dtype=np.uint32).reshape(-1)
+    stack = []
+    i = 0
+    while i < len(w):
+        op = int(w[i])
+        i += 1
+        if op == HALT:
+            break
+        if op in (CONST, VAR):
+            if i >= len(w):
+                raise ValueError("truncated operand")
+            a = w[i:i + 1]
+            i += 1
+            stack.append(Node(CONST, float(a.view(np.float32)[0])) if op == CONST
+                         else Node(VAR, float(int(a[0]))))
+            continue
+        k = arity(op)
+        if op not in NAMES or len(stack) < k:
+            raise ValueError(f"bad operator word {op}")
+        kids = stack[len(stack) - k:]
+        del stack[len(stack) - k:]
+        stack.append(Node(op, 0.0, kids))
+    else:
+        raise ValueError("no HALT")
+    if len(stack) != 1:
+        raise ValueError("program leaves %d values" % len(stack))
+    return stack[0]

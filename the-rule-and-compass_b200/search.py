@@ -1,0 +1,132 @@
+"""A generation loop over the device path.
+
+The island search of the reference (my-version/src/search.rs:5607, the
+generation loop, and :1075-1120, `GpuSearch::score`) runs each generation as
+screen -> admit -> fit -> rescore -> vary. Here every step runs on the
+device behind the library's C ABI, and only the bookkeeping between them is
+host code:
+
+  screen   rc_pool_score of every slot of the current pool (squared error
+           with the programs' own constants);
+  admit    rch_select_promoted (search.rs:3033-3074): per island, the best
+           screened offspring that have constants, as many as
+           rch_admission_count allows (everyone with constants at >= 2^20
+           rows);
+  fit      the admitted programs, decoded into trees and flattened into fit
+           plans, through rc_fit_batch_fused (the fused adjoint LM);
+  rescore  the fitted constants written back into their slots (a usable,
+           finite answer only: fit/gpu.rs:103-105), the pool re-uploaded and
+           rescored, so selection sees the fitted constants;
+  vary     rc_pool_vary builds the next generation from the scores
+           (tournament, crossover, mutation, dedup: postfix.rs:511-567).
+
+`GenerationLoop.generation()` returns what the fit step saw and answered, so
+a caller (or a test) can hold every device answer against the exact CPU
+fit of the same candidate.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import expr as E
+from .device import GenomePool
+from .host import (DEFAULT_VARIATION_OPS, CompileError, GpuFitReject, compile_program,
+                   fit_status_usable, gpu_fit_plan, select_promoted, width_for)
+
+
+class FitRecord:
+    """One admitted candidate of one generation: its slot, the tree it was
+    fitted from, its plan, and the device's answer."""
+
+    __slots__ = ("slot", "tree", "plan", "c", "loss", "status")
+
+    def __init__(self, slot, tree, plan, c, loss, status):
+        self.slot, self.tree, self.plan = slot, tree, plan
+        self.c, self.loss, self.status = c, loss, status
+
+    def fitted(self):
+        return self.plan.apply(self.tree, self.c[: self.plan.nconst])
+
+
+class GenerationLoop:
+    """Island-model generations of `islands` x `pop` fixed-width programs
+    over the evaluator's resident rows (the training rows)."""
+
+    def __init__(self, ev, islands, pop, nvars, max_complexity=30, fit_iters=8, seed=0,
+                 ops=DEFAULT_VARIATION_OPS, init_depth=3, fit_metric=0):
+        self.ev = ev
+        self.islands, self.pop = islands, pop
+        self.nvars, self.max_complexity = nvars, max_complexity
+        self.fit_iters, self.fit_metric = fit_iters, fit_metric
+        self.seed, self.ops, self.init_depth = seed, ops, init_depth
+        self.width = width_for(max_complexity)
+        self.train_rows = ev.n
+        self.pool = GenomePool(ev, islands, pop, self.width)
+        n = islands * pop
+        # generation 0: random programs built on the device (every island
+        # restarts from an all-x0 pool)
+        words = np.full((n, self.width), E.HALT, np.uint32)
+        words[:, 0], words[:, 1] = E.VAR, 0
+        self.pool.upload(0, words)
+        out = self.pool.vary(0, np.zeros(n), 0, nvars, max_complexity, seed, ops,
+                             init_depth=init_depth, restart=[1] * islands)
+        self.words = out[0].copy()
+        self.cur = 1
+        self.gen = 0
+        self.device_ms = 0.0
+
+    def _trees(self):
+        trees = []
+        for w in self.words:
+            try:
+                trees.append(E.from_postfix(w))
+            except ValueError:
+                trees.append(None)
+        return trees
+
+    def generation(self):
+        """Run one generation; returns (records, errors after the rescore)."""
+        n = self.islands * self.pop
+        err, _, ms = self.pool.score(self.cur, 0)
+        self.device_ms += ms
+        trees = self._trees()
+        cx = np.array([t.size() if t is not None else 1 << 20 for t in trees], np.float64)
+        hasc = np.array([t is not None and len(t.constants()) > 0 for t in trees], np.uint8)
+        pending = [(i // self.pop, i % self.pop) for i in range(n)]
+        admitted = select_promoted([self.pop] * self.islands, pending, err, cx, hasc,
+                                   self.train_rows)
+        slots, plans = [], []
+        for isl, j in admitted:
+            s = isl * self.pop + j
+            try:
+                plans.append(gpu_fit_plan(trees[s]))
+                slots.append(s)
+            except GpuFitReject:
+                continue
+        records = []
+        if plans:
+            c, loss, status, ms = self.ev.fit_plans(plans, self.fit_iters, self.fit_metric)
+            self.device_ms += ms
+            for k, (s, pl) in enumerate(zip(slots, plans)):
+                rec = FitRecord(s, trees[s], pl, c[k].copy(), float(loss[k]), int(status[k]))
+                records.append(rec)
+                if not fit_status_usable(rec.status) or \
+                        not np.all(np.isfinite(rec.c[: pl.nconst])):
+                    continue
+                try:
+                    w, _ = compile_program(rec.fitted())
+                except CompileError:
+                    continue
+                if len(w) <= self.width:
+                    self.words[s, :] = E.HALT
+                    self.words[s, : len(w)] = w
+            self.pool.upload(self.cur, self.words)
+            err, _, ms = self.pool.score(self.cur, 0)
+            self.device_ms += ms
+        self.gen += 1
+        out = self.pool.vary(self.cur, err, self.gen, self.nvars, self.max_complexity, self.seed,
+                             self.ops, init_depth=self.init_depth)
+        self.device_ms += out[5]
+        self.words = out[0].copy()
+        self.cur ^= 1
+        return records, err

@@ -158,3 +158,17 @@ def heavy_tail_data(n, seed=0):
     x = np.concatenate([g, t])
     y = 0.8 * x[0] / (1.0 + x[1] ** 2) + np.log1p(np.abs(x[3])) + 0.1 * rng.standard_t(3.0, n)
     return x, y
+
+
+def line_workload(n=10000, seed=0, test_frac=0.2):
+    """The plain-method configuration: one feature x ~ U(-5, 5),
+    y = 2x + 1 + N(0, 0.1^2), split into training and test rows by a seeded
+    permutation (the last `test_frac` of it held out). Returns
+    (x_train [1][n_train] f64, y_train, x_test [1][n_test], y_test)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    x = rng.uniform(-5.0, 5.0, n)
+    y = 2.0 * x + 1.0 + rng.normal(0.0, 0.1, n)
+    perm = rng.permutation(n)
+    n_test = int(round(n * test_frac))
+    tr, te = perm[: n - n_test], perm[n - n_test:]
+    return x[tr][None, :], y[tr], x[te][None, :], y[te]
