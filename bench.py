@@ -797,6 +797,97 @@ def bench_vary(args, rank, pkg, flushbuf, steps, warmup):
                       f"max complexity {mc}, {nvars} inputs, default operator set, dedup on"}
 
 
+def oracle_fit_agreement(records, cols, n, v, y, iters, threads, metric=0):
+    """The device answers of a generation loop's fitted candidates against the
+    oracle's CPU fit of the same candidates on the same rows: the share whose
+    device loss (the oracle's exact objective at the device's constants) is
+    within 1e-6 relative of the CPU fit's or below it."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.lib()
+    om = {0: O.SQUARED, 4: O.ABSOLUTE}[metric]
+
+    def one(r):
+        cpu, _ = O.fit(r.tree, cols, n, v, y, iters, om)
+        dev = (O.flat_sse(r.fitted(), cols, n, v, y) if metric == 0
+               else O.score(r.fitted(), cols, n, v, y, om))
+        return cpu, dev, r.status
+
+    with cf.ThreadPoolExecutor(threads) as ex:
+        res = list(ex.map(one, records))
+    cpu = np.array([q[0] for q in res])
+    dev = np.array([q[1] for q in res])
+    st = np.array([q[2] for q in res], np.int64)
+    ok = np.isin(st, [0, 4, 5, 6, 7, 8]) & np.isfinite(cpu)
+    within = dev[ok] <= cpu[ok] * (1.0 + 1e-6) + 1e-300
+    return {"checked": int(len(res)), "usable_finite": int(ok.sum()),
+            "within_1e-6_or_better": float(within.mean()) if ok.any() else None,
+            "status_histogram": np.bincount(st, minlength=9).tolist()}
+
+
+def bench_c1(pkg, W, gens=200, sample_every=20):
+    """The plain-method configuration through the build's own generation loop
+    (seed 0, 10,000 rows, 80/20 split, 4 islands x 200, squared error, 8 LM
+    iterations, max complexity 30): generations/s and fitted candidates/s end
+    to end (device steps and the host bookkeeping between them), the device
+    time of each step, and every `sample_every`-th generation's fitted
+    candidates against the oracle's CPU fit."""
+    x, y, _, _ = W.line_workload(10000, seed=0)
+    n = x.shape[1]
+    ev = pkg.GpuEvaluator(x.astype(np.float32).reshape(-1), n, 1, y.astype(np.float32))
+    ev.set_fit_data(x.reshape(-1), y)
+    loop = pkg.GenerationLoop(ev, 4, 200, 1, max_complexity=30, fit_iters=8, seed=0)
+    sample, nfit = [], 0
+    t0 = time.perf_counter()
+    for g in range(gens):
+        recs, err = loop.generation()
+        nfit += len(recs)
+        if g % sample_every == 0:
+            sample += recs
+    wall = time.perf_counter() - t0
+    ev.close()
+    agree = oracle_fit_agreement(sample, np.ascontiguousarray(x.reshape(-1)), n, 1, y, 8,
+                                 os.cpu_count() or 1)
+    return {"generations_per_s": gens / wall, "fitted_candidates_per_s": nfit / wall,
+            "generations": gens, "fitted_candidates": nfit, "wall_s": wall,
+            "device_ms": loop.device_ms, "step_ms": loop.timing,
+            "best_train_mse": float(np.nanmin(err)), "agreement": agree,
+            "config": "plain-method search: seed 0, N=10000 (8000 train rows), x ~ U(-5,5), "
+                      "y = 2x + 1 + N(0, 0.1^2), 4 islands x pop 200, 200 generations, squared "
+                      "error, 8 LM iterations, max complexity 30"}
+
+
+def bench_c5gen(args, pkg, W):
+    """One generation of the heavy-tailed configuration at its stated size:
+    16 islands x pop 1000 over N = 4,194,304 rows x 10 features, absolute
+    error (screen and rescore with the absolute score, L1 IRLS fit with up to
+    20 constants, 20 iterations). At >= 2^20 rows every offspring with
+    constants is admitted. Reports the device time of each step (screen, fit,
+    rescore, vary) and the host time between them, and the plain
+    one-candidate-per-launch fit of 16 of the admitted candidates."""
+    islands = args.P or 16
+    N = args.N or (1 << 22)
+    x, y = W.heavy_tail_data(N, seed=0)
+    ev = pkg.GpuEvaluator(x.astype(np.float32).reshape(-1), N, 10, y.astype(np.float32))
+    ev.set_fit_data(x.reshape(-1), y)
+    loop = pkg.GenerationLoop(ev, islands, 1000, 10, max_complexity=30, fit_iters=20, seed=5,
+                              fit_metric=4, score_kind=1)
+    t0 = time.perf_counter()
+    recs, err = loop.generation()
+    wall = time.perf_counter() - t0
+    plans = [r.plan for r in recs[:16]]
+    prog, off, pcount, c0, gauge, kmax = pkg.pack_plans(plans)
+    _, _, _, pms = ev.fit_batch_plain(prog, off, pcount, c0, gauge, kmax, 20, 4)
+    ev.close()
+    fused = len(recs) / (loop.timing["fit"] / 1e3)
+    plain = len(plans) / (pms / 1e3)
+    return {"generation_s": wall, "admitted": len(recs), "step_ms": loop.timing,
+            "fit_fused": fused, "fit_plain": plain, "fused_over_plain": fused / plain,
+            "status_histogram": np.bincount([r.status for r in recs], minlength=9).tolist(),
+            "config": f"one generation, {islands} islands x pop 1000, N={N} rows x 10 "
+                      f"heavy-tailed features, absolute error, L1 IRLS, 20 iterations"}
+
+
 def fit_roofline(r, peaks):
     per = float(np.mean(r["dev_ms"])) / 1e3
     achieved = r["lane_ops"] / per / 1e9
@@ -859,6 +950,10 @@ def secondary(args, rank, world, local, pkg, W, flushbuf, peaks, line):
                 c5_fit_roofline_frac=fs["roofline"]["frac"], c5_fit_cpu_baseline=_cpu(fs),
                 c5_rank=rk["value"], c5_rank_e2e=rk["e2e"],
                 c5_rank_roofline_frac=rk["roofline"]["frac"], c5_rank_cpu_baseline=_cpu(rk))
+    c1 = line["c1"] = bench_c1(pkg, W)
+    line.update(c1_generations_per_s=c1["generations_per_s"],
+                c1_fitted_candidates_per_s=c1["fitted_candidates_per_s"],
+                c1_agreement=c1["agreement"]["within_1e-6_or_better"])
     vy = line["vary"] = bench_vary(args, rank, pkg, flushbuf, 5, 3)
     line.update(vary_children=vy["value"], vary_children_e2e=vy["e2e"],
                 vary_same_as_cpu=vy["same_as_cpu"], vary_cpu_baseline=_cpu(vy))
@@ -891,7 +986,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="score",
-                    choices=["score", "fit", "rank", "implicit", "c5", "vary", "refit"])
+                    choices=["score", "fit", "rank", "implicit", "c5", "vary", "refit", "c1",
+                             "c5gen"])
     ap.add_argument("--P", type=int, default=0)
     ap.add_argument("--N", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -928,6 +1024,16 @@ def main():
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
+    if args.workload in ("c1", "c5gen"):
+        # the generation loop: one GPU, rank 0 reports
+        r = bench_c1(pkg, W) if args.workload == "c1" else bench_c5gen(args, pkg, W)
+        if rank == 0:
+            print(json.dumps({"metric": "generation", "workload": args.workload, **r},
+                             default=float), flush=True)
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     if args.workload in ("rank", "implicit", "c5", "vary"):
         # one-GPU stages: each rank measures its own copy; rank 0 reports
         if args.workload == "vary":

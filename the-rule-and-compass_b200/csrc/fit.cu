@@ -55,8 +55,32 @@
 
 enum {
     FOP_NONE = 0, FOP_ASM32 = 1, FOP_ASM64 = 2, FOP_LOSS32 = 3, FOP_LOSS64 = 4,
-    FOP_IJAC = 5, FOP_ICOST = 6, FOP_CASM = 7, FOP_CSCORE = 8, FOP_IJACS = 9, FOP_COUNT = 10
+    FOP_IJAC = 5, FOP_ICOST = 6, FOP_CASM = 7, FOP_CSCORE = 8, FOP_IJACS = 9,
+    /* the assembly queues of candidates with 64 and 32 active threads: their
+       sweeps run in blocks of that many threads, sized for their class */
+    FOP_ASM32_64 = 10, FOP_ASM32_32 = 11, FOP_ASM64_64 = 12, FOP_ASM64_32 = 13,
+    FOP_COUNT = 14
 };
+
+/* The kind a queue's sweep performs (a class queue performs its base kind). */
+__host__ __device__ constexpr int ft_base_kind(int k)
+{
+    return (k == FOP_ASM32_64 || k == FOP_ASM32_32)   ? FOP_ASM32
+           : (k == FOP_ASM64_64 || k == FOP_ASM64_32) ? FOP_ASM64
+                                                      : k;
+}
+
+/* The queue of a sweep request: f32 / f64 assemblies go to the queue of the
+   candidate's active-thread class. */
+__host__ __device__ inline int ft_queue_kind(int op, int A)
+{
+    if (op == FOP_ASM32) return A == 64 ? FOP_ASM32_64 : (A == 32 ? FOP_ASM32_32 : op);
+    if (op == FOP_ASM64) return A == 64 ? FOP_ASM64_64 : (A == 32 ? FOP_ASM64_32 : op);
+    return op;
+}
+
+/* Index of an active-thread class: 128, 64, 32 threads. */
+__host__ __device__ constexpr int ft_class_of(int A) { return A >= 128 ? 0 : (A >= 64 ? 1 : 2); }
 
 enum {
     PC_INIT = 0, PC_AFTER_FIRST_ASM, PC_ROUND, PC_ITER, PC_AFTER_ASM, PC_SOLVE,
@@ -153,7 +177,8 @@ struct FitArgs {
     int fslots;            /* spill slots needed by the batch */
     int ftape;             /* partial-tape slots needed by the batch */
     int fmaxins;           /* longest forward + reverse list */
-    size_t asm_region;     /* f32 assembly region of the launch */
+    size_t asm_region;     /* assembly region of a 128-thread launch over every class */
+    size_t asm_reg[3];     /* assembly region of the 128-, 64- and 32-thread class launches */
     const int2 *fcinfo;    /* [P] cached forward count (after the reverse list),
                               first cache column */
     float *cache;          /* [columns][npad] values of constant-free subtrees */
@@ -190,6 +215,7 @@ struct FitArgs {
 
 __host__ __device__ inline bool ft_op_assembles(int opk)
 {
+    opk = ft_base_kind(opk);
     return opk == FOP_ASM32 || opk == FOP_ASM64 || opk == FOP_IJAC || opk == FOP_CASM ||
            opk == FOP_IJACS;
 }
@@ -500,7 +526,10 @@ inline int ft_asm_threads(int slots, int tape, int ncols)
     return A;
 }
 
-__host__ __device__ inline bool ft_op_f64(int opk) { return opk == FOP_ASM64 || opk == FOP_LOSS64; }
+__host__ __device__ inline bool ft_op_f64(int opk)
+{
+    return ft_base_kind(opk) == FOP_ASM64 || opk == FOP_LOSS64;
+}
 
 /* Shared memory of a four-row sweep: forward and reverse instructions,
    constants, the assembly region (or the spill slots of an objective sweep),
@@ -873,19 +902,24 @@ __device__ void ft_tile_corr_score(const FitArgs &a, const FIns *ins, const floa
 template <int OPK, int T>
 __global__ void __launch_bounds__(T) ft_sweep4(FitArgs a, int q)
 {
-    using V = typename std::conditional<OPK == FOP_ASM64 || OPK == FOP_LOSS64, double, float>::type;
-    constexpr int NR = (OPK == FOP_ASM32 || OPK == FOP_CASM) ? FT_ASM32_NR
-                       : OPK == FOP_ASM64                      ? FT_ASM64_NR
-                       : (OPK == FOP_LOSS32 || OPK == FOP_CSCORE) ? FT_LOSS32_NR
-                                                                  : FT_LOSS64_NR;
+    constexpr int BK = ft_base_kind(OPK);
+    using V = typename std::conditional<BK == FOP_ASM64 || BK == FOP_LOSS64, double, float>::type;
+    constexpr int NR = (BK == FOP_ASM32 || BK == FOP_CASM) ? FT_ASM32_NR
+                       : BK == FOP_ASM64                     ? FT_ASM64_NR
+                       : (BK == FOP_LOSS32 || BK == FOP_CSCORE) ? FT_LOSS32_NR
+                                                                : FT_LOSS64_NR;
     using V4 = typename FiV<V, NR>::V4;
     extern __shared__ __align__(16) unsigned char sm[];
     FIns *ins = reinterpret_cast<FIns *>(sm);
     V *cv = reinterpret_cast<V *>(sm + 8 * (size_t)((a.fmaxins + 1) & ~1));
     unsigned char *region = reinterpret_cast<unsigned char *>(sm + 8 * (size_t)((a.fmaxins + 1) & ~1) +
                                                               8 * FT_MAX_CONST);
+    /* a class queue's region is sized for its class; the 128-thread launch
+       of a base assembly kind for every candidate it may hold */
+    const size_t asm_reg = OPK != BK ? a.asm_reg[ft_class_of(T)]
+                           : (BK == FOP_CASM ? a.asm_region : a.asm_reg[0]);
     double *red = reinterpret_cast<double *>(
-        region + (ft_op_assembles(OPK) ? a.asm_region
+        region + (ft_op_assembles(OPK) ? asm_reg
                                        : 16 * (size_t)(a.fslots > 0 ? a.fslots : 1) * T));
     __shared__ int s_item;
     const int tid = threadIdx.x;
@@ -926,9 +960,9 @@ __global__ void __launch_bounds__(T) ft_sweep4(FitArgs a, int q)
         const int r1 = min(a.n, r0 + FT_TILE_ROWS);
         double *pt = a.part + ((size_t)cand * a.ntiles + tile) * FT_PART_STRIDE;
         if (ft_op_assembles(OPK))
-            ft_tile_asm<V, NR, T, OPK == FOP_CASM>(a, ins, ins + nf, nr, p, info.z, info.w & 0xffff,
-                                                   info.w >> 16, cv, region, red, r0, r1, pt, ccols);
-        else if (OPK == FOP_CSCORE)
+            ft_tile_asm<V, NR, T, BK == FOP_CASM>(a, ins, ins + nf, nr, p, info.z, info.w & 0xffff,
+                                                  info.w >> 16, cv, region, red, r0, r1, pt, ccols);
+        else if (BK == FOP_CSCORE)
             ft_tile_corr_score<NR, T>(a, ins, reinterpret_cast<const float *>(cv),
                                       reinterpret_cast<typename FiV<float, NR>::V4 *>(region), red,
                                       r0, r1, pt, reinterpret_cast<const float *>(ccols));
@@ -1615,7 +1649,7 @@ __global__ void __launch_bounds__(FT_CTRL_T) ft_control(FitArgs a, int q, int in
                         base += a.counts[q * FOP_COUNT + k];
                         ++k;
                     }
-                    op = k;
+                    op = ft_base_kind(k);
                     cand = a.lists[((size_t)q * FOP_COUNT + k) * a.nprog + (t - base)];
                 }
                 s_cand = cand;
@@ -1723,8 +1757,9 @@ __global__ void __launch_bounds__(FT_CTRL_T) ft_control(FitArgs a, int q, int in
             for (int i = tid; i < (int)(sizeof(FitState) / 8); i += FT_CTRL_T) dst[i] = src[i];
         }
         if (tid == 0 && sst.op != FOP_NONE) {
-            const int k = atomicAdd(&a.counts[nq * FOP_COUNT + sst.op], 1);
-            a.lists[((size_t)nq * FOP_COUNT + sst.op) * a.nprog + k] = cand;
+            const int kq = ft_queue_kind(sst.op, a.finfo[cand].z);
+            const int k = atomicAdd(&a.counts[nq * FOP_COUNT + kq], 1);
+            a.lists[((size_t)nq * FOP_COUNT + kq) * a.nprog + k] = cand;
         }
         __syncthreads();
     }
@@ -2042,6 +2077,10 @@ void prep_batch(const unsigned int *off, const unsigned int *prog, const int *pc
     b.fins_off.assign(nprog + 1, 0);
     b.finfo.assign(nprog, make_int4(0, 0, 32, 0));
     b.asm_region = FT_ASM_BUDGET;
+    for (int k = 0; k < 3; ++k) {
+        b.asm_reg[k] = 256;
+        b.nclass[k] = 0;
+    }
     const bool caching = cache_bytes_per_col > 0;
     b.fcinfo.assign(nprog, make_int2(0, 0));
     b.sub_fins.clear();
@@ -2106,8 +2145,10 @@ void prep_batch(const unsigned int *off, const unsigned int *prog, const int *pc
         const int ncols = pcount[i] + 1 + extra_cols;
         const int A = ft_asm_threads(ns, nt, ncols);
         b.finfo[i] = make_int4((int)fwd.size(), (int)rev.size(), A, ns | (nt << 16));
-        b.asm_region = std::max(b.asm_region,
-                                ft_asm_region(A, ns, nt, 8 * ((ncols + 7) / 8)));
+        const size_t reg = ft_asm_region(A, ns, nt, 8 * ((ncols + 7) / 8));
+        b.asm_region = std::max(b.asm_region, reg);
+        b.asm_reg[ft_class_of(A)] = std::max(b.asm_reg[ft_class_of(A)], reg);
+        b.nclass[ft_class_of(A)]++;
         b.fslots = std::max(b.fslots, ns);
         b.ftape = std::max(b.ftape, nt);
         b.fmaxins = std::max(b.fmaxins, (int)(fwd.size() + rev.size()));
@@ -2288,7 +2329,10 @@ SweepLaunch sweep4_launch(RcCtx *c, const FitPrep &b, int Wmax)
     SweepLaunch s;
     s.fn = (const void *)ft_sweep4<OPK, T>;
     (void)Wmax;
-    s.smem = ft_sweep4_smem(OPK, b.fmaxins, b.fslots, b.asm_region, T);
+    const int bk = ft_base_kind(OPK);
+    const size_t reg = OPK != bk ? b.asm_reg[ft_class_of(T)]
+                       : (bk == FOP_CASM ? b.asm_region : b.asm_reg[0]);
+    s.smem = ft_sweep4_smem(OPK, b.fmaxins, b.fslots, reg, T);
     if (s.smem > 48 * 1024)
         cudaFuncSetAttribute(s.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
     s.grid = c->sm_count * occupancy(s.fn, T, s.smem);
@@ -2461,6 +2505,7 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     a.xslots = xp.slots;
     a.xtape = xp.tape;
     a.asm_region = b.asm_region;
+    for (int k = 0; k < 3; ++k) a.asm_reg[k] = b.asm_reg[k];
     a.fslots = b.fslots;
     a.ftape = b.ftape;
     a.fmaxins = b.fmaxins;
@@ -2480,7 +2525,7 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     a.outsse = reinterpret_cast<double *>(dev + o_sse);
     a.outstatus = reinterpret_cast<int *>(dev + o_status);
 
-    SweepLaunch sw[4];
+    SweepLaunch sw[8];
     int nk = 0;
     if (metric == FM_IMPLICIT) {
         const IjacSplit js = ijac_split(c, b, Wmax);
@@ -2496,12 +2541,18 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
         sw[nk] = sweep4_launch<FOP_CASM, FT_ASM_T>(c, b, Wmax); ++nk;
         sw[nk] = sweep4_launch<FOP_CSCORE, 128>(c, b, Wmax); ++nk;
     } else {
-        sw[nk] = sweep4_launch<FOP_ASM32, FT_ASM_T>(c, b, Wmax); ++nk;
+        /* one assembly launch per active-thread class present in the batch,
+           each in blocks of that many threads */
+        if (b.nclass[0]) { sw[nk] = sweep4_launch<FOP_ASM32, FT_ASM_T>(c, b, Wmax); ++nk; }
+        if (b.nclass[1]) { sw[nk] = sweep4_launch<FOP_ASM32_64, 64>(c, b, Wmax); ++nk; }
+        if (b.nclass[2]) { sw[nk] = sweep4_launch<FOP_ASM32_32, 32>(c, b, Wmax); ++nk; }
         sw[nk] = sweep4_launch<FOP_LOSS32, 128>(c, b, Wmax); ++nk;
         /* the f64 sweeps serve the polish and the f64 rescue */
         if ((flags & (FT_FLAG_NO_POLISH | FT_FLAG_NO_RESCUE)) !=
             (FT_FLAG_NO_POLISH | FT_FLAG_NO_RESCUE)) {
-            sw[nk] = sweep4_launch<FOP_ASM64, FT_ASM_T>(c, b, Wmax); ++nk;
+            if (b.nclass[0]) { sw[nk] = sweep4_launch<FOP_ASM64, FT_ASM_T>(c, b, Wmax); ++nk; }
+            if (b.nclass[1]) { sw[nk] = sweep4_launch<FOP_ASM64_64, 64>(c, b, Wmax); ++nk; }
+            if (b.nclass[2]) { sw[nk] = sweep4_launch<FOP_ASM64_32, 32>(c, b, Wmax); ++nk; }
             sw[nk] = sweep4_launch<FOP_LOSS64, 128>(c, b, Wmax); ++nk;
         }
     }
@@ -2544,9 +2595,11 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
                  nprog, kmax, ntiles, b.mmax, Wmax, iters, metric, flags, steps, io_end, b.fslots,
                  b.ftape, b.fmaxins, b.asm_region);
         const size_t kl = strlen(key);
-        snprintf(key + kl, sizeof(key) - kl, "|%d|%d|%d|%d|%d|%d|%d|%d|%d|%d|%d", b.ncache,
-                 a.nsub, b.sub_slots, b.sub_maxins, xp.maxins, xp.slots, xp.tape, use64 ? 1 : 0,
-                 a.ijac_small, a.ijac_tape, a.ijac_tape_small);
+        snprintf(key + kl, sizeof(key) - kl,
+                 "|%d|%d|%d|%d|%d|%d|%d|%d|%d|%d|%d|%zu|%zu|%zu|%d|%d|%d", b.ncache, a.nsub,
+                 b.sub_slots, b.sub_maxins, xp.maxins, xp.slots, xp.tape, use64 ? 1 : 0,
+                 a.ijac_small, a.ijac_tape, a.ijac_tape_small, b.asm_reg[0], b.asm_reg[1],
+                 b.asm_reg[2], b.nclass[0], b.nclass[1], b.nclass[2]);
         if (!c->fit_graph || c->fit_graph_key != key) {
             if (c->fit_graph) {
                 cudaGraphExecDestroy(c->fit_graph);

@@ -6,8 +6,9 @@ screen -> admit -> fit -> rescore -> vary. Here every step runs on the
 device behind the library's C ABI, and only the bookkeeping between them is
 host code:
 
-  screen   rc_pool_score of every slot of the current pool (squared error
-           with the programs' own constants);
+  screen   rc_pool_score of every slot of the current pool (the configured
+           score kind, squared error by default, with the programs' own
+           constants);
   admit    rch_select_promoted (search.rs:3033-3074): per island, the best
            screened offspring that have constants, as many as
            rch_admission_count allows (everyone with constants at >= 2^20
@@ -25,6 +26,8 @@ a caller (or a test) can hold every device answer against the exact CPU
 fit of the same candidate.
 """
 from __future__ import annotations
+
+import time
 
 import numpy as np
 
@@ -53,11 +56,13 @@ class GenerationLoop:
     over the evaluator's resident rows (the training rows)."""
 
     def __init__(self, ev, islands, pop, nvars, max_complexity=30, fit_iters=8, seed=0,
-                 ops=DEFAULT_VARIATION_OPS, init_depth=3, fit_metric=0):
+                 ops=DEFAULT_VARIATION_OPS, init_depth=3, fit_metric=0, score_kind=0):
         self.ev = ev
         self.islands, self.pop = islands, pop
         self.nvars, self.max_complexity = nvars, max_complexity
         self.fit_iters, self.fit_metric = fit_iters, fit_metric
+        self.score_kind = score_kind
+        self.timing = {"screen": 0.0, "host": 0.0, "fit": 0.0, "rescore": 0.0, "vary": 0.0}
         self.seed, self.ops, self.init_depth = seed, ops, init_depth
         self.width = width_for(max_complexity)
         self.train_rows = ev.n
@@ -85,10 +90,14 @@ class GenerationLoop:
         return trees
 
     def generation(self):
-        """Run one generation; returns (records, errors after the rescore)."""
+        """Run one generation; returns (records, errors after the rescore).
+        `timing` accumulates the device ms of the screen, fit, rescore and
+        vary calls and the host ms of the steps between them."""
         n = self.islands * self.pop
-        err, _, ms = self.pool.score(self.cur, 0)
+        err, _, ms = self.pool.score(self.cur, self.score_kind)
         self.device_ms += ms
+        self.timing["screen"] += ms
+        t0 = time.perf_counter()
         trees = self._trees()
         cx = np.array([t.size() if t is not None else 1 << 20 for t in trees], np.float64)
         hasc = np.array([t is not None and len(t.constants()) > 0 for t in trees], np.uint8)
@@ -104,9 +113,12 @@ class GenerationLoop:
             except GpuFitReject:
                 continue
         records = []
+        self.timing["host"] += 1e3 * (time.perf_counter() - t0)
         if plans:
             c, loss, status, ms = self.ev.fit_plans(plans, self.fit_iters, self.fit_metric)
             self.device_ms += ms
+            self.timing["fit"] += ms
+            t0 = time.perf_counter()
             for k, (s, pl) in enumerate(zip(slots, plans)):
                 rec = FitRecord(s, trees[s], pl, c[k].copy(), float(loss[k]), int(status[k]))
                 records.append(rec)
@@ -121,12 +133,15 @@ class GenerationLoop:
                     self.words[s, :] = E.HALT
                     self.words[s, : len(w)] = w
             self.pool.upload(self.cur, self.words)
-            err, _, ms = self.pool.score(self.cur, 0)
+            self.timing["host"] += 1e3 * (time.perf_counter() - t0)
+            err, _, ms = self.pool.score(self.cur, self.score_kind)
             self.device_ms += ms
+            self.timing["rescore"] += ms
         self.gen += 1
         out = self.pool.vary(self.cur, err, self.gen, self.nvars, self.max_complexity, self.seed,
                              self.ops, init_depth=self.init_depth)
         self.device_ms += out[5]
+        self.timing["vary"] += out[5]
         self.words = out[0].copy()
         self.cur ^= 1
         return records, err
