@@ -212,6 +212,21 @@ float rc_fit_batch_plain(void *ctx, const unsigned int *prog, const unsigned int
                          const int *pcount, int nprog, int kmax, const double *c0,
                          const int *gauge, int iters, int metric, double *outc,
                          double *outsse, int *outstatus);
+/* Fit autotuner: per length bucket of the batch (fit programs of <= 16,
+   <= 32, <= 64 and more records) the assembly region budget that sets each
+   candidate's active threads, chosen by timing the fused fit of up to
+   `sample` (0: 64) of the bucket's candidates at budgets of 24-80 KB, kept in
+   the context for its (N, feature count) and, with a path, cached in that
+   text file ("fit n v bucket budget_kb" lines; a cached bucket is not
+   re-timed). The other arguments are rc_fit_batch_fused's. Returns the
+   number of buckets with a budget, or -1. No counterpart in the reference
+   ABI (its kernel shape is fixed at build time). */
+int rc_fit_autotune(void *ctx, const unsigned int *prog, const unsigned int *off,
+                    const int *pcount, int nprog, int kmax, const double *c0, const int *gauge,
+                    int iters, int metric, int sample, const char *path);
+/* The context's fit budgets in KB per length bucket (out_kb[4], 0 = the
+   built-in default). Returns 0, or -1. */
+int rc_fit_budgets(void *ctx, int *out_kb);
 /* Sweeps each candidate of the context's last fit ran (valid until the next
    call on the context), out[4 * cand + k]: k = 0 f32 assembly sweeps, 1 f32
    objective sweeps, 2 f64 assembly sweeps (implicit: Jacobian sweeps), 3 f64

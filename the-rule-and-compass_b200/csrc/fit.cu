@@ -37,6 +37,7 @@
 #include <cstddef>
 #include <cstdio>
 #include <cstring>
+#include <fstream>
 #include <string>
 #include <type_traits>
 #include <vector>
@@ -516,15 +517,19 @@ __host__ __device__ inline size_t ft_asm_region(int A, int slots, int tape, int 
 }
 
 /* Active threads of a candidate: the most (128, 64 or 32) whose region fits
-   the fixed budget. It depends on the candidate alone, so its summation
-   order does not depend on the batch. */
-inline int ft_asm_threads(int slots, int tape, int ncols)
+   the budget of its length bucket (FT_ASM_BUDGET unless the context's fit
+   autotuner chose another). It depends on the candidate and the context's
+   table alone, so its summation order does not depend on the batch. */
+inline int ft_asm_threads(int slots, int tape, int ncols, size_t budget)
 {
     const int W8 = 8 * ((ncols + 7) / 8);
     int A = FT_ASM_T;
-    while (A > 32 && ft_asm_region(A, slots, tape, W8) > FT_ASM_BUDGET) A /= 2;
+    while (A > 32 && ft_asm_region(A, slots, tape, W8) > budget) A /= 2;
     return A;
 }
+
+/* Length bucket of a fit program of m records (the autotuner's key). */
+inline int ft_length_bucket(int m) { return m <= 16 ? 0 : (m <= 32 ? 1 : (m <= 64 ? 2 : 3)); }
 
 __host__ __device__ inline bool ft_op_f64(int opk)
 {
@@ -2048,7 +2053,8 @@ bool validate_records(const uint32_t *rec, int m, int p, int v)
 
 /* Decode and check a batch of fit-record programs for the device sweeps. */
 void prep_batch(const unsigned int *off, const unsigned int *prog, const int *pcount, int nprog,
-                int v, FitPrep &b, int extra_cols, size_t cache_bytes_per_col, size_t cache_cap)
+                int v, FitPrep &b, int extra_cols, size_t cache_bytes_per_col, size_t cache_cap,
+                const int *bucket_budget_kb)
 {
     b.node_off.resize(nprog + 1);
     b.valid.resize(nprog);
@@ -2076,7 +2082,7 @@ void prep_batch(const unsigned int *off, const unsigned int *prog, const int *pc
     b.fins.clear();
     b.fins_off.assign(nprog + 1, 0);
     b.finfo.assign(nprog, make_int4(0, 0, 32, 0));
-    b.asm_region = FT_ASM_BUDGET;
+    b.asm_region = 256;
     for (int k = 0; k < 3; ++k) {
         b.asm_reg[k] = 256;
         b.nclass[k] = 0;
@@ -2143,7 +2149,11 @@ void prep_batch(const unsigned int *off, const unsigned int *prog, const int *pc
             b.fcinfo[i] = make_int2((int)fwd.size(), 0);
         }
         const int ncols = pcount[i] + 1 + extra_cols;
-        const int A = ft_asm_threads(ns, nt, ncols);
+        const int bkt = ft_length_bucket(m);
+        const size_t budget = (bucket_budget_kb && bucket_budget_kb[bkt] > 0)
+                                  ? (size_t)bucket_budget_kb[bkt] * 1024
+                                  : (size_t)FT_ASM_BUDGET;
+        const int A = ft_asm_threads(ns, nt, ncols, budget);
         b.finfo[i] = make_int4((int)fwd.size(), (int)rev.size(), A, ns | (nt << 16));
         const size_t reg = ft_asm_region(A, ns, nt, 8 * ((ncols + 7) / 8));
         b.asm_region = std::max(b.asm_region, reg);
@@ -2401,7 +2411,7 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     const size_t cache_cap = std::min<size_t>((size_t)48 << 30, free_b / 3);
     const bool use_cache = metric != FM_IMPLICIT;
     prep_batch(off, prog, pcount, nprog, c->v, b, corr ? 2 : 0,
-               use_cache ? sizeof(float) * (size_t)c->npad : 0, cache_cap);
+               use_cache ? sizeof(float) * (size_t)c->npad : 0, cache_cap, c->fit_budget_kb);
     XPrep xp;
     if (metric == FM_IMPLICIT) prep_inputs(off, prog, nprog, b.node_off, b.valid, xp);
     else xp.fins.resize(1);
@@ -2682,6 +2692,116 @@ float rc_fit_batch_plain(void *ctx, const unsigned int *prog, const unsigned int
 {
     return fit_run((RcCtx *)ctx, prog, off, pcount, nprog, kmax, c0, gauge, iters, metric, 0, outc,
                    outsse, outstatus, 1);
+}
+
+/* The fit autotuner. Per length bucket of the caller's batch (fit programs
+   of <= 16, <= 32, <= 64 and more records), the assembly region budget that
+   sets each candidate's active threads (and so how many of its rows are in
+   flight beside its spill slots, tape and Jacobian rows) is chosen by timing
+   the fused fit of up to `sample` of the bucket's candidates (the first
+   ones) at each budget in {24, 32, 40, 56, 80} KB: one warm-up fit, then the
+   fastest of two. The choice is kept in the context for its (N, feature
+   count) and, with a path, read from / written to that file as lines
+   "fit n v bucket budget_kb" (a bucket found there is not re-timed). The
+   budget changes a candidate's active threads and with it the order of its
+   sums: results depend on the table, never on the batch. Returns the number
+   of buckets with a budget, or -1. */
+int rc_fit_autotune(void *ctx, const unsigned int *prog, const unsigned int *off,
+                    const int *pcount, int nprog, int kmax, const double *c0, const int *gauge,
+                    int iters, int metric, int sample, const char *path)
+{
+    RcCtx *c = (RcCtx *)ctx;
+    if (!c || !prog || !off || !pcount || !c0 || nprog <= 0 || kmax <= 0 || kmax > FT_MAX_CONST)
+        return -1;
+    if (sample <= 0) sample = 64;
+    int have[4] = {0, 0, 0, 0};
+    std::vector<std::string> keep;
+    if (path) {
+        std::ifstream in(path);
+        std::string line;
+        while (std::getline(in, line)) {
+            long long n, v;
+            int bkt, kb;
+            char tag[8] = {0};
+            if (sscanf(line.c_str(), "%7s %lld %lld %d %d", tag, &n, &v, &bkt, &kb) == 5 &&
+                strcmp(tag, "fit") == 0 && n == c->n && v == c->v && bkt >= 0 && bkt < 4 &&
+                kb >= 8 && kb <= 200) {
+                c->fit_budget_kb[bkt] = kb;
+                have[bkt] = 1;
+            } else if (!line.empty()) {
+                keep.push_back(line);
+            }
+        }
+    }
+    /* the candidates of each bucket, up to `sample` */
+    std::vector<int> pick[4];
+    for (int i = 0; i < nprog; ++i) {
+        const int m = (int)((off[i + 1] - off[i]) / 4);
+        const int b = ft_length_bucket(m);
+        if ((int)pick[b].size() < sample) pick[b].push_back(i);
+    }
+    static const int budgets[] = {24, 32, 40, 56, 80};
+    for (int b = 0; b < 4; ++b) {
+        if (have[b] || pick[b].empty()) continue;
+        const int k = (int)pick[b].size();
+        std::vector<unsigned int> sp, so(1, 0);
+        std::vector<int> spc(k), sg(2 * (size_t)k, -1);
+        std::vector<double> sc0((size_t)k * kmax);
+        for (int j = 0; j < k; ++j) {
+            const int i = pick[b][j];
+            sp.insert(sp.end(), prog + off[i], prog + off[i + 1]);
+            so.push_back((unsigned int)sp.size());
+            spc[j] = pcount[i];
+            if (gauge) {
+                sg[2 * j] = gauge[2 * i];
+                sg[2 * j + 1] = gauge[2 * i + 1];
+            }
+            memcpy(&sc0[(size_t)j * kmax], c0 + (size_t)i * kmax, sizeof(double) * kmax);
+        }
+        std::vector<double> oc((size_t)k * kmax), osse(k);
+        std::vector<int> ost(k);
+        float best = -1.0f;
+        int best_kb = 0;
+        for (int kb : budgets) {
+            c->fit_budget_kb[b] = kb;
+            float t = fit_run(c, sp.data(), so.data(), spc.data(), k, kmax, sc0.data(),
+                              gauge ? sg.data() : nullptr, iters, metric, 0, oc.data(),
+                              osse.data(), ost.data(), 0);
+            if (t < 0.0f) continue;
+            for (int r = 0; r < 2; ++r) {
+                const float u = fit_run(c, sp.data(), so.data(), spc.data(), k, kmax, sc0.data(),
+                                        gauge ? sg.data() : nullptr, iters, metric, 0, oc.data(),
+                                        osse.data(), ost.data(), 0);
+                if (u >= 0.0f && u < t) t = u;
+            }
+            if (best < 0.0f || t < best) {
+                best = t;
+                best_kb = kb;
+            }
+        }
+        c->fit_budget_kb[b] = best_kb;
+        have[b] = best_kb > 0;
+    }
+    if (path) {
+        std::ofstream out(path, std::ios::trunc);
+        for (const auto &l : keep) out << l << "\n";
+        for (int b = 0; b < 4; ++b)
+            if (c->fit_budget_kb[b] > 0)
+                out << "fit " << c->n << " " << c->v << " " << b << " " << c->fit_budget_kb[b]
+                    << "\n";
+    }
+    int count = 0;
+    for (int b = 0; b < 4; ++b) count += c->fit_budget_kb[b] > 0;
+    return count;
+}
+
+/* The context's fit assembly budgets (KB) per length bucket, 0 = default. */
+int rc_fit_budgets(void *ctx, int *out_kb)
+{
+    RcCtx *c = (RcCtx *)ctx;
+    if (!c || !out_kb) return -1;
+    for (int b = 0; b < 4; ++b) out_kb[b] = c->fit_budget_kb[b];
+    return 0;
 }
 
 /* Sweeps each candidate of the context's last fit ran, out[4 * cand + k]:

@@ -267,12 +267,18 @@ __device__ __forceinline__ void ft_syrk_finish(const Syrk &s, double acc[16], do
 
    The step of one LM iteration solves (S + lambda diag S + 1e-12 I) u = -D^-1 g
    for the Jacobi-equilibrated normal matrix S = D^-1 (J^T J) D^-1,
-   D = sqrt(diag J^T J), and returns delta = D^-1 u. The answer and its labels
-   are the reference's (eval.cu:1873-1949, fit.rs:1686-1760): 1 when a diagonal
-   entry of J^T J is not positive and finite, a scaled entry is not finite, or
-   the damped factor breaks down (pivot <= 1e-18); 4 (rank deficient, the step
-   is still returned) when the undamped factor of S breaks down or
-   ln det S < ln 1e-12; else 0.
+   D = sqrt(diag J^T J), and returns delta = D^-1 u. The labels are the
+   reference kernel's (eval.cu:1873-1949): 1 when a diagonal entry of J^T J is
+   negative or not finite, a scaled entry is not finite, or the damped factor
+   breaks down (pivot <= 1e-18); 4 (rank deficient, the step is still
+   returned) when the undamped factor of S breaks down or ln det S <
+   ln 1e-12; else 0. One case follows the CPU fit instead (fit.rs:1686-1727):
+   a constant whose Jacobian column is exactly zero (a zero diagonal; its
+   gradient is then zero too) is held where it is, as the CPU's unscaled solve
+   does through its 1e-12 ridge, and the others' step is solved without it
+   (label 4). The reference kernel gives up the whole step there (label 1),
+   and in f32 such columns are common (a saturated logistic or tanh, an exp
+   that underflows), so its LM stopped where the CPU's went on.
 
    Layout: lane i (< p) keeps row i of both Cholesky factors of S, the
    undamped one (for the rank label) and the damped one (for the step), in
@@ -293,17 +299,23 @@ __device__ __forceinline__ int ft_solve_warp(const double *jtj, const double *jt
     const int lane = threadIdx.x & 31;
     const bool mine = lane < p;
     const double aii = mine ? jtj[lane * (lane + 1) / 2 + lane] : 1.0;
-    if (__any_sync(FT_FULL_MASK, !(aii > 0.0) || !isfinite(aii))) return 1;
-    const double di = sqrt(aii);
+    if (__any_sync(FT_FULL_MASK, aii < 0.0 || !isfinite(aii))) return 1;
+    /* a zero column: its row and column of S become the unit row and its
+       right-hand side zero, so its step is zero */
+    const bool held = mine && aii == 0.0;
+    const bool any_held = __any_sync(FT_FULL_MASK, held);
+    const double di = held ? 1.0 : sqrt(aii);
 
     double u[FT_MAX_CONST], l[FT_MAX_CONST];
     bool nonfinite = false;
 #pragma unroll
     for (int j = 0; j < FT_MAX_CONST; ++j) {
         const double dj = __shfl_sync(FT_FULL_MASK, di, j);
+        const bool hj = __shfl_sync(FT_FULL_MASK, held ? 1 : 0, j) != 0;
         double sij = 0.0;
         if (mine && j <= lane) {
-            sij = jtj[lane * (lane + 1) / 2 + j] / (di * dj);
+            if (held || hj) sij = (j == lane) ? 1.0 : 0.0;
+            else sij = jtj[lane * (lane + 1) / 2 + j] / (di * dj);
             nonfinite = nonfinite || !isfinite(sij);
         }
         u[j] = sij;
@@ -337,10 +349,11 @@ __device__ __forceinline__ int ft_solve_warp(const double *jtj, const double *jt
             l[k] = sd / rd;
         }
     }
-    const int label = (broke || !isfinite(lndet) || lndet < FT_LN_DET_FLOOR) ? 4 : 0;
+    const int label =
+        (any_held || broke || !isfinite(lndet) || lndet < FT_LN_DET_FLOOR) ? 4 : 0;
 
     /* forward: L y = -D^-1 g */
-    double yv = mine ? -jtr[lane] / di : 0.0;
+    double yv = (mine && !held) ? -jtr[lane] / di : 0.0;
 #pragma unroll
     for (int k = 0; k < FT_MAX_CONST; ++k) {
         if (k >= p) break;

@@ -44,7 +44,9 @@ struct FitPrep {
    assembly's Gram beyond p + 1 columns (the correlation moments use 2).
    With cache_bytes_per_col > 0, constant-free subtrees are cached (columns of
    that many bytes) while the total stays within cache_cap bytes; later
-   candidates keep their full forward list. */
+   candidates keep their full forward list. `bucket_budget_kb` (4 entries,
+   0 = the default) is the assembly region budget of each length bucket,
+   which sets a candidate's active threads. */
 void prep_batch(const unsigned int *off, const unsigned int *prog, const int *pcount, int nprog,
                 int v, FitPrep &b, int extra_cols = 0, size_t cache_bytes_per_col = 0,
-                size_t cache_cap = 0);
+                size_t cache_cap = 0, const int *bucket_budget_kb = nullptr);

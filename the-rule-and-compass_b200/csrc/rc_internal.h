@@ -126,6 +126,8 @@ struct RcCtx {
 
     /* autotuned scoring shapes: key = (bucket) -> (group, subtiles) */
     std::map<int, std::pair<int, int>> tune;
+    /* autotuned fit assembly budget (KB) per length bucket, 0 = default */
+    int fit_budget_kb[4];
 
     /* cached CUDA graph of the fused fit for a repeated batch shape */
     cudaGraphExec_t fit_graph;

@@ -75,6 +75,9 @@ SIGNATURES = {
     "rc_rank_debug_b": (ci, [cvp, i64p]),
     "rc_launch_count": (ci, [cvp, u64p]),
     "rc_last_fit_sweeps": (ci, [cvp, ci, ctypes.POINTER(ctypes.c_int32)]),
+    "rc_fit_autotune": (ci, [cvp, u32p, u32p, i32p, ci, ci, f64p, i32p, ci, ci, ci,
+                             ctypes.c_char_p]),
+    "rc_fit_budgets": (ci, [cvp, i32p]),
     "rc_last_score_profile": (ci, [cvp, ctypes.POINTER(ctypes.c_float),
                                    ctypes.POINTER(ctypes.c_float), u64p, u64p, u64p, u64p]),
     "rc_order_stat_score_batch": (cf, [cvp, u32p, u32p, i32p, ci, ci, ci, f64p, ci, f64p,
@@ -393,6 +396,27 @@ class GpuEvaluator:
         if lib().rc_launch_count(self.ctx, _p(out, ctypes.c_uint64)) != 0:
             raise DeviceError("rc_launch_count failed")
         return int(out[0])
+
+    def fit_autotune(self, plans, iters=20, metric=LOSS_SQUARED, sample=64, path=None):
+        """Tune the fit's assembly budget per length bucket on these plans
+        (rc_fit_autotune); returns the budgets in KB per bucket."""
+        from .host import pack_plans
+        prog, off, pcount, c0, gauge, kmax = pack_plans(plans)
+        prog, off = _c(prog, np.uint32), _c(off, np.uint32)
+        pcount, gauge, c0 = _c(pcount, np.int32), _c(gauge, np.int32), _c(c0, np.float64)
+        rc = lib().rc_fit_autotune(self.ctx, _p(prog, ctypes.c_uint32), _p(off, ctypes.c_uint32),
+                                   _p(pcount, ctypes.c_int32), len(off) - 1, kmax,
+                                   _p(c0, ctypes.c_double), _p(gauge, ctypes.c_int32), iters,
+                                   metric, sample, None if path is None else path.encode())
+        if rc < 0:
+            raise DeviceError("rc_fit_autotune failed")
+        return self.fit_budgets()
+
+    def fit_budgets(self):
+        out = np.zeros(4, np.int32)
+        if lib().rc_fit_budgets(self.ctx, _p(out, ctypes.c_int32)) != 0:
+            raise DeviceError("rc_fit_budgets failed")
+        return out.tolist()
 
     def fit_sweeps(self, nprog):
         """Sweeps per candidate of the last fit: int32 [P][4] (f32 assembly,
