@@ -438,14 +438,20 @@ def fit_setup(pkg, W, case, P, N, seed):
     return ev, plans, trees, x, y, metric, what
 
 
-def time_fit(pkg, ev, plans, metric, N, steps, warmup, flushbuf, plain_n, seed):
+def time_fit(pkg, ev, plans, metric, N, steps, warmup, flushbuf, plain_n, seed, tune=True):
     """Fused fits of the whole batch (graph-replayed), timed per step on the
     device and end to end; then the plain one-candidate-per-launch form on a
     seeded random sample of the same candidates (its cost is linear in the
-    candidate count), whose losses must equal the fused ones bit for bit."""
+    candidate count), whose losses must equal the fused ones bit for bit.
+    Before timing (and outside it), the library's fit autotuner chooses the
+    assembly budget per length bucket on this batch (`rc_fit_autotune`); both
+    arms then run with the chosen table."""
     import torch
     iters = 20
     P = len(plans)
+    # the tuning sample shrinks with N so that tuning stays a few seconds
+    sample = max(16, min(64, int(64 * 262144 // max(N, 1))))
+    budgets = ev.fit_autotune(plans, iters, metric, sample=sample) if tune else None
     prog, off, pcount, c0, gauge, kmax = pkg.pack_plans(plans)
     for _ in range(warmup):
         ev.fit_batch_fused(prog, off, pcount, c0, gauge, kmax, iters, metric)
@@ -466,7 +472,7 @@ def time_fit(pkg, ev, plans, metric, N, steps, warmup, flushbuf, plain_n, seed):
                unit_count=float(P), status=np.bincount(st, minlength=9).tolist(),
                h2d=int(prog.nbytes + off.nbytes + pcount.nbytes + c0.nbytes + gauge.nbytes),
                d2h=int(P * (kmax * 8 + 8 + 4)), loss=loss, status_list=st,
-               sweeps_mean=sweeps.mean(0).tolist(),
+               sweeps_mean=sweeps.mean(0).tolist(), fit_budgets_kb=budgets,
                lane_ops=fit_lane_ops(plans, sweeps, N, metric))
     if plain_n:
         rng = np.random.Generator(np.random.PCG64(seed + 77))
@@ -494,7 +500,8 @@ def fit_summary(r, peaks, what):
          "e2e": r["unit_count"] * len(r["wall"]) / sum(r["wall"]),
          "ms_per_step": float(np.mean(r["dev_ms"])), "steps": len(r["dev_ms"]),
          "config": what, "gpu_launches": r["launches"], "status_histogram": r["status"],
-         "sweeps_per_candidate": r["sweeps_mean"], "clocks": r["clocks"]}
+         "sweeps_per_candidate": r["sweeps_mean"], "fit_budgets_kb": r.get("fit_budgets_kb"),
+         "clocks": r["clocks"]}
     for k in ("status_histogram_reference_mode", "status57_classified", "cpu_baseline"):
         if k in r:
             d[k] = r[k]
@@ -604,7 +611,8 @@ def bench_implicit(args, rank, pkg, W, flushbuf, steps, warmup, fit_steps, fit_w
              "config": f"implicit |f|/||grad f|| scoring, P={P}, N={N} rows x 4 inputs"}
     fplans = [pkg.gpu_fit_plan(t) for t in trees if t.constants()]
     ftrees = [t for t in trees if t.constants()]
-    fit = time_fit(pkg, ev, fplans, 6, N, fit_steps, fit_warmup, flushbuf, 16, rank)
+    # the implicit sweeps' shapes do not depend on the assembly budget
+    fit = time_fit(pkg, ev, fplans, 6, N, fit_steps, fit_warmup, flushbuf, 16, rank, tune=False)
     ev.close()
     if not args.no_cpu_baseline:
         threads = os.cpu_count() or 1

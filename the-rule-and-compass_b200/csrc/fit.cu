@@ -2204,6 +2204,7 @@ struct SweepLaunch {
     size_t smem;
     int grid;
     int threads;
+    int opk; /* the queue kind it serves */
 };
 
 /* Input-mode translation (fi_decode with `inputs`) of every valid candidate:
@@ -2249,6 +2250,7 @@ SweepLaunch icost_launch(RcCtx *c, const XPrep &x)
 {
     SweepLaunch s;
     s.fn = (const void *)ft_sweep<FOP_ICOST, FT_ITHREADS>;
+    s.opk = FOP_ICOST;
     s.smem = 8 * (size_t)((x.maxins + 1) & ~1) + 8 * FT_MAX_CONST +
              8 * (size_t)FT_ITHREADS * (x.slots + x.tape + c->v) + 8 * (size_t)FT_ITHREADS;
     if (s.smem > 48 * 1024)
@@ -2263,6 +2265,7 @@ SweepLaunch sweep_launch(RcCtx *c, int mrec, int tcap, int Wmax)
 {
     SweepLaunch s;
     s.fn = (const void *)ft_jac_sweep<OPK, FT_ITHREADS>;
+    s.opk = OPK;
     s.smem = ft_ijac_smem(mrec, tcap, Wmax, FT_ITHREADS);
     if (s.smem > 48 * 1024)
         cudaFuncSetAttribute(s.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
@@ -2338,6 +2341,7 @@ SweepLaunch sweep4_launch(RcCtx *c, const FitPrep &b, int Wmax)
 {
     SweepLaunch s;
     s.fn = (const void *)ft_sweep4<OPK, T>;
+    s.opk = OPK;
     (void)Wmax;
     const int bk = ft_base_kind(OPK);
     const size_t reg = OPK != bk ? b.asm_reg[ft_class_of(T)]
@@ -2596,7 +2600,18 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
             one.outc = a.outc + (size_t)i * kmax;
             one.outsse = a.outsse + i;
             one.outstatus = a.outstatus + i;
-            c->launches += enqueue_fit(c->s, c->sm_count, one, steps, sw, nk);
+            /* only the assembly launches of this candidate's class */
+            SweepLaunch swc[8];
+            int nkc = 0;
+            const int cls = ft_class_of(b.finfo[i].z);
+            for (int k = 0; k < nk; ++k) {
+                const int o = sw[k].opk;
+                const bool asm_cls = o == FOP_ASM32 || o == FOP_ASM64 || o == FOP_ASM32_64 ||
+                                     o == FOP_ASM32_32 || o == FOP_ASM64_64 || o == FOP_ASM64_32;
+                if (asm_cls && ft_class_of(sw[k].threads) != cls) continue;
+                swc[nkc++] = sw[k];
+            }
+            c->launches += enqueue_fit(c->s, c->sm_count, one, steps, swc, nkc);
             ok = cudaGetLastError() == cudaSuccess;
         }
     } else {
