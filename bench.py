@@ -122,6 +122,18 @@ SCORE_SAMPLE_PROGS, SCORE_SAMPLE_ROWS = 64, 1 << 16
 # DRAM bytes (read + write) of one launch of the f32 scoring kernel on the
 # P = 4096, N = 1,048,576 workload, from ncu (profiles/rc_score_kernel_P4096_N1M.md).
 SCORE_TRAFFIC = 25.69e6
+# DRAM bytes per candidate*row of one f32 assembly sweep of the fit (ncu on
+# the first assembly of P = 256 at N = 1,048,576: 1.90 GB and 2.05 GB for the
+# two active-thread classes of 128 candidates each; mostly the constant-free
+# subtree cache columns), profiles/ft_sweep4_classes_fit_P256_N1M.md.
+FIT_ASM_TRAFFIC = {"bytes_per_candidate_row_f32_assembly": 15.0,
+                   "source": "profiles/ft_sweep4_classes_fit_P256_N1M.md"}
+# DRAM bytes per candidate*row of the whole rank stage, from the per-kernel
+# ncu figures of profiles/rank_stage_P16_N1M.md: keys and rows written
+# (12 B), the digit count read (8 B), eight sort passes at 21.7 B per key
+# (203 MB + 161 MB per 16.8 M keys), the run pass (about 12 B).
+RANK_TRAFFIC = {"bytes_per_candidate_row": 206.0, "algorithmic": 32.0,
+                "source": "profiles/rank_stage_P16_N1M.md"}
 
 
 def flush_l2(buf):
@@ -679,7 +691,7 @@ def rank_stage(pkg, ev, plans, N, flushbuf, steps, warmup):
             "d2h": int(P * (4 * 8 + 4) + 16 * len(chunks)), "calls_per_step": len(chunks),
             "finite_segments": int((status == 0).sum()),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak, "traffic": RANK_TRAFFIC,
                          "note": "algorithmic 32 B per candidate*row (f64 eval, 8 B key, 4 B "
                                  "row, read back, 8 B gathered target rank) / event time; "
                                  "peak = measured copy bandwidth (MEASURED_PEAKS.json)"}}
@@ -901,7 +913,7 @@ def fit_roofline(r, peaks):
     achieved = r["lane_ops"] / per / 1e9
     peak = 148 * 128 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e9
     return {"bound": "fp32_issue", "achieved": achieved, "peak": peak, "unit": "Glane-op/s",
-            "frac": achieved / peak, "traffic": r.get("traffic"),
+            "frac": achieved / peak, "traffic": FIT_ASM_TRAFFIC,
             "note": "the sweeps each candidate ran (device counts) x N x their per-row "
                     "FP32-lane-op equivalents (f32 assembly 3.5 L + 2 G, f32 objective L + 2, "
                     "f64 sweeps twice the f32 cost; G = p(p+1)/2 + p + 1 FMAs of the Gram "

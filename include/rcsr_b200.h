@@ -270,6 +270,30 @@ int rc_last_score_profile(void *ctx, float *ms_f32, float *ms_rest,
                           unsigned long long *rows_f32, unsigned long long *rows_f64,
                           unsigned long long *ops_f32, unsigned long long *ops_f64);
 
+/* ---- several GPUs behind one handle (no counterpart in the reference) -- */
+
+/* One context per device in devices[ndev] (a device may be named twice),
+   each holding the rows. The batch calls split the candidates into
+   contiguous slices balanced by program words, run each slice on its device
+   from its own host thread, and write every candidate's outputs at its place
+   in the caller's arrays; a candidate answers exactly what a single context
+   would. They return the slowest slice's kernel ms, or a negative value when
+   any slice failed (then every output is to be discarded). NULL / -1 on
+   failure. */
+void *rc_multi_create(const float *cols, int n, int v, const float *y, int ndev,
+                      const int *devices);
+void rc_multi_destroy(void *multi);
+int rc_multi_set_fit_data(void *multi, const double *cols, const double *y, const double *w);
+float rc_multi_score_batch(void *multi, const unsigned int *prog, const unsigned int *off,
+                           int nprog, int kind, const int *pcount, double *out, int *status);
+float rc_multi_fit_batch(void *multi, const unsigned int *prog, const unsigned int *off,
+                         const int *pcount, int nprog, int kmax, const double *c0,
+                         const int *gauge, int iters, int metric, int flags, double *outc,
+                         double *outsse, int *outstatus);
+/* The number of devices; with ctx_out[ndev], each device's context (make that
+   device current before passing it to a single-device call). */
+int rc_multi_devices(void *multi, void **ctx_out);
+
 /* Scoring for callers that cannot allocate device memory. No counterpart in
    the reference: it exists for host applications whose device memory is
    owned by another allocator, and for pipelined callers on their own streams

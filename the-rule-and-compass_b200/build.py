@@ -26,7 +26,7 @@ NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + INCLUDE,
               "-I" + CSRC]
-SOURCES = ["ctx.cu", "score.cu", "fit.cu", "rank.cu", "vary.cu"]
+SOURCES = ["ctx.cu", "score.cu", "fit.cu", "rank.cu", "vary.cu", "multi.cu"]
 
 
 def _stale(target, deps):

@@ -75,6 +75,13 @@ SIGNATURES = {
     "rc_rank_debug_b": (ci, [cvp, i64p]),
     "rc_launch_count": (ci, [cvp, u64p]),
     "rc_last_fit_sweeps": (ci, [cvp, ci, ctypes.POINTER(ctypes.c_int32)]),
+    "rc_multi_create": (cvp, [f32p, ci, ci, f32p, ci, i32p]),
+    "rc_multi_destroy": (None, [cvp]),
+    "rc_multi_set_fit_data": (ci, [cvp, f64p, f64p, f64p]),
+    "rc_multi_score_batch": (cf, [cvp, u32p, u32p, ci, ci, i32p, f64p, i32p]),
+    "rc_multi_fit_batch": (cf, [cvp, u32p, u32p, i32p, ci, ci, f64p, i32p, ci, ci, ci, f64p,
+                                f64p, i32p]),
+    "rc_multi_devices": (ci, [cvp, ctypes.POINTER(cvp)]),
     "rc_fit_autotune": (ci, [cvp, u32p, u32p, i32p, ci, ci, f64p, i32p, ci, ci, ci,
                              ctypes.c_char_p]),
     "rc_fit_budgets": (ci, [cvp, i32p]),
@@ -538,3 +545,68 @@ class GenomePool:
         if ms < 0:
             raise DeviceError("rc_pool_vary failed")
         return (None if ow is None else ow.reshape(n, self.width)), ol, oc, oh, oe, ms
+
+
+class MultiEvaluator:
+    """Several GPUs behind one handle (`rc_multi_*`): one context per device,
+    each holding the rows; batches are split into contiguous candidate slices
+    run concurrently, and the outputs gathered in place."""
+
+    def __init__(self, cols, n, v, y, devices):
+        c, yy = _c(cols, np.float32), _c(y, np.float32)
+        d = np.ascontiguousarray(devices, np.int32)
+        self.n, self.v, self.ndev = n, v, len(d)
+        self.h = lib().rc_multi_create(_p(c, ctypes.c_float), n, v, _p(yy, ctypes.c_float),
+                                       len(d), _p(d, ctypes.c_int32))
+        if not self.h:
+            raise DeviceError("rc_multi_create failed")
+
+    def close(self):
+        if self.h:
+            lib().rc_multi_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_fit_data(self, cols64, y64, w=None):
+        c, y = _c(cols64, np.float64), _c(y64, np.float64)
+        w = _c(w, np.float64) if w is not None else None
+        if lib().rc_multi_set_fit_data(self.h, _p(c, ctypes.c_double), _p(y, ctypes.c_double),
+                                       _p(w, ctypes.c_double)) != 0:
+            raise DeviceError("rc_multi_set_fit_data failed")
+
+    def score_batch(self, prog, off, kind, pcount=None):
+        prog, off = _c(prog, np.uint32), _c(off, np.uint32)
+        P_ = len(off) - 1
+        pc = _c(pcount if pcount is not None else np.zeros(P_), np.int32)
+        out = np.zeros(P_, np.float64)
+        st = np.zeros(P_, np.int32)
+        ms = lib().rc_multi_score_batch(self.h, _p(prog, ctypes.c_uint32),
+                                        _p(off, ctypes.c_uint32), P_, kind,
+                                        _p(pc, ctypes.c_int32), _p(out, ctypes.c_double),
+                                        _p(st, ctypes.c_int32))
+        if ms < 0:
+            raise DeviceError("rc_multi_score_batch failed")
+        return out, st, ms
+
+    def fit_plans(self, plans, iters, metric=LOSS_SQUARED, flags=0):
+        from .host import pack_plans
+        prog, off, pcount, c0, gauge, kmax = pack_plans(plans)
+        prog, off = _c(prog, np.uint32), _c(off, np.uint32)
+        pcount, gauge, c0 = _c(pcount, np.int32), _c(gauge, np.int32), _c(c0, np.float64)
+        P_ = len(off) - 1
+        outc = np.zeros((P_, kmax), np.float64)
+        outsse = np.zeros(P_, np.float64)
+        st = np.zeros(P_, np.int32)
+        ms = lib().rc_multi_fit_batch(self.h, _p(prog, ctypes.c_uint32), _p(off, ctypes.c_uint32),
+                                      _p(pcount, ctypes.c_int32), P_, kmax,
+                                      _p(c0, ctypes.c_double), _p(gauge, ctypes.c_int32), iters,
+                                      metric, flags, _p(outc, ctypes.c_double),
+                                      _p(outsse, ctypes.c_double), _p(st, ctypes.c_int32))
+        if ms < 0:
+            raise DeviceError("rc_multi_fit_batch failed")
+        return outc, outsse, st, ms

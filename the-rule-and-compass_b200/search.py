@@ -76,18 +76,30 @@ class GenerationLoop:
         out = self.pool.vary(0, np.zeros(n), 0, nvars, max_complexity, seed, ops,
                              init_depth=init_depth, restart=[1] * islands)
         self.words = out[0].copy()
+        self.cost = out[2].astype(np.float64)
         self.cur = 1
         self.gen = 0
         self.device_ms = 0.0
 
-    def _trees(self):
-        trees = []
-        for w in self.words:
-            try:
-                trees.append(E.from_postfix(w))
-            except ValueError:
-                trees.append(None)
-        return trees
+    def _tree(self, s):
+        try:
+            return E.from_postfix(self.words[s])
+        except ValueError:
+            return None
+
+    @staticmethod
+    def _has_constant(w):
+        """Whether a postfix program pushes a constant (a CONST opcode word,
+        not an operand word)."""
+        i, n = 0, len(w)
+        while i < n:
+            op = w[i]
+            if op == E.HALT:
+                return False
+            if op == E.CONST:
+                return True
+            i += 2 if op == E.VAR else 1
+        return False
 
     def generation(self):
         """Run one generation; returns (records, errors after the rescore).
@@ -98,18 +110,23 @@ class GenerationLoop:
         self.device_ms += ms
         self.timing["screen"] += ms
         t0 = time.perf_counter()
-        trees = self._trees()
-        cx = np.array([t.size() if t is not None else 1 << 20 for t in trees], np.float64)
-        hasc = np.array([t is not None and len(t.constants()) > 0 for t in trees], np.uint8)
+        # admission ranks by the screened error and the complexity the
+        # variation engine reports; only the admitted programs are decoded
+        wl = self.words.tolist()
+        hasc = np.array([self._has_constant(w) for w in wl], np.uint8)
         pending = [(i // self.pop, i % self.pop) for i in range(n)]
-        admitted = select_promoted([self.pop] * self.islands, pending, err, cx, hasc,
+        admitted = select_promoted([self.pop] * self.islands, pending, err, self.cost, hasc,
                                    self.train_rows)
-        slots, plans = [], []
+        slots, plans, trees = [], [], {}
         for isl, j in admitted:
             s = isl * self.pop + j
+            t = self._tree(s)
+            if t is None:
+                continue
             try:
-                plans.append(gpu_fit_plan(trees[s]))
+                plans.append(gpu_fit_plan(t))
                 slots.append(s)
+                trees[s] = t
             except GpuFitReject:
                 continue
         records = []
@@ -143,5 +160,6 @@ class GenerationLoop:
         self.device_ms += out[5]
         self.timing["vary"] += out[5]
         self.words = out[0].copy()
+        self.cost = out[2].astype(np.float64)
         self.cur ^= 1
         return records, err
