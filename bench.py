@@ -461,9 +461,8 @@ def time_fit(pkg, ev, plans, metric, N, steps, warmup, flushbuf, plain_n, seed, 
     import torch
     iters = 20
     P = len(plans)
-    # the tuning sample shrinks with N so that tuning stays a few seconds
-    sample = max(16, min(64, int(64 * 262144 // max(N, 1))))
-    budgets = ev.fit_autotune(plans, iters, metric, sample=sample) if tune else None
+    # sample 0: a tuning batch of about 16,384 (candidate, tile) items per bucket
+    budgets = ev.fit_autotune(plans, iters, metric, sample=0) if tune else None
     prog, off, pcount, c0, gauge, kmax = pkg.pack_plans(plans)
     for _ in range(warmup):
         ev.fit_batch_fused(prog, off, pcount, c0, gauge, kmax, iters, metric)

@@ -214,11 +214,14 @@ float rc_fit_batch_plain(void *ctx, const unsigned int *prog, const unsigned int
                          double *outsse, int *outstatus);
 /* Fit autotuner: per length bucket of the batch (fit programs of <= 16,
    <= 32, <= 64 and more records) the assembly region budget that sets each
-   candidate's active threads, chosen by timing the fused fit of up to
-   `sample` (0: 64) of the bucket's candidates at budgets of 24-80 KB, kept in
-   the context for its (N, feature count) and, with a path, cached in that
-   text file ("fit n v bucket budget_kb" lines; a cached bucket is not
-   re-timed). The other arguments are rc_fit_batch_fused's. Returns the
+   candidate's active threads, chosen by timing the fused fit of a tuning
+   batch of the bucket's candidates at budgets of 24-80 KB (`sample`
+   candidates, or with sample <= 0 as many as make about 16,384 (candidate,
+   tile) work items, so that the tuning batch fills the GPU like a real one;
+   the bucket's first candidates repeated when it has fewer); a budget
+   replaces the default only when at least 3 % faster. Kept in the context
+   for its (N, feature count) and, with a path, cached in that text file
+   ("fit n v bucket budget_kb" lines; a cached bucket is not re-timed). The other arguments are rc_fit_batch_fused's. Returns the
    number of buckets with a budget, or -1. No counterpart in the reference
    ABI (its kernel shape is fixed at build time). */
 int rc_fit_autotune(void *ctx, const unsigned int *prog, const unsigned int *off,

@@ -57,31 +57,66 @@
 enum {
     FOP_NONE = 0, FOP_ASM32 = 1, FOP_ASM64 = 2, FOP_LOSS32 = 3, FOP_LOSS64 = 4,
     FOP_IJAC = 5, FOP_ICOST = 6, FOP_CASM = 7, FOP_CSCORE = 8, FOP_IJACS = 9,
-    /* the assembly queues of candidates with 64 and 32 active threads: their
-       sweeps run in blocks of that many threads, sized for their class */
+    /* the assembly queues of the other launch classes (ft_cls_*): their
+       sweeps run in blocks of the class's threads, sized for the class */
     FOP_ASM32_64 = 10, FOP_ASM32_32 = 11, FOP_ASM64_64 = 12, FOP_ASM64_32 = 13,
-    FOP_COUNT = 14
+    FOP_ASM32_64A = 14, FOP_ASM32_64B = 15, FOP_ASM64_64A = 16, FOP_ASM64_64B = 17,
+    FOP_COUNT = 18
 };
+
+/* Launch classes of the assemblies. A candidate's active threads A and its
+   shared region decide it: 0: A = 128; 1, 2, 3: A = 64 with a region of at
+   most 21 KB, at most 30 KB, or more; 4: A = 32. A class's launch uses
+   blocks of A threads and the largest region of its candidates, so the
+   small-region classes fit more blocks on an SM (10, 7 and 5 of 64 threads
+   at 21, 30 and 40 KB). Which launch runs a candidate does not change its
+   arithmetic (that depends on A alone). */
+#define FT_NCLS 5
+__host__ __device__ constexpr int ft_cls_threads(int cls)
+{
+    return cls == 0 ? 128 : (cls == 4 ? 32 : 64);
+}
+
+inline int ft_cls_of(int A, size_t region)
+{
+    if (A >= 128) return 0;
+    if (A <= 32) return 4;
+    return region <= 21 * 1024 ? 1 : (region <= 30 * 1024 ? 2 : 3);
+}
 
 /* The kind a queue's sweep performs (a class queue performs its base kind). */
 __host__ __device__ constexpr int ft_base_kind(int k)
 {
-    return (k == FOP_ASM32_64 || k == FOP_ASM32_32)   ? FOP_ASM32
-           : (k == FOP_ASM64_64 || k == FOP_ASM64_32) ? FOP_ASM64
-                                                      : k;
+    return (k == FOP_ASM32_64 || k == FOP_ASM32_32 || k == FOP_ASM32_64A || k == FOP_ASM32_64B)
+               ? FOP_ASM32
+           : (k == FOP_ASM64_64 || k == FOP_ASM64_32 || k == FOP_ASM64_64A ||
+              k == FOP_ASM64_64B)
+               ? FOP_ASM64
+               : k;
+}
+
+/* The launch class of an assembly queue kind (0 for the base kinds). */
+__host__ __device__ constexpr int ft_kind_cls(int k)
+{
+    return (k == FOP_ASM32_64A || k == FOP_ASM64_64A)   ? 1
+           : (k == FOP_ASM32_64B || k == FOP_ASM64_64B) ? 2
+           : (k == FOP_ASM32_64 || k == FOP_ASM64_64)   ? 3
+           : (k == FOP_ASM32_32 || k == FOP_ASM64_32)   ? 4
+                                                        : 0;
 }
 
 /* The queue of a sweep request: f32 / f64 assemblies go to the queue of the
-   candidate's active-thread class. */
-__host__ __device__ inline int ft_queue_kind(int op, int A)
+   candidate's launch class. */
+__host__ __device__ inline int ft_queue_kind(int op, int cls)
 {
-    if (op == FOP_ASM32) return A == 64 ? FOP_ASM32_64 : (A == 32 ? FOP_ASM32_32 : op);
-    if (op == FOP_ASM64) return A == 64 ? FOP_ASM64_64 : (A == 32 ? FOP_ASM64_32 : op);
+    static constexpr int k32[FT_NCLS] = {FOP_ASM32, FOP_ASM32_64A, FOP_ASM32_64B, FOP_ASM32_64,
+                                         FOP_ASM32_32};
+    static constexpr int k64[FT_NCLS] = {FOP_ASM64, FOP_ASM64_64A, FOP_ASM64_64B, FOP_ASM64_64,
+                                         FOP_ASM64_32};
+    if (op == FOP_ASM32) return k32[cls];
+    if (op == FOP_ASM64) return k64[cls];
     return op;
 }
-
-/* Index of an active-thread class: 128, 64, 32 threads. */
-__host__ __device__ constexpr int ft_class_of(int A) { return A >= 128 ? 0 : (A >= 64 ? 1 : 2); }
 
 enum {
     PC_INIT = 0, PC_AFTER_FIRST_ASM, PC_ROUND, PC_ITER, PC_AFTER_ASM, PC_SOLVE,
@@ -173,13 +208,14 @@ struct FitArgs {
     const int *valid;
     const FIns *fins;      /* stack-machine translation of the records */
     const int *fins_off;   /* [P+1] start of [forward | reverse] */
-    const int4 *finfo;     /* [P] forward count, reverse count, active threads,
+    const int4 *finfo;     /* [P] forward count, reverse count, active threads | launch
+                              class << 16,
                               spill slots | tape slots << 16 */
     int fslots;            /* spill slots needed by the batch */
     int ftape;             /* partial-tape slots needed by the batch */
     int fmaxins;           /* longest forward + reverse list */
     size_t asm_region;     /* assembly region of a 128-thread launch over every class */
-    size_t asm_reg[3];     /* assembly region of the 128-, 64- and 32-thread class launches */
+    size_t asm_reg[5];     /* assembly region of each launch class (ft_cls_of) */
     const int2 *fcinfo;    /* [P] cached forward count (after the reverse list),
                               first cache column */
     float *cache;          /* [columns][npad] values of constant-free subtrees */
@@ -921,7 +957,7 @@ __global__ void __launch_bounds__(T) ft_sweep4(FitArgs a, int q)
                                                               8 * FT_MAX_CONST);
     /* a class queue's region is sized for its class; the 128-thread launch
        of a base assembly kind for every candidate it may hold */
-    const size_t asm_reg = OPK != BK ? a.asm_reg[ft_class_of(T)]
+    const size_t asm_reg = OPK != BK ? a.asm_reg[ft_kind_cls(OPK)]
                            : (BK == FOP_CASM ? a.asm_region : a.asm_reg[0]);
     double *red = reinterpret_cast<double *>(
         region + (ft_op_assembles(OPK) ? asm_reg
@@ -965,7 +1001,8 @@ __global__ void __launch_bounds__(T) ft_sweep4(FitArgs a, int q)
         const int r1 = min(a.n, r0 + FT_TILE_ROWS);
         double *pt = a.part + ((size_t)cand * a.ntiles + tile) * FT_PART_STRIDE;
         if (ft_op_assembles(OPK))
-            ft_tile_asm<V, NR, T, BK == FOP_CASM>(a, ins, ins + nf, nr, p, info.z, info.w & 0xffff,
+            ft_tile_asm<V, NR, T, BK == FOP_CASM>(a, ins, ins + nf, nr, p, info.z & 0xffff,
+                                                  info.w & 0xffff,
                                                   info.w >> 16, cv, region, red, r0, r1, pt, ccols);
         else if (BK == FOP_CSCORE)
             ft_tile_corr_score<NR, T>(a, ins, reinterpret_cast<const float *>(cv),
@@ -1762,7 +1799,7 @@ __global__ void __launch_bounds__(FT_CTRL_T) ft_control(FitArgs a, int q, int in
             for (int i = tid; i < (int)(sizeof(FitState) / 8); i += FT_CTRL_T) dst[i] = src[i];
         }
         if (tid == 0 && sst.op != FOP_NONE) {
-            const int kq = ft_queue_kind(sst.op, a.finfo[cand].z);
+            const int kq = ft_queue_kind(sst.op, a.finfo[cand].z >> 16);
             const int k = atomicAdd(&a.counts[nq * FOP_COUNT + kq], 1);
             a.lists[((size_t)nq * FOP_COUNT + kq) * a.nprog + k] = cand;
         }
@@ -2083,7 +2120,7 @@ void prep_batch(const unsigned int *off, const unsigned int *prog, const int *pc
     b.fins_off.assign(nprog + 1, 0);
     b.finfo.assign(nprog, make_int4(0, 0, 32, 0));
     b.asm_region = 256;
-    for (int k = 0; k < 3; ++k) {
+    for (int k = 0; k < FT_NCLS; ++k) {
         b.asm_reg[k] = 256;
         b.nclass[k] = 0;
     }
@@ -2154,11 +2191,14 @@ void prep_batch(const unsigned int *off, const unsigned int *prog, const int *pc
                                   ? (size_t)bucket_budget_kb[bkt] * 1024
                                   : (size_t)FT_ASM_BUDGET;
         const int A = ft_asm_threads(ns, nt, ncols, budget);
-        b.finfo[i] = make_int4((int)fwd.size(), (int)rev.size(), A, ns | (nt << 16));
         const size_t reg = ft_asm_region(A, ns, nt, 8 * ((ncols + 7) / 8));
+        const int cls = ft_cls_of(A, reg);
+        /* z: active threads, launch class above bit 16 */
+        b.finfo[i] = make_int4((int)fwd.size(), (int)rev.size(), A | (cls << 16),
+                               ns | (nt << 16));
         b.asm_region = std::max(b.asm_region, reg);
-        b.asm_reg[ft_class_of(A)] = std::max(b.asm_reg[ft_class_of(A)], reg);
-        b.nclass[ft_class_of(A)]++;
+        b.asm_reg[cls] = std::max(b.asm_reg[cls], reg);
+        b.nclass[cls]++;
         b.fslots = std::max(b.fslots, ns);
         b.ftape = std::max(b.ftape, nt);
         b.fmaxins = std::max(b.fmaxins, (int)(fwd.size() + rev.size()));
@@ -2344,7 +2384,7 @@ SweepLaunch sweep4_launch(RcCtx *c, const FitPrep &b, int Wmax)
     s.opk = OPK;
     (void)Wmax;
     const int bk = ft_base_kind(OPK);
-    const size_t reg = OPK != bk ? b.asm_reg[ft_class_of(T)]
+    const size_t reg = OPK != bk ? b.asm_reg[ft_kind_cls(OPK)]
                        : (bk == FOP_CASM ? b.asm_region : b.asm_reg[0]);
     s.smem = ft_sweep4_smem(OPK, b.fmaxins, b.fslots, reg, T);
     if (s.smem > 48 * 1024)
@@ -2519,7 +2559,7 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     a.xslots = xp.slots;
     a.xtape = xp.tape;
     a.asm_region = b.asm_region;
-    for (int k = 0; k < 3; ++k) a.asm_reg[k] = b.asm_reg[k];
+    for (int k = 0; k < FT_NCLS; ++k) a.asm_reg[k] = b.asm_reg[k];
     a.fslots = b.fslots;
     a.ftape = b.ftape;
     a.fmaxins = b.fmaxins;
@@ -2539,7 +2579,7 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
     a.outsse = reinterpret_cast<double *>(dev + o_sse);
     a.outstatus = reinterpret_cast<int *>(dev + o_status);
 
-    SweepLaunch sw[8];
+    SweepLaunch sw[16];
     int nk = 0;
     if (metric == FM_IMPLICIT) {
         const IjacSplit js = ijac_split(c, b, Wmax);
@@ -2558,15 +2598,19 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
         /* one assembly launch per active-thread class present in the batch,
            each in blocks of that many threads */
         if (b.nclass[0]) { sw[nk] = sweep4_launch<FOP_ASM32, FT_ASM_T>(c, b, Wmax); ++nk; }
-        if (b.nclass[1]) { sw[nk] = sweep4_launch<FOP_ASM32_64, 64>(c, b, Wmax); ++nk; }
-        if (b.nclass[2]) { sw[nk] = sweep4_launch<FOP_ASM32_32, 32>(c, b, Wmax); ++nk; }
+        if (b.nclass[1]) { sw[nk] = sweep4_launch<FOP_ASM32_64A, 64>(c, b, Wmax); ++nk; }
+        if (b.nclass[2]) { sw[nk] = sweep4_launch<FOP_ASM32_64B, 64>(c, b, Wmax); ++nk; }
+        if (b.nclass[3]) { sw[nk] = sweep4_launch<FOP_ASM32_64, 64>(c, b, Wmax); ++nk; }
+        if (b.nclass[4]) { sw[nk] = sweep4_launch<FOP_ASM32_32, 32>(c, b, Wmax); ++nk; }
         sw[nk] = sweep4_launch<FOP_LOSS32, 128>(c, b, Wmax); ++nk;
         /* the f64 sweeps serve the polish and the f64 rescue */
         if ((flags & (FT_FLAG_NO_POLISH | FT_FLAG_NO_RESCUE)) !=
             (FT_FLAG_NO_POLISH | FT_FLAG_NO_RESCUE)) {
             if (b.nclass[0]) { sw[nk] = sweep4_launch<FOP_ASM64, FT_ASM_T>(c, b, Wmax); ++nk; }
-            if (b.nclass[1]) { sw[nk] = sweep4_launch<FOP_ASM64_64, 64>(c, b, Wmax); ++nk; }
-            if (b.nclass[2]) { sw[nk] = sweep4_launch<FOP_ASM64_32, 32>(c, b, Wmax); ++nk; }
+            if (b.nclass[1]) { sw[nk] = sweep4_launch<FOP_ASM64_64A, 64>(c, b, Wmax); ++nk; }
+            if (b.nclass[2]) { sw[nk] = sweep4_launch<FOP_ASM64_64B, 64>(c, b, Wmax); ++nk; }
+            if (b.nclass[3]) { sw[nk] = sweep4_launch<FOP_ASM64_64, 64>(c, b, Wmax); ++nk; }
+            if (b.nclass[4]) { sw[nk] = sweep4_launch<FOP_ASM64_32, 32>(c, b, Wmax); ++nk; }
             sw[nk] = sweep4_launch<FOP_LOSS64, 128>(c, b, Wmax); ++nk;
         }
     }
@@ -2601,14 +2645,13 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
             one.outsse = a.outsse + i;
             one.outstatus = a.outstatus + i;
             /* only the assembly launches of this candidate's class */
-            SweepLaunch swc[8];
+            SweepLaunch swc[16];
             int nkc = 0;
-            const int cls = ft_class_of(b.finfo[i].z);
+            const int cls = b.finfo[i].z >> 16;
             for (int k = 0; k < nk; ++k) {
                 const int o = sw[k].opk;
-                const bool asm_cls = o == FOP_ASM32 || o == FOP_ASM64 || o == FOP_ASM32_64 ||
-                                     o == FOP_ASM32_32 || o == FOP_ASM64_64 || o == FOP_ASM64_32;
-                if (asm_cls && ft_class_of(sw[k].threads) != cls) continue;
+                const int bk = ft_base_kind(o);
+                if ((bk == FOP_ASM32 || bk == FOP_ASM64) && ft_kind_cls(o) != cls) continue;
                 swc[nkc++] = sw[k];
             }
             c->launches += enqueue_fit(c->s, c->sm_count, one, steps, swc, nkc);
@@ -2625,6 +2668,9 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
                  b.sub_slots, b.sub_maxins, xp.maxins, xp.slots, xp.tape, use64 ? 1 : 0,
                  a.ijac_small, a.ijac_tape, a.ijac_tape_small, b.asm_reg[0], b.asm_reg[1],
                  b.asm_reg[2], b.nclass[0], b.nclass[1], b.nclass[2]);
+        const size_t kl2 = strlen(key);
+        snprintf(key + kl2, sizeof(key) - kl2, "|%zu|%zu|%d|%d", b.asm_reg[3], b.asm_reg[4],
+                 b.nclass[3], b.nclass[4]);
         if (!c->fit_graph || c->fit_graph_key != key) {
             if (c->fit_graph) {
                 cudaGraphExecDestroy(c->fit_graph);
@@ -2713,14 +2759,19 @@ float rc_fit_batch_plain(void *ctx, const unsigned int *prog, const unsigned int
    of <= 16, <= 32, <= 64 and more records), the assembly region budget that
    sets each candidate's active threads (and so how many of its rows are in
    flight beside its spill slots, tape and Jacobian rows) is chosen by timing
-   the fused fit of up to `sample` of the bucket's candidates (the first
-   ones) at each budget in {24, 32, 40, 56, 80} KB: one warm-up fit, then the
-   fastest of two. The choice is kept in the context for its (N, feature
-   count) and, with a path, read from / written to that file as lines
-   "fit n v bucket budget_kb" (a bucket found there is not re-timed). The
-   budget changes a candidate's active threads and with it the order of its
-   sums: results depend on the table, never on the batch. Returns the number
-   of buckets with a budget, or -1. */
+   the fused fit of a tuning batch of the bucket's candidates at each budget
+   in {24, 32, 40, 56, 80} KB: one warm-up fit, then the fastest of two. The
+   tuning batch must fill the GPU the way the real batch does, or it would
+   favour the latency of a few candidates over throughput: it holds about
+   16,384 (candidate, tile) work items (`sample` candidates when given > 0),
+   the bucket's first candidates repeated when the bucket has fewer. A budget
+   replaces the built-in default only when it is at least 3 % faster. The
+   choice is kept in the context for its (N, feature count) and, with a path,
+   read from / written to that file as lines "fit n v bucket budget_kb" (a
+   bucket found there is not re-timed). The budget changes a candidate's
+   active threads and with it the order of its sums: results depend on the
+   table, never on the batch. Returns the number of buckets with a budget,
+   or -1. */
 int rc_fit_autotune(void *ctx, const unsigned int *prog, const unsigned int *off,
                     const int *pcount, int nprog, int kmax, const double *c0, const int *gauge,
                     int iters, int metric, int sample, const char *path)
@@ -2728,7 +2779,10 @@ int rc_fit_autotune(void *ctx, const unsigned int *prog, const unsigned int *off
     RcCtx *c = (RcCtx *)ctx;
     if (!c || !prog || !off || !pcount || !c0 || nprog <= 0 || kmax <= 0 || kmax > FT_MAX_CONST)
         return -1;
-    if (sample <= 0) sample = 64;
+    if (sample <= 0) {
+        const int ntiles = (c->n + FT_TILE_ROWS - 1) / FT_TILE_ROWS;
+        sample = std::max(16, std::min(512, (16384 + ntiles - 1) / std::max(ntiles, 1)));
+    }
     int have[4] = {0, 0, 0, 0};
     std::vector<std::string> keep;
     if (path) {
@@ -2748,14 +2802,19 @@ int rc_fit_autotune(void *ctx, const unsigned int *prog, const unsigned int *off
             }
         }
     }
-    /* the candidates of each bucket, up to `sample` */
+    /* the candidates of each bucket, up to `sample`, repeated up to it */
     std::vector<int> pick[4];
     for (int i = 0; i < nprog; ++i) {
         const int m = (int)((off[i + 1] - off[i]) / 4);
         const int b = ft_length_bucket(m);
         if ((int)pick[b].size() < sample) pick[b].push_back(i);
     }
-    static const int budgets[] = {24, 32, 40, 56, 80};
+    for (int b = 0; b < 4; ++b) {
+        const size_t have_b = pick[b].size();
+        for (size_t j = have_b; have_b > 0 && j < (size_t)sample; ++j)
+            pick[b].push_back(pick[b][j % have_b]);
+    }
+    static const int budgets[] = {40, 24, 32, 56, 80}; /* the default first */
     for (int b = 0; b < 4; ++b) {
         if (have[b] || pick[b].empty()) continue;
         const int k = (int)pick[b].size();
@@ -2775,7 +2834,7 @@ int rc_fit_autotune(void *ctx, const unsigned int *prog, const unsigned int *off
         }
         std::vector<double> oc((size_t)k * kmax), osse(k);
         std::vector<int> ost(k);
-        float best = -1.0f;
+        float best = -1.0f, base = -1.0f;
         int best_kb = 0;
         for (int kb : budgets) {
             c->fit_budget_kb[b] = kb;
@@ -2789,11 +2848,14 @@ int rc_fit_autotune(void *ctx, const unsigned int *prog, const unsigned int *off
                                         osse.data(), ost.data(), 0);
                 if (u >= 0.0f && u < t) t = u;
             }
+            if (kb == FT_ASM_BUDGET / 1024) base = t;
             if (best < 0.0f || t < best) {
                 best = t;
                 best_kb = kb;
             }
         }
+        /* keep the default unless another budget is clearly faster */
+        if (base >= 0.0f && best > 0.97f * base) best_kb = FT_ASM_BUDGET / 1024;
         c->fit_budget_kb[b] = best_kb;
         have[b] = best_kb > 0;
     }

@@ -15,12 +15,11 @@ struct FitPrep {
     std::vector<int> ninternal;       /* per candidate: records that are not leaves */
     std::vector<FIns> fins;           /* per candidate: forward list | reverse list */
     std::vector<int> fins_off;        /* [P+1] */
-    std::vector<int4> finfo;          /* forward count, reverse count, assembly threads,
-                                         spill slots | tape slots << 16 */
+    std::vector<int4> finfo;          /* forward count, reverse count, assembly threads |
+                                         launch class << 16, spill slots | tape slots << 16 */
     size_t asm_region = 0;            /* assembly shared region of the batch */
-    size_t asm_reg[3] = {256, 256, 256}; /* ... of the candidates with 128, 64, 32 active
-                                         threads */
-    int nclass[3] = {0, 0, 0};        /* candidates of each active-thread class */
+    size_t asm_reg[5] = {256, 256, 256, 256, 256}; /* ... of each assembly launch class */
+    int nclass[5] = {0, 0, 0, 0, 0};  /* candidates of each assembly launch class */
     int mmax = 1;                     /* most records */
     int pmax = 0;                     /* most constants */
     int fslots = 1;                   /* most spill slots */

@@ -404,9 +404,10 @@ class GpuEvaluator:
             raise DeviceError("rc_launch_count failed")
         return int(out[0])
 
-    def fit_autotune(self, plans, iters=20, metric=LOSS_SQUARED, sample=64, path=None):
+    def fit_autotune(self, plans, iters=20, metric=LOSS_SQUARED, sample=0, path=None):
         """Tune the fit's assembly budget per length bucket on these plans
-        (rc_fit_autotune); returns the budgets in KB per bucket."""
+        (rc_fit_autotune; sample 0: a GPU-filling tuning batch); returns the
+        budgets in KB per bucket."""
         from .host import pack_plans
         prog, off, pcount, c0, gauge, kmax = pack_plans(plans)
         prog, off = _c(prog, np.uint32), _c(off, np.uint32)
