@@ -562,7 +562,8 @@ def bench_fit(args, rank, world, dev, pkg, W, flushbuf, steps=None, warmup=None,
     steps = args.steps if steps is None else steps
     warmup = args.warmup if warmup is None else warmup
     ev, plans, trees, x, y, metric, what = fit_setup(pkg, W, "c3", P, N, rank)
-    out = time_fit(pkg, ev, plans, metric, N, steps, warmup, flushbuf, 64 if plain else 0, rank)
+    out = time_fit(pkg, ev, plans, metric, N, steps, warmup, flushbuf, 64 if plain else 0, rank,
+                   tune=not args.no_tune)
     threads = os.cpu_count() or 1
     if classify:
         fit_reference_mode(pkg, ev, plans, metric, trees, x, y, out, threads)
@@ -718,7 +719,8 @@ def bench_c5(args, rank, pkg, W, flushbuf, steps, warmup, fit_steps, fit_warmup)
     P = args.P if args.workload == "c5" and args.P else 1000
     N = args.N if args.workload == "c5" and args.N else 1 << 22
     ev, plans, trees, x, y, metric, what = fit_setup(pkg, W, "c5", P, N, rank)
-    fit = time_fit(pkg, ev, plans, metric, N, fit_steps, fit_warmup, flushbuf, 16, rank)
+    fit = time_fit(pkg, ev, plans, metric, N, fit_steps, fit_warmup, flushbuf, 16, rank,
+                   tune=not args.no_tune)
     rk = rank_stage(pkg, ev, plans, N, flushbuf, steps, warmup)
     rk["config"] = (f"exact rank-correlation sums, P={P} candidates x 1 trial, N={N} rows x "
                     f"10 heavy-tailed features")
@@ -1010,6 +1012,8 @@ def main():
     ap.add_argument("--P", type=int, default=0)
     ap.add_argument("--N", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="fit with the built-in assembly budgets instead of tuning them first")
     ap.add_argument("--no-secondary", action="store_true",
                     help="skip the fit, implicit and heavy-tailed measurements of the "
                          "default line")

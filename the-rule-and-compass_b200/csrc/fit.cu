@@ -61,25 +61,28 @@ enum {
        sweeps run in blocks of the class's threads, sized for the class */
     FOP_ASM32_64 = 10, FOP_ASM32_32 = 11, FOP_ASM64_64 = 12, FOP_ASM64_32 = 13,
     FOP_ASM32_64A = 14, FOP_ASM32_64B = 15, FOP_ASM64_64A = 16, FOP_ASM64_64B = 17,
-    FOP_COUNT = 18
+    FOP_ASM32_128L = 18, FOP_ASM64_128L = 19,
+    FOP_COUNT = 20
 };
 
 /* Launch classes of the assemblies. A candidate's active threads A and its
-   shared region decide it: 0: A = 128; 1, 2, 3: A = 64 with a region of at
-   most 21 KB, at most 30 KB, or more; 4: A = 32. A class's launch uses
-   blocks of A threads and the largest region of its candidates, so the
-   small-region classes fit more blocks on an SM (10, 7 and 5 of 64 threads
-   at 21, 30 and 40 KB). Which launch runs a candidate does not change its
-   arithmetic (that depends on A alone). */
-#define FT_NCLS 5
+   shared region decide it: 0: A = 128 with a region of at most 41 KB; 5:
+   A = 128 with a larger one (a length bucket the autotuner gave a bigger
+   budget); 1, 2, 3: A = 64 with a region of at most 21 KB, at most 30 KB, or
+   more; 4: A = 32. A class's launch uses blocks of A threads and the largest
+   region of its candidates, so the small-region classes fit more blocks on
+   an SM (10, 7 and 5 of 64 threads at 21, 30 and 40 KB), and a large region
+   never shrinks the launch of the others. Which launch runs a candidate does
+   not change its arithmetic (that depends on A alone). */
+#define FT_NCLS 6
 __host__ __device__ constexpr int ft_cls_threads(int cls)
 {
-    return cls == 0 ? 128 : (cls == 4 ? 32 : 64);
+    return (cls == 0 || cls == 5) ? 128 : (cls == 4 ? 32 : 64);
 }
 
 inline int ft_cls_of(int A, size_t region)
 {
-    if (A >= 128) return 0;
+    if (A >= 128) return region <= 41 * 1024 ? 0 : 5;
     if (A <= 32) return 4;
     return region <= 21 * 1024 ? 1 : (region <= 30 * 1024 ? 2 : 3);
 }
@@ -87,10 +90,11 @@ inline int ft_cls_of(int A, size_t region)
 /* The kind a queue's sweep performs (a class queue performs its base kind). */
 __host__ __device__ constexpr int ft_base_kind(int k)
 {
-    return (k == FOP_ASM32_64 || k == FOP_ASM32_32 || k == FOP_ASM32_64A || k == FOP_ASM32_64B)
+    return (k == FOP_ASM32_64 || k == FOP_ASM32_32 || k == FOP_ASM32_64A || k == FOP_ASM32_64B ||
+            k == FOP_ASM32_128L)
                ? FOP_ASM32
            : (k == FOP_ASM64_64 || k == FOP_ASM64_32 || k == FOP_ASM64_64A ||
-              k == FOP_ASM64_64B)
+              k == FOP_ASM64_64B || k == FOP_ASM64_128L)
                ? FOP_ASM64
                : k;
 }
@@ -102,6 +106,7 @@ __host__ __device__ constexpr int ft_kind_cls(int k)
            : (k == FOP_ASM32_64B || k == FOP_ASM64_64B) ? 2
            : (k == FOP_ASM32_64 || k == FOP_ASM64_64)   ? 3
            : (k == FOP_ASM32_32 || k == FOP_ASM64_32)   ? 4
+           : (k == FOP_ASM32_128L || k == FOP_ASM64_128L) ? 5
                                                         : 0;
 }
 
@@ -110,9 +115,9 @@ __host__ __device__ constexpr int ft_kind_cls(int k)
 __host__ __device__ inline int ft_queue_kind(int op, int cls)
 {
     static constexpr int k32[FT_NCLS] = {FOP_ASM32, FOP_ASM32_64A, FOP_ASM32_64B, FOP_ASM32_64,
-                                         FOP_ASM32_32};
+                                         FOP_ASM32_32, FOP_ASM32_128L};
     static constexpr int k64[FT_NCLS] = {FOP_ASM64, FOP_ASM64_64A, FOP_ASM64_64B, FOP_ASM64_64,
-                                         FOP_ASM64_32};
+                                         FOP_ASM64_32, FOP_ASM64_128L};
     if (op == FOP_ASM32) return k32[cls];
     if (op == FOP_ASM64) return k64[cls];
     return op;
@@ -215,7 +220,7 @@ struct FitArgs {
     int ftape;             /* partial-tape slots needed by the batch */
     int fmaxins;           /* longest forward + reverse list */
     size_t asm_region;     /* assembly region of a 128-thread launch over every class */
-    size_t asm_reg[5];     /* assembly region of each launch class (ft_cls_of) */
+    size_t asm_reg[6];     /* assembly region of each launch class (ft_cls_of) */
     const int2 *fcinfo;    /* [P] cached forward count (after the reverse list),
                               first cache column */
     float *cache;          /* [columns][npad] values of constant-free subtrees */
@@ -2602,6 +2607,7 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
         if (b.nclass[2]) { sw[nk] = sweep4_launch<FOP_ASM32_64B, 64>(c, b, Wmax); ++nk; }
         if (b.nclass[3]) { sw[nk] = sweep4_launch<FOP_ASM32_64, 64>(c, b, Wmax); ++nk; }
         if (b.nclass[4]) { sw[nk] = sweep4_launch<FOP_ASM32_32, 32>(c, b, Wmax); ++nk; }
+        if (b.nclass[5]) { sw[nk] = sweep4_launch<FOP_ASM32_128L, 128>(c, b, Wmax); ++nk; }
         sw[nk] = sweep4_launch<FOP_LOSS32, 128>(c, b, Wmax); ++nk;
         /* the f64 sweeps serve the polish and the f64 rescue */
         if ((flags & (FT_FLAG_NO_POLISH | FT_FLAG_NO_RESCUE)) !=
@@ -2611,6 +2617,7 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
             if (b.nclass[2]) { sw[nk] = sweep4_launch<FOP_ASM64_64B, 64>(c, b, Wmax); ++nk; }
             if (b.nclass[3]) { sw[nk] = sweep4_launch<FOP_ASM64_64, 64>(c, b, Wmax); ++nk; }
             if (b.nclass[4]) { sw[nk] = sweep4_launch<FOP_ASM64_32, 32>(c, b, Wmax); ++nk; }
+            if (b.nclass[5]) { sw[nk] = sweep4_launch<FOP_ASM64_128L, 128>(c, b, Wmax); ++nk; }
             sw[nk] = sweep4_launch<FOP_LOSS64, 128>(c, b, Wmax); ++nk;
         }
     }
@@ -2658,7 +2665,7 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
             ok = cudaGetLastError() == cudaSuccess;
         }
     } else {
-        char key[512];
+        char key[1024];
         snprintf(key, sizeof(key), "%p|%d|%d|%d|%d|%d|%d|%d|%d|%d|%zu|%d|%d|%d|%zu", (void *)dev,
                  nprog, kmax, ntiles, b.mmax, Wmax, iters, metric, flags, steps, io_end, b.fslots,
                  b.ftape, b.fmaxins, b.asm_region);
@@ -2669,8 +2676,8 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
                  a.ijac_small, a.ijac_tape, a.ijac_tape_small, b.asm_reg[0], b.asm_reg[1],
                  b.asm_reg[2], b.nclass[0], b.nclass[1], b.nclass[2]);
         const size_t kl2 = strlen(key);
-        snprintf(key + kl2, sizeof(key) - kl2, "|%zu|%zu|%d|%d", b.asm_reg[3], b.asm_reg[4],
-                 b.nclass[3], b.nclass[4]);
+        snprintf(key + kl2, sizeof(key) - kl2, "|%zu|%zu|%zu|%d|%d|%d", b.asm_reg[3],
+                 b.asm_reg[4], b.asm_reg[5], b.nclass[3], b.nclass[4], b.nclass[5]);
         if (!c->fit_graph || c->fit_graph_key != key) {
             if (c->fit_graph) {
                 cudaGraphExecDestroy(c->fit_graph);

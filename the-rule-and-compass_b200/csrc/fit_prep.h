@@ -18,8 +18,8 @@ struct FitPrep {
     std::vector<int4> finfo;          /* forward count, reverse count, assembly threads |
                                          launch class << 16, spill slots | tape slots << 16 */
     size_t asm_region = 0;            /* assembly shared region of the batch */
-    size_t asm_reg[5] = {256, 256, 256, 256, 256}; /* ... of each assembly launch class */
-    int nclass[5] = {0, 0, 0, 0, 0};  /* candidates of each assembly launch class */
+    size_t asm_reg[6] = {256, 256, 256, 256, 256, 256}; /* ... of each assembly launch class */
+    int nclass[6] = {0, 0, 0, 0, 0, 0}; /* candidates of each assembly launch class */
     int mmax = 1;                     /* most records */
     int pmax = 0;                     /* most constants */
     int fslots = 1;                   /* most spill slots */
