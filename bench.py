@@ -455,9 +455,10 @@ def time_fit(pkg, ev, plans, metric, N, steps, warmup, flushbuf, plain_n, seed, 
     device and end to end; then the plain one-candidate-per-launch form on a
     seeded random sample of the same candidates (its cost is linear in the
     candidate count), whose losses must equal the fused ones bit for bit.
-    Before timing (and outside it), the library's fit autotuner chooses the
-    assembly budget per length bucket on this batch (`rc_fit_autotune`); both
-    arms then run with the chosen table."""
+    With `tune`, before timing (and outside it), the library's fit autotuner
+    chooses the assembly budget per length bucket on this batch
+    (`rc_fit_autotune`, which keeps the built-in budgets unless the whole
+    batch is faster with its choice); both arms then run with that table."""
     import torch
     iters = 20
     P = len(plans)
@@ -556,14 +557,14 @@ def fit_reference_mode(pkg, ev, plans, metric, trees, x, y, r, threads):
 
 
 def bench_fit(args, rank, world, dev, pkg, W, flushbuf, steps=None, warmup=None, plain=True,
-              N=None, classify=False, cpu=False):
+              N=None, classify=False, cpu=False, tune=True):
     P = args.P if args.workload == "fit" and args.P else 2048
     N = N or (args.N if args.workload == "fit" and args.N else 262144)
     steps = args.steps if steps is None else steps
     warmup = args.warmup if warmup is None else warmup
     ev, plans, trees, x, y, metric, what = fit_setup(pkg, W, "c3", P, N, rank)
     out = time_fit(pkg, ev, plans, metric, N, steps, warmup, flushbuf, 64 if plain else 0, rank,
-                   tune=not args.no_tune)
+                   tune=tune and not args.no_tune)
     threads = os.cpu_count() or 1
     if classify:
         fit_reference_mode(pkg, ev, plans, metric, trees, x, y, out, threads)
@@ -719,8 +720,9 @@ def bench_c5(args, rank, pkg, W, flushbuf, steps, warmup, fit_steps, fit_warmup)
     P = args.P if args.workload == "c5" and args.P else 1000
     N = args.N if args.workload == "c5" and args.N else 1 << 22
     ev, plans, trees, x, y, metric, what = fit_setup(pkg, W, "c5", P, N, rank)
+    # tuning at 4M rows takes minutes of whole-batch checks: built-in budgets here
     fit = time_fit(pkg, ev, plans, metric, N, fit_steps, fit_warmup, flushbuf, 16, rank,
-                   tune=not args.no_tune)
+                   tune=False)
     rk = rank_stage(pkg, ev, plans, N, flushbuf, steps, warmup)
     rk["config"] = (f"exact rank-correlation sums, P={P} candidates x 1 trial, N={N} rows x "
                     f"10 heavy-tailed features")
@@ -945,7 +947,7 @@ def secondary(args, rank, world, local, pkg, W, flushbuf, peaks, line):
                 fit_f32_only_failures=cls.get("rescue_on", {}).get("f32_only"),
                 fit_f32_only_failures_reference_mode=cls.get("reference_mode", {}).get("f32_only"))
     f = bench_fit(args, rank, world, local, pkg, W, flushbuf, steps=2, warmup=3, N=1 << 20,
-                  cpu=True)
+                  cpu=True, tune=False)
     fs = line["fit_1m"] = fit_summary(f, peaks, f["what"])
     line.update(fit_1m_fused=fs["value"], fit_1m_fused_e2e=fs["e2e"],
                 fit_1m_plain=fs["plain"]["value"], fused_over_plain_1m=fs["fused_over_plain"],

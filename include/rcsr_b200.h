@@ -219,7 +219,9 @@ float rc_fit_batch_plain(void *ctx, const unsigned int *prog, const unsigned int
    candidates, or with sample <= 0 as many as make about 16,384 (candidate,
    tile) work items, so that the tuning batch fills the GPU like a real one;
    the bucket's first candidates repeated when it has fewer); a budget
-   replaces the default only when at least 3 % faster. Kept in the context
+   replaces the default only when at least 3 % faster, and the new table
+   only when the caller's whole batch fits at least 3 % faster with it than
+   with the defaults. Kept in the context
    for its (N, feature count) and, with a path, cached in that text file
    ("fit n v bucket budget_kb" lines; a cached bucket is not re-timed). The other arguments are rc_fit_batch_fused's. Returns the
    number of buckets with a budget, or -1. No counterpart in the reference

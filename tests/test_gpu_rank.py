@@ -77,6 +77,31 @@ def test_rank_sums_are_bit_identical(pkg, E, O, n):
     ev.close()
 
 
+@pytest.mark.parametrize("n", [500, 5000])
+def test_rank_sums_resolve_runs_of_equal_upper_key_halves(pkg, E, O, n):
+    """The rank sums sort by the upper 32 key bits and resolve each run of
+    equal upper halves by the lower halves (a run longer than 64 keys is
+    sorted in full instead). Integer x0 plus a 1e-9 x1 perturbation puts
+    about n / 13 keys with distinct lower halves in each run: both ways at
+    n = 500 (the clustered model's runs are short), all at n = 5000, mixed in
+    one batch with models that need neither."""
+    cols, y = _fixture(n, seed=17)
+    ev = _evaluator(pkg, cols, y)
+    clustered = E.node(E.ADD, [E.node(E.MUL, [E.constant(0.5), E.input(0)]),
+                               E.node(E.MUL, [E.constant(1e-9), E.input(1)])])
+    near = E.node(E.ADD, [E.constant(1.0), E.node(E.MUL, [E.constant(1e-12), E.input(2)])])
+    models = _models(E)
+    trees = [models["linear"], clustered, near, models["tied"]]
+    plans, prog, off, pcount, c0, kmax = _pack(pkg, trees)
+    sums, status, bb, _ = ev.rank_sums(prog, off, pcount, c0, kmax)
+    for k, t in enumerate(trees):
+        ab, aa, bb_cpu = O.rank_sums(_oracle_pred(O, t, cols), y)
+        assert status[k] == 0
+        assert sums[k] == (ab, aa), (k, sums[k], (ab, aa))
+        assert bb == bb_cpu
+    ev.close()
+
+
 def test_rank_sums_of_random_models_and_trials(pkg, E, O):
     W = importlib.import_module("the-rule-and-compass_b200.workloads")
     trees, x, _ = W.fit_workload(24, 9000, seed=3, nvars=3)

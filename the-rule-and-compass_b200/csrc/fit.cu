@@ -2772,7 +2772,9 @@ float rc_fit_batch_plain(void *ctx, const unsigned int *prog, const unsigned int
    favour the latency of a few candidates over throughput: it holds about
    16,384 (candidate, tile) work items (`sample` candidates when given > 0),
    the bucket's first candidates repeated when the bucket has fewer. A budget
-   replaces the built-in default only when it is at least 3 % faster. The
+   replaces the built-in default only when it is at least 3 % faster, and
+   the new table as a whole only when the caller's whole batch is at least
+   3 % faster with it than with the defaults. The
    choice is kept in the context for its (N, feature count) and, with a path,
    read from / written to that file as lines "fit n v bucket budget_kb" (a
    bucket found there is not re-timed). The budget changes a candidate's
@@ -2822,6 +2824,7 @@ int rc_fit_autotune(void *ctx, const unsigned int *prog, const unsigned int *off
             pick[b].push_back(pick[b][j % have_b]);
     }
     static const int budgets[] = {40, 24, 32, 56, 80}; /* the default first */
+    bool tuned[4] = {false, false, false, false};
     for (int b = 0; b < 4; ++b) {
         if (have[b] || pick[b].empty()) continue;
         const int k = (int)pick[b].size();
@@ -2864,8 +2867,34 @@ int rc_fit_autotune(void *ctx, const unsigned int *prog, const unsigned int *off
         /* keep the default unless another budget is clearly faster */
         if (base >= 0.0f && best > 0.97f * base) best_kb = FT_ASM_BUDGET / 1024;
         c->fit_budget_kb[b] = best_kb;
-        have[b] = best_kb > 0;
+        tuned[b] = best_kb != FT_ASM_BUDGET / 1024;
     }
+    /* A bucket's budget also changes the launches the other buckets share,
+       which the per-bucket timing cannot see: the caller's whole batch is
+       timed with the new table and with the default one, and the new
+       choices are kept only when the whole batch is at least 3 % faster. */
+    if (tuned[0] || tuned[1] || tuned[2] || tuned[3]) {
+        std::vector<double> oc((size_t)nprog * kmax), osse(nprog);
+        std::vector<int> ost(nprog);
+        auto whole = [&]() {
+            float t = -1.0f;
+            for (int r = 0; r < 3; ++r) {
+                const float u = fit_run(c, prog, off, pcount, nprog, kmax, c0, gauge, iters,
+                                        metric, 0, oc.data(), osse.data(), ost.data(), 0);
+                if (r > 0 && u >= 0.0f && (t < 0.0f || u < t)) t = u;
+            }
+            return t;
+        };
+        int table[4];
+        for (int b = 0; b < 4; ++b) table[b] = c->fit_budget_kb[b];
+        const float t_new = whole();
+        for (int b = 0; b < 4; ++b)
+            if (tuned[b]) c->fit_budget_kb[b] = FT_ASM_BUDGET / 1024;
+        const float t_def = whole();
+        if (t_new >= 0.0f && t_def >= 0.0f && t_new <= 0.97f * t_def)
+            for (int b = 0; b < 4; ++b) c->fit_budget_kb[b] = table[b];
+    }
+    for (int b = 0; b < 4; ++b) have[b] = have[b] || c->fit_budget_kb[b] > 0;
     if (path) {
         std::ofstream out(path, std::ios::trunc);
         for (const auto &l : keep) out << l << "\n";
