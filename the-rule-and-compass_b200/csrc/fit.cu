@@ -2678,31 +2678,42 @@ float fit_run(RcCtx *c, const unsigned int *prog, const unsigned int *off, const
         const size_t kl2 = strlen(key);
         snprintf(key + kl2, sizeof(key) - kl2, "|%zu|%zu|%zu|%d|%d|%d", b.asm_reg[3],
                  b.asm_reg[4], b.asm_reg[5], b.nclass[3], b.nclass[4], b.nclass[5]);
-        if (!c->fit_graph || c->fit_graph_key != key) {
-            if (c->fit_graph) {
-                cudaGraphExecDestroy(c->fit_graph);
-                c->fit_graph = nullptr;
+        const bool replay = c->fit_graph && c->fit_graph_key == key;
+        if (!replay && c->fit_seen_key != key) {
+            /* a batch shape seen for the first time runs its steps directly:
+               a generation loop rarely repeats one, and capturing and
+               instantiating the graph costs more than launching it once.
+               The second call of a shape captures it, later ones replay. */
+            c->fit_seen_key = key;
+            c->launches += enqueue_fit(c->s, c->sm_count, a, steps, sw, nk);
+            ok = cudaGetLastError() == cudaSuccess;
+        } else {
+            if (!replay) {
+                if (c->fit_graph) {
+                    cudaGraphExecDestroy(c->fit_graph);
+                    c->fit_graph = nullptr;
+                }
+                cudaGraph_t g = nullptr;
+                cudaStream_t cap = nullptr;
+                cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
+                ok = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+                if (ok) {
+                    c->fit_graph_kernels = enqueue_fit(cap, c->sm_count, a, steps, sw, nk);
+                    ok = cudaStreamEndCapture(cap, &g) == cudaSuccess && g;
+                }
+                if (ok) ok = cudaGraphInstantiate(&c->fit_graph, g, 0) == cudaSuccess;
+                if (g) cudaGraphDestroy(g);
+                cudaStreamDestroy(cap);
+                if (!ok) {
+                    cudaGetLastError();
+                    c->fit_graph = nullptr;
+                } else {
+                    c->fit_graph_key = key;
+                }
             }
-            cudaGraph_t g = nullptr;
-            cudaStream_t cap = nullptr;
-            cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
-            ok = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
-            if (ok) {
-                c->fit_graph_kernels = enqueue_fit(cap, c->sm_count, a, steps, sw, nk);
-                ok = cudaStreamEndCapture(cap, &g) == cudaSuccess && g;
-            }
-            if (ok) ok = cudaGraphInstantiate(&c->fit_graph, g, 0) == cudaSuccess;
-            if (g) cudaGraphDestroy(g);
-            cudaStreamDestroy(cap);
-            if (!ok) {
-                cudaGetLastError();
-                c->fit_graph = nullptr;
-            } else {
-                c->fit_graph_key = key;
-            }
+            if (ok) ok = cudaGraphLaunch(c->fit_graph, c->s) == cudaSuccess;
+            if (ok) c->launches += c->fit_graph_kernels;
         }
-        if (ok) ok = cudaGraphLaunch(c->fit_graph, c->s) == cudaSuccess;
-        if (ok) c->launches += c->fit_graph_kernels;
     }
     cudaEventRecord(c->t1, c->s);
     st->launch_ms += rc_now_ms() - t;

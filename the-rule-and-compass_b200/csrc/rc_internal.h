@@ -132,6 +132,7 @@ struct RcCtx {
     /* cached CUDA graph of the fused fit for a repeated batch shape */
     cudaGraphExec_t fit_graph;
     std::string fit_graph_key;
+    std::string fit_seen_key;             /* the last batch shape run without a graph */
     unsigned long long fit_graph_kernels; /* kernel nodes in one replay */
 
     /* kernels this context has launched (graph replays count their nodes) */
