@@ -78,13 +78,13 @@ def test_rank_sums_are_bit_identical(pkg, E, O, n):
 
 
 @pytest.mark.parametrize("n", [500, 5000])
-def test_rank_sums_resolve_runs_of_equal_upper_key_halves(pkg, E, O, n):
-    """The rank sums sort by the upper 32 key bits and resolve each run of
-    equal upper halves by the lower halves (a run longer than 64 keys is
-    sorted in full instead). Integer x0 plus a 1e-9 x1 perturbation puts
-    about n / 13 keys with distinct lower halves in each run: both ways at
-    n = 500 (the clustered model's runs are short), all at n = 5000, mixed in
-    one batch with models that need neither."""
+def test_rank_sums_of_keys_that_agree_in_their_upper_halves(pkg, E, O, n):
+    """Predictions whose f64 bit patterns share their upper 32 bits in long
+    groups and differ below: integer x0 plus a 1e-9 x1 perturbation puts
+    about n / 13 distinct keys in each group, and 1 + 1e-12 x2 puts all of
+    them in one; the lower digit passes alone order them. Mixed in one batch
+    with models whose keys spread over every digit, the sums must equal the
+    CPU's exactly."""
     cols, y = _fixture(n, seed=17)
     ev = _evaluator(pkg, cols, y)
     clustered = E.node(E.ADD, [E.node(E.MUL, [E.constant(0.5), E.input(0)]),

@@ -73,7 +73,6 @@ __global__ void __launch_bounds__(RK_T) rk_keys(const FIns *fins, const int *fin
                                                 int seg0, int tiles, int maxins, u64 *keys,
                                                 unsigned int *rows, int *status)
 {
-    /* (the segments of a launch are seg0 + blockIdx.x / tiles) */
     using V4 = FiV<double, 2>::V4;
     extern __shared__ __align__(16) unsigned char sm[];
     FIns *ins = reinterpret_cast<FIns *>(sm);
@@ -236,7 +235,7 @@ __global__ void __launch_bounds__(RS_T) rs_count(const u64 *keys, int n, int nbl
 /* Per segment: digit counts -> first output positions (in place), the mask
    of skipped passes, and the buffer that holds the sorted keys. */
 __global__ void __launch_bounds__(256) rs_prep(unsigned int *count, int n, unsigned char *skip,
-                                               unsigned char *par, unsigned lowmask)
+                                               unsigned char *par)
 {
     __shared__ unsigned int wsum[8];
     const int seg = blockIdx.x, d = threadIdx.x, lane = d & 31, w = d >> 5;
@@ -258,7 +257,6 @@ __global__ void __launch_bounds__(256) rs_prep(unsigned int *count, int n, unsig
         if (all) mask |= 1u << pass;
         __syncthreads();
     }
-    mask |= lowmask;
     if (d == 0) {
         skip[seg] = (unsigned char)mask;
         par[seg] = (unsigned char)(__popc(~mask & 0xffu) & 1);
@@ -449,8 +447,7 @@ struct RsBuffers {
    kernels launched. A look-back that gave up, or a position out of range,
    sets *abort_flag (which the caller zeroes once and checks after). */
 template <bool VALS>
-unsigned long long rs_sort(const RsBuffers &b, int nseg, int n, int *abort_flag, cudaStream_t s,
-                           int first_pass = 0)
+unsigned long long rs_sort(const RsBuffers &b, int nseg, int n, int *abort_flag, cudaStream_t s)
 {
     const int ntiles = (n + RS_TILE - 1) / RS_TILE;
     const int nblk = (ntiles + RS_COUNT_TILES - 1) / RS_COUNT_TILES;
@@ -460,13 +457,13 @@ unsigned long long rs_sort(const RsBuffers &b, int nseg, int n, int *abort_flag,
     cudaMemsetAsync(b.state, 0, sizeof(u64) * 256 * (size_t)ntiles * (size_t)nseg, s);
     cudaMemsetAsync(b.ticket, 0, sizeof(int) * RS_PASSES, s);
     rs_count<<<(unsigned)nseg * (unsigned)nblk, RS_T, 0, s>>>(b.ka, n, nblk, b.count);
-    rs_prep<<<nseg, 256, 0, s>>>(b.count, n, b.skip, b.par, (1u << first_pass) - 1u);
+    rs_prep<<<nseg, 256, 0, s>>>(b.count, n, b.skip, b.par);
     const unsigned grid = (unsigned)nseg * (unsigned)ntiles;
-    for (int pass = first_pass; pass < RS_PASSES; ++pass)
+    for (int pass = 0; pass < RS_PASSES; ++pass)
         rs_pass<VALS><<<grid, RS_T, rs_pass_smem<VALS>(), s>>>(
             b.ka, b.kb, b.va, b.vb, b.skip, b.count, b.state, b.ticket, abort_flag, n, ntiles,
             pass);
-    return 2 + RS_PASSES - first_pass;
+    return 2 + RS_PASSES;
 }
 
 /* ---- runs and exact sums ----------------------------------------------- */
@@ -511,68 +508,47 @@ __device__ __forceinline__ int rk_excl_min_right(int v, int *sh)
     return min(after, ex);
 }
 
+/* First index in [lo, hi) whose key is >= k (keys sorted). */
+__device__ int rk_lower(const u64 *keys, int lo, int hi, u64 k)
+{
+    while (lo < hi) {
+        const int mid = lo + ((hi - lo) >> 1);
+        if (keys[mid] < k) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+/* First index in [lo, hi) whose key is > k (keys sorted), or hi. */
+__device__ int rk_upper(const u64 *keys, int lo, int hi, u64 k)
+{
+    while (lo < hi) {
+        const int mid = lo + ((hi - lo) >> 1);
+        if (keys[mid] <= k) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
 enum { RK_SUMS = 0, RK_FILL = 1 };
 
-/* Longest run of equal upper key halves resolved in the half-sorted form;
-   a segment with a longer one is sorted in full instead. */
-#define RK_RUN_MAX 64
-
-/* The part of a key the run scan compares: all of it, or (HI) the upper 32
-   bits the half sort ordered by. */
-template <bool HI>
-__device__ __forceinline__ u64 rk_part(u64 k) { return HI ? (k >> 32) : k; }
-
-/* First index in [lo, hi) whose key part is >= k, and first whose part is
-   > k (parts sorted). */
-template <bool HI>
-__device__ int rk_lower_part(const u64 *keys, int lo, int hi, u64 k)
-{
-    while (lo < hi) {
-        const int mid = lo + ((hi - lo) >> 1);
-        if (rk_part<HI>(keys[mid]) < k) lo = mid + 1;
-        else hi = mid;
-    }
-    return lo;
-}
-
-template <bool HI>
-__device__ int rk_upper_part(const u64 *keys, int lo, int hi, u64 k)
-{
-    while (lo < hi) {
-        const int mid = lo + ((hi - lo) >> 1);
-        if (rk_part<HI>(keys[mid]) <= k) lo = mid + 1;
-        else hi = mid;
-    }
-    return lo;
-}
-
-/* One tile of a sorted segment: every position's run [i, j) of equal keys
-   (block scans of the run starts inside the tile; a binary search for a run
-   that crosses the tile's edge), A = i + j - n, and the tile's exact partial
-   sums. RK_SUMS: part = (sum A * B[row], sum A^2). RK_FILL (the target):
-   B[row] = A and part = (0, sum A^2).
-
-   HI: the segment is sorted by the upper 32 key bits only (the four upper
-   digit passes; the lower ones are not run). A run of equal upper halves
-   [s, e) then holds, in some order, exactly the keys that a full sort puts
-   at [s, e), so a key's run of equal full keys is
-   [s + #{lower half < its}, s + #{lower half <= its}), counted over the run:
-   the same A as the full sort gives. A run longer than RK_RUN_MAX marks the
-   segment in `longrun` (its sums are then redone with the full sort).
-   With `only`, segments it does not mark are skipped. */
-template <int MODE, bool HI>
+/* One tile of a sorted segment: every position's run [i, j) (block scans
+   of the run starts inside the tile; a binary search for a run that crosses
+   the tile's edge), A = i + j - n, and the tile's exact partial sums.
+   RK_SUMS: part = (sum A * B[row], sum A^2). RK_FILL (the target): B[row] = A
+   and part = (0, sum A^2). */
+template <int MODE>
 __global__ void __launch_bounds__(RS_T) rk_runs(const u64 *ka, const u64 *kb,
                                                 const unsigned int *va, const unsigned int *vb,
                                                 const unsigned char *par, int n, int ntiles,
                                                 const long long *B, long long *Bout,
-                                                __int128 *part, int *longrun, const int *only)
+                                                __int128 *part)
 {
     __shared__ int sh[RS_WARPS];
     __shared__ int s_left, s_right;
     __shared__ __int128 red[RS_T];
     const int seg = blockIdx.x / ntiles, tile = blockIdx.x % ntiles;
     const int tid = threadIdx.x;
-    if (only && !only[seg]) return;
     const size_t sb = (size_t)seg * n;
     const bool p = par[seg] != 0;
     const u64 *keys = (p ? kb : ka) + sb;
@@ -581,16 +557,15 @@ __global__ void __launch_bounds__(RS_T) rk_runs(const u64 *ka, const u64 *kb,
     const int q0 = t0 + tid * RS_ITEMS;
     u64 k[RS_ITEMS];
     bool f[RS_ITEMS];
-    u64 prev = (q0 > 0 && q0 < t1) ? rk_part<HI>(keys[q0 - 1]) : 0ULL;
+    u64 prev = (q0 > 0 && q0 < t1) ? keys[q0 - 1] : 0ULL;
     int last = -1, first = 0x7fffffff;
 #pragma unroll
     for (int j = 0; j < RS_ITEMS; ++j) {
         const int q = q0 + j;
         const bool in = q < t1;
         k[j] = in ? keys[q] : 0ULL;
-        const u64 kp = rk_part<HI>(k[j]);
-        f[j] = in && (q == 0 || kp != prev);
-        prev = kp;
+        f[j] = in && (q == 0 || k[j] != prev);
+        prev = k[j];
         if (f[j]) {
             last = q;
             first = min(first, q);
@@ -599,11 +574,9 @@ __global__ void __launch_bounds__(RS_T) rk_runs(const u64 *ka, const u64 *kb,
     if (tid == 0) {
         /* the run holding the tile's first position may start earlier; the
            one holding its last position may end later */
-        const u64 kf = rk_part<HI>(keys[t0]), kl = rk_part<HI>(keys[t1 - 1]);
-        s_left = (t0 > 0 && rk_part<HI>(keys[t0 - 1]) == kf) ? rk_lower_part<HI>(keys, 0, t0, kf)
-                                                             : t0;
-        s_right = (t1 < n && rk_part<HI>(keys[t1]) == kl) ? rk_upper_part<HI>(keys, t1, n, kl)
-                                                          : t1;
+        const u64 kf = keys[t0], kl = keys[t1 - 1];
+        s_left = (t0 > 0 && keys[t0 - 1] == kf) ? rk_lower(keys, 0, t0, kf) : t0;
+        s_right = (t1 < n && keys[t1] == kl) ? rk_upper(keys, t1, n, kl) : t1;
     }
     const int ex_start = rk_excl_max(last, sh);
     const int ex_end = rk_excl_min_right(first, sh);
@@ -619,28 +592,11 @@ __global__ void __launch_bounds__(RS_T) rk_runs(const u64 *ka, const u64 *kb,
         }
     }
     __int128 ab = 0, aa = 0;
-    bool too_long = false;
 #pragma unroll
     for (int j = RS_ITEMS - 1; j >= 0; --j) {
         const int q = q0 + j;
         if (q < t1) {
-            long long i0 = st[j], j0 = end;
-            if (HI && end - st[j] > 1) {
-                if (end - st[j] > RK_RUN_MAX) {
-                    too_long = true;
-                } else {
-                    const unsigned int lo = (unsigned int)k[j];
-                    int lt = 0, le = 0;
-                    for (int r = st[j]; r < end; ++r) {
-                        const unsigned int o = (unsigned int)keys[r];
-                        lt += o < lo;
-                        le += o <= lo;
-                    }
-                    i0 = st[j] + lt;
-                    j0 = st[j] + le;
-                }
-            }
-            const long long A = i0 + j0 - (long long)n;
+            const long long A = (long long)st[j] + (long long)end - (long long)n;
             const unsigned int row = vals[q];
             aa += (__int128)A * A;
             if (MODE == RK_SUMS) ab += (__int128)A * B[row];
@@ -648,7 +604,6 @@ __global__ void __launch_bounds__(RS_T) rk_runs(const u64 *ka, const u64 *kb,
             if (f[j]) end = q;
         }
     }
-    if (HI && too_long) atomicOr(longrun + seg, 1);
     /* fixed-order block sums (integers: exact in any order) */
     red[tid] = ab;
     __syncthreads();
@@ -900,9 +855,8 @@ int rk_prepare(RcCtx *c)
     const int ntiles = (n + RS_TILE - 1) / RS_TILE;
     rk_target_keys<<<(n + 255) / 256, 256, 0, c->s>>>(c->d_y64, n, b.ka, b.va);
     c->launches += 3 + rs_sort<true>(b, 1, n, d_abort, c->s);
-    rk_runs<RK_FILL, false><<<ntiles, RS_T, 0, c->s>>>(b.ka, b.kb, b.va, b.vb, b.par, n, ntiles,
-                                                       nullptr, c->d_rank_b, part, nullptr,
-                                                       nullptr);
+    rk_runs<RK_FILL><<<ntiles, RS_T, 0, c->s>>>(b.ka, b.kb, b.va, b.vb, b.par, n, ntiles, nullptr,
+                                                c->d_rank_b, part);
     rk_final<<<1, 32, 0, c->s>>>(part, ntiles, 1, reinterpret_cast<u64 *>(c->dev + o_out));
     cudaMemcpyAsync(c->host + o_out, c->dev + o_out, io_end - o_out, cudaMemcpyDeviceToHost, c->s);
     if (rc_finish(c) != 0) return -1;
@@ -984,7 +938,6 @@ float rc_rank_score_batch(void *ctx, const unsigned int *prog, const unsigned in
     stat_inputs(c, prog, off, pcount, nsets, nsegs, kmax, c0, &cur, sp);
     const size_t o_out = rc_take(&cur, sizeof(u64) * 4 * (size_t)nsegs);
     const size_t o_status = rc_take(&cur, sizeof(int) * (size_t)nsegs);
-    const size_t o_long = rc_take(&cur, sizeof(int) * (size_t)nsegs);
     const size_t o_abort = rc_take(&cur, sizeof(int));
     const size_t io_end = rc_take(&cur, 0);
     const int wseg = wave_segments(nsegs, n, true);
@@ -994,10 +947,8 @@ float rc_rank_score_batch(void *ctx, const unsigned int *prog, const unsigned in
     stat_copy(c, pcount, nsets, nsegs, kmax, c0, sp);
     unsigned char *dev = c->dev;
     int *d_status = reinterpret_cast<int *>(dev + o_status);
-    int *d_long = reinterpret_cast<int *>(dev + o_long);
     int *d_abort = reinterpret_cast<int *>(dev + o_abort);
     cudaMemsetAsync(d_status, 0, sizeof(int) * nsegs, c->s);
-    cudaMemsetAsync(d_long, 0, sizeof(int) * nsegs, c->s);
     cudaMemsetAsync(d_abort, 0, sizeof(int), c->s);
     const size_t smem = key_smem(sp);
     if (smem > 48 * 1024 &&
@@ -1006,12 +957,9 @@ float rc_rank_score_batch(void *ctx, const unsigned int *prog, const unsigned in
         return -1.0f;
     const int ktiles = (n + RK_TILE - 1) / RK_TILE;
     const int ntiles = (n + RS_TILE - 1) / RS_TILE;
-    /* One wave of segments [s0, s0 + ns): keys, the sort, the run pass and
-       the per-segment sums. `half`: sort by the upper 32 key bits only and
-       resolve the runs of equal upper halves by their lower halves (a
-       segment with a run longer than RK_RUN_MAX is marked in d_long and
-       redone in full below). */
-    auto wave = [&](int s0, int ns, bool half) {
+    cudaEventRecord(c->t0, c->s);
+    for (int s0 = 0; s0 < nsegs; s0 += wseg) {
+        const int ns = std::min(wseg, nsegs - s0);
         size_t wc = work;
         __int128 *part = nullptr;
         const RsBuffers b = rs_carve(dev, &wc, ns, n, true, &part);
@@ -1022,38 +970,16 @@ float rc_rank_score_batch(void *ctx, const unsigned int *prog, const unsigned in
             reinterpret_cast<const int *>(dev + sp.o_valid),
             reinterpret_cast<const double *>(dev + sp.o_c0), kmax, c->d_cols64, c->d_y64, c->npad,
             n, ntrials, s0, ktiles, sp.b.fmaxins, b.ka, b.va, d_status);
-        c->launches += 3 + rs_sort<true>(b, ns, n, d_abort, c->s, half ? RS_PASSES / 2 : 0);
-        if (half)
-            rk_runs<RK_SUMS, true><<<(unsigned)ns * ntiles, RS_T, 0, c->s>>>(
-                b.ka, b.kb, b.va, b.vb, b.par, n, ntiles, c->d_rank_b, nullptr, part, d_long + s0,
-                nullptr);
-        else
-            rk_runs<RK_SUMS, false><<<(unsigned)ns * ntiles, RS_T, 0, c->s>>>(
-                b.ka, b.kb, b.va, b.vb, b.par, n, ntiles, c->d_rank_b, nullptr, part, nullptr,
-                nullptr);
+        c->launches += 3 + rs_sort<true>(b, ns, n, d_abort, c->s);
+        rk_runs<RK_SUMS><<<(unsigned)ns * ntiles, RS_T, 0, c->s>>>(
+            b.ka, b.kb, b.va, b.vb, b.par, n, ntiles, c->d_rank_b, nullptr, part);
         rk_final<<<(ns + 127) / 128, 128, 0, c->s>>>(part, ntiles, ns,
                                                      reinterpret_cast<u64 *>(dev + o_out) + 4 * (size_t)s0);
-    };
-    cudaEventRecord(c->t0, c->s);
-    for (int s0 = 0; s0 < nsegs; s0 += wseg) wave(s0, std::min(wseg, nsegs - s0), true);
+    }
+    cudaEventRecord(c->t1, c->s);
     if (cudaGetLastError() != cudaSuccess) return -1.0f;
     cudaMemcpyAsync(c->host + sp.in_end, dev + sp.in_end, io_end - sp.in_end,
                     cudaMemcpyDeviceToHost, c->s);
-    if (rc_finish(c) != 0) return -1.0f;
-    /* segments with a long run of equal upper halves: the full sort */
-    const int *h_long = reinterpret_cast<const int *>(c->host + o_long);
-    bool redo = false;
-    for (int g = 0; g < nsegs; ++g)
-        if (h_long[g]) {
-            wave(g, 1, false);
-            redo = true;
-        }
-    cudaEventRecord(c->t1, c->s);
-    if (redo) {
-        if (cudaGetLastError() != cudaSuccess) return -1.0f;
-        cudaMemcpyAsync(c->host + sp.in_end, dev + sp.in_end, io_end - sp.in_end,
-                        cudaMemcpyDeviceToHost, c->s);
-    }
     if (rc_finish(c) != 0) return -1.0f;
     if (*reinterpret_cast<const int *>(c->host + o_abort) != 0) return -1.0f;
     memcpy(out, c->host + o_out, sizeof(u64) * 4 * (size_t)nsegs);
