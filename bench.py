@@ -394,6 +394,7 @@ def bench_score(args, rank, world, dev, pkg, W, flushbuf):
     launches = ev.launch_count() - n0
     stats = ev.last_stats()
     clocks = clk.summary()
+    extra = score_plain_and_absolute(ev, prog, off, pcount, vals, N, flushbuf, seed=rank)
     ev.close()
     h2d = int(prog.nbytes + off.nbytes + pcount.nbytes)
     d2h = int(P * (8 + 4))
@@ -401,7 +402,45 @@ def bench_score(args, rank, world, dev, pkg, W, flushbuf):
     return dict(P=P, N=N, dev_ms=dev_ms, wall=wall, alg_ops=alg_ops, clocks=clocks,
                 h2d=h2d, d2h=d2h, trees=trees, x=x, y=y, stats=stats, prof=prof,
                 launches=launches, unit_count=float(P) * N,
-                finite=int(finite.sum()), alg_ops_finite=float(N) * float((ops[finite] + 2).sum()))
+                finite=int(finite.sum()), alg_ops_finite=float(N) * float((ops[finite] + 2).sum()),
+                **extra)
+
+
+def score_plain_and_absolute(ev, prog, off, pcount, vals, N, flushbuf, seed, sample=64,
+                             abs_steps=3):
+    """Outside the timed region, the two other forms the scoring
+    configuration names: the plain form, one program per scoring call (one
+    launch sequence each) on a seeded random sample of the batch, whose
+    scores must equal the batched ones; and the batched form under absolute
+    error (L2 flushed before each call)."""
+    import torch
+    P = len(off) - 1
+    rng = np.random.Generator(np.random.PCG64(seed + 77))
+    pick = np.sort(rng.choice(P, size=min(sample, P), replace=False))
+    ms_plain, same = 0.0, True
+    for i in pick:
+        one = np.ascontiguousarray(prog[off[i]:off[i + 1]])
+        o1 = np.array([0, len(one)], np.uint32)
+        ev.score_batch(one, o1, 0, pcount[i:i + 1])  # its own warm-up
+        flush_l2(flushbuf)
+        torch.cuda.synchronize()
+        v1, _, ms = ev.score_batch(one, o1, 0, pcount[i:i + 1])
+        ms_plain += ms
+        same = same and bool(np.array_equal(np.asarray(v1).view(np.uint64),
+                                            np.asarray(vals)[i:i + 1].view(np.uint64)))
+    plain = float(len(pick)) * N / (ms_plain / 1e3)
+    ev.score_batch(prog, off, 1, pcount)
+    ms_abs = []
+    for _ in range(abs_steps):
+        flush_l2(flushbuf)
+        torch.cuda.synchronize()
+        ms_abs.append(ev.score_batch(prog, off, 1, pcount)[2])
+    absolute = float(P) * N / (float(np.mean(ms_abs)) / 1e3)
+    return {"plain": {"value": plain, "unit": "expr*row/s", "same_scores": same,
+                      "sample": f"{len(pick)} programs drawn at random (seeded) from the batch, "
+                                "one scoring call each"},
+            "absolute": {"value": absolute, "unit": "expr*row/s", "steps": abs_steps,
+                         "config": "the same batch and rows, absolute error"}}
 
 
 def fit_lane_ops(plans, sweeps, N, metric):
@@ -1158,6 +1197,9 @@ def main():
             line["rows_evaluated_per_step"] = rows_f32
             line["rows_f64_rescored_per_step"] = rows_f64
             line["candidates_finite"] = r["finite"]
+            line["plain"] = r["plain"]
+            line["batched_over_plain"] = value / r["plain"]["value"]
+            line["absolute_error_value"] = r["absolute"]["value"]
         if args.workload == "fit" and "plain" in r:
             line["plain"] = r["plain"]
             line["fused_over_plain"] = value / r["plain"]["value"]

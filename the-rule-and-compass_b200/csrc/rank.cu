@@ -40,6 +40,7 @@ typedef unsigned long long u64;
 #define RK_T 256                  /* key threads (two rows each per step) */
 #define RK_TILE 8192              /* rows per key block */
 #define RK_WAVE_BYTES ((size_t)3 << 30)
+#define RS_PASSES 8               /* 8-bit digits of a u64 key */
 
 /* ---- keys -------------------------------------------------------------- */
 
@@ -59,20 +60,68 @@ __device__ __forceinline__ double rk_key_abs_value(u64 k) { return __longlong_as
 
 enum { RK_RANK = 0, RK_ABS = 1 };
 
+/* Adds the counts of all eight digits of keys[r0, r1) to the block's
+   shared table cnt[pass][digit]; all RS_T threads of the block call it. */
+__device__ __forceinline__ void rs_count_keys(const u64 *src, long long r0, long long r1,
+                                              unsigned int (*cnt)[256])
+{
+    const int tid = threadIdx.x, lane = tid & 31;
+    for (long long c = r0; c < r1; c += 4 * RS_T) {
+        /* four loads in flight per thread; every lane takes part in the
+           warp votes, out-of-range ones with no digit */
+        u64 k[4];
+        bool in[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const long long idx = c + i * RS_T + tid;
+            in[i] = idx < r1;
+            k[i] = in[i] ? src[idx] : 0ULL;
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int d = 0; d < RS_PASSES; ++d) {
+                const unsigned dg = in[i] ? (unsigned)(k[i] >> (8 * d)) & 255u : 256u;
+                /* a digit the whole warp shares (a constant segment, the
+                   exponent bytes) is one add; the exponent bytes take few
+                   values, so they are grouped; mantissa bytes scatter over
+                   the bins and add one by one */
+                if (__all_sync(0xffffffffu, dg == __shfl_sync(0xffffffffu, dg, 0))) {
+                    if (lane == 0 && dg < 256u) atomicAdd(&cnt[d][dg], 32u);
+                } else if (d >= 6) {
+                    /* match_any here: this count is bound by its shared-memory
+                       atomics, and the ballots' extra instructions cost more
+                       than the match saves */
+                    const unsigned peers = __match_any_sync(0xffffffffu, dg);
+                    if (dg < 256u && lane == __ffs(peers) - 1)
+                        atomicAdd(&cnt[d][dg], (unsigned)__popc(peers));
+                } else if (dg < 256u) {
+                    atomicAdd(&cnt[d][dg], 1u);
+                }
+            }
+    }
+}
+
+
 /* Keys of segments [seg0, seg0 + gridDim.x / tiles) over all rows: the f64
    forward sweep of the segment's candidate at its constants
    (c0[seg * kmax + slot]), two rows per thread. RK_RANK keys the
    prediction; RK_ABS keys |pred - y| and flags a row whose prediction is
    not finite or exceeds 1e30 (eval.cu:4388-4418). A non-finite key marks
-   the segment's status 2. */
+   the segment's status 2. The block then counts the eight digits of the
+   keys it wrote (still in L2) into count[local segment][pass][256], which
+   the caller zeroed, so the sort needs no counting read of its own. */
+static_assert(RK_T == RS_T, "the digit count runs on the key kernel's blocks");
 template <int MODE>
 __global__ void __launch_bounds__(RK_T) rk_keys(const FIns *fins, const int *fins_off,
                                                 const int4 *finfo, const int *valid,
                                                 const double *c0, int kmax, const double *cols,
                                                 const double *y, int npad, int n, int ntrials,
                                                 int seg0, int tiles, int maxins, u64 *keys,
-                                                unsigned int *rows, int *status)
+                                                unsigned int *rows, unsigned int *count,
+                                                int *status)
 {
+    __shared__ unsigned int cnt[RS_PASSES][256];
     using V4 = FiV<double, 2>::V4;
     extern __shared__ __align__(16) unsigned char sm[];
     FIns *ins = reinterpret_cast<FIns *>(sm);
@@ -85,6 +134,8 @@ __global__ void __launch_bounds__(RK_T) rk_keys(const FIns *fins, const int *fin
     const int tid = threadIdx.x;
     const bool ok = valid[cand] != 0;
     const int nf = finfo[cand].x;
+#pragma unroll
+    for (int d = 0; d < RS_PASSES; ++d) cnt[d][tid] = 0;
     if (ok) {
         for (int i = tid; i < nf; i += RK_T) ins[i] = fins[fins_off[cand] + i];
         if (tid < FT_MAX_CONST) cv[tid] = tid < kmax ? c0[(size_t)seg * kmax + tid] : 0.0;
@@ -122,7 +173,13 @@ __global__ void __launch_bounds__(RK_T) rk_keys(const FIns *fins, const int *fin
             if (rseg) rseg[rr] = (unsigned int)rr;
         }
     }
+    /* (the barrier also makes the block's key writes visible to its reads) */
     if (__syncthreads_or(bad) && tid == 0) status[seg] = 2;
+    rs_count_keys(kseg, r0, r1, cnt);
+    __syncthreads();
+#pragma unroll
+    for (int d = 0; d < RS_PASSES; ++d)
+        if (cnt[d][tid]) atomicAdd(&count[((size_t)ls * RS_PASSES + d) * 256 + tid], cnt[d][tid]);
 }
 
 /* Keys of the target (one segment). */
@@ -148,7 +205,6 @@ __global__ void rk_target_keys(const double *y, int n, u64 *keys, unsigned int *
  * wait that gives up raises a flag that stops every other wait and every
  * write, and fails the call. */
 
-#define RS_PASSES 8
 #define RS_ST_AGG 1ULL    /* published word: the tile's own counts */
 #define RS_ST_PREFIX 2ULL /* published word: counts of this and every earlier tile */
 #define RS_SPIN_LIMIT (1u << 22)
@@ -185,47 +241,14 @@ __global__ void __launch_bounds__(RS_T) rs_count(const u64 *keys, int n, int nbl
 {
     __shared__ unsigned int cnt[RS_PASSES][256];
     const int seg = blockIdx.x / nblk, blk = blockIdx.x % nblk;
-    const int tid = threadIdx.x, lane = tid & 31;
+    const int tid = threadIdx.x;
     const u64 *src = keys + (size_t)seg * n;
 #pragma unroll
     for (int d = 0; d < RS_PASSES; ++d) cnt[d][tid] = 0;
     __syncthreads();
     const long long r0 = (long long)blk * RS_COUNT_TILES * RS_TILE;
     const long long r1 = min((long long)n, r0 + (long long)RS_COUNT_TILES * RS_TILE);
-    for (long long c = r0; c < r1; c += 4 * RS_T) {
-        /* four loads in flight per thread; every lane takes part in the
-           warp votes, out-of-range ones with no digit */
-        u64 k[4];
-        bool in[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const long long idx = c + i * RS_T + tid;
-            in[i] = idx < r1;
-            k[i] = in[i] ? src[idx] : 0ULL;
-        }
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int d = 0; d < RS_PASSES; ++d) {
-                const unsigned dg = in[i] ? (unsigned)(k[i] >> (8 * d)) & 255u : 256u;
-                /* a digit the whole warp shares (a constant segment, the
-                   exponent bytes) is one add; the exponent bytes take few
-                   values, so they are grouped; mantissa bytes scatter over
-                   the bins and add one by one */
-                if (__all_sync(0xffffffffu, dg == __shfl_sync(0xffffffffu, dg, 0))) {
-                    if (lane == 0 && dg < 256u) atomicAdd(&cnt[d][dg], 32u);
-                } else if (d >= 6) {
-                    /* match_any here: this kernel is bound by its shared-memory
-                       atomics, and the ballots' extra instructions cost more
-                       than the match saves */
-                    const unsigned peers = __match_any_sync(0xffffffffu, dg);
-                    if (dg < 256u && lane == __ffs(peers) - 1)
-                        atomicAdd(&cnt[d][dg], (unsigned)__popc(peers));
-                } else if (dg < 256u) {
-                    atomicAdd(&cnt[d][dg], 1u);
-                }
-            }
-    }
+    rs_count_keys(src, r0, r1, cnt);
     __syncthreads();
 #pragma unroll
     for (int d = 0; d < RS_PASSES; ++d)
@@ -447,23 +470,26 @@ struct RsBuffers {
    kernels launched. A look-back that gave up, or a position out of range,
    sets *abort_flag (which the caller zeroes once and checks after). */
 template <bool VALS>
-unsigned long long rs_sort(const RsBuffers &b, int nseg, int n, int *abort_flag, cudaStream_t s)
+unsigned long long rs_sort(const RsBuffers &b, int nseg, int n, int *abort_flag, cudaStream_t s,
+                           bool counted)
 {
     const int ntiles = (n + RS_TILE - 1) / RS_TILE;
     const int nblk = (ntiles + RS_COUNT_TILES - 1) / RS_COUNT_TILES;
     cudaFuncSetAttribute(rs_pass<VALS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)rs_pass_smem<VALS>());
-    cudaMemsetAsync(b.count, 0, sizeof(unsigned int) * RS_PASSES * 256 * (size_t)nseg, s);
     cudaMemsetAsync(b.state, 0, sizeof(u64) * 256 * (size_t)ntiles * (size_t)nseg, s);
     cudaMemsetAsync(b.ticket, 0, sizeof(int) * RS_PASSES, s);
-    rs_count<<<(unsigned)nseg * (unsigned)nblk, RS_T, 0, s>>>(b.ka, n, nblk, b.count);
+    if (!counted) {
+        cudaMemsetAsync(b.count, 0, sizeof(unsigned int) * RS_PASSES * 256 * (size_t)nseg, s);
+        rs_count<<<(unsigned)nseg * (unsigned)nblk, RS_T, 0, s>>>(b.ka, n, nblk, b.count);
+    }
     rs_prep<<<nseg, 256, 0, s>>>(b.count, n, b.skip, b.par);
     const unsigned grid = (unsigned)nseg * (unsigned)ntiles;
     for (int pass = 0; pass < RS_PASSES; ++pass)
         rs_pass<VALS><<<grid, RS_T, rs_pass_smem<VALS>(), s>>>(
             b.ka, b.kb, b.va, b.vb, b.skip, b.count, b.state, b.ticket, abort_flag, n, ntiles,
             pass);
-    return 2 + RS_PASSES;
+    return (counted ? 1 : 2) + RS_PASSES;
 }
 
 /* ---- runs and exact sums ----------------------------------------------- */
@@ -531,6 +557,23 @@ __device__ int rk_upper(const u64 *keys, int lo, int hi, u64 k)
 }
 
 enum { RK_SUMS = 0, RK_FILL = 1 };
+
+/* Sum of a 128-bit integer over the block's RS_T threads (a tree in shared
+   memory; integers, so exact in any order). Every thread gets the sum. */
+__device__ __forceinline__ __int128 rk_block_sum(__int128 v, __int128 *red)
+{
+    const int tid = threadIdx.x;
+    red[tid] = v;
+    __syncthreads();
+#pragma unroll
+    for (int h = RS_T / 2; h > 0; h >>= 1) {
+        if (tid < h) red[tid] += red[tid + h];
+        __syncthreads();
+    }
+    const __int128 s = red[0];
+    __syncthreads();
+    return s;
+}
 
 /* One tile of a sorted segment: every position's run [i, j) (block scans
    of the run starts inside the tile; a binary search for a run that crosses
@@ -604,40 +647,33 @@ __global__ void __launch_bounds__(RS_T) rk_runs(const u64 *ka, const u64 *kb,
             if (f[j]) end = q;
         }
     }
-    /* fixed-order block sums (integers: exact in any order) */
-    red[tid] = ab;
-    __syncthreads();
+    const __int128 sab = rk_block_sum(ab, red);
+    const __int128 saa = rk_block_sum(aa, red);
     if (tid == 0) {
-        __int128 s = 0;
-        for (int i = 0; i < RS_T; ++i) s += red[i];
-        part[((size_t)seg * ntiles + tile) * 2 + 0] = s;
-    }
-    __syncthreads();
-    red[tid] = aa;
-    __syncthreads();
-    if (tid == 0) {
-        __int128 s = 0;
-        for (int i = 0; i < RS_T; ++i) s += red[i];
-        part[((size_t)seg * ntiles + tile) * 2 + 1] = s;
+        part[((size_t)seg * ntiles + tile) * 2 + 0] = sab;
+        part[((size_t)seg * ntiles + tile) * 2 + 1] = saa;
     }
 }
 
-/* Per segment: the tile partials summed into two 128-bit values, written as
-   (hi, lo) u64 pairs at out[4 * seg ...] (two's complement). */
-__global__ void rk_final(const __int128 *part, int ntiles, int nseg, u64 *out)
+/* One block per segment: the tile partials summed into two 128-bit values,
+   written as (hi, lo) u64 pairs at out[4 * seg ...] (two's complement). */
+__global__ void __launch_bounds__(RS_T) rk_final(const __int128 *part, int ntiles, u64 *out)
 {
-    const int seg = blockIdx.x * blockDim.x + threadIdx.x;
-    if (seg >= nseg) return;
+    __shared__ __int128 red[RS_T];
+    const int seg = blockIdx.x, tid = threadIdx.x;
     __int128 ab = 0, aa = 0;
-    for (int t = 0; t < ntiles; ++t) {
+    for (int t = tid; t < ntiles; t += RS_T) {
         ab += part[((size_t)seg * ntiles + t) * 2 + 0];
         aa += part[((size_t)seg * ntiles + t) * 2 + 1];
     }
-    const unsigned __int128 uab = (unsigned __int128)ab, uaa = (unsigned __int128)aa;
-    out[(size_t)seg * 4 + 0] = (u64)(uab >> 64);
-    out[(size_t)seg * 4 + 1] = (u64)uab;
-    out[(size_t)seg * 4 + 2] = (u64)(uaa >> 64);
-    out[(size_t)seg * 4 + 3] = (u64)uaa;
+    const unsigned __int128 uab = (unsigned __int128)rk_block_sum(ab, red);
+    const unsigned __int128 uaa = (unsigned __int128)rk_block_sum(aa, red);
+    if (tid == 0) {
+        out[(size_t)seg * 4 + 0] = (u64)(uab >> 64);
+        out[(size_t)seg * 4 + 1] = (u64)uab;
+        out[(size_t)seg * 4 + 2] = (u64)(uaa >> 64);
+        out[(size_t)seg * 4 + 3] = (u64)uaa;
+    }
 }
 
 /* ---- order statistics --------------------------------------------------- */
@@ -854,10 +890,10 @@ int rk_prepare(RcCtx *c)
     const RsBuffers b = rs_carve(c->dev, &wc, 1, n, true, &part);
     const int ntiles = (n + RS_TILE - 1) / RS_TILE;
     rk_target_keys<<<(n + 255) / 256, 256, 0, c->s>>>(c->d_y64, n, b.ka, b.va);
-    c->launches += 3 + rs_sort<true>(b, 1, n, d_abort, c->s);
+    c->launches += 3 + rs_sort<true>(b, 1, n, d_abort, c->s, false);
     rk_runs<RK_FILL><<<ntiles, RS_T, 0, c->s>>>(b.ka, b.kb, b.va, b.vb, b.par, n, ntiles, nullptr,
                                                 c->d_rank_b, part);
-    rk_final<<<1, 32, 0, c->s>>>(part, ntiles, 1, reinterpret_cast<u64 *>(c->dev + o_out));
+    rk_final<<<1, RS_T, 0, c->s>>>(part, ntiles, reinterpret_cast<u64 *>(c->dev + o_out));
     cudaMemcpyAsync(c->host + o_out, c->dev + o_out, io_end - o_out, cudaMemcpyDeviceToHost, c->s);
     if (rc_finish(c) != 0) return -1;
     if (*reinterpret_cast<const int *>(c->host + o_abort) != 0) return -1;
@@ -951,8 +987,9 @@ float rc_rank_score_batch(void *ctx, const unsigned int *prog, const unsigned in
     cudaMemsetAsync(d_status, 0, sizeof(int) * nsegs, c->s);
     cudaMemsetAsync(d_abort, 0, sizeof(int), c->s);
     const size_t smem = key_smem(sp);
-    if (smem > 48 * 1024 &&
-        cudaFuncSetAttribute(rk_keys<RK_RANK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    /* (every call: the kernel's static digit table counts against the
+       default dynamic limit) */
+    if (cudaFuncSetAttribute(rk_keys<RK_RANK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem) != cudaSuccess)
         return -1.0f;
     const int ktiles = (n + RK_TILE - 1) / RK_TILE;
@@ -963,18 +1000,19 @@ float rc_rank_score_batch(void *ctx, const unsigned int *prog, const unsigned in
         size_t wc = work;
         __int128 *part = nullptr;
         const RsBuffers b = rs_carve(dev, &wc, ns, n, true, &part);
+        cudaMemsetAsync(b.count, 0, sizeof(unsigned int) * RS_PASSES * 256 * (size_t)ns, c->s);
         rk_keys<RK_RANK><<<(unsigned)ns * ktiles, RK_T, smem, c->s>>>(
             reinterpret_cast<const FIns *>(dev + sp.o_fins),
             reinterpret_cast<const int *>(dev + sp.o_finsoff),
             reinterpret_cast<const int4 *>(dev + sp.o_finfo),
             reinterpret_cast<const int *>(dev + sp.o_valid),
             reinterpret_cast<const double *>(dev + sp.o_c0), kmax, c->d_cols64, c->d_y64, c->npad,
-            n, ntrials, s0, ktiles, sp.b.fmaxins, b.ka, b.va, d_status);
-        c->launches += 3 + rs_sort<true>(b, ns, n, d_abort, c->s);
+            n, ntrials, s0, ktiles, sp.b.fmaxins, b.ka, b.va, b.count, d_status);
+        c->launches += 3 + rs_sort<true>(b, ns, n, d_abort, c->s, true);
         rk_runs<RK_SUMS><<<(unsigned)ns * ntiles, RS_T, 0, c->s>>>(
             b.ka, b.kb, b.va, b.vb, b.par, n, ntiles, c->d_rank_b, nullptr, part);
-        rk_final<<<(ns + 127) / 128, 128, 0, c->s>>>(part, ntiles, ns,
-                                                     reinterpret_cast<u64 *>(dev + o_out) + 4 * (size_t)s0);
+        rk_final<<<ns, RS_T, 0, c->s>>>(part, ntiles,
+                                        reinterpret_cast<u64 *>(dev + o_out) + 4 * (size_t)s0);
     }
     cudaEventRecord(c->t1, c->s);
     if (cudaGetLastError() != cudaSuccess) return -1.0f;
@@ -1034,8 +1072,9 @@ float rc_order_stat_score_batch(void *ctx, const unsigned int *prog, const unsig
     cudaMemsetAsync(d_status, 0, sizeof(int) * nsegs, c->s);
     cudaMemsetAsync(d_abort, 0, sizeof(int), c->s);
     const size_t smem = key_smem(sp);
-    if (smem > 48 * 1024 &&
-        cudaFuncSetAttribute(rk_keys<RK_ABS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    /* (every call: the kernel's static digit table counts against the
+       default dynamic limit) */
+    if (cudaFuncSetAttribute(rk_keys<RK_ABS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem) != cudaSuccess)
         return -1.0f;
     const int ktiles = (n + RK_TILE - 1) / RK_TILE;
@@ -1045,14 +1084,15 @@ float rc_order_stat_score_batch(void *ctx, const unsigned int *prog, const unsig
         size_t wc = work;
         __int128 *part = nullptr;
         const RsBuffers b = rs_carve(dev, &wc, ns, n, false, &part);
+        cudaMemsetAsync(b.count, 0, sizeof(unsigned int) * RS_PASSES * 256 * (size_t)ns, c->s);
         rk_keys<RK_ABS><<<(unsigned)ns * ktiles, RK_T, smem, c->s>>>(
             reinterpret_cast<const FIns *>(dev + sp.o_fins),
             reinterpret_cast<const int *>(dev + sp.o_finsoff),
             reinterpret_cast<const int4 *>(dev + sp.o_finfo),
             reinterpret_cast<const int *>(dev + sp.o_valid),
             reinterpret_cast<const double *>(dev + sp.o_c0), kmax, c->d_cols64, c->d_y64, c->npad,
-            n, ntrials, s0, ktiles, sp.b.fmaxins, b.ka, nullptr, d_status);
-        c->launches += 2 + rs_sort<false>(b, ns, n, d_abort, c->s);
+            n, ntrials, s0, ktiles, sp.b.fmaxins, b.ka, nullptr, b.count, d_status);
+        c->launches += 2 + rs_sort<false>(b, ns, n, d_abort, c->s, true);
         os_pick<<<ns, OS_T, 0, c->s>>>(b.ka, b.kb, b.par, n, s0, ns, what, d_status,
                                        reinterpret_cast<double *>(dev + o_val));
     }

@@ -746,6 +746,7 @@ __global__ void rc_score_finalize(int nprog, const int *__restrict__ cand_tiles,
     }
     if (mode == SM_PREDICT) return;
     const double dn = (double)n;
+    /* (the comparisons below flag a bound that is not a number) */
     bool flag = false;
     if (bad[cand]) {
         if (out) out[cand] = INFINITY;
@@ -766,20 +767,20 @@ __global__ void rc_score_finalize(int nprog, const int *__restrict__ cand_tiles,
                 const double rho = (s[0] <= 0.0 || syy <= 0.0) ? 0.0
                                                                : s[1] / (sqrt(s[0]) * sqrt(syy));
                 v = mode == SM_CORRELATION_SIGNED ? 1.0 - rho : 1.0 - fabs(rho);
-                flag = s[2] > RC_FLAG_TOL * s[0] ||
-                       s[3] > RC_FLAG_TOL * (fabs(s[1]) + RC_FLAG_TOL * sqrt(fmax(s[0], 0.0) * syy));
+                flag = !(s[2] <= RC_FLAG_TOL * s[0]) ||
+                       !(s[3] <= RC_FLAG_TOL * (fabs(s[1]) + RC_FLAG_TOL * sqrt(fmax(s[0], 0.0) * syy)));
             } break;
             case SM_AIC: case SM_AICC: case SM_BIC:
                 v = s[0]; /* RSS; the host applies the penalty */
-                flag = s[2] > RC_FLAG_TOL * fabs(s[0]);
+                flag = !(s[2] <= RC_FLAG_TOL * fabs(s[0]));
                 break;
             case SM_SIGNED:
                 v = fabs(s[0]) / dn;
-                flag = s[2] > RC_FLAG_TOL * fabs(s[0]);
+                flag = !(s[2] <= RC_FLAG_TOL * fabs(s[0]));
                 break;
             case SM_MAXIMUM:
                 v = s[0];
-                flag = s[2] > RC_FLAG_TOL * s[0];
+                flag = !(s[2] <= RC_FLAG_TOL * s[0]);
                 break;
             case SM_LOG_LOSS: case SM_BRIER: case SM_HINGE_SIGMOID: case SM_HINGE_ORDINARY:
             case SM_HINGE_SQUARED:
@@ -788,12 +789,12 @@ __global__ void rc_score_finalize(int nprog, const int *__restrict__ cand_tiles,
                     st = RC_SCORE_ALL_ZERO_WEIGHT;
                 } else {
                     v = s[0] / s[1];
-                    flag = s[2] > RC_FLAG_TOL * fabs(s[0]);
+                    flag = !(s[2] <= RC_FLAG_TOL * fabs(s[0]));
                 }
                 break;
             default:
                 v = s[0] / dn;
-                flag = s[2] > RC_FLAG_TOL * fabs(s[0]);
+                flag = !(s[2] <= RC_FLAG_TOL * fabs(s[0]));
                 break;
         }
         out[cand] = v;
