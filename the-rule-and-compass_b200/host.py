@@ -40,6 +40,15 @@ def lib():
                                    P(ctypes.c_uint32), ctypes.c_int, P(ctypes.c_double),
                                    ctypes.c_int, P(ctypes.c_int32), P(ctypes.c_int),
                                    ctypes.c_int]
+        L.rch_fit_plan_postfix.restype = ctypes.c_int
+        L.rch_fit_plan_postfix.argtypes = [P(ctypes.c_uint32), ctypes.c_int, P(ctypes.c_uint32),
+                                           ctypes.c_int, P(ctypes.c_double), ctypes.c_int,
+                                           P(ctypes.c_int32), P(ctypes.c_int), ctypes.c_int]
+        L.rch_fit_plans_postfix.restype = ctypes.c_int
+        L.rch_fit_plans_postfix.argtypes = [ctypes.c_int, P(ctypes.c_uint32), ctypes.c_int,
+                                            P(ctypes.c_uint32), P(ctypes.c_double),
+                                            P(ctypes.c_int32), P(ctypes.c_int32),
+                                            P(ctypes.c_int32), ctypes.c_int]
         L.rch_admission_count.restype = ctypes.c_int
         L.rch_admission_count.argtypes = [ctypes.c_int, ctypes.c_longlong]
         L.rch_select_promoted.restype = ctypes.c_int
@@ -176,6 +185,54 @@ def gpu_fit_plan(tree: E.Node, allow_no_constants=False) -> GpuFitPlan:
         raise GpuFitReject(m)
     k = nconst.value
     return GpuFitPlan(words[: 4 * m].copy(), c0[:k].copy(), gauge.copy(), k)
+
+
+def gpu_fit_plan_words(words, allow_no_constants=False) -> GpuFitPlan:
+    """gpu_fit_plan of a postfix program (its words up to HALT, as the pool
+    holds them) without building the tree: the same plan, the same
+    rejections, and "malformed" for a program that is not one expression."""
+    w = np.ascontiguousarray(words, np.uint32).reshape(-1)
+    cap = 4 * max(len(w), 1)
+    out = np.zeros(cap, np.uint32)
+    c0 = np.zeros(max(len(w), 1), np.float64)
+    gauge = np.full(2, -1, np.int32)
+    nconst = ctypes.c_int(0)
+    m = lib().rch_fit_plan_postfix(_p(w, ctypes.c_uint32), len(w), _p(out, ctypes.c_uint32), cap,
+                                   _p(c0, ctypes.c_double), len(c0), _p(gauge, ctypes.c_int32),
+                                   ctypes.byref(nconst), 1 if allow_no_constants else 0)
+    if m < 0:
+        raise GpuFitReject(m)
+    k = nconst.value
+    return GpuFitPlan(out[: 4 * m].copy(), c0[:k].copy(), gauge.copy(), k)
+
+
+def gpu_fit_plans_words(words, allow_no_constants=False):
+    """gpu_fit_plan_words of every row of a [programs, width] word array in
+    one native call: a list with, per row, its GpuFitPlan or the rejection
+    label."""
+    w = np.ascontiguousarray(words, np.uint32)
+    n, width = w.shape
+    if n == 0:
+        return []
+    out = np.zeros((n, 4 * width), np.uint32)
+    c0 = np.zeros((n, width), np.float64)
+    gauge = np.full((n, 2), -1, np.int32)
+    nconst = np.zeros(n, np.int32)
+    status = np.zeros(n, np.int32)
+    if lib().rch_fit_plans_postfix(n, _p(w, ctypes.c_uint32), width, _p(out, ctypes.c_uint32),
+                                   _p(c0, ctypes.c_double), _p(gauge, ctypes.c_int32),
+                                   _p(nconst, ctypes.c_int32), _p(status, ctypes.c_int32),
+                                   1 if allow_no_constants else 0) < 0:
+        raise RuntimeError("rch_fit_plans_postfix failed")
+    res = []
+    for i in range(n):
+        m = int(status[i])
+        if m < 0:
+            res.append(REJECT.get(m, str(m)))
+        else:
+            k = int(nconst[i])
+            res.append(GpuFitPlan(out[i, : 4 * m].copy(), c0[i, :k].copy(), gauge[i].copy(), k))
+    return res
 
 
 def pack_plans(plans, kmax=None):

@@ -78,6 +78,43 @@ bool load(const int *ops, const double *vals, int n, Node &t)
     return parse(ops, vals, n, pos, t, 0) && pos == n;
 }
 
+/* The tree of one postfix program of `len` words (the words `emit` writes
+   and the device variation engine builds): [CONST, f32 bits] (the value
+   widened to f64), [VAR, index], operator words, up to HALT. False for a
+   program that is not one well-formed expression (a truncated operand, an
+   unknown or under-supplied operator, no HALT, or not exactly one value). */
+bool load_postfix(const uint32_t *w, int len, Node &t)
+{
+    std::vector<Node> st;
+    for (int i = 0; i < len;) {
+        const int op = (int)w[i++];
+        if (op == HALT) {
+            if (st.size() != 1) return false;
+            t = std::move(st.back());
+            return true;
+        }
+        if (op == CONST || op == VAR) {
+            if (i >= len) return false;
+            const uint32_t a = w[i++];
+            if (op == CONST) {
+                float f;
+                memcpy(&f, &a, sizeof f);
+                st.push_back(Node{CONST, (double)f, {}});
+            } else {
+                st.push_back(Node{VAR, (double)a, {}});
+            }
+            continue;
+        }
+        const int k = arity(op);
+        if (!known(op) || (int)st.size() < k) return false;
+        Node n{op, 0.0, {}};
+        n.kids.assign(std::make_move_iterator(st.end() - k), std::make_move_iterator(st.end()));
+        st.erase(st.end() - k, st.end());
+        st.push_back(std::move(n));
+    }
+    return false;
+}
+
 /* gpu.rs:320-345 `lower`. */
 Node lower(const Node &n, bool &changed)
 {
@@ -174,6 +211,58 @@ bool fit_opcode(int op)
     }
 }
 
+/* gpu_fit_plan_reason of a loaded tree (rch_fit_plan's contract). */
+int plan_tree(const Node &t, uint32_t *words, int cap, double *c0, int cap_c, int *gauge,
+              int *nconst, int allow_no_constants)
+{
+    Flat f;
+    build(t, f);
+    const int m = (int)f.op.size();
+    if (f.nconst == 0 && !allow_no_constants) return -3;
+    if (f.nconst > GPU_FIT_MAX_CONSTANTS) return -1;
+    if (m > GPU_FIT_MAX_NODES) return -2;
+    for (int i = 0; i < m; ++i)
+        if (!fit_opcode(f.op[i])) return -5;
+    if (4 * m > cap || f.nconst > cap_c) return -6;
+    for (int i = 0; i < m; ++i) {
+        uint32_t slot;
+        if (f.cslot[i] >= 0) slot = (uint32_t)f.cslot[i];
+        else if (f.op[i] == VAR) slot = (uint32_t)f.val[i];
+        else slot = 0xFFFFFFFFu;
+        const int a = arity(f.op[i]);
+        words[4 * i] = (uint32_t)f.op[i];
+        words[4 * i + 1] = a >= 1 ? (uint32_t)f.k0[i] : 0u;
+        words[4 * i + 2] = a >= 2 ? (uint32_t)f.k1[i] : 0u;
+        words[4 * i + 3] = slot;
+        if (f.cslot[i] >= 0) c0[f.cslot[i]] = f.val[i];
+    }
+    /* fit/correlation.rs:83-128 `gauge_of`. */
+    gauge[0] = -1;
+    gauge[1] = -1;
+    const int root = m - 1;
+    if (f.op[root] == MUL) {
+        const int a = f.k0[root], b = f.k1[root];
+        if (f.cslot[a] >= 0 && f.cslot[b] < 0) gauge[0] = f.cslot[a];
+        else if (f.cslot[b] >= 0 && f.cslot[a] < 0) gauge[0] = f.cslot[b];
+    } else if (f.op[root] == ADD) {
+        const int ks[2] = {f.k0[root], f.k1[root]};
+        for (int side = 0; side < 2; ++side) {
+            const int mm = ks[side], bb = ks[1 - side];
+            if (f.op[mm] != MUL || f.cslot[bb] < 0) continue;
+            const int x = f.k0[mm], y = f.k1[mm];
+            int scale;
+            if (f.cslot[x] >= 0 && f.cslot[y] < 0) scale = f.cslot[x];
+            else if (f.cslot[y] >= 0 && f.cslot[x] < 0) scale = f.cslot[y];
+            else continue;
+            gauge[0] = scale;
+            gauge[1] = f.cslot[bb];
+            break;
+        }
+    }
+    *nconst = f.nconst;
+    return m;
+}
+
 }  // namespace
 
 extern "C" {
@@ -224,52 +313,39 @@ int rch_fit_plan(const int *ops, const double *vals, int nn, uint32_t *words, in
 {
     Node t;
     if (!load(ops, vals, nn, t)) return -4;
-    Flat f;
-    build(t, f);
-    const int m = (int)f.op.size();
-    if (f.nconst == 0 && !allow_no_constants) return -3;
-    if (f.nconst > GPU_FIT_MAX_CONSTANTS) return -1;
-    if (m > GPU_FIT_MAX_NODES) return -2;
-    for (int i = 0; i < m; ++i)
-        if (!fit_opcode(f.op[i])) return -5;
-    if (4 * m > cap || f.nconst > cap_c) return -6;
-    for (int i = 0; i < m; ++i) {
-        uint32_t slot;
-        if (f.cslot[i] >= 0) slot = (uint32_t)f.cslot[i];
-        else if (f.op[i] == VAR) slot = (uint32_t)f.val[i];
-        else slot = 0xFFFFFFFFu;
-        const int a = arity(f.op[i]);
-        words[4 * i] = (uint32_t)f.op[i];
-        words[4 * i + 1] = a >= 1 ? (uint32_t)f.k0[i] : 0u;
-        words[4 * i + 2] = a >= 2 ? (uint32_t)f.k1[i] : 0u;
-        words[4 * i + 3] = slot;
-        if (f.cslot[i] >= 0) c0[f.cslot[i]] = f.val[i];
+    return plan_tree(t, words, cap, c0, cap_c, gauge, nconst, allow_no_constants);
+}
+
+/* rch_fit_plan of a postfix program (`len` words, up to its HALT) instead of
+   a pre-order tree: the same plan and the same rejections, -4 for a
+   malformed program. */
+int rch_fit_plan_postfix(const uint32_t *prog, int len, uint32_t *words, int cap, double *c0,
+                         int cap_c, int *gauge, int *nconst, int allow_no_constants)
+{
+    Node t;
+    if (!prog || len <= 0 || !load_postfix(prog, len, t)) return -4;
+    return plan_tree(t, words, cap, c0, cap_c, gauge, nconst, allow_no_constants);
+}
+
+/* rch_fit_plan_postfix of `nprog` programs, row i of prog[nprog][width]:
+   status[i] = its node count or rejection; its plan at words + 4 * width * i
+   (4 * width words), c0 + width * i, gauge + 2 * i and nconst[i]. Returns
+   the number of accepted programs, or -1 for a bad argument. */
+int rch_fit_plans_postfix(int nprog, const uint32_t *prog, int width, uint32_t *words,
+                          double *c0, int *gauge, int *nconst, int *status,
+                          int allow_no_constants)
+{
+    if (nprog < 0 || width <= 0 || !prog || !words || !c0 || !gauge || !nconst || !status)
+        return -1;
+    int ok = 0;
+    for (int i = 0; i < nprog; ++i) {
+        status[i] = rch_fit_plan_postfix(prog + (size_t)width * i, width,
+                                         words + (size_t)4 * width * i, 4 * width,
+                                         c0 + (size_t)width * i, width, gauge + 2 * i,
+                                         nconst + i, allow_no_constants);
+        if (status[i] >= 0) ++ok;
     }
-    /* fit/correlation.rs:83-128 `gauge_of`. */
-    gauge[0] = -1;
-    gauge[1] = -1;
-    const int root = m - 1;
-    if (f.op[root] == MUL) {
-        const int a = f.k0[root], b = f.k1[root];
-        if (f.cslot[a] >= 0 && f.cslot[b] < 0) gauge[0] = f.cslot[a];
-        else if (f.cslot[b] >= 0 && f.cslot[a] < 0) gauge[0] = f.cslot[b];
-    } else if (f.op[root] == ADD) {
-        const int ks[2] = {f.k0[root], f.k1[root]};
-        for (int side = 0; side < 2; ++side) {
-            const int mm = ks[side], bb = ks[1 - side];
-            if (f.op[mm] != MUL || f.cslot[bb] < 0) continue;
-            const int x = f.k0[mm], y = f.k1[mm];
-            int scale;
-            if (f.cslot[x] >= 0 && f.cslot[y] < 0) scale = f.cslot[x];
-            else if (f.cslot[y] >= 0 && f.cslot[x] < 0) scale = f.cslot[y];
-            else continue;
-            gauge[0] = scale;
-            gauge[1] = f.cslot[bb];
-            break;
-        }
-    }
-    *nconst = f.nconst;
-    return m;
+    return ok;
 }
 
 /* my-version/src/search.rs:3006-3031 `admission_count`: how many of an

@@ -13,8 +13,9 @@ host code:
            screened offspring that have constants, as many as
            rch_admission_count allows (everyone with constants at >= 2^20
            rows);
-  fit      the admitted programs, decoded into trees and flattened into fit
-           plans, through rc_fit_batch_fused (the fused adjoint LM);
+  fit      the admitted programs flattened into fit plans straight from
+           their words (only the accepted ones are decoded into trees),
+           through rc_fit_batch_fused (the fused adjoint LM);
   rescore  the fitted constants written back into their slots (a usable,
            finite answer only: fit/gpu.rs:103-105), the pool re-uploaded and
            rescored, so selection sees the fitted constants;
@@ -33,8 +34,8 @@ import numpy as np
 
 from . import expr as E
 from .device import GenomePool
-from .host import (DEFAULT_VARIATION_OPS, CompileError, GpuFitReject, compile_program,
-                   fit_status_usable, gpu_fit_plan, select_promoted, width_for)
+from .host import (DEFAULT_VARIATION_OPS, CompileError, compile_program,
+                   fit_status_usable, gpu_fit_plans_words, select_promoted, width_for)
 
 
 class FitRecord:
@@ -118,17 +119,16 @@ class GenerationLoop:
         admitted = select_promoted([self.pop] * self.islands, pending, err, self.cost, hasc,
                                    self.train_rows)
         slots, plans, trees = [], [], {}
-        for isl, j in admitted:
-            s = isl * self.pop + j
+        adm = [isl * self.pop + j for isl, j in admitted]
+        for s, plan in zip(adm, gpu_fit_plans_words(self.words[adm])):
+            if isinstance(plan, str):
+                continue
             t = self._tree(s)
             if t is None:
                 continue
-            try:
-                plans.append(gpu_fit_plan(t))
-                slots.append(s)
-                trees[s] = t
-            except GpuFitReject:
-                continue
+            plans.append(plan)
+            slots.append(s)
+            trees[s] = t
         records = []
         self.timing["host"] += 1e3 * (time.perf_counter() - t0)
         if plans:
