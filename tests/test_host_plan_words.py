@@ -110,3 +110,45 @@ def test_batched_plans_match_one_at_a_time(pkg, E):
             one = e.label
         assert _same(b, one), (b, one)
     assert H.gpu_fit_plans_words(np.zeros((0, 64), np.uint32)) == []
+
+
+def test_constants_written_into_words_match_the_compiled_fitted_tree(pkg, E):
+    """The generation loop writes a fit's constants straight into the pool
+    words; compiling the fitted tree and storing it in the slot (the tree
+    path) must give the same words, HALT padding included."""
+    H = pkg.host
+    W = importlib.import_module("the-rule-and-compass_b200.workloads")
+    trees, _, _ = W.fit_workload(150, 16, seed=11, nvars=3)
+    rng = np.random.Generator(np.random.PCG64(4))
+    width = 64
+    rows, want, cs, ks = [], [], [], []
+    for t in trees:
+        words, _ = pkg.compile_program(t)
+        if len(words) > width:
+            continue
+        slot = np.full(width, 255, np.uint32)
+        slot[: len(words)] = words
+        slot[len(words):] = rng.integers(0, 300, width - len(words))  # junk after HALT
+        try:
+            plan = H.gpu_fit_plan(E.from_postfix(slot))
+        except H.GpuFitReject:
+            continue
+        c = rng.normal(0.0, 3.0, plan.nconst) * 10.0 ** rng.integers(-8, 8, plan.nconst)
+        w2, _ = pkg.compile_program(plan.apply(E.from_postfix(slot), c))
+        ref = np.full(width, 255, np.uint32)
+        ref[: len(w2)] = w2
+        rows.append(slot)
+        want.append(ref)
+        cs.append(np.pad(c, (0, 20 - len(c))))
+        ks.append(plan.nconst)
+    assert len(rows) > 50
+    pool = np.ascontiguousarray(np.stack(rows))
+    st = H.set_postfix_constants(pool, np.arange(len(rows)), np.stack(cs), ks)
+    assert np.all(st >= np.asarray(ks))
+    assert np.array_equal(pool, np.stack(want))
+    # a malformed row and one with too few constants are left as they were
+    bad = np.ascontiguousarray(np.stack([np.full(width, E.ADD, np.uint32), rows[0].copy()]))
+    keep = bad.copy()
+    st = H.set_postfix_constants(bad, [0, 1], np.zeros((2, 25)), [0, 25])
+    assert list(st) == [-4, -3]
+    assert np.array_equal(bad, keep)

@@ -49,6 +49,11 @@ def lib():
                                             P(ctypes.c_uint32), P(ctypes.c_double),
                                             P(ctypes.c_int32), P(ctypes.c_int32),
                                             P(ctypes.c_int32), ctypes.c_int]
+        L.rch_set_postfix_constants_rows.restype = ctypes.c_int
+        L.rch_set_postfix_constants_rows.argtypes = [ctypes.c_int, P(ctypes.c_uint32),
+                                                     ctypes.c_int, P(ctypes.c_int32),
+                                                     P(ctypes.c_double), ctypes.c_int,
+                                                     P(ctypes.c_int32), P(ctypes.c_int32)]
         L.rch_admission_count.restype = ctypes.c_int
         L.rch_admission_count.argtypes = [ctypes.c_int, ctypes.c_longlong]
         L.rch_select_promoted.restype = ctypes.c_int
@@ -233,6 +238,29 @@ def gpu_fit_plans_words(words, allow_no_constants=False):
             k = int(nconst[i])
             res.append(GpuFitPlan(out[i, : 4 * m].copy(), c0[i, :k].copy(), gauge[i].copy(), k))
     return res
+
+
+def set_postfix_constants(words, rows, c, k):
+    """Write fitted constants into pool programs in place: row rows[r] of the
+    [programs, width] uint32 array `words` gets c[r, :k[r]] (f32-rounded) in
+    its constant operands, in the tree's pre-order slot order, and HALT after
+    its end, as compile_program of the fitted tree would emit it. Returns
+    each row's status (its constant count, or -4 malformed, -2 stack beyond
+    the host limit, -3 fewer constants than k: that row is left as it was)."""
+    assert words.dtype == np.uint32 and words.flags.c_contiguous
+    rows = np.ascontiguousarray(rows, np.int32)
+    n = len(rows)
+    c = np.ascontiguousarray(c, np.float64).reshape(n, -1) if n else np.zeros((0, 1))
+    k = np.ascontiguousarray(k, np.int32)
+    status = np.zeros(n, np.int32)
+    if n == 0:
+        return status
+    if lib().rch_set_postfix_constants_rows(n, _p(words, ctypes.c_uint32), words.shape[1],
+                                            _p(rows, ctypes.c_int32), _p(c, ctypes.c_double),
+                                            c.shape[1], _p(k, ctypes.c_int32),
+                                            _p(status, ctypes.c_int32)) < 0:
+        raise RuntimeError("rch_set_postfix_constants_rows failed")
+    return status
 
 
 def pack_plans(plans, kmax=None):

@@ -348,6 +348,62 @@ int rch_fit_plans_postfix(int nprog, const uint32_t *prog, int width, uint32_t *
     return ok;
 }
 
+/* Writes c[0..k) into the constant operands of a postfix program in place
+   (the i-th CONST word's operand becomes the f32 rounding of c[i], the
+   order of the tree's pre-order constant slots), which is what compiling the
+   tree with those constants emits for a program without inverse
+   hyperbolics. Returns the number of constants, -4 for a malformed program,
+   -2 when its stack grows past the host limit (the compiler refuses such a
+   program), -3 when it holds fewer than k constants; the words change only
+   on success, when those after the HALT are reset to HALT (as a caller
+   writing the compiled program into a fixed-width slot leaves them). */
+int rch_set_postfix_constants(uint32_t *w, int len, const double *c, int k)
+{
+    if (!w || len <= 0 || k < 0 || (k > 0 && !c)) return -4;
+    std::vector<int> at;
+    int depth = 0, peak = 0, i = 0;
+    for (;;) {
+        if (i >= len) return -4;
+        const int op = (int)w[i++];
+        if (op == HALT) break;
+        if (op == CONST || op == VAR) {
+            if (i >= len) return -4;
+            if (op == CONST) at.push_back(i);
+            ++i;
+            peak = std::max(peak, ++depth);
+            continue;
+        }
+        const int a = arity(op);
+        if (!known(op) || op == ASINH || op == ACOSH || op == ATANH || depth < a) return -4;
+        depth -= a - 1;
+    }
+    if (depth != 1) return -4;
+    if (peak > HOST_MAX_STACK) return -2;
+    if ((int)at.size() < k) return -3;
+    for (int j = 0; j < k; ++j) {
+        const float f = (float)c[j];
+        memcpy(&w[at[j]], &f, 4);
+    }
+    for (int j = i; j < len; ++j) w[j] = HALT;
+    return (int)at.size();
+}
+
+/* rch_set_postfix_constants on rows[r] of words[][width] with c + kmax * r
+   and k[r] constants, for r < nrec; status[r] gets each answer. Returns the
+   number of rows written. */
+int rch_set_postfix_constants_rows(int nrec, uint32_t *words, int width, const int *rows,
+                                   const double *c, int kmax, const int *k, int *status)
+{
+    if (nrec < 0 || width <= 0 || !words || !rows || !c || !k || !status) return -1;
+    int done = 0;
+    for (int r = 0; r < nrec; ++r) {
+        status[r] = rch_set_postfix_constants(words + (size_t)width * rows[r], width,
+                                              c + (size_t)kmax * r, k[r]);
+        if (status[r] >= 0) ++done;
+    }
+    return done;
+}
+
 /* my-version/src/search.rs:3006-3031 `admission_count`: how many of an
    island's offspring enter the fitted batch. From 2^20 training rows every
    candidate with constants; below, a quarter of the island floored at 32 and

@@ -16,9 +16,10 @@ host code:
   fit      the admitted programs flattened into fit plans straight from
            their words (only the accepted ones are decoded into trees),
            through rc_fit_batch_fused (the fused adjoint LM);
-  rescore  the fitted constants written back into their slots (a usable,
-           finite answer only: fit/gpu.rs:103-105), the pool re-uploaded and
-           rescored, so selection sees the fitted constants;
+  rescore  the fitted constants written back into their slots' words (a
+           usable, finite answer only: fit/gpu.rs:103-105; the words the
+           compiled fitted tree would be), the pool re-uploaded and rescored,
+           so selection sees the fitted constants;
   vary     rc_pool_vary builds the next generation from the scores
            (tournament, crossover, mutation, dedup: postfix.rs:511-567).
 
@@ -34,19 +35,26 @@ import numpy as np
 
 from . import expr as E
 from .device import GenomePool
-from .host import (DEFAULT_VARIATION_OPS, CompileError, compile_program,
-                   fit_status_usable, gpu_fit_plans_words, select_promoted, width_for)
+from .host import (DEFAULT_VARIATION_OPS, fit_status_usable, gpu_fit_plans_words,
+                   select_promoted, set_postfix_constants, width_for)
 
 
 class FitRecord:
-    """One admitted candidate of one generation: its slot, the tree it was
-    fitted from, its plan, and the device's answer."""
+    """One admitted candidate of one generation: its slot, the program words
+    it was fitted from (and their tree, decoded when first asked for), its
+    plan, and the device's answer."""
 
-    __slots__ = ("slot", "tree", "plan", "c", "loss", "status")
+    __slots__ = ("slot", "words", "_tree", "plan", "c", "loss", "status")
 
-    def __init__(self, slot, tree, plan, c, loss, status):
-        self.slot, self.tree, self.plan = slot, tree, plan
+    def __init__(self, slot, words, plan, c, loss, status):
+        self.slot, self.words, self._tree, self.plan = slot, words, None, plan
         self.c, self.loss, self.status = c, loss, status
+
+    @property
+    def tree(self):
+        if self._tree is None:
+            self._tree = E.from_postfix(self.words)
+        return self._tree
 
     def fitted(self):
         return self.plan.apply(self.tree, self.c[: self.plan.nconst])
@@ -82,12 +90,6 @@ class GenerationLoop:
         self.gen = 0
         self.device_ms = 0.0
 
-    def _tree(self, s):
-        try:
-            return E.from_postfix(self.words[s])
-        except ValueError:
-            return None
-
     @staticmethod
     def _has_constant(w):
         """Whether a postfix program pushes a constant (a CONST opcode word,
@@ -118,17 +120,12 @@ class GenerationLoop:
         pending = [(i // self.pop, i % self.pop) for i in range(n)]
         admitted = select_promoted([self.pop] * self.islands, pending, err, self.cost, hasc,
                                    self.train_rows)
-        slots, plans, trees = [], [], {}
+        slots, plans = [], []
         adm = [isl * self.pop + j for isl, j in admitted]
         for s, plan in zip(adm, gpu_fit_plans_words(self.words[adm])):
-            if isinstance(plan, str):
-                continue
-            t = self._tree(s)
-            if t is None:
-                continue
-            plans.append(plan)
-            slots.append(s)
-            trees[s] = t
+            if not isinstance(plan, str):
+                plans.append(plan)
+                slots.append(s)
         records = []
         self.timing["host"] += 1e3 * (time.perf_counter() - t0)
         if plans:
@@ -136,19 +133,15 @@ class GenerationLoop:
             self.device_ms += ms
             self.timing["fit"] += ms
             t0 = time.perf_counter()
+            back, kc = [], []
             for k, (s, pl) in enumerate(zip(slots, plans)):
-                rec = FitRecord(s, trees[s], pl, c[k].copy(), float(loss[k]), int(status[k]))
+                rec = FitRecord(s, self.words[s].copy(), pl, c[k].copy(), float(loss[k]),
+                                int(status[k]))
                 records.append(rec)
-                if not fit_status_usable(rec.status) or \
-                        not np.all(np.isfinite(rec.c[: pl.nconst])):
-                    continue
-                try:
-                    w, _ = compile_program(rec.fitted())
-                except CompileError:
-                    continue
-                if len(w) <= self.width:
-                    self.words[s, :] = E.HALT
-                    self.words[s, : len(w)] = w
+                if fit_status_usable(rec.status) and np.all(np.isfinite(rec.c[: pl.nconst])):
+                    back.append(k)
+                    kc.append(pl.nconst)
+            set_postfix_constants(self.words, np.asarray(slots, np.int32)[back], c[back], kc)
             self.pool.upload(self.cur, self.words)
             self.timing["host"] += 1e3 * (time.perf_counter() - t0)
             err, _, ms = self.pool.score(self.cur, self.score_kind)
