@@ -57,7 +57,8 @@ static_assert(sizeof(RcIns) == 8, "RcIns is 8 bytes");
    count, fills `nslots` with the number of spill slots it uses, and emits a
    single K_NAN instruction for a program the device must score as NaN on
    every row (stack under/overflow, a missing HALT, a variable column >= v,
-   or a program longer than RC_MAX_INS). */
+   or a program longer than RC_MAX_INS). `out` needs room for max(nwords, 1)
+   instructions (at most one per word is written). */
 int rc_decode_postfix(const uint32_t *words, size_t nwords, int v, RcIns *out, int *nslots);
 
 /* ---- context ---------------------------------------------------------- */

@@ -62,9 +62,10 @@ int rc_decode_postfix(const uint32_t *words, size_t nwords, int v, RcIns *out, i
 {
     /* Walk the words exactly like the reference's device loop (eval.cu:404-573)
        with a symbolic stack depth; any condition under which the reference
-       returns NaN for every row makes the program a single K_NAN. */
-    std::vector<RcIns> ins;
-    ins.reserve(64);
+       returns NaN for every row makes the program a single K_NAN. The
+       instructions are written straight into `out` (at most one per word,
+       so `nwords` of room; a word-free program needs one). */
+    int n = 0;
     int depth = 0, maxslot = -1;
     bool ok = true, halted = false;
     size_t i = 0;
@@ -84,12 +85,12 @@ int rc_decode_postfix(const uint32_t *words, size_t nwords, int v, RcIns *out, i
             in.imm = a; /* f32 bits of a constant, or the column of a variable */
             if (depth >= 1) maxslot = std::max(maxslot, depth - 1);
             ++depth;
-            ins.push_back(in);
+            out[n++] = in;
         } else if (w == OP_HALT) {
             if (depth < 1) { ok = false; break; }
             in.kind = K_HALT;
             in.arg = depth == 1 ? 1 : 0;
-            ins.push_back(in);
+            out[n++] = in;
             halted = true;
             break;
         } else if (is_binary(w)) {
@@ -100,8 +101,8 @@ int rc_decode_postfix(const uint32_t *words, size_t nwords, int v, RcIns *out, i
             --depth;
             /* Fuse "push x; op" into one instruction: the push's spill slot is
                exactly the slot the operator would pop. */
-            if (!ins.empty() && fusable(w)) {
-                RcIns &prev = ins.back();
+            if (n > 0 && fusable(w)) {
+                RcIns &prev = out[n - 1];
                 if ((prev.kind == K_PUSH_VAR || prev.kind == K_PUSH_CONST) && prev.spill != 0xff &&
                     prev.spill == in.arg) {
                     uint8_t kind = prev.kind == K_PUSH_VAR ? K_BIN_V : K_BIN_C;
@@ -111,13 +112,13 @@ int rc_decode_postfix(const uint32_t *words, size_t nwords, int v, RcIns *out, i
                     continue;
                 }
             }
-            ins.push_back(in);
+            out[n++] = in;
         } else if (w == OP_IF) {
             if (depth < 3) { ok = false; break; }
             in.kind = K_IF;
             in.arg = (uint8_t)(depth - 3);
             depth -= 2;
-            ins.push_back(in);
+            out[n++] = in;
         } else {
             /* Unary, including unknown codes, which evaluate to NaN
                (eval.cu:567). */
@@ -125,10 +126,10 @@ int rc_decode_postfix(const uint32_t *words, size_t nwords, int v, RcIns *out, i
             in.kind = K_UNARY;
             in.op = (uint8_t)(w > 255 ? 255 : w);
             if (w > 255 || w == OP_HALT) in.op = 254; /* unknown: NaN */
-            ins.push_back(in);
+            out[n++] = in;
         }
     }
-    if (!ok || !halted || (int)ins.size() > RC_MAX_INS) {
+    if (!ok || !halted || n > RC_MAX_INS) {
         RcIns bad;
         memset(&bad, 0, sizeof(bad));
         bad.kind = K_NAN;
@@ -137,9 +138,8 @@ int rc_decode_postfix(const uint32_t *words, size_t nwords, int v, RcIns *out, i
         *nslots = 0;
         return 1;
     }
-    memcpy(out, ins.data(), sizeof(RcIns) * ins.size());
     *nslots = maxslot + 1;
-    return (int)ins.size();
+    return n;
 }
 
 /* ---- host launcher -------------------------------------------------- */
@@ -226,13 +226,19 @@ float rc_score_run(RcCtx *c, const uint32_t *words, const uint32_t *off, int wid
     RcStats *st = &c->stats;
     const double t_begin = rc_now_ms();
 
-    /* 1. decode */
-    std::vector<RcIns> ins;
-    ins.reserve((size_t)nprog * 16);
+    /* 1. decode, each program straight into its place (room for one
+       instruction per word) */
     std::vector<int> ins_off(nprog + 1, 0);
     std::vector<int> nslots(nprog, 0);
     std::vector<int> opw(nprog, 0);
-    std::vector<RcIns> local;
+    size_t room = 0;
+    for (int p = 0; p < nprog; ++p) {
+        const size_t b = width > 0 ? (size_t)p * (size_t)width : off[p];
+        const size_t e = width > 0 ? b + (size_t)width : off[p + 1];
+        room += std::max<size_t>(e > b ? e - b : 0, 1);
+    }
+    std::vector<RcIns> ins(room);
+    size_t pos = 0;
     for (int p = 0; p < nprog; ++p) {
         size_t b = width > 0 ? (size_t)p * (size_t)width : off[p];
         size_t e = width > 0 ? b + (size_t)width : off[p + 1];
@@ -242,14 +248,14 @@ float rc_score_run(RcCtx *c, const uint32_t *words, const uint32_t *off, int wid
         for (size_t q = b; q < e && words[q] != OP_HALT; ++ops)
             q += (words[q] == OP_CONST || words[q] == OP_VAR) ? 2 : 1;
         opw[p] = ops + 2;
-        local.resize(std::max<size_t>(e - b, 1) + 1);
         int ns = 0;
-        const int cnt = rc_decode_postfix(words + b, e - b, c->v, local.data(), &ns);
-        ins_off[p] = (int)ins.size();
-        ins.insert(ins.end(), local.begin(), local.begin() + cnt);
+        const int cnt = rc_decode_postfix(words + b, e - b, c->v, ins.data() + pos, &ns);
+        ins_off[p] = (int)pos;
+        pos += (size_t)cnt;
         nslots[p] = ns;
     }
-    ins_off[nprog] = (int)ins.size();
+    ins.resize(pos);
+    ins_off[nprog] = (int)pos;
 
     /* 2. bucket by depth; longest program first */
     Bucket bk[2];
@@ -1069,9 +1075,11 @@ extern "C" int rc_autotune(void *ctx, const unsigned int *prog, const unsigned i
     std::vector<uint32_t> words[2], offs[2];
     offs[0].push_back(0);
     offs[1].push_back(0);
-    std::vector<RcIns> tmp(RC_MAX_INS);
+    std::vector<RcIns> tmp;
     for (int i = 0; i < nprog; ++i) {
         int ns = 0;
+        /* (room for one instruction per word) */
+        tmp.resize(std::max<size_t>(off[i + 1] > off[i] ? off[i + 1] - off[i] : 0, 1));
         const int cnt = rc_decode_postfix(prog + off[i], off[i + 1] - off[i], c->v, tmp.data(), &ns);
         if (cnt <= 0) continue;
         const int b = ns <= RC_SHALLOW_SLOTS ? 0 : 1;
