@@ -920,14 +920,16 @@ def bench_c1(pkg, W, gens=200, sample_every=20):
                       "error, 8 LM iterations, max complexity 30"}
 
 
-def bench_c5gen(args, pkg, W):
+def bench_c5gen(args, pkg, W, agree=16):
     """One generation of the heavy-tailed configuration at its stated size:
     16 islands x pop 1000 over N = 4,194,304 rows x 10 features, absolute
     error (screen and rescore with the absolute score, L1 IRLS fit with up to
     20 constants, 20 iterations). At >= 2^20 rows every offspring with
     constants is admitted. Reports the device time of each step (screen, fit,
-    rescore, vary) and the host time between them, and the plain
-    one-candidate-per-launch fit of 16 of the admitted candidates."""
+    rescore, vary) and the host time between them, the plain
+    one-candidate-per-launch fit of 16 of the admitted candidates, and (with
+    `agree`) a seeded sample of the fitted candidates against the oracle's
+    CPU IRLS fit of the same candidates on the same rows."""
     islands = args.P or 16
     N = args.N or (1 << 22)
     x, y = W.heavy_tail_data(N, seed=0)
@@ -944,7 +946,14 @@ def bench_c5gen(args, pkg, W):
     ev.close()
     fused = len(recs) / (loop.timing["fit"] / 1e3)
     plain = len(plans) / (pms / 1e3)
-    return {"generation_s": wall, "admitted": len(recs), "step_ms": loop.timing,
+    out = {}
+    if agree and recs:
+        rng = np.random.Generator(np.random.PCG64(23))
+        pick = [recs[i] for i in np.sort(rng.choice(len(recs), min(agree, len(recs)),
+                                                     replace=False))]
+        out["agreement"] = oracle_fit_agreement(pick, np.ascontiguousarray(x.reshape(-1)), N,
+                                                10, y, 20, os.cpu_count() or 1, metric=4)
+    return {"generation_s": wall, "admitted": len(recs), "step_ms": loop.timing, **out,
             "fit_fused": fused, "fit_plain": plain, "fused_over_plain": fused / plain,
             "status_histogram": np.bincount([r.status for r in recs], minlength=9).tolist(),
             "config": f"one generation, {islands} islands x pop 1000, N={N} rows x 10 "
@@ -1017,6 +1026,10 @@ def secondary(args, rank, world, local, pkg, W, flushbuf, peaks, line):
     line.update(c1_generations_per_s=c1["generations_per_s"],
                 c1_fitted_candidates_per_s=c1["fitted_candidates_per_s"],
                 c1_agreement=c1["agreement"]["within_1e-6_or_better"])
+    g5 = line["c5_generation"] = bench_c5gen(argparse.Namespace(P=0, N=0), pkg, W)
+    line.update(c5gen_generation_s=g5["generation_s"], c5gen_fit_fused=g5["fit_fused"],
+                c5gen_fused_over_plain=g5["fused_over_plain"],
+                c5gen_agreement=g5.get("agreement", {}).get("within_1e-6_or_better"))
     vy = line["vary"] = bench_vary(args, rank, pkg, flushbuf, 5, 3)
     line.update(vary_children=vy["value"], vary_children_e2e=vy["e2e"],
                 vary_same_as_cpu=vy["same_as_cpu"], vary_cpu_baseline=_cpu(vy))
