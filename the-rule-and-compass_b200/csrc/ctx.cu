@@ -8,11 +8,14 @@
  * :3469-3512 the arena report). Rows are stored column-major and padded to
  * RC_ROW_PAD rows so every kernel reads whole aligned float4/double2 groups.
  */
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <ctime>
+#include <map>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -23,6 +26,35 @@ double rc_now_ms()
     struct timespec ts;
     clock_gettime(CLOCK_MONOTONIC, &ts);
     return (double)ts.tv_sec * 1e3 + (double)ts.tv_nsec / 1e6;
+}
+
+/* Raise a kernel's dynamic shared-memory limit on the current device to at
+   least `bytes`. The limit only ever grows: every path and context that
+   launches the kernel on the device shares it, and lowering it for a small
+   launch would make a larger one (queued by another context, or held in a
+   captured graph) fail. It is never set below 48 KB (the default a launch
+   that needs no raise relies on), so a kernel with static shared memory
+   gets room for both. Returns 0, or -1 when the device refuses the size. */
+int rc_raise_smem(const void *fn, size_t bytes)
+{
+    bytes = std::max(bytes, (size_t)48 * 1024);
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return -1;
+    }
+    static std::mutex mu;
+    static std::map<std::pair<const void *, int>, size_t> raised;
+    std::lock_guard<std::mutex> lock(mu);
+    size_t &cur = raised[std::make_pair(fn, dev)];
+    if (bytes <= cur) return 0;
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) !=
+        cudaSuccess) {
+        cudaGetLastError();
+        return -1;
+    }
+    cur = bytes;
+    return 0;
 }
 
 size_t rc_take(size_t *cur, size_t bytes)

@@ -2298,8 +2298,7 @@ SweepLaunch icost_launch(RcCtx *c, const XPrep &x)
     s.opk = FOP_ICOST;
     s.smem = 8 * (size_t)((x.maxins + 1) & ~1) + 8 * FT_MAX_CONST +
              8 * (size_t)FT_ITHREADS * (x.slots + x.tape + c->v) + 8 * (size_t)FT_ITHREADS;
-    if (s.smem > 48 * 1024)
-        cudaFuncSetAttribute(s.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
+    rc_raise_smem(s.fn, s.smem);
     s.grid = c->sm_count * occupancy(s.fn, FT_ITHREADS, s.smem);
     s.threads = FT_ITHREADS;
     return s;
@@ -2312,8 +2311,7 @@ SweepLaunch sweep_launch(RcCtx *c, int mrec, int tcap, int Wmax)
     s.fn = (const void *)ft_jac_sweep<OPK, FT_ITHREADS>;
     s.opk = OPK;
     s.smem = ft_ijac_smem(mrec, tcap, Wmax, FT_ITHREADS);
-    if (s.smem > 48 * 1024)
-        cudaFuncSetAttribute(s.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
+    rc_raise_smem(s.fn, s.smem);
     s.grid = c->sm_count * occupancy(s.fn, FT_ITHREADS, s.smem);
     s.threads = FT_ITHREADS;
     return s;
@@ -2346,12 +2344,7 @@ IjacSplit ijac_split(RcCtx *c, const FitPrep &b, int Wmax)
     const void *fn = (const void *)ft_jac_sweep<FOP_IJACS, FT_ITHREADS>;
     /* occupancy queries up to the largest layout the split can choose */
     const size_t smax = ft_ijac_smem(b.mmax, out.tape, Wmax, FT_ITHREADS);
-    if (smax > 48 * 1024 &&
-        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax) !=
-            cudaSuccess) {
-        cudaGetLastError();
-        return out;
-    }
+    if (rc_raise_smem(fn, smax) != 0) return out;
     std::sort(ms.begin(), ms.end());
     auto occ = [&](int mrec, int tcap) {
         return (double)occupancy(fn, FT_ITHREADS, ft_ijac_smem(mrec, tcap, Wmax, FT_ITHREADS));
@@ -2392,8 +2385,7 @@ SweepLaunch sweep4_launch(RcCtx *c, const FitPrep &b, int Wmax)
     const size_t reg = OPK != bk ? b.asm_reg[ft_kind_cls(OPK)]
                        : (bk == FOP_CASM ? b.asm_region : b.asm_reg[0]);
     s.smem = ft_sweep4_smem(OPK, b.fmaxins, b.fslots, reg, T);
-    if (s.smem > 48 * 1024)
-        cudaFuncSetAttribute(s.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
+    rc_raise_smem(s.fn, s.smem);
     s.grid = c->sm_count * occupancy(s.fn, T, s.smem);
     s.threads = T;
     return s;
@@ -3023,11 +3015,7 @@ int rc_grad_batch(void *ctx, const unsigned int *prog, const unsigned int *off, 
         const size_t smem = 8 * (size_t)((b.fmaxins + 1) & ~1) + 4 * FT_MAX_CONST +
                             4 * NR * 32 * (size_t)(b.fslots + b.ftape) +
                             4 * (size_t)(b.pmax > 0 ? b.pmax : 1) * (NR * 32 + 4);
-        if (cudaFuncSetAttribute(ft_grad4_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem) != cudaSuccess) {
-            cudaGetLastError();
-            return -1;
-        }
+        if (rc_raise_smem((const void *)ft_grad4_kernel, smem) != 0) return -1;
         rc->launches += 1;
         ft_grad4_kernel<<<nprog * ntiles, 32, smem, rc->s>>>(
             a, row0, nrows, ntiles, reinterpret_cast<float *>(dev + o_val),
@@ -3038,11 +3026,7 @@ int rc_grad_batch(void *ctx, const unsigned int *prog, const unsigned int *off, 
     const size_t smem = sizeof(uint4) * mmax + sizeof(float) * FT_MAX_CONST +
                         sizeof(float) * (size_t)mmax * T + sizeof(double) * FT_MAX_CONST * T +
                         sizeof(float) * (size_t)rc->v * T + 64;
-    if (cudaFuncSetAttribute(ft_grad_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem) != cudaSuccess) {
-        cudaGetLastError();
-        return -1;
-    }
+    if (rc_raise_smem((const void *)ft_grad_kernel<128>, smem) != 0) return -1;
     rc->launches += 1;
     ft_grad_kernel<128><<<nprog * ntiles, T, smem, rc->s>>>(
         a, want, row0, nrows, ntiles, reinterpret_cast<float *>(dev + o_val),
@@ -3104,12 +3088,7 @@ float rc_implicit_score_batch(void *ctx, const unsigned int *prog, const unsigne
     using V4 = FiV<float, NR>::V4;
     const size_t smem = 8 * (size_t)((maxins + 1) & ~1) + sizeof(float) * FT_MAX_CONST +
                         sizeof(V4) * (size_t)(slots + ntape + rc->v) * T + sizeof(double) * T;
-    if (smem > 48 * 1024 &&
-        cudaFuncSetAttribute(ft_implicit_score_x<128, NR>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
-        cudaGetLastError();
-        return -1.0f;
-    }
+    if (rc_raise_smem((const void *)ft_implicit_score_x<128, NR>, smem) != 0) return -1.0f;
     cudaEventRecord(rc->t0, rc->s);
     rc->launches += 2;
     ft_implicit_score_x<128, NR><<<nprog * ntiles, T, smem, rc->s>>>(

@@ -475,8 +475,7 @@ unsigned long long rs_sort(const RsBuffers &b, int nseg, int n, int *abort_flag,
 {
     const int ntiles = (n + RS_TILE - 1) / RS_TILE;
     const int nblk = (ntiles + RS_COUNT_TILES - 1) / RS_COUNT_TILES;
-    cudaFuncSetAttribute(rs_pass<VALS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)rs_pass_smem<VALS>());
+    rc_raise_smem((const void *)rs_pass<VALS>, rs_pass_smem<VALS>());
     cudaMemsetAsync(b.state, 0, sizeof(u64) * 256 * (size_t)ntiles * (size_t)nseg, s);
     cudaMemsetAsync(b.ticket, 0, sizeof(int) * RS_PASSES, s);
     if (!counted) {
@@ -987,11 +986,7 @@ float rc_rank_score_batch(void *ctx, const unsigned int *prog, const unsigned in
     cudaMemsetAsync(d_status, 0, sizeof(int) * nsegs, c->s);
     cudaMemsetAsync(d_abort, 0, sizeof(int), c->s);
     const size_t smem = key_smem(sp);
-    /* (every call: the kernel's static digit table counts against the
-       default dynamic limit) */
-    if (cudaFuncSetAttribute(rk_keys<RK_RANK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem) != cudaSuccess)
-        return -1.0f;
+    if (rc_raise_smem((const void *)rk_keys<RK_RANK>, smem) != 0) return -1.0f;
     const int ktiles = (n + RK_TILE - 1) / RK_TILE;
     const int ntiles = (n + RS_TILE - 1) / RS_TILE;
     cudaEventRecord(c->t0, c->s);
@@ -1072,11 +1067,7 @@ float rc_order_stat_score_batch(void *ctx, const unsigned int *prog, const unsig
     cudaMemsetAsync(d_status, 0, sizeof(int) * nsegs, c->s);
     cudaMemsetAsync(d_abort, 0, sizeof(int), c->s);
     const size_t smem = key_smem(sp);
-    /* (every call: the kernel's static digit table counts against the
-       default dynamic limit) */
-    if (cudaFuncSetAttribute(rk_keys<RK_ABS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem) != cudaSuccess)
-        return -1.0f;
+    if (rc_raise_smem((const void *)rk_keys<RK_ABS>, smem) != 0) return -1.0f;
     const int ktiles = (n + RK_TILE - 1) / RK_TILE;
     cudaEventRecord(c->t0, c->s);
     for (int s0 = 0; s0 < nsegs; s0 += wseg) {
@@ -1144,10 +1135,7 @@ float rc_max_scan_batch(void *ctx, const unsigned int *prog, const unsigned int 
     const size_t smem = 8 * (size_t)((sp.b.fmaxins + 1) & ~1) + 8 * FT_MAX_CONST +
                         8 * (size_t)MX_T * (sp.b.fslots + sp.b.ftape + pmax);
     if (smem > 200 * 1024) return -1.0f;
-    if (smem > 48 * 1024 &&
-        cudaFuncSetAttribute(mx_scan, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-            cudaSuccess)
-        return -1.0f;
+    if (rc_raise_smem((const void *)mx_scan, smem) != 0) return -1.0f;
     cudaEventRecord(c->t0, c->s);
     c->launches += 1;
     mx_scan<<<nsegs, MX_T, smem, c->s>>>(

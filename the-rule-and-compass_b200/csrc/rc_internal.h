@@ -158,6 +158,10 @@ double rc_now_ms();
 /* Grow the per-call device / pinned regions (high-water mark, counted). */
 int rc_reserve(RcCtx *c, size_t dev_bytes, size_t host_bytes);
 size_t rc_take(size_t *cur, size_t bytes);
+/* Raise a kernel's dynamic shared-memory limit on the current device to at
+   least `bytes`; the limit only ever grows (shared by every context and
+   path). Returns 0, or -1 when the device refuses the size. */
+int rc_raise_smem(const void *fn, size_t bytes);
 /* Make sure the f64 twins exist (cast from the f32 rows when the caller never
    uploaded exact rows). */
 int rc_ensure_f64(RcCtx *c);

@@ -186,31 +186,9 @@ void launch_score_kernel(int T, bool track, int grid, size_t smem, cudaStream_t 
     }
 }
 
-/* Raise a kernel's dynamic shared-memory limit to at least `smem` on the
-   current device. The limit only ever grows: every path that launches the
-   kernel shares it, and lowering it for a small launch would make a larger
-   launch on another path fail. */
-int set_smem(const void *fn, size_t smem)
-{
-    if (smem <= 48 * 1024) return 0;
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) {
-        cudaGetLastError();
-        return -1;
-    }
-    static std::mutex mu;
-    static std::map<std::pair<const void *, int>, size_t> raised;
-    std::lock_guard<std::mutex> lock(mu);
-    size_t &cur = raised[std::make_pair(fn, dev)];
-    if (smem <= cur) return 0;
-    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-        cudaSuccess) {
-        cudaGetLastError();
-        return -1;
-    }
-    cur = smem;
-    return 0;
-}
+/* The kernel's dynamic shared-memory limit raised to at least `smem`
+   (monotone, shared with every other path: rc_raise_smem). */
+int set_smem(const void *fn, size_t smem) { return rc_raise_smem(fn, smem); }
 
 size_t lane_smem(int nslots) { return (size_t)nslots * LANE_T * 16 + RC_MAX_INS * sizeof(RcIns) + LANE_T * 8; }
 
