@@ -70,6 +70,42 @@ struct RcPending {
     cudaEvent_t done;
 };
 
+/* A page-locked host array of words: device-to-host copies into it run at
+   full speed and need no staging. */
+struct RcPinnedWords {
+    uint32_t *p = nullptr;
+    size_t n = 0;
+    uint32_t *data() { return p; }
+    const uint32_t *data() const { return p; }
+    /* `count` words, all `v` (reallocated when larger); 0, or -1 when the
+       allocation fails (the array is then empty). */
+    int assign(size_t count, uint32_t v)
+    {
+        if (count > n) {
+            release();
+            if (cudaHostAlloc((void **)&p, sizeof(uint32_t) * (count ? count : 1),
+                              cudaHostAllocPortable) != cudaSuccess) {
+                cudaGetLastError();
+                p = nullptr;
+                return -1;
+            }
+            n = count;
+        }
+        for (size_t i = 0; i < count; ++i) p[i] = v;
+        return 0;
+    }
+    void release()
+    {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        n = 0;
+    }
+    RcPinnedWords() = default;
+    RcPinnedWords(const RcPinnedWords &) = delete;
+    RcPinnedWords &operator=(const RcPinnedWords &) = delete;
+    ~RcPinnedWords() { release(); }
+};
+
 struct RcCtx {
     int n;      /* rows */
     int v;      /* columns */
@@ -101,8 +137,9 @@ struct RcCtx {
     std::vector<uint32_t> prog_off;
     int nprog;
 
-    /* fixed-stride pool */
-    std::vector<uint32_t> pool_host[2];
+    /* fixed-stride pool (host mirrors page-locked: the new pool comes back
+       every generation) */
+    RcPinnedWords pool_host[2];
     unsigned int *d_pool[2];
     int pool_cap;
     int pool_width;

@@ -600,7 +600,10 @@ int rc_pool_reserve(void *ctx, int nprog, int width)
         }
         c->alloc_calls++;
         if (c->warm) c->steady_alloc_calls++;
-        c->pool_host[i].assign((size_t)nprog * width, (uint32_t)OP_HALT);
+        if (c->pool_host[i].assign((size_t)nprog * width, (uint32_t)OP_HALT) != 0) {
+            c->stats.failed = 1;
+            return -1;
+        }
     }
     c->pool_cap = nprog;
     c->pool_width = width;

@@ -375,9 +375,13 @@ extern "C" float rc_pool_vary(void *ctx, int which, int islands, int pop, int wi
                                        c->d_pool[b], c->d_pool[b ^ 1]);
     c->launches += 1;
     cudaEventRecord(c->t1, c->s);
-    /* the host mirror of the new pool, which the pool scorers read */
+    /* the host mirror of the new pool, which the pool scorers read, and the
+       caller's copy, both straight from the device */
     cudaMemcpyAsync(c->pool_host[b ^ 1].data(), c->d_pool[b ^ 1], sizeof(uint32_t) * total,
                     cudaMemcpyDeviceToHost, c->s);
+    if (out_words)
+        cudaMemcpyAsync(out_words, c->d_pool[b ^ 1], sizeof(uint32_t) * total,
+                        cudaMemcpyDeviceToHost, c->s);
     if (rc_finish(c) != 0) return -1.0f;
     for (int k = 0; k < nslots; ++k) {
         if (out_len) out_len[k] = choice[k].len;
@@ -385,7 +389,6 @@ extern "C" float rc_pool_vary(void *ctx, int which, int islands, int pop, int wi
         if (out_hash) out_hash[k] = choice[k].hash;
         if (out_err) out_err[k] = choice[k].err;
     }
-    if (out_words) memcpy(out_words, c->pool_host[b ^ 1].data(), sizeof(uint32_t) * total);
     float ms = -1.0f;
     cudaEventElapsedTime(&ms, c->t0, c->t1);
     return ms;
