@@ -91,3 +91,24 @@ def test_benchmark_sized_generation(pkg, O):
     """One generation of 16 islands x 1000 (the heavy-tailed configuration's
     population), width 64."""
     _case(pkg, O, 16, 1000, 64, 10, 30, 2024, 1, err_fn=lambda i: ((i * 7919) % 10007) / 10007.0)
+
+
+def test_a_parent_that_is_not_a_program_fails_the_call(pkg, O):
+    """A pool slot that is not a valid program (here an operator with no
+    operands) fails the whole call: nothing is built from it, and the pool
+    still serves the next, valid call."""
+    islands, pop, width = 2, 50, 24
+    w, err = _parents(pkg, O, islands, pop, width, 2, 10, 4, 3, lambda i: float(i))
+    bad = w.copy()
+    bad[17, :] = HALT
+    bad[17, 0] = 2  # ADD with an empty stack
+    ev = _evaluator(pkg)
+    pool = pkg.GenomePool(ev, islands, pop, width)
+    pool.upload(0, bad)
+    with pytest.raises(pkg.DeviceError):
+        pool.vary(0, err, 1, 2, 10, 4, pkg.DEFAULT_VARIATION_OPS)
+    pool.upload(0, w)
+    dev = pool.vary(0, err, 1, 2, 10, 4, pkg.DEFAULT_VARIATION_OPS)
+    ref = O.next_generation(w, err, islands, pop, width, 2, 10, 4, 1, pkg.DEFAULT_VARIATION_OPS)
+    _same(dev, ref)
+    ev.close()

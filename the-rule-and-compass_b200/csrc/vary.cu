@@ -37,15 +37,21 @@ namespace {
    not a valid program), hash. */
 __global__ void __launch_bounds__(RV_T) rv_parents(const uint32_t *__restrict__ words, int width,
                                                    int nslots, uint16_t *len, int *cost,
-                                                   unsigned long long *hash)
+                                                   uint16_t *cost16, unsigned long long *hash,
+                                                   int *bad)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nslots) return;
     const uint32_t *s = words + (size_t)k * width;
     uint32_t spans[RV_WMAX];
     const int n = rv_logical_len(s, width);
+    const int cst = n >= 2 ? rv_parse(s, n, spans, true) : -1;
     len[k] = (uint16_t)n;
-    cost[k] = n >= 2 ? rv_parse(s, n, spans, true) : -1;
+    cost[k] = cst;
+    /* the tournament's tie-break key; a slot that is not a valid program
+       fails the whole call (the children are not built from it) */
+    cost16[k] = (uint16_t)(cst < 0 ? 0 : min(cst, 65535));
+    if (cst < 0) atomicOr(bad, 1);
     hash[k] = rv_hash(s, n);
 }
 
@@ -58,11 +64,13 @@ struct RvItem {
 
 __global__ void __launch_bounds__(RV_T) rv_children(RvConfig c, RvParents par,
                                                     const uint8_t *__restrict__ restart,
-                                                    RvItem *items, uint32_t *progs)
+                                                    const int *__restrict__ bad, RvItem *items,
+                                                    uint32_t *progs)
 {
     const int nslots = c.islands * c.pop;
     const int it = blockIdx.x * blockDim.x + threadIdx.x;
     if (it >= nslots * RV_K) return;
+    if (*bad) return; /* an invalid parent: the call fails, nothing is built */
     const int k = it / RV_K, attempt = it % RV_K;
     const int island = k / c.pop, slot = k % c.pop;
     uint32_t prog[RV_WMAX], spans[RV_WMAX], other[RV_WMAX], tmp[RV_WMAX];
@@ -213,12 +221,13 @@ extern "C" float rc_pool_vary(void *ctx, int which, int islands, int pop, int wi
     const size_t in_end = rc_take(&cur, 0);
     const size_t o_plen = rc_take(&cur, sizeof(uint16_t) * nslots);
     const size_t o_pcost = rc_take(&cur, sizeof(int) * nslots);
+    const size_t o_pcost16 = rc_take(&cur, sizeof(uint16_t) * nslots);
     const size_t o_phash = rc_take(&cur, sizeof(unsigned long long) * nslots);
+    const size_t o_bad = rc_take(&cur, sizeof(int));
     const size_t o_items = rc_take(&cur, sizeof(RvItem) * nitems);
     const size_t meta_end = rc_take(&cur, 0);
     const size_t o_choice = rc_take(&cur, sizeof(RvChoice) * nslots);
     const size_t o_hprog = rc_take(&cur, sizeof(uint32_t) * (size_t)nslots * width);
-    const size_t o_pcost16 = rc_take(&cur, sizeof(uint16_t) * nslots);
     const size_t host_end = rc_take(&cur, 0);
     const size_t o_progs = rc_take(&cur, sizeof(uint32_t) * (size_t)nitems * width);
     const size_t dev_end = rc_take(&cur, 0);
@@ -231,24 +240,16 @@ extern "C" float rc_pool_vary(void *ctx, int which, int islands, int pop, int wi
     cudaEventRecord(c->t0, c->s);
     cudaMemcpyAsync(dev, host, in_end, cudaMemcpyHostToDevice, c->s);
 
-    /* 1. parent metadata, to the host as well (the tie-break and the elite) */
+    /* 1. parent metadata (read back with the items below: the tie-break and
+       the elite) */
     uint16_t *d_plen = reinterpret_cast<uint16_t *>(dev + o_plen);
     int *d_pcost = reinterpret_cast<int *>(dev + o_pcost);
-    unsigned long long *d_phash = reinterpret_cast<unsigned long long *>(dev + o_phash);
-    rv_parents<<<(nslots + RV_T - 1) / RV_T, RV_T, 0, c->s>>>(c->d_pool[b], width, nslots, d_plen,
-                                                             d_pcost, d_phash);
-    cudaMemcpyAsync(host + o_plen, dev + o_plen, o_items - o_plen, cudaMemcpyDeviceToHost, c->s);
-    if (rc_finish(c) != 0) return -1.0f;
-    const int *pcost = reinterpret_cast<const int *>(host + o_pcost);
-    std::vector<uint16_t> cost16(nslots);
-    for (int k = 0; k < nslots; ++k) {
-        if (pcost[k] < 0) return -1.0f; /* a parent slot is not a valid program */
-        cost16[k] = (uint16_t)std::min(pcost[k], 65535);
-    }
-    memcpy(host + o_pcost16, cost16.data(), sizeof(uint16_t) * nslots);
     uint16_t *d_pcost16 = reinterpret_cast<uint16_t *>(dev + o_pcost16);
-    cudaMemcpyAsync(d_pcost16, host + o_pcost16, sizeof(uint16_t) * nslots,
-                    cudaMemcpyHostToDevice, c->s);
+    unsigned long long *d_phash = reinterpret_cast<unsigned long long *>(dev + o_phash);
+    int *d_bad = reinterpret_cast<int *>(dev + o_bad);
+    cudaMemsetAsync(d_bad, 0, sizeof(int), c->s);
+    rv_parents<<<(nslots + RV_T - 1) / RV_T, RV_T, 0, c->s>>>(c->d_pool[b], width, nslots, d_plen,
+                                                             d_pcost, d_pcost16, d_phash, d_bad);
 
     /* 2. the first RV_K attempts of every child slot */
     RvParents dpar;
@@ -260,11 +261,13 @@ extern "C" float rc_pool_vary(void *ctx, int which, int islands, int pop, int wi
     RvItem *d_items = reinterpret_cast<RvItem *>(dev + o_items);
     uint32_t *d_progs = reinterpret_cast<uint32_t *>(dev + o_progs);
     rv_children<<<(nitems + RV_T - 1) / RV_T, RV_T, 0, c->s>>>(
-        cfg, dpar, reinterpret_cast<const uint8_t *>(dev + o_restart), d_items, d_progs);
-    cudaMemcpyAsync(host + o_items, dev + o_items, sizeof(RvItem) * nitems, cudaMemcpyDeviceToHost,
-                    c->s);
+        cfg, dpar, reinterpret_cast<const uint8_t *>(dev + o_restart), d_bad, d_items, d_progs);
+    cudaMemcpyAsync(host + o_plen, dev + o_plen, meta_end - o_plen, cudaMemcpyDeviceToHost, c->s);
     c->launches += 2;
     if (rc_finish(c) != 0) return -1.0f;
+    /* a parent slot that is not a valid program fails the call */
+    if (*reinterpret_cast<const int *>(host + o_bad) != 0) return -1.0f;
+    const uint16_t *cost16 = reinterpret_cast<const uint16_t *>(host + o_pcost16);
 
     /* 3. the duplicate rule, in slot order */
     const RvItem *items = reinterpret_cast<const RvItem *>(host + o_items);
@@ -276,7 +279,7 @@ extern "C" float rc_pool_vary(void *ctx, int which, int islands, int pop, int wi
     RvParents hpar;
     hpar.words = c->pool_host[b].data();
     hpar.err = err;
-    hpar.cost = cost16.data();
+    hpar.cost = cost16;
     hpar.front = front;
     hpar.front_off = front_off;
     uint32_t prog[RV_WMAX], spans[RV_WMAX], other[RV_WMAX], tmp[RV_WMAX];
@@ -292,9 +295,9 @@ extern "C" float rc_pool_vary(void *ctx, int which, int islands, int pop, int wi
         const bool rs = restart && restart[i];
         int elite = i * pop;
         if (!rs) {
-            RvKey kb = rv_key(err, cost16.data(), elite);
+            RvKey kb = rv_key(err, cost16, elite);
             for (int k = i * pop + 1; k < (i + 1) * pop; ++k) {
-                const RvKey kk = rv_key(err, cost16.data(), k);
+                const RvKey kk = rv_key(err, cost16, k);
                 if (rv_less(kk, kb)) {
                     elite = k;
                     kb = kk;
