@@ -245,10 +245,19 @@ float rc_score_run(RcCtx *c, const uint32_t *words, const uint32_t *off, int wid
         bk[b].maxins = std::max(bk[b].maxins, ins_off[p + 1] - ins_off[p]);
         max_slots = std::max(max_slots, nslots[p]);
     }
+    /* longest program first, ties in slot order: a stable counting sort on
+       the instruction count (1..RC_MAX_INS) */
     for (int b = 0; b < 2; ++b) {
-        std::stable_sort(bk[b].cands.begin(), bk[b].cands.end(), [&](int x, int y) {
-            return (ins_off[x + 1] - ins_off[x]) > (ins_off[y + 1] - ins_off[y]);
-        });
+        std::vector<int> &v = bk[b].cands;
+        std::vector<int> at(RC_MAX_INS + 1, 0), sorted(v.size());
+        auto key = [&](int x) {
+            const int len = std::min(std::max(ins_off[x + 1] - ins_off[x], 1), RC_MAX_INS);
+            return RC_MAX_INS - len;
+        };
+        for (int x : v) at[key(x) + 1]++;
+        for (int k = 0; k < RC_MAX_INS; ++k) at[k + 1] += at[k];
+        for (int x : v) sorted[at[key(x)]++] = x;
+        v.swap(sorted);
     }
     const int Tb[2] = {256, 64};
     /* the scoring kernel reads features from L2; nothing is staged */
