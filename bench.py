@@ -376,6 +376,10 @@ def bench_score(args, rank, world, dev, pkg, W, flushbuf):
     ops = postfix_ops(prog, off)
     alg_ops = float(N) * float((ops + 2).sum())      # lane-ops per launch
     pcount = np.zeros(P, np.int32)
+    # the scorer's autotuner (candidates per work item, per length bucket)
+    # on this batch, before and outside the timed steps; a candidate's score
+    # does not depend on the choice
+    ev.autotune(prog, off)
     # warm-up
     for _ in range(args.warmup):
         ev.score_batch(prog, off, 0, pcount)
@@ -1227,6 +1231,8 @@ def main():
             line["rows_evaluated_per_step"] = rows_f32
             line["rows_f64_rescored_per_step"] = rows_f64
             line["candidates_finite"] = r["finite"]
+            line["scorer_tuning"] = ("candidates per work item chosen per length bucket by "
+                                     "rc_autotune on the batch, before the warm-up")
             line["plain"] = r["plain"]
             line["batched_over_plain"] = value / r["plain"]["value"]
             line["absolute_error_value"] = r["absolute"]["value"]
