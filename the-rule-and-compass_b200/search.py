@@ -114,7 +114,8 @@ class GenerationLoop:
         self.timing["screen"] += ms
         t0 = time.perf_counter()
         # admission ranks by the screened error and the complexity the
-        # variation engine reports; only the admitted programs are decoded
+        # variation engine reports; the admitted programs' fit plans are built
+        # straight from their words (a record decodes its tree when asked)
         wl = self.words.tolist()
         hasc = np.array([self._has_constant(w) for w in wl], np.uint8)
         pending = [(i // self.pop, i % self.pop) for i in range(n)]
