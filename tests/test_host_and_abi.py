@@ -123,6 +123,17 @@ def test_host_library_exports_every_refit_symbol(pkg):
     assert all(hasattr(lib, n) for n in names)
 
 
+def test_host_library_exports_every_host_symbol(pkg):
+    """include/rcsr_host.h (the compiler, fit plans, admission, constant
+    write-back) is served by librcsr_host.so."""
+    src = open(os.path.join(ROOT, "include", "rcsr_host.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = sorted(set(re.findall(r"\b(rch_[a-z0-9_]+)\s*\(", src)))
+    assert len(names) == 9, names
+    lib = ctypes.CDLL(os.path.join(ROOT, "the-rule-and-compass_b200", "librcsr_host.so"))
+    assert all(hasattr(lib, n) for n in names), [n for n in names if not hasattr(lib, n)]
+
+
 def test_fit_kernel_info_contract(pkg):
     L = pkg.cuda_lib()
     t, s, m = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()

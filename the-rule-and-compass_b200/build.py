@@ -76,7 +76,7 @@ def build_host():
     a separately rounded IEEE operation, which the refit's bit-identity with
     the reference's CPU path relies on."""
     srcs = [os.path.join(HERE, "host", f) for f in ("rcsr_host.cpp", "refit.cpp")]
-    deps = srcs + [os.path.join(INCLUDE, "rcsr_refit.h")]
+    deps = srcs + [os.path.join(INCLUDE, "rcsr_refit.h"), os.path.join(INCLUDE, "rcsr_host.h")]
     if _stale(HOST_LIB, deps):
         cmd = ["g++", "-O3", "-std=c++17", "-ffp-contract=off", "-fPIC", "-shared", "-pthread",
                "-fopenmp", "-Wall", "-I" + INCLUDE, "-o", HOST_LIB, *srcs]

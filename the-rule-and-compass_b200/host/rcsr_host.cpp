@@ -15,6 +15,8 @@
  * device opcodes, 64..66 the inverse hyperbolics. Exposed through a small C
  * API (rch_*) for the Python package and the benchmark.
  */
+#include "rcsr_host.h"
+
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
