@@ -2396,7 +2396,11 @@ SweepLaunch sweep4_launch(RcCtx *c, const FitPrep &b, int Wmax)
 unsigned long long enqueue_fit(cudaStream_t s_, int sm_count, const FitArgs &a, int steps,
                                const SweepLaunch *sw, int nkinds)
 {
-    const int ctrl_grid = sm_count * 8;
+    /* persistent grids take their items from work counters, so a grid no
+       larger than the items that can exist (a small batch) answers the
+       same and launches no idle blocks */
+    const int ctrl_grid = std::min(sm_count * 8, std::max(a.nprog, 1));
+    const int max_items = (int)std::min<long long>((long long)a.nprog * a.ntiles, 1LL << 30);
     unsigned long long k = 0;
     if (a.nsub > 0) {
         const size_t smem = 8 * (size_t)((a.sub_maxins + 1) & ~1) +
@@ -2417,7 +2421,8 @@ unsigned long long enqueue_fit(cudaStream_t s_, int sm_count, const FitArgs &a, 
         for (int k = 0; k < nkinds; ++k) {
             const SweepLaunch &L = sw[k];
             void *args[] = {(void *)&a, (void *)&q};
-            cudaLaunchKernel(L.fn, dim3(L.grid), dim3(L.threads), args, L.smem, s_);
+            const int grid = std::max(1, std::min(L.grid, max_items));
+            cudaLaunchKernel(L.fn, dim3(grid), dim3(L.threads), args, L.smem, s_);
         }
         ft_control<<<ctrl_grid, FT_CTRL_T, 0, s_>>>(a, q, 0);
     }
