@@ -12,7 +12,7 @@
  * B200 design. The reference runs one block per candidate for the whole LM,
  * so a candidate's 262,144 rows are swept by 128 threads while most of the
  * GPU waits for the slowest candidate. Here every sweep is spread over
- * (candidate x 4,096-row tile) work items for all active candidates at once:
+ * (candidate x 2,048-row tile) work items for all active candidates at once:
  *
  *   step s:  sweep kernels, one per kind (f32 assembly, f64 assembly, f32
  *            objective, f64 objective; implicit Jacobian / cost), each a
@@ -46,7 +46,7 @@
 #include "fit_interp.cuh"
 #include "fit_prep.h"
 
-#define FT_TILE_ROWS 4096
+#define FT_TILE_ROWS 2048
 #define FT_NBLK_MAX 21                     /* 4x4 blocks of a 24-wide augmented Gram */
 #define FT_PART_LOSS (FT_NBLK_MAX * 16)
 #define FT_PART_BAD (FT_PART_LOSS + 1)
@@ -1021,7 +1021,7 @@ __global__ void __launch_bounds__(T) ft_sweep4(FitArgs a, int q)
 }
 
 /* Values of the cached constant-free subtrees over all rows, once per fit:
-   one block per (subtree, 4096-row tile), four rows per thread, the same
+   one block per (subtree, 2048-row tile), four rows per thread, the same
    f32 forward sweep the other kinds run (so a cached value is bit-identical
    to the value a full forward sweep computes). */
 #define FT_FILL_T 128
@@ -1676,6 +1676,7 @@ __global__ void __launch_bounds__(FT_CTRL_T) ft_control(FitArgs a, int q, int in
     __shared__ double gram[24 * 24];
     __shared__ int s_task, s_cand, s_op;
     __shared__ double s_loss;
+    __shared__ double red[FT_CTRL_T];
     __shared__ int s_bad, s_skip;
     const int tid = threadIdx.x;
     const int nq = q ^ 1;
@@ -1748,30 +1749,53 @@ __global__ void __launch_bounds__(FT_CTRL_T) ft_control(FitArgs a, int q, int in
                 }
             }
         }
-        if (tid == 0) {
+        /* loss, flags and (correlation score) moments over the tiles: each
+           thread takes every FT_CTRL_T-th tile, then a fixed-order tree */
+        {
             double loss = 0.0;
+            double m[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
             int bad = 0, skip = 0;
             if (!init) {
-                for (int t = 0; t < a.ntiles; ++t) {
+                const bool asm_ = ft_op_assembles(op), csc = op == FOP_CSCORE;
+                for (int t = tid; t < a.ntiles; t += FT_CTRL_T) {
                     const double *pp = pt + (size_t)t * FT_PART_STRIDE;
                     loss += pp[FT_PART_LOSS];
                     bad |= pp[FT_PART_BAD] != 0.0;
-                    if (ft_op_assembles(op)) skip |= pp[FT_PART_SKIP] != 0.0;
-                }
-                if (op == FOP_CASM) {
-                    int cb = 0;
-                    loss = ft_corr_moments(gram, W, p, a.metric, sst, cb);
-                    bad |= cb;
-                } else if (op == FOP_CSCORE) {
-                    double m[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-                    for (int t = 0; t < a.ntiles; ++t)
-                        for (int k = 0; k < 6; ++k) m[k] += pt[(size_t)t * FT_PART_STRIDE + k];
-                    loss = bad ? INFINITY : ft_corr_trial(m, a.metric);
+                    if (asm_) skip |= pp[FT_PART_SKIP] != 0.0;
+                    if (csc)
+                        for (int k = 0; k < 6; ++k) m[k] += pp[k];
                 }
             }
-            s_loss = loss;
-            s_bad = bad;
-            s_skip = skip;
+            bad = __syncthreads_or(bad);
+            skip = __syncthreads_or(skip);
+            const int nsum = op == FOP_CSCORE ? 7 : 1;
+            for (int k = 0; k < nsum; ++k) {
+                red[tid] = k == 0 ? loss : m[k - 1];
+                __syncthreads();
+                for (int h = FT_CTRL_T / 2; h > 0; h >>= 1) {
+                    if (tid < h) red[tid] += red[tid + h];
+                    __syncthreads();
+                }
+                if (tid == 0) {
+                    if (k == 0) loss = red[0];
+                    else m[k - 1] = red[0];
+                }
+                __syncthreads();
+            }
+            if (tid == 0) {
+                if (!init) {
+                    if (op == FOP_CASM) {
+                        int cb = 0;
+                        loss = ft_corr_moments(gram, W, p, a.metric, sst, cb);
+                        bad |= cb;
+                    } else if (op == FOP_CSCORE) {
+                        loss = bad ? INFINITY : ft_corr_trial(m, a.metric);
+                    }
+                }
+                s_loss = init ? 0.0 : loss;
+                s_bad = init ? 0 : bad;
+                s_skip = init ? 0 : skip;
+            }
         }
         __syncthreads();
         /* the state machine on thread 0; a solve it requests runs on warp 0
