@@ -190,7 +190,7 @@ int rc_unified(void);
 
 /* Batched LM with the fused forward+adjoint sweep: every LM iteration of
    every candidate runs on the device as a fixed sequence of steps (persistent
-   sweeps over (candidate, 4,096-row tile) work items, then a control kernel
+   sweeps over (candidate, 2,048-row tile) work items, then a control kernel
    that reduces, solves and queues each candidate's next sweep), captured once
    as a CUDA graph per batch shape and replayed. Arguments, outputs and status
    codes are rc_fit_batch's; metric adds 6 = implicit (minimises
@@ -252,6 +252,19 @@ int rc_grad_batch(void *ctx, const unsigned int *prog, const unsigned int *off,
 float rc_implicit_score_batch(void *ctx, const unsigned int *prog, const unsigned int *off,
                               const int *pcount, int nprog, int kmax, const double *c,
                               double *out, int *status);
+/* Rank-sum method of rc_rank_score_batch on this context. By default a
+   segment's keys are cut into buckets by splitters from a sample of them and
+   each bucket is ranked on its own (a bucket holding a group of more than
+   group_max distinct keys that one digit cannot tell apart is sorted whole);
+   a segment with a bucket over capacity (bucket_cap keys, at most 8192) is
+   redone by the radix sort. 0 keeps the built-in value; bucket_cap -1 uses
+   the radix sort for every segment. The sums are the same bits either way. No counterpart in
+   the reference ABI. Returns 0, or -1 for a bad argument. */
+int rc_rank_tuning(void *ctx, int bucket_cap, int group_max);
+/* Segments of the context's last rc_rank_score_batch that the radix sort
+   summed (all of them when the buckets were off or n is past 4,194,304
+   rows), or -1 on a null context. No counterpart in the reference ABI. */
+int rc_rank_last_fallbacks(void *ctx);
 /* Kernels this context has launched so far (a replayed fit graph counts its
    kernel nodes). No counterpart in the reference: telemetry for callers that
    check the device path really ran. Returns 0, or -1 on a null argument. */

@@ -205,3 +205,72 @@ def test_max_scan_and_level_intervals(pkg, E, O):
             assert o[2] == np.max(np.minimum(e1[nz], e2[nz]))
             assert o[3] == np.min(np.maximum(e1[nz], e2[nz]))
     ev.close()
+
+
+def _bucket_models(E):
+    """Keys of every shape the bucketed sums meet: distinct (linear), few
+    values with many ties (integer x0), 2,001 values with ties (x1 rounded
+    to 1/500, column 3), one value (flat), long groups sharing their upper
+    bits (clustered, near-constant) and a heavy tail whose last buckets span
+    many binades (exp)."""
+    m = _models(E)
+    clustered = E.node(E.ADD, [E.node(E.MUL, [E.constant(0.5), E.input(0)]),
+                               E.node(E.MUL, [E.constant(1e-9), E.input(1)])])
+    near = E.node(E.ADD, [E.constant(1.0), E.node(E.MUL, [E.constant(1e-12), E.input(2)])])
+    step = E.node(E.MUL, [E.constant(1.5), E.input(3)])
+    tail = E.node(E.EXP, [E.node(E.MUL, [E.constant(3.0), E.input(2)])])
+    return [m["linear"], m["tied"], m["flat"], clustered, near, step, tail]
+
+
+def _fixture4(n, seed):
+    cols, y = _fixture(n, seed=seed)
+    return np.concatenate([cols, np.round(cols[1:2] * 500.0) / 500.0]), y
+
+
+def _check_sums(O, trees, cols, y, sums, status):
+    for k, t in enumerate(trees):
+        ab, aa, _ = O.rank_sums(_oracle_pred(O, t, cols), y)
+        assert status[k] == 0
+        assert sums[k] == (ab, aa), (k, sums[k], (ab, aa))
+
+
+@pytest.mark.parametrize("n", [8192, 8193, 300007])
+def test_bucketed_rank_sums_match_the_oracle(pkg, E, O, n):
+    """One range bucket (8,192 rows), the smallest multi-bucket size and 147
+    buckets: the sums equal the CPU's exactly, and no segment needs the
+    radix sort."""
+    cols, y = _fixture4(n, seed=n % 1000)
+    ev = _evaluator(pkg, cols, y)
+    trees = _bucket_models(E)
+    plans, prog, off, pcount, c0, kmax = _pack(pkg, trees)
+    sums, status, _, _ = ev.rank_sums(prog, off, pcount, c0, kmax)
+    _check_sums(O, trees, cols, y, sums, status)
+    assert ev.rank_fallbacks() == 0
+    ev.close()
+
+
+@pytest.mark.parametrize("cap,gmax", [(64, 0), (0, 1), (-1, 0)])
+def test_rank_sums_on_the_radix_fallback(pkg, E, O, cap, gmax):
+    """Buckets of 64 slots overflow (those segments go to the radix sort one
+    at a time), a comparison bound of one sorts every bucket holding two
+    distinct keys with one digit, and -1 turns the buckets off (the radix
+    sort for all): the same sums each way."""
+    n = 100003
+    cols, y = _fixture4(n, seed=7)
+    ev = _evaluator(pkg, cols, y)
+    trees = _bucket_models(E)
+    plans, prog, off, pcount, c0, kmax = _pack(pkg, trees)
+    ev.rank_tuning(cap, gmax)
+    sums, status, _, _ = ev.rank_sums(prog, off, pcount, c0, kmax)
+    _check_sums(O, trees, cols, y, sums, status)
+    fb = ev.rank_fallbacks()
+    if cap < 0:
+        assert fb == len(trees)
+    elif cap > 0:
+        assert 1 <= fb < len(trees)  # the flat model's one value never overflows
+    else:
+        assert fb == 0
+    ev.rank_tuning(0, 0)
+    sums2, _, _, _ = ev.rank_sums(prog, off, pcount, c0, kmax)
+    assert sums2 == sums
+    ev.close()

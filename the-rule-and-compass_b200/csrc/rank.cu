@@ -110,7 +110,8 @@ __device__ __forceinline__ void rs_count_keys(const u64 *src, long long r0, long
    not finite or exceeds 1e30 (eval.cu:4388-4418). A non-finite key marks
    the segment's status 2. The block then counts the eight digits of the
    keys it wrote (still in L2) into count[local segment][pass][256], which
-   the caller zeroed, so the sort needs no counting read of its own. */
+   the caller zeroed, so the sort needs no counting read of its own (with
+   count NULL it counts nothing). */
 static_assert(RK_T == RS_T, "the digit count runs on the key kernel's blocks");
 template <int MODE>
 __global__ void __launch_bounds__(RK_T) rk_keys(const FIns *fins, const int *fins_off,
@@ -175,6 +176,7 @@ __global__ void __launch_bounds__(RK_T) rk_keys(const FIns *fins, const int *fin
     }
     /* (the barrier also makes the block's key writes visible to its reads) */
     if (__syncthreads_or(bad) && tid == 0) status[seg] = 2;
+    if (!count) return; /* the bucketed sums count nothing here */
     rs_count_keys(kseg, r0, r1, cnt);
     __syncthreads();
 #pragma unroll
@@ -675,6 +677,491 @@ __global__ void __launch_bounds__(RS_T) rk_final(const __int128 *part, int ntile
     }
 }
 
+/* ---- bucketed rank sums -------------------------------------------------
+ *
+ * The sums need every key's run [i, j) of equal keys in sorted order, not the
+ * sorted array. So a segment is cut into buckets that are ordered among
+ * themselves: splitters taken from a sorted sample of its keys (RB_OVS
+ * samples per bucket, from rows spread over the segment by a fixed hash)
+ * give a range bucket between consecutive splitters and an equality bucket
+ * for each splitter. One pass puts every key of a range bucket, with its
+ * row's B, into the bucket's fixed-capacity slots (block-aggregated
+ * reservations); a key equal to a splitter only adds to its equality
+ * bucket's count and B sum. A scan per segment gives every bucket its first
+ * position. One block per range bucket then groups its keys by a 10-bit
+ * digit of their offset from the bucket's smallest key, scaled to the bits
+ * that vary inside the bucket: a group of equal keys is one run, and a small
+ * group of distinct keys ranks each key by comparison; a bucket with a large
+ * group of distinct keys is sorted in shared memory instead. A bucket over
+ * its capacity sends the whole segment to the radix sort above. The sums are
+ * integers, so they are the same bits on every path. */
+#define RB_AVG 2048                /* keys per range bucket aimed at */
+#define RB_CAP 8192                /* slots per range bucket */
+#define RB_OVS 8                   /* samples per range bucket */
+#define RB_MAXB 2048               /* range buckets per segment at most */
+#define RB_MAXS (RB_OVS * RB_MAXB) /* samples per segment at most (a power of two) */
+#define RB_DIG 1024                /* digit groups of a range bucket */
+#define RB_GMAX 48                 /* largest group of distinct keys ranked by comparison */
+static_assert((RB_CAP & (RB_CAP - 1)) == 0, "a sorted bucket pads to a power of two");
+#define RB_CT 4096                 /* keys per scatter block */
+#define RB_T 256
+#define RB_CR (RB_CT / RB_T)
+#define RB_ST 1024 /* splitter and scan threads */
+static_assert(RB_T == RS_T, "the bucket kernels use the block sum of the run pass");
+static_assert(RB_CT <= 65536 && 2 * RB_MAXB <= 65536, "bucket and rank pack into 16 bits each");
+
+__device__ __forceinline__ unsigned rb_hash(unsigned a, unsigned b)
+{
+    unsigned h = a * 0x9E3779B1u ^ (b + 0x7F4A7C15u);
+    h ^= h >> 16;
+    h *= 0x85EBCA6Bu;
+    h ^= h >> 13;
+    h *= 0xC2B2AE35u;
+    h ^= h >> 16;
+    return h;
+}
+
+/* Keys of S sample rows per segment: S / 2 row pairs, pair p at rows 2q and
+   2q + 1 with q drawn by a fixed hash from the p-th of S / 2 equal strata of
+   the n / 2 pairs; the f64 sweep and the keys of rk_keys. */
+__global__ void __launch_bounds__(RK_T) rb_sample(const FIns *fins, const int *fins_off,
+                                                  const int4 *finfo, const int *valid,
+                                                  const double *c0, int kmax, const double *cols,
+                                                  int npad, int n, int ntrials, int seg0,
+                                                  int sblocks, int S, int maxins, u64 *samp)
+{
+    using V4 = FiV<double, 2>::V4;
+    extern __shared__ __align__(16) unsigned char sm[];
+    FIns *ins = reinterpret_cast<FIns *>(sm);
+    double *cv = reinterpret_cast<double *>(sm + 8 * (size_t)((maxins + 1) & ~1));
+    V4 *stk = reinterpret_cast<V4 *>(cv + FT_MAX_CONST);
+    const int ls = blockIdx.x / sblocks, blk = blockIdx.x % sblocks;
+    const int seg = seg0 + ls;
+    const int cand = seg / ntrials;
+    const int tid = threadIdx.x;
+    const bool ok = valid[cand] != 0;
+    if (ok) {
+        const int nf = finfo[cand].x;
+        for (int i = tid; i < nf; i += RK_T) ins[i] = fins[fins_off[cand] + i];
+        if (tid < FT_MAX_CONST) cv[tid] = tid < kmax ? c0[(size_t)seg * kmax + tid] : 0.0;
+    }
+    __syncthreads();
+    const int hp = S / 2, p = blk * RK_T + tid;
+    if (p >= hp) return;
+    const int stride = (n / 2) / hp;
+    const int q = p * stride + (int)(rb_hash((unsigned)seg, (unsigned)p) % (unsigned)stride);
+    double pr[2] = {CUDART_NAN, CUDART_NAN};
+    if (ok) fi_forward<double, 2, false>(ins, cv, cols, npad, 2 * q, stk, nullptr, RK_T, tid, pr);
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+        samp[(size_t)ls * RB_MAXS + 2 * p + i] = isfinite(pr[i]) ? rk_key(pr[i]) : ~0ULL;
+}
+
+/* One block per segment: the S samples sorted (bitonic, padded to P2 with the
+   largest key), splitter j = sample (j + 1) * S / m for j < m - 1 with
+   repeats dropped, into spl[seg][..] and their count into nspl[seg]. */
+__global__ void __launch_bounds__(RB_ST) rb_splitters(const u64 *samp, int S, int P2, int m,
+                                                      u64 *spl, int *nspl)
+{
+    extern __shared__ __align__(16) unsigned char sm[];
+    u64 *s = reinterpret_cast<u64 *>(sm);
+    const int ls = blockIdx.x, tid = threadIdx.x;
+    const u64 *src = samp + (size_t)ls * RB_MAXS;
+    for (int i = tid; i < P2; i += RB_ST) s[i] = i < S ? src[i] : ~0ULL;
+    __syncthreads();
+    for (int k = 2; k <= P2; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = tid; i < P2; i += RB_ST) {
+                const int l = i ^ j;
+                if (l > i) {
+                    const u64 a = s[i], b = s[l];
+                    if ((a > b) == ((i & k) == 0)) {
+                        s[i] = b;
+                        s[l] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    if (tid < 32) {
+        int cnt = 0;
+        for (int j0 = 0; j0 < m - 1; j0 += 32) {
+            const int j = j0 + tid;
+            u64 v = 0;
+            bool keep = false;
+            if (j < m - 1) {
+                v = s[(j + 1) * S / m];
+                keep = j == 0 || v != s[j * S / m];
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, keep);
+            if (keep) spl[(size_t)ls * RB_MAXB + cnt + __popc(bal & ((1u << tid) - 1u))] = v;
+            cnt += __popc(bal);
+        }
+        if (tid == 0) nspl[ls] = cnt;
+    }
+}
+
+/* Bucket b of a key among ns splitters: 2 * (splitters below it), plus one
+   when it equals the next splitter (an equality bucket). */
+__device__ __forceinline__ unsigned rb_bucket(const u64 *spl, int ns, u64 k)
+{
+    int lo = 0, hi = ns;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (spl[mid] < k) lo = mid + 1;
+        else hi = mid;
+    }
+    return 2u * (unsigned)lo + ((lo < ns && spl[lo] == k) ? 1u : 0u);
+}
+
+/* RB_CT keys per block: each key's bucket, the block's count per bucket (a
+   key's rank among the block's keys of its bucket from the shared-memory
+   count), one reservation per range bucket the block touches, then the
+   range keys and their B written to their slots. Equality buckets only add
+   counts and B sums. A slot at or past `cap` flags the segment. */
+__global__ void __launch_bounds__(RB_T) rb_scatter(const u64 *keys, int n, int ctiles, int m,
+                                                   int cap, const long long *B, const u64 *spl,
+                                                   const int *nspl, unsigned *rcur,
+                                                   unsigned *ecnt, unsigned long long *esum,
+                                                   u64 *bkey, int *bval, int *ovf)
+{
+    __shared__ u64 sspl[RB_MAXB];
+    __shared__ unsigned hist[2 * RB_MAXB];
+    __shared__ unsigned long long ssum[RB_MAXB];
+    const int ls = blockIdx.x / ctiles, tile = blockIdx.x % ctiles, tid = threadIdx.x;
+    const int ns = nspl[ls], nb = 2 * ns + 1;
+    for (int i = tid; i < ns; i += RB_T) {
+        sspl[i] = spl[(size_t)ls * RB_MAXB + i];
+        ssum[i] = 0ULL;
+    }
+    for (int i = tid; i < nb; i += RB_T) hist[i] = 0u;
+    __syncthreads();
+    const u64 *ks = keys + (size_t)ls * n;
+    const int t0 = tile * RB_CT;
+    u64 key[RB_CR];
+    unsigned pk[RB_CR];
+#pragma unroll
+    for (int r = 0; r < RB_CR; ++r) {
+        const int i = t0 + r * RB_T + tid;
+        pk[r] = 0xffffffffu;
+        key[r] = 0ULL;
+        if (i < n) {
+            const u64 k = ks[i];
+            const unsigned b = rb_bucket(sspl, ns, k);
+            const unsigned rank = atomicAdd(&hist[b], 1u);
+            if (b & 1u) atomicAdd(&ssum[b >> 1], (unsigned long long)B[i]);
+            key[r] = k;
+            pk[r] = (b << 16) | rank;
+        }
+    }
+    __syncthreads();
+    for (int b = tid; b < nb; b += RB_T) {
+        const unsigned h = hist[b];
+        if (!h) continue;
+        const size_t j = (size_t)ls * RB_MAXB + (b >> 1);
+        if (b & 1) {
+            atomicAdd(&ecnt[j], h);
+            atomicAdd(&esum[j], ssum[b >> 1]);
+        } else {
+            hist[b] = atomicAdd(&rcur[j], h);
+        }
+    }
+    __syncthreads();
+    bool over = false;
+#pragma unroll
+    for (int r = 0; r < RB_CR; ++r) {
+        if (pk[r] == 0xffffffffu) continue;
+        const unsigned b = pk[r] >> 16;
+        if (b & 1u) continue;
+        const unsigned pos = hist[b] + (pk[r] & 0xffffu);
+        if (pos >= (unsigned)cap) {
+            over = true;
+            continue;
+        }
+        const size_t slot = ((size_t)ls * m + (b >> 1)) * RB_CAP + pos;
+        bkey[slot] = key[r];
+        bval[slot] = (int)B[t0 + r * RB_T + tid];
+    }
+    if (over) ovf[ls] = 1;
+}
+
+/* One block per segment: bucket sizes in order (range 0, equality 0, range
+   1, ...), their first positions, and the equality buckets' partial sums
+   (one run [O, O + c) each: A = 2 O + c - n). A range bucket over `cap`, or
+   sizes that do not add up to n, flag the segment. */
+__global__ void __launch_bounds__(RB_ST) rb_scan(int n, int cap, const int *nspl,
+                                                 const unsigned *rcur, const unsigned *ecnt,
+                                                 const unsigned long long *esum, unsigned *boff,
+                                                 __int128 *part, int *ovf)
+{
+    __shared__ unsigned wsum[RB_ST / 32];
+    const int ls = blockIdx.x, tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int nb = 2 * nspl[ls] + 1;
+    unsigned sz[4], tot = 0;
+    bool bad = false;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int b = 4 * tid + k;
+        unsigned v = 0;
+        if (b < nb) {
+            const size_t j = (size_t)ls * RB_MAXB + (b >> 1);
+            v = (b & 1) ? ecnt[j] : rcur[j];
+            if (!(b & 1) && v > (unsigned)cap) bad = true;
+        }
+        sz[k] = v;
+        tot += v;
+    }
+    unsigned x = tot;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[w] = x;
+    __syncthreads();
+    unsigned run = x - tot;
+    for (int k = 0; k < w; ++k) run += wsum[k];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int b = 4 * tid + k;
+        if (b < nb) {
+            const size_t e = (size_t)ls * 2 * RB_MAXB + b;
+            boff[e] = run;
+            if (b & 1) {
+                const long long c = sz[k];
+                const long long A = 2LL * run + c - n;
+                const long long sb = (long long)esum[(size_t)ls * RB_MAXB + (b >> 1)];
+                part[e * 2 + 0] = (__int128)A * sb;
+                part[e * 2 + 1] = (__int128)c * A * A;
+            }
+        }
+        run += sz[k];
+    }
+    if (tid == RB_ST - 1 && run != (unsigned)n) bad = true;
+    if (bad) ovf[ls] = 1;
+}
+
+/* Shared layout of rb_local: the bucket's keys and B in digit order, the
+   digit groups' first positions (RB_DIG + 1), their cursors and flags. */
+__host__ __device__ constexpr size_t rb_local_smem()
+{
+    return (size_t)RB_CAP * (sizeof(u64) + sizeof(int)) + (2 * RB_DIG + 1) * sizeof(unsigned) +
+           RB_DIG;
+}
+
+/* One block per (segment, range bucket): runs and partial sums of its c
+   keys, which hold positions [O, O + c) of the segment's order. */
+__global__ void __launch_bounds__(RB_T, 2) rb_local(int n, int m, int cap, int gmax,
+                                                    const int *nspl, const unsigned *rcur,
+                                                    const unsigned *boff, const u64 *bkey,
+                                                    const int *bval, __int128 *part, int *ovf)
+{
+    extern __shared__ __align__(16) unsigned char sm[];
+    u64 *sk = reinterpret_cast<u64 *>(sm);
+    int *sv = reinterpret_cast<int *>(sk + RB_CAP);
+    unsigned *gst = reinterpret_cast<unsigned *>(sv + RB_CAP);
+    unsigned *cur = gst + RB_DIG + 1;
+    unsigned char *mixed = reinterpret_cast<unsigned char *>(cur + RB_DIG);
+    __shared__ __int128 red[RB_T];
+    __shared__ u64 s_lo[RB_T / 32], s_hi[RB_T / 32];
+    __shared__ unsigned wsum[RB_T / 32];
+    __shared__ int s_skip;
+    const int ls = blockIdx.x / m, idx = blockIdx.x % m;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    /* other blocks of the segment may raise its flag meanwhile: one read,
+       shared, so the whole block takes the same branch */
+    if (tid == 0) s_skip = *(volatile const int *)(ovf + ls) || idx > nspl[ls];
+    __syncthreads();
+    if (s_skip) return;
+    const int c = (int)rcur[(size_t)ls * RB_MAXB + idx];
+    if (c > cap) return; /* the scan has flagged the segment */
+    const long long O = boff[(size_t)ls * 2 * RB_MAXB + 2 * idx];
+    const size_t base = ((size_t)ls * m + idx) * RB_CAP;
+    const u64 *bk = bkey + base;
+    const int *bv = bval + base;
+    __int128 *pp = part + ((size_t)ls * 2 * RB_MAXB + 2 * idx) * 2;
+
+    u64 lo = ~0ULL, hi = 0ULL;
+    for (int q = tid; q < c; q += RB_T) {
+        const u64 k = bk[q];
+        lo = k < lo ? k : lo;
+        hi = k > hi ? k : hi;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const u64 a = __shfl_xor_sync(0xffffffffu, lo, o), b = __shfl_xor_sync(0xffffffffu, hi, o);
+        lo = a < lo ? a : lo;
+        hi = b > hi ? b : hi;
+    }
+    if (lane == 0) {
+        s_lo[w] = lo;
+        s_hi[w] = hi;
+    }
+    __syncthreads();
+    for (int k = 0; k < RB_T / 32; ++k) {
+        lo = s_lo[k] < lo ? s_lo[k] : lo;
+        hi = s_hi[k] > hi ? s_hi[k] : hi;
+    }
+    if (c == 0 || lo == hi) {
+        /* one run [O, O + c) */
+        long long s = 0;
+        for (int q = tid; q < c; q += RB_T) s += bv[q];
+        const __int128 sb = rk_block_sum((__int128)s, red);
+        if (tid == 0) {
+            const long long A = 2 * O + c - n;
+            pp[0] = (__int128)A * sb;
+            pp[1] = (__int128)c * A * A;
+        }
+        return;
+    }
+    const int nbits = 64 - __clzll((long long)(hi - lo));
+    const int shift = nbits > 10 ? nbits - 10 : 0;
+    for (int d = tid; d < RB_DIG; d += RB_T) {
+        cur[d] = 0u;
+        mixed[d] = 0;
+    }
+    __syncthreads();
+    for (int q = tid; q < c; q += RB_T) atomicAdd(&cur[(unsigned)((bk[q] - lo) >> shift)], 1u);
+    __syncthreads();
+    {
+        static_assert(RB_DIG == 4 * RB_T, "four digit groups per thread");
+        unsigned a[4], t = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            a[k] = cur[4 * tid + k];
+            t += a[k];
+        }
+        unsigned x = t;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) wsum[w] = x;
+        __syncthreads();
+        unsigned run = x - t;
+        for (int k = 0; k < w; ++k) run += wsum[k];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            gst[4 * tid + k] = run;
+            cur[4 * tid + k] = run;
+            run += a[k];
+        }
+        if (tid == 0) gst[RB_DIG] = (unsigned)c;
+    }
+    __syncthreads();
+    for (int q = tid; q < c; q += RB_T) {
+        const u64 k = bk[q];
+        const unsigned p = atomicAdd(&cur[(unsigned)((k - lo) >> shift)], 1u);
+        sk[p] = k;
+        sv[p] = bv[q];
+    }
+    __syncthreads();
+    for (int q = tid; q < c; q += RB_T) {
+        const u64 k = sk[q];
+        const unsigned d = (unsigned)((k - lo) >> shift);
+        if (k != sk[gst[d]]) mixed[d] = 1;
+    }
+    __syncthreads();
+    /* per thread at most RB_CAP / RB_T keys, each |A * B| and A^2 at most n^2:
+       the thread's sums fit 64 bits for the n this path takes */
+    long long ab = 0, aa = 0;
+    bool big = false;
+    for (int q = tid; q < c; q += RB_T) {
+        const u64 k = sk[q];
+        const unsigned d = (unsigned)((k - lo) >> shift);
+        const unsigned gs = gst[d], ge = gst[d + 1];
+        long long i = gs, j = ge;
+        if (mixed[d]) {
+            if (ge - gs <= (unsigned)gmax) {
+                unsigned lt = 0, le = 0;
+                for (unsigned t = gs; t < ge; ++t) {
+                    const u64 o = sk[t];
+                    lt += o < k;
+                    le += o <= k;
+                }
+                i = gs + lt;
+                j = gs + le;
+            } else {
+                big = true;
+            }
+        }
+        const long long A = 2 * O + i + j - n;
+        ab += A * (long long)sv[q];
+        aa += A * A;
+    }
+    if (__syncthreads_or(big)) {
+        /* the digit could not tell a large group apart (keys spread over many
+           binades, as in a tail bucket): sort the bucket (bitonic, padded to
+           a power of two by entries that order after every key, B marked
+           INT_MIN) and take each key's run by binary search */
+        int P2 = 1;
+        while (P2 < c) P2 <<= 1;
+        for (int q = c + tid; q < P2; q += RB_T) {
+            sk[q] = ~0ULL;
+            sv[q] = INT_MIN;
+        }
+        __syncthreads();
+        for (int k = 2; k <= P2; k <<= 1)
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                for (int i = tid; i < P2; i += RB_T) {
+                    const int l = i ^ j;
+                    if (l > i) {
+                        const u64 a = sk[i], b = sk[l];
+                        const int va = sv[i], vb = sv[l];
+                        const bool agt = a > b || (a == b && va == INT_MIN && vb != INT_MIN);
+                        if (agt == ((i & k) == 0)) {
+                            sk[i] = b;
+                            sk[l] = a;
+                            sv[i] = vb;
+                            sv[l] = va;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+        ab = 0;
+        aa = 0;
+        for (int q = tid; q < c; q += RB_T) {
+            const u64 k = sk[q];
+            const long long A = 2 * O + rk_lower(sk, 0, c, k) + rk_upper(sk, 0, c, k) - n;
+            ab += A * (long long)sv[q];
+            aa += A * A;
+        }
+    }
+    const __int128 sab = rk_block_sum((__int128)ab, red);
+    const __int128 saa = rk_block_sum((__int128)aa, red);
+    if (tid == 0) {
+        pp[0] = sab;
+        pp[1] = saa;
+    }
+}
+
+/* One block per segment not flagged: the bucket partials summed into the
+   two 128-bit sums, written as rk_final writes them. */
+__global__ void __launch_bounds__(RS_T) rb_final(const int *nspl, const __int128 *part,
+                                                 const int *ovf, u64 *out)
+{
+    __shared__ __int128 red[RS_T];
+    const int ls = blockIdx.x, tid = threadIdx.x;
+    if (ovf[ls]) return;
+    const int nb = 2 * nspl[ls] + 1;
+    __int128 ab = 0, aa = 0;
+    for (int b = tid; b < nb; b += RS_T) {
+        const size_t e = (size_t)ls * 2 * RB_MAXB + b;
+        ab += part[e * 2 + 0];
+        aa += part[e * 2 + 1];
+    }
+    const unsigned __int128 uab = (unsigned __int128)rk_block_sum(ab, red);
+    const unsigned __int128 uaa = (unsigned __int128)rk_block_sum(aa, red);
+    if (tid == 0) {
+        out[(size_t)ls * 4 + 0] = (u64)(uab >> 64);
+        out[(size_t)ls * 4 + 1] = (u64)uab;
+        out[(size_t)ls * 4 + 2] = (u64)(uaa >> 64);
+        out[(size_t)ls * 4 + 3] = (u64)uaa;
+    }
+}
+
 /* ---- order statistics --------------------------------------------------- */
 
 #define OS_T 256
@@ -951,6 +1438,72 @@ int wave_segments(int nsegs, int n, bool vals)
     return (int)std::min<size_t>(w, (size_t)nsegs);
 }
 
+/* Range buckets of the bucketed sums for n rows: one up to RB_CAP rows,
+   else ceil(n / RB_AVG); 0 past the rows the path takes (RB_AVG * RB_MAXB). */
+int rb_buckets(int n)
+{
+    if (n <= RB_CAP) return 1;
+    const long long m = ((long long)n + RB_AVG - 1) / RB_AVG;
+    return m <= RB_MAXB ? (int)m : 0;
+}
+
+struct RbBuffers {
+    u64 *keys;                /* [nseg][n] keys in row order */
+    u64 *samp;                /* [nseg][RB_MAXS] sample keys */
+    u64 *spl;                 /* [nseg][RB_MAXB] splitters */
+    int *nspl;                /* [nseg] */
+    u64 *bkey;                /* [nseg][m][RB_CAP] range-bucket slots */
+    int *bval;                /* [nseg][m][RB_CAP] their B */
+    unsigned *rcur, *ecnt;    /* [nseg][RB_MAXB] range / equality bucket sizes */
+    unsigned long long *esum; /* [nseg][RB_MAXB] equality buckets' B sums */
+    unsigned *boff;           /* [nseg][2 * RB_MAXB] first positions */
+    __int128 *part;           /* [nseg][2 * RB_MAXB][2] bucket partial sums */
+    unsigned char *zero;      /* rcur, ecnt and esum, zeroed per wave */
+    size_t zero_bytes;
+};
+
+size_t rb_bytes(int nseg, int n, int m)
+{
+    const size_t ns = (size_t)nseg;
+    size_t s = sizeof(u64) * ns * (size_t)n + sizeof(u64) * ns * (RB_MAXS + RB_MAXB) +
+               sizeof(int) * ns;
+    s += (sizeof(u64) + sizeof(int)) * ns * (size_t)m * RB_CAP;
+    s += (2 * sizeof(unsigned) + sizeof(unsigned long long)) * ns * RB_MAXB;
+    s += sizeof(unsigned) * ns * 2 * RB_MAXB + 2 * sizeof(__int128) * ns * 2 * RB_MAXB;
+    return s + 16 * 256;
+}
+
+RbBuffers rb_carve(unsigned char *base, size_t *cur, int nseg, int n, int m)
+{
+    const size_t ns = (size_t)nseg;
+    RbBuffers r;
+    r.keys = reinterpret_cast<u64 *>(base + rc_take(cur, sizeof(u64) * ns * (size_t)n));
+    r.samp = reinterpret_cast<u64 *>(base + rc_take(cur, sizeof(u64) * ns * RB_MAXS));
+    r.spl = reinterpret_cast<u64 *>(base + rc_take(cur, sizeof(u64) * ns * RB_MAXB));
+    r.nspl = reinterpret_cast<int *>(base + rc_take(cur, sizeof(int) * ns));
+    r.bkey = reinterpret_cast<u64 *>(base + rc_take(cur, sizeof(u64) * ns * (size_t)m * RB_CAP));
+    r.bval = reinterpret_cast<int *>(base + rc_take(cur, sizeof(int) * ns * (size_t)m * RB_CAP));
+    r.zero_bytes = (2 * sizeof(unsigned) + sizeof(unsigned long long)) * ns * RB_MAXB;
+    r.zero = base + rc_take(cur, r.zero_bytes);
+    r.rcur = reinterpret_cast<unsigned *>(r.zero);
+    r.ecnt = r.rcur + ns * RB_MAXB;
+    r.esum = reinterpret_cast<unsigned long long *>(r.ecnt + ns * RB_MAXB);
+    r.boff = reinterpret_cast<unsigned *>(base + rc_take(cur, sizeof(unsigned) * ns * 2 * RB_MAXB));
+    r.part = reinterpret_cast<__int128 *>(
+        base + rc_take(cur, 2 * sizeof(__int128) * ns * 2 * RB_MAXB));
+    return r;
+}
+
+#define RB_WAVE_BYTES ((size_t)4 << 30)
+
+int rb_wave_segments(int nsegs, int n, int m)
+{
+    const size_t per = rb_bytes(1, n, m);
+    size_t w = RB_WAVE_BYTES / (per ? per : 1);
+    if (w < 1) w = 1;
+    return (int)std::min<size_t>(w, (size_t)nsegs);
+}
+
 }  // namespace
 
 extern "C" {
@@ -968,46 +1521,97 @@ float rc_rank_score_batch(void *ctx, const unsigned int *prog, const unsigned in
     if (total > 0x7fffffffLL) return -1.0f;
     if (rk_prepare(c) != 0) return -1.0f;
     const int nsegs = nsets * ntrials;
+    /* the bucketed sums unless turned off or past their rows */
+    const int m = c->rank_cap < 0 ? 0 : rb_buckets(n);
+    const int cap = c->rank_cap > 0 ? std::min(c->rank_cap, RB_CAP) : RB_CAP;
+    const int gmax = c->rank_gmax > 0 ? c->rank_gmax : RB_GMAX;
     StatPrep sp;
     size_t cur = 0;
     stat_inputs(c, prog, off, pcount, nsets, nsegs, kmax, c0, &cur, sp);
     const size_t o_out = rc_take(&cur, sizeof(u64) * 4 * (size_t)nsegs);
     const size_t o_status = rc_take(&cur, sizeof(int) * (size_t)nsegs);
+    const size_t o_ovf = rc_take(&cur, sizeof(int) * (size_t)nsegs);
     const size_t o_abort = rc_take(&cur, sizeof(int));
     const size_t io_end = rc_take(&cur, 0);
-    const int wseg = wave_segments(nsegs, n, true);
+    const int wseg = m > 0 ? rb_wave_segments(nsegs, n, m) : wave_segments(nsegs, n, true);
     const size_t work = cur;
-    if (rc_reserve(c, work + rs_bytes((size_t)wseg * n, wseg, n, true) + 4096, io_end) != 0)
-        return -1.0f;
+    const size_t wbytes = m > 0 ? std::max(rb_bytes(wseg, n, m), rs_bytes((size_t)n, 1, n, true))
+                                : rs_bytes((size_t)wseg * n, wseg, n, true);
+    if (rc_reserve(c, work + wbytes + 4096, io_end) != 0) return -1.0f;
     stat_copy(c, pcount, nsets, nsegs, kmax, c0, sp);
     unsigned char *dev = c->dev;
     int *d_status = reinterpret_cast<int *>(dev + o_status);
+    int *d_ovf = reinterpret_cast<int *>(dev + o_ovf);
     int *d_abort = reinterpret_cast<int *>(dev + o_abort);
+    u64 *d_out = reinterpret_cast<u64 *>(dev + o_out);
     cudaMemsetAsync(d_status, 0, sizeof(int) * nsegs, c->s);
+    cudaMemsetAsync(d_ovf, 0, sizeof(int) * nsegs, c->s);
     cudaMemsetAsync(d_abort, 0, sizeof(int), c->s);
     const size_t smem = key_smem(sp);
     if (rc_raise_smem((const void *)rk_keys<RK_RANK>, smem) != 0) return -1.0f;
+    if (m > 0 && (rc_raise_smem((const void *)rb_sample, smem) != 0 ||
+                  rc_raise_smem((const void *)rb_splitters, sizeof(u64) * RB_MAXS) != 0 ||
+                  rc_raise_smem((const void *)rb_local, rb_local_smem()) != 0))
+        return -1.0f;
     const int ktiles = (n + RK_TILE - 1) / RK_TILE;
     const int ntiles = (n + RS_TILE - 1) / RS_TILE;
-    cudaEventRecord(c->t0, c->s);
-    for (int s0 = 0; s0 < nsegs; s0 += wseg) {
-        const int ns = std::min(wseg, nsegs - s0);
+    const FIns *d_fins = reinterpret_cast<const FIns *>(dev + sp.o_fins);
+    const int *d_finsoff = reinterpret_cast<const int *>(dev + sp.o_finsoff);
+    const int4 *d_finfo = reinterpret_cast<const int4 *>(dev + sp.o_finfo);
+    const int *d_valid = reinterpret_cast<const int *>(dev + sp.o_valid);
+    const double *d_c0 = reinterpret_cast<const double *>(dev + sp.o_c0);
+    /* the radix-sort sums of segments [s0, s0 + ns) */
+    auto radix_wave = [&](int s0, int ns) {
         size_t wc = work;
         __int128 *part = nullptr;
         const RsBuffers b = rs_carve(dev, &wc, ns, n, true, &part);
         cudaMemsetAsync(b.count, 0, sizeof(unsigned int) * RS_PASSES * 256 * (size_t)ns, c->s);
         rk_keys<RK_RANK><<<(unsigned)ns * ktiles, RK_T, smem, c->s>>>(
-            reinterpret_cast<const FIns *>(dev + sp.o_fins),
-            reinterpret_cast<const int *>(dev + sp.o_finsoff),
-            reinterpret_cast<const int4 *>(dev + sp.o_finfo),
-            reinterpret_cast<const int *>(dev + sp.o_valid),
-            reinterpret_cast<const double *>(dev + sp.o_c0), kmax, c->d_cols64, c->d_y64, c->npad,
-            n, ntrials, s0, ktiles, sp.b.fmaxins, b.ka, b.va, b.count, d_status);
+            d_fins, d_finsoff, d_finfo, d_valid, d_c0, kmax, c->d_cols64, c->d_y64, c->npad, n,
+            ntrials, s0, ktiles, sp.b.fmaxins, b.ka, b.va, b.count, d_status);
         c->launches += 3 + rs_sort<true>(b, ns, n, d_abort, c->s, true);
         rk_runs<RK_SUMS><<<(unsigned)ns * ntiles, RS_T, 0, c->s>>>(
             b.ka, b.kb, b.va, b.vb, b.par, n, ntiles, c->d_rank_b, nullptr, part);
-        rk_final<<<ns, RS_T, 0, c->s>>>(part, ntiles,
-                                        reinterpret_cast<u64 *>(dev + o_out) + 4 * (size_t)s0);
+        rk_final<<<ns, RS_T, 0, c->s>>>(part, ntiles, d_out + 4 * (size_t)s0);
+    };
+    /* the bucketed sums of segments [s0, s0 + ns); a flagged segment is left
+       to the radix sort */
+    auto bucket_wave = [&](int s0, int ns) {
+        size_t wc = work;
+        const RbBuffers r = rb_carve(dev, &wc, ns, n, m);
+        cudaMemsetAsync(r.zero, 0, r.zero_bytes, c->s);
+        if (m > 1) {
+            const int S = RB_OVS * m;
+            int P2 = 1;
+            while (P2 < S) P2 <<= 1;
+            const int sblocks = (S / 2 + RK_T - 1) / RK_T;
+            rb_sample<<<(unsigned)ns * sblocks, RK_T, smem, c->s>>>(
+                d_fins, d_finsoff, d_finfo, d_valid, d_c0, kmax, c->d_cols64, c->npad, n, ntrials,
+                s0, sblocks, S, sp.b.fmaxins, r.samp);
+            rb_splitters<<<ns, RB_ST, sizeof(u64) * P2, c->s>>>(r.samp, S, P2, m, r.spl, r.nspl);
+            c->launches += 2;
+        } else {
+            cudaMemsetAsync(r.nspl, 0, sizeof(int) * ns, c->s);
+        }
+        rk_keys<RK_RANK><<<(unsigned)ns * ktiles, RK_T, smem, c->s>>>(
+            d_fins, d_finsoff, d_finfo, d_valid, d_c0, kmax, c->d_cols64, c->d_y64, c->npad, n,
+            ntrials, s0, ktiles, sp.b.fmaxins, r.keys, nullptr, nullptr, d_status);
+        const int ctiles = (n + RB_CT - 1) / RB_CT;
+        rb_scatter<<<(unsigned)ns * ctiles, RB_T, 0, c->s>>>(
+            r.keys, n, ctiles, m, cap, c->d_rank_b, r.spl, r.nspl, r.rcur, r.ecnt, r.esum, r.bkey,
+            r.bval, d_ovf + s0);
+        rb_scan<<<ns, RB_ST, 0, c->s>>>(n, cap, r.nspl, r.rcur, r.ecnt, r.esum, r.boff, r.part,
+                                        d_ovf + s0);
+        rb_local<<<(unsigned)ns * m, RB_T, rb_local_smem(), c->s>>>(
+            n, m, cap, gmax, r.nspl, r.rcur, r.boff, r.bkey, r.bval, r.part, d_ovf + s0);
+        rb_final<<<ns, RS_T, 0, c->s>>>(r.nspl, r.part, d_ovf + s0, d_out + 4 * (size_t)s0);
+        c->launches += 5;
+    };
+    cudaEventRecord(c->t0, c->s);
+    for (int s0 = 0; s0 < nsegs; s0 += wseg) {
+        const int ns = std::min(wseg, nsegs - s0);
+        if (m > 0) bucket_wave(s0, ns);
+        else radix_wave(s0, ns);
     }
     cudaEventRecord(c->t1, c->s);
     if (cudaGetLastError() != cudaSuccess) return -1.0f;
@@ -1015,6 +1619,24 @@ float rc_rank_score_batch(void *ctx, const unsigned int *prog, const unsigned in
                     cudaMemcpyDeviceToHost, c->s);
     if (rc_finish(c) != 0) return -1.0f;
     if (*reinterpret_cast<const int *>(c->host + o_abort) != 0) return -1.0f;
+    c->rank_fallbacks = m > 0 ? 0 : nsegs;
+    if (m > 0) {
+        /* segments the buckets could not take: the radix sort, one each */
+        const int *h_ovf = reinterpret_cast<const int *>(c->host + o_ovf);
+        std::vector<int> redo;
+        for (int s = 0; s < nsegs; ++s)
+            if (h_ovf[s]) redo.push_back(s);
+        if (!redo.empty()) {
+            for (int s : redo) radix_wave(s, 1);
+            cudaEventRecord(c->t1, c->s);
+            if (cudaGetLastError() != cudaSuccess) return -1.0f;
+            cudaMemcpyAsync(c->host + sp.in_end, dev + sp.in_end, io_end - sp.in_end,
+                            cudaMemcpyDeviceToHost, c->s);
+            if (rc_finish(c) != 0) return -1.0f;
+            if (*reinterpret_cast<const int *>(c->host + o_abort) != 0) return -1.0f;
+        }
+        c->rank_fallbacks = (int)redo.size();
+    }
     memcpy(out, c->host + o_out, sizeof(u64) * 4 * (size_t)nsegs);
     memcpy(out_status, c->host + o_status, sizeof(int) * (size_t)nsegs);
     out_bb[0] = c->rank_bb[0];
@@ -1022,6 +1644,21 @@ float rc_rank_score_batch(void *ctx, const unsigned int *prog, const unsigned in
     float ms = -1.0f;
     cudaEventElapsedTime(&ms, c->t0, c->t1);
     return ms;
+}
+
+int rc_rank_tuning(void *ctx, int bucket_cap, int group_max)
+{
+    RcCtx *c = (RcCtx *)ctx;
+    if (!c || bucket_cap < -1 || bucket_cap > RB_CAP || group_max < 0) return -1;
+    c->rank_cap = bucket_cap;
+    c->rank_gmax = group_max;
+    return 0;
+}
+
+int rc_rank_last_fallbacks(void *ctx)
+{
+    RcCtx *c = (RcCtx *)ctx;
+    return c ? c->rank_fallbacks : -1;
 }
 
 int rc_rank_debug_b(void *ctx, long long *out)

@@ -150,6 +150,12 @@ struct RcCtx {
     long long *d_rank_b;
     int rank_ready;
     unsigned long long rank_bb[2];
+    /* rank sums: bucket capacity (0 = built in, -1 = radix sort only), the
+       largest group of distinct keys ranked by comparison (0 = built in),
+       and the segments of the last call that took the radix sort */
+    int rank_cap;
+    int rank_gmax;
+    int rank_fallbacks;
 
     /* ledger and arena accounting */
     RcStats stats;

@@ -74,6 +74,8 @@ SIGNATURES = {
     "rc_rank_score_batch": (cf, [cvp, u32p, u32p, i32p, ci, ci, ci, f64p, u64p, i32p, u64p]),
     "rc_rank_debug_b": (ci, [cvp, i64p]),
     "rc_launch_count": (ci, [cvp, u64p]),
+    "rc_rank_tuning": (ci, [cvp, ci, ci]),
+    "rc_rank_last_fallbacks": (ci, [cvp]),
     "rc_last_fit_sweeps": (ci, [cvp, ci, ctypes.POINTER(ctypes.c_int32)]),
     "rc_multi_create": (cvp, [f32p, ci, ci, f32p, ci, i32p]),
     "rc_multi_destroy": (None, [cvp]),
@@ -340,6 +342,16 @@ class GpuEvaluator:
             else:
                 sums.append((_i128(out[4 * s], out[4 * s + 1]), _i128(out[4 * s + 2], out[4 * s + 3])))
         return sums, status, _i128(bb[0], bb[1]), ms
+
+    def rank_tuning(self, bucket_cap=0, group_max=0):
+        """Rank-sum method: bucket capacity (0 built in, -1 radix sort only)
+        and the largest group of distinct keys ranked by comparison."""
+        if lib().rc_rank_tuning(self.ctx, int(bucket_cap), int(group_max)) != 0:
+            raise ValueError("rc_rank_tuning refused its arguments")
+
+    def rank_fallbacks(self):
+        """Segments of the last rank_sums call that the radix sort summed."""
+        return int(lib().rc_rank_last_fallbacks(self.ctx))
 
     def rank_target(self):
         out = np.zeros(self.n, np.int64)
