@@ -704,10 +704,9 @@ __global__ void __launch_bounds__(RS_T) rk_final(const __int128 *part, int ntile
 #define RB_GMAX 48                 /* largest group of distinct keys ranked by comparison */
 static_assert((RB_CAP & (RB_CAP - 1)) == 0, "a sorted bucket pads to a power of two");
 #define RB_CT 4096                 /* keys per scatter block */
-#define RB_T 256
-#define RB_CR (RB_CT / RB_T)
+#define RB_CTT 256                 /* scatter threads */
+#define RB_CR (RB_CT / RB_CTT)
 #define RB_ST 1024 /* splitter and scan threads */
-static_assert(RB_T == RS_T, "the bucket kernels use the block sum of the run pass");
 static_assert(RB_CT <= 65536 && 2 * RB_MAXB <= 65536, "bucket and rank pack into 16 bits each");
 
 __device__ __forceinline__ unsigned rb_hash(unsigned a, unsigned b)
@@ -801,25 +800,12 @@ __global__ void __launch_bounds__(RB_ST) rb_splitters(const u64 *samp, int S, in
     }
 }
 
-/* Bucket b of a key among ns splitters: 2 * (splitters below it), plus one
-   when it equals the next splitter (an equality bucket). */
-__device__ __forceinline__ unsigned rb_bucket(const u64 *spl, int ns, u64 k)
-{
-    int lo = 0, hi = ns;
-    while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (spl[mid] < k) lo = mid + 1;
-        else hi = mid;
-    }
-    return 2u * (unsigned)lo + ((lo < ns && spl[lo] == k) ? 1u : 0u);
-}
-
 /* RB_CT keys per block: each key's bucket, the block's count per bucket (a
    key's rank among the block's keys of its bucket from the shared-memory
    count), one reservation per range bucket the block touches, then the
    range keys and their B written to their slots. Equality buckets only add
    counts and B sums. A slot at or past `cap` flags the segment. */
-__global__ void __launch_bounds__(RB_T) rb_scatter(const u64 *keys, int n, int ctiles, int m,
+__global__ void __launch_bounds__(RB_CTT, 3) rb_scatter(const u64 *keys, int n, int ctiles, int m,
                                                    int cap, const long long *B, const u64 *spl,
                                                    const int *nspl, unsigned *rcur,
                                                    unsigned *ecnt, unsigned long long *esum,
@@ -830,32 +816,52 @@ __global__ void __launch_bounds__(RB_T) rb_scatter(const u64 *keys, int n, int c
     __shared__ unsigned long long ssum[RB_MAXB];
     const int ls = blockIdx.x / ctiles, tile = blockIdx.x % ctiles, tid = threadIdx.x;
     const int ns = nspl[ls], nb = 2 * ns + 1;
-    for (int i = tid; i < ns; i += RB_T) {
+    for (int i = tid; i < ns; i += RB_CTT) {
         sspl[i] = spl[(size_t)ls * RB_MAXB + i];
         ssum[i] = 0ULL;
     }
-    for (int i = tid; i < nb; i += RB_T) hist[i] = 0u;
+    for (int i = tid; i < nb; i += RB_CTT) hist[i] = 0u;
     __syncthreads();
     const u64 *ks = keys + (size_t)ls * n;
     const int t0 = tile * RB_CT;
+    /* every key and its B loaded first, then all of them searched a level at
+       a time (the lower bound among the splitters by binary lifting), so
+       the loads and the shared-memory probes overlap */
     u64 key[RB_CR];
+    int bv[RB_CR];
     unsigned pk[RB_CR];
 #pragma unroll
     for (int r = 0; r < RB_CR; ++r) {
-        const int i = t0 + r * RB_T + tid;
-        pk[r] = 0xffffffffu;
-        key[r] = 0ULL;
-        if (i < n) {
-            const u64 k = ks[i];
-            const unsigned b = rb_bucket(sspl, ns, k);
-            const unsigned rank = atomicAdd(&hist[b], 1u);
-            if (b & 1u) atomicAdd(&ssum[b >> 1], (unsigned long long)B[i]);
-            key[r] = k;
-            pk[r] = (b << 16) | rank;
+        const int i = t0 + r * RB_CTT + tid;
+        const bool in = i < n;
+        key[r] = in ? ks[i] : 0ULL;
+        bv[r] = in ? (int)B[i] : 0;
+        pk[r] = 0u;
+    }
+    int top = 1;
+    while (top <= ns) top <<= 1;
+    for (int step = top >> 1; step > 0; step >>= 1) {
+#pragma unroll
+        for (int r = 0; r < RB_CR; ++r) {
+            const unsigned p = pk[r] + (unsigned)step;
+            if (p <= (unsigned)ns && sspl[p - 1] < key[r]) pk[r] = p;
         }
     }
+#pragma unroll
+    for (int r = 0; r < RB_CR; ++r) {
+        if (t0 + r * RB_CTT + tid >= n) {
+            pk[r] = 0xffffffffu;
+            continue;
+        }
+        const unsigned p = pk[r];
+        const bool eq = p < (unsigned)ns && sspl[p] == key[r];
+        const unsigned b = 2u * p + (eq ? 1u : 0u);
+        const unsigned rank = atomicAdd(&hist[b], 1u);
+        if (eq) atomicAdd(&ssum[p], (unsigned long long)(long long)bv[r]);
+        pk[r] = (b << 16) | rank;
+    }
     __syncthreads();
-    for (int b = tid; b < nb; b += RB_T) {
+    for (int b = tid; b < nb; b += RB_CTT) {
         const unsigned h = hist[b];
         if (!h) continue;
         const size_t j = (size_t)ls * RB_MAXB + (b >> 1);
@@ -880,7 +886,7 @@ __global__ void __launch_bounds__(RB_T) rb_scatter(const u64 *keys, int n, int c
         }
         const size_t slot = ((size_t)ls * m + (b >> 1)) * RB_CAP + pos;
         bkey[slot] = key[r];
-        bval[slot] = (int)B[t0 + r * RB_T + tid];
+        bval[slot] = bv[r];
     }
     if (over) ovf[ls] = 1;
 }
@@ -949,12 +955,34 @@ __host__ __device__ constexpr size_t rb_local_smem()
            RB_DIG;
 }
 
+/* Sum of a 64-bit integer over a block of NT threads: warp butterflies, then
+   warp partials in order (integers: exact in any order). Every thread gets
+   the sum; `ws` holds NT / 32 values. */
+template <int NT>
+__device__ __forceinline__ long long rb_block_sum64(long long v, long long *ws)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = v;
+    __syncthreads();
+    long long s = 0;
+#pragma unroll
+    for (int k = 0; k < NT / 32; ++k) s += ws[k];
+    __syncthreads();
+    return s;
+}
+
+#define RB_LT 512 /* rb_local threads */
+static_assert(RB_DIG == 2 * RB_LT, "two digit groups per thread");
+
 /* One block per (segment, range bucket): runs and partial sums of its c
-   keys, which hold positions [O, O + c) of the segment's order. */
-__global__ void __launch_bounds__(RB_T, 2) rb_local(int n, int m, int cap, int gmax,
-                                                    const int *nspl, const unsigned *rcur,
-                                                    const unsigned *boff, const u64 *bkey,
-                                                    const int *bval, __int128 *part, int *ovf)
+   keys, which hold positions [O, O + c) of the segment's order. A thread
+   holds at most RB_CAP / RB_LT keys, each |A * B| and A^2 at most n^2, so
+   per-thread and block sums fit 64 bits for the n this path takes. */
+__global__ void __launch_bounds__(RB_LT, 2) rb_local(int n, int m, int cap, int gmax,
+                                                     const int *nspl, const unsigned *rcur,
+                                                     const unsigned *boff, const u64 *bkey,
+                                                     const int *bval, __int128 *part, int *ovf)
 {
     extern __shared__ __align__(16) unsigned char sm[];
     u64 *sk = reinterpret_cast<u64 *>(sm);
@@ -962,15 +990,19 @@ __global__ void __launch_bounds__(RB_T, 2) rb_local(int n, int m, int cap, int g
     unsigned *gst = reinterpret_cast<unsigned *>(sv + RB_CAP);
     unsigned *cur = gst + RB_DIG + 1;
     unsigned char *mixed = reinterpret_cast<unsigned char *>(cur + RB_DIG);
-    __shared__ __int128 red[RB_T];
-    __shared__ u64 s_lo[RB_T / 32], s_hi[RB_T / 32];
-    __shared__ unsigned wsum[RB_T / 32];
+    __shared__ u64 s_lo[RB_LT / 32], s_hi[RB_LT / 32];
+    __shared__ unsigned wsum[RB_LT / 32];
+    __shared__ long long ws[RB_LT / 32];
     __shared__ int s_skip;
     const int ls = blockIdx.x / m, idx = blockIdx.x % m;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     /* other blocks of the segment may raise its flag meanwhile: one read,
        shared, so the whole block takes the same branch */
     if (tid == 0) s_skip = *(volatile const int *)(ovf + ls) || idx > nspl[ls];
+    for (int d = tid; d < RB_DIG; d += RB_LT) {
+        cur[d] = 0u;
+        mixed[d] = 0;
+    }
     __syncthreads();
     if (s_skip) return;
     const int c = (int)rcur[(size_t)ls * RB_MAXB + idx];
@@ -982,7 +1014,7 @@ __global__ void __launch_bounds__(RB_T, 2) rb_local(int n, int m, int cap, int g
     __int128 *pp = part + ((size_t)ls * 2 * RB_MAXB + 2 * idx) * 2;
 
     u64 lo = ~0ULL, hi = 0ULL;
-    for (int q = tid; q < c; q += RB_T) {
+    for (int q = tid; q < c; q += RB_LT) {
         const u64 k = bk[q];
         lo = k < lo ? k : lo;
         hi = k > hi ? k : hi;
@@ -998,15 +1030,15 @@ __global__ void __launch_bounds__(RB_T, 2) rb_local(int n, int m, int cap, int g
         s_hi[w] = hi;
     }
     __syncthreads();
-    for (int k = 0; k < RB_T / 32; ++k) {
+    for (int k = 0; k < RB_LT / 32; ++k) {
         lo = s_lo[k] < lo ? s_lo[k] : lo;
         hi = s_hi[k] > hi ? s_hi[k] : hi;
     }
     if (c == 0 || lo == hi) {
         /* one run [O, O + c) */
-        long long s = 0;
-        for (int q = tid; q < c; q += RB_T) s += bv[q];
-        const __int128 sb = rk_block_sum((__int128)s, red);
+        long long sb = 0;
+        for (int q = tid; q < c; q += RB_LT) sb += bv[q];
+        sb = rb_block_sum64<RB_LT>(sb, ws);
         if (tid == 0) {
             const long long A = 2 * O + c - n;
             pp[0] = (__int128)A * sb;
@@ -1016,21 +1048,10 @@ __global__ void __launch_bounds__(RB_T, 2) rb_local(int n, int m, int cap, int g
     }
     const int nbits = 64 - __clzll((long long)(hi - lo));
     const int shift = nbits > 10 ? nbits - 10 : 0;
-    for (int d = tid; d < RB_DIG; d += RB_T) {
-        cur[d] = 0u;
-        mixed[d] = 0;
-    }
-    __syncthreads();
-    for (int q = tid; q < c; q += RB_T) atomicAdd(&cur[(unsigned)((bk[q] - lo) >> shift)], 1u);
+    for (int q = tid; q < c; q += RB_LT) atomicAdd(&cur[(unsigned)((bk[q] - lo) >> shift)], 1u);
     __syncthreads();
     {
-        static_assert(RB_DIG == 4 * RB_T, "four digit groups per thread");
-        unsigned a[4], t = 0;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            a[k] = cur[4 * tid + k];
-            t += a[k];
-        }
+        const unsigned a0 = cur[2 * tid], a1 = cur[2 * tid + 1], t = a0 + a1;
         unsigned x = t;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -1041,33 +1062,29 @@ __global__ void __launch_bounds__(RB_T, 2) rb_local(int n, int m, int cap, int g
         __syncthreads();
         unsigned run = x - t;
         for (int k = 0; k < w; ++k) run += wsum[k];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            gst[4 * tid + k] = run;
-            cur[4 * tid + k] = run;
-            run += a[k];
-        }
+        gst[2 * tid] = run;
+        cur[2 * tid] = run;
+        gst[2 * tid + 1] = run + a0;
+        cur[2 * tid + 1] = run + a0;
         if (tid == 0) gst[RB_DIG] = (unsigned)c;
     }
     __syncthreads();
-    for (int q = tid; q < c; q += RB_T) {
+    for (int q = tid; q < c; q += RB_LT) {
         const u64 k = bk[q];
         const unsigned p = atomicAdd(&cur[(unsigned)((k - lo) >> shift)], 1u);
         sk[p] = k;
         sv[p] = bv[q];
     }
     __syncthreads();
-    for (int q = tid; q < c; q += RB_T) {
+    for (int q = tid; q < c; q += RB_LT) {
         const u64 k = sk[q];
         const unsigned d = (unsigned)((k - lo) >> shift);
         if (k != sk[gst[d]]) mixed[d] = 1;
     }
     __syncthreads();
-    /* per thread at most RB_CAP / RB_T keys, each |A * B| and A^2 at most n^2:
-       the thread's sums fit 64 bits for the n this path takes */
     long long ab = 0, aa = 0;
     bool big = false;
-    for (int q = tid; q < c; q += RB_T) {
+    for (int q = tid; q < c; q += RB_LT) {
         const u64 k = sk[q];
         const unsigned d = (unsigned)((k - lo) >> shift);
         const unsigned gs = gst[d], ge = gst[d + 1];
@@ -1097,14 +1114,14 @@ __global__ void __launch_bounds__(RB_T, 2) rb_local(int n, int m, int cap, int g
            INT_MIN) and take each key's run by binary search */
         int P2 = 1;
         while (P2 < c) P2 <<= 1;
-        for (int q = c + tid; q < P2; q += RB_T) {
+        for (int q = c + tid; q < P2; q += RB_LT) {
             sk[q] = ~0ULL;
             sv[q] = INT_MIN;
         }
         __syncthreads();
         for (int k = 2; k <= P2; k <<= 1)
             for (int j = k >> 1; j > 0; j >>= 1) {
-                for (int i = tid; i < P2; i += RB_T) {
+                for (int i = tid; i < P2; i += RB_LT) {
                     const int l = i ^ j;
                     if (l > i) {
                         const u64 a = sk[i], b = sk[l];
@@ -1122,15 +1139,15 @@ __global__ void __launch_bounds__(RB_T, 2) rb_local(int n, int m, int cap, int g
             }
         ab = 0;
         aa = 0;
-        for (int q = tid; q < c; q += RB_T) {
+        for (int q = tid; q < c; q += RB_LT) {
             const u64 k = sk[q];
             const long long A = 2 * O + rk_lower(sk, 0, c, k) + rk_upper(sk, 0, c, k) - n;
             ab += A * (long long)sv[q];
             aa += A * A;
         }
     }
-    const __int128 sab = rk_block_sum((__int128)ab, red);
-    const __int128 saa = rk_block_sum((__int128)aa, red);
+    const long long sab = rb_block_sum64<RB_LT>(ab, ws);
+    const long long saa = rb_block_sum64<RB_LT>(aa, ws);
     if (tid == 0) {
         pp[0] = sab;
         pp[1] = saa;
@@ -1597,12 +1614,12 @@ float rc_rank_score_batch(void *ctx, const unsigned int *prog, const unsigned in
             d_fins, d_finsoff, d_finfo, d_valid, d_c0, kmax, c->d_cols64, c->d_y64, c->npad, n,
             ntrials, s0, ktiles, sp.b.fmaxins, r.keys, nullptr, nullptr, d_status);
         const int ctiles = (n + RB_CT - 1) / RB_CT;
-        rb_scatter<<<(unsigned)ns * ctiles, RB_T, 0, c->s>>>(
+        rb_scatter<<<(unsigned)ns * ctiles, RB_CTT, 0, c->s>>>(
             r.keys, n, ctiles, m, cap, c->d_rank_b, r.spl, r.nspl, r.rcur, r.ecnt, r.esum, r.bkey,
             r.bval, d_ovf + s0);
         rb_scan<<<ns, RB_ST, 0, c->s>>>(n, cap, r.nspl, r.rcur, r.ecnt, r.esum, r.boff, r.part,
                                         d_ovf + s0);
-        rb_local<<<(unsigned)ns * m, RB_T, rb_local_smem(), c->s>>>(
+        rb_local<<<(unsigned)ns * m, RB_LT, rb_local_smem(), c->s>>>(
             n, m, cap, gmax, r.nspl, r.rcur, r.boff, r.bkey, r.bval, r.part, d_ovf + s0);
         rb_final<<<ns, RS_T, 0, c->s>>>(r.nspl, r.part, d_ovf + s0, d_out + 4 * (size_t)s0);
         c->launches += 5;
