@@ -129,12 +129,12 @@ SCORE_TRAFFIC = 25.69e6
 FIT_ASM_TRAFFIC = {"bytes_per_candidate_row_f32_assembly": 15.0,
                    "source": "profiles/ft_sweep4_classes_fit_P256_N1M.md"}
 # DRAM bytes per candidate*row of the whole rank stage, from the per-kernel
-# ncu launch list of profiles/rank_stage_P16_N1M.md (the digit count in the
-# key kernel): 10,781 MB over 3 calls of 16 x 1,048,576 rows -- the key
-# kernel's column reads and key and row writes (about 32 B), eight sort
-# passes at about 21.7 B per key, the run pass (about 12.5 B).
-RANK_TRAFFIC = {"bytes_per_candidate_row": 214.0, "algorithmic": 32.0,
-                "source": "profiles/rank_stage_P16_N1M.md"}
+# ncu launch list of profiles/rank_buckets_P16_N1M_P100_N4M.md (bucketed
+# sums): 2,847 MB over 3 calls of 16 x 1,048,576 rows -- the key kernel's
+# column reads and key writes (19.2 B), the bucket scatter (24.1 B), the
+# local ranking pass (12.1 B), sampling and splitters (1.1 B).
+RANK_TRAFFIC = {"bytes_per_candidate_row": 56.6, "algorithmic": 32.0,
+                "source": "profiles/rank_buckets_P16_N1M_P100_N4M.md"}
 
 
 def flush_l2(buf):
