@@ -704,12 +704,16 @@ def rank_stage(pkg, ev, plans, N, flushbuf, steps, warmup):
     per_call = max(1, 0x7FFFFFFF // N)
     chunks = [pkg.pack_plans(plans[s:s + per_call]) for s in range(0, P, per_call)]
 
+    fb = [0]
+
     def run():
         ms, st = 0.0, []
+        fb[0] = 0
         for cp, co, cc, c0_, _, km in chunks:
             _, s, _, m = ev.rank_sums(cp, co, cc, c0_, km)
             ms += m
             st.append(s)
+            fb[0] += ev.rank_fallbacks()
         return np.concatenate(st), ms
 
     ev.rank_target()
@@ -725,6 +729,20 @@ def rank_stage(pkg, ev, plans, N, flushbuf, steps, warmup):
         wall.append(time.perf_counter() - t0)
         dev_ms.append(ms)
     launches = ev.launch_count() - n0
+    fallbacks = fb[0]
+    # the same calls through the eight-pass radix sort (the bucketed sums'
+    # fallback), timed beside them; the sums must be the same bits
+    sums_b = [sm for cp, co, cc, c0_, _, km in chunks[:1]
+              for sm in ev.rank_sums(cp, co, cc, c0_, km)[0]]
+    ev.rank_tuning(-1, 0)
+    radix_ms = []
+    for k in range(2):
+        flush_l2(flushbuf)
+        torch.cuda.synchronize()
+        radix_ms.append(run()[1])
+    sums_r = [sm for cp, co, cc, c0_, _, km in chunks[:1]
+              for sm in ev.rank_sums(cp, co, cc, c0_, km)[0]]
+    ev.rank_tuning(0, 0)
     rows = float(P) * N
     per = float(np.mean(dev_ms)) / 1e3
     achieved = 32.0 * rows / per / 1e9
@@ -735,6 +753,11 @@ def rank_stage(pkg, ev, plans, N, flushbuf, steps, warmup):
                            for c in chunks)),
             "d2h": int(P * (4 * 8 + 4) + 16 * len(chunks)), "calls_per_step": len(chunks),
             "finite_segments": int((status == 0).sum()),
+            "method": "bucketed sums (sample splitters, one scatter, per-bucket ranking)",
+            "radix_fallback_segments": fallbacks,
+            "radix_sort_ms_per_step": float(np.median(radix_ms)),
+            "bucketed_over_radix": float(np.median(radix_ms)) / (1e3 * per),
+            "same_sums_as_radix": sums_b == sums_r,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": RANK_TRAFFIC,
                          "note": "algorithmic 32 B per candidate*row (f64 eval, 8 B key, 4 B "
