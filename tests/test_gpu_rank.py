@@ -274,3 +274,22 @@ def test_rank_sums_on_the_radix_fallback(pkg, E, O, cap, gmax):
     sums2, _, _, _ = ev.rank_sums(prog, off, pcount, c0, kmax)
     assert sums2 == sums
     ev.close()
+
+
+@pytest.mark.parametrize("n,bucketed", [(4194304, True), (4194305, False)])
+def test_rank_sums_at_the_bucket_row_limit(pkg, E, n, bucketed):
+    """4,194,304 rows is the largest segment the buckets take (2,048 range
+    buckets, 16,384 samples); one row more goes to the radix sort for every
+    segment. Either way the sums equal the radix sort's bit for bit."""
+    cols, y = _fixture4(n, seed=3)
+    ev = _evaluator(pkg, cols, y)
+    trees = _bucket_models(E)
+    plans, prog, off, pcount, c0, kmax = _pack(pkg, trees)
+    sums, status, _, _ = ev.rank_sums(prog, off, pcount, c0, kmax)
+    assert list(status) == [0] * len(trees)
+    assert ev.rank_fallbacks() == (0 if bucketed else len(trees))
+    ev.rank_tuning(-1, 0)
+    sums_r, _, _, _ = ev.rank_sums(prog, off, pcount, c0, kmax)
+    assert ev.rank_fallbacks() == len(trees)
+    assert sums == sums_r
+    ev.close()
