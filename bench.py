@@ -1063,7 +1063,9 @@ def secondary(args, rank, world, local, pkg, W, flushbuf, peaks, line):
                 c5_fused_over_plain=fs["fused_over_plain"],
                 c5_fit_roofline_frac=fs["roofline"]["frac"], c5_fit_cpu_baseline=_cpu(fs),
                 c5_rank=rk["value"], c5_rank_e2e=rk["e2e"],
-                c5_rank_roofline_frac=rk["roofline"]["frac"], c5_rank_cpu_baseline=_cpu(rk))
+                c5_rank_roofline_frac=rk["roofline"]["frac"], c5_rank_cpu_baseline=_cpu(rk),
+                c5_rank_bucketed_over_radix=rk["bucketed_over_radix"],
+                c5_rank_same_sums_as_radix=rk["same_sums_as_radix"])
     c1 = line["c1"] = bench_c1(pkg, W)
     line.update(c1_generations_per_s=c1["generations_per_s"],
                 c1_fitted_candidates_per_s=c1["fitted_candidates_per_s"],
