@@ -142,6 +142,16 @@ def test_fit_kernel_info_contract(pkg):
     assert L.rc_fit_kernel_info(21, ctypes.byref(t), ctypes.byref(s), ctypes.byref(m)) == -1
 
 
+def test_rank_method_switch_refuses_bad_arguments(pkg):
+    """rc_rank_tuning and rc_rank_last_fallbacks return -1 on a null context
+    (no device needed)."""
+    L = pkg.cuda_lib()
+    L.rc_rank_tuning.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+    L.rc_rank_last_fallbacks.argtypes = [ctypes.c_void_p]
+    assert L.rc_rank_tuning(None, 0, 0) == -1
+    assert L.rc_rank_last_fallbacks(None) == -1
+
+
 def test_fit_admission_rules(pkg):
     """search.rs:3006-3074: admission_count and select_promoted."""
     H = importlib.import_module("the-rule-and-compass_b200.host")

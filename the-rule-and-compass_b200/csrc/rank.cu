@@ -6,14 +6,19 @@
  *
  * Rank sums. A (candidate, trial) segment's f64 predictions over all n rows
  * become order-preserving u64 keys (-0 folded onto +0, anything not finite
- * onto the largest key). A segmented LSD radix sort (8-bit digits, one
- * kernel per pass with decoupled look-back, a pass whose digit is constant
- * over a segment skipped) orders them with the row as payload. One pass over the sorted keys then gives every position q its
- * run [i, j) of equal keys, twice its centred average rank A = i + j - n,
- * and the exact sums sum A * B[row] and sum A^2 in 128-bit integers, B being
- * the target's own A (computed once per context the same way). Integer sums
- * do not depend on order, so the result is bit-identical to the CPU's
- * `RankTarget::sums` (metrics.rs:1359-1416) for the same predictions.
+ * onto the largest key). Every position q needs its run [i, j) of equal keys
+ * in sorted order, twice its centred average rank A = i + j - n, and the
+ * exact sums sum A * B[row] and sum A^2 in 128-bit integers, B being the
+ * target's own A. By default (up to 4,194,304 rows) the keys are cut into
+ * buckets by splitters from a sorted sample and each bucket is ranked on its
+ * own (the bucketed sums below). The radix path, which ranks the target once
+ * per context, takes segments whose bucket overflows and serves the order
+ * statistics, is a segmented LSD radix sort (8-bit digits, one kernel per
+ * pass with decoupled look-back, a pass whose digit is constant over a
+ * segment skipped) with the row as payload, then one pass over the sorted
+ * keys for the runs. Integer sums do not depend on order, so either path is
+ * bit-identical to the CPU's `RankTarget::sums` (metrics.rs:1359-1416) for
+ * the same predictions.
  *
  * Order statistics sort the bit patterns of |pred - y| (non-negative, so
  * they order like the values) and pick the median or average the
